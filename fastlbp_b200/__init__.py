@@ -1,0 +1,11 @@
+"""B200-native causal loopy belief propagation (drop-in for FastLBP's CausalBP PARALL path).
+
+The product is the shared library libfastlbp_b200.so (CUDA sm_100a kernels,
+the C ABI of include/fastlbp_b200.h and the libDAI-style C++ API of
+include/ext/*.h). This package loads it with ctypes.
+"""
+
+from .api import CausalBP, CausalFactorGraph, Engine, PropertySet  # noqa: F401
+from ._native import FlbpError, lib  # noqa: F401
+
+__all__ = ["CausalBP", "CausalFactorGraph", "Engine", "PropertySet", "FlbpError", "lib"]

@@ -1,0 +1,336 @@
+"""Python mirror of the drop-in API, over the C ABI.
+
+Names and argument meanings follow FastLBP's C++ classes
+(include/ext/causal_fg.h, include/ext/causal_bp.h, include/lbp/properties.h):
+``CausalFactorGraph.ReadFromFile / clamp / nrVars ...``, ``CausalBP(fg, opts)``,
+``init()``, the three ``run`` forms, ``newBelief`` and ``belief``. Errors raise
+``FlbpError`` instead of exiting the process.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from typing import Dict, Optional, Sequence
+
+import numpy as np
+
+from . import _native as N
+from ._native import check, lib
+
+_CLEANUP = {}
+
+
+class PropertySet(dict):
+    """String-keyed parameters (include/lbp/properties.h:21-59)."""
+
+    def set(self, key, val):
+        self[key] = val
+        return self
+
+    def hasKey(self, key):  # noqa: N802 (reference name)
+        return key in self
+
+    def getStringAs(self, typ, key):  # noqa: N802
+        v = self[key]
+        if isinstance(v, typ) and not (typ is int and isinstance(v, bool)):
+            return v
+        print("get properties error")
+        return typ()
+
+
+class CausalFactorGraph:
+    """A causal factor graph held by the library (include/ext/causal_fg.h)."""
+
+    def __init__(self, handle=None):
+        self._h = handle
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                lib().flbp_fg_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    # construction ---------------------------------------------------------
+    @classmethod
+    def read_file(cls, path: str) -> "CausalFactorGraph":
+        h = C.c_void_p()
+        check(lib().flbp_fg_read_file(path.encode(), C.byref(h)))
+        return cls(h)
+
+    def ReadFromFile(self, path: str) -> None:  # noqa: N802
+        other = CausalFactorGraph.read_file(path)
+        self._h, other._h = other._h, None
+
+    @classmethod
+    def from_text(cls, text: str) -> "CausalFactorGraph":
+        h = C.c_void_p()
+        check(lib().flbp_fg_read_string(text.encode(), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_factors(cls, fl) -> "CausalFactorGraph":
+        """From a ``workloads.FactorList`` (CausalFactorGraph(std::vector<CausalFactor>))."""
+        h = C.c_void_p()
+        check(lib().flbp_fg_from_factors(
+            fl.n, np.ascontiguousarray(fl.kind, np.int32), np.ascontiguousarray(fl.head, np.int64),
+            np.ascontiguousarray(fl.body_off, np.int64), np.ascontiguousarray(fl.body, np.int64),
+            np.ascontiguousarray(fl.p, np.float64), np.ascontiguousarray(fl.q, np.float64), C.byref(h)))
+        return cls(h)
+
+    def rebuild(self) -> "CausalFactorGraph":
+        """CausalFactorGraph(fg.factors()): the topology after clamps (fl_wrapper.cu:45)."""
+        h = C.c_void_p()
+        check(lib().flbp_fg_rebuild(self._h, C.byref(h)))
+        return CausalFactorGraph(h)
+
+    # queries --------------------------------------------------------------
+    def _sizes(self):
+        c = np.zeros(4, np.int64)
+        check(lib().flbp_fg_sizes(self._h, c))
+        return c
+
+    def nrVars(self):  # noqa: N802
+        return int(self._sizes()[0])
+
+    def nrFactors(self):  # noqa: N802
+        return int(self._sizes()[1])
+
+    def nrEdges(self):  # noqa: N802
+        return int(self._sizes()[2])
+
+    def nrSlots(self):  # noqa: N802
+        return int(self._sizes()[3])
+
+    def var_labels(self) -> np.ndarray:
+        out = np.zeros(self.nrVars(), np.int64)
+        check(lib().flbp_fg_var_labels(self._h, out, out.size))
+        return out
+
+    def findVar(self, label: int) -> int:  # noqa: N802
+        labels = self.var_labels()
+        i = int(np.searchsorted(labels, label))
+        return i if i < labels.size and labels[i] == label else labels.size
+
+    def factor_info(self) -> Dict[str, np.ndarray]:
+        F, S = self.nrFactors(), self.nrSlots()
+        d = dict(type=np.zeros(F, np.int32), head=np.zeros(F, np.int64), p=np.zeros(F), q=np.zeros(F),
+                 clamped=np.zeros(F, np.int32), mask0=np.zeros(F), mask1=np.zeros(F),
+                 vars_off=np.zeros(F + 1, np.int64), vars=np.zeros(S, np.int64))
+        check(lib().flbp_fg_factors(self._h, d["type"], d["head"], d["p"], d["q"], d["clamped"], d["mask0"],
+                                    d["mask1"], d["vars_off"], d["vars"]))
+        d["nvars"] = np.diff(d["vars_off"])
+        return d
+
+    def neighbors(self, factor_side: bool):
+        n = self.nrFactors() if factor_side else self.nrVars()
+        E = self.nrEdges()
+        off = np.zeros(n + 1, np.int64)
+        node, it, du = (np.zeros(E, np.int64) for _ in range(3))
+        check(lib().flbp_fg_neighbors(self._h, 1 if factor_side else 0, off, node, it, du))
+        return off, node, it, du
+
+    def construct(self) -> Dict[str, np.ndarray]:
+        """Reference-order arrays of CausalBP::construct() (causal_bp.cu:310-407)."""
+        F, V, S = self.nrFactors(), self.nrVars(), self.nrSlots()
+        d = dict(factor_offsets=np.zeros(F + 1, np.int64), slot_var=np.zeros(S, np.int64),
+                 factor_head=np.zeros(F, np.int64), row_ptr_fv=np.zeros(V + 1, np.int64),
+                 col_ind_fv=np.zeros(S, np.int64))
+        check(lib().flbp_fg_construct(self._h, d["factor_offsets"], d["slot_var"], d["factor_head"],
+                                      d["row_ptr_fv"], d["col_ind_fv"]))
+        return d
+
+    def graph_arrays(self) -> Dict[str, np.ndarray]:
+        """Everything flbp_engine_create() takes, as numpy arrays."""
+        c = self.construct()
+        f = self.factor_info()
+        return dict(n_vars=self.nrVars(), factor_offsets=c["factor_offsets"], slot_var=c["slot_var"],
+                    factor_head=c["factor_head"], factor_type=f["type"], factor_p=f["p"], factor_q=f["q"],
+                    factor_head_clamped=f["clamped"], factor_mask0=f["mask0"], factor_mask1=f["mask1"])
+
+    # evidence -------------------------------------------------------------
+    def clamp(self, i: int, x: int) -> None:
+        check(lib().flbp_fg_clamp(self._h, int(i), int(x)))
+
+    def clamp_labels(self, clamps: Dict[int, int]) -> None:
+        """fl_wrapper's loop: each (label, value) in ascending label order (fl_wrapper.cu:29-43)."""
+        labels = self.var_labels()
+        for lab in sorted(clamps):
+            i = int(np.searchsorted(labels, lab))
+            if i < labels.size and labels[i] == lab:
+                self.clamp(i, clamps[lab])
+
+
+def _desc_from_arrays(a: Dict[str, np.ndarray], keep: list) -> N.GraphDesc:
+    def ptr(name, dt):
+        v = a.get(name)
+        if v is None:
+            return None
+        arr = np.ascontiguousarray(v, dt)
+        keep.append(arr)
+        return arr.ctypes.data
+
+    off = np.ascontiguousarray(a["factor_offsets"], np.int64)
+    keep.append(off)
+    d = N.GraphDesc()
+    d.n_vars = int(a["n_vars"])
+    d.n_factors = off.size - 1
+    d.n_slots = int(off[-1]) if off.size else 0
+    d.factor_offsets = off.ctypes.data
+    d.slot_var = ptr("slot_var", np.int64)
+    d.factor_head = ptr("factor_head", np.int64)
+    d.factor_type = ptr("factor_type", np.int32)
+    d.factor_p = ptr("factor_p", np.float64)
+    d.factor_q = ptr("factor_q", np.float64)
+    d.factor_head_clamped = ptr("factor_head_clamped", np.int32)
+    d.factor_mask0 = ptr("factor_mask0", np.float64)
+    d.factor_mask1 = ptr("factor_mask1", np.float64)
+    return d
+
+
+class Engine:
+    """The C-ABI engine over reference-order graph arrays (flbp_engine_*)."""
+
+    def __init__(self, arrays: Dict[str, np.ndarray], precision: int = 32, damping: float = 0.0,
+                 stream: Optional[int] = None, device: int = -1):
+        keep = []
+        desc = _desc_from_arrays(arrays, keep)
+        opts = N.EngineOpts(int(precision), int(device), float(damping), stream)
+        h = C.c_void_p()
+        check(lib().flbp_engine_create(C.byref(desc), C.byref(opts), C.byref(h)))
+        self._h = h
+        self.n_vars = int(desc.n_vars)
+        self.n_slots = int(desc.n_slots)
+        self.info = None
+
+    @classmethod
+    def from_graph(cls, fg: CausalFactorGraph, **kw) -> "Engine":
+        return cls(fg.graph_arrays(), **kw)
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().flbp_engine_destroy(h)
+            self._h = None
+
+    __del__ = close
+
+    def init(self):
+        check(lib().flbp_init(self._h))
+
+    def sweep(self, n: int = 1):
+        check(lib().flbp_sweep(self._h, int(n)))
+
+    def _info(self):
+        self.info = N.RunInfo()
+        return C.byref(self.info)
+
+    def run_tol(self, tol=1e-9, maxiter=10000, maxtime=10.0):
+        check(lib().flbp_run_tol(self._h, float(tol), int(maxiter), float(maxtime), self._info()))
+        return self.info.as_dict()
+
+    def run_fixed(self, sweeps: int):
+        check(lib().flbp_run_fixed(self._h, int(sweeps), self._info()))
+        return self.info.as_dict()
+
+    def run_lowpass(self, tol, min_iters, max_iters, hist, maxtime=1e9):
+        check(lib().flbp_run_lowpass(self._h, float(tol), int(min_iters), int(max_iters), int(hist),
+                                     float(maxtime), self._info()))
+        return self.info.as_dict()
+
+    def beliefs(self) -> np.ndarray:
+        out = np.zeros(self.n_vars)
+        check(lib().flbp_get_beliefs(self._h, out, out.size))
+        return out
+
+    def lowpass(self) -> np.ndarray:
+        out = np.zeros(self.n_vars)
+        check(lib().flbp_get_lowpass(self._h, out, out.size))
+        return out
+
+    def compute_beliefs(self) -> np.ndarray:
+        out = np.zeros(self.n_vars)
+        check(lib().flbp_compute_beliefs(self._h, out, out.size))
+        return out
+
+    def fv_messages(self):
+        m0, m1 = np.zeros(self.n_slots), np.zeros(self.n_slots)
+        check(lib().flbp_get_fv_messages(self._h, m0, m1, self.n_slots))
+        return m0, m1
+
+    def vf_messages(self):
+        m0, m1 = np.zeros(self.n_slots), np.zeros(self.n_slots)
+        check(lib().flbp_get_vf_messages(self._h, m0, m1, self.n_slots))
+        return m0, m1
+
+    def stats(self) -> Dict[str, int]:
+        c = np.zeros(8, np.int64)
+        check(lib().flbp_engine_stats(self._h, c, c.size))
+        keys = ["vars", "factors", "slots", "active_factors", "active_slots", "warp_factors", "warp_vars", "bytes"]
+        return dict(zip(keys, (int(x) for x in c)))
+
+    def last_run_ms(self) -> float:
+        v = C.c_double()
+        check(lib().flbp_last_run_ms(self._h, C.byref(v)))
+        return v.value
+
+
+class CausalBP:
+    """CausalBP(fg, opts) with the reference's run semantics (include/ext/causal_bp.h:167-193)."""
+
+    def __init__(self, fg: CausalFactorGraph, opts: PropertySet):
+        self.fg = fg
+        get = lambda k, d: opts[k] if k in opts else d
+        self.tol = float(get("tol", 1e-9))
+        self.maxiter = int(get("maxiter", 10000))
+        self.maxtime = float(get("maxtime", 10.0))
+        self.updates = get("updates", "SEQFIX")
+        prec = str(get("precision", "FP32")).upper()
+        self.engine = Engine.from_graph(fg, precision=64 if prec == "FP64" else 32,
+                                        damping=float(get("damping", 0.0)))
+        self._beliefs = np.zeros(self.engine.n_vars)
+        self._lowpass = None
+        self._iters = 0
+
+    def init(self):
+        self.engine.init()
+
+    def run(self, *args):
+        if len(args) == 0:  # run(): tolerance loop with the properties
+            info = self.engine.run_tol(self.tol, self.maxiter, self.maxtime)
+            self._beliefs = self.engine.beliefs()
+            self._lowpass = self._beliefs.copy()
+            self._iters = info["total_sweeps"]
+            return None
+        if len(args) == 3:  # run(tol, maxIters, histLength)
+            info = self.engine.run_fixed(int(args[1]))
+            self._beliefs = self.engine.beliefs()
+            self._lowpass = self.engine.lowpass()
+            self._iters = info["total_sweeps"]
+            return 1.0
+        if len(args) == 4:  # run(tol, minIters, maxIters, histLength)
+            info = self.engine.run_lowpass(args[0], args[1], args[2], args[3], self.maxtime)
+            self._beliefs = self.engine.beliefs()
+            self._lowpass = self.engine.lowpass()
+            self._iters = info["total_sweeps"]
+            return info["frac"]
+        raise TypeError("run() takes 0, 3 or 4 arguments")
+
+    def newBelief(self, i: int) -> float:  # noqa: N802
+        return float(self._lowpass[i])
+
+    def belief(self, i: int):
+        b = float(self._beliefs[i])
+        return (1.0 - b, b)
+
+    def beliefs(self) -> np.ndarray:
+        return self._beliefs.copy()
+
+    def lowpass_beliefs(self) -> np.ndarray:
+        return None if self._lowpass is None else self._lowpass.copy()
+
+    @property
+    def iterations(self) -> int:
+        return self._iters

@@ -1,0 +1,821 @@
+// C-ABI engine: device buffers, sweep launches, the three run loops of
+// CausalBP and host exports. Kernels live in kernels.cuh.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "engine_internal.h"
+#include "kernels.cuh"
+
+namespace flbp {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+#define FLBP_CUDA(call)                                                                             \
+    do {                                                                                            \
+        cudaError_t err_ = (call);                                                                  \
+        if (err_ != cudaSuccess) {                                                                  \
+            set_error(std::string("CUDA error: ") + cudaGetErrorString(err_) + " at " #call);      \
+            return err_ == cudaErrorMemoryAllocation ? FLBP_ERR_NOMEM : FLBP_ERR_CUDA;              \
+        }                                                                                           \
+    } while (0)
+
+}  // namespace flbp
+
+using namespace flbp;
+
+struct flbp_engine {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int prec = 32;
+    double damping = 0.0;
+    HostLayout L;
+    size_t tsize = 4;
+
+    void *d_vf = nullptr, *d_fv = nullptr, *d_f_pq = nullptr;
+    uint32_t *d_fg_base = nullptr, *d_fb_off = nullptr, *d_vg_base = nullptr, *d_vb_off = nullptr, *d_v_ent = nullptr;
+    uint32_t *d_ftiles = nullptr, *d_vtiles = nullptr;  // 16-word headers per tile
+    uint32_t f_tile_blocks = 0, v_tile_blocks = 0;
+    uint8_t *d_f_kind = nullptr, *d_f_deg = nullptr;
+    void *d_prior = nullptr;
+    double *d_belief = nullptr, *d_lowpass = nullptr, *d_hist = nullptr;
+    double *d_scratch = nullptr;  // beliefs evaluated on demand (leave the run state untouched)
+    uint32_t *d_hist_next = nullptr, *d_hist_count = nullptr;
+    uint32_t hist_cap = 0;
+    Ctl *d_ctl = nullptr;
+    Ctl *h_ctl = nullptr;  // pinned mirror
+
+    int factor_grid = 1, var_grid = 1;
+    std::map<std::pair<int, int>, cudaGraphExec_t> graphs;  // (mode, sweeps) -> executable graph
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_ms = 0.f;
+
+    long long iters = 0;   // the reference's _iters (sweeps since construction)
+    long long t = 0;       // sweeps since init()
+    long long launches = 0;
+    bool lowpass_valid = false;
+    size_t bytes = 0;
+};
+
+namespace {
+
+template <typename T>
+FactorArgs factor_args(flbp_engine *e) {
+    FactorArgs a;
+    a.fg_base = e->d_fg_base;
+    a.fb_off = e->d_fb_off;
+    a.f_kind = e->d_f_kind;
+    a.f_deg = e->d_f_deg;
+    a.f_pq = e->d_f_pq;
+    a.nf_sell = e->L.nf_sell;
+    a.nf_big = e->L.nf_big;
+    a.n_fgroups = e->L.n_fgroups();
+    a.thdr = reinterpret_cast<const uint4 *>(e->d_ftiles);
+    a.n_tiles = (uint32_t)e->L.ftiles.size() - 1;
+    a.n_tile_blocks = e->f_tile_blocks;
+    return a;
+}
+
+VarArgs var_args(flbp_engine *e) {
+    VarArgs a;
+    a.vg_base = e->d_vg_base;
+    a.vb_off = e->d_vb_off;
+    a.v_ent = e->d_v_ent;
+    a.prior = e->d_prior;
+    a.belief = e->d_belief;
+    a.hist = e->d_hist;
+    a.hist_next = e->d_hist_next;
+    a.hist_count = e->d_hist_count;
+    a.nv_sell = e->L.nv_sell;
+    a.nv_big = e->L.nv_big;
+    a.n_vgroups = e->L.n_vgroups();
+    a.thdr = reinterpret_cast<const uint4 *>(e->d_vtiles);
+    a.n_tiles = (uint32_t)e->L.vtiles.size() - 1;
+    a.n_tile_blocks = e->v_tile_blocks;
+    a.hist_len = e->hist_cap;
+    return a;
+}
+
+constexpr int kStages = 3;          // bulk-copy pipeline depth of both passes
+constexpr int kBlockThreads = 288;  // 8 consumer warps + 1 producer warp
+
+template <typename T, bool DAMP>
+constexpr size_t factor_smem() {
+    return (size_t)kStages * FactorStage<T, DAMP>::bytes;
+}
+
+template <typename T>
+constexpr size_t var_smem() {
+    return (size_t)kStages * VarStage<T>::bytes;
+}
+
+// Opt every kernel instantiation of precision T into its dynamic shared
+// memory size; returns the resident blocks per SM of the factor and
+// variable passes.
+template <typename T>
+cudaError_t configure_kernels(int *fb, int *vb) {
+    cudaError_t err = cudaSuccess;
+    auto set = [&](const void *fn, size_t bytes) {
+        cudaError_t e2 = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e2 != cudaSuccess) err = e2;
+    };
+    set((const void *)factor_pass_kernel<T, true, kStages>, factor_smem<T, true>());
+    set((const void *)factor_pass_kernel<T, false, kStages>, factor_smem<T, false>());
+    set((const void *)var_pass_kernel<T, 0, true, kStages>, var_smem<T>());
+    set((const void *)var_pass_kernel<T, 1, true, kStages>, var_smem<T>());
+    set((const void *)var_pass_kernel<T, 2, true, kStages>, var_smem<T>());
+    set((const void *)var_pass_kernel<T, 3, false, kStages>, var_smem<T>());
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(fb, factor_pass_kernel<T, true, kStages>, kBlockThreads,
+                                                  factor_smem<T, true>());
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(vb, var_pass_kernel<T, 2, true, kStages>, kBlockThreads,
+                                                  var_smem<T>());
+    return err;
+}
+
+// mode 0: bare sweep; 1: tolerance loop sweep; 2: low-pass loop sweep.
+template <typename T>
+void launch_sweep(flbp_engine *e, int mode) {
+    const T d = (T)e->damping;
+    const T *vf_c = (const T *)e->d_vf;
+    T *vf = (T *)e->d_vf;
+    T *fv = (T *)e->d_fv;
+    const FactorArgs fa = factor_args<T>(e);
+    const VarArgs va = var_args(e);
+    if (e->damping != 0.0)
+        factor_pass_kernel<T, true, kStages>
+            <<<e->factor_grid, kBlockThreads, factor_smem<T, true>(), e->stream>>>(fa, vf_c, fv, d, e->d_ctl);
+    else
+        factor_pass_kernel<T, false, kStages>
+            <<<e->factor_grid, kBlockThreads, factor_smem<T, false>(), e->stream>>>(fa, vf_c, fv, d, e->d_ctl);
+    if (mode == 0)
+        var_pass_kernel<T, 0, true, kStages><<<e->var_grid, kBlockThreads, var_smem<T>(), e->stream>>>(va, fv, vf, e->d_ctl);
+    else if (mode == 1)
+        var_pass_kernel<T, 1, true, kStages><<<e->var_grid, kBlockThreads, var_smem<T>(), e->stream>>>(va, fv, vf, e->d_ctl);
+    else
+        var_pass_kernel<T, 2, true, kStages><<<e->var_grid, kBlockThreads, var_smem<T>(), e->stream>>>(va, fv, vf, e->d_ctl);
+}
+
+void launch_sweep_any(flbp_engine *e, int mode) {
+    if (e->prec == 64) launch_sweep<double>(e, mode);
+    else launch_sweep<float>(e, mode);
+}
+
+void launch_beliefs_only(flbp_engine *e, double *dst) {
+    VarArgs a = var_args(e);
+    a.belief = dst;
+    if (e->prec == 64)
+        var_pass_kernel<double, 3, false, kStages><<<e->var_grid, kBlockThreads, var_smem<double>(), e->stream>>>(
+            a, (const double *)e->d_fv, (double *)e->d_vf, e->d_ctl);
+    else
+        var_pass_kernel<float, 3, false, kStages><<<e->var_grid, kBlockThreads, var_smem<float>(), e->stream>>>(
+            a, (const float *)e->d_fv, (float *)e->d_vf, e->d_ctl);
+    e->launches += 1;
+}
+
+// Executable graph of `n` consecutive sweeps of a mode, captured once.
+int sweep_graph(flbp_engine *e, int mode, int n, cudaGraphExec_t *out) {
+    auto key = std::make_pair(mode, n);
+    auto it = e->graphs.find(key);
+    if (it != e->graphs.end()) {
+        *out = it->second;
+        return FLBP_OK;
+    }
+    cudaGraph_t g = nullptr;
+    FLBP_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < n; i++) launch_sweep_any(e, mode);
+    FLBP_CUDA(cudaStreamEndCapture(e->stream, &g));
+    cudaGraphExec_t x = nullptr;
+    cudaError_t err = cudaGraphInstantiateWithFlags(&x, g, 0);
+    cudaGraphDestroy(g);
+    if (err != cudaSuccess) {
+        set_error(std::string("CUDA graph instantiation failed: ") + cudaGetErrorString(err));
+        return FLBP_ERR_CUDA;
+    }
+    e->graphs[key] = x;
+    *out = x;
+    return FLBP_OK;
+}
+
+// Launch n sweeps as power-of-two graph chunks.
+int launch_sweeps(flbp_engine *e, int mode, long long n) {
+    if (e->L.nf_sell + e->L.nf_big == 0 && e->L.V == 0) return FLBP_OK;
+    while (n > 0) {
+        int k = 1;
+        while ((long long)k * 2 <= n && k < 64) k *= 2;
+        cudaGraphExec_t x;
+        int rc = sweep_graph(e, mode, k, &x);
+        if (rc) return rc;
+        FLBP_CUDA(cudaGraphLaunch(x, e->stream));
+        e->launches += 2LL * k;
+        n -= k;
+    }
+    return FLBP_OK;
+}
+
+int upload_ctl(flbp_engine *e) {
+    FLBP_CUDA(cudaMemcpyAsync(e->d_ctl, e->h_ctl, sizeof(Ctl), cudaMemcpyHostToDevice, e->stream));
+    return FLBP_OK;
+}
+
+int download_ctl(flbp_engine *e) {
+    FLBP_CUDA(cudaMemcpyAsync(e->h_ctl, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->stream));
+    FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    if (e->h_ctl->status != 0) {
+        set_error("a device-side wait for a shared-memory copy timed out; results of this call are invalid");
+        return FLBP_ERR_TIMEOUT;
+    }
+    return FLBP_OK;
+}
+
+void reset_ctl_for_run(flbp_engine *e, int mode) {
+    Ctl &c = *e->h_ctl;
+    std::memset(&c, 0, sizeof(Ctl));
+    c.t = e->t;
+    c.mode = mode;
+    c.iters0 = e->iters;
+    c.n_vars = e->L.V;
+    c.maxtime_ns = 1e300;
+    c.reason = FLBP_DIVERGED;
+    c.damping = e->damping;
+    c.pscale = (e->damping == 0.0) ? 1.0 : 1.0 - std::pow(e->damping, (double)e->t);
+}
+
+template <typename X>
+int dalloc(flbp_engine *e, X **p, size_t n) {
+    *p = nullptr;
+    if (n == 0) n = 1;
+    FLBP_CUDA(cudaMalloc((void **)p, n * sizeof(X)));
+    e->bytes += n * sizeof(X);
+    return FLBP_OK;
+}
+
+template <typename X>
+int upload(flbp_engine *e, X *dst, const std::vector<X> &src) {
+    if (src.empty()) return FLBP_OK;
+    FLBP_CUDA(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(X), cudaMemcpyHostToDevice, e->stream));
+    return FLBP_OK;
+}
+
+int begin_call(flbp_engine *e) {
+    if (!e) {
+        set_error("null engine handle");
+        return FLBP_ERR_INVALID;
+    }
+    FLBP_CUDA(cudaSetDevice(e->device));
+    return FLBP_OK;
+}
+
+int record_start(flbp_engine *e) {
+    FLBP_CUDA(cudaEventRecord(e->ev0, e->stream));
+    return FLBP_OK;
+}
+
+int record_stop(flbp_engine *e) {
+    FLBP_CUDA(cudaEventRecord(e->ev1, e->stream));
+    FLBP_CUDA(cudaEventSynchronize(e->ev1));
+    FLBP_CUDA(cudaEventElapsedTime(&e->last_ms, e->ev0, e->ev1));
+    FLBP_CUDA(cudaGetLastError());
+    return FLBP_OK;
+}
+
+void fill_info(flbp_engine *e, flbp_run_info *info, long long sweeps, long long launches0) {
+    if (!info) return;
+    info->sweeps = sweeps;
+    info->total_sweeps = e->iters;
+    info->maxdiff = e->h_ctl->mode ? e->h_ctl->maxdiff : std::numeric_limits<double>::quiet_NaN();
+    info->frac = e->h_ctl->mode == 2 ? e->h_ctl->frac : 1.0;
+    info->reason = e->h_ctl->reason;
+    info->status = e->h_ctl->status;
+    info->launches = e->launches - launches0;
+}
+
+// Stop-rule driven loop: chunks of sweeps until the device sets ctl->done.
+int run_loop(flbp_engine *e, int mode, long long cap) {
+    long long launched = 0;
+    int k = 1;
+    while (launched < cap) {
+        const long long n = std::min<long long>(k, cap - launched);
+        int rc = launch_sweeps(e, mode, n);
+        if (rc) return rc;
+        launched += n;
+        rc = download_ctl(e);
+        if (rc) return rc;
+        if (e->h_ctl->done) break;
+        k = std::min(k * 2, 64);
+    }
+    return FLBP_OK;
+}
+
+double sigmoid_d(double x) { return x >= 0 ? 1.0 / (1.0 + std::exp(-x)) : std::exp(x) / (1.0 + std::exp(x)); }
+
+}  // namespace
+
+extern "C" {
+
+const char *flbp_last_error(void) { return g_last_error.c_str(); }
+
+const char *flbp_version(void) { return "fastlbp_b200 0.1 (sm_100a)"; }
+
+int flbp_engine_create(const flbp_graph_desc *graph, const flbp_engine_opts *opts, flbp_engine **out) {
+    if (!graph || !out) {
+        set_error("null argument");
+        return FLBP_ERR_INVALID;
+    }
+    *out = nullptr;
+    flbp_engine_opts o{32, -1, 0.0, nullptr};
+    if (opts) o = *opts;
+    if (o.precision != 32 && o.precision != 64) {
+        set_error("precision must be 32 or 64");
+        return FLBP_ERR_INVALID;
+    }
+    if (!(o.damping >= 0.0 && o.damping < 1.0)) {
+        set_error("damping must lie in [0,1)");
+        return FLBP_ERR_INVALID;
+    }
+    flbp_engine *e = new (std::nothrow) flbp_engine();
+    if (!e) {
+        set_error("host allocation failed");
+        return FLBP_ERR_NOMEM;
+    }
+    std::string err;
+    int rc = build_layout(*graph, e->L, err);
+    if (rc) {
+        set_error(err);
+        delete e;
+        return rc;
+    }
+    e->prec = o.precision;
+    e->tsize = o.precision == 64 ? 8 : 4;
+    e->damping = o.damping;
+    auto fail = [&](int code) {
+        std::string msg = g_last_error;
+        flbp_engine_destroy(e);
+        set_error(msg);
+        return code;
+    };
+    if (o.device >= 0) {
+        cudaError_t ce = cudaSetDevice(o.device);
+        if (ce != cudaSuccess) {
+            set_error(std::string("cudaSetDevice failed: ") + cudaGetErrorString(ce));
+            delete e;
+            return FLBP_ERR_CUDA;
+        }
+    }
+    if (cudaGetDevice(&e->device) != cudaSuccess) {
+        set_error("no CUDA device");
+        delete e;
+        return FLBP_ERR_CUDA;
+    }
+    if (o.stream) {
+        e->stream = (cudaStream_t)o.stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            set_error("stream creation failed");
+            delete e;
+            return FLBP_ERR_CUDA;
+        }
+        e->own_stream = true;
+    }
+    if (cudaEventCreate(&e->ev0) != cudaSuccess || cudaEventCreate(&e->ev1) != cudaSuccess) {
+        set_error("event creation failed");
+        return fail(FLBP_ERR_CUDA);
+    }
+    const HostLayout &L = e->L;
+    const uint32_t nf = L.nf_sell + L.nf_big;
+    const size_t ns = std::max<uint64_t>(1, L.n_slots);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
+    // One full wave of resident blocks; the kernels stride over tiles and large items.
+    int fb = 1, vb = 1;
+    cudaError_t cfg = (e->prec == 64) ? configure_kernels<double>(&fb, &vb) : configure_kernels<float>(&fb, &vb);
+    if (cfg != cudaSuccess) {
+        set_error(std::string("kernel configuration failed: ") + cudaGetErrorString(cfg));
+        return fail(FLBP_ERR_CUDA);
+    }
+    fb = std::max(fb, 1);
+    vb = std::max(vb, 1);
+    // Tile blocks run the shared-memory pipeline; the remaining blocks take the
+    // large-degree items concurrently, in proportion to their share of the work.
+    const char *split_env = getenv("FLBP_SPLIT_BLOCKS");
+    const bool dedicated = split_env && split_env[0] == '1';
+    auto split = [&](uint32_t n_tiles, uint64_t tile_work, uint32_t n_big, uint64_t big_work, int per_sm,
+                     uint32_t &tile_blocks) -> int {
+        const uint64_t total = (uint64_t)sms * (uint64_t)per_sm;
+        if (!dedicated) {  // every block takes large items first, then tiles
+            const uint64_t g = std::max<uint64_t>(1, std::min<uint64_t>(total, std::max<uint64_t>(n_tiles, (n_big + 7) / 8)));
+            tile_blocks = (uint32_t)g;
+            return (int)g;
+        }
+        uint64_t bigb = 0;
+        if (n_big) {
+            bigb = (total * big_work + (tile_work + big_work) - 1) / std::max<uint64_t>(1, tile_work + big_work);
+            bigb = std::max<uint64_t>(1, std::min<uint64_t>(bigb, (n_big + 8) / 9));
+            if (n_tiles) bigb = std::min<uint64_t>(bigb, total > 1 ? total - 1 : 1);
+        }
+        tile_blocks = (uint32_t)std::min<uint64_t>(n_tiles, std::max<uint64_t>(1, total - bigb));
+        return (int)std::max<uint64_t>(1, tile_blocks + bigb);
+    };
+    const uint32_t n_ft = (uint32_t)L.ftiles.size() - 1, n_vt = (uint32_t)L.vtiles.size() - 1;
+    const uint64_t f_big_slots = L.fb_off.empty() ? 0 : L.fb_off.back() - L.fb_off.front();
+    const uint64_t v_big_ents = L.vb_off.empty() ? 0 : L.vb_off.back() - L.vb_off.front();
+    e->factor_grid = split(n_ft, L.fg_base.empty() ? 0 : L.fg_base.back(), L.nf_big, f_big_slots, fb, e->f_tile_blocks);
+    e->var_grid = split(n_vt, L.vg_base.empty() ? 0 : L.vg_base.back(), L.nv_big, v_big_ents, vb, e->v_tile_blocks);
+
+    // Per-item arrays are padded to whole groups of 32 so that the tile copies
+    // of the last group stay in bounds.
+    const size_t nf_pad = std::max<size_t>(nf, 32ull * L.n_fgroups());
+    const size_t nv_pad = std::max<size_t>((size_t)L.V, 32ull * L.n_vgroups());
+    const size_t psz = e->prec == 64 ? 16 : 8;
+    if ((rc = dalloc(e, (char **)&e->d_vf, ns * e->tsize)) || (rc = dalloc(e, (char **)&e->d_fv, ns * e->tsize)) ||
+        (rc = dalloc(e, (char **)&e->d_f_pq, 2 * nf_pad * e->tsize)) ||
+        (rc = dalloc(e, &e->d_fg_base, L.fg_base.size())) || (rc = dalloc(e, &e->d_fb_off, L.fb_off.size())) ||
+        (rc = dalloc(e, &e->d_f_kind, nf_pad)) || (rc = dalloc(e, &e->d_f_deg, nf_pad)) ||
+        (rc = dalloc(e, &e->d_vg_base, L.vg_base.size())) || (rc = dalloc(e, &e->d_vb_off, L.vb_off.size())) ||
+        (rc = dalloc(e, &e->d_v_ent, L.v_ent.size())) || (rc = dalloc(e, &e->d_ftiles, 16ull * n_ft)) ||
+        (rc = dalloc(e, &e->d_vtiles, 16ull * n_vt)) ||
+        (rc = dalloc(e, (char **)&e->d_prior, std::max<size_t>(1, nv_pad) * psz)) ||
+        (rc = dalloc(e, &e->d_belief, nv_pad)) || (rc = dalloc(e, &e->d_lowpass, (size_t)L.V)) ||
+        (rc = dalloc(e, &e->d_ctl, 1)))
+        return fail(rc);
+    if (cudaMallocHost((void **)&e->h_ctl, sizeof(Ctl)) != cudaSuccess) {
+        set_error("pinned allocation failed");
+        return fail(FLBP_ERR_NOMEM);
+    }
+    std::memset(e->h_ctl, 0, sizeof(Ctl));
+    std::vector<uint32_t> prior(std::max<size_t>(1, nv_pad) * (psz / 4), 0u);
+    for (int64_t i = 0; i < L.V; i++) {
+        if (e->prec == 64) {
+            std::memcpy(&prior[4 * i], &L.prior_fin[i], 8);
+            prior[4 * i + 2] = L.prior_cnt[i];
+        } else {
+            const float f = (float)L.prior_fin[i];
+            std::memcpy(&prior[2 * i], &f, 4);
+            prior[2 * i + 1] = L.prior_cnt[i];
+        }
+    }
+    // 16-word tile headers: first group, group count, group offsets (end repeated).
+    auto headers = [](const std::vector<uint32_t> &tiles, const std::vector<uint32_t> &base) {
+        std::vector<uint32_t> h;
+        for (size_t t = 0; t + 1 < tiles.size(); t++) {
+            const uint32_t g0 = tiles[t], n = tiles[t + 1] - g0;
+            h.push_back(g0);
+            h.push_back(n);
+            for (uint32_t j = 0; j < 14; j++) h.push_back(base[g0 + std::min(j, n)]);
+        }
+        return h;
+    };
+    const std::vector<uint32_t> fhdr = headers(L.ftiles, L.fg_base), vhdr = headers(L.vtiles, L.vg_base);
+    std::vector<uint8_t> kind_pad(nf_pad, 0), deg_pad(nf_pad, 0);
+    std::copy(L.f_kind.begin(), L.f_kind.end(), kind_pad.begin());
+    std::copy(L.f_deg.begin(), L.f_deg.end(), deg_pad.begin());
+    std::vector<double> pq64(2 * nf_pad, 0.0);
+    std::copy(L.f_pq.begin(), L.f_pq.end(), pq64.begin());
+    std::vector<float> pq32;
+    if (e->prec == 64) {
+        if ((rc = upload(e, (double *)e->d_f_pq, pq64))) return fail(rc);
+    } else {
+        pq32.assign(pq64.begin(), pq64.end());
+        if ((rc = upload(e, (float *)e->d_f_pq, pq32))) return fail(rc);
+    }
+    if ((rc = upload(e, e->d_fg_base, L.fg_base)) || (rc = upload(e, e->d_fb_off, L.fb_off)) ||
+        (rc = upload(e, e->d_f_kind, kind_pad)) || (rc = upload(e, e->d_f_deg, deg_pad)) ||
+        (rc = upload(e, e->d_vg_base, L.vg_base)) || (rc = upload(e, e->d_vb_off, L.vb_off)) ||
+        (rc = upload(e, e->d_v_ent, L.v_ent)) || (rc = upload(e, (uint32_t *)e->d_prior, prior)) ||
+        (rc = upload(e, e->d_ftiles, fhdr)) || (rc = upload(e, e->d_vtiles, vhdr)))
+        return fail(rc);
+    cudaError_t ce = cudaSuccess;
+    if ((ce = cudaStreamSynchronize(e->stream)) != cudaSuccess ||
+        (ce = cudaMemsetAsync(e->d_belief, 0, std::max<size_t>(1, nv_pad) * sizeof(double), e->stream)) != cudaSuccess ||
+        (ce = cudaMemsetAsync(e->d_vf, 0, ns * e->tsize, e->stream)) != cudaSuccess ||
+        (ce = cudaMemsetAsync(e->d_fv, 0, ns * e->tsize, e->stream)) != cudaSuccess ||
+        (ce = cudaStreamSynchronize(e->stream)) != cudaSuccess) {
+        set_error(std::string("device initialisation failed: ") + cudaGetErrorString(ce));
+        return fail(FLBP_ERR_CUDA);
+    }
+    *out = e;
+    return FLBP_OK;
+}
+
+int flbp_engine_destroy(flbp_engine *e) {
+    if (!e) return FLBP_OK;
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    for (auto &kv : e->graphs) cudaGraphExecDestroy(kv.second);
+    void *bufs[] = {e->d_vf,     e->d_fv,       e->d_f_pq,   e->d_fg_base,   e->d_fb_off,     e->d_f_kind,
+                    e->d_f_deg,  e->d_vg_base,  e->d_vb_off, e->d_v_ent,     e->d_prior,      e->d_belief,
+                    e->d_lowpass, e->d_hist,    e->d_hist_next, e->d_hist_count, e->d_ctl,    e->d_scratch,
+                    e->d_ftiles, e->d_vtiles};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    if (e->h_ctl) cudaFreeHost(e->h_ctl);
+    if (e->ev0) cudaEventDestroy(e->ev0);
+    if (e->ev1) cudaEventDestroy(e->ev1);
+    if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+    return FLBP_OK;
+}
+
+int flbp_init(flbp_engine *e) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    const size_t ns = std::max<size_t>(1, e->L.n_slots);
+    FLBP_CUDA(cudaMemsetAsync(e->d_vf, 0, ns * e->tsize, e->stream));
+    FLBP_CUDA(cudaMemsetAsync(e->d_fv, 0, ns * e->tsize, e->stream));
+    e->t = 0;
+    e->lowpass_valid = false;
+    return FLBP_OK;
+}
+
+int flbp_sweep(flbp_engine *e, int64_t n) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    if (n < 0) {
+        set_error("negative sweep count");
+        return FLBP_ERR_INVALID;
+    }
+    reset_ctl_for_run(e, 0);
+    if ((rc = upload_ctl(e)) || (rc = launch_sweeps(e, 0, n)) || (rc = download_ctl(e))) return rc;
+    e->t += n;
+    e->iters += n;
+    return FLBP_OK;
+}
+
+int flbp_run_fixed(flbp_engine *e, int64_t sweeps, flbp_run_info *info) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    if (sweeps < 0) {
+        set_error("negative sweep count");
+        return FLBP_ERR_INVALID;
+    }
+    const long long l0 = e->launches;
+    reset_ctl_for_run(e, 0);
+    if ((rc = record_start(e)) || (rc = upload_ctl(e)) || (rc = launch_sweeps(e, 0, sweeps))) return rc;
+    launch_beliefs_only(e, e->d_belief);
+    FLBP_CUDA(cudaMemcpyAsync(e->d_lowpass, e->d_belief, std::max<size_t>(1, e->L.V) * sizeof(double),
+                              cudaMemcpyDeviceToDevice, e->stream));
+    if ((rc = record_stop(e)) || (rc = download_ctl(e))) return rc;
+    e->t += sweeps;
+    e->iters += sweeps;
+    e->lowpass_valid = true;
+    fill_info(e, info, sweeps, l0);
+    if (info) info->frac = 1.0;
+    return FLBP_OK;
+}
+
+int flbp_run_tol(flbp_engine *e, double tol, int64_t maxiter, double maxtime, flbp_run_info *info) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    const long long l0 = e->launches;
+    reset_ctl_for_run(e, 1);
+    Ctl &c = *e->h_ctl;
+    c.tol = tol;
+    c.maxiter = maxiter;
+    c.maxtime_ns = maxtime * 1e9;
+    c.maxdiff = INFINITY;
+    if ((rc = record_start(e))) return rc;
+    long long done_sweeps = 0;
+    if (e->iters < maxiter && maxtime > 0.0 && INFINITY > tol) {
+        if ((rc = upload_ctl(e)) || (rc = run_loop(e, 1, maxiter - e->iters))) return rc;
+        if ((rc = download_ctl(e))) return rc;
+        done_sweeps = e->h_ctl->run_sweeps;
+    }
+    if ((rc = record_stop(e))) return rc;
+    e->t += done_sweeps;
+    e->iters += done_sweeps;
+    fill_info(e, info, done_sweeps, l0);
+    return FLBP_OK;
+}
+
+int flbp_run_lowpass(flbp_engine *e, double tol, int64_t min_iters, int64_t max_iters, int64_t hist_length,
+                     double maxtime, flbp_run_info *info) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    if (hist_length <= 0) {
+        set_error("belief history length must be positive");
+        return FLBP_ERR_INVALID;
+    }
+    if (max_iters <= min_iters || min_iters < 0) {
+        set_error("low-pass run needs 0 <= minIters < maxIters");
+        return FLBP_ERR_INVALID;
+    }
+    const size_t V = (size_t)e->L.V;
+    if ((uint64_t)hist_length > e->hist_cap) {
+        if (e->d_hist) cudaFree(e->d_hist);
+        if (e->d_hist_next) cudaFree(e->d_hist_next);
+        if (e->d_hist_count) cudaFree(e->d_hist_count);
+        e->d_hist = nullptr;
+        e->d_hist_next = e->d_hist_count = nullptr;
+        e->hist_cap = 0;
+        if ((rc = dalloc(e, &e->d_hist, std::max<size_t>(1, V) * (size_t)hist_length)) ||
+            (rc = dalloc(e, &e->d_hist_next, V)) || (rc = dalloc(e, &e->d_hist_count, V)))
+            return rc;
+    }
+    e->hist_cap = (uint32_t)hist_length;
+    FLBP_CUDA(cudaMemsetAsync(e->d_hist_next, 0, std::max<size_t>(1, V) * sizeof(uint32_t), e->stream));
+    FLBP_CUDA(cudaMemsetAsync(e->d_hist_count, 0, std::max<size_t>(1, V) * sizeof(uint32_t), e->stream));
+    // Graphs captured with a different history length are stale.
+    for (auto it = e->graphs.begin(); it != e->graphs.end();) {
+        if (it->first.first == 2) {
+            cudaGraphExecDestroy(it->second);
+            it = e->graphs.erase(it);
+        } else {
+            ++it;
+        }
+    }
+    const long long l0 = e->launches;
+    reset_ctl_for_run(e, 2);
+    Ctl &c = *e->h_ctl;
+    c.tol = tol;
+    c.min_iters = min_iters;
+    c.max_iters = max_iters;
+    c.maxtime_ns = maxtime * 1e9;
+    c.frac = 1.0;
+    c.maxdiff = INFINITY;
+    if ((rc = record_start(e))) return rc;
+    long long done_sweeps = 0;
+    if (maxtime >= 0.0) {
+        if ((rc = upload_ctl(e)) || (rc = run_loop(e, 2, max_iters + 1))) return rc;
+        if ((rc = download_ctl(e))) return rc;
+        done_sweeps = e->h_ctl->run_sweeps;
+    }
+    if (e->h_ctl->reason == FLBP_ALL_CONVERGED && done_sweeps > 0) {
+        FLBP_CUDA(cudaMemcpyAsync(e->d_lowpass, e->d_belief, std::max<size_t>(1, V) * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, e->stream));
+    } else if (V > 0) {
+        lowpass_kernel<<<(unsigned)((V + 255) / 256), 256, 0, e->stream>>>(
+            e->d_hist, e->d_hist_next, e->d_hist_count, e->hist_cap, (uint32_t)V, e->d_lowpass);
+        e->launches += 1;
+    }
+    if ((rc = record_stop(e))) return rc;
+    e->t += done_sweeps;
+    e->iters += done_sweeps;
+    e->lowpass_valid = true;
+    fill_info(e, info, done_sweeps, l0);
+    if (info && done_sweeps == 0) info->frac = 1.0;
+    return FLBP_OK;
+}
+
+static int fetch_internal(flbp_engine *e, const double *dsrc, double *out, int64_t n) {
+    if (n != e->L.V) {
+        set_error("output length must equal the number of variables");
+        return FLBP_ERR_INVALID;
+    }
+    std::vector<double> tmp((size_t)n);
+    if (n) {
+        FLBP_CUDA(cudaMemcpyAsync(tmp.data(), dsrc, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+        FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    }
+    for (int64_t i = 0; i < n; i++) out[i] = tmp[e->L.internal_of_var[i]];
+    return FLBP_OK;
+}
+
+int flbp_get_beliefs(flbp_engine *e, double *out, int64_t n) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    return fetch_internal(e, e->d_belief, out, n);
+}
+
+int flbp_get_lowpass(flbp_engine *e, double *out, int64_t n) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    if (!e->lowpass_valid) return fetch_internal(e, e->d_belief, out, n);
+    return fetch_internal(e, e->d_lowpass, out, n);
+}
+
+int flbp_compute_beliefs(flbp_engine *e, double *out, int64_t n) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    reset_ctl_for_run(e, 0);
+    if (!e->d_scratch && (rc = dalloc(e, &e->d_scratch, (size_t)e->L.V))) return rc;
+    if ((rc = upload_ctl(e))) return rc;
+    launch_beliefs_only(e, e->d_scratch);
+    FLBP_CUDA(cudaGetLastError());
+    return fetch_internal(e, e->d_scratch, out, n);
+}
+
+static int fv_lambda(flbp_engine *e, std::vector<double> &lam) {
+    const HostLayout &L = e->L;
+    const size_t ns = L.n_slots;
+    std::vector<double> act(ns);
+    if (ns) {
+        if (e->prec == 64) {
+            FLBP_CUDA(cudaMemcpyAsync(act.data(), e->d_fv, ns * 8, cudaMemcpyDeviceToHost, e->stream));
+        } else {
+            std::vector<float> f(ns);
+            FLBP_CUDA(cudaMemcpyAsync(f.data(), e->d_fv, ns * 4, cudaMemcpyDeviceToHost, e->stream));
+            FLBP_CUDA(cudaStreamSynchronize(e->stream));
+            for (size_t i = 0; i < ns; i++) act[i] = f[i];
+        }
+        FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    }
+    const double scale = (e->damping == 0.0) ? 1.0 : 1.0 - std::pow(e->damping, (double)e->t);
+    lam.assign((size_t)L.E, 0.0);
+    for (int64_t k = 0; k < L.E; k++) {
+        const int64_t s = L.ref_fv_src[k];
+        if (s >= 0) lam[k] = act[s];
+        else if (s == -2) lam[k] = INFINITY;
+        else if (s == -3) lam[k] = -INFINITY;
+        else lam[k] = L.ref_const[k] * scale;
+    }
+    return FLBP_OK;
+}
+
+static void pair_of(double lam, double &m0, double &m1) {
+    if (lam == INFINITY) {
+        m0 = 0.0;
+        m1 = 1.0;
+    } else if (lam == -INFINITY) {
+        m0 = 1.0;
+        m1 = 0.0;
+    } else {
+        m1 = sigmoid_d(lam);
+        m0 = sigmoid_d(-lam);
+    }
+}
+
+int flbp_get_fv_messages(flbp_engine *e, double *m0, double *m1, int64_t n) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    if (n != e->L.E) {
+        set_error("output length must equal the number of edge slots");
+        return FLBP_ERR_INVALID;
+    }
+    if (e->t == 0) {  // init() fills both states with 1 (causal_bp.cu:825-841)
+        for (int64_t k = 0; k < n; k++) m0[k] = m1[k] = 1.0;
+        return FLBP_OK;
+    }
+    std::vector<double> lam;
+    if ((rc = fv_lambda(e, lam))) return rc;
+    for (int64_t k = 0; k < n; k++) pair_of(lam[k], m0[k], m1[k]);
+    return FLBP_OK;
+}
+
+int flbp_get_vf_messages(flbp_engine *e, double *m0, double *m1, int64_t n) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    const HostLayout &L = e->L;
+    if (n != L.E) {
+        set_error("output length must equal the number of edge slots");
+        return FLBP_ERR_INVALID;
+    }
+    if (e->t == 0) {
+        for (int64_t k = 0; k < n; k++) m0[k] = m1[k] = 1.0;
+        return FLBP_OK;
+    }
+    std::vector<double> lam;
+    if ((rc = fv_lambda(e, lam))) return rc;
+    std::vector<double> S((size_t)L.V, 0.0);
+    std::vector<int> np((size_t)L.V, 0), nn((size_t)L.V, 0);
+    for (int64_t k = 0; k < L.E; k++) {
+        const int64_t v = L.vm_var[k];
+        if (lam[k] == INFINITY) np[v]++;
+        else if (lam[k] == -INFINITY) nn[v]++;
+        else S[v] += lam[k];
+    }
+    for (int64_t e_ = 0; e_ < L.E; e_++) {
+        const int64_t k = L.fm_to_vm[e_], v = L.vm_var[k];
+        double s = S[v];
+        int a = np[v], b = nn[v];
+        if (lam[k] == INFINITY) a--;
+        else if (lam[k] == -INFINITY) b--;
+        else s -= lam[k];
+        const double x = (a > 0 && b > 0) ? 0.0 : a > 0 ? INFINITY : b > 0 ? -INFINITY : s;
+        pair_of(x, m0[e_], m1[e_]);
+    }
+    return FLBP_OK;
+}
+
+int flbp_engine_stats(flbp_engine *e, int64_t *c, int64_t n) {
+    if (!e || !c) {
+        set_error("null argument");
+        return FLBP_ERR_INVALID;
+    }
+    const int64_t v[8] = {e->L.V, e->L.F, e->L.E, (int64_t)(e->L.nf_sell + e->L.nf_big),
+                          (int64_t)e->L.n_active_slots, (int64_t)e->L.nf_big, (int64_t)e->L.nv_big,
+                          (int64_t)e->bytes};
+    for (int64_t i = 0; i < n && i < 8; i++) c[i] = v[i];
+    return FLBP_OK;
+}
+
+int flbp_last_run_ms(flbp_engine *e, double *ms) {
+    if (!e || !ms) {
+        set_error("null argument");
+        return FLBP_ERR_INVALID;
+    }
+    *ms = e->last_ms;
+    return FLBP_OK;
+}
+
+}  // extern "C"

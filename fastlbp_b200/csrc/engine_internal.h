@@ -1,0 +1,92 @@
+// Internal declarations shared by the host layout builder (layout.cpp) and
+// the CUDA engine (engine.cu). Not part of the public interface.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/fastlbp_b200.h"
+
+namespace flbp {
+
+// Kind byte of an active AND/OR factor.
+enum : uint8_t {
+    KIND_OR = 1,          // bit 0: OR factor (else AND)
+    HEAD_FREE = 0 << 1,   // head message comes from the head variable
+    HEAD_ONE = 1 << 1,    // head clamped to 1: effective head log-odds +inf
+    HEAD_ZERO = 2 << 1,   // head clamped to 0: effective head log-odds -inf
+    HEAD_NONE = 3 << 1,   // head mask (0,0): the reference's arithmetic yields NaN
+    HEAD_MASK = 3 << 1,
+};
+
+// Items up to these degrees go to the sliced-ELL (one item per lane) paths,
+// larger ones to the warp-per-item paths.
+constexpr uint32_t kSellFactorDegree = 16;
+constexpr uint32_t kSellVarDegree = 16;
+constexpr uint32_t kSentinel = 0xffffffffu;  // padding entry in the variable layout
+constexpr uint32_t kTileGroupsHost = 8;      // groups per tile (= warps per block of the passes)
+constexpr uint32_t kTileSlotsHost = 2048;    // slot budget of a tile (shared-memory stage size)
+
+// Host-built device layout.
+//
+// Active factors are the AND/OR factors with at least one body variable; all
+// other factors (singletons, AND/OR factors reduced to their head, and the
+// head output of head-clamped factors) send constant messages and are folded
+// into per-variable priors.
+//
+// Factor side, "sliced ELL" of width 32: active factors with degree <=
+// kSellFactorDegree are sorted by degree (stable) and cut into groups of 32;
+// group g owns slots [fg_base[g], fg_base[g+1]) laid out column-major, slot k
+// of the group's lane-th factor at fg_base[g] + 32*k + lane, k = 0 being the
+// head. Larger factors follow as contiguous runs (fb_off), head first.
+//
+// Variable side: variables are sorted by degree (stable) and cut into groups
+// of 32 the same way; entry k of the lane-th variable of group g is
+// v_ent[vg_base[g] + 32*k + lane], the factor-side slot whose message
+// reaches the variable (kSentinel for padding). Variables of larger degree
+// follow with contiguous entry runs (vb_off).
+struct HostLayout {
+    int64_t V = 0, F = 0, E = 0;  // reference sizes
+
+    uint32_t nf_sell = 0, nf_big = 0;  // active factors per path
+    std::vector<uint32_t> fg_base;     // n_fgroups + 1
+    std::vector<uint32_t> fb_off;      // nf_big + 1 (absolute slot ids)
+    std::vector<uint8_t> f_kind;       // per active factor (internal order)
+    std::vector<uint8_t> f_deg;        // per sell factor
+    std::vector<double> f_pq;          // 2 per active factor: p, q
+    uint64_t n_slots = 0;              // slots incl. padding
+
+    uint32_t nv_sell = 0, nv_big = 0;
+    std::vector<uint32_t> vg_base;     // n_vgroups + 1 (entry ids)
+    std::vector<uint32_t> vb_off;      // nv_big + 1 (entry ids)
+    std::vector<uint32_t> v_ent;       // entries incl. padding
+    std::vector<double> prior_fin;     // per internal variable: finite constant log-odds (damping-scaled)
+    std::vector<uint32_t> prior_cnt;   // per internal variable: (#+inf) | (#-inf << 16)
+    std::vector<uint32_t> var_of_internal;  // internal variable -> reference variable
+    std::vector<uint32_t> internal_of_var;  // reference variable -> internal variable
+    uint64_t n_active_slots = 0;       // real (non-padding) slots of active factors
+
+    // Reference variable-major slot (row_ptr_fv order) -> source of its f->v message:
+    // >= 0 device slot; -1 constant finite (value in ref_const, damping-scaled);
+    // -2 constant +inf; -3 constant -inf.
+    std::vector<int64_t> ref_fv_src;
+    std::vector<double> ref_const;
+    std::vector<int64_t> row_ptr_fv;  // reference variable-major CSR (V+1)
+    std::vector<int64_t> fm_to_vm;    // reference factor-major slot -> variable-major position
+    std::vector<int64_t> vm_var;      // variable-major position -> reference variable
+
+    // Tiles of at most kTileGroupsHost groups and kTileSlotsHost slots (entries):
+    // first group of each tile, n_tiles + 1 entries.
+    std::vector<uint32_t> ftiles, vtiles;
+
+    uint32_t n_fgroups() const { return fg_base.empty() ? 0 : (uint32_t)fg_base.size() - 1; }
+    uint32_t n_vgroups() const { return vg_base.empty() ? 0 : (uint32_t)vg_base.size() - 1; }
+};
+
+// Builds the layout; returns FLBP_OK or an error code with `err` filled in.
+int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err);
+
+void set_error(const std::string &msg);
+
+}  // namespace flbp

@@ -1,0 +1,890 @@
+// sm_100a kernels of one synchronous (PARALL) causal-BP sweep.
+//
+// Messages are log-odds lambda = log(m1/m0), one value per device slot, in
+// two arrays: vf (variable -> factor) and fv (factor -> variable). A sweep is
+//   factor pass:   fv <- f(vf) for every active factor, all its outputs;
+//   variable pass: per variable the sum of its incoming fv plus its constant
+//                  prior, then vf <- total - own message, beliefs, residual.
+// This is the reference's FV -> Prod -> VF sequence
+// (csrc/ext/causal_bp.cu:409-444) restated in log-odds.
+//
+// Exact zeros of the reference's probability arithmetic become +-inf
+// log-odds. On the factor side zeros flow through sums of log-sigmoids as
+// -inf (prefix/suffix sums never subtract); on the variable side +inf / -inf
+// counts play the role of the reference's num_zeros counters
+// (causal_bp_parall.cu:36-45, 74-83).
+//
+// OR factors are evaluated as AND factors on negated log-odds (the states 0
+// and 1 swap roles, causal_bp_parall.cu:152-190 vs :113-151) and their
+// outputs negated back.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "engine_internal.h"
+
+namespace flbp {
+
+// Control block of one engine (device memory). Written by block 0 of the
+// factor pass (sweep counters, residual reset) and by the last block of the
+// variable pass (stop decision); read by every block at kernel entry.
+struct Ctl {
+    unsigned long long maxdiff_bits;  // max |belief change| of this sweep, double bits
+    unsigned long long nonconv;       // variables with |belief change| > tol
+    unsigned int arrive;              // variable-pass blocks finished this sweep
+    int done;                         // set: every kernel returns at entry
+    long long t;                      // sweeps since init (damping exponent)
+    long long run_sweeps;             // sweeps of the current run call
+    long long iters0;                 // reference _iters at the start of the run call
+    unsigned long long t_start_ns;    // %globaltimer at the first sweep of the run call
+    int mode;                         // 0 none, 1 tolerance loop, 2 low-pass loop
+    int reason;
+    int status;
+    int pad;
+    double tol;
+    long long maxiter;                // mode 1
+    long long min_iters, max_iters;   // mode 2
+    double maxtime_ns;
+    double maxdiff;                   // last sweep's residual (decoded)
+    double frac;                      // last sweep's non-converged fraction
+    double node_frac_tol;
+    long long n_vars;
+    double damping;
+    double pscale;                    // 1 - damping^t: weight of the finite constant priors
+};
+
+template <typename T>
+struct Num;
+
+template <>
+struct Num<float> {
+    static __device__ __forceinline__ float inf() { return __int_as_float(0x7f800000); }
+    static __device__ __forceinline__ float nan() { return __int_as_float(0x7fffffff); }
+    static __device__ __forceinline__ float exp(float x) { return __expf(x); }
+    static __device__ __forceinline__ float log(float x) { return __logf(x); }
+    static __device__ __forceinline__ float log1p(float x) { return ::log1pf(x); }
+    static __device__ __forceinline__ float expm1(float x) { return ::expm1f(x); }
+};
+
+template <>
+struct Num<double> {
+    static __device__ __forceinline__ double inf() { return __longlong_as_double(0x7ff0000000000000ll); }
+    static __device__ __forceinline__ double nan() { return __longlong_as_double(0x7fffffffffffffffll); }
+    static __device__ __forceinline__ double exp(double x) { return ::exp(x); }
+    static __device__ __forceinline__ double log(double x) { return ::log(x); }
+    static __device__ __forceinline__ double log1p(double x) { return ::log1p(x); }
+    static __device__ __forceinline__ double expm1(double x) { return ::expm1(x); }
+};
+
+template <typename T>
+__device__ __forceinline__ bool is_nan(T x) {
+    return x != x;
+}
+
+// Streaming loads (read once per sweep): evict-first in L2 so that the
+// message arrays, reused every pass, stay resident.
+__device__ __forceinline__ uint32_t ld_stream(const uint32_t *p) { return __ldcs(p); }
+__device__ __forceinline__ uint2 ld_stream(const uint2 *p) { return __ldcs(p); }
+__device__ __forceinline__ uint8_t ld_stream(const uint8_t *p) {
+    return (uint8_t)__ldcs(reinterpret_cast<const unsigned char *>(p));
+}
+__device__ __forceinline__ float ld_stream(const float *p) { return __ldcs(p); }
+__device__ __forceinline__ double ld_stream(const double *p) { return __ldcs(p); }
+
+// log(sigmoid(x)) = min(x,0) - log1p(exp(-|x|)); +inf -> 0, -inf -> -inf, NaN -> NaN.
+template <typename T>
+__device__ __forceinline__ T log_sigmoid(T x) {
+    return fmin(x, T(0)) - Num<T>::log1p(Num<T>::exp(-fabs(x)));
+}
+
+// AND -> head (causal_bp_parall.cu:113-151 in log-odds). With P = product of
+// sigma over the body = exp(lo) and R = 1 - P:
+//   m1 ~ p P + q R,   m0 ~ (1-p) P + (1-q) R   (m0 + m1 = 1).
+// lp = log p, used for q == 0 so that tiny P does not underflow.
+template <typename T>
+__device__ __forceinline__ T head_out(T lo, T p, T q, T lp) {
+    const T P = Num<T>::exp(lo), R = -Num<T>::expm1(lo);
+    const T B = (T(1) - p) * P + (T(1) - q) * R;
+    const T la = (q == T(0)) ? lp + lo : Num<T>::log(p * P + q * R);
+    return la - Num<T>::log(B);
+}
+
+// AND -> body (types 5/7, causal_bp_parall.cu:289-314, 341-366). With
+// Po = product of sigma over the other body slots = exp(lo), Ro = 1 - Po,
+// a = p Po + q Ro, b = 1 - a and head log-odds lh:
+//   m1 ~ sigma(lh) a + sigma(-lh) b,   m0 ~ sigma(lh) q + sigma(-lh) (1-q).
+// Both are divided by max(sigma(lh), sigma(-lh)); r = exp(-|lh|). Terms that
+// are exactly zero are taken in log space so that large |lh| cannot
+// underflow them. When m0 == 0 exactly (the reference's prod_10 == 0, which
+// skips its loop) the result is +inf if (p-q)(m1h-m0h) > 0 and NaN
+// otherwise, as the reference's scale() of (x, 0) and (0, 0) gives.
+// The m0 side depends only on the factor (head message, q), so it is
+// evaluated once per factor: lden = log of the scaled m0 and the value
+// returned when m0 == 0 exactly.
+template <typename T>
+struct BodyDen {
+    T lden, zero_out, r, lh;
+};
+
+template <typename T>
+__device__ __forceinline__ BodyDen<T> body_den(T lh, T p, T q) {
+    BodyDen<T> D;
+    D.lh = lh;
+    D.r = Num<T>::exp(-fabs(lh));
+    if (lh >= T(0)) D.lden = (q == T(0)) ? -lh : Num<T>::log(fma(D.r, T(1) - q, q));
+    else D.lden = (q == T(1)) ? lh : Num<T>::log(fma(D.r, q, T(1) - q));
+    const T s = (lh >= T(0)) ? (p - q) : (q - p);
+    D.zero_out = is_nan(lh) ? lh : ((s > T(0)) ? Num<T>::inf() : Num<T>::nan());
+    if (is_nan(lh)) D.lden = -Num<T>::inf();
+    return D;
+}
+
+template <typename T>
+__device__ __forceinline__ T body_out(T lo, T p, T q, const BodyDen<T> &D) {
+    if (D.lden == -Num<T>::inf()) return D.zero_out;
+    const T P = Num<T>::exp(lo), R = -Num<T>::expm1(lo);
+    const T a = p * P + q * R, b = (T(1) - p) * P + (T(1) - q) * R;
+    T lnum;
+    if (D.lh >= T(0)) lnum = (a == T(0)) ? Num<T>::log(b) - D.lh : Num<T>::log(fma(D.r, b, a));
+    else lnum = (b == T(0)) ? D.lh + Num<T>::log(a) : Num<T>::log(fma(D.r, a, b));
+    return lnum - D.lden;
+}
+
+// Damping of an f->v message in log-odds: (1-d) new + d old, with exact
+// zeros dominating (0^(1-d) = 0^d = 0) and opposite zeros giving (0.5, 0.5).
+template <typename T>
+__device__ __forceinline__ T damp_mix(T nw, T old, T d) {
+    const T inf = Num<T>::inf();
+    const bool ni = fabs(nw) == inf, oi = fabs(old) == inf;
+    if (ni || oi) {
+        if (ni && oi) return (nw == old) ? nw : T(0);
+        return ni ? nw : old;
+    }
+    return (T(1) - d) * nw + d * old;
+}
+
+struct FactorArgs {
+    const uint32_t *fg_base;  // sliced-ELL groups (n_fgroups + 1)
+    const uint32_t *fb_off;   // big factors (nf_big + 1)
+    const uint8_t *f_kind;
+    const uint8_t *f_deg;
+    const void *f_pq;         // T[2 * nf]
+    const uint4 *thdr;        // 64-byte header per tile (see TileHdr)
+    uint32_t nf_sell, nf_big, n_fgroups, n_tiles, n_tile_blocks;
+};
+
+struct VarArgs {
+    const uint32_t *vg_base;  // sliced-ELL groups (n_vgroups + 1)
+    const uint32_t *vb_off;   // big variables (nv_big + 1)
+    const uint32_t *v_ent;
+    const void *prior;        // per variable: FP32 engines uint2 (float bits of the finite prior,
+                              // +inf | -inf << 16 counts); FP64 engines uint4 (double bits, counts, 0)
+    double *belief;           // per internal variable, previous / current belief
+    double *hist;             // low-pass history [hist_len][n_vars], or null
+    uint32_t *hist_next;      // per variable ring cursor
+    uint32_t *hist_count;     // per variable number of stored samples
+    const uint4 *thdr;        // 64-byte header per tile (see TileHdr)
+    uint32_t nv_sell, nv_big, n_vgroups, n_tiles, n_tile_blocks;
+    uint32_t hist_len;
+};
+
+template <typename T, bool DAMP>
+__device__ __forceinline__ void store_fv(T *fv, uint32_t s, T val, T d) {
+    if (DAMP) val = damp_mix(val, fv[s], d);
+    fv[s] = val;
+}
+
+template <typename T>
+__device__ __forceinline__ T head_effective(uint8_t kind, T vf_head) {
+    const uint8_t hs = kind & HEAD_MASK;
+    const T inf = Num<T>::inf();
+    if (hs == HEAD_FREE) return vf_head;
+    if (hs == HEAD_ONE) return inf;
+    if (hs == HEAD_ZERO) return -inf;
+    return Num<T>::nan();
+}
+
+// ------------------------------------------------------------------ TMA staging
+//
+// Both passes run persistent blocks of 8 warps over "tiles" of 8 sliced-ELL
+// groups (256 items). The contiguous per-tile streams (messages of the
+// tile's slots, indices, per-item constants) are brought into shared memory
+// by one thread with 1-D bulk copies (cp.async.bulk, completion tracked by an
+// mbarrier per pipeline stage); the factor pass writes its outputs back with
+// a bulk store. All waits are bounded: on a timeout the block records
+// FLBP_ERR_TIMEOUT in ctl->status, drains its copies and returns.
+
+constexpr int kTileGroups = 8;                            // groups per tile = warps per block
+constexpr int kTileItems = 32 * kTileGroups;              // factors / variables per tile
+constexpr int kTileSlots = 2048;                          // slot (entry) budget of a tile
+constexpr long long kWaitCycles = 4000000000ll;           // ~2 s at 2 GHz
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for a stage; false on timeout.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity)) {
+        if (clock64() - t0 > kWaitCycles) return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_s2g(void *dst, const void *src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ size_t align128(size_t x) { return (x + 127) & ~(size_t)127; }
+
+// Shared-memory layout of one factor-pass stage.
+template <typename T, bool DAMP>
+struct FactorStage {
+    static constexpr size_t hdr = 0;                                     // uint32 gbase[kTileGroups + 1]
+    static constexpr size_t vbuf = 128;                                  // T[kTileSlots]: vf in, fv out
+    static constexpr size_t obuf = vbuf + sizeof(T) * kTileSlots;        // T[kTileSlots]: previous fv (DAMP)
+    static constexpr size_t deg = obuf + (DAMP ? sizeof(T) * kTileSlots : 0);  // uint8[kTileItems]
+    static constexpr size_t kind = deg + kTileItems;                     // uint8[kTileItems]
+    static constexpr size_t pq = kind + kTileItems;                      // T[2 * kTileItems]
+    static constexpr size_t bytes = (pq + 2 * sizeof(T) * kTileItems + 127) & ~(size_t)127;
+};
+
+template <typename T>
+struct VarStage {
+    static constexpr size_t hdr = 0;                                     // uint32 gbase[kTileGroups + 1]
+    static constexpr size_t ent = 128;                                   // uint32[kTileSlots]
+    static constexpr size_t prior = ent + 4 * kTileSlots;                // uint2 / uint4 [kTileItems]
+    static constexpr size_t bold = prior + (sizeof(T) == 4 ? 8 : 16) * kTileItems;  // double[kTileItems]
+    static constexpr size_t bytes = bold + 8 * kTileItems;
+};
+
+// One sliced-ELL group of 32 factors of width W, staged in shared memory:
+// lane = factor, slot k of the factor at vb[32 k + lane]. Per factor: the
+// log-sigmoids of the body, suffix sums, then one pass with a running prefix
+// sum; slot k's output uses the sum over all other body slots (prefix +
+// suffix, never a subtraction). Outputs replace the inputs in vb.
+template <typename T, bool DAMP, int W>
+__device__ __forceinline__ void factor_group_w(T *vb, const T *ob, const uint8_t *dg, const uint8_t *kd, const T *pq,
+                                               int lane, T d) {
+    const int deg = dg[lane];
+    const uint8_t kind = kd[lane];
+    const T p = pq[2 * lane], q = pq[2 * lane + 1];
+    const T s = (kind & KIND_OR) ? T(-1) : T(1);
+    T x[W];
+    const T vh = vb[lane];
+#pragma unroll
+    for (int k = 1; k < W; k++) x[k] = (k < deg) ? log_sigmoid<T>(s * vb[32 * k + lane]) : T(0);
+    const bool free_head = (kind & HEAD_MASK) == HEAD_FREE;
+    const T lh = s * head_effective<T>(kind, vh);
+    T suf[W + 1];
+    suf[W] = T(0);
+#pragma unroll
+    for (int k = W - 1; k >= 1; k--) suf[k] = suf[k + 1] + x[k];
+    if (deg > 0 && free_head) {
+        T o = s * head_out<T>(suf[1], p, q, Num<T>::log(p));
+        if (DAMP) o = damp_mix(o, ob[lane], d);
+        vb[lane] = o;
+    }
+    const BodyDen<T> D = body_den<T>(lh, p, q);
+    T pre = T(0);
+#pragma unroll
+    for (int k = 1; k < W; k++) {
+        if (k < deg) {
+            T o = s * body_out<T>(pre + suf[k + 1], p, q, D);
+            if (DAMP) o = damp_mix(o, ob[32 * k + lane], d);
+            vb[32 * k + lane] = o;
+        }
+        pre += x[k];
+    }
+}
+
+template <typename T, bool DAMP>
+__device__ __forceinline__ void factor_group(int w, T *vb, const T *ob, const uint8_t *dg, const uint8_t *kd,
+                                             const T *pq, int lane, T d) {
+    switch (w) {
+#define FLBP_W(N) \
+    case N: factor_group_w<T, DAMP, N>(vb, ob, dg, kd, pq, lane, d); break;
+        FLBP_W(2) FLBP_W(3) FLBP_W(4) FLBP_W(5) FLBP_W(6) FLBP_W(7) FLBP_W(8) FLBP_W(9) FLBP_W(10) FLBP_W(11)
+        FLBP_W(12) FLBP_W(13) FLBP_W(14) FLBP_W(15) FLBP_W(16)
+#undef FLBP_W
+        default: break;
+    }
+}
+
+// One large factor, one warp: lanes stride over the body; the body sum is a
+// double with a count of -inf terms so that each slot can remove its own term.
+template <typename T, bool DAMP>
+__device__ void factor_warp(const FactorArgs &a, uint32_t b, int lane, const T *__restrict__ vf, T *__restrict__ fv,
+                            T d) {
+    const uint32_t fi = a.nf_sell + b;
+    const uint32_t s0 = a.fb_off[b], s1 = a.fb_off[b + 1];
+    const uint8_t kind = a.f_kind[fi];
+    const T *pq = reinterpret_cast<const T *>(a.f_pq);
+    const T p = pq[2 * fi], q = pq[2 * fi + 1];
+    const T s = (kind & KIND_OR) ? T(-1) : T(1);
+    const T inf = Num<T>::inf();
+    const bool free_head = (kind & HEAD_MASK) == HEAD_FREE;
+    const T lh = s * head_effective<T>(kind, vf[s0]);
+    double L = 0.0;
+    int nz = 0;
+    for (uint32_t k = s0 + 1 + lane; k < s1; k += 32) {
+        const T ls = log_sigmoid<T>(s * vf[k]);
+        if (ls == -inf) nz++;
+        else L += (double)ls;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        L += __shfl_xor_sync(0xffffffffu, L, o);
+        nz += __shfl_xor_sync(0xffffffffu, nz, o);
+    }
+    if (free_head && lane == 0) store_fv<T, DAMP>(fv, s0, s * head_out<T>(nz ? -inf : (T)L, p, q, Num<T>::log(p)), d);
+    const BodyDen<T> D = body_den<T>(lh, p, q);
+    for (uint32_t k = s0 + 1 + lane; k < s1; k += 32) {
+        const T ls = log_sigmoid<T>(s * vf[k]);
+        const bool z = (ls == -inf);
+        const T lo = (nz - (int)z) ? -inf : (T)(z ? L : L - (double)ls);
+        store_fv<T, DAMP>(fv, k, s * body_out<T>(lo, p, q, D), d);
+    }
+}
+
+__device__ __forceinline__ void record_timeout(Ctl *ctl) { atomicExch(&ctl->status, FLBP_ERR_TIMEOUT); }
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Per-tile header (16 words, host-built): [0] first group, [1] number of
+// groups n (1..8), [2 + j] slot (entry) offset of group j for j = 0..n, the
+// rest repeating the end offset.
+struct TileHdr {
+    uint32_t w[16];
+};
+
+__device__ __forceinline__ void load_hdr(const uint4 *src, uint4 (&h)[4]) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) h[i] = __ldcg(src + i);
+}
+
+__device__ __forceinline__ uint32_t hdr_word(const uint4 (&h)[4], int i) {
+    const uint4 v = h[i >> 2];
+    const int k = i & 3;
+    return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w;
+}
+
+// Factor pass, warp-specialised. Blocks [0, n_tile_blocks) run a
+// STAGES-deep pipeline over tiles: warp 8 (one lane) is the producer - it
+// waits until the consumers have released a stage, bulk-stores the outputs
+// that stage holds, and bulk-loads the next tile (messages, previous
+// outputs when damping, per-factor constants) into it; warps 0-7 wait for a
+// stage to fill, compute one group each in shared memory and release it.
+// Blocks [n_tile_blocks, grid) take the large factors, one per warp.
+template <typename T, bool DAMP, int STAGES>
+__global__ void __launch_bounds__(288) factor_pass_kernel(FactorArgs a, const T *__restrict__ vf,
+                                                          T *__restrict__ fv, T d, Ctl *ctl) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES];
+    typedef FactorStage<T, DAMP> FS;
+    if (*(volatile int *)&ctl->done) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        unsigned long long now;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+        if (ctl->run_sweeps == 0) ctl->t_start_ns = now;
+        ctl->t += 1;
+        ctl->run_sweeps += 1;
+        ctl->pscale = (ctl->damping == 0.0) ? 1.0 : 1.0 - pow(ctl->damping, (double)ctl->t);
+        ctl->maxdiff_bits = 0ull;
+        ctl->nonconv = 0ull;
+        ctl->arrive = 0u;
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (blockIdx.x >= a.n_tile_blocks) {  // large factors
+        const uint32_t warp = (blockIdx.x - a.n_tile_blocks) * (blockDim.x >> 5) + wid;
+        const uint32_t nwarps = (gridDim.x - a.n_tile_blocks) * (blockDim.x >> 5);
+        for (uint32_t b = warp; b < a.nf_big; b += nwarps) factor_warp<T, DAMP>(a, b, lane, vf, fv, d);
+        return;
+    }
+    const uint32_t n_tiles = a.n_tiles, nb = a.n_tile_blocks;
+    const uint32_t my_tiles = (blockIdx.x < n_tiles) ? (n_tiles - blockIdx.x + nb - 1) / nb : 0;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], kTileGroups);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const T *pq_g = reinterpret_cast<const T *>(a.f_pq);
+
+    if (wid == kTileGroups) {  // producer warp
+        if (lane != 0) return;
+        bool ok = true;
+        auto store_stage = [&](int s) {
+            unsigned char *st = smem + (size_t)s * FS::bytes;
+            const uint32_t *gb = reinterpret_cast<const uint32_t *>(st + FS::hdr);
+            const uint32_t n = gb[1];
+            const uint32_t nbytes = (gb[2 + n] - gb[2]) * (uint32_t)sizeof(T);
+            if (nbytes) {
+                bulk_s2g(fv + gb[2], st + FS::vbuf, nbytes);
+                bulk_commit();
+            }
+        };
+        uint4 h[4];
+        uint32_t issued = 0;
+        if (my_tiles) load_hdr(a.thdr + 4ull * blockIdx.x, h);
+        for (uint32_t it = 0; it < my_tiles; it++, issued++) {
+            const int s = (int)(it % STAGES);
+            if (it >= (uint32_t)STAGES) {
+                if (!mbar_wait_bounded(&empty[s], ((it / STAGES) - 1) & 1u)) {
+                    ok = false;
+                    break;
+                }
+                store_stage(s);
+                bulk_wait_read_all();
+            }
+            unsigned char *st = smem + (size_t)s * FS::bytes;
+            uint32_t *gb = reinterpret_cast<uint32_t *>(st + FS::hdr);
+#pragma unroll
+            for (int i = 0; i < 16; i++) gb[i] = hdr_word(h, i);
+            const uint32_t g0 = gb[0], n = gb[1];
+            const uint32_t nbytes = (gb[2 + n] - gb[2]) * (uint32_t)sizeof(T);
+            const uint32_t items = 32u * n;
+            mbar_arrive_expect_tx(&full[s], nbytes * (DAMP ? 2u : 1u) + 2u * items + 2u * items * (uint32_t)sizeof(T));
+            if (nbytes) {
+                bulk_g2s(st + FS::vbuf, vf + gb[2], nbytes, &full[s]);
+                if (DAMP) bulk_g2s(st + FS::obuf, fv + gb[2], nbytes, &full[s]);
+            }
+            bulk_g2s(st + FS::deg, a.f_deg + 32ull * g0, items, &full[s]);
+            bulk_g2s(st + FS::kind, a.f_kind + 32ull * g0, items, &full[s]);
+            bulk_g2s(st + FS::pq, pq_g + 64ull * g0, 2u * items * (uint32_t)sizeof(T), &full[s]);
+            const uint32_t nt = blockIdx.x + (it + 1) * nb;
+            if (nt < n_tiles) load_hdr(a.thdr + 4ull * nt, h);
+        }
+        if (ok) {  // outputs still held by the last stages
+            const uint32_t first = my_tiles > (uint32_t)STAGES ? my_tiles - STAGES : 0;
+            for (uint32_t it = first; it < my_tiles; it++) {
+                const int s = (int)(it % STAGES);
+                if (!mbar_wait_bounded(&empty[s], (it / STAGES) & 1u)) {
+                    ok = false;
+                    break;
+                }
+                store_stage(s);
+            }
+        }
+        if (!ok) {
+            record_timeout(ctl);
+            // let this block's own loads in flight land before the block exits
+            for (uint32_t k = issued > (uint32_t)STAGES ? issued - STAGES : 0; k < issued; k++)
+                mbar_wait_bounded(&full[k % STAGES], (k / STAGES) & 1u);
+        }
+        bulk_wait_all();
+        return;
+    }
+
+    // consumer warps; when no blocks are dedicated to large factors, they take
+    // those first, while the producer's first loads are in flight
+    if (nb == gridDim.x) {
+        const uint32_t warp = blockIdx.x * kTileGroups + wid, nwarps = gridDim.x * kTileGroups;
+        for (uint32_t b = warp; b < a.nf_big; b += nwarps) factor_warp<T, DAMP>(a, b, lane, vf, fv, d);
+    }
+    for (uint32_t it = 0; it < my_tiles; it++) {
+        const int s = (int)(it % STAGES);
+        if (!mbar_wait_bounded(&full[s], (it / STAGES) & 1u)) {
+            record_timeout(ctl);
+            return;
+        }
+        unsigned char *st = smem + (size_t)s * FS::bytes;
+        const uint32_t *gb = reinterpret_cast<const uint32_t *>(st + FS::hdr);
+        if ((uint32_t)wid < gb[1]) {
+            const int w = (int)((gb[3 + wid] - gb[2 + wid]) >> 5);
+            T *vb = reinterpret_cast<T *>(st + FS::vbuf) + (gb[2 + wid] - gb[2]);
+            const T *ob = reinterpret_cast<const T *>(st + FS::obuf) + (gb[2 + wid] - gb[2]);
+            factor_group<T, DAMP>(w, vb, ob, st + FS::deg + 32 * wid, st + FS::kind + 32 * wid,
+                                  reinterpret_cast<const T *>(st + FS::pq) + 64 * wid, lane, d);
+        }
+        fence_proxy_async();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
+    }
+}
+
+// Leave-one-out message of a variable to the factor of one entry: remove
+// `x` from (S, npos, nneg); both kinds of zero left -> (0.5,0.5); otherwise
+// the remaining zero wins (causal_bp_parall.cu:74-90).
+template <typename T>
+__device__ __forceinline__ T excl_msg(double S, int npos, int nneg, T x) {
+    const T inf = Num<T>::inf();
+    if (x == inf) npos--;
+    else if (x == -inf) nneg--;
+    else S -= (double)x;
+    if (npos > 0 && nneg > 0) return T(0);
+    if (npos > 0) return inf;
+    if (nneg > 0) return -inf;
+    return (T)S;
+}
+
+// Belief P(x=1): b_s = prod_s * [zeros_s == 0], belief = b1 / (b0 + b1)
+// (causal_bp_seq.cu:102-111, causal_bp.cu:510-514).
+__device__ __forceinline__ double belief_of(double S, int npos, int nneg) {
+    if (npos > 0 && nneg > 0) return __longlong_as_double(0x7ff8000000000000ll);
+    if (npos > 0) return 1.0;
+    if (nneg > 0) return 0.0;
+    return 1.0 / (1.0 + ::exp(-S));
+}
+
+// BMODE: 0 no beliefs; 1 beliefs + residual; 2 beliefs + residual + count +
+// history; 3 beliefs only (no residual, no history).
+template <int BMODE>
+__device__ __forceinline__ double var_finish(const VarArgs &a, uint32_t v, double S, int npos, int nneg, double tol,
+                                             double bold, unsigned long long &cnt) {
+    double diff = 0.0;
+    if (BMODE != 0) {
+        const double b = belief_of(S, npos, nneg);
+        if (BMODE == 1 || BMODE == 2) {
+            const double dd = fabs(bold - b);
+            diff = dd;
+            if (BMODE == 2) {
+                if (dd > tol) cnt++;
+                if (isfinite(b)) {
+                    uint32_t slot = a.hist_next[v];
+                    a.hist[(size_t)slot * (a.nv_sell + a.nv_big) + v] = b;
+                    if (++slot == a.hist_len) slot = 0;
+                    a.hist_next[v] = slot;
+                    if (a.hist_count[v] < a.hist_len) a.hist_count[v]++;
+                }
+            }
+        }
+        a.belief[v] = b;
+    }
+    return diff;
+}
+
+template <typename T>
+__device__ __forceinline__ void decode_prior(const void *pr, uint32_t i, double pscale, double &S, int &npos,
+                                             int &nneg) {
+    uint32_t cnt;
+    if (sizeof(T) == 4) {
+        const uint2 x = reinterpret_cast<const uint2 *>(pr)[i];
+        S = (double)__uint_as_float(x.x) * pscale;
+        cnt = x.y;
+    } else {
+        const uint4 x = reinterpret_cast<const uint4 *>(pr)[i];
+        S = __hiloint2double((int)x.y, (int)x.x) * pscale;
+        cnt = x.z;
+    }
+    npos = (int)(cnt & 0xffffu);
+    nneg = (int)(cnt >> 16);
+}
+
+// One sliced-ELL group of 32 variables of width W, staged in shared memory:
+// entry k of the lane-th variable at en[32 k + lane], its prior at pr[lane],
+// its previous belief at bo[lane]. Gathers fv, sums, scatters vf.
+template <typename T, int BMODE, bool WRITE_VF, int W>
+__device__ __forceinline__ double var_group_w(const VarArgs &a, uint32_t v, bool ok, const uint32_t *en,
+                                              const void *pr, const double *bo, int lane, const T *__restrict__ fv,
+                                              T *__restrict__ vf, double pscale, double tol, unsigned long long &cnt) {
+    double S = 0.0;
+    int npos = 0, nneg = 0;
+    if (ok) decode_prior<T>(pr, lane, pscale, S, npos, nneg);
+    const T inf = Num<T>::inf();
+    uint32_t e[W > 0 ? W : 1];
+    T x[W > 0 ? W : 1];
+#pragma unroll
+    for (int k = 0; k < W; k++) e[k] = en[32 * k + lane];
+#pragma unroll
+    for (int k = 0; k < W; k++) x[k] = (e[k] != kSentinel) ? fv[e[k]] : T(0);
+#pragma unroll
+    for (int k = 0; k < W; k++) {
+        if (x[k] == inf) npos++;
+        else if (x[k] == -inf) nneg++;
+        else S += (double)x[k];
+    }
+    if (WRITE_VF) {
+#pragma unroll
+        for (int k = 0; k < W; k++)
+            if (e[k] != kSentinel) vf[e[k]] = excl_msg<T>(S, npos, nneg, x[k]);
+    }
+    return ok ? var_finish<BMODE>(a, v, S, npos, nneg, tol, (BMODE == 1 || BMODE == 2) ? bo[lane] : 0.0, cnt) : 0.0;
+}
+
+template <typename T, int BMODE, bool WRITE_VF>
+__device__ __forceinline__ double var_group(int w, const VarArgs &a, uint32_t v, bool ok, const uint32_t *en,
+                                            const void *pr, const double *bo, int lane, const T *__restrict__ fv,
+                                            T *__restrict__ vf, double pscale, double tol, unsigned long long &cnt) {
+    switch (w) {
+#define FLBP_W(N) \
+    case N: return var_group_w<T, BMODE, WRITE_VF, N>(a, v, ok, en, pr, bo, lane, fv, vf, pscale, tol, cnt);
+        FLBP_W(0) FLBP_W(1) FLBP_W(2) FLBP_W(3) FLBP_W(4) FLBP_W(5) FLBP_W(6) FLBP_W(7) FLBP_W(8) FLBP_W(9)
+        FLBP_W(10) FLBP_W(11) FLBP_W(12) FLBP_W(13) FLBP_W(14) FLBP_W(15) FLBP_W(16)
+#undef FLBP_W
+        default: return 0.0;
+    }
+}
+
+// One large variable, one warp (direct loads).
+template <typename T, int BMODE, bool WRITE_VF>
+__device__ double var_warp(const VarArgs &a, uint32_t b, int lane, const T *__restrict__ fv, T *__restrict__ vf,
+                           double pscale, double tol, unsigned long long &cnt) {
+    const uint32_t v = a.nv_sell + b;
+    const uint32_t k0 = a.vb_off[b], k1 = a.vb_off[b + 1];
+    const T inf = Num<T>::inf();
+    double S = 0.0;
+    int npos = 0, nneg = 0;
+    for (uint32_t k = k0 + lane; k < k1; k += 32) {
+        const T x = fv[a.v_ent[k]];
+        if (x == inf) npos++;
+        else if (x == -inf) nneg++;
+        else S += (double)x;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        S += __shfl_xor_sync(0xffffffffu, S, o);
+        npos += __shfl_xor_sync(0xffffffffu, npos, o);
+        nneg += __shfl_xor_sync(0xffffffffu, nneg, o);
+    }
+    double S0;
+    int p0, n0;
+    decode_prior<T>(a.prior, v, pscale, S0, p0, n0);
+    S += S0;
+    npos += p0;
+    nneg += n0;
+    if (WRITE_VF) {
+        for (uint32_t k = k0 + lane; k < k1; k += 32) {
+            const uint32_t e = a.v_ent[k];
+            vf[e] = excl_msg<T>(S, npos, nneg, fv[e]);
+        }
+    }
+    return (lane == 0) ? var_finish<BMODE>(a, v, S, npos, nneg, tol, a.belief[v], cnt) : 0.0;
+}
+
+__device__ __forceinline__ double warp_max(double x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+    return x;
+}
+
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+// Stop rules evaluated after a sweep by the last block of the variable pass,
+// so that the next launches see ctl->done.
+__device__ void stop_rules(Ctl *ctl) {
+    const double maxdiff = __longlong_as_double((long long)ctl->maxdiff_bits);
+    ctl->maxdiff = maxdiff;
+    unsigned long long now;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+    const double elapsed = (double)(now - ctl->t_start_ns);
+    const long long n = ctl->run_sweeps;
+    if (ctl->status != 0) {  // a device wait gave up: stop the run
+        ctl->done = 1;
+        ctl->reason = FLBP_DIVERGED;
+        return;
+    }
+    if (ctl->mode == 1) {  // causal_bp.cu:866
+        const long long iters = ctl->iters0 + n;
+        const bool cont = iters < ctl->maxiter && maxdiff > ctl->tol && elapsed < ctl->maxtime_ns;
+        if (!cont) {
+            ctl->done = 1;
+            ctl->reason = (maxdiff > ctl->tol) ? FLBP_DIVERGED : FLBP_ALL_CONVERGED;
+        }
+    } else if (ctl->mode == 2) {  // causal_bp.cu:1037-1054, evaluated for the next numIters
+        const double frac = (double)ctl->nonconv / (double)ctl->n_vars;
+        ctl->frac = frac;
+        if (n >= ctl->min_iters)
+            ctl->node_frac_tol = (double)(n - ctl->min_iters) / (double)(ctl->max_iters - ctl->min_iters);
+        if (maxdiff <= ctl->tol) {
+            ctl->done = 1;
+            ctl->reason = FLBP_ALL_CONVERGED;
+        } else if (n > ctl->min_iters && frac < ctl->node_frac_tol) {
+            ctl->done = 1;
+            ctl->reason = FLBP_BIG_FRAC_CONVERGED;
+        } else if (n > ctl->max_iters) {
+            ctl->done = 1;
+            ctl->reason = FLBP_DIVERGED;
+        } else if (elapsed > ctl->maxtime_ns) {
+            ctl->done = 1;
+            ctl->reason = FLBP_DIVERGED;
+        }
+    }
+}
+
+// Variable pass, warp-specialised like the factor pass: warp 8 bulk-loads
+// each tile's entries, priors and (with a residual) previous beliefs; warps
+// 0-7 gather, sum and scatter one group each. Blocks [n_tile_blocks, grid)
+// take the large variables. With BMODE 1/2 the block maxima of |belief
+// change| are combined with an atomic max and the last block to finish
+// applies the stop rules.
+template <typename T, int BMODE, bool WRITE_VF, int STAGES>
+__global__ void __launch_bounds__(288) var_pass_kernel(VarArgs a, const T *__restrict__ fv, T *__restrict__ vf,
+                                                       Ctl *ctl) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES];
+    typedef VarStage<T> VS;
+    constexpr bool RESID = (BMODE == 1 || BMODE == 2);
+    constexpr uint32_t psz = sizeof(T) == 4 ? 8u : 16u;
+    if (*(volatile int *)&ctl->done) return;
+    const double pscale = ctl->pscale;
+    const double tol = ctl->tol;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint32_t n_tiles = a.n_tiles, nb = a.n_tile_blocks;
+    const bool tile_block = blockIdx.x < nb;
+    const uint32_t my_tiles = (tile_block && blockIdx.x < n_tiles) ? (n_tiles - blockIdx.x + nb - 1) / nb : 0;
+    double dmax = 0.0;
+    unsigned long long cnt = 0;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], kTileGroups);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (!tile_block) {  // large variables
+        const uint32_t warp = (blockIdx.x - nb) * (blockDim.x >> 5) + wid;
+        const uint32_t nwarps = (gridDim.x - nb) * (blockDim.x >> 5);
+        for (uint32_t b = warp; b < a.nv_big; b += nwarps)
+            dmax = fmax(dmax, var_warp<T, BMODE, WRITE_VF>(a, b, lane, fv, vf, pscale, tol, cnt));
+    } else if (wid == kTileGroups) {  // producer warp
+        if (lane == 0) {
+            uint4 h[4];
+            if (my_tiles) load_hdr(a.thdr + 4ull * blockIdx.x, h);
+            for (uint32_t it = 0; it < my_tiles; it++) {
+                const int s = (int)(it % STAGES);
+                if (it >= (uint32_t)STAGES && !mbar_wait_bounded(&empty[s], ((it / STAGES) - 1) & 1u)) {
+                    record_timeout(ctl);
+                    // let this block's own loads in flight land before the block moves on
+                    for (uint32_t k = it > (uint32_t)STAGES ? it - STAGES : 0; k < it; k++)
+                        mbar_wait_bounded(&full[k % STAGES], (k / STAGES) & 1u);
+                    break;
+                }
+                unsigned char *st = smem + (size_t)s * VS::bytes;
+                uint32_t *gb = reinterpret_cast<uint32_t *>(st + VS::hdr);
+#pragma unroll
+                for (int i = 0; i < 16; i++) gb[i] = hdr_word(h, i);
+                const uint32_t g0 = gb[0], n = gb[1];
+                const uint32_t ebytes = (gb[2 + n] - gb[2]) * 4u;
+                const uint32_t items = 32u * n;
+                mbar_arrive_expect_tx(&full[s], ebytes + psz * items + (RESID ? 8u * items : 0u));
+                if (ebytes) bulk_g2s(st + VS::ent, a.v_ent + gb[2], ebytes, &full[s]);
+                bulk_g2s(st + VS::prior, reinterpret_cast<const unsigned char *>(a.prior) + 32ull * g0 * psz,
+                         psz * items, &full[s]);
+                if (RESID) bulk_g2s(st + VS::bold, a.belief + 32ull * g0, 8u * items, &full[s]);
+                const uint32_t nt = blockIdx.x + (it + 1) * nb;
+                if (nt < n_tiles) load_hdr(a.thdr + 4ull * nt, h);
+            }
+        }
+    } else {  // consumer warps (large variables first when no blocks are dedicated to them)
+        if (nb == gridDim.x) {
+            const uint32_t warp = blockIdx.x * kTileGroups + wid, nwarps = gridDim.x * kTileGroups;
+            for (uint32_t b = warp; b < a.nv_big; b += nwarps)
+                dmax = fmax(dmax, var_warp<T, BMODE, WRITE_VF>(a, b, lane, fv, vf, pscale, tol, cnt));
+        }
+        for (uint32_t it = 0; it < my_tiles; it++) {
+            const int s = (int)(it % STAGES);
+            if (!mbar_wait_bounded(&full[s], (it / STAGES) & 1u)) {
+                record_timeout(ctl);
+                break;
+            }
+            unsigned char *st = smem + (size_t)s * VS::bytes;
+            const uint32_t *gb = reinterpret_cast<const uint32_t *>(st + VS::hdr);
+            if ((uint32_t)wid < gb[1]) {
+                const int w = (int)((gb[3 + wid] - gb[2 + wid]) >> 5);
+                const uint32_t v = (gb[0] + wid) * 32 + lane;
+                dmax = fmax(dmax, var_group<T, BMODE, WRITE_VF>(
+                                      w, a, v, v < a.nv_sell,
+                                      reinterpret_cast<const uint32_t *>(st + VS::ent) + (gb[2 + wid] - gb[2]),
+                                      st + VS::prior + (size_t)psz * 32 * wid,
+                                      reinterpret_cast<const double *>(st + VS::bold) + 32 * wid, lane, fv, vf,
+                                      pscale, tol, cnt));
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[s]);
+        }
+    }
+    if (RESID) {
+        __shared__ double s_max[9];
+        __shared__ unsigned long long s_cnt[9];
+        __shared__ bool s_last;
+        dmax = warp_max(dmax);
+        cnt = warp_sum(cnt);
+        if (lane == 0) {
+            s_max[wid] = dmax;
+            s_cnt[wid] = cnt;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double m = 0.0;
+            unsigned long long c = 0;
+            for (int i = 0; i < (int)(blockDim.x >> 5); i++) {
+                m = fmax(m, s_max[i]);
+                c += s_cnt[i];
+            }
+            atomicMax(&ctl->maxdiff_bits, (unsigned long long)__double_as_longlong(m));
+            if (BMODE == 2) atomicAdd(&ctl->nonconv, c);
+            __threadfence();
+            const unsigned int prev = atomicAdd(&ctl->arrive, 1u);
+            s_last = (prev == gridDim.x - 1);
+        }
+        __syncthreads();
+        if (s_last && threadIdx.x == 0) {
+            __threadfence();
+            stop_rules(ctl);
+        }
+    }
+}
+
+// Low-pass belief mean, oldest to newest, then one division
+// (HostBeliefHistory::mean, causal_bp.cu:65-77).
+__global__ void lowpass_kernel(const double *hist, const uint32_t *hist_next, const uint32_t *hist_count,
+                               uint32_t hist_len, uint32_t n, double *out) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const uint32_t cnt = hist_count[v];
+    uint32_t slot = (cnt == hist_len) ? hist_next[v] : 0;
+    double sum = 0.0;
+    for (uint32_t s = 0; s < cnt; s++) {
+        sum += hist[(size_t)slot * n + v];
+        if (++slot == hist_len) slot = 0;
+    }
+    if (cnt > 0) sum /= (double)cnt;
+    out[v] = sum;
+}
+
+}  // namespace flbp

@@ -1,0 +1,364 @@
+// Host-side construction of the engine's device layout from a graph in the
+// reference's factor-major order (the arrays of CausalBP::construct(),
+// csrc/ext/causal_bp.cu:310-407).
+//
+// What differs from the reference layout, and why:
+// * Factors whose f->v messages never depend on other messages are folded
+//   into per-variable priors instead of being recomputed every sweep:
+//   singletons (type 0, causal_bp_parall.cu:110-112), AND/OR factors reduced
+//   to their head (the `end_ind - start_ind == 1` cases, :115-117, :154-156),
+//   and the head output of head-clamped factors (types 3/4, :222-238: with a
+//   0/1 mask the normalised result is always the mask's one-hot state).
+// * Factors and variables are sorted by degree and stored as sliced ELL of
+//   width 32 (see engine_internal.h), so a warp handles 32 items of equal
+//   degree with coalesced loads and no divergence; the head of every factor
+//   is its slot 0.
+// * All offsets and indices are 32-bit.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "engine_internal.h"
+
+namespace flbp {
+
+namespace {
+
+constexpr double kInf = std::numeric_limits<double>::infinity();
+
+inline double logit(double p) { return std::log(p) - std::log1p(-p); }
+
+}  // namespace
+
+int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err) {
+    const int64_t V = g.n_vars, F = g.n_factors, E = g.n_slots;
+    if (V < 0 || F < 0 || E < 0) {
+        err = "negative graph size";
+        return FLBP_ERR_INVALID;
+    }
+    if ((F > 0 || E > 0) && (!g.factor_offsets || !g.slot_var || !g.factor_head || !g.factor_type ||
+                             !g.factor_p || !g.factor_q)) {
+        err = "missing graph array";
+        return FLBP_ERR_INVALID;
+    }
+    if (V >= (int64_t)UINT32_MAX || E >= (int64_t)UINT32_MAX) {
+        err = "graph exceeds 2^32-1 variables or edge slots";
+        return FLBP_ERR_LIMIT;
+    }
+    const int64_t *off = g.factor_offsets;
+    if (F > 0 && (off[0] != 0 || off[F] != E)) {
+        err = "factor_offsets must start at 0 and end at n_slots";
+        return FLBP_ERR_INVALID;
+    }
+    if (F == 0 && E != 0) {
+        err = "edge slots without factors";
+        return FLBP_ERR_INVALID;
+    }
+    for (int64_t I = 0; I < F; I++) {
+        if (off[I + 1] < off[I]) {
+            err = "factor_offsets not monotone at factor " + std::to_string(I);
+            return FLBP_ERR_INVALID;
+        }
+    }
+    for (int64_t e = 0; e < E; e++) {
+        if (g.slot_var[e] < 0 || g.slot_var[e] >= V) {
+            err = "slot_var out of range at slot " + std::to_string(e);
+            return FLBP_ERR_INVALID;
+        }
+    }
+
+    L = HostLayout();
+    L.V = V;
+    L.F = F;
+    L.E = E;
+
+    // --- classify factors -------------------------------------------------
+    std::vector<uint8_t> active(F, 0);
+    std::vector<uint8_t> head_state(F, HEAD_FREE);
+    std::vector<double> fconst(F, 0.0);  // constant message of non-active factors / clamped heads
+    for (int64_t I = 0; I < F; I++) {
+        const int64_t d = off[I + 1] - off[I];
+        const int32_t t = g.factor_type[I];
+        const double p = g.factor_p[I], q = g.factor_q[I];
+        if (t != FLBP_SINGLETON && t != FLBP_AND && t != FLBP_OR) {
+            err = "unknown factor type at factor " + std::to_string(I);
+            return FLBP_ERR_INVALID;
+        }
+        if (!(p >= 0.0 && p <= 1.0) || !(q >= 0.0 && q <= 1.0)) {
+            err = "factor probabilities must lie in [0,1] (factor " + std::to_string(I) + ")";
+            return FLBP_ERR_INVALID;
+        }
+        if (d < 1) {
+            err = "factor without variables at factor " + std::to_string(I);
+            return FLBP_ERR_INVALID;
+        }
+        const int64_t h = g.factor_head[I];
+        if (h < off[I] || h >= off[I + 1]) {
+            err = "factor_head outside the factor's slots at factor " + std::to_string(I);
+            return FLBP_ERR_INVALID;
+        }
+        if (t == FLBP_SINGLETON) {
+            if (d != 1) {
+                err = "singleton factor with more than one variable at factor " + std::to_string(I);
+                return FLBP_ERR_INVALID;
+            }
+            fconst[I] = logit(p);  // (1-p, p), causal_bp_parall.cu:110-112
+            continue;
+        }
+        bool clamped = g.factor_head_clamped && g.factor_head_clamped[I];
+        if (clamped) {
+            const double m0 = g.factor_mask0 ? g.factor_mask0[I] : 1.0;
+            const double m1 = g.factor_mask1 ? g.factor_mask1[I] : 1.0;
+            if (!((m0 == 0.0 || m0 == 1.0) && (m1 == 0.0 || m1 == 1.0))) {
+                err = "head_mask entries must be 0 or 1 (factor " + std::to_string(I) + ")";
+                return FLBP_ERR_INVALID;
+            }
+            if (m0 == 1.0 && m1 == 1.0) {
+                clamped = false;  // multiplying by (1,1) changes nothing
+            } else {
+                // causal_bp_parall.cu:222-238 / 271-287: marg*mask normalised, else the mask fallback.
+                fconst[I] = (m0 == 0.0) ? kInf : -kInf;
+                head_state[I] = (m0 == 0.0 && m1 == 1.0) ? HEAD_ONE : (m0 == 1.0 && m1 == 0.0) ? HEAD_ZERO : HEAD_NONE;
+            }
+        }
+        if (d == 1) {
+            if (!clamped) fconst[I] = (t == FLBP_AND) ? logit(p) : -logit(p);  // :115-117, :154-156
+            continue;
+        }
+        active[I] = 1;
+    }
+
+    // --- internal factor order: sliced-ELL factors by degree, then big ones ---------
+    std::vector<int64_t> fact_of_int;
+    uint32_t nf_sell = 0, nf_big = 0;
+    {
+        std::vector<uint32_t> cnt(kSellFactorDegree + 1, 0);
+        for (int64_t I = 0; I < F; I++) {
+            if (!active[I]) continue;
+            const uint64_t d = (uint64_t)(off[I + 1] - off[I]);
+            if (d <= kSellFactorDegree) cnt[d]++, nf_sell++;
+            else nf_big++;
+        }
+        std::vector<uint32_t> pos(kSellFactorDegree + 1, 0);
+        for (uint32_t d = 1; d <= kSellFactorDegree; d++) pos[d] = pos[d - 1] + cnt[d - 1];
+        fact_of_int.assign((size_t)nf_sell + nf_big, 0);
+        uint32_t b = nf_sell;
+        for (int64_t I = 0; I < F; I++) {
+            if (!active[I]) continue;
+            const uint64_t d = (uint64_t)(off[I + 1] - off[I]);
+            if (d <= kSellFactorDegree) fact_of_int[pos[d]++] = I;
+            else fact_of_int[b++] = I;
+        }
+    }
+    const uint32_t nf = nf_sell + nf_big;
+    L.nf_sell = nf_sell;
+    L.nf_big = nf_big;
+    L.f_kind.assign(nf, 0);
+    L.f_deg.assign(nf_sell, 0);
+    L.f_pq.assign(2 * (size_t)nf, 0.0);
+    for (uint32_t f = 0; f < nf; f++) {
+        const int64_t I = fact_of_int[f];
+        L.f_kind[f] = (uint8_t)((g.factor_type[I] == FLBP_OR ? KIND_OR : 0) | head_state[I]);
+        L.f_pq[2 * f] = g.factor_p[I];
+        L.f_pq[2 * f + 1] = g.factor_q[I];
+        if (f < nf_sell) L.f_deg[f] = (uint8_t)(off[I + 1] - off[I]);
+    }
+
+    // --- device slots --------------------------------------------------------------
+    std::vector<uint32_t> dev_slot(E, UINT32_MAX);  // reference slot -> device slot
+    {
+        uint64_t next = 0;
+        const uint32_t ng = (nf_sell + 31) / 32;
+        L.fg_base.assign(ng + 1, 0);
+        for (uint32_t gi = 0; gi < ng; gi++) {
+            const uint32_t f0 = gi * 32, f1 = std::min(nf_sell, gi * 32 + 32);
+            uint32_t w = 0;
+            for (uint32_t f = f0; f < f1; f++) w = std::max<uint32_t>(w, L.f_deg[f]);
+            L.fg_base[gi] = (uint32_t)next;
+            for (uint32_t f = f0; f < f1; f++) {
+                const int64_t I = fact_of_int[f];
+                const uint32_t lane = f - f0;
+                uint64_t k = 0;
+                dev_slot[g.factor_head[I]] = (uint32_t)(next + lane);
+                for (int64_t e = off[I]; e < off[I + 1]; e++)
+                    if (e != g.factor_head[I]) dev_slot[e] = (uint32_t)(next + 32ull * (++k) + lane);
+            }
+            next += 32ull * w;
+            if (next >= UINT32_MAX) break;
+        }
+        if (next < UINT32_MAX) {
+            L.fg_base[ng] = (uint32_t)next;
+            L.fb_off.assign((size_t)nf_big + 1, 0);
+            for (uint32_t b = 0; b < nf_big && next < UINT32_MAX; b++) {
+                const int64_t I = fact_of_int[nf_sell + b];
+                L.fb_off[b] = (uint32_t)next;
+                dev_slot[g.factor_head[I]] = (uint32_t)next++;
+                for (int64_t e = off[I]; e < off[I + 1]; e++)
+                    if (e != g.factor_head[I]) dev_slot[e] = (uint32_t)next++;
+            }
+        }
+        if (next >= UINT32_MAX) {
+            err = "graph exceeds 2^32-1 device slots";
+            return FLBP_ERR_LIMIT;
+        }
+        L.fb_off[nf_big] = (uint32_t)next;
+        L.n_slots = next;
+    }
+
+    // --- variable entries ----------------------------------------------------------
+    // A reference slot reaches its variable through the engine when it is an
+    // active body slot or the head slot of an active factor with a free head.
+    std::vector<uint8_t> entry(E, 0);
+    std::vector<uint32_t> vdeg(V, 0);
+    std::vector<uint32_t> vfirst(V, UINT32_MAX);
+    uint64_t n_act = 0;
+    for (int64_t I = 0; I < F; I++) {
+        if (!active[I]) continue;
+        n_act += (uint64_t)(off[I + 1] - off[I]);
+        for (int64_t e = off[I]; e < off[I + 1]; e++) {
+            if (e == g.factor_head[I] && head_state[I] != HEAD_FREE) continue;
+            entry[e] = 1;
+            const int64_t v = g.slot_var[e];
+            vdeg[v]++;
+            vfirst[v] = std::min(vfirst[v], dev_slot[e]);
+        }
+    }
+    L.n_active_slots = n_act;
+
+    // internal variable order: sliced-ELL variables by (degree, first slot), then big ones
+    std::vector<uint32_t> order(V);
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+        const bool sa = vdeg[a] <= kSellVarDegree, sb = vdeg[b] <= kSellVarDegree;
+        if (sa != sb) return sa;
+        if (!sa) return false;  // big variables keep their order
+        if (vdeg[a] != vdeg[b]) return vdeg[a] < vdeg[b];
+        return vfirst[a] < vfirst[b];
+    });
+    uint32_t nv_sell = 0;
+    for (int64_t i = 0; i < V; i++)
+        if (vdeg[i] <= kSellVarDegree) nv_sell++;
+    L.nv_sell = nv_sell;
+    L.nv_big = (uint32_t)V - nv_sell;
+    L.var_of_internal.assign(order.begin(), order.end());
+    L.internal_of_var.assign(V, 0);
+    for (uint32_t iv = 0; iv < (uint32_t)V; iv++) L.internal_of_var[order[iv]] = iv;
+
+    // per-variable entry lists, sorted by device slot
+    std::vector<uint64_t> vstart((size_t)V + 1, 0);
+    for (int64_t i = 0; i < V; i++) vstart[i + 1] = vstart[i] + vdeg[i];
+    std::vector<uint32_t> ents(vstart[V]);
+    {
+        std::vector<uint64_t> cur(vstart.begin(), vstart.end() - 1);
+        for (int64_t e = 0; e < E; e++)
+            if (entry[e]) ents[cur[g.slot_var[e]]++] = dev_slot[e];
+        for (int64_t i = 0; i < V; i++) std::sort(ents.begin() + vstart[i], ents.begin() + vstart[i + 1]);
+    }
+    {
+        const uint32_t ng = (nv_sell + 31) / 32;
+        L.vg_base.assign(ng + 1, 0);
+        uint64_t nent = 0;
+        for (uint32_t gi = 0; gi < ng; gi++) {
+            uint32_t w = 0;
+            for (uint32_t iv = gi * 32; iv < std::min(nv_sell, gi * 32 + 32); iv++) w = std::max(w, vdeg[order[iv]]);
+            L.vg_base[gi] = (uint32_t)nent;
+            nent += 32ull * w;
+        }
+        uint64_t nbig = 0;
+        for (uint32_t iv = nv_sell; iv < (uint32_t)V; iv++) nbig += vdeg[order[iv]];
+        if (nent + nbig >= UINT32_MAX) {
+            err = "graph exceeds 2^32-1 variable entries";
+            return FLBP_ERR_LIMIT;
+        }
+        L.vg_base[ng] = (uint32_t)nent;
+        L.v_ent.assign(nent + nbig, kSentinel);
+        for (uint32_t gi = 0; gi < ng; gi++) {
+            for (uint32_t iv = gi * 32; iv < std::min(nv_sell, gi * 32 + 32); iv++) {
+                const uint32_t v = order[iv], lane = iv - gi * 32;
+                for (uint32_t k = 0; k < vdeg[v]; k++) L.v_ent[L.vg_base[gi] + 32ull * k + lane] = ents[vstart[v] + k];
+            }
+        }
+        L.vb_off.assign((size_t)L.nv_big + 1, 0);
+        uint64_t pos = nent;
+        for (uint32_t b = 0; b < L.nv_big; b++) {
+            const uint32_t v = order[nv_sell + b];
+            L.vb_off[b] = (uint32_t)pos;
+            for (uint32_t k = 0; k < vdeg[v]; k++) L.v_ent[pos++] = ents[vstart[v] + k];
+        }
+        L.vb_off[L.nv_big] = (uint32_t)pos;
+    }
+
+    // --- tiles: up to kTileGroupsHost groups within kTileSlotsHost slots ----------------
+    auto make_tiles = [](const std::vector<uint32_t> &base, std::vector<uint32_t> &tiles) {
+        tiles.clear();
+        const uint32_t ng = base.empty() ? 0 : (uint32_t)base.size() - 1;
+        uint32_t g = 0;
+        tiles.push_back(0);
+        while (g < ng) {
+            uint32_t n = 0, slots = 0;
+            while (g < ng && n < kTileGroupsHost && slots + (base[g + 1] - base[g]) <= kTileSlotsHost) {
+                slots += base[g + 1] - base[g];
+                n++;
+                g++;
+            }
+            tiles.push_back(g);
+        }
+    };
+    make_tiles(L.fg_base, L.ftiles);
+    make_tiles(L.vg_base, L.vtiles);
+
+    // --- priors ------------------------------------------------------------------
+    L.prior_fin.assign(V, 0.0);
+    L.prior_cnt.assign(V, 0);
+    {
+        std::vector<double> fin(V, 0.0);
+        for (int64_t I = 0; I < F; I++) {
+            if (active[I] && head_state[I] == HEAD_FREE) continue;
+            const uint32_t iv = L.internal_of_var[g.slot_var[g.factor_head[I]]];
+            const double c = fconst[I];
+            if (c == kInf) {
+                if ((L.prior_cnt[iv] & 0xffffu) != 0xffffu) L.prior_cnt[iv] += 1u;
+            } else if (c == -kInf) {
+                if ((L.prior_cnt[iv] >> 16) != 0xffffu) L.prior_cnt[iv] += 1u << 16;
+            } else {
+                fin[iv] += c;
+            }
+        }
+        L.prior_fin = fin;
+    }
+
+    // --- message export map (reference variable-major order) ------------------------
+    L.row_ptr_fv.assign((size_t)V + 1, 0);
+    for (int64_t e = 0; e < E; e++) L.row_ptr_fv[g.slot_var[e] + 1]++;
+    for (int64_t i = 0; i < V; i++) L.row_ptr_fv[i + 1] += L.row_ptr_fv[i];
+    L.ref_fv_src.assign(E, 0);
+    L.ref_const.assign(E, 0.0);
+    L.fm_to_vm.assign(E, 0);
+    L.vm_var.assign(E, 0);
+    {
+        std::vector<int64_t> cur(L.row_ptr_fv.begin(), L.row_ptr_fv.end() - 1);
+        for (int64_t I = 0; I < F; I++) {
+            for (int64_t e = off[I]; e < off[I + 1]; e++) {
+                const int64_t pos = cur[g.slot_var[e]]++;
+                L.fm_to_vm[e] = pos;
+                L.vm_var[pos] = g.slot_var[e];
+                if (entry[e]) {
+                    L.ref_fv_src[pos] = dev_slot[e];
+                } else {
+                    const double c = fconst[I];
+                    L.ref_fv_src[pos] = (c == kInf) ? -2 : (c == -kInf) ? -3 : -1;
+                    L.ref_const[pos] = c;
+                }
+            }
+        }
+    }
+    return FLBP_OK;
+}
+
+}  // namespace flbp

@@ -1,0 +1,210 @@
+/* fastlbp_b200.h - C ABI of the B200 causal loopy-belief-propagation engine.
+ *
+ * This is the drop-in boundary underneath the libDAI-style C++ API
+ * (include/ext/causal_bp.h). Every entry point uses plain pointers and sizes,
+ * returns an int status (FLBP_OK == 0) and never exits the process; the
+ * message of the last failure on the calling thread is available from
+ * flbp_last_error(). Host arrays passed in are copied; the engine owns its
+ * device buffers. One engine handle must be driven by one host thread at a
+ * time; all of its GPU work goes to the stream given at creation (or to a
+ * stream the engine creates).
+ *
+ * FastLBP has no C ABI of its own: each entry point below names the
+ * reference member function (path:line within the FastLBP project) whose
+ * job it takes over.
+ */
+#ifndef FASTLBP_B200_H
+#define FASTLBP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FLBP_OK 0
+#define FLBP_ERR_INVALID 1 /* bad argument or malformed graph */
+#define FLBP_ERR_CUDA 2    /* CUDA runtime error */
+#define FLBP_ERR_NOMEM 3   /* device or host allocation failed */
+#define FLBP_ERR_STATE 4   /* call not valid in the engine's current state */
+#define FLBP_ERR_LIMIT 5   /* graph exceeds an engine limit (e.g. 2^32-1 edge slots) */
+#define FLBP_ERR_TIMEOUT 6 /* a device-side bounded wait gave up */
+
+/* Factor types, as returned by CausalFactor::type() (csrc/ext/causal_factor.cpp:39-50). */
+#define FLBP_SINGLETON 0
+#define FLBP_AND 1
+#define FLBP_OR 2
+
+/* Stop reasons of the run entry points. */
+#define FLBP_ALL_CONVERGED 0
+#define FLBP_BIG_FRAC_CONVERGED 1
+#define FLBP_DIVERGED 2 /* iteration or time limit reached */
+
+/* A causal factor graph in the reference's factor-major edge order: the
+ * arrays CausalBP::construct() derives (csrc/ext/causal_bp.cu:310-407).
+ * Factor I owns edge slots [factor_offsets[I], factor_offsets[I+1]) holding
+ * the indices of vars(I) in ascending label order; factor_head[I] is the
+ * absolute slot of its head variable. */
+typedef struct flbp_graph_desc {
+    int64_t n_vars;
+    int64_t n_factors;
+    int64_t n_slots;                    /* == factor_offsets[n_factors] */
+    const int64_t *factor_offsets;      /* n_factors + 1   (row_ptr_vf)          */
+    const int64_t *slot_var;            /* n_slots         (col_ind_vf)          */
+    const int64_t *factor_head;         /* n_factors       (h_head)              */
+    const int32_t *factor_type;         /* n_factors       FLBP_SINGLETON/AND/OR */
+    const double *factor_p;             /* n_factors       prob()                */
+    const double *factor_q;             /* n_factors       prob_default()        */
+    const int32_t *factor_head_clamped; /* n_factors, may be NULL (none clamped) */
+    const double *factor_mask0;         /* n_factors, may be NULL; head_mask[0], 0 or 1 */
+    const double *factor_mask1;         /* n_factors, may be NULL; head_mask[1], 0 or 1 */
+} flbp_graph_desc;
+
+typedef struct flbp_engine_opts {
+    int32_t precision; /* 32: FP32 log-odds messages (default); 64: FP64 */
+    int32_t device;    /* CUDA device ordinal, -1 = current device */
+    double damping;    /* f->v damping d in [0,1): log-odds mix (1-d)*new + d*old */
+    void *stream;      /* cudaStream_t to use, NULL = engine-owned stream */
+} flbp_engine_opts;
+
+typedef struct flbp_run_info {
+    int64_t sweeps;       /* sweeps performed by this call */
+    int64_t total_sweeps; /* sweeps since init() (the reference's _iters) */
+    double maxdiff;       /* last max |belief change| (NaN when not computed) */
+    double frac;          /* the reference's yetToConvergeFraction */
+    int32_t reason;       /* FLBP_ALL_CONVERGED / BIG_FRAC_CONVERGED / DIVERGED */
+    int32_t status;       /* device status word (0 = ok) */
+    int64_t launches;     /* engine kernels launched by this call */
+} flbp_run_info;
+
+typedef struct flbp_engine flbp_engine;
+
+/* Thread-local text of the last error. */
+const char *flbp_last_error(void);
+
+/* Library version string. */
+const char *flbp_version(void);
+
+/* Build the device layout of a graph and allocate its message buffers.
+ * Replaces CausalBP::construct() + putParallUpdateSeqToKernelFused()
+ * (csrc/ext/causal_bp.cu:310-407, 724-817). */
+int flbp_engine_create(const flbp_graph_desc *graph, const flbp_engine_opts *opts, flbp_engine **out);
+
+/* Release every device and host resource of the engine. */
+int flbp_engine_destroy(flbp_engine *eng);
+
+/* Reset all messages to uniform, beliefs to 0 and the sweep count to 0.
+ * Replaces CausalBP::init() (csrc/ext/causal_bp.cu:824-856). */
+int flbp_init(flbp_engine *eng);
+
+/* Tolerance-driven loop: sweep while sweeps < maxiter, max |belief change| >
+ * tol and elapsed < maxtime seconds. Replaces CausalBP::run()
+ * (csrc/ext/causal_bp.cu:858-910). */
+int flbp_run_tol(flbp_engine *eng, double tol, int64_t maxiter, double maxtime, flbp_run_info *info);
+
+/* Exactly `sweeps` sweeps, then one belief evaluation; low-pass beliefs equal
+ * the beliefs and the returned fraction is 1. Replaces
+ * CausalBP::run(tol, maxIters, histLength) (csrc/ext/causal_bp.cu:912-1004). */
+int flbp_run_fixed(flbp_engine *eng, int64_t sweeps, flbp_run_info *info);
+
+/* Convergence loop with the big-fraction rule and the low-pass belief
+ * history mean. Replaces CausalBP::run(tol, minIters, maxIters, histLength)
+ * (csrc/ext/causal_bp.cu:1006-1143). */
+int flbp_run_lowpass(flbp_engine *eng, double tol, int64_t min_iters, int64_t max_iters, int64_t hist_length,
+                     double maxtime, flbp_run_info *info);
+
+/* `n` bare sweeps (f->v, per-variable totals, v->f) with no belief work.
+ * Replaces calcNewMessageFusedAll() (csrc/ext/causal_bp.cu:409-444). */
+int flbp_sweep(flbp_engine *eng, int64_t n);
+
+/* Beliefs P(x=1) of all variables after the last run, in graph variable
+ * order. Replaces transferBeliefToHost() / beliefV()
+ * (csrc/ext/causal_bp.cu:521-554). */
+int flbp_get_beliefs(flbp_engine *eng, double *out, int64_t n_vars);
+
+/* Low-pass beliefs of the last run (newBelief(), include/ext/causal_bp.h:182-184). */
+int flbp_get_lowpass(flbp_engine *eng, double *out, int64_t n_vars);
+
+/* Beliefs evaluated now from the current messages (no run needed). */
+int flbp_compute_beliefs(flbp_engine *eng, double *out, int64_t n_vars);
+
+/* Current f->v messages as (P(x=0), P(x=1)) pairs in the reference's
+ * variable-major slot order. Replaces transferMessagesToHost()
+ * (csrc/ext/causal_bp.cu:1145-1161). */
+int flbp_get_fv_messages(flbp_engine *eng, double *m0, double *m1, int64_t n_slots);
+
+/* Current v->f messages in the reference's factor-major slot order (slots to
+ * singleton factors and to factors whose outputs are constant report the
+ * variable's message all the same). */
+int flbp_get_vf_messages(flbp_engine *eng, double *m0, double *m1, int64_t n_slots);
+
+/* Layout statistics: counts[0..7] = vars, factors, slots, active factors,
+ * active slots, factors handled warp-wide, variables handled warp-wide,
+ * bytes of device memory held. */
+int flbp_engine_stats(flbp_engine *eng, int64_t *counts, int64_t n_counts);
+
+/* Device duration in milliseconds of the engine's GPU work recorded by the
+ * last run call (CUDA events on the engine stream). */
+int flbp_last_run_ms(flbp_engine *eng, double *ms);
+
+/* ------------------------------------------------------------------------
+ * Graph model (host). The libDAI-style CausalFactorGraph of the C++ API,
+ * exposed for callers without C++ (Python ctypes, other FFIs).
+ * ---------------------------------------------------------------------- */
+
+typedef struct flbp_fg flbp_fg;
+
+/* Read a .causal_fg file. Replaces CausalFactorGraph::ReadFromFile()
+ * (csrc/ext/causal_fg.cpp:118-127, 129-279). */
+int flbp_fg_read_file(const char *path, flbp_fg **out);
+
+/* Parse .causal_fg text held in memory. */
+int flbp_fg_read_string(const char *text, flbp_fg **out);
+
+/* Build from parallel factor arrays (bodies as label CSR; body_off has n+1
+ * entries). Replaces CausalFactorGraph(const std::vector<CausalFactor>&)
+ * (csrc/ext/causal_fg.cpp:50-68). */
+int flbp_fg_from_factors(int64_t n, const int32_t *type, const int64_t *head, const int64_t *body_off,
+                         const int64_t *body, const double *p, const double *q, flbp_fg **out);
+
+int flbp_fg_destroy(flbp_fg *fg);
+
+/* Clamp variable index i to x (0/1). Replaces CausalFactorGraph::clamp()
+ * (csrc/ext/causal_fg.cpp:17-26). Topology is left as it was, as in the
+ * reference; flbp_fg_rebuild() then gives fl_wrapper's rebuilt graph. */
+int flbp_fg_clamp(flbp_fg *fg, int64_t i, int64_t x);
+
+/* New graph from this graph's factors (CausalFactorGraph(fg.factors()),
+ * examples/fl_wrapper.cu:45). */
+int flbp_fg_rebuild(const flbp_fg *fg, flbp_fg **out);
+
+/* Sizes: counts[0..3] = vars, factors, edges (sum of neighbour lists),
+ * slots (sum of |vars(factor)|). */
+int flbp_fg_sizes(const flbp_fg *fg, int64_t *counts);
+
+int flbp_fg_var_labels(const flbp_fg *fg, int64_t *labels, int64_t n);
+
+/* Per-factor fields; vars_off has n_factors+1 entries, vars has n_slots. */
+int flbp_fg_factors(const flbp_fg *fg, int32_t *type, int64_t *head, double *p, double *q, int32_t *clamped,
+                    double *mask0, double *mask1, int64_t *vars_off, int64_t *vars);
+
+/* Neighbour lists (node, iter, dual) of variables (which = 0) or factors
+ * (which = 1), in CSR form. */
+int flbp_fg_neighbors(const flbp_fg *fg, int32_t which, int64_t *off, int64_t *node, int64_t *iter, int64_t *dual);
+
+/* The factor-major arrays of CausalBP::construct() for this graph's factors
+ * (topology rebuilt from vars(), as fl_wrapper does): offsets (F+1),
+ * slot_var, head, plus the per-variable CSR of the variable-major order
+ * (row_ptr_fv, V+1) and its factor column (col_ind_fv). */
+int flbp_fg_construct(const flbp_fg *fg, int64_t *factor_offsets, int64_t *slot_var, int64_t *factor_head,
+                      int64_t *row_ptr_fv, int64_t *col_ind_fv);
+
+/* Engine straight from a graph-model handle (what CausalBP's constructor does). */
+int flbp_engine_create_from_fg(const flbp_fg *fg, const flbp_engine_opts *opts, flbp_engine **out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FASTLBP_B200_H */

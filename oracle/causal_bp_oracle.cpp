@@ -1,0 +1,959 @@
+// FP64 CPU restatement of FastLBP's causal loopy-BP PARALL path.
+//
+// TEST INFRASTRUCTURE ONLY. This file is the correctness oracle: only the
+// tests, the smoke check and the CPU-baseline leg of the benchmark may load
+// it, and only as the checker. The product path (fastlbp_b200/) never links,
+// loads or calls anything in oracle/.
+//
+// Every routine restates one piece of the reference (paths relative to the
+// FastLBP project root) in plain double-precision C++:
+//   * .causal_fg reader ........ csrc/ext/causal_fg.cpp:129-279, include/utils/utils.h:109-113
+//   * graph construction ....... csrc/ext/causal_fg.cpp:28-68, csrc/lbp/bipgraph.cpp:24-42
+//   * clamping ................. csrc/ext/causal_fg.cpp:17-26, csrc/ext/causal_factor.cpp:63-100
+//   * CSR + edge records ....... csrc/ext/causal_bp.cu:310-407, 556-581, 724-817
+//   * init ..................... csrc/ext/causal_bp.cu:824-856
+//   * f->v kernel (types 0-8) .. csrc/kernel/causal_bp_parall.cu:14-18, 94-398
+//   * per-variable product ..... csrc/kernel/causal_bp_parall.cu:20-53
+//   * v->f kernel .............. csrc/kernel/causal_bp_parall.cu:55-92
+//   * beliefs .................. csrc/kernel/causal_bp_seq.cu:102-111, csrc/ext/causal_bp.cu:483-515
+//   * run loops ................ csrc/ext/causal_bp.cu:858-910, 912-1004, 1006-1143 (+ HostBeliefHistory :28-78)
+//
+// Damping is not part of the reference. It is defined here once, for the
+// oracle and the GPU engine alike: after the f->v sweep each new f->v message
+// is mixed geometrically with the previous one, m <- m_new^(1-d) * m_old^d,
+// then normalised; a (0,0) result becomes (0.5,0.5) (the reference's rule for
+// an all-zero message). With d == 0 the mixing step is skipped entirely, so
+// the restatement reduces exactly to the reference.
+//
+// Built with -ffp-contract=off so results are deterministic; expect agreement
+// with the reference GPU binary to ~1e-12, not bit-exactly (nvcc contracts
+// multiply-adds into FMAs by default).
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <limits>
+#include <map>
+#include <set>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <sys/time.h>
+#include <unordered_map>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// ---------------------------------------------------------------- graph model
+
+struct OFactor {
+    int type = 0;                 // 0 Singleton 'I', 1 DefiniteAnd '*', 2 DefiniteOr '+'
+    uint64_t head = 0;            // label
+    std::vector<uint64_t> body;   // sorted unique labels
+    std::vector<uint64_t> vars;   // sorted unique labels of body + head
+    double p = 0.0, q = 0.0;
+    bool head_clamped = false;
+    double mask0 = 1.0, mask1 = 1.0;
+};
+
+struct ONb {
+    size_t iter, node, dual;
+};
+
+struct OGraph {
+    std::vector<OFactor> factors;
+    std::vector<uint64_t> vars;           // sorted labels
+    std::vector<std::vector<ONb>> nbV;    // per variable: factors in factor order
+    std::vector<std::vector<ONb>> nbF;    // per factor: variables in label order
+};
+
+void insert_sorted(std::vector<uint64_t> &s, uint64_t x) {
+    auto it = std::lower_bound(s.begin(), s.end(), x);
+    if (it == s.end() || *it != x) s.insert(it, x);
+}
+
+void erase_sorted(std::vector<uint64_t> &s, uint64_t x) {
+    auto it = std::lower_bound(s.begin(), s.end(), x);
+    if (it != s.end() && *it == x) s.erase(it);
+}
+
+OFactor make_singleton(uint64_t v, double p) {
+    OFactor f;
+    f.type = 0;
+    f.head = v;
+    f.p = p;
+    f.q = 0.0;
+    f.vars = {v};
+    return f;
+}
+
+OFactor make_rule(uint64_t head, std::vector<uint64_t> body, bool is_and, double p, double q) {
+    OFactor f;
+    f.type = is_and ? 1 : 2;
+    f.head = head;
+    std::sort(body.begin(), body.end());
+    body.erase(std::unique(body.begin(), body.end()), body.end());
+    f.body = body;
+    f.vars = body;
+    insert_sorted(f.vars, head);
+    f.p = p;
+    f.q = q;
+    return f;
+}
+
+// csrc/ext/causal_fg.cpp:50-68 and :28-48; csrc/lbp/bipgraph.cpp:24-42 (no duplicate check).
+OGraph build_graph(const std::vector<OFactor> &facs) {
+    OGraph g;
+    g.factors = facs;
+    std::set<uint64_t> vs;
+    for (auto &f : facs) vs.insert(f.vars.begin(), f.vars.end());
+    g.vars.assign(vs.begin(), vs.end());
+    std::unordered_map<uint64_t, size_t> idx;
+    idx.reserve(g.vars.size() * 2 + 1);
+    for (size_t i = 0; i < g.vars.size(); i++) idx[g.vars[i]] = i;
+    g.nbV.assign(g.vars.size(), {});
+    g.nbF.assign(facs.size(), {});
+    for (size_t I = 0; I < facs.size(); I++) {
+        for (uint64_t lab : facs[I].vars) {
+            size_t i = idx[lab];
+            ONb n1{g.nbV[i].size(), I, g.nbF[I].size()};
+            ONb n2{n1.dual, i, n1.iter};
+            g.nbV[i].push_back(n1);
+            g.nbF[I].push_back(n2);
+        }
+    }
+    return g;
+}
+
+// include/utils/utils.h:109-113: skip following lines that start with '#'.
+void skip_annotation(std::istream &is) {
+    std::string tmp;
+    while (is.peek() == '#') std::getline(is, tmp);
+}
+
+// csrc/ext/causal_fg.cpp:129-279.
+std::vector<OFactor> parse_causal_fg(std::istream &is) {
+    std::vector<OFactor> facs;
+    std::string line;
+    std::getline(is, line);
+    skip_annotation(is);
+    size_t nr = (size_t)std::stoi(line);
+    std::set<uint64_t> heads, all_vars;
+    for (size_t I = 0; I < nr; I++) {
+        std::getline(is, line);  // the separating blank line (content ignored)
+        std::getline(is, line);
+        skip_annotation(is);
+        uint64_t head = (uint64_t)(size_t)std::stoi(line);
+        heads.insert(head);
+        all_vars.insert(head);
+        std::getline(is, line);
+        skip_annotation(is);
+        char ch = line.front();
+        if (ch != 'I' && ch != '*' && ch != '+') throw std::runtime_error("Unreachable");
+        if (ch == 'I') {
+            std::getline(is, line);
+            skip_annotation(is);
+            double prob = (double)std::stold(line);
+            facs.push_back(make_singleton(head, prob));
+        } else {
+            double prob = 1.0, prob_default = 0.0;
+            if (line.length() > 1) {
+                size_t sp = line.find(';');
+                if (sp > 1) prob = (double)std::stold(line.substr(1, sp - 1));
+                if (sp != std::string::npos && sp + 1 != line.length())
+                    prob_default = (double)std::stold(line.substr(sp + 1));
+            }
+            std::getline(is, line);
+            skip_annotation(is);
+            size_t blen = (size_t)std::stoi(line);
+            std::getline(is, line);
+            skip_annotation(is);
+            std::istringstream ss(line);
+            std::vector<uint64_t> body;
+            for (size_t b = 0; b < blen; b++) {
+                long id = 0;
+                ss >> id;
+                body.push_back((uint64_t)(size_t)id);
+                all_vars.insert((uint64_t)(size_t)id);
+            }
+            facs.push_back(make_rule(head, body, ch == '*', prob, prob_default));
+        }
+    }
+    for (uint64_t v : all_vars)
+        if (!heads.count(v)) facs.push_back(make_singleton(v, 0.5));
+    return facs;
+}
+
+// csrc/ext/causal_factor.cpp:63-100.
+OFactor gen_clamped(const OFactor &f, uint64_t v, size_t x) {
+    OFactor nf = f;
+    if (f.type == 0) {
+        if (v == f.head) nf.p = (double)x;
+        return nf;
+    }
+    if (v == f.head) {
+        nf.head_clamped = true;
+        double m0 = (x == 0) ? 1.0 : 0.0, m1 = (x == 1) ? 1.0 : 0.0;
+        if (x > 1) throw std::out_of_range("clamp value");
+        if (f.head_clamped) {
+            m0 *= f.mask0;
+            m1 *= f.mask1;
+        }
+        nf.mask0 = m0;
+        nf.mask1 = m1;
+    } else if (std::binary_search(f.body.begin(), f.body.end(), v)) {
+        erase_sorted(nf.body, v);
+        erase_sorted(nf.vars, v);
+        if ((x == 0 && f.type == 1) || (x > 0 && f.type == 2)) {
+            nf.p = f.q;
+            nf.body.clear();
+            nf.vars = {f.head};
+        }
+    }
+    return nf;
+}
+
+// csrc/ext/causal_fg.cpp:17-26 (topology is deliberately left as it was).
+void clamp_graph(OGraph &g, size_t i, size_t x) {
+    std::map<size_t, OFactor> nf;
+    for (auto &n : g.nbV[i]) nf.emplace(n.node, gen_clamped(g.factors[n.node], g.vars[i], x));
+    for (auto &kv : nf) g.factors[kv.first] = kv.second;
+}
+
+// ------------------------------------------------------------ CSR + records
+
+struct ORec {  // Index6Real4 of include/utils/utils.h:48-51
+    size_t type, v, src, start, end, head;
+    double q, p, m0, m1;
+};
+
+struct OVfRec {  // Index3 of include/utils/utils.h:29-31
+    size_t ind, v, src;
+};
+
+struct OLayout {
+    std::vector<size_t> row_ptr_vf, col_ind_vf, row_ptr_fv, col_ind_fv, head;
+    std::vector<ORec> rec;     // variable-major order
+    std::vector<OVfRec> vf;    // factor-major order
+};
+
+// csrc/ext/causal_bp.cu:556-581.
+void coo2csr(const std::vector<size_t> &rows, const std::vector<size_t> &cols, size_t nrows,
+             std::vector<size_t> &ptr, std::vector<size_t> &ind) {
+    ptr.assign(nrows + 1, 0);
+    ind.assign(rows.size(), 0);
+    std::vector<size_t> cnt(nrows, 0);
+    for (size_t r : rows) cnt[r]++;
+    for (size_t i = 0; i < nrows; i++) ptr[i + 1] = ptr[i] + cnt[i];
+    std::vector<size_t> cur(nrows, 0);
+    for (size_t k = 0; k < rows.size(); k++) {
+        size_t r = rows[k];
+        ind[ptr[r] + cur[r]++] = cols[k];
+    }
+}
+
+// csrc/ext/causal_bp.cu:310-407 and :724-817 (PARALL branch).
+OLayout construct(const OGraph &g) {
+    OLayout L;
+    size_t F = g.factors.size(), V = g.vars.size();
+    size_t len = 0;
+    for (auto &f : g.factors) len += f.vars.size();
+    std::vector<size_t> rows(len), cols(len);
+    L.head.assign(F, 0);
+    size_t idx = 0;
+    for (size_t I = 0; I < F; I++) {
+        uint64_t hl = g.factors[I].head;
+        for (auto &n : g.nbF[I]) {
+            rows[idx] = I;
+            cols[idx] = n.node;
+            if (g.vars[n.node] == hl) L.head[I] = idx;
+            idx++;
+        }
+    }
+    coo2csr(rows, cols, F, L.row_ptr_vf, L.col_ind_vf);
+    idx = 0;
+    for (size_t i = 0; i < V; i++) {
+        for (auto &n : g.nbV[i]) {
+            rows[idx] = i;
+            cols[idx] = n.node;
+            idx++;
+        }
+    }
+    coo2csr(rows, cols, V, L.row_ptr_fv, L.col_ind_fv);
+
+    L.rec.reserve(len);
+    for (size_t i = 0; i < V; i++) {
+        for (auto &n : g.nbV[i]) {
+            size_t I = n.node;
+            const OFactor &f = g.factors[I];
+            ORec r;
+            r.v = i;
+            r.src = L.row_ptr_vf[I] + n.dual;
+            r.start = L.row_ptr_vf[I];
+            r.end = L.row_ptr_vf[I + 1];
+            r.head = L.head[I];
+            r.q = f.q;
+            r.p = f.p;
+            r.m0 = f.mask0;
+            r.m1 = f.mask1;
+            bool is_head = (f.head == g.vars[i]);
+            if (f.type == 0) r.type = 0;
+            else if (f.type == 1) r.type = f.head_clamped ? (is_head ? 3 : 7) : (is_head ? 1 : 5);
+            else r.type = f.head_clamped ? (is_head ? 4 : 8) : (is_head ? 2 : 6);
+            L.rec.push_back(r);
+        }
+    }
+    L.vf.reserve(len);
+    for (size_t I = 0; I < F; I++)
+        for (auto &n : g.nbF[I])
+            L.vf.push_back({L.row_ptr_vf[I] + n.iter, n.node, L.row_ptr_fv[n.node] + n.dual});
+    return L;
+}
+
+// ------------------------------------------------------------------ kernels
+
+inline void scale2(double &x, double &y) {  // csrc/kernel/causal_bp_parall.cu:14-18
+    double m = std::fmax(x, y);
+    x /= m;
+    y /= m;
+}
+
+// One f->v message, csrc/kernel/causal_bp_parall.cu:102-397.
+void fv_message(const ORec &r, const double *vf0, const double *vf1, double &out0, double &out1) {
+    const size_t type = r.type, src = r.src, h = r.head, s = r.start, e = r.end;
+    const double p0 = r.q, p1 = r.p, mask0 = r.m0, mask1 = r.m1;
+    double marg0 = 0.0, marg1 = 0.0;
+    if (type == 0) {
+        marg0 = 1 - p1;
+        marg1 = p1;
+    } else if (type == 1 || type == 3) {
+        double prod_1 = 1.0, prod_10 = 1.0;
+        if (e - s == 1) {
+            marg0 = 1 - p1;
+            marg1 = p1;
+        } else if (e - s == 2) {
+            size_t j = s;
+            if (s == src) j++;
+            double m_0 = vf0[j], m_1 = vf1[j];
+            marg0 = (1 - p1) * m_1 + (1 - p0) * m_0;
+            marg1 = p1 * m_1 + p0 * m_0;
+        } else {
+            double e1 = 0;
+            for (size_t j = s; j < e; j++) {
+                if (j == src) continue;
+                double m_0 = vf0[j], m_1 = vf1[j];
+                double a0 = m_0 + m_1, a1 = m_1;
+                prod_1 *= a1;
+                prod_10 *= a0;
+                scale2(prod_1, prod_10);
+                double delta = m_0;
+                if (a1 != 0 && a0 == a1 && delta != 0) e1 += delta / a1;
+            }
+            marg0 = (1 - p1) * prod_1 + (1 - p0) * (e1 * prod_10 + (prod_10 - prod_1));
+            marg1 = p1 * prod_1 + p0 * (e1 * prod_10 + (prod_10 - prod_1));
+        }
+        if (type == 3) {
+            marg0 *= mask0;
+            marg1 *= mask1;
+        }
+        double marg = marg0 + marg1;
+        if (marg != 0) {
+            marg0 = marg0 / marg;
+            marg1 = marg1 / marg;
+        } else if (type == 3 && mask0 == 0) {
+            marg0 = 0.0;
+            marg1 = 1.0;
+        } else if (type == 3 && mask1 == 0) {
+            marg0 = 1.0;
+            marg1 = 0.0;
+        } else {
+            marg0 = 0.5;
+            marg1 = 0.5;
+        }
+    } else if (type == 2 || type == 4) {
+        double prod_0 = 1.0, prod_10 = 1.0;
+        if (e - s == 1) {
+            marg0 = p1;
+            marg1 = 1 - p1;
+        } else if (e - s == 2) {
+            size_t j = s;
+            if (s == src) j++;
+            double m_0 = vf0[j], m_1 = vf1[j];
+            marg0 = p1 * m_0 + p0 * m_1;
+            marg1 = (1 - p1) * m_0 + (1 - p0) * m_1;
+        } else {
+            double e1 = 0;
+            for (size_t j = s; j < e; j++) {
+                if (j == src) continue;
+                double m_0 = vf0[j], m_1 = vf1[j];
+                double a0 = m_0 + m_1, a1 = m_0;
+                prod_0 *= a1;
+                prod_10 *= a0;
+                scale2(prod_0, prod_10);
+                double delta = m_1;
+                if (a1 != 0 && a0 == a1 && delta != 0) e1 += delta / a1;
+            }
+            marg0 = p1 * prod_0 + p0 * (e1 * prod_10 + (prod_10 - prod_0));
+            marg1 = (1 - p1) * prod_0 + (1 - p0) * (e1 * prod_10 + (prod_10 - prod_0));
+        }
+        if (type == 4) {
+            marg0 *= mask0;
+            marg1 *= mask1;
+        }
+        double marg = marg0 + marg1;
+        if (marg != 0) {
+            marg0 = marg0 / marg;
+            marg1 = marg1 / marg;
+        } else if (type == 4 && mask0 == 0) {
+            marg0 = 0.0;
+            marg1 = 1.0;
+        } else if (type == 4 && mask1 == 0) {
+            marg0 = 1.0;
+            marg1 = 0.0;
+        } else {
+            marg0 = 0.5;
+            marg1 = 0.5;
+        }
+    } else if (type == 5 || type == 7) {
+        double m0h = vf0[h], m1h = vf1[h];
+        double prod_1, prod_10;
+        if (type == 5) {
+            prod_1 = (p1 - p0) * (m1h - m0h);
+            prod_10 = p0 * m1h + (1 - p0) * m0h;
+        } else {
+            prod_1 = (p1 - p0) * (m1h * mask1 - m0h * mask0);
+            prod_10 = p0 * m1h * mask1 + (1 - p0) * m0h * mask0;
+        }
+        scale2(prod_1, prod_10);
+        if (prod_10 != 0) {
+            for (size_t j = s; j < e; j++) {
+                if (j == src || j == h) continue;
+                double m0 = vf0[j], m1 = vf1[j], m = m0 + m1;
+                prod_10 *= m;
+                prod_1 *= m1;
+                scale2(prod_1, prod_10);
+            }
+        }
+        marg0 = prod_10;
+        marg1 = prod_10 + prod_1;
+        double marg = marg0 + marg1;
+        if (marg != 0) {
+            marg0 = marg0 / marg;
+            marg1 = marg1 / marg;
+        } else {
+            marg0 = 0.5;
+            marg1 = 0.5;
+        }
+    } else {  // 6 or 8
+        double m0h = vf0[h], m1h = vf1[h];
+        double prod_0, prod_10;
+        if (type == 6) {
+            prod_0 = (p1 - p0) * (m0h - m1h);
+            prod_10 = p0 * m0h + (1 - p0) * m1h;
+        } else {
+            prod_0 = (p1 - p0) * (m0h * mask0 - m1h * mask1);
+            prod_10 = p0 * m0h * mask0 + (1 - p0) * m1h * mask1;
+        }
+        scale2(prod_0, prod_10);
+        if (prod_10 != 0) {
+            for (size_t j = s; j < e; j++) {
+                if (j == src || j == h) continue;
+                double m0 = vf0[j], m1 = vf1[j], m = m0 + m1;
+                prod_10 *= m;
+                prod_0 *= m0;
+                scale2(prod_0, prod_10);
+            }
+        }
+        marg0 = prod_0 + prod_10;
+        marg1 = prod_10;
+        double marg = marg0 + marg1;
+        if (marg != 0) {
+            marg0 = marg0 / marg;
+            marg1 = marg1 / marg;
+        } else {
+            marg0 = 0.5;
+            marg1 = 0.5;
+        }
+    }
+    out0 = marg0;
+    out1 = marg1;
+}
+
+double now_s() {
+    struct timeval tv;
+    gettimeofday(&tv, nullptr);
+    return (double)tv.tv_sec + (double)tv.tv_usec / 1e6;
+}
+
+// ------------------------------------------------------------- BP engine
+
+struct OBP {
+    OGraph g;  // CausalBP copies the graph (include/lbp/daialg.h:21)
+    OLayout L;
+    size_t V = 0, E = 0;
+    double damping = 0.0;
+    int nthreads = 1;
+    std::vector<double> fv0, fv1, vf0, vf1, prod0, prod1, bel0, bel1;
+    std::vector<size_t> nz0, nz1;
+    std::vector<double> oldBeliefs, beliefs, lowpass;
+    std::vector<double> damp_old0, damp_old1;
+    size_t iters = 0;
+    double maxdiff_member = 0.0;
+    bool logdomain = false;
+};
+
+void bp_init(OBP &b) {  // csrc/ext/causal_bp.cu:824-856
+    double c = b.logdomain ? 0.0 : 1.0;
+    std::fill(b.fv0.begin(), b.fv0.end(), c);
+    std::fill(b.fv1.begin(), b.fv1.end(), c);
+    std::fill(b.vf0.begin(), b.vf0.end(), c);
+    std::fill(b.vf1.begin(), b.vf1.end(), c);
+    std::fill(b.prod0.begin(), b.prod0.end(), c);
+    std::fill(b.prod1.begin(), b.prod1.end(), c);
+    std::fill(b.nz0.begin(), b.nz0.end(), 0);
+    std::fill(b.nz1.begin(), b.nz1.end(), 0);
+}
+
+inline double powz(double x, double a) {  // x^a with 0^0 = 1 and 0^a = 0 for a > 0
+    if (a == 0.0) return 1.0;
+    if (x == 0.0) return 0.0;
+    return std::pow(x, a);
+}
+
+// csrc/ext/causal_bp.cu:409-444: f->v, per-variable product, v->f.
+void bp_sweep(OBP &b) {
+    const long E = (long)b.E, V = (long)b.V;
+    const double d = b.damping;
+    const ORec *rec = b.L.rec.data();
+#pragma omp parallel for schedule(dynamic, 4096) num_threads(b.nthreads)
+    for (long i = 0; i < E; i++) {
+        double o0, o1;
+        fv_message(rec[i], b.vf0.data(), b.vf1.data(), o0, o1);
+        if (d != 0.0) {
+            double n0 = powz(o0, 1.0 - d) * powz(b.fv0[i], d);
+            double n1 = powz(o1, 1.0 - d) * powz(b.fv1[i], d);
+            if (n0 == 0 && n1 == 0) {
+                n0 = 0.5;
+                n1 = 0.5;
+            }
+            double s = n0 + n1;
+            o0 = n0 / s;
+            o1 = n1 / s;
+        }
+        b.fv0[i] = o0;
+        b.fv1[i] = o1;
+    }
+    const size_t *rp = b.L.row_ptr_fv.data();
+#pragma omp parallel for schedule(dynamic, 4096) num_threads(b.nthreads)
+    for (long i = 0; i < V; i++) {  // csrc/kernel/causal_bp_parall.cu:30-52
+        double pr0 = 1.0, pr1 = 1.0;
+        size_t z0 = 0, z1 = 0;
+        for (size_t j = rp[i]; j < rp[i + 1]; j++) {
+            double m0 = b.fv0[j], m1 = b.fv1[j];
+            if (m0 == 0) z0++;
+            else pr0 *= m0;
+            if (m1 == 0) z1++;
+            else pr1 *= m1;
+            scale2(pr0, pr1);
+        }
+        b.prod0[i] = pr0;
+        b.prod1[i] = pr1;
+        b.nz0[i] = z0;
+        b.nz1[i] = z1;
+    }
+    const OVfRec *vr = b.L.vf.data();
+#pragma omp parallel for schedule(dynamic, 4096) num_threads(b.nthreads)
+    for (long k = 0; k < E; k++) {  // csrc/kernel/causal_bp_parall.cu:67-91
+        const OVfRec &x = vr[k];
+        size_t c0 = b.nz0[x.v], c1 = b.nz1[x.v];
+        double ms0 = b.fv0[x.src], ms1 = b.fv1[x.src];
+        double pr0 = b.prod0[x.v], pr1 = b.prod1[x.v];
+        if (c0 >= 2 || (c0 == 1 && ms0 != 0)) pr0 = 0.0;
+        else if (ms0 != 0) pr0 = pr0 / ms0;
+        if (c1 >= 2 || (c1 == 1 && ms1 != 0)) pr1 = 0.0;
+        else if (ms1 != 0) pr1 = pr1 / ms1;
+        if (pr0 == 0 && pr1 == 0) pr0 = pr1 = 0.5;
+        double pr = pr0 + pr1;
+        b.vf0[x.ind] = pr0 / pr;
+        b.vf1[x.ind] = pr1 / pr;
+    }
+}
+
+// csrc/ext/causal_bp.cu:483-515 with getBeliefsV (causal_bp_seq.cu:102-111).
+void bp_beliefs(const OBP &b, std::vector<double> &out) {
+    out.resize(b.V);
+    for (size_t i = 0; i < b.V; i++) {
+        double x = b.prod0[i] * (double)(!b.nz0[i]);
+        double y = b.prod1[i] * (double)(!b.nz1[i]);
+        out[i] = y / (x + y);
+    }
+}
+
+OBP *bp_create(const OGraph &g, double damping, int nthreads) {
+    OBP *b = new OBP();
+    b->g = g;
+    b->L = construct(b->g);
+    b->V = g.vars.size();
+    b->E = b->L.rec.size();
+    b->damping = damping;
+    b->nthreads = nthreads < 1 ? 1 : nthreads;
+    b->fv0.assign(b->E, 0);
+    b->fv1.assign(b->E, 0);
+    b->vf0.assign(b->E, 0);
+    b->vf1.assign(b->E, 0);
+    b->prod0.assign(b->V, 0);
+    b->prod1.assign(b->V, 0);
+    b->nz0.assign(b->V, 0);
+    b->nz1.assign(b->V, 0);
+    b->oldBeliefs.assign(b->V, 0.0);  // value-initialised device vector (causal_bp.cu:371)
+    b->beliefs.assign(b->V, 0.0);
+    return b;
+}
+
+// csrc/ext/causal_bp.cu:858-910.
+void bp_run_tol(OBP &b, double tol, size_t maxiter, double maxtime, double *maxdiff_out) {
+    double tic = now_s();
+    double maxDiff = INFINITY;
+    std::vector<double> nb;
+    for (; b.iters < maxiter && maxDiff > tol && (now_s() - tic) < maxtime; b.iters++) {
+        bp_sweep(b);
+        maxDiff = -INFINITY;
+        bp_beliefs(b, nb);
+        double diff = 0.0;  // thrust::reduce(max) with init 0.0
+        for (size_t i = 0; i < b.V; i++) {
+            double dd = std::fabs(b.oldBeliefs[i] - nb[i]);
+            diff = (diff < dd) ? dd : diff;  // thrust::maximum keeps the left operand on NaN
+        }
+        maxDiff = std::max(diff, maxDiff);
+        b.oldBeliefs = nb;
+    }
+    b.beliefs = b.oldBeliefs;
+    if (maxdiff_out) *maxdiff_out = maxDiff;
+}
+
+// csrc/ext/causal_bp.cu:912-1004: exactly maxIters sweeps, beliefs once at the end.
+double bp_run_fixed(OBP &b, double /*tol*/, size_t maxIters, size_t /*hist*/) {
+    for (size_t n = 0; n < maxIters; n++, b.iters++) bp_sweep(b);
+    std::vector<double> nb;
+    bp_beliefs(b, nb);
+    b.oldBeliefs = nb;
+    b.beliefs = b.oldBeliefs;
+    b.lowpass = b.beliefs;
+    return 1.0;
+}
+
+// csrc/ext/causal_bp.cu:1006-1143 with HostBeliefHistory (:28-78).
+double bp_run_lowpass(OBP &b, double tol, size_t minIters, size_t maxIters, size_t hist, double maxtime,
+                      int *reason_out, size_t *sweeps_out) {
+    double tic = now_s();
+    size_t numIters = 0;
+    double maxDiff = INFINITY, frac = 1.0, nodeFracTol = 0.0;
+    const size_t V = b.V;
+    std::vector<double> hvals(V * (hist ? hist : 1));
+    std::vector<size_t> hnext(V, 0), hcount(V, 0);
+    int reason = 2;  // 0 ALL_CONVERGED, 1 BIG_FRAC_CONVERGED, 2 DIVERGED
+    std::vector<double> nb;
+    for (;; numIters++, b.iters++) {
+        if (numIters >= minIters) nodeFracTol = (double)(numIters - minIters) / (double)(maxIters - minIters);
+        if (maxDiff <= tol) {
+            reason = 0;
+            break;
+        } else if (numIters > minIters && frac < nodeFracTol) {
+            reason = 1;
+            break;
+        } else if (numIters > maxIters) {
+            reason = 2;
+            break;
+        } else if ((now_s() - tic) > maxtime) {
+            reason = 2;
+            break;
+        }
+        bp_sweep(b);
+        bp_beliefs(b, nb);
+        double diff = 0.0;
+        size_t nonconv = 0;
+        for (size_t i = 0; i < V; i++) {
+            double dd = std::fabs(b.oldBeliefs[i] - nb[i]);
+            diff = (diff < dd) ? dd : diff;
+            nonconv += (size_t)(dd > tol);
+        }
+        b.oldBeliefs = nb;
+        maxDiff = std::max(diff, -(double)INFINITY);
+        for (size_t i = 0; i < V; i++) {
+            double v = nb[i];
+            int c = std::fpclassify(v);
+            if (c != FP_NORMAL && c != FP_SUBNORMAL && c != FP_ZERO) continue;
+            size_t slot = hnext[i];
+            hvals[slot * V + i] = v;
+            if (++slot == hist) slot = 0;
+            hnext[i] = slot;
+            if (hcount[i] < hist) hcount[i]++;
+        }
+        frac = V ? (double)nonconv / (double)V : NAN;
+    }
+    if (maxDiff > b.maxdiff_member) b.maxdiff_member = maxDiff;
+    b.beliefs = b.oldBeliefs;
+    b.lowpass.assign(V, 0.0);
+    for (size_t i = 0; i < V; i++) {
+        if (reason == 0) {
+            b.lowpass[i] = b.beliefs[i];
+        } else {
+            size_t cnt = hcount[i];
+            size_t slot = (cnt == hist) ? hnext[i] : 0;
+            double sum = 0.0;
+            for (size_t s = 0; s < cnt; s++) {
+                sum += hvals[slot * V + i];
+                if (++slot == hist) slot = 0;
+            }
+            if (cnt > 0) sum /= (double)cnt;
+            b.lowpass[i] = sum;
+        }
+    }
+    if (reason_out) *reason_out = reason;
+    if (sweeps_out) *sweeps_out = numIters;
+    return frac;
+}
+
+thread_local std::string g_err;
+
+template <class F>
+int guarded(F &&f) {
+    try {
+        f();
+        return 0;
+    } catch (const std::exception &e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ C ABI
+
+extern "C" {
+
+const char *orc_last_error() { return g_err.c_str(); }
+
+void *orc_read_file(const char *path) {
+    OGraph *g = nullptr;
+    int rc = guarded([&] {
+        std::ifstream in(path);
+        if (!in.is_open()) throw std::runtime_error(std::string("Cannot read from file ") + path);
+        g = new OGraph(build_graph(parse_causal_fg(in)));
+    });
+    return rc ? nullptr : g;
+}
+
+void *orc_read_string(const char *text) {
+    OGraph *g = nullptr;
+    int rc = guarded([&] {
+        std::istringstream in(text);
+        g = new OGraph(build_graph(parse_causal_fg(in)));
+    });
+    return rc ? nullptr : g;
+}
+
+// Factors given as parallel arrays; body labels in CSR form (body_off has n+1 entries).
+void *orc_from_factors(int64_t n, const int32_t *type, const int64_t *head, const int64_t *body_off,
+                       const int64_t *body, const double *p, const double *q) {
+    OGraph *g = nullptr;
+    int rc = guarded([&] {
+        std::vector<OFactor> facs;
+        facs.reserve((size_t)n);
+        for (int64_t I = 0; I < n; I++) {
+            if (type[I] == 0) {
+                facs.push_back(make_singleton((uint64_t)head[I], p[I]));
+            } else {
+                std::vector<uint64_t> b;
+                for (int64_t k = body_off[I]; k < body_off[I + 1]; k++) b.push_back((uint64_t)body[k]);
+                facs.push_back(make_rule((uint64_t)head[I], b, type[I] == 1, p[I], q[I]));
+            }
+        }
+        g = new OGraph(build_graph(facs));
+    });
+    return rc ? nullptr : g;
+}
+
+void orc_free(void *g) { delete (OGraph *)g; }
+
+int orc_clamp(void *g, int64_t i, int64_t x) {
+    return guarded([&] { clamp_graph(*(OGraph *)g, (size_t)i, (size_t)x); });
+}
+
+void *orc_rebuild(void *g) { return new OGraph(build_graph(((OGraph *)g)->factors)); }
+
+int64_t orc_nr_vars(void *g) { return (int64_t)((OGraph *)g)->vars.size(); }
+int64_t orc_nr_factors(void *g) { return (int64_t)((OGraph *)g)->factors.size(); }
+int64_t orc_nr_edges(void *g) {
+    int64_t s = 0;
+    for (auto &n : ((OGraph *)g)->nbV) s += (int64_t)n.size();
+    return s;
+}
+// Sum of |vars()| over factors (the message length of causal_bp.cu:319-322).
+int64_t orc_nr_slots(void *g) {
+    int64_t s = 0;
+    for (auto &f : ((OGraph *)g)->factors) s += (int64_t)f.vars.size();
+    return s;
+}
+
+void orc_vars(void *g, int64_t *labels) {
+    auto &G = *(OGraph *)g;
+    for (size_t i = 0; i < G.vars.size(); i++) labels[i] = (int64_t)G.vars[i];
+}
+
+void orc_factor_info(void *g, int32_t *type, int64_t *head, double *p, double *q, int32_t *clamped,
+                     double *m0, double *m1, int64_t *nvars) {
+    auto &G = *(OGraph *)g;
+    for (size_t I = 0; I < G.factors.size(); I++) {
+        auto &f = G.factors[I];
+        type[I] = f.type;
+        head[I] = (int64_t)f.head;
+        p[I] = f.p;
+        q[I] = f.q;
+        clamped[I] = f.head_clamped ? 1 : 0;
+        m0[I] = f.mask0;
+        m1[I] = f.mask1;
+        nvars[I] = (int64_t)f.vars.size();
+    }
+}
+
+// Per-factor vars() labels in CSR form (off has F+1 entries).
+void orc_factor_vars(void *g, int64_t *off, int64_t *labels) {
+    auto &G = *(OGraph *)g;
+    int64_t k = 0;
+    off[0] = 0;
+    for (size_t I = 0; I < G.factors.size(); I++) {
+        for (uint64_t l : G.factors[I].vars) labels[k++] = (int64_t)l;
+        off[I + 1] = k;
+    }
+}
+
+// nbV / nbF neighbour lists (node, iter, dual) in CSR form.
+void orc_neighbors(void *g, int which_factor, int64_t *off, int64_t *node, int64_t *iter, int64_t *dual) {
+    auto &G = *(OGraph *)g;
+    auto &nb = which_factor ? G.nbF : G.nbV;
+    int64_t k = 0;
+    off[0] = 0;
+    for (size_t a = 0; a < nb.size(); a++) {
+        for (auto &n : nb[a]) {
+            node[k] = (int64_t)n.node;
+            iter[k] = (int64_t)n.iter;
+            dual[k] = (int64_t)n.dual;
+            k++;
+        }
+        off[a + 1] = k;
+    }
+}
+
+// construct() outputs. Sizes: row_ptr_vf F+1, col_ind_vf E, row_ptr_fv V+1, col_ind_fv E, head F,
+// rec_* E (variable-major), vf_* E (factor-major).
+void orc_construct(void *g, int64_t *row_ptr_vf, int64_t *col_ind_vf, int64_t *row_ptr_fv, int64_t *col_ind_fv,
+                   int64_t *head, int64_t *rec_i, double *rec_r, int64_t *vf_i) {
+    OLayout L = construct(*(OGraph *)g);
+    for (size_t a = 0; a < L.row_ptr_vf.size(); a++) row_ptr_vf[a] = (int64_t)L.row_ptr_vf[a];
+    for (size_t a = 0; a < L.col_ind_vf.size(); a++) col_ind_vf[a] = (int64_t)L.col_ind_vf[a];
+    for (size_t a = 0; a < L.row_ptr_fv.size(); a++) row_ptr_fv[a] = (int64_t)L.row_ptr_fv[a];
+    for (size_t a = 0; a < L.col_ind_fv.size(); a++) col_ind_fv[a] = (int64_t)L.col_ind_fv[a];
+    for (size_t a = 0; a < L.head.size(); a++) head[a] = (int64_t)L.head[a];
+    for (size_t k = 0; k < L.rec.size(); k++) {
+        const ORec &r = L.rec[k];
+        int64_t *o = rec_i + 6 * k;
+        o[0] = (int64_t)r.type;
+        o[1] = (int64_t)r.v;
+        o[2] = (int64_t)r.src;
+        o[3] = (int64_t)r.start;
+        o[4] = (int64_t)r.end;
+        o[5] = (int64_t)r.head;
+        double *d = rec_r + 4 * k;
+        d[0] = r.q;
+        d[1] = r.p;
+        d[2] = r.m0;
+        d[3] = r.m1;
+    }
+    for (size_t k = 0; k < L.vf.size(); k++) {
+        vf_i[3 * k] = (int64_t)L.vf[k].ind;
+        vf_i[3 * k + 1] = (int64_t)L.vf[k].v;
+        vf_i[3 * k + 2] = (int64_t)L.vf[k].src;
+    }
+}
+
+void *orc_bp_create(void *g, double damping, int nthreads, int logdomain) {
+    OBP *b = bp_create(*(OGraph *)g, damping, nthreads);
+    b->logdomain = logdomain != 0;
+    return b;
+}
+void orc_bp_free(void *b) { delete (OBP *)b; }
+int64_t orc_bp_nr_vars(void *b) { return (int64_t)((OBP *)b)->V; }
+int64_t orc_bp_nr_slots(void *b) { return (int64_t)((OBP *)b)->E; }
+int64_t orc_bp_iters(void *b) { return (int64_t)((OBP *)b)->iters; }
+void orc_bp_set_threads(void *b, int n) { ((OBP *)b)->nthreads = n < 1 ? 1 : n; }
+void orc_bp_init(void *b) { bp_init(*(OBP *)b); }
+void orc_bp_sweep(void *b) { bp_sweep(*(OBP *)b); }
+
+double orc_bp_run_tol(void *b, double tol, int64_t maxiter, double maxtime) {
+    double md = 0;
+    bp_run_tol(*(OBP *)b, tol, (size_t)maxiter, maxtime, &md);
+    return md;
+}
+
+double orc_bp_run_fixed(void *b, double tol, int64_t maxIters, int64_t hist) {
+    return bp_run_fixed(*(OBP *)b, tol, (size_t)maxIters, (size_t)hist);
+}
+
+double orc_bp_run_lowpass(void *b, double tol, int64_t minIters, int64_t maxIters, int64_t hist, double maxtime,
+                          int32_t *reason, int64_t *sweeps) {
+    size_t sw = 0;
+    int rs = 0;
+    double r = bp_run_lowpass(*(OBP *)b, tol, (size_t)minIters, (size_t)maxIters, (size_t)hist, maxtime, &rs, &sw);
+    if (reason) *reason = rs;
+    if (sweeps) *sweeps = (int64_t)sw;
+    return r;
+}
+
+// _beliefsV (host copy after a run), _lowPassBeliefs, and the current b1/(b0+b1).
+void orc_bp_beliefs(void *b, double *out) {
+    auto &B = *(OBP *)b;
+    for (size_t i = 0; i < B.V; i++) out[i] = B.beliefs[i];
+}
+int orc_bp_lowpass(void *b, double *out) {
+    auto &B = *(OBP *)b;
+    if (B.lowpass.size() != B.V) return -1;
+    for (size_t i = 0; i < B.V; i++) out[i] = B.lowpass[i];
+    return 0;
+}
+void orc_bp_current_beliefs(void *b, double *out) {
+    std::vector<double> nb;
+    bp_beliefs(*(OBP *)b, nb);
+    for (size_t i = 0; i < nb.size(); i++) out[i] = nb[i];
+}
+
+// Messages: f->v in variable-major order, v->f in factor-major order.
+void orc_bp_messages(void *b, double *fv0, double *fv1, double *vf0, double *vf1) {
+    auto &B = *(OBP *)b;
+    for (size_t k = 0; k < B.E; k++) {
+        fv0[k] = B.fv0[k];
+        fv1[k] = B.fv1[k];
+        vf0[k] = B.vf0[k];
+        vf1[k] = B.vf1[k];
+    }
+}
+
+// Overwrite v->f messages (factor-major); lets tests drive single f->v evaluations.
+void orc_bp_set_vf(void *b, const double *vf0, const double *vf1) {
+    auto &B = *(OBP *)b;
+    for (size_t k = 0; k < B.E; k++) {
+        B.vf0[k] = vf0[k];
+        B.vf1[k] = vf1[k];
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,163 @@
+"""GPU parity of the CUDA engine against the FP64 oracle and exact marginals.
+
+Tolerances: FP64 engine within 1e-9 of the oracle (log-odds vs probability
+arithmetic differ only by rounding); FP32 engine within 1e-5 absolute on
+beliefs, the target of the FP32 log-domain design.
+"""
+
+import numpy as np
+import pytest
+
+import brute
+import oracle as O
+import trees
+from fastlbp_b200 import CausalFactorGraph, Engine, workloads
+
+pytestmark = pytest.mark.gpu
+
+TOL = {64: 1e-9, 32: 1e-5}
+
+
+def _pair(fl, clamps=None):
+    g = CausalFactorGraph.from_factors(fl)
+    og = O.OracleGraph.from_factors(fl)
+    if clamps:
+        g.clamp_labels(clamps)
+        og.clamp_labels(clamps)
+        g, og = g.rebuild(), og.rebuild()
+    return g, og
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+def test_trees_exact_marginals(prec):
+    checked = 0
+    for seed in range(120):
+        fl = trees.random_tree(seed, n_factors=5)
+        labels = sorted(set(fl.head.tolist()) | set(fl.body.tolist()))
+        rng = np.random.default_rng(seed + 7)
+        cl = {int(l): int(rng.integers(0, 2)) for l in labels if rng.random() < 0.2}
+        with np.errstate(all="ignore"):
+            ex = brute.marginals(labels, trees.as_brute_factors(fl, cl))
+        if not np.all(np.isfinite(ex)):
+            continue  # contradictory evidence
+        g, _ = _pair(fl, cl)
+        eng = Engine.from_graph(g, precision=prec)
+        eng.init()
+        eng.run_tol(1e-13 if prec == 64 else 1e-7, 2000, 100.0)
+        b = eng.beliefs()
+        pos = {l: i for i, l in enumerate(labels)}
+        want = np.array([ex[pos[int(l)]] for l in g.var_labels()])
+        assert np.max(np.abs(b - want)) <= (1e-9 if prec == 64 else 2e-5), seed
+        checked += 1
+    assert checked > 80
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+def test_config0_tolerance_run(prec):
+    fl = workloads.config0(0)
+    g, og = _pair(fl)
+    bp = O.OracleBP(og)
+    bp.init()
+    bp.run(1e-6, 1000, 100.0)
+    eng = Engine.from_graph(g, precision=prec)
+    eng.init()
+    info = eng.run_tol(1e-6, 1000, 100.0)
+    assert np.max(np.abs(eng.beliefs() - bp.beliefs())) <= TOL[prec]
+    if prec == 64:
+        assert info["sweeps"] == bp.iters
+    else:
+        assert abs(info["sweeps"] - bp.iters) <= 2
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+def test_config0_clamped_fixed_sweeps(prec):
+    fl = workloads.config0(0)
+    cl = {int(a): int(i % 2) for i, a in enumerate(fl.alarms)}
+    g, og = _pair(fl, cl)
+    bp = O.OracleBP(og)
+    bp.init()
+    bp.run_fixed(1e-6, 500, 1)
+    eng = Engine.from_graph(g, precision=prec)
+    eng.init()
+    info = eng.run_fixed(500)
+    assert info["sweeps"] == 500
+    assert np.max(np.abs(eng.lowpass() - bp.lowpass())) <= TOL[prec]
+    assert np.max(np.abs(eng.beliefs() - bp.beliefs())) <= TOL[prec]
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+def test_damped_sweeps(prec):
+    fl = workloads.config1(seed=5, scale=0.002)
+    g, og = _pair(fl)
+    bp = O.OracleBP(og, damping=0.1)
+    bp.init()
+    bp.run_fixed(1e-6, 200, 1)
+    eng = Engine.from_graph(g, precision=prec, damping=0.1)
+    eng.init()
+    eng.run_fixed(200)
+    assert np.max(np.abs(eng.beliefs() - bp.beliefs())) <= TOL[prec]
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+def test_lowpass_run(prec):
+    fl = workloads.config0(3)
+    cl = {int(a): int(i % 2) for i, a in enumerate(fl.alarms)}
+    g, og = _pair(fl, cl)
+    bp = O.OracleBP(og)
+    bp.init()
+    frac, reason, sweeps = bp.run_lowpass(1e-6, 50, 120, 20)
+    eng = Engine.from_graph(g, precision=prec)
+    eng.init()
+    info = eng.run_lowpass(1e-6, 50, 120, 20)
+    if prec == 64:
+        assert (info["reason"], info["sweeps"]) == (reason, sweeps)
+        assert abs(info["frac"] - frac) <= 1e-12
+    assert np.max(np.abs(eng.lowpass() - bp.lowpass())) <= TOL[prec] * (1 if prec == 64 else 2)
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+def test_messages_each_sweep(prec):
+    fl = workloads.config0(1)
+    cl = {int(a): int(i % 2) for i, a in enumerate(fl.alarms[:8])}
+    g, og = _pair(fl, cl)
+    bp = O.OracleBP(og)
+    bp.init()
+    eng = Engine.from_graph(g, precision=prec)
+    eng.init()
+    for _ in range(6):
+        bp.sweep()
+        eng.sweep(1)
+        fv0, fv1, vf0, vf1 = bp.messages()
+        m0, m1 = eng.fv_messages()
+        assert np.max(np.abs(m1 - fv1 / (fv0 + fv1))) <= (1e-12 if prec == 64 else 2e-6)
+        n0, n1 = eng.vf_messages()
+        assert np.max(np.abs(n1 - vf1 / (vf0 + vf1))) <= (1e-12 if prec == 64 else 2e-6)
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+def test_high_fanin_fault_localisation(prec):
+    fl, cl = workloads.config2(seed=4, scale=0.01)
+    g, og = _pair(fl, cl)
+    eng = Engine.from_graph(g, precision=prec)
+    assert eng.stats()["warp_factors"] > 0
+    bp = O.OracleBP(og)
+    bp.init()
+    bp.run_fixed(1e-6, 100, 1)
+    eng.init()
+    eng.run_fixed(100)
+    assert np.max(np.abs(eng.beliefs() - bp.beliefs())) <= TOL[prec]
+
+
+def test_repeat_runs_continue_iteration_count():
+    fl = workloads.config0(2)
+    g, og = _pair(fl)
+    bp = O.OracleBP(og)
+    bp.init()
+    bp.run_fixed(1e-6, 7, 1)
+    bp.run(1e-6, 1000, 100.0)
+    eng = Engine.from_graph(g, precision=64)
+    eng.init()
+    eng.run_fixed(7)
+    info = eng.run_tol(1e-6, 1000, 100.0)
+    assert info["total_sweeps"] == bp.iters
+    assert np.max(np.abs(eng.beliefs() - bp.beliefs())) <= 1e-9

@@ -1,0 +1,348 @@
+#!/usr/bin/env python
+"""Benchmark of the causal LBP sweep on the 1M-variable Bingo-style graph.
+
+Workload (one "step"): init() + 200 synchronous (PARALL) sweeps with damping
+0.1 in FP32 log-odds messages, then one belief evaluation, on the seeded
+synthetic graph of 1,000,000 tuple variables (+1,500,000 rule variables,
+2.32 M factors, 6.32 M edge slots): 10,000 inputs at 0.99, noisy-AND fan-in
+1+Geom(0.6) clipped at 8, OR fan-in Zipf(2) capped at 256, 5 % back edges,
+p ~ U[0.8, 0.999].
+
+Metric: edge-message updates per second = 2 * E * sweeps / time, E = the
+reference's edge-slot count (sum of |vars(factor)|).
+
+  python bench.py [--gpus N --steps K --warmup W]            this engine
+  python bench.py --impl reference [...]                       FastLBP's own code
+
+`value` is device-resident throughput (graph already in HBM, CUDA events on
+the engine stream, L2 flushed between steps); `e2e` goes through the C ABI
+from host arrays: flbp_engine_create (host layout + H2D) + init + run +
+belief D2H per step. Multi-GPU runs are replicas of the same graph on every
+rank (a single graph does not shard); `value` sums all ranks' updates over
+the slowest rank's time.
+"""
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "edge msg updates/s"
+UNIT = "updates/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--sweeps", type=int, default=200)
+    ap.add_argument("--damping", type=float, default=0.1)
+    ap.add_argument("--precision", type=int, default=32)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--scale", type=float, default=1.0, help="graph size factor (1.0 = the 1M-variable graph)")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    if world > 1 and not dist.is_initialized():
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                                timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allreduce_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def graph_arrays(args):
+    """Reference-order arrays of the workload graph (cached per seed/scale)."""
+    from fastlbp_b200 import CausalFactorGraph, workloads
+
+    cache = os.path.join(tempfile.gettempdir(), "fastlbp_b200_cfg1_s%d_x%g.npz" % (args.seed, args.scale))
+    fl = workloads.config1(args.seed, scale=args.scale)
+    if os.path.exists(cache):
+        z = np.load(cache)
+        return fl, {k: z[k] for k in z.files}
+    g = CausalFactorGraph.from_factors(fl)
+    a = g.graph_arrays()
+    a["n_vars"] = np.int64(a["n_vars"])
+    np.savez(cache, **a)
+    return fl, a
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(tempfile.gettempdir(), "fastlbp_clocks_%d_%d.csv" % (os.getpid(), index))
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per launch from the committed ncu summary (profiles/)."""
+    path = os.path.join(ROOT, "profiles", "traffic_cfg1.txt")
+    out = {}
+    if os.path.exists(path):
+        for line in open(path):
+            if line.startswith("TRAFFIC "):
+                _, name, val = line.split()[:3]
+                out[name] = float(val)
+    return out
+
+
+def cpu_baseline(fl, args):
+    """FP64 oracle (CPU restatement of the reference's PARALL math), OpenMP over
+    all host cores, timed on a bounded number of sweeps of the same graph."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    cores = os.cpu_count() or 1
+    g = O.OracleGraph.from_factors(fl)
+    bp = O.OracleBP(g, damping=args.damping, threads=cores)
+    bp.init()
+    E = bp.E
+    t0 = time.perf_counter()
+    bp.sweep()
+    one = time.perf_counter() - t0
+    n = max(1, int(args.cpu_seconds / max(one, 1e-3)))
+    t0 = time.perf_counter()
+    for _ in range(n):
+        bp.sweep()
+    dt = time.perf_counter() - t0
+    return {"value": 2.0 * E * n / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "%d FP64 sweeps of the same graph (damping %g) by the oracle's OpenMP loop, %.1f s" % (n, args.damping, dt)}
+
+
+def run_ours(args, rank, world, local):
+    import torch
+
+    from fastlbp_b200 import Engine
+
+    fl, arr = graph_arrays(args)
+    E = int(arr["factor_offsets"][-1])
+    F = int(arr["factor_offsets"].size - 1)
+    V = int(arr["n_vars"])
+    stream = torch.cuda.current_stream()
+    eng = Engine(arr, precision=args.precision, damping=args.damping, stream=stream.cuda_stream)
+    st = eng.stats()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    for _ in range(args.warmup):
+        eng.init()
+        eng.run_fixed(args.sweeps)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = Clocks(local)
+    clocks.start()
+    times, launches = [], 0
+    for _ in range(args.steps):
+        flush.zero_()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        eng.init()
+        info = eng.run_fixed(args.sweeps)
+        e.record(stream)
+        times.append((s, e))
+        launches += info["launches"]
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    total_ms = sum(s.elapsed_time(e) for s, e in times)
+    total_ms = allreduce_max(total_ms, world)
+    updates = 2.0 * E * args.sweeps * args.steps * world
+    value = updates / (total_ms / 1e3)
+
+    # Per-pass durations: the same steps again with CUDA events around each pass.
+    eng.set_kernel_timing(True)
+    for _ in range(args.steps):
+        flush.zero_()
+        eng.init()
+        eng.run_fixed(args.sweeps)
+    torch.cuda.synchronize()
+    f_ms, v_ms, f_n, v_n = eng.kernel_times()
+    eng.set_kernel_timing(False)
+    per = {"factor_pass": f_ms / max(f_n, 1), "var_pass": v_ms / max(v_n, 1)}
+    # Algorithmic bytes per launch (per-unit figures x units): factor pass
+    # 12 B per edge slot + 16 B per factor; variable pass 12 B per slot + 12 B per variable.
+    alg = {"factor_pass": 12.0 * E + 16.0 * F, "var_pass": 12.0 * E + 12.0 * V}
+    dom = max(per, key=per.get)
+    peak, peak_kind = peaks()
+    achieved = alg[dom] / (per[dom] / 1e3) / 1e9
+    traffic = ncu_traffic().get(dom)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                "traffic": traffic, "alg_bytes_per_launch": alg[dom],
+                "launch_ms": {k: round(v, 5) for k, v in per.items()}}
+
+    # End to end through the C ABI with host arrays.
+    e2e_ms, h2d = [], 0
+    out = np.zeros(V)
+    for i in range(args.e2e_steps + 1):
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        t0 = time.perf_counter()
+        eng2 = Engine(arr, precision=args.precision, damping=args.damping, stream=stream.cuda_stream)
+        eng2.init()
+        eng2.run_fixed(args.sweeps)
+        out = eng2.beliefs()
+        e.record(stream)
+        torch.cuda.synchronize()
+        wall = (time.perf_counter() - t0) * 1e3
+        h2d = eng2.stats()["h2d_bytes"]
+        eng2.close()
+        if i > 0:  # the first call pays one-time kernel configuration
+            e2e_ms.append(max(s.elapsed_time(e), wall))
+    e2e_val = 2.0 * E * args.sweeps * world / (allreduce_max(statistics.mean(e2e_ms), world) / 1e3)
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == 32 else "f64",
+            "data": "synthetic (seeded Bingo-style generator)",
+            "config": {"workload": "1M-tuple Bingo-style graph, 200 PARALL sweeps, damping 0.1, FP32 log-odds",
+                       "vars": V, "factors": F, "edge_slots": E, "sweeps": args.sweeps, "damping": args.damping,
+                       "seed": args.seed, "scale": args.scale, "replicas": world,
+                       "l2": "256 MB buffer written between timed steps; working set > L2"},
+            "roofline": roofline, "clocks": clk, "gpu_launches": launches,
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": V * 8,
+                    "ms_per_step": statistics.mean(e2e_ms)}}
+    if rank == 0 and world == 1:
+        line["cpu_baseline"] = cpu_baseline(fl, args)
+    eng.close()
+    return line
+
+
+def run_reference(args, rank, world):
+    """FastLBP's own code (oracle/_ref/ref_bp, compiled from its sources) on the
+    same graph. The reference path exists only as GPU code; it has no damping,
+    so it runs the same sweep count undamped."""
+    if rank != 0:
+        return None
+    fl, arr = graph_arrays(args)
+    E = int(arr["factor_offsets"][-1])
+    ref_bp = os.path.join(ROOT, "oracle", "_ref", "ref_bp")
+    base = {"metric": METRIC, "unit": UNIT, "impl": "reference", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "data": "synthetic (seeded Bingo-style generator)",
+            "config": {"workload": "1M-tuple Bingo-style graph, 200 PARALL sweeps, FP64 (reference has no damping)",
+                       "edge_slots": E, "sweeps": args.sweeps, "seed": args.seed, "scale": args.scale}}
+    import torch
+    if not (os.path.exists(ref_bp) and torch.cuda.is_available()):
+        return dict(base, unavailable="oracle/_ref/ref_bp not built on this machine")
+    path = os.path.join(tempfile.gettempdir(), "fastlbp_ref_cfg1_s%d_x%g.causal_fg" % (args.seed, args.scale))
+    if not os.path.exists(path):
+        fl.write(path)
+    rep = args.warmup + args.steps
+    r = subprocess.run([ref_bp, path, "-", "-", "fixed", str(args.sweeps), "repeat", str(rep)],
+                       capture_output=True, text=True, timeout=3000)
+    if r.returncode != 0:
+        return dict(base, unavailable="reference run failed: " + (r.stderr or r.stdout)[-200:])
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    runs = d["run_event_all_s"][args.warmup:]
+    cons = d["construct_all_s"][args.warmup:]
+    value = 2.0 * E * args.sweeps / statistics.mean(runs)
+    line = dict(base, value=value, ms_per_step=statistics.mean(runs) * 1e3, dtype="f64",
+                reference_construct_s=statistics.mean(cons), reference_read_s=d["read_s"])
+    line["cpu_baseline"] = {"value": value, "unit": UNIT, "kind": "reference", "cores": 1,
+                            "sample": "FastLBP CausalBP (updates=PARALL) built from its sources, run(tol, %d, 1) "
+                                      "on the B200 from one host thread; its path has no CPU implementation" % args.sweeps}
+    line["e2e"] = {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    line["gpu_launches"] = None
+    return line
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_setup(args)
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+    else:
+        line = run_ours(args, rank, world, local)
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

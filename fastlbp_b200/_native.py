@@ -78,6 +78,8 @@ def lib():
         "flbp_get_vf_messages": [_vp, _f64p, _f64p, C.c_int64],
         "flbp_engine_stats": [_vp, _i64p, C.c_int64],
         "flbp_last_run_ms": [_vp, P(C.c_double)],
+        "flbp_set_kernel_timing": [_vp, C.c_int32],
+        "flbp_kernel_times": [_vp, _f64p, _i64p],
         "flbp_fg_read_file": [C.c_char_p, P(_vp)],
         "flbp_fg_read_string": [C.c_char_p, P(_vp)],
         "flbp_fg_from_factors": [C.c_int64, _i32p, _i64p, _i64p, _i64p, _f64p, _f64p, P(_vp)],
@@ -111,7 +113,7 @@ def last_error() -> str:
 EXPORTED = ["flbp_last_error", "flbp_version", "flbp_engine_create", "flbp_engine_destroy", "flbp_init",
             "flbp_run_tol", "flbp_run_fixed", "flbp_run_lowpass", "flbp_sweep", "flbp_get_beliefs",
             "flbp_get_lowpass", "flbp_compute_beliefs", "flbp_get_fv_messages", "flbp_get_vf_messages",
-            "flbp_engine_stats", "flbp_last_run_ms", "flbp_fg_read_file", "flbp_fg_read_string",
+            "flbp_engine_stats", "flbp_last_run_ms", "flbp_set_kernel_timing", "flbp_kernel_times", "flbp_fg_read_file", "flbp_fg_read_string",
             "flbp_fg_from_factors", "flbp_fg_destroy", "flbp_fg_clamp", "flbp_fg_rebuild", "flbp_fg_sizes",
             "flbp_fg_var_labels", "flbp_fg_factors", "flbp_fg_neighbors", "flbp_fg_construct",
             "flbp_engine_create_from_fg"]

@@ -266,10 +266,20 @@ class Engine:
         return m0, m1
 
     def stats(self) -> Dict[str, int]:
-        c = np.zeros(8, np.int64)
+        c = np.zeros(10, np.int64)
         check(lib().flbp_engine_stats(self._h, c, c.size))
-        keys = ["vars", "factors", "slots", "active_factors", "active_slots", "warp_factors", "warp_vars", "bytes"]
+        keys = ["vars", "factors", "slots", "active_factors", "active_slots", "warp_factors", "warp_vars", "bytes",
+                "h2d_bytes", "launches"]
         return dict(zip(keys, (int(x) for x in c)))
+
+    def set_kernel_timing(self, enable: bool) -> None:
+        check(lib().flbp_set_kernel_timing(self._h, 1 if enable else 0))
+
+    def kernel_times(self):
+        """(factor-pass ms, variable-pass ms, factor launches, variable launches) in timing mode."""
+        ms, n = np.zeros(2), np.zeros(2, np.int64)
+        check(lib().flbp_kernel_times(self._h, ms, n))
+        return float(ms[0]), float(ms[1]), int(n[0]), int(n[1])
 
     def last_run_ms(self) -> float:
         v = C.c_double()

@@ -67,6 +67,15 @@ struct flbp_engine {
     long long launches = 0;
     bool lowpass_valid = false;
     size_t bytes = 0;
+    size_t h2d_bytes = 0;  // host->device bytes copied by create
+
+    // Per-kernel timing mode: sweeps are launched without graphs, with events
+    // around each pass; collect_kernel_times() folds them into kt_ms / kt_n.
+    bool ktime = false;
+    std::vector<cudaEvent_t> kev;
+    size_t kev_used = 0;
+    double kt_ms[2] = {0.0, 0.0};
+    long long kt_n[2] = {0, 0};
 };
 
 namespace {
@@ -145,20 +154,24 @@ cudaError_t configure_kernels(int *fb, int *vb) {
 }
 
 // mode 0: bare sweep; 1: tolerance loop sweep; 2: low-pass loop sweep.
+// which: bit 0 launches the factor pass, bit 1 the variable pass.
 template <typename T>
-void launch_sweep(flbp_engine *e, int mode) {
+void launch_sweep(flbp_engine *e, int mode, int which = 3) {
     const T d = (T)e->damping;
     const T *vf_c = (const T *)e->d_vf;
     T *vf = (T *)e->d_vf;
     T *fv = (T *)e->d_fv;
     const FactorArgs fa = factor_args<T>(e);
     const VarArgs va = var_args(e);
+    if (which & 1) {
     if (e->damping != 0.0)
         factor_pass_kernel<T, true, kStages>
             <<<e->factor_grid, kBlockThreads, factor_smem<T, true>(), e->stream>>>(fa, vf_c, fv, d, e->d_ctl);
     else
         factor_pass_kernel<T, false, kStages>
             <<<e->factor_grid, kBlockThreads, factor_smem<T, false>(), e->stream>>>(fa, vf_c, fv, d, e->d_ctl);
+    }
+    if (!(which & 2)) return;
     if (mode == 0)
         var_pass_kernel<T, 0, true, kStages><<<e->var_grid, kBlockThreads, var_smem<T>(), e->stream>>>(va, fv, vf, e->d_ctl);
     else if (mode == 1)
@@ -167,9 +180,9 @@ void launch_sweep(flbp_engine *e, int mode) {
         var_pass_kernel<T, 2, true, kStages><<<e->var_grid, kBlockThreads, var_smem<T>(), e->stream>>>(va, fv, vf, e->d_ctl);
 }
 
-void launch_sweep_any(flbp_engine *e, int mode) {
-    if (e->prec == 64) launch_sweep<double>(e, mode);
-    else launch_sweep<float>(e, mode);
+void launch_sweep_any(flbp_engine *e, int mode, int which = 3) {
+    if (e->prec == 64) launch_sweep<double>(e, mode, which);
+    else launch_sweep<float>(e, mode, which);
 }
 
 void launch_beliefs_only(flbp_engine *e, double *dst) {
@@ -211,6 +224,24 @@ int sweep_graph(flbp_engine *e, int mode, int n, cudaGraphExec_t *out) {
 // Launch n sweeps as power-of-two graph chunks.
 int launch_sweeps(flbp_engine *e, int mode, long long n) {
     if (e->L.nf_sell + e->L.nf_big == 0 && e->L.V == 0) return FLBP_OK;
+    if (e->ktime) {  // no graphs: events around each pass
+        for (long long i = 0; i < n; i++) {
+            while (e->kev.size() < e->kev_used + 3) {
+                cudaEvent_t ev;
+                FLBP_CUDA(cudaEventCreate(&ev));
+                e->kev.push_back(ev);
+            }
+            cudaEvent_t *ev = &e->kev[e->kev_used];
+            e->kev_used += 3;
+            FLBP_CUDA(cudaEventRecord(ev[0], e->stream));
+            launch_sweep_any(e, mode, 1);
+            FLBP_CUDA(cudaEventRecord(ev[1], e->stream));
+            launch_sweep_any(e, mode, 2);
+            FLBP_CUDA(cudaEventRecord(ev[2], e->stream));
+            e->launches += 2;
+        }
+        return FLBP_OK;
+    }
     while (n > 0) {
         int k = 1;
         while ((long long)k * 2 <= n && k < 64) k *= 2;
@@ -265,6 +296,7 @@ template <typename X>
 int upload(flbp_engine *e, X *dst, const std::vector<X> &src) {
     if (src.empty()) return FLBP_OK;
     FLBP_CUDA(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(X), cudaMemcpyHostToDevice, e->stream));
+    e->h2d_bytes += src.size() * sizeof(X);
     return FLBP_OK;
 }
 
@@ -287,6 +319,17 @@ int record_stop(flbp_engine *e) {
     FLBP_CUDA(cudaEventSynchronize(e->ev1));
     FLBP_CUDA(cudaEventElapsedTime(&e->last_ms, e->ev0, e->ev1));
     FLBP_CUDA(cudaGetLastError());
+    // fold per-pass event pairs of the timing mode
+    for (size_t k = 0; k + 3 <= e->kev_used; k += 3) {
+        float a = 0.f, b = 0.f;
+        FLBP_CUDA(cudaEventElapsedTime(&a, e->kev[k], e->kev[k + 1]));
+        FLBP_CUDA(cudaEventElapsedTime(&b, e->kev[k + 1], e->kev[k + 2]));
+        e->kt_ms[0] += a;
+        e->kt_ms[1] += b;
+        e->kt_n[0]++;
+        e->kt_n[1]++;
+    }
+    e->kev_used = 0;
     return FLBP_OK;
 }
 
@@ -513,6 +556,7 @@ int flbp_engine_destroy(flbp_engine *e) {
     cudaSetDevice(e->device);
     if (e->stream) cudaStreamSynchronize(e->stream);
     for (auto &kv : e->graphs) cudaGraphExecDestroy(kv.second);
+    for (auto ev : e->kev) cudaEventDestroy(ev);
     void *bufs[] = {e->d_vf,     e->d_fv,       e->d_f_pq,   e->d_fg_base,   e->d_fb_off,     e->d_f_kind,
                     e->d_f_deg,  e->d_vg_base,  e->d_vb_off, e->d_v_ent,     e->d_prior,      e->d_belief,
                     e->d_lowpass, e->d_hist,    e->d_hist_next, e->d_hist_count, e->d_ctl,    e->d_scratch,
@@ -802,10 +846,33 @@ int flbp_engine_stats(flbp_engine *e, int64_t *c, int64_t n) {
         set_error("null argument");
         return FLBP_ERR_INVALID;
     }
-    const int64_t v[8] = {e->L.V, e->L.F, e->L.E, (int64_t)(e->L.nf_sell + e->L.nf_big),
-                          (int64_t)e->L.n_active_slots, (int64_t)e->L.nf_big, (int64_t)e->L.nv_big,
-                          (int64_t)e->bytes};
-    for (int64_t i = 0; i < n && i < 8; i++) c[i] = v[i];
+    const int64_t v[10] = {e->L.V, e->L.F, e->L.E, (int64_t)(e->L.nf_sell + e->L.nf_big),
+                           (int64_t)e->L.n_active_slots, (int64_t)e->L.nf_big, (int64_t)e->L.nv_big,
+                           (int64_t)e->bytes, (int64_t)e->h2d_bytes, (int64_t)e->launches};
+    for (int64_t i = 0; i < n && i < 10; i++) c[i] = v[i];
+    return FLBP_OK;
+}
+
+int flbp_set_kernel_timing(flbp_engine *e, int32_t enable) {
+    if (!e) {
+        set_error("null engine handle");
+        return FLBP_ERR_INVALID;
+    }
+    e->ktime = enable != 0;
+    e->kt_ms[0] = e->kt_ms[1] = 0.0;
+    e->kt_n[0] = e->kt_n[1] = 0;
+    return FLBP_OK;
+}
+
+int flbp_kernel_times(flbp_engine *e, double *ms, int64_t *counts) {
+    if (!e || !ms || !counts) {
+        set_error("null argument");
+        return FLBP_ERR_INVALID;
+    }
+    for (int i = 0; i < 2; i++) {
+        ms[i] = e->kt_ms[i];
+        counts[i] = e->kt_n[i];
+    }
     return FLBP_OK;
 }
 

@@ -139,10 +139,20 @@ int flbp_get_fv_messages(flbp_engine *eng, double *m0, double *m1, int64_t n_slo
  * variable's message all the same). */
 int flbp_get_vf_messages(flbp_engine *eng, double *m0, double *m1, int64_t n_slots);
 
-/* Layout statistics: counts[0..7] = vars, factors, slots, active factors,
+/* Layout statistics: counts[0..9] = vars, factors, slots, active factors,
  * active slots, factors handled warp-wide, variables handled warp-wide,
- * bytes of device memory held. */
+ * bytes of device memory held, host->device bytes copied by create, engine
+ * kernels launched so far. */
 int flbp_engine_stats(flbp_engine *eng, int64_t *counts, int64_t n_counts);
+
+/* Per-pass timing mode (for measurement): while enabled, sweeps are launched
+ * one kernel at a time with CUDA events around the factor and variable
+ * passes instead of as CUDA graphs. Enabling resets the accumulators. */
+int flbp_set_kernel_timing(flbp_engine *eng, int32_t enable);
+
+/* Accumulated device time (ms) and launch counts of the factor pass [0] and
+ * the variable pass [1] recorded in timing mode. */
+int flbp_kernel_times(flbp_engine *eng, double *ms, int64_t *counts);
 
 /* Device duration in milliseconds of the engine's GPU work recorded by the
  * last run call (CUDA events on the engine stream). */

@@ -84,6 +84,7 @@ int main(int argc, char **argv) {
     opts.set("logdomain", false);
 
     double best_construct = 1e30, best_run = 1e30, best_run_ev = 1e30;
+    std::vector<double> all_construct, all_run_ev;
     double ret = 0;
     std::unique_ptr<CausalBP> bp;
     cudaEvent_t e0, e1;
@@ -109,7 +110,16 @@ int main(int argc, char **argv) {
         best_construct = std::min(best_construct, c1 - c0);
         best_run = std::min(best_run, c2 - c1);
         best_run_ev = std::min(best_run_ev, (double)ms / 1e3);
+        all_construct.push_back(c1 - c0);
+        all_run_ev.push_back((double)ms / 1e3);
     }
+    std::string runs = "[", cons = "[";
+    for (size_t r = 0; r < all_run_ev.size(); r++) {
+        runs += (r ? ", " : "") + std::to_string(all_run_ev[r]);
+        cons += (r ? ", " : "") + std::to_string(all_construct[r]);
+    }
+    runs += "]";
+    cons += "]";
     cudaError_t err = cudaGetLastError();
 
     if (outf != "-") {
@@ -123,8 +133,9 @@ int main(int argc, char **argv) {
     size_t E = 0;
     for (size_t I = 0; I < nfg.nrFactors(); I++) E += nfg.factor(I).vars().size();
     printf("{\"vars\": %zu, \"factors\": %zu, \"slots\": %zu, \"read_s\": %.6f, \"construct_s\": %.6f, "
-           "\"run_s\": %.6f, \"run_event_s\": %.6f, \"ret\": %.17g, \"repeat\": %d, \"cuda\": \"%s\"}\n",
+           "\"run_s\": %.6f, \"run_event_s\": %.6f, \"ret\": %.17g, \"repeat\": %d, \"cuda\": \"%s\", "
+           "\"run_event_all_s\": %s, \"construct_all_s\": %s}\n",
            nfg.nrVars(), nfg.nrFactors(), E, t_read, best_construct, best_run, best_run_ev, ret, repeat,
-           cudaGetErrorString(err));
+           cudaGetErrorString(err), runs.c_str(), cons.c_str());
     return err == cudaSuccess ? 0 : 1;
 }

@@ -35,6 +35,17 @@ class EngineOpts(C.Structure):
     _fields_ = [("precision", C.c_int32), ("device", C.c_int32), ("damping", C.c_double), ("stream", _vp)]
 
 
+class DeviceGraph(C.Structure):
+    """flbp_device_graph: a graph in device memory for the allocation-free solve."""
+    _fields_ = [("n_vars", C.c_int32), ("n_factors", C.c_int32), ("n_slots", C.c_int32),
+                ("factor_offsets", _vp), ("slot_var", _vp), ("factor_head", _vp), ("factor_type", _vp),
+                ("factor_head_state", _vp), ("factor_p", _vp), ("factor_q", _vp), ("var_offsets", _vp),
+                ("var_slots", _vp)]
+
+
+NOALLOC_MAX_SLOTS = 1 << 19
+
+
 class RunInfo(C.Structure):
     _fields_ = [("sweeps", C.c_int64), ("total_sweeps", C.c_int64), ("maxdiff", C.c_double), ("frac", C.c_double),
                 ("reason", C.c_int32), ("status", C.c_int32), ("launches", C.c_int64)]
@@ -92,6 +103,7 @@ def lib():
         "flbp_fg_neighbors": [_vp, C.c_int32, _i64p, _i64p, _i64p, _i64p],
         "flbp_fg_construct": [_vp, _i64p, _i64p, _i64p, _i64p, _i64p],
         "flbp_engine_create_from_fg": [_vp, P(EngineOpts), P(_vp)],
+        "flbp_run_fixed_device_noalloc": [P(DeviceGraph), C.c_int64, C.c_double, _vp, _vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -116,4 +128,4 @@ EXPORTED = ["flbp_last_error", "flbp_version", "flbp_engine_create", "flbp_engin
             "flbp_engine_stats", "flbp_last_run_ms", "flbp_set_kernel_timing", "flbp_kernel_times", "flbp_fg_read_file", "flbp_fg_read_string",
             "flbp_fg_from_factors", "flbp_fg_destroy", "flbp_fg_clamp", "flbp_fg_rebuild", "flbp_fg_sizes",
             "flbp_fg_var_labels", "flbp_fg_factors", "flbp_fg_neighbors", "flbp_fg_construct",
-            "flbp_engine_create_from_fg"]
+            "flbp_engine_create_from_fg", "flbp_run_fixed_device_noalloc"]

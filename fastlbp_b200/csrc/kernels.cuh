@@ -705,7 +705,7 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long x) {
 
 // Stop rules evaluated after a sweep by the last block of the variable pass,
 // so that the next launches see ctl->done.
-__device__ void stop_rules(Ctl *ctl) {
+static __device__ void stop_rules(Ctl *ctl) {
     const double maxdiff = __longlong_as_double((long long)ctl->maxdiff_bits);
     ctl->maxdiff = maxdiff;
     unsigned long long now;
@@ -872,7 +872,7 @@ __global__ void __launch_bounds__(288) var_pass_kernel(VarArgs a, const T *__res
 
 // Low-pass belief mean, oldest to newest, then one division
 // (HostBeliefHistory::mean, causal_bp.cu:65-77).
-__global__ void lowpass_kernel(const double *hist, const uint32_t *hist_next, const uint32_t *hist_count,
+static __global__ void lowpass_kernel(const double *hist, const uint32_t *hist_next, const uint32_t *hist_count,
                                uint32_t hist_len, uint32_t n, double *out) {
     const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n) return;

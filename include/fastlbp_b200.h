@@ -154,6 +154,53 @@ int flbp_set_kernel_timing(flbp_engine *eng, int32_t enable);
  * the variable pass [1] recorded in timing mode. */
 int flbp_kernel_times(flbp_engine *eng, double *ms, int64_t *counts);
 
+/* ------------------------------------------------------------------------
+ * Allocation-free solve. No counterpart in FastLBP.
+ *
+ * For callers that may not allocate GPU memory when they solve: code running
+ * under CUDA stream capture (cudaMalloc cannot be recorded and synchronises
+ * the device), serving loops whose policy forbids allocation after start-up,
+ * and processes whose GPU memory belongs to another allocator. The caller
+ * passes the graph and the belief output as device arrays it owns; the two
+ * message arrays live in a fixed scratch array inside the library (2 x
+ * FLBP_NOALLOC_MAX_SLOTS floats = 4 MiB, held by every GPU that loads the
+ * library until the process exits). Nothing is allocated or freed.
+ *
+ * - Graphs with more than FLBP_NOALLOC_MAX_SLOTS edge slots are rejected
+ *   with FLBP_ERR_LIMIT.
+ * - The first call on a device looks up the scratch address on that device
+ *   (cudaGetSymbolAddress, with the device current); make that first call
+ *   before any stream capture.
+ * - All calls share the one scratch array and it keeps the last call's
+ *   messages; each call resets them to uniform first. Calls whose GPU work
+ *   overlaps (different streams or host threads without ordering) race on
+ *   the scratch and give wrong results: order them.
+ * - Work is launched on `stream` (NULL: the legacy default stream); the
+ *   call returns without waiting for it.
+ * ---------------------------------------------------------------------- */
+#define FLBP_NOALLOC_MAX_SLOTS (1 << 19)
+
+/* A graph in device memory, in the reference's orders (the arrays of
+ * CausalBP::construct()), 32-bit. */
+typedef struct flbp_device_graph {
+    int32_t n_vars, n_factors, n_slots;
+    const int32_t *factor_offsets;     /* n_factors + 1: factor-major slot offsets (row_ptr_vf) */
+    const int32_t *slot_var;           /* n_slots: variable of each slot (col_ind_vf) */
+    const int32_t *factor_head;        /* n_factors: absolute slot of each factor's head */
+    const int32_t *factor_type;        /* n_factors: FLBP_SINGLETON / FLBP_AND / FLBP_OR */
+    const uint8_t *factor_head_state;  /* n_factors or NULL: 0 free, 1 head clamped to 1, 2 to 0, 3 mask (0,0) */
+    const float *factor_p;             /* n_factors: prob() */
+    const float *factor_q;             /* n_factors: prob_default() */
+    const int32_t *var_offsets;        /* n_vars + 1: variable-major offsets (row_ptr_fv) */
+    const int32_t *var_slots;          /* n_slots: factor-major slot of each variable-major entry */
+} flbp_device_graph;
+
+/* `sweeps` synchronous sweeps from uniform messages with f->v damping
+ * `damping`, then beliefs P(x=1) into beliefs_out (n_vars doubles, device).
+ * FP32 log-odds messages, the same arithmetic as the engine. */
+int flbp_run_fixed_device_noalloc(const flbp_device_graph *graph, int64_t sweeps, double damping,
+                                  double *beliefs_out, void *stream);
+
 /* Device duration in milliseconds of the engine's GPU work recorded by the
  * last run call (CUDA events on the engine stream). */
 int flbp_last_run_ms(flbp_engine *eng, double *ms);

@@ -44,9 +44,14 @@ struct flbp_engine {
     HostLayout L;
     size_t tsize = 4;
 
-    void *d_vf = nullptr, *d_fv = nullptr, *d_f_pq = nullptr;
+    void *d_vf = nullptr;   // per slot
+    void *d_fv = nullptr;   // per variable entry
+    void *d_fvd = nullptr;  // per variable entry: damped f->v messages (damping only)
+    void *d_f_pq = nullptr;
+    uint32_t *d_f_pos = nullptr;  // per slot: entry of its f->v message
+    size_t n_ent = 0;
     uint32_t *d_fg_base = nullptr, *d_fb_off = nullptr, *d_vg_base = nullptr, *d_vb_off = nullptr, *d_v_ent = nullptr;
-    uint32_t *d_ftiles = nullptr, *d_vtiles = nullptr;  // 16-word headers per tile
+    uint32_t *d_ftiles = nullptr, *d_vtiles = nullptr;  // kHdrWords-word headers per tile
     uint32_t f_tile_blocks = 0, v_tile_blocks = 0;
     uint8_t *d_f_kind = nullptr, *d_f_deg = nullptr;
     void *d_prior = nullptr;
@@ -85,6 +90,7 @@ FactorArgs factor_args(flbp_engine *e) {
     FactorArgs a;
     a.fg_base = e->d_fg_base;
     a.fb_off = e->d_fb_off;
+    a.f_pos = e->d_f_pos;
     a.f_kind = e->d_f_kind;
     a.f_deg = e->d_f_deg;
     a.f_pq = e->d_f_pq;
@@ -117,67 +123,77 @@ VarArgs var_args(flbp_engine *e) {
     return a;
 }
 
-constexpr int kStages = 3;          // bulk-copy pipeline depth of both passes
-constexpr int kBlockThreads = 288;  // 8 consumer warps + 1 producer warp
-
-template <typename T, bool DAMP>
-constexpr size_t factor_smem() {
-    return (size_t)kStages * FactorStage<T, DAMP>::bytes;
-}
+constexpr int kStages = 3;                        // bulk-copy pipeline depth of both passes
+constexpr int kBlockThreads = kBlockThreadsDev;  // 16 consumer warps + 1 producer warp
 
 template <typename T>
-constexpr size_t var_smem() {
-    return (size_t)kStages * VarStage<T>::bytes;
+constexpr size_t factor_smem() {
+    return (size_t)kStages * FactorStage<T>::bytes;
 }
+
+template <typename T, bool DAMP>
+constexpr size_t var_smem() {
+    return (size_t)kStages * VarStage<T, DAMP>::bytes;
+}
+static_assert(factor_smem<double>() <= 227 * 1024, "factor-pass stages exceed shared memory");
+static_assert(var_smem<double, true>() <= 227 * 1024, "variable-pass stages exceed shared memory");
+static_assert(kTileGroupsHost == (uint32_t)kTileGroups && kTileSlotsHost == (uint32_t)kTileSlots,
+              "host tiling must match the kernels' stage sizes");
 
 // Opt every kernel instantiation of precision T into its dynamic shared
 // memory size; returns the resident blocks per SM of the factor and
 // variable passes.
 template <typename T>
-cudaError_t configure_kernels(int *fb, int *vb) {
+cudaError_t configure_kernels(bool damp, int *fb, int *vb) {
     cudaError_t err = cudaSuccess;
     auto set = [&](const void *fn, size_t bytes) {
         cudaError_t e2 = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         if (e2 != cudaSuccess) err = e2;
     };
-    set((const void *)factor_pass_kernel<T, true, kStages>, factor_smem<T, true>());
-    set((const void *)factor_pass_kernel<T, false, kStages>, factor_smem<T, false>());
-    set((const void *)var_pass_kernel<T, 0, true, kStages>, var_smem<T>());
-    set((const void *)var_pass_kernel<T, 1, true, kStages>, var_smem<T>());
-    set((const void *)var_pass_kernel<T, 2, true, kStages>, var_smem<T>());
-    set((const void *)var_pass_kernel<T, 3, false, kStages>, var_smem<T>());
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(fb, factor_pass_kernel<T, true, kStages>, kBlockThreads,
-                                                  factor_smem<T, true>());
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(vb, var_pass_kernel<T, 2, true, kStages>, kBlockThreads,
-                                                  var_smem<T>());
+    set((const void *)factor_pass_kernel<T, kStages>, factor_smem<T>());
+    set((const void *)var_pass_kernel<T, 0, true, false, kStages>, var_smem<T, false>());
+    set((const void *)var_pass_kernel<T, 1, true, false, kStages>, var_smem<T, false>());
+    set((const void *)var_pass_kernel<T, 2, true, false, kStages>, var_smem<T, false>());
+    set((const void *)var_pass_kernel<T, 0, true, true, kStages>, var_smem<T, true>());
+    set((const void *)var_pass_kernel<T, 1, true, true, kStages>, var_smem<T, true>());
+    set((const void *)var_pass_kernel<T, 2, true, true, kStages>, var_smem<T, true>());
+    set((const void *)var_pass_kernel<T, 3, false, false, kStages>, var_smem<T, false>());
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(fb, factor_pass_kernel<T, kStages>, kBlockThreads, factor_smem<T>());
+    if (damp)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(vb, var_pass_kernel<T, 2, true, true, kStages>, kBlockThreads,
+                                                      var_smem<T, true>());
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(vb, var_pass_kernel<T, 2, true, false, kStages>, kBlockThreads,
+                                                      var_smem<T, false>());
     return err;
+}
+
+template <typename T, int BMODE, bool DAMP>
+void launch_var(flbp_engine *e, const VarArgs &va) {
+    var_pass_kernel<T, BMODE, true, DAMP, kStages><<<e->var_grid, kBlockThreads, var_smem<T, DAMP>(), e->stream>>>(
+        va, (const T *)e->d_fv, (T *)e->d_vf, (T *)e->d_fvd, (T)e->damping, e->d_ctl);
+}
+
+template <typename T, bool DAMP>
+void launch_var_mode(flbp_engine *e, const VarArgs &va, int mode) {
+    if (mode == 0) launch_var<T, 0, DAMP>(e, va);
+    else if (mode == 1) launch_var<T, 1, DAMP>(e, va);
+    else launch_var<T, 2, DAMP>(e, va);
 }
 
 // mode 0: bare sweep; 1: tolerance loop sweep; 2: low-pass loop sweep.
 // which: bit 0 launches the factor pass, bit 1 the variable pass.
 template <typename T>
 void launch_sweep(flbp_engine *e, int mode, int which = 3) {
-    const T d = (T)e->damping;
-    const T *vf_c = (const T *)e->d_vf;
-    T *vf = (T *)e->d_vf;
-    T *fv = (T *)e->d_fv;
-    const FactorArgs fa = factor_args<T>(e);
-    const VarArgs va = var_args(e);
     if (which & 1) {
-    if (e->damping != 0.0)
-        factor_pass_kernel<T, true, kStages>
-            <<<e->factor_grid, kBlockThreads, factor_smem<T, true>(), e->stream>>>(fa, vf_c, fv, d, e->d_ctl);
-    else
-        factor_pass_kernel<T, false, kStages>
-            <<<e->factor_grid, kBlockThreads, factor_smem<T, false>(), e->stream>>>(fa, vf_c, fv, d, e->d_ctl);
+        const FactorArgs fa = factor_args<T>(e);
+        factor_pass_kernel<T, kStages><<<e->factor_grid, kBlockThreads, factor_smem<T>(), e->stream>>>(
+            fa, (const T *)e->d_vf, (T *)e->d_fv, e->d_ctl);
     }
     if (!(which & 2)) return;
-    if (mode == 0)
-        var_pass_kernel<T, 0, true, kStages><<<e->var_grid, kBlockThreads, var_smem<T>(), e->stream>>>(va, fv, vf, e->d_ctl);
-    else if (mode == 1)
-        var_pass_kernel<T, 1, true, kStages><<<e->var_grid, kBlockThreads, var_smem<T>(), e->stream>>>(va, fv, vf, e->d_ctl);
-    else
-        var_pass_kernel<T, 2, true, kStages><<<e->var_grid, kBlockThreads, var_smem<T>(), e->stream>>>(va, fv, vf, e->d_ctl);
+    const VarArgs va = var_args(e);
+    if (e->damping != 0.0) launch_var_mode<T, true>(e, va, mode);
+    else launch_var_mode<T, false>(e, va, mode);
 }
 
 void launch_sweep_any(flbp_engine *e, int mode, int which = 3) {
@@ -185,15 +201,20 @@ void launch_sweep_any(flbp_engine *e, int mode, int which = 3) {
     else launch_sweep<float>(e, mode, which);
 }
 
-void launch_beliefs_only(flbp_engine *e, double *dst) {
+// Beliefs of the current messages (the damped ones under damping), without
+// touching the run state.
+template <typename T>
+void launch_beliefs_only_t(flbp_engine *e, double *dst) {
     VarArgs a = var_args(e);
     a.belief = dst;
-    if (e->prec == 64)
-        var_pass_kernel<double, 3, false, kStages><<<e->var_grid, kBlockThreads, var_smem<double>(), e->stream>>>(
-            a, (const double *)e->d_fv, (double *)e->d_vf, e->d_ctl);
-    else
-        var_pass_kernel<float, 3, false, kStages><<<e->var_grid, kBlockThreads, var_smem<float>(), e->stream>>>(
-            a, (const float *)e->d_fv, (float *)e->d_vf, e->d_ctl);
+    const T *src = (const T *)(e->damping != 0.0 ? e->d_fvd : e->d_fv);
+    var_pass_kernel<T, 3, false, false, kStages><<<e->var_grid, kBlockThreads, var_smem<T, false>(), e->stream>>>(
+        a, src, (T *)e->d_vf, nullptr, (T)0, e->d_ctl);
+}
+
+void launch_beliefs_only(flbp_engine *e, double *dst) {
+    if (e->prec == 64) launch_beliefs_only_t<double>(e, dst);
+    else launch_beliefs_only_t<float>(e, dst);
     e->launches += 1;
 }
 
@@ -442,7 +463,9 @@ int flbp_engine_create(const flbp_graph_desc *graph, const flbp_engine_opts *opt
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
     // One full wave of resident blocks; the kernels stride over tiles and large items.
     int fb = 1, vb = 1;
-    cudaError_t cfg = (e->prec == 64) ? configure_kernels<double>(&fb, &vb) : configure_kernels<float>(&fb, &vb);
+    const bool damp = e->damping != 0.0;
+    cudaError_t cfg =
+        (e->prec == 64) ? configure_kernels<double>(damp, &fb, &vb) : configure_kernels<float>(damp, &fb, &vb);
     if (cfg != cudaSuccess) {
         set_error(std::string("kernel configuration failed: ") + cudaGetErrorString(cfg));
         return fail(FLBP_ERR_CUDA);
@@ -457,14 +480,15 @@ int flbp_engine_create(const flbp_graph_desc *graph, const flbp_engine_opts *opt
                      uint32_t &tile_blocks) -> int {
         const uint64_t total = (uint64_t)sms * (uint64_t)per_sm;
         if (!dedicated) {  // every block takes large items first, then tiles
-            const uint64_t g = std::max<uint64_t>(1, std::min<uint64_t>(total, std::max<uint64_t>(n_tiles, (n_big + 7) / 8)));
+            const uint64_t g = std::max<uint64_t>(
+                1, std::min<uint64_t>(total, std::max<uint64_t>(n_tiles, (n_big + kConsumerWarps - 1) / kConsumerWarps)));
             tile_blocks = (uint32_t)g;
             return (int)g;
         }
         uint64_t bigb = 0;
         if (n_big) {
             bigb = (total * big_work + (tile_work + big_work) - 1) / std::max<uint64_t>(1, tile_work + big_work);
-            bigb = std::max<uint64_t>(1, std::min<uint64_t>(bigb, (n_big + 8) / 9));
+            bigb = std::max<uint64_t>(1, std::min<uint64_t>(bigb, (n_big + kConsumerWarps) / (kConsumerWarps + 1)));
             if (n_tiles) bigb = std::min<uint64_t>(bigb, total > 1 ? total - 1 : 1);
         }
         tile_blocks = (uint32_t)std::min<uint64_t>(n_tiles, std::max<uint64_t>(1, total - bigb));
@@ -481,13 +505,16 @@ int flbp_engine_create(const flbp_graph_desc *graph, const flbp_engine_opts *opt
     const size_t nf_pad = std::max<size_t>(nf, 32ull * L.n_fgroups());
     const size_t nv_pad = std::max<size_t>((size_t)L.V, 32ull * L.n_vgroups());
     const size_t psz = e->prec == 64 ? 16 : 8;
-    if ((rc = dalloc(e, (char **)&e->d_vf, ns * e->tsize)) || (rc = dalloc(e, (char **)&e->d_fv, ns * e->tsize)) ||
+    e->n_ent = std::max<size_t>(1, L.v_ent.size());
+    const size_t ne = e->n_ent;
+    if ((rc = dalloc(e, (char **)&e->d_vf, ns * e->tsize)) || (rc = dalloc(e, (char **)&e->d_fv, ne * e->tsize)) ||
+        (damp && (rc = dalloc(e, (char **)&e->d_fvd, ne * e->tsize))) || (rc = dalloc(e, &e->d_f_pos, ns)) ||
         (rc = dalloc(e, (char **)&e->d_f_pq, 2 * nf_pad * e->tsize)) ||
         (rc = dalloc(e, &e->d_fg_base, L.fg_base.size())) || (rc = dalloc(e, &e->d_fb_off, L.fb_off.size())) ||
         (rc = dalloc(e, &e->d_f_kind, nf_pad)) || (rc = dalloc(e, &e->d_f_deg, nf_pad)) ||
         (rc = dalloc(e, &e->d_vg_base, L.vg_base.size())) || (rc = dalloc(e, &e->d_vb_off, L.vb_off.size())) ||
-        (rc = dalloc(e, &e->d_v_ent, L.v_ent.size())) || (rc = dalloc(e, &e->d_ftiles, 16ull * n_ft)) ||
-        (rc = dalloc(e, &e->d_vtiles, 16ull * n_vt)) ||
+        (rc = dalloc(e, &e->d_v_ent, L.v_ent.size())) || (rc = dalloc(e, &e->d_ftiles, (size_t)kHdrWords * n_ft)) ||
+        (rc = dalloc(e, &e->d_vtiles, (size_t)kHdrWords * n_vt)) ||
         (rc = dalloc(e, (char **)&e->d_prior, std::max<size_t>(1, nv_pad) * psz)) ||
         (rc = dalloc(e, &e->d_belief, nv_pad)) || (rc = dalloc(e, &e->d_lowpass, (size_t)L.V)) ||
         (rc = dalloc(e, &e->d_ctl, 1)))
@@ -508,14 +535,14 @@ int flbp_engine_create(const flbp_graph_desc *graph, const flbp_engine_opts *opt
             prior[2 * i + 1] = L.prior_cnt[i];
         }
     }
-    // 16-word tile headers: first group, group count, group offsets (end repeated).
+    // Tile headers (kHdrWords words): first group, group count, group offsets (end repeated).
     auto headers = [](const std::vector<uint32_t> &tiles, const std::vector<uint32_t> &base) {
         std::vector<uint32_t> h;
         for (size_t t = 0; t + 1 < tiles.size(); t++) {
             const uint32_t g0 = tiles[t], n = tiles[t + 1] - g0;
             h.push_back(g0);
             h.push_back(n);
-            for (uint32_t j = 0; j < 14; j++) h.push_back(base[g0 + std::min(j, n)]);
+            for (uint32_t j = 0; j + 2 < (uint32_t)kHdrWords; j++) h.push_back(base[g0 + std::min(j, n)]);
         }
         return h;
     };
@@ -533,6 +560,7 @@ int flbp_engine_create(const flbp_graph_desc *graph, const flbp_engine_opts *opt
         if ((rc = upload(e, (float *)e->d_f_pq, pq32))) return fail(rc);
     }
     if ((rc = upload(e, e->d_fg_base, L.fg_base)) || (rc = upload(e, e->d_fb_off, L.fb_off)) ||
+        (rc = upload(e, e->d_f_pos, L.f_pos)) ||
         (rc = upload(e, e->d_f_kind, kind_pad)) || (rc = upload(e, e->d_f_deg, deg_pad)) ||
         (rc = upload(e, e->d_vg_base, L.vg_base)) || (rc = upload(e, e->d_vb_off, L.vb_off)) ||
         (rc = upload(e, e->d_v_ent, L.v_ent)) || (rc = upload(e, (uint32_t *)e->d_prior, prior)) ||
@@ -542,7 +570,8 @@ int flbp_engine_create(const flbp_graph_desc *graph, const flbp_engine_opts *opt
     if ((ce = cudaStreamSynchronize(e->stream)) != cudaSuccess ||
         (ce = cudaMemsetAsync(e->d_belief, 0, std::max<size_t>(1, nv_pad) * sizeof(double), e->stream)) != cudaSuccess ||
         (ce = cudaMemsetAsync(e->d_vf, 0, ns * e->tsize, e->stream)) != cudaSuccess ||
-        (ce = cudaMemsetAsync(e->d_fv, 0, ns * e->tsize, e->stream)) != cudaSuccess ||
+        (ce = cudaMemsetAsync(e->d_fv, 0, ne * e->tsize, e->stream)) != cudaSuccess ||
+        (damp && (ce = cudaMemsetAsync(e->d_fvd, 0, ne * e->tsize, e->stream)) != cudaSuccess) ||
         (ce = cudaStreamSynchronize(e->stream)) != cudaSuccess) {
         set_error(std::string("device initialisation failed: ") + cudaGetErrorString(ce));
         return fail(FLBP_ERR_CUDA);
@@ -557,7 +586,7 @@ int flbp_engine_destroy(flbp_engine *e) {
     if (e->stream) cudaStreamSynchronize(e->stream);
     for (auto &kv : e->graphs) cudaGraphExecDestroy(kv.second);
     for (auto ev : e->kev) cudaEventDestroy(ev);
-    void *bufs[] = {e->d_vf,     e->d_fv,       e->d_f_pq,   e->d_fg_base,   e->d_fb_off,     e->d_f_kind,
+    void *bufs[] = {e->d_vf,     e->d_fv,       e->d_fvd,    e->d_f_pos,     e->d_f_pq,   e->d_fg_base,   e->d_fb_off,     e->d_f_kind,
                     e->d_f_deg,  e->d_vg_base,  e->d_vb_off, e->d_v_ent,     e->d_prior,      e->d_belief,
                     e->d_lowpass, e->d_hist,    e->d_hist_next, e->d_hist_count, e->d_ctl,    e->d_scratch,
                     e->d_ftiles, e->d_vtiles};
@@ -576,7 +605,8 @@ int flbp_init(flbp_engine *e) {
     if (rc) return rc;
     const size_t ns = std::max<size_t>(1, e->L.n_slots);
     FLBP_CUDA(cudaMemsetAsync(e->d_vf, 0, ns * e->tsize, e->stream));
-    FLBP_CUDA(cudaMemsetAsync(e->d_fv, 0, ns * e->tsize, e->stream));
+    FLBP_CUDA(cudaMemsetAsync(e->d_fv, 0, e->n_ent * e->tsize, e->stream));
+    if (e->d_fvd) FLBP_CUDA(cudaMemsetAsync(e->d_fvd, 0, e->n_ent * e->tsize, e->stream));
     e->t = 0;
     e->lowpass_valid = false;
     return FLBP_OK;
@@ -749,18 +779,22 @@ int flbp_compute_beliefs(flbp_engine *e, double *out, int64_t n) {
     return fetch_internal(e, e->d_scratch, out, n);
 }
 
+// f->v messages in the reference's variable-major slot order: from the
+// entry array in use (the damped one under damping) for computed messages,
+// the folded constants otherwise.
 static int fv_lambda(flbp_engine *e, std::vector<double> &lam) {
     const HostLayout &L = e->L;
-    const size_t ns = L.n_slots;
-    std::vector<double> act(ns);
-    if (ns) {
+    const size_t ne = L.v_ent.size();
+    const void *src = e->d_fvd ? e->d_fvd : e->d_fv;
+    std::vector<double> ent(ne);
+    if (ne) {
         if (e->prec == 64) {
-            FLBP_CUDA(cudaMemcpyAsync(act.data(), e->d_fv, ns * 8, cudaMemcpyDeviceToHost, e->stream));
+            FLBP_CUDA(cudaMemcpyAsync(ent.data(), src, ne * 8, cudaMemcpyDeviceToHost, e->stream));
         } else {
-            std::vector<float> f(ns);
-            FLBP_CUDA(cudaMemcpyAsync(f.data(), e->d_fv, ns * 4, cudaMemcpyDeviceToHost, e->stream));
+            std::vector<float> f(ne);
+            FLBP_CUDA(cudaMemcpyAsync(f.data(), src, ne * 4, cudaMemcpyDeviceToHost, e->stream));
             FLBP_CUDA(cudaStreamSynchronize(e->stream));
-            for (size_t i = 0; i < ns; i++) act[i] = f[i];
+            for (size_t i = 0; i < ne; i++) ent[i] = f[i];
         }
         FLBP_CUDA(cudaStreamSynchronize(e->stream));
     }
@@ -768,7 +802,7 @@ static int fv_lambda(flbp_engine *e, std::vector<double> &lam) {
     lam.assign((size_t)L.E, 0.0);
     for (int64_t k = 0; k < L.E; k++) {
         const int64_t s = L.ref_fv_src[k];
-        if (s >= 0) lam[k] = act[s];
+        if (s >= 0) lam[k] = (L.f_pos[s] != kSentinel) ? ent[L.f_pos[s]] : 0.0;
         else if (s == -2) lam[k] = INFINITY;
         else if (s == -3) lam[k] = -INFINITY;
         else lam[k] = L.ref_const[k] * scale;

@@ -21,11 +21,12 @@ enum : uint8_t {
 };
 
 // Items up to these degrees go to the sliced-ELL (one item per lane) paths,
-// larger ones to the warp-per-item paths.
-constexpr uint32_t kSellFactorDegree = 16;
+// larger ones to the warp-per-item paths. A sliced-ELL factor keeps all of
+// its slots in registers, which bounds its degree tighter.
+constexpr uint32_t kSellFactorDegree = 8;
 constexpr uint32_t kSellVarDegree = 16;
 constexpr uint32_t kSentinel = 0xffffffffu;  // padding entry in the variable layout
-constexpr uint32_t kTileGroupsHost = 8;      // groups per tile (= warps per block of the passes)
+constexpr uint32_t kTileGroupsHost = 16;     // groups per tile (items = threads of a pass's consumers)
 constexpr uint32_t kTileSlotsHost = 2048;    // slot budget of a tile (shared-memory stage size)
 
 // Host-built device layout.
@@ -46,6 +47,11 @@ constexpr uint32_t kTileSlotsHost = 2048;    // slot budget of a tile (shared-me
 // v_ent[vg_base[g] + 32*k + lane], the factor-side slot whose message
 // reaches the variable (kSentinel for padding). Variables of larger degree
 // follow with contiguous entry runs (vb_off).
+//
+// Messages: vf (variable -> factor) is indexed by factor-side slot, fv
+// (factor -> variable) by variable entry; f_pos maps each slot to the entry
+// that receives its f->v message, v_ent each entry back to its slot, so that
+// both passes read contiguously and scatter their outputs.
 struct HostLayout {
     int64_t V = 0, F = 0, E = 0;  // reference sizes
 
@@ -61,6 +67,7 @@ struct HostLayout {
     std::vector<uint32_t> vg_base;     // n_vgroups + 1 (entry ids)
     std::vector<uint32_t> vb_off;      // nv_big + 1 (entry ids)
     std::vector<uint32_t> v_ent;       // entries incl. padding
+    std::vector<uint32_t> f_pos;       // per slot: entry of its f->v message (kSentinel: none)
     std::vector<double> prior_fin;     // per internal variable: finite constant log-odds (damping-scaled)
     std::vector<uint32_t> prior_cnt;   // per internal variable: (#+inf) | (#-inf << 16)
     std::vector<uint32_t> var_of_internal;  // internal variable -> reference variable
@@ -68,7 +75,7 @@ struct HostLayout {
     uint64_t n_active_slots = 0;       // real (non-padding) slots of active factors
 
     // Reference variable-major slot (row_ptr_fv order) -> source of its f->v message:
-    // >= 0 device slot; -1 constant finite (value in ref_const, damping-scaled);
+    // >= 0 device slot (its value lives at entry f_pos[slot]); -1 constant finite (value in ref_const, damping-scaled);
     // -2 constant +inf; -3 constant -inf.
     std::vector<int64_t> ref_fv_src;
     std::vector<double> ref_const;

@@ -1,12 +1,17 @@
 // sm_100a kernels of one synchronous (PARALL) causal-BP sweep.
 //
-// Messages are log-odds lambda = log(m1/m0), one value per device slot, in
-// two arrays: vf (variable -> factor) and fv (factor -> variable). A sweep is
+// Messages are log-odds lambda = log(m1/m0) in two arrays: vf (variable ->
+// factor) in factor-slot order and fv (factor -> variable) in variable-entry
+// order, so that each pass reads its inputs as contiguous streams and
+// scatters its outputs into the other pass's order (stores only; no pass
+// waits on a gather). A sweep is
 //   factor pass:   fv <- f(vf) for every active factor, all its outputs;
 //   variable pass: per variable the sum of its incoming fv plus its constant
 //                  prior, then vf <- total - own message, beliefs, residual.
 // This is the reference's FV -> Prod -> VF sequence
-// (csrc/ext/causal_bp.cu:409-444) restated in log-odds.
+// (csrc/ext/causal_bp.cu:409-444) restated in log-odds. With damping the
+// variable pass mixes each new f->v message with the previous damped one
+// (array fvd, variable-entry order) before using it.
 //
 // Exact zeros of the reference's probability arithmetic become +-inf
 // log-odds. On the factor side zeros flow through sums of log-sigmoids as
@@ -65,6 +70,8 @@ struct Num<float> {
     static __device__ __forceinline__ float log(float x) { return __logf(x); }
     static __device__ __forceinline__ float log1p(float x) { return ::log1pf(x); }
     static __device__ __forceinline__ float expm1(float x) { return ::expm1f(x); }
+    static __device__ __forceinline__ float rcp(float x) { return __fdividef(1.0f, x); }  // x in [1, 2] here
+    static __device__ __forceinline__ float tiny() { return 1.17549435e-38f; }           // smallest normal
 };
 
 template <>
@@ -75,6 +82,8 @@ struct Num<double> {
     static __device__ __forceinline__ double log(double x) { return ::log(x); }
     static __device__ __forceinline__ double log1p(double x) { return ::log1p(x); }
     static __device__ __forceinline__ double expm1(double x) { return ::expm1(x); }
+    static __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
+    static __device__ __forceinline__ double tiny() { return 2.2250738585072014e-308; }  // smallest normal
 };
 
 template <typename T>
@@ -167,33 +176,28 @@ __device__ __forceinline__ T damp_mix(T nw, T old, T d) {
 struct FactorArgs {
     const uint32_t *fg_base;  // sliced-ELL groups (n_fgroups + 1)
     const uint32_t *fb_off;   // big factors (nf_big + 1)
+    const uint32_t *f_pos;    // per device slot: fv position of its output (kSentinel: none)
     const uint8_t *f_kind;
     const uint8_t *f_deg;
     const void *f_pq;         // T[2 * nf]
-    const uint4 *thdr;        // 64-byte header per tile (see TileHdr)
+    const uint4 *thdr;        // kHdrWords-word header per tile (see TileHdr)
     uint32_t nf_sell, nf_big, n_fgroups, n_tiles, n_tile_blocks;
 };
 
 struct VarArgs {
     const uint32_t *vg_base;  // sliced-ELL groups (n_vgroups + 1)
     const uint32_t *vb_off;   // big variables (nv_big + 1)
-    const uint32_t *v_ent;
+    const uint32_t *v_ent;    // per entry: device slot of the factor side (kSentinel: padding)
     const void *prior;        // per variable: FP32 engines uint2 (float bits of the finite prior,
                               // +inf | -inf << 16 counts); FP64 engines uint4 (double bits, counts, 0)
     double *belief;           // per internal variable, previous / current belief
     double *hist;             // low-pass history [hist_len][n_vars], or null
     uint32_t *hist_next;      // per variable ring cursor
     uint32_t *hist_count;     // per variable number of stored samples
-    const uint4 *thdr;        // 64-byte header per tile (see TileHdr)
+    const uint4 *thdr;        // kHdrWords-word header per tile (see TileHdr)
     uint32_t nv_sell, nv_big, n_vgroups, n_tiles, n_tile_blocks;
     uint32_t hist_len;
 };
-
-template <typename T, bool DAMP>
-__device__ __forceinline__ void store_fv(T *fv, uint32_t s, T val, T d) {
-    if (DAMP) val = damp_mix(val, fv[s], d);
-    fv[s] = val;
-}
 
 template <typename T>
 __device__ __forceinline__ T head_effective(uint8_t kind, T vf_head) {
@@ -207,18 +211,26 @@ __device__ __forceinline__ T head_effective(uint8_t kind, T vf_head) {
 
 // ------------------------------------------------------------------ TMA staging
 //
-// Both passes run persistent blocks of 8 warps over "tiles" of 8 sliced-ELL
-// groups (256 items). The contiguous per-tile streams (messages of the
-// tile's slots, indices, per-item constants) are brought into shared memory
-// by one thread with 1-D bulk copies (cp.async.bulk, completion tracked by an
-// mbarrier per pipeline stage); the factor pass writes its outputs back with
-// a bulk store. All waits are bounded: on a timeout the block records
-// FLBP_ERR_TIMEOUT in ctl->status, drains its copies and returns.
+// Both passes run persistent blocks of kConsumerWarps consumer warps plus one
+// producer warp over "tiles" of up to kTileGroups sliced-ELL groups and
+// kTileSlots slots (entries). The producer brings each tile's contiguous
+// streams (messages, scatter indices, per-item constants) into a
+// STAGES-deep shared-memory ring with 1-D bulk copies (cp.async.bulk,
+// completion tracked by one mbarrier per stage, no multicast). Each consumer
+// warp takes one group of the staged tile (lane = item), scatters its
+// outputs to global memory and releases the stage; warps never wait for one
+// another. All waits are bounded: on a timeout the block records
+// FLBP_ERR_TIMEOUT in ctl->status, lets its own copies land and returns.
 
-constexpr int kTileGroups = 8;                            // groups per tile = warps per block
-constexpr int kTileItems = 32 * kTileGroups;              // factors / variables per tile
-constexpr int kTileSlots = 2048;                          // slot (entry) budget of a tile
-constexpr long long kWaitCycles = 4000000000ll;           // ~2 s at 2 GHz
+constexpr int kConsumerWarps = 16;
+constexpr int kConsumers = 32 * kConsumerWarps;    // consumer threads per block
+constexpr int kBlockThreadsDev = kConsumers + 32;  // + one producer warp
+constexpr int kTileGroups = 16;                    // groups per tile = consumer warps
+constexpr int kTileItems = 32 * kTileGroups;       // factors / variables per tile
+constexpr int kTileSlots = 2048;                   // slot (entry) budget of a tile
+constexpr int kHdrWords = 32;                      // tile header: 128 bytes
+static_assert(kTileGroups == kConsumerWarps, "one consumer warp per group of a tile");
+constexpr long long kWaitCycles = 4000000000ll;    // ~2 s at 2 GHz
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -229,6 +241,10 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                  : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
@@ -259,103 +275,207 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
                  : "memory");
 }
 
-__device__ __forceinline__ void bulk_s2g(void *dst, const void *src, uint32_t bytes) {
-    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
-                 "r"(bytes)
-                 : "memory");
+__device__ __forceinline__ void record_timeout(Ctl *ctl) { atomicExch(&ctl->status, FLBP_ERR_TIMEOUT); }
+
+
+// Waits for a stage on every lane of a warp; true on all lanes, or false on
+// all lanes when any of them gave up.
+__device__ __forceinline__ bool warp_wait_stage(uint64_t *bar, uint32_t parity) {
+    return __all_sync(0xffffffffu, mbar_wait_bounded(bar, parity));
 }
 
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-__device__ __forceinline__ size_t align128(size_t x) { return (x + 127) & ~(size_t)127; }
+// Per-tile header (kHdrWords words, host-built): [0] first group, [1] number
+// of groups n (1..kTileGroups), [2 + j] slot (entry) offset of group j for
+// j = 0..n, the remaining words repeating the end offset. The producer loads
+// the next tile's header into registers while the current tile's copies are
+// in flight, so that header latency stays off the pipeline's critical path.
+struct TileHdr {
+    uint4 w[kHdrWords / 4];
+    __device__ __forceinline__ void load(const uint4 *src) {
+#pragma unroll
+        for (int i = 0; i < kHdrWords / 4; i++) w[i] = __ldcg(src + i);
+    }
+    __device__ __forceinline__ void store(uint32_t *dst) const {
+        uint4 *d = reinterpret_cast<uint4 *>(dst);
+#pragma unroll
+        for (int i = 0; i < kHdrWords / 4; i++) d[i] = w[i];
+    }
+};
 
 // Shared-memory layout of one factor-pass stage.
-template <typename T, bool DAMP>
+template <typename T>
 struct FactorStage {
-    static constexpr size_t hdr = 0;                                     // uint32 gbase[kTileGroups + 1]
-    static constexpr size_t vbuf = 128;                                  // T[kTileSlots]: vf in, fv out
-    static constexpr size_t obuf = vbuf + sizeof(T) * kTileSlots;        // T[kTileSlots]: previous fv (DAMP)
-    static constexpr size_t deg = obuf + (DAMP ? sizeof(T) * kTileSlots : 0);  // uint8[kTileItems]
-    static constexpr size_t kind = deg + kTileItems;                     // uint8[kTileItems]
-    static constexpr size_t pq = kind + kTileItems;                      // T[2 * kTileItems]
+    static constexpr size_t hdr = 0;                                   // uint32[kHdrWords]
+    static constexpr size_t vbuf = 128;                                // T[kTileSlots]: incoming vf
+    static constexpr size_t pos = vbuf + sizeof(T) * kTileSlots;       // uint32[kTileSlots]: fv position per slot
+    static constexpr size_t deg = pos + 4 * kTileSlots;                // uint8[kTileItems]
+    static constexpr size_t kind = deg + kTileItems;                   // uint8[kTileItems]
+    static constexpr size_t pq = kind + kTileItems;                    // T[2 * kTileItems]
     static constexpr size_t bytes = (pq + 2 * sizeof(T) * kTileItems + 127) & ~(size_t)127;
 };
 
-template <typename T>
+// Shared-memory layout of one variable-pass stage.
+template <typename T, bool DAMP>
 struct VarStage {
-    static constexpr size_t hdr = 0;                                     // uint32 gbase[kTileGroups + 1]
-    static constexpr size_t ent = 128;                                   // uint32[kTileSlots]
-    static constexpr size_t prior = ent + 4 * kTileSlots;                // uint2 / uint4 [kTileItems]
+    static constexpr size_t hdr = 0;                                             // uint32[kHdrWords]
+    static constexpr size_t ent = 128;                                           // uint32[kTileSlots]
+    static constexpr size_t x = ent + 4 * kTileSlots;                            // T[kTileSlots]: incoming fv
+    static constexpr size_t xo = x + sizeof(T) * kTileSlots;                     // T[kTileSlots]: previous damped fv
+    static constexpr size_t prior = xo + (DAMP ? sizeof(T) * kTileSlots : 0);   // uint2 / uint4 [kTileItems]
     static constexpr size_t bold = prior + (sizeof(T) == 4 ? 8 : 16) * kTileItems;  // double[kTileItems]
     static constexpr size_t bytes = bold + 8 * kTileItems;
 };
 
-// One sliced-ELL group of 32 factors of width W, staged in shared memory:
-// lane = factor, slot k of the factor at vb[32 k + lane]. Per factor: the
-// log-sigmoids of the body, suffix sums, then one pass with a running prefix
-// sum; slot k's output uses the sum over all other body slots (prefix +
-// suffix, never a subtraction). Outputs replace the inputs in vb.
-template <typename T, bool DAMP, int W>
-__device__ __forceinline__ void factor_group_w(T *vb, const T *ob, const uint8_t *dg, const uint8_t *kd, const T *pq,
-                                               int lane, T d) {
-    const int deg = dg[lane];
-    const uint8_t kind = kd[lane];
-    const T p = pq[2 * lane], q = pq[2 * lane + 1];
-    const T s = (kind & KIND_OR) ? T(-1) : T(1);
-    T x[W];
-    const T vh = vb[lane];
-#pragma unroll
-    for (int k = 1; k < W; k++) x[k] = (k < deg) ? log_sigmoid<T>(s * vb[32 * k + lane]) : T(0);
-    const bool free_head = (kind & HEAD_MASK) == HEAD_FREE;
-    const T lh = s * head_effective<T>(kind, vh);
-    T suf[W + 1];
-    suf[W] = T(0);
-#pragma unroll
-    for (int k = W - 1; k >= 1; k--) suf[k] = suf[k + 1] + x[k];
-    if (deg > 0 && free_head) {
-        T o = s * head_out<T>(suf[1], p, q, Num<T>::log(p));
-        if (DAMP) o = damp_mix(o, ob[lane], d);
-        vb[lane] = o;
-    }
-    const BodyDen<T> D = body_den<T>(lh, p, q);
-    T pre = T(0);
+// sigma(x) and 1 - sigma(x) without cancellation, from e = exp(-|x|):
+// +inf -> (1, 0), -inf -> (0, 1), NaN -> (NaN, NaN).
+template <typename T>
+__device__ __forceinline__ void sig_pair(T x, T &sg, T &tau) {
+    const T e = Num<T>::exp(-fabs(x));
+    const T inv = Num<T>::rcp(T(1) + e);
+    const bool pos = x >= T(0);
+    sg = pos ? inv : e * inv;
+    tau = pos ? e * inv : inv;
+}
+
+// AND -> body output from the leave-one-out pair (Po, Ro = 1 - Po) and the
+// factor's denominator (see body_out).
+template <typename T>
+__device__ __forceinline__ T body_out_pr(T Po, T Ro, T p, T q, const BodyDen<T> &D) {
+    if (D.lden == -Num<T>::inf()) return D.zero_out;
+    const T a = p * Po + q * Ro, b = (T(1) - p) * Po + (T(1) - q) * Ro;
+    T lnum;
+    if (D.lh >= T(0)) lnum = (a == T(0)) ? Num<T>::log(b) - D.lh : Num<T>::log(fma(D.r, b, a));
+    else lnum = (b == T(0)) ? D.lh + Num<T>::log(a) : Num<T>::log(fma(D.r, a, b));
+    return lnum - D.lden;
+}
+
+template <typename T>
+__device__ __forceinline__ void put_fv(T *__restrict__ fv, uint32_t e, T o) {
+    if (e != kSentinel) fv[e] = o;
+}
+
+// One factor of a sliced-ELL group of width W, one lane, all in registers:
+// slot k of the factor at vb[32 k + lane] (head at k = 0), the fv position
+// of its output at ps[32 k + lane]. With sigma_k, tau_k = 1 - sigma_k of the
+// body messages (AND orientation), pairs combine as
+//   (P1, R1) o (P2, R2) = (P1 P2, R1 + P1 R2),
+// a product and its complement: every term is non-negative, so P and 1 - P
+// both keep full relative precision and exact zeros stay exact. Suffix pairs
+// (backwards) then prefix pairs (forwards) give each body slot the pair of
+// all other body slots without a division.
+//   head:  m1 ~ p P + q R,  m0 ~ (1-p) P + (1-q) R   over the whole body
+//   body:  body_out_pr over the other body slots (causal_bp_parall.cu:113-151,
+//          289-314, 341-366 in log-odds; OR = AND on negated log-odds).
+template <typename T, int W>
+__device__ __forceinline__ void factor_reg(const T *vb, const uint32_t *ps, int deg, uint8_t kind, T p, T q, int lane,
+                                           T *__restrict__ fv) {
+    const T sgn = (kind & KIND_OR) ? T(-1) : T(1);
+    T sg[W], ta[W];
 #pragma unroll
     for (int k = 1; k < W; k++) {
         if (k < deg) {
-            T o = s * body_out<T>(pre + suf[k + 1], p, q, D);
-            if (DAMP) o = damp_mix(o, ob[32 * k + lane], d);
-            vb[32 * k + lane] = o;
+            sig_pair<T>(sgn * vb[32 * k + lane], sg[k], ta[k]);
+        } else {  // padding slot: the identity pair
+            sg[k] = T(1);
+            ta[k] = T(0);
         }
-        pre += x[k];
+    }
+    T sP[W], sR[W];
+    T P = T(1), R = T(0);
+#pragma unroll
+    for (int k = W - 1; k >= 1; k--) {
+        sP[k] = P;
+        sR[k] = R;
+        R = fma(sg[k], R, ta[k]);
+        P = sg[k] * P;
+    }
+    const T lh = sgn * head_effective<T>(kind, vb[lane]);
+    if ((kind & HEAD_MASK) == HEAD_FREE) {
+        T la;
+        if (q == T(0) && P < Num<T>::tiny()) {  // p P in log space when P is not a normal number
+            T lP = T(0);
+#pragma unroll
+            for (int k = 1; k < W; k++)
+                if (k < deg) lP += log_sigmoid<T>(sgn * vb[32 * k + lane]);
+            la = Num<T>::log(p) + lP;
+        } else {
+            la = Num<T>::log(fma(p, P, q * R));
+        }
+        put_fv<T>(fv, ps[lane], sgn * (la - Num<T>::log(fma(T(1) - p, P, (T(1) - q) * R))));
+    }
+    const BodyDen<T> D = body_den<T>(lh, p, q);
+    T Pp = T(1), Rp = T(0);
+#pragma unroll
+    for (int k = 1; k < W; k++) {
+        if (k < deg) put_fv<T>(fv, ps[32 * k + lane], sgn * body_out_pr<T>(Pp * sP[k], fma(Pp, sR[k], Rp), p, q, D));
+        Rp = fma(Pp, ta[k], Rp);
+        Pp = Pp * sg[k];
     }
 }
 
-template <typename T, bool DAMP>
-__device__ __forceinline__ void factor_group(int w, T *vb, const T *ob, const uint8_t *dg, const uint8_t *kd,
-                                             const T *pq, int lane, T d) {
+template <typename T>
+__device__ __forceinline__ void factor_group(int w, const T *vb, const uint32_t *ps, int deg, uint8_t kind, T p, T q,
+                                             int lane, T *__restrict__ fv) {
     switch (w) {
 #define FLBP_W(N) \
-    case N: factor_group_w<T, DAMP, N>(vb, ob, dg, kd, pq, lane, d); break;
-        FLBP_W(2) FLBP_W(3) FLBP_W(4) FLBP_W(5) FLBP_W(6) FLBP_W(7) FLBP_W(8) FLBP_W(9) FLBP_W(10) FLBP_W(11)
-        FLBP_W(12) FLBP_W(13) FLBP_W(14) FLBP_W(15) FLBP_W(16)
+    case N: factor_reg<T, N>(vb, ps, deg, kind, p, q, lane, fv); break;
+        FLBP_W(2) FLBP_W(3) FLBP_W(4) FLBP_W(5) FLBP_W(6) FLBP_W(7) FLBP_W(8)
 #undef FLBP_W
         default: break;
     }
 }
+static_assert(kSellFactorDegree == 8, "factor_group instantiates widths 2..8");
 
-// One large factor, one warp: lanes stride over the body; the body sum is a
-// double with a count of -inf terms so that each slot can remove its own term.
-template <typename T, bool DAMP>
-__device__ void factor_warp(const FactorArgs &a, uint32_t b, int lane, const T *__restrict__ vf, T *__restrict__ fv,
-                            T d) {
-    const uint32_t fi = a.nf_sell + b;
-    const uint32_t s0 = a.fb_off[b], s1 = a.fb_off[b + 1];
-    const uint8_t kind = a.f_kind[fi];
-    const T *pq = reinterpret_cast<const T *>(a.f_pq);
-    const T p = pq[2 * fi], q = pq[2 * fi + 1];
+// One large factor, one warp, with at most 32 NV body slots held in
+// registers: every lane issues all of its loads at once, so the warp waits
+// for memory once per factor. The body sum is a double with a count of -inf
+// terms so that each slot can remove its own term exactly.
+template <typename T, int NV>
+__device__ __forceinline__ void factor_warp_nv(const FactorArgs &a, uint32_t s0, uint32_t nbody, uint8_t kind, T p,
+                                               T q, int lane, const T *__restrict__ vf, T *__restrict__ fv) {
+    const T s = (kind & KIND_OR) ? T(-1) : T(1);
+    const T inf = Num<T>::inf();
+    T ls[NV];
+    uint32_t e[NV];
+#pragma unroll
+    for (int u = 0; u < NV; u++) {
+        const uint32_t k = lane + 32u * u;
+        ls[u] = (k < nbody) ? vf[s0 + 1 + k] : T(0);
+        e[u] = (k < nbody) ? a.f_pos[s0 + 1 + k] : kSentinel;
+    }
+    const T vh = vf[s0];
+    double L = 0.0;
+    int nz = 0;
+#pragma unroll
+    for (int u = 0; u < NV; u++) {
+        if (lane + 32u * u < nbody) {
+            ls[u] = log_sigmoid<T>(s * ls[u]);
+            if (ls[u] == -inf) nz++;
+            else L += (double)ls[u];
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        L += __shfl_xor_sync(0xffffffffu, L, o);
+        nz += __shfl_xor_sync(0xffffffffu, nz, o);
+    }
+    if ((kind & HEAD_MASK) == HEAD_FREE && lane == 0)
+        put_fv<T>(fv, a.f_pos[s0], s * head_out<T>(nz ? -inf : (T)L, p, q, Num<T>::log(p)));
+    const BodyDen<T> D = body_den<T>(s * head_effective<T>(kind, vh), p, q);
+#pragma unroll
+    for (int u = 0; u < NV; u++) {
+        if (lane + 32u * u < nbody) {
+            const bool z = (ls[u] == -inf);
+            const T lo = (nz - (int)z) ? -inf : (T)(z ? L : L - (double)ls[u]);
+            put_fv<T>(fv, e[u], s * body_out<T>(lo, p, q, D));
+        }
+    }
+}
+
+// Larger factors: lanes stride over the body, reading it twice.
+template <typename T>
+__device__ __noinline__ void factor_warp_loop(const FactorArgs &a, uint32_t s0, uint32_t s1, uint8_t kind, T p, T q,
+                                              int lane, const T *__restrict__ vf, T *__restrict__ fv) {
     const T s = (kind & KIND_OR) ? T(-1) : T(1);
     const T inf = Num<T>::inf();
     const bool free_head = (kind & HEAD_MASK) == HEAD_FREE;
@@ -372,53 +492,47 @@ __device__ void factor_warp(const FactorArgs &a, uint32_t b, int lane, const T *
         L += __shfl_xor_sync(0xffffffffu, L, o);
         nz += __shfl_xor_sync(0xffffffffu, nz, o);
     }
-    if (free_head && lane == 0) store_fv<T, DAMP>(fv, s0, s * head_out<T>(nz ? -inf : (T)L, p, q, Num<T>::log(p)), d);
+    if (free_head && lane == 0) put_fv<T>(fv, a.f_pos[s0], s * head_out<T>(nz ? -inf : (T)L, p, q, Num<T>::log(p)));
     const BodyDen<T> D = body_den<T>(lh, p, q);
     for (uint32_t k = s0 + 1 + lane; k < s1; k += 32) {
         const T ls = log_sigmoid<T>(s * vf[k]);
         const bool z = (ls == -inf);
         const T lo = (nz - (int)z) ? -inf : (T)(z ? L : L - (double)ls);
-        store_fv<T, DAMP>(fv, k, s * body_out<T>(lo, p, q, D), d);
+        put_fv<T>(fv, a.f_pos[k], s * body_out<T>(lo, p, q, D));
     }
 }
 
-__device__ __forceinline__ void record_timeout(Ctl *ctl) { atomicExch(&ctl->status, FLBP_ERR_TIMEOUT); }
-
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+// Large factor b (internal index nf_sell + b), one warp.
+template <typename T>
+__device__ __forceinline__ void factor_warp(const FactorArgs &a, uint32_t b, int lane, const T *__restrict__ vf,
+                                            T *__restrict__ fv) {
+    const uint32_t fi = a.nf_sell + b;
+    const uint32_t s0 = a.fb_off[b], s1 = a.fb_off[b + 1];
+    const uint8_t kind = a.f_kind[fi];
+    const T *pq = reinterpret_cast<const T *>(a.f_pq);
+    const T p = pq[2 * fi], q = pq[2 * fi + 1];
+    const uint32_t nbody = s1 - s0 - 1;
+    if (nbody <= 32) factor_warp_nv<T, 1>(a, s0, nbody, kind, p, q, lane, vf, fv);
+    else if (nbody <= 64) factor_warp_nv<T, 2>(a, s0, nbody, kind, p, q, lane, vf, fv);
+    else if (nbody <= 128) factor_warp_nv<T, 4>(a, s0, nbody, kind, p, q, lane, vf, fv);
+    else if (nbody <= 256) factor_warp_nv<T, 8>(a, s0, nbody, kind, p, q, lane, vf, fv);
+    else factor_warp_loop<T>(a, s0, s1, kind, p, q, lane, vf, fv);
 }
 
-// Per-tile header (16 words, host-built): [0] first group, [1] number of
-// groups n (1..8), [2 + j] slot (entry) offset of group j for j = 0..n, the
-// rest repeating the end offset.
-struct TileHdr {
-    uint32_t w[16];
-};
-
-__device__ __forceinline__ void load_hdr(const uint4 *src, uint4 (&h)[4]) {
-#pragma unroll
-    for (int i = 0; i < 4; i++) h[i] = __ldcg(src + i);
-}
-
-__device__ __forceinline__ uint32_t hdr_word(const uint4 (&h)[4], int i) {
-    const uint4 v = h[i >> 2];
-    const int k = i & 3;
-    return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w;
-}
-
-// Factor pass, warp-specialised. Blocks [0, n_tile_blocks) run a
-// STAGES-deep pipeline over tiles: warp 8 (one lane) is the producer - it
-// waits until the consumers have released a stage, bulk-stores the outputs
-// that stage holds, and bulk-loads the next tile (messages, previous
-// outputs when damping, per-factor constants) into it; warps 0-7 wait for a
-// stage to fill, compute one group each in shared memory and release it.
-// Blocks [n_tile_blocks, grid) take the large factors, one per warp.
-template <typename T, bool DAMP, int STAGES>
-__global__ void __launch_bounds__(288) factor_pass_kernel(FactorArgs a, const T *__restrict__ vf,
-                                                          T *__restrict__ fv, T d, Ctl *ctl) {
+// Factor pass. Blocks [0, n_tile_blocks) run a STAGES-deep pipeline over
+// tiles: warp kConsumerWarps (one lane) is the producer - it waits until the
+// consumer warps have released a stage and bulk-loads the next tile
+// (messages, fv positions, per-factor constants) into it; consumer warp j
+// evaluates group j of the staged tile, one factor per lane, and scatters
+// the outputs to fv. Blocks [n_tile_blocks, grid) take the large factors,
+// one per warp; without such blocks the consumer warps take them first,
+// while the producer's first loads are in flight.
+template <typename T, int STAGES>
+__global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArgs a, const T *__restrict__ vf,
+                                                                       T *__restrict__ fv, Ctl *ctl) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES];
-    typedef FactorStage<T, DAMP> FS;
+    typedef FactorStage<T> FS;
     if (*(volatile int *)&ctl->done) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         unsigned long long now;
@@ -435,7 +549,7 @@ __global__ void __launch_bounds__(288) factor_pass_kernel(FactorArgs a, const T 
     if (blockIdx.x >= a.n_tile_blocks) {  // large factors
         const uint32_t warp = (blockIdx.x - a.n_tile_blocks) * (blockDim.x >> 5) + wid;
         const uint32_t nwarps = (gridDim.x - a.n_tile_blocks) * (blockDim.x >> 5);
-        for (uint32_t b = warp; b < a.nf_big; b += nwarps) factor_warp<T, DAMP>(a, b, lane, vf, fv, d);
+        for (uint32_t b = warp; b < a.nf_big; b += nwarps) factor_warp<T>(a, b, lane, vf, fv);
         return;
     }
     const uint32_t n_tiles = a.n_tiles, nb = a.n_tile_blocks;
@@ -443,67 +557,40 @@ __global__ void __launch_bounds__(288) factor_pass_kernel(FactorArgs a, const T 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; s++) {
             mbar_init(&full[s], 1);
-            mbar_init(&empty[s], kTileGroups);
+            mbar_init(&empty[s], kConsumerWarps);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    const T *pq_g = reinterpret_cast<const T *>(a.f_pq);
 
-    if (wid == kTileGroups) {  // producer warp
+    if (wid == kConsumerWarps) {  // producer warp
         if (lane != 0) return;
+        const T *pq_g = reinterpret_cast<const T *>(a.f_pq);
         bool ok = true;
-        auto store_stage = [&](int s) {
-            unsigned char *st = smem + (size_t)s * FS::bytes;
-            const uint32_t *gb = reinterpret_cast<const uint32_t *>(st + FS::hdr);
-            const uint32_t n = gb[1];
-            const uint32_t nbytes = (gb[2 + n] - gb[2]) * (uint32_t)sizeof(T);
-            if (nbytes) {
-                bulk_s2g(fv + gb[2], st + FS::vbuf, nbytes);
-                bulk_commit();
-            }
-        };
-        uint4 h[4];
         uint32_t issued = 0;
-        if (my_tiles) load_hdr(a.thdr + 4ull * blockIdx.x, h);
+        TileHdr h;
+        if (my_tiles) h.load(a.thdr + (size_t)(kHdrWords / 4) * blockIdx.x);
         for (uint32_t it = 0; it < my_tiles; it++, issued++) {
             const int s = (int)(it % STAGES);
-            if (it >= (uint32_t)STAGES) {
-                if (!mbar_wait_bounded(&empty[s], ((it / STAGES) - 1) & 1u)) {
-                    ok = false;
-                    break;
-                }
-                store_stage(s);
-                bulk_wait_read_all();
+            if (it >= (uint32_t)STAGES && !mbar_wait_bounded(&empty[s], ((it / STAGES) - 1) & 1u)) {
+                ok = false;
+                break;
             }
             unsigned char *st = smem + (size_t)s * FS::bytes;
             uint32_t *gb = reinterpret_cast<uint32_t *>(st + FS::hdr);
-#pragma unroll
-            for (int i = 0; i < 16; i++) gb[i] = hdr_word(h, i);
+            h.store(gb);
             const uint32_t g0 = gb[0], n = gb[1];
-            const uint32_t nbytes = (gb[2 + n] - gb[2]) * (uint32_t)sizeof(T);
+            const uint32_t ns = gb[2 + n] - gb[2];
             const uint32_t items = 32u * n;
-            mbar_arrive_expect_tx(&full[s], nbytes * (DAMP ? 2u : 1u) + 2u * items + 2u * items * (uint32_t)sizeof(T));
-            if (nbytes) {
-                bulk_g2s(st + FS::vbuf, vf + gb[2], nbytes, &full[s]);
-                if (DAMP) bulk_g2s(st + FS::obuf, fv + gb[2], nbytes, &full[s]);
+            mbar_arrive_expect_tx(&full[s], ns * (uint32_t)(sizeof(T) + 4) + 2u * items + 2u * items * (uint32_t)sizeof(T));
+            if (ns) {
+                bulk_g2s(st + FS::vbuf, vf + gb[2], ns * (uint32_t)sizeof(T), &full[s]);
+                bulk_g2s(st + FS::pos, a.f_pos + gb[2], ns * 4u, &full[s]);
             }
             bulk_g2s(st + FS::deg, a.f_deg + 32ull * g0, items, &full[s]);
             bulk_g2s(st + FS::kind, a.f_kind + 32ull * g0, items, &full[s]);
             bulk_g2s(st + FS::pq, pq_g + 64ull * g0, 2u * items * (uint32_t)sizeof(T), &full[s]);
-            const uint32_t nt = blockIdx.x + (it + 1) * nb;
-            if (nt < n_tiles) load_hdr(a.thdr + 4ull * nt, h);
-        }
-        if (ok) {  // outputs still held by the last stages
-            const uint32_t first = my_tiles > (uint32_t)STAGES ? my_tiles - STAGES : 0;
-            for (uint32_t it = first; it < my_tiles; it++) {
-                const int s = (int)(it % STAGES);
-                if (!mbar_wait_bounded(&empty[s], (it / STAGES) & 1u)) {
-                    ok = false;
-                    break;
-                }
-                store_stage(s);
-            }
+            if (it + 1 < my_tiles) h.load(a.thdr + (size_t)(kHdrWords / 4) * (blockIdx.x + (size_t)(it + 1) * nb));
         }
         if (!ok) {
             record_timeout(ctl);
@@ -511,32 +598,31 @@ __global__ void __launch_bounds__(288) factor_pass_kernel(FactorArgs a, const T 
             for (uint32_t k = issued > (uint32_t)STAGES ? issued - STAGES : 0; k < issued; k++)
                 mbar_wait_bounded(&full[k % STAGES], (k / STAGES) & 1u);
         }
-        bulk_wait_all();
         return;
     }
 
-    // consumer warps; when no blocks are dedicated to large factors, they take
-    // those first, while the producer's first loads are in flight
     if (nb == gridDim.x) {
-        const uint32_t warp = blockIdx.x * kTileGroups + wid, nwarps = gridDim.x * kTileGroups;
-        for (uint32_t b = warp; b < a.nf_big; b += nwarps) factor_warp<T, DAMP>(a, b, lane, vf, fv, d);
+        const uint32_t warp = blockIdx.x * kConsumerWarps + wid, nwarps = gridDim.x * kConsumerWarps;
+        for (uint32_t b = warp; b < a.nf_big; b += nwarps) factor_warp<T>(a, b, lane, vf, fv);
     }
     for (uint32_t it = 0; it < my_tiles; it++) {
         const int s = (int)(it % STAGES);
-        if (!mbar_wait_bounded(&full[s], (it / STAGES) & 1u)) {
-            record_timeout(ctl);
+        if (!warp_wait_stage(&full[s], (it / STAGES) & 1u)) {
+            if (lane == 0) record_timeout(ctl);
             return;
         }
-        unsigned char *st = smem + (size_t)s * FS::bytes;
+        const unsigned char *st = smem + (size_t)s * FS::bytes;
         const uint32_t *gb = reinterpret_cast<const uint32_t *>(st + FS::hdr);
         if ((uint32_t)wid < gb[1]) {
+            const uint32_t base = gb[2 + wid] - gb[2], f = 32u * wid + lane;
             const int w = (int)((gb[3 + wid] - gb[2 + wid]) >> 5);
-            T *vb = reinterpret_cast<T *>(st + FS::vbuf) + (gb[2 + wid] - gb[2]);
-            const T *ob = reinterpret_cast<const T *>(st + FS::obuf) + (gb[2 + wid] - gb[2]);
-            factor_group<T, DAMP>(w, vb, ob, st + FS::deg + 32 * wid, st + FS::kind + 32 * wid,
-                                  reinterpret_cast<const T *>(st + FS::pq) + 64 * wid, lane, d);
+            const int deg = st[FS::deg + f];
+            const T *pq = reinterpret_cast<const T *>(st + FS::pq);
+            if (deg > 0)
+                factor_group<T>(w, reinterpret_cast<const T *>(st + FS::vbuf) + base,
+                                reinterpret_cast<const uint32_t *>(st + FS::pos) + base, deg, st[FS::kind + f],
+                                pq[2 * f], pq[2 * f + 1], lane, fv);
         }
-        fence_proxy_async();
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[s]);
     }
@@ -610,62 +696,77 @@ __device__ __forceinline__ void decode_prior(const void *pr, uint32_t i, double 
     nneg = (int)(cnt >> 16);
 }
 
-// One sliced-ELL group of 32 variables of width W, staged in shared memory:
-// entry k of the lane-th variable at en[32 k + lane], its prior at pr[lane],
-// its previous belief at bo[lane]. Gathers fv, sums, scatters vf.
-template <typename T, int BMODE, bool WRITE_VF, int W>
-__device__ __forceinline__ double var_group_w(const VarArgs &a, uint32_t v, bool ok, const uint32_t *en,
-                                              const void *pr, const double *bo, int lane, const T *__restrict__ fv,
-                                              T *__restrict__ vf, double pscale, double tol, unsigned long long &cnt) {
+
+// Incoming f->v message of one entry: the new one, or with damping the mix
+// of the new one with the previous damped one, which is then stored back.
+template <typename T, bool DAMP>
+__device__ __forceinline__ T take_fv(T x, T old, T d) {
+    return DAMP ? damp_mix(x, old, d) : x;
+}
+
+// One large variable, one warp, with at most 32 NV entries held in
+// registers: all loads of a lane are in flight at once.
+template <typename T, int BMODE, bool WRITE_VF, bool DAMP, int NV>
+__device__ __forceinline__ double var_warp_nv(const VarArgs &a, uint32_t v, uint32_t k0, uint32_t n, int lane,
+                                              const T *__restrict__ fv, T *__restrict__ vf, T *__restrict__ fvd,
+                                              T d, double pscale, double tol, unsigned long long &cnt) {
+    const T inf = Num<T>::inf();
+    uint32_t e[NV];
+    T x[NV], xo[DAMP ? NV : 1];
+#pragma unroll
+    for (int u = 0; u < NV; u++) {
+        const uint32_t k = lane + 32u * u;
+        e[u] = (k < n) ? a.v_ent[k0 + k] : kSentinel;
+        x[u] = (k < n) ? fv[k0 + k] : T(0);
+        if (DAMP) xo[u] = (k < n) ? fvd[k0 + k] : T(0);
+    }
     double S = 0.0;
     int npos = 0, nneg = 0;
-    if (ok) decode_prior<T>(pr, lane, pscale, S, npos, nneg);
-    const T inf = Num<T>::inf();
-    uint32_t e[W > 0 ? W : 1];
-    T x[W > 0 ? W : 1];
 #pragma unroll
-    for (int k = 0; k < W; k++) e[k] = en[32 * k + lane];
-#pragma unroll
-    for (int k = 0; k < W; k++) x[k] = (e[k] != kSentinel) ? fv[e[k]] : T(0);
-#pragma unroll
-    for (int k = 0; k < W; k++) {
-        if (x[k] == inf) npos++;
-        else if (x[k] == -inf) nneg++;
-        else S += (double)x[k];
+    for (int u = 0; u < NV; u++) {
+        if (DAMP) {
+            x[u] = take_fv<T, DAMP>(x[u], xo[u], d);
+            if (lane + 32u * u < n) fvd[k0 + lane + 32u * u] = x[u];
+        }
+        if (x[u] == inf) npos++;
+        else if (x[u] == -inf) nneg++;
+        else S += (double)x[u];
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        S += __shfl_xor_sync(0xffffffffu, S, o);
+        npos += __shfl_xor_sync(0xffffffffu, npos, o);
+        nneg += __shfl_xor_sync(0xffffffffu, nneg, o);
+    }
+    double S0;
+    int p0, n0;
+    decode_prior<T>(a.prior, v, pscale, S0, p0, n0);
+    S += S0;
+    npos += p0;
+    nneg += n0;
     if (WRITE_VF) {
 #pragma unroll
-        for (int k = 0; k < W; k++)
-            if (e[k] != kSentinel) vf[e[k]] = excl_msg<T>(S, npos, nneg, x[k]);
+        for (int u = 0; u < NV; u++)
+            if (e[u] != kSentinel) vf[e[u]] = excl_msg<T>(S, npos, nneg, x[u]);
     }
-    return ok ? var_finish<BMODE>(a, v, S, npos, nneg, tol, (BMODE == 1 || BMODE == 2) ? bo[lane] : 0.0, cnt) : 0.0;
+    return (lane == 0) ? var_finish<BMODE>(a, v, S, npos, nneg, tol, a.belief[v], cnt) : 0.0;
 }
 
-template <typename T, int BMODE, bool WRITE_VF>
-__device__ __forceinline__ double var_group(int w, const VarArgs &a, uint32_t v, bool ok, const uint32_t *en,
-                                            const void *pr, const double *bo, int lane, const T *__restrict__ fv,
-                                            T *__restrict__ vf, double pscale, double tol, unsigned long long &cnt) {
-    switch (w) {
-#define FLBP_W(N) \
-    case N: return var_group_w<T, BMODE, WRITE_VF, N>(a, v, ok, en, pr, bo, lane, fv, vf, pscale, tol, cnt);
-        FLBP_W(0) FLBP_W(1) FLBP_W(2) FLBP_W(3) FLBP_W(4) FLBP_W(5) FLBP_W(6) FLBP_W(7) FLBP_W(8) FLBP_W(9)
-        FLBP_W(10) FLBP_W(11) FLBP_W(12) FLBP_W(13) FLBP_W(14) FLBP_W(15) FLBP_W(16)
-#undef FLBP_W
-        default: return 0.0;
-    }
-}
-
-// One large variable, one warp (direct loads).
-template <typename T, int BMODE, bool WRITE_VF>
-__device__ double var_warp(const VarArgs &a, uint32_t b, int lane, const T *__restrict__ fv, T *__restrict__ vf,
-                           double pscale, double tol, unsigned long long &cnt) {
-    const uint32_t v = a.nv_sell + b;
-    const uint32_t k0 = a.vb_off[b], k1 = a.vb_off[b + 1];
+// Larger variables: lanes stride over the entries, reading them twice.
+template <typename T, int BMODE, bool WRITE_VF, bool DAMP>
+__device__ __noinline__ double var_warp_loop(const VarArgs &a, uint32_t v, uint32_t k0, uint32_t k1, int lane,
+                                             const T *__restrict__ fv, T *__restrict__ vf, T *__restrict__ fvd, T d,
+                                             double pscale, double tol, unsigned long long &cnt) {
     const T inf = Num<T>::inf();
+    const T *src = DAMP ? fvd : fv;  // after the first loop, fvd holds the messages in use
     double S = 0.0;
     int npos = 0, nneg = 0;
     for (uint32_t k = k0 + lane; k < k1; k += 32) {
-        const T x = fv[a.v_ent[k]];
+        T x = fv[k];
+        if (DAMP) {
+            x = take_fv<T, DAMP>(x, fvd[k], d);
+            fvd[k] = x;
+        }
         if (x == inf) npos++;
         else if (x == -inf) nneg++;
         else S += (double)x;
@@ -685,10 +786,23 @@ __device__ double var_warp(const VarArgs &a, uint32_t b, int lane, const T *__re
     if (WRITE_VF) {
         for (uint32_t k = k0 + lane; k < k1; k += 32) {
             const uint32_t e = a.v_ent[k];
-            vf[e] = excl_msg<T>(S, npos, nneg, fv[e]);
+            if (e != kSentinel) vf[e] = excl_msg<T>(S, npos, nneg, src[k]);
         }
     }
     return (lane == 0) ? var_finish<BMODE>(a, v, S, npos, nneg, tol, a.belief[v], cnt) : 0.0;
+}
+
+// Large variable b (internal index nv_sell + b), one warp.
+template <typename T, int BMODE, bool WRITE_VF, bool DAMP>
+__device__ __forceinline__ double var_warp(const VarArgs &a, uint32_t b, int lane, const T *__restrict__ fv,
+                                           T *__restrict__ vf, T *__restrict__ fvd, T d, double pscale, double tol,
+                                           unsigned long long &cnt) {
+    const uint32_t v = a.nv_sell + b;
+    const uint32_t k0 = a.vb_off[b], k1 = a.vb_off[b + 1], n = k1 - k0;
+    if (n <= 32) return var_warp_nv<T, BMODE, WRITE_VF, DAMP, 1>(a, v, k0, n, lane, fv, vf, fvd, d, pscale, tol, cnt);
+    if (n <= 64) return var_warp_nv<T, BMODE, WRITE_VF, DAMP, 2>(a, v, k0, n, lane, fv, vf, fvd, d, pscale, tol, cnt);
+    if (n <= 128) return var_warp_nv<T, BMODE, WRITE_VF, DAMP, 4>(a, v, k0, n, lane, fv, vf, fvd, d, pscale, tol, cnt);
+    return var_warp_loop<T, BMODE, WRITE_VF, DAMP>(a, v, k0, k1, lane, fv, vf, fvd, d, pscale, tol, cnt);
 }
 
 __device__ __forceinline__ double warp_max(double x) {
@@ -745,18 +859,23 @@ static __device__ void stop_rules(Ctl *ctl) {
     }
 }
 
-// Variable pass, warp-specialised like the factor pass: warp 8 bulk-loads
-// each tile's entries, priors and (with a residual) previous beliefs; warps
-// 0-7 gather, sum and scatter one group each. Blocks [n_tile_blocks, grid)
-// take the large variables. With BMODE 1/2 the block maxima of |belief
-// change| are combined with an atomic max and the last block to finish
-// applies the stop rules.
-template <typename T, int BMODE, bool WRITE_VF, int STAGES>
-__global__ void __launch_bounds__(288) var_pass_kernel(VarArgs a, const T *__restrict__ fv, T *__restrict__ vf,
-                                                       Ctl *ctl) {
+// Variable pass, warp-specialised like the factor pass: the producer warp
+// bulk-loads each tile's entries (factor-side slots), incoming messages, the
+// previous damped messages (with damping), priors and (with a residual)
+// previous beliefs; consumer warp j takes group j, one variable per lane:
+// the FP64 sum of its incoming messages with +-inf counts and its prior,
+// belief and residual, then the leave-one-out messages scattered to vf.
+// Blocks [n_tile_blocks, grid) take the large variables. With BMODE 1/2 the
+// block maxima of |belief change| are combined with an atomic max and the
+// last block to finish applies the stop rules. DAMP mixes each new message
+// with the previous damped one (fvd) and stores the result back to fvd.
+template <typename T, int BMODE, bool WRITE_VF, bool DAMP, int STAGES>
+__global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, const T *__restrict__ fv,
+                                                                    T *__restrict__ vf, T *__restrict__ fvd, T d,
+                                                                    Ctl *ctl) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES];
-    typedef VarStage<T> VS;
+    typedef VarStage<T, DAMP> VS;
     constexpr bool RESID = (BMODE == 1 || BMODE == 2);
     constexpr uint32_t psz = sizeof(T) == 4 ? 8u : 16u;
     if (*(volatile int *)&ctl->done) return;
@@ -766,12 +885,13 @@ __global__ void __launch_bounds__(288) var_pass_kernel(VarArgs a, const T *__res
     const uint32_t n_tiles = a.n_tiles, nb = a.n_tile_blocks;
     const bool tile_block = blockIdx.x < nb;
     const uint32_t my_tiles = (tile_block && blockIdx.x < n_tiles) ? (n_tiles - blockIdx.x + nb - 1) / nb : 0;
+    const T inf = Num<T>::inf();
     double dmax = 0.0;
     unsigned long long cnt = 0;
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; s++) {
             mbar_init(&full[s], 1);
-            mbar_init(&empty[s], kTileGroups);
+            mbar_init(&empty[s], kConsumerWarps);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -780,11 +900,11 @@ __global__ void __launch_bounds__(288) var_pass_kernel(VarArgs a, const T *__res
         const uint32_t warp = (blockIdx.x - nb) * (blockDim.x >> 5) + wid;
         const uint32_t nwarps = (gridDim.x - nb) * (blockDim.x >> 5);
         for (uint32_t b = warp; b < a.nv_big; b += nwarps)
-            dmax = fmax(dmax, var_warp<T, BMODE, WRITE_VF>(a, b, lane, fv, vf, pscale, tol, cnt));
-    } else if (wid == kTileGroups) {  // producer warp
+            dmax = fmax(dmax, var_warp<T, BMODE, WRITE_VF, DAMP>(a, b, lane, fv, vf, fvd, d, pscale, tol, cnt));
+    } else if (wid == kConsumerWarps) {  // producer warp
         if (lane == 0) {
-            uint4 h[4];
-            if (my_tiles) load_hdr(a.thdr + 4ull * blockIdx.x, h);
+            TileHdr h;
+            if (my_tiles) h.load(a.thdr + (size_t)(kHdrWords / 4) * blockIdx.x);
             for (uint32_t it = 0; it < my_tiles; it++) {
                 const int s = (int)(it % STAGES);
                 if (it >= (uint32_t)STAGES && !mbar_wait_bounded(&empty[s], ((it / STAGES) - 1) & 1u)) {
@@ -796,51 +916,79 @@ __global__ void __launch_bounds__(288) var_pass_kernel(VarArgs a, const T *__res
                 }
                 unsigned char *st = smem + (size_t)s * VS::bytes;
                 uint32_t *gb = reinterpret_cast<uint32_t *>(st + VS::hdr);
-#pragma unroll
-                for (int i = 0; i < 16; i++) gb[i] = hdr_word(h, i);
+                h.store(gb);
                 const uint32_t g0 = gb[0], n = gb[1];
-                const uint32_t ebytes = (gb[2 + n] - gb[2]) * 4u;
+                const uint32_t ns = gb[2 + n] - gb[2];
                 const uint32_t items = 32u * n;
-                mbar_arrive_expect_tx(&full[s], ebytes + psz * items + (RESID ? 8u * items : 0u));
-                if (ebytes) bulk_g2s(st + VS::ent, a.v_ent + gb[2], ebytes, &full[s]);
+                mbar_arrive_expect_tx(&full[s], ns * (4u + (DAMP ? 2u : 1u) * (uint32_t)sizeof(T)) + psz * items +
+                                                    (RESID ? 8u * items : 0u));
+                if (ns) {
+                    bulk_g2s(st + VS::ent, a.v_ent + gb[2], ns * 4u, &full[s]);
+                    bulk_g2s(st + VS::x, fv + gb[2], ns * (uint32_t)sizeof(T), &full[s]);
+                    if (DAMP) bulk_g2s(st + VS::xo, fvd + gb[2], ns * (uint32_t)sizeof(T), &full[s]);
+                }
                 bulk_g2s(st + VS::prior, reinterpret_cast<const unsigned char *>(a.prior) + 32ull * g0 * psz,
                          psz * items, &full[s]);
                 if (RESID) bulk_g2s(st + VS::bold, a.belief + 32ull * g0, 8u * items, &full[s]);
-                const uint32_t nt = blockIdx.x + (it + 1) * nb;
-                if (nt < n_tiles) load_hdr(a.thdr + 4ull * nt, h);
+                if (it + 1 < my_tiles) h.load(a.thdr + (size_t)(kHdrWords / 4) * (blockIdx.x + (size_t)(it + 1) * nb));
             }
         }
     } else {  // consumer warps (large variables first when no blocks are dedicated to them)
         if (nb == gridDim.x) {
-            const uint32_t warp = blockIdx.x * kTileGroups + wid, nwarps = gridDim.x * kTileGroups;
+            const uint32_t warp = blockIdx.x * kConsumerWarps + wid, nwarps = gridDim.x * kConsumerWarps;
             for (uint32_t b = warp; b < a.nv_big; b += nwarps)
-                dmax = fmax(dmax, var_warp<T, BMODE, WRITE_VF>(a, b, lane, fv, vf, pscale, tol, cnt));
+                dmax = fmax(dmax, var_warp<T, BMODE, WRITE_VF, DAMP>(a, b, lane, fv, vf, fvd, d, pscale, tol, cnt));
         }
         for (uint32_t it = 0; it < my_tiles; it++) {
             const int s = (int)(it % STAGES);
-            if (!mbar_wait_bounded(&full[s], (it / STAGES) & 1u)) {
-                record_timeout(ctl);
+            if (!warp_wait_stage(&full[s], (it / STAGES) & 1u)) {
+                if (lane == 0) record_timeout(ctl);
                 break;
             }
             unsigned char *st = smem + (size_t)s * VS::bytes;
             const uint32_t *gb = reinterpret_cast<const uint32_t *>(st + VS::hdr);
             if ((uint32_t)wid < gb[1]) {
+                const uint32_t base = gb[2 + wid] - gb[2];
                 const int w = (int)((gb[3 + wid] - gb[2 + wid]) >> 5);
-                const uint32_t v = (gb[0] + wid) * 32 + lane;
-                dmax = fmax(dmax, var_group<T, BMODE, WRITE_VF>(
-                                      w, a, v, v < a.nv_sell,
-                                      reinterpret_cast<const uint32_t *>(st + VS::ent) + (gb[2 + wid] - gb[2]),
-                                      st + VS::prior + (size_t)psz * 32 * wid,
-                                      reinterpret_cast<const double *>(st + VS::bold) + 32 * wid, lane, fv, vf,
-                                      pscale, tol, cnt));
+                const uint32_t t = 32u * wid + lane, v = 32u * gb[0] + t;
+                const uint32_t *en = reinterpret_cast<const uint32_t *>(st + VS::ent) + base;
+                T *x = reinterpret_cast<T *>(st + VS::x) + base;
+                const T *xo = reinterpret_cast<const T *>(st + VS::xo) + base;
+                double S = 0.0;
+                int npos = 0, nneg = 0;
+                if (v < a.nv_sell) decode_prior<T>(st + VS::prior, t, pscale, S, npos, nneg);
+                for (int k = 0; k < w; k++) {  // padding entries hold 0
+                    const int i = 32 * k + lane;
+                    T xv = x[i];
+                    if (DAMP) {
+                        xv = take_fv<T, DAMP>(xv, xo[i], d);
+                        x[i] = xv;
+                        fvd[gb[2] + base + i] = xv;
+                    }
+                    if (xv == inf) npos++;
+                    else if (xv == -inf) nneg++;
+                    else S += (double)xv;
+                }
+                if (v < a.nv_sell)
+                    dmax = fmax(dmax, var_finish<BMODE>(a, v, S, npos, nneg, tol,
+                                                        RESID ? reinterpret_cast<const double *>(st + VS::bold)[t]
+                                                              : 0.0,
+                                                        cnt));
+                if (WRITE_VF) {
+                    for (int k = 0; k < w; k++) {
+                        const int i = 32 * k + lane;
+                        const uint32_t e = en[i];
+                        if (e != kSentinel) vf[e] = excl_msg<T>(S, npos, nneg, x[i]);
+                    }
+                }
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[s]);
         }
     }
     if (RESID) {
-        __shared__ double s_max[9];
-        __shared__ unsigned long long s_cnt[9];
+        __shared__ double s_max[kConsumerWarps + 1];
+        __shared__ unsigned long long s_cnt[kConsumerWarps + 1];
         __shared__ bool s_last;
         dmax = warp_max(dmax);
         cnt = warp_sum(cnt);

@@ -155,6 +155,9 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err) {
             if (d <= kSellFactorDegree) fact_of_int[pos[d]++] = I;
             else fact_of_int[b++] = I;
         }
+        // large factors by decreasing degree: warps deal them round-robin, largest first
+        std::stable_sort(fact_of_int.begin() + nf_sell, fact_of_int.end(),
+                         [&](int64_t x, int64_t y) { return off[x + 1] - off[x] > off[y + 1] - off[y]; });
     }
     const uint32_t nf = nf_sell + nf_big;
     L.nf_sell = nf_sell;
@@ -232,12 +235,13 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err) {
     L.n_active_slots = n_act;
 
     // internal variable order: sliced-ELL variables by (degree, first slot), then big ones
+    // by decreasing degree
     std::vector<uint32_t> order(V);
     std::iota(order.begin(), order.end(), 0u);
     std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
         const bool sa = vdeg[a] <= kSellVarDegree, sb = vdeg[b] <= kSellVarDegree;
         if (sa != sb) return sa;
-        if (!sa) return false;  // big variables keep their order
+        if (!sa) return vdeg[a] > vdeg[b];
         if (vdeg[a] != vdeg[b]) return vdeg[a] < vdeg[b];
         return vfirst[a] < vfirst[b];
     });
@@ -293,6 +297,10 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err) {
         }
         L.vb_off[L.nv_big] = (uint32_t)pos;
     }
+    // slot -> entry receiving its f->v message
+    L.f_pos.assign(L.n_slots, kSentinel);
+    for (size_t i = 0; i < L.v_ent.size(); i++)
+        if (L.v_ent[i] != kSentinel) L.f_pos[L.v_ent[i]] = (uint32_t)i;
 
     // --- tiles: up to kTileGroupsHost groups within kTileSlotsHost slots ----------------
     auto make_tiles = [](const std::vector<uint32_t> &base, std::vector<uint32_t> &tiles) {

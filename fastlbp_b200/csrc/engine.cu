@@ -783,6 +783,7 @@ int flbp_compute_beliefs(flbp_engine *e, double *out, int64_t n) {
 // entry array in use (the damped one under damping) for computed messages,
 // the folded constants otherwise.
 static int fv_lambda(flbp_engine *e, std::vector<double> &lam) {
+    build_export_maps(e->L);
     const HostLayout &L = e->L;
     const size_t ne = L.v_ent.size();
     const void *src = e->d_fvd ? e->d_fvd : e->d_fv;
@@ -802,7 +803,7 @@ static int fv_lambda(flbp_engine *e, std::vector<double> &lam) {
     lam.assign((size_t)L.E, 0.0);
     for (int64_t k = 0; k < L.E; k++) {
         const int64_t s = L.ref_fv_src[k];
-        if (s >= 0) lam[k] = (L.f_pos[s] != kSentinel) ? ent[L.f_pos[s]] : 0.0;
+        if (s >= 0) lam[k] = ent[s];
         else if (s == -2) lam[k] = INFINITY;
         else if (s == -3) lam[k] = -INFINITY;
         else lam[k] = L.ref_const[k] * scale;

@@ -21,9 +21,8 @@ enum : uint8_t {
 };
 
 // Items up to these degrees go to the sliced-ELL (one item per lane) paths,
-// larger ones to the warp-per-item paths. A sliced-ELL factor keeps all of
-// its slots in registers, which bounds its degree tighter.
-constexpr uint32_t kSellFactorDegree = 8;
+// larger ones to the warp-per-item paths.
+constexpr uint32_t kSellFactorDegree = 16;
 constexpr uint32_t kSellVarDegree = 16;
 constexpr uint32_t kSentinel = 0xffffffffu;  // padding entry in the variable layout
 constexpr uint32_t kTileGroupsHost = 16;     // groups per tile (items = threads of a pass's consumers)
@@ -74,9 +73,18 @@ struct HostLayout {
     std::vector<uint32_t> internal_of_var;  // reference variable -> internal variable
     uint64_t n_active_slots = 0;       // real (non-padding) slots of active factors
 
-    // Reference variable-major slot (row_ptr_fv order) -> source of its f->v message:
-    // >= 0 device slot (its value lives at entry f_pos[slot]); -1 constant finite (value in ref_const, damping-scaled);
-    // -2 constant +inf; -3 constant -inf.
+    // Reference order, kept for message export: factor offsets, slot ->
+    // variable, slot -> fv entry of its message (kSentinel: constant message),
+    // factor -> its constant message.
+    std::vector<int64_t> ref_off;
+    std::vector<uint32_t> ref_slot_var;
+    std::vector<uint32_t> ref_ent;
+    std::vector<double> ref_fconst;
+    // Built by build_export_maps() on first use. Reference variable-major
+    // slot (row_ptr_fv order) -> source of its f->v message: >= 0 fv entry;
+    // -1 constant finite (value in ref_const, damping-scaled); -2 constant
+    // +inf; -3 constant -inf.
+    bool export_ready = false;
     std::vector<int64_t> ref_fv_src;
     std::vector<double> ref_const;
     std::vector<int64_t> row_ptr_fv;  // reference variable-major CSR (V+1)
@@ -93,6 +101,9 @@ struct HostLayout {
 
 // Builds the layout; returns FLBP_OK or an error code with `err` filled in.
 int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err);
+
+// Fills the variable-major export maps of L (idempotent).
+void build_export_maps(HostLayout &L);
 
 void set_error(const std::string &msg);
 

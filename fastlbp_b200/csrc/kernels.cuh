@@ -131,33 +131,43 @@ __device__ __forceinline__ T head_out(T lo, T p, T q, T lp) {
 // The m0 side depends only on the factor (head message, q), so it is
 // evaluated once per factor: lden = log of the scaled m0 and the value
 // returned when m0 == 0 exactly.
+// With u = a, w = b for lh >= 0 and u = b, w = a otherwise, the scaled
+// numerator is u + r w, taken as log(w) - |lh| when u == 0 (so that r cannot
+// underflow it), and the denominator likewise with (q, 1-q). Both forms are
+// selected without branches.
 template <typename T>
 struct BodyDen {
-    T lden, zero_out, r, lh;
+    T lden, zero_out, r, alh;  // alh = |lh|
+    bool pos;                  // lh >= 0
 };
 
 template <typename T>
 __device__ __forceinline__ BodyDen<T> body_den(T lh, T p, T q) {
     BodyDen<T> D;
-    D.lh = lh;
-    D.r = Num<T>::exp(-fabs(lh));
-    if (lh >= T(0)) D.lden = (q == T(0)) ? -lh : Num<T>::log(fma(D.r, T(1) - q, q));
-    else D.lden = (q == T(1)) ? lh : Num<T>::log(fma(D.r, q, T(1) - q));
-    const T s = (lh >= T(0)) ? (p - q) : (q - p);
+    D.pos = lh >= T(0);
+    D.alh = fabs(lh);
+    D.r = Num<T>::exp(-D.alh);
+    const T u = D.pos ? q : T(1) - q, w = D.pos ? T(1) - q : q;
+    D.lden = Num<T>::log(u == T(0) ? w : fma(D.r, w, u)) - (u == T(0) ? D.alh : T(0));
+    const T s = D.pos ? (p - q) : (q - p);
     D.zero_out = is_nan(lh) ? lh : ((s > T(0)) ? Num<T>::inf() : Num<T>::nan());
     if (is_nan(lh)) D.lden = -Num<T>::inf();
     return D;
 }
 
+// Body output from the pair (Po, Ro = 1 - Po) of the other body slots.
+template <typename T>
+__device__ __forceinline__ T body_out_pr(T Po, T Ro, T p, T q, const BodyDen<T> &D) {
+    const T a = p * Po + q * Ro, b = (T(1) - p) * Po + (T(1) - q) * Ro;
+    const T u = D.pos ? a : b, w = D.pos ? b : a;
+    const T lnum = Num<T>::log(u == T(0) ? w : fma(D.r, w, u)) - (u == T(0) ? D.alh : T(0));
+    return (D.lden == -Num<T>::inf()) ? D.zero_out : lnum - D.lden;
+}
+
+// Body output from lo = log Po.
 template <typename T>
 __device__ __forceinline__ T body_out(T lo, T p, T q, const BodyDen<T> &D) {
-    if (D.lden == -Num<T>::inf()) return D.zero_out;
-    const T P = Num<T>::exp(lo), R = -Num<T>::expm1(lo);
-    const T a = p * P + q * R, b = (T(1) - p) * P + (T(1) - q) * R;
-    T lnum;
-    if (D.lh >= T(0)) lnum = (a == T(0)) ? Num<T>::log(b) - D.lh : Num<T>::log(fma(D.r, b, a));
-    else lnum = (b == T(0)) ? D.lh + Num<T>::log(a) : Num<T>::log(fma(D.r, a, b));
-    return lnum - D.lden;
+    return body_out_pr<T>(Num<T>::exp(lo), -Num<T>::expm1(lo), p, q, D);
 }
 
 // Damping of an f->v message in log-odds: (1-d) new + d old, with exact
@@ -337,21 +347,19 @@ __device__ __forceinline__ void sig_pair(T x, T &sg, T &tau) {
     tau = pos ? e * inv : inv;
 }
 
-// AND -> body output from the leave-one-out pair (Po, Ro = 1 - Po) and the
-// factor's denominator (see body_out).
-template <typename T>
-__device__ __forceinline__ T body_out_pr(T Po, T Ro, T p, T q, const BodyDen<T> &D) {
-    if (D.lden == -Num<T>::inf()) return D.zero_out;
-    const T a = p * Po + q * Ro, b = (T(1) - p) * Po + (T(1) - q) * Ro;
-    T lnum;
-    if (D.lh >= T(0)) lnum = (a == T(0)) ? Num<T>::log(b) - D.lh : Num<T>::log(fma(D.r, b, a));
-    else lnum = (b == T(0)) ? D.lh + Num<T>::log(a) : Num<T>::log(fma(D.r, a, b));
-    return lnum - D.lden;
-}
-
 template <typename T>
 __device__ __forceinline__ void put_fv(T *__restrict__ fv, uint32_t e, T o) {
     if (e != kSentinel) fv[e] = o;
+}
+
+// Head output of an AND factor from the pair (P, R = 1 - P) of its whole
+// body: m1 ~ p P + q R, m0 ~ (1-p) P + (1-q) R (causal_bp_parall.cu:113-151
+// in log-odds). With q == 0 and P not a normal number, p P is taken in log
+// space from lP(), the sum of the body's log-sigmoids.
+template <typename T, typename LogP>
+__device__ __forceinline__ T head_from_pair(T P, T R, T p, T q, LogP lP) {
+    const T la = (q == T(0) && P < Num<T>::tiny()) ? Num<T>::log(p) + lP() : Num<T>::log(fma(p, P, q * R));
+    return la - Num<T>::log(fma(T(1) - p, P, (T(1) - q) * R));
 }
 
 // One factor of a sliced-ELL group of width W, one lane, all in registers:
@@ -360,56 +368,81 @@ __device__ __forceinline__ void put_fv(T *__restrict__ fv, uint32_t e, T o) {
 // body messages (AND orientation), pairs combine as
 //   (P1, R1) o (P2, R2) = (P1 P2, R1 + P1 R2),
 // a product and its complement: every term is non-negative, so P and 1 - P
-// both keep full relative precision and exact zeros stay exact. Suffix pairs
-// (backwards) then prefix pairs (forwards) give each body slot the pair of
-// all other body slots without a division.
-//   head:  m1 ~ p P + q R,  m0 ~ (1-p) P + (1-q) R   over the whole body
-//   body:  body_out_pr over the other body slots (causal_bp_parall.cu:113-151,
-//          289-314, 341-366 in log-odds; OR = AND on negated log-odds).
+// both keep full relative precision and exact zeros stay exact. Prefix and
+// suffix pairs give each body slot the pair of all other body slots without
+// a division; its output is body_out_pr (causal_bp_parall.cu:289-314,
+// 341-366 in log-odds; OR = AND on negated log-odds). Widths up to 8 keep
+// sigma, tau and the suffix pairs of every slot (4 W registers); wider
+// groups keep only the prefix pairs and evaluate sigma again on the way back.
 template <typename T, int W>
 __device__ __forceinline__ void factor_reg(const T *vb, const uint32_t *ps, int deg, uint8_t kind, T p, T q, int lane,
                                            T *__restrict__ fv) {
     const T sgn = (kind & KIND_OR) ? T(-1) : T(1);
-    T sg[W], ta[W];
+    auto logP = [&]() {
+        T l = T(0);
 #pragma unroll
-    for (int k = 1; k < W; k++) {
-        if (k < deg) {
-            sig_pair<T>(sgn * vb[32 * k + lane], sg[k], ta[k]);
-        } else {  // padding slot: the identity pair
-            sg[k] = T(1);
-            ta[k] = T(0);
-        }
-    }
-    T sP[W], sR[W];
-    T P = T(1), R = T(0);
-#pragma unroll
-    for (int k = W - 1; k >= 1; k--) {
-        sP[k] = P;
-        sR[k] = R;
-        R = fma(sg[k], R, ta[k]);
-        P = sg[k] * P;
-    }
+        for (int k = 1; k < W; k++)
+            if (k < deg) l += log_sigmoid<T>(sgn * vb[32 * k + lane]);
+        return l;
+    };
     const T lh = sgn * head_effective<T>(kind, vb[lane]);
-    if ((kind & HEAD_MASK) == HEAD_FREE) {
-        T la;
-        if (q == T(0) && P < Num<T>::tiny()) {  // p P in log space when P is not a normal number
-            T lP = T(0);
+    if constexpr (W <= 8) {
+        T sg[W], ta[W];
 #pragma unroll
-            for (int k = 1; k < W; k++)
-                if (k < deg) lP += log_sigmoid<T>(sgn * vb[32 * k + lane]);
-            la = Num<T>::log(p) + lP;
-        } else {
-            la = Num<T>::log(fma(p, P, q * R));
+        for (int k = 1; k < W; k++) {
+            if (k < deg) {
+                sig_pair<T>(sgn * vb[32 * k + lane], sg[k], ta[k]);
+            } else {  // padding slot: the identity pair
+                sg[k] = T(1);
+                ta[k] = T(0);
+            }
         }
-        put_fv<T>(fv, ps[lane], sgn * (la - Num<T>::log(fma(T(1) - p, P, (T(1) - q) * R))));
-    }
-    const BodyDen<T> D = body_den<T>(lh, p, q);
-    T Pp = T(1), Rp = T(0);
+        T sP[W], sR[W];
+        T P = T(1), R = T(0);
 #pragma unroll
-    for (int k = 1; k < W; k++) {
-        if (k < deg) put_fv<T>(fv, ps[32 * k + lane], sgn * body_out_pr<T>(Pp * sP[k], fma(Pp, sR[k], Rp), p, q, D));
-        Rp = fma(Pp, ta[k], Rp);
-        Pp = Pp * sg[k];
+        for (int k = W - 1; k >= 1; k--) {
+            sP[k] = P;
+            sR[k] = R;
+            R = fma(sg[k], R, ta[k]);
+            P = sg[k] * P;
+        }
+        if ((kind & HEAD_MASK) == HEAD_FREE) put_fv<T>(fv, ps[lane], sgn * head_from_pair<T>(P, R, p, q, logP));
+        const BodyDen<T> D = body_den<T>(lh, p, q);
+        T Pp = T(1), Rp = T(0);
+#pragma unroll
+        for (int k = 1; k < W; k++) {
+            if (k < deg)
+                put_fv<T>(fv, ps[32 * k + lane], sgn * body_out_pr<T>(Pp * sP[k], fma(Pp, sR[k], Rp), p, q, D));
+            Rp = fma(Pp, ta[k], Rp);
+            Pp = Pp * sg[k];
+        }
+    } else {
+        T pP[W], pR[W];
+        T P = T(1), R = T(0);
+#pragma unroll
+        for (int k = 1; k < W; k++) {
+            pP[k] = P;
+            pR[k] = R;
+            if (k < deg) {
+                T sk, tk;
+                sig_pair<T>(sgn * vb[32 * k + lane], sk, tk);
+                R = fma(P, tk, R);
+                P = P * sk;
+            }
+        }
+        if ((kind & HEAD_MASK) == HEAD_FREE) put_fv<T>(fv, ps[lane], sgn * head_from_pair<T>(P, R, p, q, logP));
+        const BodyDen<T> D = body_den<T>(lh, p, q);
+        T Ps = T(1), Rs = T(0);
+#pragma unroll
+        for (int k = W - 1; k >= 1; k--) {
+            if (k < deg) {
+                T sk, tk;
+                sig_pair<T>(sgn * vb[32 * k + lane], sk, tk);
+                put_fv<T>(fv, ps[32 * k + lane], sgn * body_out_pr<T>(pP[k] * Ps, fma(pP[k], Rs, pR[k]), p, q, D));
+                Rs = fma(sk, Rs, tk);
+                Ps = sk * Ps;
+            }
+        }
     }
 }
 
@@ -419,56 +452,109 @@ __device__ __forceinline__ void factor_group(int w, const T *vb, const uint32_t 
     switch (w) {
 #define FLBP_W(N) \
     case N: factor_reg<T, N>(vb, ps, deg, kind, p, q, lane, fv); break;
-        FLBP_W(2) FLBP_W(3) FLBP_W(4) FLBP_W(5) FLBP_W(6) FLBP_W(7) FLBP_W(8)
+        FLBP_W(2) FLBP_W(3) FLBP_W(4) FLBP_W(5) FLBP_W(6) FLBP_W(7) FLBP_W(8) FLBP_W(9) FLBP_W(10) FLBP_W(11)
+        FLBP_W(12) FLBP_W(13) FLBP_W(14) FLBP_W(15) FLBP_W(16)
 #undef FLBP_W
         default: break;
     }
 }
-static_assert(kSellFactorDegree == 8, "factor_group instantiates widths 2..8");
+static_assert(kSellFactorDegree == 16, "factor_group instantiates widths 2..16");
 
-// One large factor, one warp, with at most 32 NV body slots held in
-// registers: every lane issues all of its loads at once, so the warp waits
-// for memory once per factor. The body sum is a double with a count of -inf
-// terms so that each slot can remove its own term exactly.
+// Pair of a warp's lanes 0..lane (forward) combined with a shuffle scan.
+template <typename T>
+__device__ __forceinline__ void warp_scan_pairs(T &P, T &R, int lane) {
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const T oP = __shfl_up_sync(0xffffffffu, P, off), oR = __shfl_up_sync(0xffffffffu, R, off);
+        if (lane >= off) {
+            R = fma(oP, R, oR);
+            P = oP * P;
+        }
+    }
+}
+
+// Pair of a warp's lanes lane..31 (backward).
+template <typename T>
+__device__ __forceinline__ void warp_rscan_pairs(T &P, T &R, int lane) {
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const T oP = __shfl_down_sync(0xffffffffu, P, off), oR = __shfl_down_sync(0xffffffffu, R, off);
+        if (lane + off < 32) {
+            R = fma(P, oR, R);
+            P = P * oP;
+        }
+    }
+}
+
+// One large factor, one warp, with at most 32 NV body slots: lane l holds
+// slots [l NV, l NV + NV) of the body as (sigma, tau) pairs, so all of its
+// loads are in flight at once. Each slot's leave-one-out pair is
+//   (lanes before) o (own earlier slots) o (own later slots) o (lanes after),
+// from two shuffle scans over the lanes' pairs; no division, exact zeros
+// stay exact.
 template <typename T, int NV>
 __device__ __forceinline__ void factor_warp_nv(const FactorArgs &a, uint32_t s0, uint32_t nbody, uint8_t kind, T p,
                                                T q, int lane, const T *__restrict__ vf, T *__restrict__ fv) {
-    const T s = (kind & KIND_OR) ? T(-1) : T(1);
-    const T inf = Num<T>::inf();
-    T ls[NV];
+    const T sgn = (kind & KIND_OR) ? T(-1) : T(1);
+    const uint32_t k0 = (uint32_t)lane * NV;  // first body slot of this lane (body index)
+    T sg[NV], ta[NV];
     uint32_t e[NV];
 #pragma unroll
     for (int u = 0; u < NV; u++) {
-        const uint32_t k = lane + 32u * u;
-        ls[u] = (k < nbody) ? vf[s0 + 1 + k] : T(0);
-        e[u] = (k < nbody) ? a.f_pos[s0 + 1 + k] : kSentinel;
+        const bool in = k0 + u < nbody;
+        const T x = in ? vf[s0 + 1 + k0 + u] : T(0);
+        e[u] = in ? a.f_pos[s0 + 1 + k0 + u] : kSentinel;
+        if (in) {
+            sig_pair<T>(sgn * x, sg[u], ta[u]);
+        } else {
+            sg[u] = T(1);
+            ta[u] = T(0);
+        }
     }
     const T vh = vf[s0];
-    double L = 0.0;
-    int nz = 0;
+    T lP = T(1), lR = T(0);  // this lane's slots
 #pragma unroll
     for (int u = 0; u < NV; u++) {
-        if (lane + 32u * u < nbody) {
-            ls[u] = log_sigmoid<T>(s * ls[u]);
-            if (ls[u] == -inf) nz++;
-            else L += (double)ls[u];
-        }
+        lR = fma(lP, ta[u], lR);
+        lP = lP * sg[u];
     }
+    T fP = lP, fR = lR, bP = lP, bR = lR;
+    warp_scan_pairs<T>(fP, fR, lane);
+    warp_rscan_pairs<T>(bP, bR, lane);
+    const T P = __shfl_sync(0xffffffffu, fP, 31), R = __shfl_sync(0xffffffffu, fR, 31);
+    T eP = __shfl_up_sync(0xffffffffu, fP, 1), eR = __shfl_up_sync(0xffffffffu, fR, 1);  // lanes before
+    T xP = __shfl_down_sync(0xffffffffu, bP, 1), xR = __shfl_down_sync(0xffffffffu, bR, 1);  // lanes after
+    if (lane == 0) eP = T(1), eR = T(0);
+    if (lane == 31) xP = T(1), xR = T(0);
+    if ((kind & HEAD_MASK) == HEAD_FREE) {
+        auto logP = [&]() {  // rare: whole-body log-sigmoid sum, by the whole warp
+            double l = 0.0;
+            for (uint32_t k = lane; k < nbody; k += 32) l += (double)log_sigmoid<T>(sgn * vf[s0 + 1 + k]);
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        L += __shfl_xor_sync(0xffffffffu, L, o);
-        nz += __shfl_xor_sync(0xffffffffu, nz, o);
+            for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+            return (T)l;
+        };
+        const T o = sgn * head_from_pair<T>(P, R, p, q, logP);
+        if (lane == 0) put_fv<T>(fv, a.f_pos[s0], o);
     }
-    if ((kind & HEAD_MASK) == HEAD_FREE && lane == 0)
-        put_fv<T>(fv, a.f_pos[s0], s * head_out<T>(nz ? -inf : (T)L, p, q, Num<T>::log(p)));
-    const BodyDen<T> D = body_den<T>(s * head_effective<T>(kind, vh), p, q);
+    const BodyDen<T> D = body_den<T>(sgn * head_effective<T>(kind, vh), p, q);
+    // own later slots, then the lanes after: suffix pairs, backwards
+    T sP[NV], sR[NV];
+    T cP = xP, cR = xR;
+#pragma unroll
+    for (int u = NV - 1; u >= 0; u--) {
+        sP[u] = cP;
+        sR[u] = cR;
+        cR = fma(sg[u], cR, ta[u]);
+        cP = sg[u] * cP;
+    }
+    T Pp = eP, Rp = eR;
 #pragma unroll
     for (int u = 0; u < NV; u++) {
-        if (lane + 32u * u < nbody) {
-            const bool z = (ls[u] == -inf);
-            const T lo = (nz - (int)z) ? -inf : (T)(z ? L : L - (double)ls[u]);
-            put_fv<T>(fv, e[u], s * body_out<T>(lo, p, q, D));
-        }
+        if (k0 + u < nbody)
+            put_fv<T>(fv, e[u], sgn * body_out_pr<T>(Pp * sP[u], fma(Pp, sR[u], Rp), p, q, D));
+        Rp = fma(Pp, ta[u], Rp);
+        Pp = Pp * sg[u];
     }
 }
 
@@ -515,7 +601,6 @@ __device__ __forceinline__ void factor_warp(const FactorArgs &a, uint32_t b, int
     if (nbody <= 32) factor_warp_nv<T, 1>(a, s0, nbody, kind, p, q, lane, vf, fv);
     else if (nbody <= 64) factor_warp_nv<T, 2>(a, s0, nbody, kind, p, q, lane, vf, fv);
     else if (nbody <= 128) factor_warp_nv<T, 4>(a, s0, nbody, kind, p, q, lane, vf, fv);
-    else if (nbody <= 256) factor_warp_nv<T, 8>(a, s0, nbody, kind, p, q, lane, vf, fv);
     else factor_warp_loop<T>(a, s0, s1, kind, p, q, lane, vf, fv);
 }
 

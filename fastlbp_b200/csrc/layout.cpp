@@ -219,7 +219,7 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err) {
     // active body slot or the head slot of an active factor with a free head.
     std::vector<uint8_t> entry(E, 0);
     std::vector<uint32_t> vdeg(V, 0);
-    std::vector<uint32_t> vfirst(V, UINT32_MAX);
+    std::vector<uint32_t> var_of_dev(L.n_slots, UINT32_MAX);  // device slot -> variable of its entry
     uint64_t n_act = 0;
     for (int64_t I = 0; I < F; I++) {
         if (!active[I]) continue;
@@ -227,43 +227,48 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err) {
         for (int64_t e = off[I]; e < off[I + 1]; e++) {
             if (e == g.factor_head[I] && head_state[I] != HEAD_FREE) continue;
             entry[e] = 1;
-            const int64_t v = g.slot_var[e];
+            const uint32_t v = (uint32_t)g.slot_var[e];
             vdeg[v]++;
-            vfirst[v] = std::min(vfirst[v], dev_slot[e]);
+            var_of_dev[dev_slot[e]] = v;
         }
     }
     L.n_active_slots = n_act;
 
-    // internal variable order: sliced-ELL variables by (degree, first slot), then big ones
-    // by decreasing degree
-    std::vector<uint32_t> order(V);
-    std::iota(order.begin(), order.end(), 0u);
-    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
-        const bool sa = vdeg[a] <= kSellVarDegree, sb = vdeg[b] <= kSellVarDegree;
-        if (sa != sb) return sa;
-        if (!sa) return vdeg[a] > vdeg[b];
-        if (vdeg[a] != vdeg[b]) return vdeg[a] < vdeg[b];
-        return vfirst[a] < vfirst[b];
-    });
+    // Internal variable order: sliced-ELL variables by degree and, within a
+    // degree, by their first device slot (so that variables reached from
+    // neighbouring factors sit together), then the large ones by decreasing
+    // degree. One scan over the device slots in increasing order finds every
+    // variable's first slot.
     uint32_t nv_sell = 0;
-    for (int64_t i = 0; i < V; i++)
-        if (vdeg[i] <= kSellVarDegree) nv_sell++;
+    std::vector<uint32_t> order(V);
+    {
+        std::vector<uint64_t> pos(kSellVarDegree + 2, 0);
+        for (int64_t i = 0; i < V; i++)
+            if (vdeg[i] <= kSellVarDegree) pos[vdeg[i] + 1]++, nv_sell++;
+        for (uint32_t d = 1; d <= kSellVarDegree + 1; d++) pos[d] += pos[d - 1];
+        for (int64_t i = 0; i < V; i++)
+            if (vdeg[i] == 0) order[pos[0]++] = (uint32_t)i;
+        std::vector<uint8_t> seen(V, 0);
+        for (uint64_t sl = 0; sl < L.n_slots; sl++) {
+            const uint32_t v = var_of_dev[sl];
+            if (v == UINT32_MAX || seen[v]) continue;
+            seen[v] = 1;
+            if (vdeg[v] <= kSellVarDegree) order[pos[vdeg[v]]++] = v;
+        }
+        uint32_t b = nv_sell;
+        for (int64_t i = 0; i < V; i++)
+            if (vdeg[i] > kSellVarDegree) order[b++] = (uint32_t)i;
+        std::stable_sort(order.begin() + nv_sell, order.end(), [&](uint32_t x, uint32_t y) { return vdeg[x] > vdeg[y]; });
+    }
     L.nv_sell = nv_sell;
     L.nv_big = (uint32_t)V - nv_sell;
     L.var_of_internal.assign(order.begin(), order.end());
     L.internal_of_var.assign(V, 0);
     for (uint32_t iv = 0; iv < (uint32_t)V; iv++) L.internal_of_var[order[iv]] = iv;
 
-    // per-variable entry lists, sorted by device slot
-    std::vector<uint64_t> vstart((size_t)V + 1, 0);
-    for (int64_t i = 0; i < V; i++) vstart[i + 1] = vstart[i] + vdeg[i];
-    std::vector<uint32_t> ents(vstart[V]);
-    {
-        std::vector<uint64_t> cur(vstart.begin(), vstart.end() - 1);
-        for (int64_t e = 0; e < E; e++)
-            if (entry[e]) ents[cur[g.slot_var[e]]++] = dev_slot[e];
-        for (int64_t i = 0; i < V; i++) std::sort(ents.begin() + vstart[i], ents.begin() + vstart[i + 1]);
-    }
+    // Entry positions: group base + 32 k + lane for sliced-ELL variables, a
+    // contiguous run for large ones; entry k of a variable is its k-th device
+    // slot in increasing order.
     {
         const uint32_t ng = (nv_sell + 31) / 32;
         L.vg_base.assign(ng + 1, 0);
@@ -281,26 +286,36 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err) {
             return FLBP_ERR_LIMIT;
         }
         L.vg_base[ng] = (uint32_t)nent;
-        L.v_ent.assign(nent + nbig, kSentinel);
-        for (uint32_t gi = 0; gi < ng; gi++) {
-            for (uint32_t iv = gi * 32; iv < std::min(nv_sell, gi * 32 + 32); iv++) {
-                const uint32_t v = order[iv], lane = iv - gi * 32;
-                for (uint32_t k = 0; k < vdeg[v]; k++) L.v_ent[L.vg_base[gi] + 32ull * k + lane] = ents[vstart[v] + k];
-            }
-        }
         L.vb_off.assign((size_t)L.nv_big + 1, 0);
         uint64_t pos = nent;
         for (uint32_t b = 0; b < L.nv_big; b++) {
-            const uint32_t v = order[nv_sell + b];
             L.vb_off[b] = (uint32_t)pos;
-            for (uint32_t k = 0; k < vdeg[v]; k++) L.v_ent[pos++] = ents[vstart[v] + k];
+            pos += vdeg[order[nv_sell + b]];
         }
         L.vb_off[L.nv_big] = (uint32_t)pos;
+        // first entry position and stride of every variable
+        std::vector<uint32_t> epos(V), estride(V);
+        for (uint32_t iv = 0; iv < (uint32_t)V; iv++) {
+            const uint32_t v = order[iv];
+            if (iv < nv_sell) {
+                epos[v] = L.vg_base[iv / 32] + (iv % 32);
+                estride[v] = 32;
+            } else {
+                epos[v] = L.vb_off[iv - nv_sell];
+                estride[v] = 1;
+            }
+        }
+        L.v_ent.assign(nent + nbig, kSentinel);
+        L.f_pos.assign(L.n_slots, kSentinel);  // slot -> entry receiving its f->v message
+        for (uint64_t sl = 0; sl < L.n_slots; sl++) {
+            const uint32_t v = var_of_dev[sl];
+            if (v == UINT32_MAX) continue;
+            const uint32_t ep = epos[v];
+            epos[v] += estride[v];
+            L.v_ent[ep] = (uint32_t)sl;
+            L.f_pos[sl] = ep;
+        }
     }
-    // slot -> entry receiving its f->v message
-    L.f_pos.assign(L.n_slots, kSentinel);
-    for (size_t i = 0; i < L.v_ent.size(); i++)
-        if (L.v_ent[i] != kSentinel) L.f_pos[L.v_ent[i]] = (uint32_t)i;
 
     // --- tiles: up to kTileGroupsHost groups within kTileSlotsHost slots ----------------
     auto make_tiles = [](const std::vector<uint32_t> &base, std::vector<uint32_t> &tiles) {
@@ -341,32 +356,44 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err) {
         L.prior_fin = fin;
     }
 
-    // --- message export map (reference variable-major order) ------------------------
+    // --- reference-order data for message export (maps built on first use) ----------
+    L.ref_off.assign(off, off + F + 1);
+    L.ref_slot_var.resize(E);
+    L.ref_ent.resize(E);
+    for (int64_t e = 0; e < E; e++) {
+        L.ref_slot_var[e] = (uint32_t)g.slot_var[e];
+        L.ref_ent[e] = entry[e] ? L.f_pos[dev_slot[e]] : kSentinel;
+    }
+    L.ref_fconst = std::move(fconst);
+    return FLBP_OK;
+}
+
+void build_export_maps(HostLayout &L) {
+    if (L.export_ready) return;
+    const int64_t V = L.V, F = L.F, E = L.E;
     L.row_ptr_fv.assign((size_t)V + 1, 0);
-    for (int64_t e = 0; e < E; e++) L.row_ptr_fv[g.slot_var[e] + 1]++;
+    for (int64_t e = 0; e < E; e++) L.row_ptr_fv[L.ref_slot_var[e] + 1]++;
     for (int64_t i = 0; i < V; i++) L.row_ptr_fv[i + 1] += L.row_ptr_fv[i];
     L.ref_fv_src.assign(E, 0);
     L.ref_const.assign(E, 0.0);
     L.fm_to_vm.assign(E, 0);
     L.vm_var.assign(E, 0);
-    {
-        std::vector<int64_t> cur(L.row_ptr_fv.begin(), L.row_ptr_fv.end() - 1);
-        for (int64_t I = 0; I < F; I++) {
-            for (int64_t e = off[I]; e < off[I + 1]; e++) {
-                const int64_t pos = cur[g.slot_var[e]]++;
-                L.fm_to_vm[e] = pos;
-                L.vm_var[pos] = g.slot_var[e];
-                if (entry[e]) {
-                    L.ref_fv_src[pos] = dev_slot[e];
-                } else {
-                    const double c = fconst[I];
-                    L.ref_fv_src[pos] = (c == kInf) ? -2 : (c == -kInf) ? -3 : -1;
-                    L.ref_const[pos] = c;
-                }
+    std::vector<int64_t> cur(L.row_ptr_fv.begin(), L.row_ptr_fv.end() - 1);
+    for (int64_t I = 0; I < F; I++) {
+        for (int64_t e = L.ref_off[I]; e < L.ref_off[I + 1]; e++) {
+            const int64_t pos = cur[L.ref_slot_var[e]]++;
+            L.fm_to_vm[e] = pos;
+            L.vm_var[pos] = L.ref_slot_var[e];
+            if (L.ref_ent[e] != kSentinel) {
+                L.ref_fv_src[pos] = L.ref_ent[e];
+            } else {
+                const double c = L.ref_fconst[I];
+                L.ref_fv_src[pos] = (c == kInf) ? -2 : (c == -kInf) ? -3 : -1;
+                L.ref_const[pos] = c;
             }
         }
     }
-    return FLBP_OK;
+    L.export_ready = true;
 }
 
 }  // namespace flbp

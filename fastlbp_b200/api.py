@@ -266,10 +266,10 @@ class Engine:
         return m0, m1
 
     def stats(self) -> Dict[str, int]:
-        c = np.zeros(10, np.int64)
+        c = np.zeros(14, np.int64)
         check(lib().flbp_engine_stats(self._h, c, c.size))
         keys = ["vars", "factors", "slots", "active_factors", "active_slots", "warp_factors", "warp_vars", "bytes",
-                "h2d_bytes", "launches"]
+                "h2d_bytes", "launches", "huge_factors", "huge_vars", "big_factor_tiles", "big_var_tiles"]
         return dict(zip(keys, (int(x) for x in c)))
 
     def set_kernel_timing(self, enable: bool) -> None:

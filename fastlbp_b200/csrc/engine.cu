@@ -52,6 +52,11 @@ struct flbp_engine {
     size_t n_ent = 0;
     uint32_t *d_fg_base = nullptr, *d_fb_off = nullptr, *d_vg_base = nullptr, *d_vb_off = nullptr, *d_v_ent = nullptr;
     uint32_t *d_ftiles = nullptr, *d_vtiles = nullptr;  // kHdrWords-word headers per tile
+    uint32_t *d_fb_deg = nullptr, *d_vb_deg = nullptr;   // big items' degrees
+    uint32_t *d_fbt_deg = nullptr, *d_vbt_deg = nullptr;  // per big tile: degrees of its items
+    uint8_t *d_fbt_kind = nullptr;                        // per big tile: kinds of its factors
+    void *d_fbt_pq = nullptr;                             // per big tile: (p, q) of its factors
+    void *d_vbt_prior = nullptr;                          // per big tile: priors of its variables
     uint32_t f_tile_blocks = 0, v_tile_blocks = 0;
     uint8_t *d_f_kind = nullptr, *d_f_deg = nullptr;
     void *d_prior = nullptr;
@@ -94,11 +99,16 @@ FactorArgs factor_args(flbp_engine *e) {
     a.f_kind = e->d_f_kind;
     a.f_deg = e->d_f_deg;
     a.f_pq = e->d_f_pq;
+    a.fb_deg = e->d_fb_deg;
+    a.bt_deg = e->d_fbt_deg;
+    a.bt_kind = e->d_fbt_kind;
+    a.bt_pq = e->d_fbt_pq;
     a.nf_sell = e->L.nf_sell;
     a.nf_big = e->L.nf_big;
+    a.nf_huge = e->L.nf_huge;
     a.n_fgroups = e->L.n_fgroups();
     a.thdr = reinterpret_cast<const uint4 *>(e->d_ftiles);
-    a.n_tiles = (uint32_t)e->L.ftiles.size() - 1;
+    a.n_tiles = e->L.n_ftiles;
     a.n_tile_blocks = e->f_tile_blocks;
     return a;
 }
@@ -107,6 +117,9 @@ VarArgs var_args(flbp_engine *e) {
     VarArgs a;
     a.vg_base = e->d_vg_base;
     a.vb_off = e->d_vb_off;
+    a.vb_deg = e->d_vb_deg;
+    a.bt_deg = e->d_vbt_deg;
+    a.bt_prior = e->d_vbt_prior;
     a.v_ent = e->d_v_ent;
     a.prior = e->d_prior;
     a.belief = e->d_belief;
@@ -115,9 +128,10 @@ VarArgs var_args(flbp_engine *e) {
     a.hist_count = e->d_hist_count;
     a.nv_sell = e->L.nv_sell;
     a.nv_big = e->L.nv_big;
+    a.nv_huge = e->L.nv_huge;
     a.n_vgroups = e->L.n_vgroups();
     a.thdr = reinterpret_cast<const uint4 *>(e->d_vtiles);
-    a.n_tiles = (uint32_t)e->L.vtiles.size() - 1;
+    a.n_tiles = e->L.n_vtiles;
     a.n_tile_blocks = e->v_tile_blocks;
     a.hist_len = e->hist_cap;
     return a;
@@ -472,33 +486,17 @@ int flbp_engine_create(const flbp_graph_desc *graph, const flbp_engine_opts *opt
     }
     fb = std::max(fb, 1);
     vb = std::max(vb, 1);
-    // Tile blocks run the shared-memory pipeline; the remaining blocks take the
-    // large-degree items concurrently, in proportion to their share of the work.
-    const char *split_env = getenv("FLBP_SPLIT_BLOCKS");
-    const bool dedicated = split_env && split_env[0] == '1';
-    auto split = [&](uint32_t n_tiles, uint64_t tile_work, uint32_t n_big, uint64_t big_work, int per_sm,
-                     uint32_t &tile_blocks) -> int {
+    // One wave of resident blocks; every block's consumer warps first take the
+    // items too large for a tile (one per warp), then the block's tiles.
+    auto grid = [&](uint32_t n_tiles, uint32_t n_huge, int per_sm, uint32_t &tile_blocks) -> int {
         const uint64_t total = (uint64_t)sms * (uint64_t)per_sm;
-        if (!dedicated) {  // every block takes large items first, then tiles
-            const uint64_t g = std::max<uint64_t>(
-                1, std::min<uint64_t>(total, std::max<uint64_t>(n_tiles, (n_big + kConsumerWarps - 1) / kConsumerWarps)));
-            tile_blocks = (uint32_t)g;
-            return (int)g;
-        }
-        uint64_t bigb = 0;
-        if (n_big) {
-            bigb = (total * big_work + (tile_work + big_work) - 1) / std::max<uint64_t>(1, tile_work + big_work);
-            bigb = std::max<uint64_t>(1, std::min<uint64_t>(bigb, (n_big + kConsumerWarps) / (kConsumerWarps + 1)));
-            if (n_tiles) bigb = std::min<uint64_t>(bigb, total > 1 ? total - 1 : 1);
-        }
-        tile_blocks = (uint32_t)std::min<uint64_t>(n_tiles, std::max<uint64_t>(1, total - bigb));
-        return (int)std::max<uint64_t>(1, tile_blocks + bigb);
+        const uint64_t g = std::max<uint64_t>(
+            1, std::min<uint64_t>(total, std::max<uint64_t>(n_tiles, (n_huge + kConsumerWarps - 1) / kConsumerWarps)));
+        tile_blocks = (uint32_t)g;
+        return (int)g;
     };
-    const uint32_t n_ft = (uint32_t)L.ftiles.size() - 1, n_vt = (uint32_t)L.vtiles.size() - 1;
-    const uint64_t f_big_slots = L.fb_off.empty() ? 0 : L.fb_off.back() - L.fb_off.front();
-    const uint64_t v_big_ents = L.vb_off.empty() ? 0 : L.vb_off.back() - L.vb_off.front();
-    e->factor_grid = split(n_ft, L.fg_base.empty() ? 0 : L.fg_base.back(), L.nf_big, f_big_slots, fb, e->f_tile_blocks);
-    e->var_grid = split(n_vt, L.vg_base.empty() ? 0 : L.vg_base.back(), L.nv_big, v_big_ents, vb, e->v_tile_blocks);
+    e->factor_grid = grid(L.n_ftiles, L.nf_huge, fb, e->f_tile_blocks);
+    e->var_grid = grid(L.n_vtiles, L.nv_huge, vb, e->v_tile_blocks);
 
     // Per-item arrays are padded to whole groups of 32 so that the tile copies
     // of the last group stay in bounds.
@@ -513,8 +511,12 @@ int flbp_engine_create(const flbp_graph_desc *graph, const flbp_engine_opts *opt
         (rc = dalloc(e, &e->d_fg_base, L.fg_base.size())) || (rc = dalloc(e, &e->d_fb_off, L.fb_off.size())) ||
         (rc = dalloc(e, &e->d_f_kind, nf_pad)) || (rc = dalloc(e, &e->d_f_deg, nf_pad)) ||
         (rc = dalloc(e, &e->d_vg_base, L.vg_base.size())) || (rc = dalloc(e, &e->d_vb_off, L.vb_off.size())) ||
-        (rc = dalloc(e, &e->d_v_ent, L.v_ent.size())) || (rc = dalloc(e, &e->d_ftiles, (size_t)kHdrWords * n_ft)) ||
-        (rc = dalloc(e, &e->d_vtiles, (size_t)kHdrWords * n_vt)) ||
+        (rc = dalloc(e, &e->d_v_ent, L.v_ent.size())) || (rc = dalloc(e, &e->d_ftiles, L.fhdr.size())) ||
+        (rc = dalloc(e, &e->d_vtiles, L.vhdr.size())) || (rc = dalloc(e, &e->d_fb_deg, L.fb_deg.size())) ||
+        (rc = dalloc(e, &e->d_vb_deg, L.vb_deg.size())) || (rc = dalloc(e, &e->d_fbt_deg, L.fbt_deg.size())) ||
+        (rc = dalloc(e, &e->d_vbt_deg, L.vbt_deg.size())) || (rc = dalloc(e, &e->d_fbt_kind, L.fbt_kind.size())) ||
+        (rc = dalloc(e, (char **)&e->d_fbt_pq, L.fbt_pq.size() * e->tsize)) ||
+        (rc = dalloc(e, (char **)&e->d_vbt_prior, L.vbt_deg.size() * psz)) ||
         (rc = dalloc(e, (char **)&e->d_prior, std::max<size_t>(1, nv_pad) * psz)) ||
         (rc = dalloc(e, &e->d_belief, nv_pad)) || (rc = dalloc(e, &e->d_lowpass, (size_t)L.V)) ||
         (rc = dalloc(e, &e->d_ctl, 1)))
@@ -535,36 +537,40 @@ int flbp_engine_create(const flbp_graph_desc *graph, const flbp_engine_opts *opt
             prior[2 * i + 1] = L.prior_cnt[i];
         }
     }
-    // Tile headers (kHdrWords words): first group, group count, group offsets (end repeated).
-    auto headers = [](const std::vector<uint32_t> &tiles, const std::vector<uint32_t> &base) {
-        std::vector<uint32_t> h;
-        for (size_t t = 0; t + 1 < tiles.size(); t++) {
-            const uint32_t g0 = tiles[t], n = tiles[t + 1] - g0;
-            h.push_back(g0);
-            h.push_back(n);
-            for (uint32_t j = 0; j + 2 < (uint32_t)kHdrWords; j++) h.push_back(base[g0 + std::min(j, n)]);
+    // priors of the variables of every big tile, in tile order
+    std::vector<uint32_t> bt_prior(std::max<size_t>(1, L.vbt_deg.size()) * (psz / 4), 0u);
+    for (uint32_t t = 0; t < L.n_vbtiles; t++) {
+        const uint32_t *h = &L.vhdr[(size_t)kHdrWordsHost * t];
+        const uint32_t b0 = h[0], n = h[1] & ~kBigTileFlag;
+        for (uint32_t j = 0; j < n; j++) {
+            const size_t k = (size_t)kTileGroupsHost * t + j, iv = (size_t)L.nv_sell + b0 + j;
+            std::copy(&prior[iv * (psz / 4)], &prior[(iv + 1) * (psz / 4)], &bt_prior[k * (psz / 4)]);
         }
-        return h;
-    };
-    const std::vector<uint32_t> fhdr = headers(L.ftiles, L.fg_base), vhdr = headers(L.vtiles, L.vg_base);
+    }
+    bt_prior.resize(L.vbt_deg.size() * (psz / 4));
     std::vector<uint8_t> kind_pad(nf_pad, 0), deg_pad(nf_pad, 0);
     std::copy(L.f_kind.begin(), L.f_kind.end(), kind_pad.begin());
     std::copy(L.f_deg.begin(), L.f_deg.end(), deg_pad.begin());
     std::vector<double> pq64(2 * nf_pad, 0.0);
     std::copy(L.f_pq.begin(), L.f_pq.end(), pq64.begin());
-    std::vector<float> pq32;
+    std::vector<float> pq32, bpq32;
     if (e->prec == 64) {
-        if ((rc = upload(e, (double *)e->d_f_pq, pq64))) return fail(rc);
+        if ((rc = upload(e, (double *)e->d_f_pq, pq64)) || (rc = upload(e, (double *)e->d_fbt_pq, L.fbt_pq)))
+            return fail(rc);
     } else {
         pq32.assign(pq64.begin(), pq64.end());
-        if ((rc = upload(e, (float *)e->d_f_pq, pq32))) return fail(rc);
+        bpq32.assign(L.fbt_pq.begin(), L.fbt_pq.end());
+        if ((rc = upload(e, (float *)e->d_f_pq, pq32)) || (rc = upload(e, (float *)e->d_fbt_pq, bpq32))) return fail(rc);
     }
     if ((rc = upload(e, e->d_fg_base, L.fg_base)) || (rc = upload(e, e->d_fb_off, L.fb_off)) ||
         (rc = upload(e, e->d_f_pos, L.f_pos)) ||
         (rc = upload(e, e->d_f_kind, kind_pad)) || (rc = upload(e, e->d_f_deg, deg_pad)) ||
         (rc = upload(e, e->d_vg_base, L.vg_base)) || (rc = upload(e, e->d_vb_off, L.vb_off)) ||
         (rc = upload(e, e->d_v_ent, L.v_ent)) || (rc = upload(e, (uint32_t *)e->d_prior, prior)) ||
-        (rc = upload(e, e->d_ftiles, fhdr)) || (rc = upload(e, e->d_vtiles, vhdr)))
+        (rc = upload(e, e->d_ftiles, L.fhdr)) || (rc = upload(e, e->d_vtiles, L.vhdr)) ||
+        (rc = upload(e, e->d_fb_deg, L.fb_deg)) || (rc = upload(e, e->d_vb_deg, L.vb_deg)) ||
+        (rc = upload(e, e->d_fbt_deg, L.fbt_deg)) || (rc = upload(e, e->d_vbt_deg, L.vbt_deg)) ||
+        (rc = upload(e, e->d_fbt_kind, L.fbt_kind)) || (rc = upload(e, (uint32_t *)e->d_vbt_prior, bt_prior)))
         return fail(rc);
     cudaError_t ce = cudaSuccess;
     if ((ce = cudaStreamSynchronize(e->stream)) != cudaSuccess ||
@@ -589,7 +595,8 @@ int flbp_engine_destroy(flbp_engine *e) {
     void *bufs[] = {e->d_vf,     e->d_fv,       e->d_fvd,    e->d_f_pos,     e->d_f_pq,   e->d_fg_base,   e->d_fb_off,     e->d_f_kind,
                     e->d_f_deg,  e->d_vg_base,  e->d_vb_off, e->d_v_ent,     e->d_prior,      e->d_belief,
                     e->d_lowpass, e->d_hist,    e->d_hist_next, e->d_hist_count, e->d_ctl,    e->d_scratch,
-                    e->d_ftiles, e->d_vtiles};
+                    e->d_ftiles, e->d_vtiles,  e->d_fb_deg, e->d_vb_deg, e->d_fbt_deg, e->d_vbt_deg,
+                    e->d_fbt_kind, e->d_fbt_pq, e->d_vbt_prior};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (e->h_ctl) cudaFreeHost(e->h_ctl);
@@ -881,10 +888,12 @@ int flbp_engine_stats(flbp_engine *e, int64_t *c, int64_t n) {
         set_error("null argument");
         return FLBP_ERR_INVALID;
     }
-    const int64_t v[10] = {e->L.V, e->L.F, e->L.E, (int64_t)(e->L.nf_sell + e->L.nf_big),
+    const int64_t v[14] = {e->L.V, e->L.F, e->L.E, (int64_t)(e->L.nf_sell + e->L.nf_big),
                            (int64_t)e->L.n_active_slots, (int64_t)e->L.nf_big, (int64_t)e->L.nv_big,
-                           (int64_t)e->bytes, (int64_t)e->h2d_bytes, (int64_t)e->launches};
-    for (int64_t i = 0; i < n && i < 10; i++) c[i] = v[i];
+                           (int64_t)e->bytes, (int64_t)e->h2d_bytes, (int64_t)e->launches,
+                           (int64_t)e->L.nf_huge, (int64_t)e->L.nv_huge, (int64_t)e->L.n_fbtiles,
+                           (int64_t)e->L.n_vbtiles};
+    for (int64_t i = 0; i < n && i < 14; i++) c[i] = v[i];
     return FLBP_OK;
 }
 

@@ -25,8 +25,12 @@ enum : uint8_t {
 constexpr uint32_t kSellFactorDegree = 16;
 constexpr uint32_t kSellVarDegree = 16;
 constexpr uint32_t kSentinel = 0xffffffffu;  // padding entry in the variable layout
-constexpr uint32_t kTileGroupsHost = 16;     // groups per tile (items = threads of a pass's consumers)
+constexpr uint32_t kTileGroupsHost = 16;     // groups (large items) per tile = consumer warps of a block
 constexpr uint32_t kTileSlotsHost = 2048;    // slot budget of a tile (shared-memory stage size)
+constexpr uint32_t kHdrWordsHost = 32;       // words per tile header
+constexpr uint32_t kBigTileFlag = 0x80000000u;  // header word 1: a tile of large items
+constexpr uint32_t kBigFactorBody = 256;     // body slots of the largest factor evaluated from a tile
+constexpr uint32_t kRunAlign = 4;            // large items' slot / entry runs start on 4-element boundaries
 
 // Host-built device layout.
 //
@@ -56,7 +60,9 @@ struct HostLayout {
 
     uint32_t nf_sell = 0, nf_big = 0;  // active factors per path
     std::vector<uint32_t> fg_base;     // n_fgroups + 1
-    std::vector<uint32_t> fb_off;      // nf_big + 1 (absolute slot ids)
+    std::vector<uint32_t> fb_off;      // nf_big + 1 (absolute slot ids; runs padded to kRunAlign)
+    std::vector<uint32_t> fb_deg;      // per big factor: degree (head included)
+    uint32_t nf_huge = 0;              // big factors [0, nf_huge) are too large for a tile
     std::vector<uint8_t> f_kind;       // per active factor (internal order)
     std::vector<uint8_t> f_deg;        // per sell factor
     std::vector<double> f_pq;          // 2 per active factor: p, q
@@ -64,7 +70,9 @@ struct HostLayout {
 
     uint32_t nv_sell = 0, nv_big = 0;
     std::vector<uint32_t> vg_base;     // n_vgroups + 1 (entry ids)
-    std::vector<uint32_t> vb_off;      // nv_big + 1 (entry ids)
+    std::vector<uint32_t> vb_off;      // nv_big + 1 (entry ids; runs padded to kRunAlign)
+    std::vector<uint32_t> vb_deg;      // per big variable: number of entries
+    uint32_t nv_huge = 0;              // big variables [0, nv_huge) are too large for a tile
     std::vector<uint32_t> v_ent;       // entries incl. padding
     std::vector<uint32_t> f_pos;       // per slot: entry of its f->v message (kSentinel: none)
     std::vector<double> prior_fin;     // per internal variable: finite constant log-odds (damping-scaled)
@@ -91,9 +99,19 @@ struct HostLayout {
     std::vector<int64_t> fm_to_vm;    // reference factor-major slot -> variable-major position
     std::vector<int64_t> vm_var;      // variable-major position -> reference variable
 
-    // Tiles of at most kTileGroupsHost groups and kTileSlotsHost slots (entries):
-    // first group of each tile, n_tiles + 1 entries.
-    std::vector<uint32_t> ftiles, vtiles;
+    // Tiles: kHdrWordsHost-word headers. Word 0: first group (sliced ELL) or
+    // first big item; word 1: item count n, | kBigTileFlag for a tile of big
+    // items; words 2..2+n: slot (entry) offsets of the items and the end; the
+    // remaining words repeat the end offset, except that word 31 of a big
+    // tile holds its ordinal among the big tiles. Big tiles come first.
+    std::vector<uint32_t> fhdr, vhdr;
+    uint32_t n_ftiles = 0, n_vtiles = 0, n_fbtiles = 0, n_vbtiles = 0;
+    // per big tile, kTileGroupsHost entries each: degree, kind, (p, q) of its factors;
+    // number of entries of its variables
+    std::vector<uint32_t> fbt_deg;
+    std::vector<uint8_t> fbt_kind;
+    std::vector<double> fbt_pq;
+    std::vector<uint32_t> vbt_deg;
 
     uint32_t n_fgroups() const { return fg_base.empty() ? 0 : (uint32_t)fg_base.size() - 1; }
     uint32_t n_vgroups() const { return vg_base.empty() ? 0 : (uint32_t)vg_base.size() - 1; }

@@ -190,13 +190,20 @@ struct FactorArgs {
     const uint8_t *f_kind;
     const uint8_t *f_deg;
     const void *f_pq;         // T[2 * nf]
+    const uint32_t *fb_deg;   // per big factor: degree
+    const uint32_t *bt_deg;   // per big tile: kTileGroups degrees
+    const uint8_t *bt_kind;   // per big tile: kTileGroups kinds
+    const void *bt_pq;        // per big tile: kTileGroups (p, q), T
     const uint4 *thdr;        // kHdrWords-word header per tile (see TileHdr)
-    uint32_t nf_sell, nf_big, n_fgroups, n_tiles, n_tile_blocks;
+    uint32_t nf_sell, nf_big, nf_huge, n_fgroups, n_tiles, n_tile_blocks;
 };
 
 struct VarArgs {
     const uint32_t *vg_base;  // sliced-ELL groups (n_vgroups + 1)
     const uint32_t *vb_off;   // big variables (nv_big + 1)
+    const uint32_t *vb_deg;   // per big variable: number of entries
+    const uint32_t *bt_deg;   // per big tile: kTileGroups entry counts
+    const void *bt_prior;     // per big tile: kTileGroups priors (layout of `prior`)
     const uint32_t *v_ent;    // per entry: device slot of the factor side (kSentinel: padding)
     const void *prior;        // per variable: FP32 engines uint2 (float bits of the finite prior,
                               // +inf | -inf << 16 counts); FP64 engines uint4 (double bits, counts, 0)
@@ -205,7 +212,7 @@ struct VarArgs {
     uint32_t *hist_next;      // per variable ring cursor
     uint32_t *hist_count;     // per variable number of stored samples
     const uint4 *thdr;        // kHdrWords-word header per tile (see TileHdr)
-    uint32_t nv_sell, nv_big, n_vgroups, n_tiles, n_tile_blocks;
+    uint32_t nv_sell, nv_big, nv_huge, n_vgroups, n_tiles, n_tile_blocks;
     uint32_t hist_len;
 };
 
@@ -240,6 +247,7 @@ constexpr int kTileItems = 32 * kTileGroups;       // factors / variables per ti
 constexpr int kTileSlots = 2048;                   // slot (entry) budget of a tile
 constexpr int kHdrWords = 32;                      // tile header: 128 bytes
 static_assert(kTileGroups == kConsumerWarps, "one consumer warp per group of a tile");
+static_assert(kHdrWords == (int)kHdrWordsHost && kTileGroups == (int)kTileGroupsHost, "tile format");
 constexpr long long kWaitCycles = 4000000000ll;    // ~2 s at 2 GHz
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -294,9 +302,12 @@ __device__ __forceinline__ bool warp_wait_stage(uint64_t *bar, uint32_t parity) 
     return __all_sync(0xffffffffu, mbar_wait_bounded(bar, parity));
 }
 
-// Per-tile header (kHdrWords words, host-built): [0] first group, [1] number
-// of groups n (1..kTileGroups), [2 + j] slot (entry) offset of group j for
-// j = 0..n, the remaining words repeating the end offset. The producer loads
+// Per-tile header (kHdrWords words, host-built): [0] first group (first big
+// item), [1] number of groups (big items) n in 1..kTileGroups, with
+// kBigTileFlag set for a tile of big items, [2 + j] slot (entry) offset of
+// item j for j = 0..n, the remaining words repeating the end offset, except
+// that word kHdrWords - 1 of a big tile holds its ordinal among the big
+// tiles (the index of its per-tile constants). The producer loads
 // the next tile's header into registers while the current tile's copies are
 // in flight, so that header latency stays off the pipeline's critical path.
 struct TileHdr {
@@ -486,24 +497,23 @@ __device__ __forceinline__ void warp_rscan_pairs(T &P, T &R, int lane) {
     }
 }
 
-// One large factor, one warp, with at most 32 NV body slots: lane l holds
-// slots [l NV, l NV + NV) of the body as (sigma, tau) pairs, so all of its
-// loads are in flight at once. Each slot's leave-one-out pair is
+// One large factor of a staged big tile, one warp, with at most 32 NV body
+// slots: vb[0] / ps[0] are the head's message and fv position, vb[1 + k] /
+// ps[1 + k] those of body slot k. Lane l holds body slots [l NV, l NV + NV)
+// as (sigma, tau) pairs. Each slot's leave-one-out pair is
 //   (lanes before) o (own earlier slots) o (own later slots) o (lanes after),
 // from two shuffle scans over the lanes' pairs; no division, exact zeros
 // stay exact.
 template <typename T, int NV>
-__device__ __forceinline__ void factor_warp_nv(const FactorArgs &a, uint32_t s0, uint32_t nbody, uint8_t kind, T p,
-                                               T q, int lane, const T *__restrict__ vf, T *__restrict__ fv) {
+__device__ __forceinline__ void factor_tile_big(const T *vb, const uint32_t *ps, uint32_t nbody, uint8_t kind, T p, T q,
+                                                int lane, T *__restrict__ fv) {
     const T sgn = (kind & KIND_OR) ? T(-1) : T(1);
     const uint32_t k0 = (uint32_t)lane * NV;  // first body slot of this lane (body index)
     T sg[NV], ta[NV];
-    uint32_t e[NV];
 #pragma unroll
     for (int u = 0; u < NV; u++) {
         const bool in = k0 + u < nbody;
-        const T x = in ? vf[s0 + 1 + k0 + u] : T(0);
-        e[u] = in ? a.f_pos[s0 + 1 + k0 + u] : kSentinel;
+        const T x = in ? vb[1 + k0 + u] : T(0);
         if (in) {
             sig_pair<T>(sgn * x, sg[u], ta[u]);
         } else {
@@ -511,7 +521,7 @@ __device__ __forceinline__ void factor_warp_nv(const FactorArgs &a, uint32_t s0,
             ta[u] = T(0);
         }
     }
-    const T vh = vf[s0];
+    const T vh = vb[0];
     T lP = T(1), lR = T(0);  // this lane's slots
 #pragma unroll
     for (int u = 0; u < NV; u++) {
@@ -529,13 +539,13 @@ __device__ __forceinline__ void factor_warp_nv(const FactorArgs &a, uint32_t s0,
     if ((kind & HEAD_MASK) == HEAD_FREE) {
         auto logP = [&]() {  // rare: whole-body log-sigmoid sum, by the whole warp
             double l = 0.0;
-            for (uint32_t k = lane; k < nbody; k += 32) l += (double)log_sigmoid<T>(sgn * vf[s0 + 1 + k]);
+            for (uint32_t k = lane; k < nbody; k += 32) l += (double)log_sigmoid<T>(sgn * vb[1 + k]);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
             return (T)l;
         };
         const T o = sgn * head_from_pair<T>(P, R, p, q, logP);
-        if (lane == 0) put_fv<T>(fv, a.f_pos[s0], o);
+        if (lane == 0) put_fv<T>(fv, ps[0], o);
     }
     const BodyDen<T> D = body_den<T>(sgn * head_effective<T>(kind, vh), p, q);
     // own later slots, then the lanes after: suffix pairs, backwards
@@ -552,7 +562,7 @@ __device__ __forceinline__ void factor_warp_nv(const FactorArgs &a, uint32_t s0,
 #pragma unroll
     for (int u = 0; u < NV; u++) {
         if (k0 + u < nbody)
-            put_fv<T>(fv, e[u], sgn * body_out_pr<T>(Pp * sP[u], fma(Pp, sR[u], Rp), p, q, D));
+            put_fv<T>(fv, ps[1 + k0 + u], sgn * body_out_pr<T>(Pp * sP[u], fma(Pp, sR[u], Rp), p, q, D));
         Rp = fma(Pp, ta[u], Rp);
         Pp = Pp * sg[u];
     }
@@ -588,30 +598,36 @@ __device__ __noinline__ void factor_warp_loop(const FactorArgs &a, uint32_t s0, 
     }
 }
 
-// Large factor b (internal index nf_sell + b), one warp.
+// Big factor b (internal index nf_sell + b) too large for a tile, one warp.
 template <typename T>
 __device__ __forceinline__ void factor_warp(const FactorArgs &a, uint32_t b, int lane, const T *__restrict__ vf,
                                             T *__restrict__ fv) {
     const uint32_t fi = a.nf_sell + b;
-    const uint32_t s0 = a.fb_off[b], s1 = a.fb_off[b + 1];
-    const uint8_t kind = a.f_kind[fi];
+    const uint32_t s0 = a.fb_off[b], s1 = s0 + a.fb_deg[b];
     const T *pq = reinterpret_cast<const T *>(a.f_pq);
-    const T p = pq[2 * fi], q = pq[2 * fi + 1];
-    const uint32_t nbody = s1 - s0 - 1;
-    if (nbody <= 32) factor_warp_nv<T, 1>(a, s0, nbody, kind, p, q, lane, vf, fv);
-    else if (nbody <= 64) factor_warp_nv<T, 2>(a, s0, nbody, kind, p, q, lane, vf, fv);
-    else if (nbody <= 128) factor_warp_nv<T, 4>(a, s0, nbody, kind, p, q, lane, vf, fv);
-    else factor_warp_loop<T>(a, s0, s1, kind, p, q, lane, vf, fv);
+    factor_warp_loop<T>(a, s0, s1, a.f_kind[fi], pq[2 * fi], pq[2 * fi + 1], lane, vf, fv);
 }
 
-// Factor pass. Blocks [0, n_tile_blocks) run a STAGES-deep pipeline over
-// tiles: warp kConsumerWarps (one lane) is the producer - it waits until the
-// consumer warps have released a stage and bulk-loads the next tile
-// (messages, fv positions, per-factor constants) into it; consumer warp j
-// evaluates group j of the staged tile, one factor per lane, and scatters
-// the outputs to fv. Blocks [n_tile_blocks, grid) take the large factors,
-// one per warp; without such blocks the consumer warps take them first,
-// while the producer's first loads are in flight.
+// Item `wid` of a staged big tile: dispatch on its body size.
+template <typename T>
+__device__ __forceinline__ void factor_tile_item(const T *vb, const uint32_t *ps, uint32_t deg, uint8_t kind, T p, T q,
+                                                 int lane, T *__restrict__ fv) {
+    const uint32_t nbody = deg - 1;
+    if (nbody <= 32) factor_tile_big<T, 1>(vb, ps, nbody, kind, p, q, lane, fv);
+    else if (nbody <= 64) factor_tile_big<T, 2>(vb, ps, nbody, kind, p, q, lane, fv);
+    else if (nbody <= 128) factor_tile_big<T, 4>(vb, ps, nbody, kind, p, q, lane, fv);
+    else factor_tile_big<T, 8>(vb, ps, nbody, kind, p, q, lane, fv);
+}
+static_assert(kBigFactorBody == 256, "factor_tile_item covers bodies of up to 256 slots");
+
+// Factor pass. Every block runs a STAGES-deep pipeline over its tiles (tile
+// blockIdx.x + i gridDim.x): warp kConsumerWarps (one lane) is the producer -
+// it waits until the consumer warps have released a stage and bulk-loads the
+// next tile (messages, fv positions, per-factor constants) into it; consumer
+// warp j evaluates item j of the staged tile - the 32 factors of sliced-ELL
+// group j, one per lane, or big factor j with the whole warp - and scatters
+// the outputs to fv. Factors too large for a tile are taken first, one per
+// warp, while the producer's first loads are in flight.
 template <typename T, int STAGES>
 __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArgs a, const T *__restrict__ vf,
                                                                        T *__restrict__ fv, Ctl *ctl) {
@@ -631,12 +647,6 @@ __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArg
         ctl->arrive = 0u;
     }
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (blockIdx.x >= a.n_tile_blocks) {  // large factors
-        const uint32_t warp = (blockIdx.x - a.n_tile_blocks) * (blockDim.x >> 5) + wid;
-        const uint32_t nwarps = (gridDim.x - a.n_tile_blocks) * (blockDim.x >> 5);
-        for (uint32_t b = warp; b < a.nf_big; b += nwarps) factor_warp<T>(a, b, lane, vf, fv);
-        return;
-    }
     const uint32_t n_tiles = a.n_tiles, nb = a.n_tile_blocks;
     const uint32_t my_tiles = (blockIdx.x < n_tiles) ? (n_tiles - blockIdx.x + nb - 1) / nb : 0;
     if (threadIdx.x == 0) {
@@ -664,17 +674,28 @@ __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArg
             unsigned char *st = smem + (size_t)s * FS::bytes;
             uint32_t *gb = reinterpret_cast<uint32_t *>(st + FS::hdr);
             h.store(gb);
-            const uint32_t g0 = gb[0], n = gb[1];
+            const uint32_t g0 = gb[0], n = gb[1] & ~kBigTileFlag;
             const uint32_t ns = gb[2 + n] - gb[2];
-            const uint32_t items = 32u * n;
-            mbar_arrive_expect_tx(&full[s], ns * (uint32_t)(sizeof(T) + 4) + 2u * items + 2u * items * (uint32_t)sizeof(T));
+            if (gb[1] & kBigTileFlag) {  // big factors: degrees, kinds and (p, q) from the tile's constants
+                const size_t bt = gb[kHdrWords - 1];
+                constexpr uint32_t cbytes = 4u * kTileGroups + kTileGroups + 2u * kTileGroups * (uint32_t)sizeof(T);
+                mbar_arrive_expect_tx(&full[s], ns * (uint32_t)(sizeof(T) + 4) + cbytes);
+                bulk_g2s(st + FS::deg, a.bt_deg + kTileGroups * bt, 4u * kTileGroups, &full[s]);
+                bulk_g2s(st + FS::kind, a.bt_kind + kTileGroups * bt, kTileGroups, &full[s]);
+                bulk_g2s(st + FS::pq, reinterpret_cast<const T *>(a.bt_pq) + 2 * kTileGroups * bt,
+                         2u * kTileGroups * (uint32_t)sizeof(T), &full[s]);
+            } else {
+                const uint32_t items = 32u * n;
+                mbar_arrive_expect_tx(&full[s],
+                                      ns * (uint32_t)(sizeof(T) + 4) + 2u * items + 2u * items * (uint32_t)sizeof(T));
+                bulk_g2s(st + FS::deg, a.f_deg + 32ull * g0, items, &full[s]);
+                bulk_g2s(st + FS::kind, a.f_kind + 32ull * g0, items, &full[s]);
+                bulk_g2s(st + FS::pq, pq_g + 64ull * g0, 2u * items * (uint32_t)sizeof(T), &full[s]);
+            }
             if (ns) {
                 bulk_g2s(st + FS::vbuf, vf + gb[2], ns * (uint32_t)sizeof(T), &full[s]);
                 bulk_g2s(st + FS::pos, a.f_pos + gb[2], ns * 4u, &full[s]);
             }
-            bulk_g2s(st + FS::deg, a.f_deg + 32ull * g0, items, &full[s]);
-            bulk_g2s(st + FS::kind, a.f_kind + 32ull * g0, items, &full[s]);
-            bulk_g2s(st + FS::pq, pq_g + 64ull * g0, 2u * items * (uint32_t)sizeof(T), &full[s]);
             if (it + 1 < my_tiles) h.load(a.thdr + (size_t)(kHdrWords / 4) * (blockIdx.x + (size_t)(it + 1) * nb));
         }
         if (!ok) {
@@ -686,9 +707,9 @@ __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArg
         return;
     }
 
-    if (nb == gridDim.x) {
+    {  // factors too large for a tile first, while the producer's first loads are in flight
         const uint32_t warp = blockIdx.x * kConsumerWarps + wid, nwarps = gridDim.x * kConsumerWarps;
-        for (uint32_t b = warp; b < a.nf_big; b += nwarps) factor_warp<T>(a, b, lane, vf, fv);
+        for (uint32_t b = warp; b < a.nf_huge; b += nwarps) factor_warp<T>(a, b, lane, vf, fv);
     }
     for (uint32_t it = 0; it < my_tiles; it++) {
         const int s = (int)(it % STAGES);
@@ -698,7 +719,16 @@ __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArg
         }
         const unsigned char *st = smem + (size_t)s * FS::bytes;
         const uint32_t *gb = reinterpret_cast<const uint32_t *>(st + FS::hdr);
-        if ((uint32_t)wid < gb[1]) {
+        if (gb[1] & kBigTileFlag) {  // one big factor per warp
+            if ((uint32_t)wid < (gb[1] & ~kBigTileFlag)) {
+                const uint32_t base = gb[2 + wid] - gb[2];
+                const T *pq = reinterpret_cast<const T *>(st + FS::pq);
+                factor_tile_item<T>(reinterpret_cast<const T *>(st + FS::vbuf) + base,
+                                    reinterpret_cast<const uint32_t *>(st + FS::pos) + base,
+                                    reinterpret_cast<const uint32_t *>(st + FS::deg)[wid], st[FS::kind + wid],
+                                    pq[2 * wid], pq[2 * wid + 1], lane, fv);
+            }
+        } else if ((uint32_t)wid < gb[1]) {
             const uint32_t base = gb[2 + wid] - gb[2], f = 32u * wid + lane;
             const int w = (int)((gb[3 + wid] - gb[2 + wid]) >> 5);
             const int deg = st[FS::deg + f];
@@ -789,33 +819,27 @@ __device__ __forceinline__ T take_fv(T x, T old, T d) {
     return DAMP ? damp_mix(x, old, d) : x;
 }
 
-// One large variable, one warp, with at most 32 NV entries held in
-// registers: all loads of a lane are in flight at once.
-template <typename T, int BMODE, bool WRITE_VF, bool DAMP, int NV>
-__device__ __forceinline__ double var_warp_nv(const VarArgs &a, uint32_t v, uint32_t k0, uint32_t n, int lane,
-                                              const T *__restrict__ fv, T *__restrict__ vf, T *__restrict__ fvd,
-                                              T d, double pscale, double tol, unsigned long long &cnt) {
+// One big variable of a staged big tile, one warp: its entries are en[k],
+// x[k] (and xo[k], the previous damped messages), k < deg, in the stage;
+// fvd_run is its run of damped messages in global memory.
+template <typename T, int BMODE, bool WRITE_VF, bool DAMP>
+__device__ __forceinline__ double var_tile_big(const VarArgs &a, uint32_t v, uint32_t deg, const uint32_t *en, T *x,
+                                               const T *xo, T *__restrict__ fvd_run, const void *prior, uint32_t pidx,
+                                               int lane, T *__restrict__ vf, T d, double pscale, double tol,
+                                               unsigned long long &cnt) {
     const T inf = Num<T>::inf();
-    uint32_t e[NV];
-    T x[NV], xo[DAMP ? NV : 1];
-#pragma unroll
-    for (int u = 0; u < NV; u++) {
-        const uint32_t k = lane + 32u * u;
-        e[u] = (k < n) ? a.v_ent[k0 + k] : kSentinel;
-        x[u] = (k < n) ? fv[k0 + k] : T(0);
-        if (DAMP) xo[u] = (k < n) ? fvd[k0 + k] : T(0);
-    }
     double S = 0.0;
     int npos = 0, nneg = 0;
-#pragma unroll
-    for (int u = 0; u < NV; u++) {
+    for (uint32_t k = lane; k < deg; k += 32) {
+        T xv = x[k];
         if (DAMP) {
-            x[u] = take_fv<T, DAMP>(x[u], xo[u], d);
-            if (lane + 32u * u < n) fvd[k0 + lane + 32u * u] = x[u];
+            xv = take_fv<T, DAMP>(xv, xo[k], d);
+            x[k] = xv;
+            fvd_run[k] = xv;
         }
-        if (x[u] == inf) npos++;
-        else if (x[u] == -inf) nneg++;
-        else S += (double)x[u];
+        if (xv == inf) npos++;
+        else if (xv == -inf) nneg++;
+        else S += (double)xv;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -825,16 +849,18 @@ __device__ __forceinline__ double var_warp_nv(const VarArgs &a, uint32_t v, uint
     }
     double S0;
     int p0, n0;
-    decode_prior<T>(a.prior, v, pscale, S0, p0, n0);
+    decode_prior<T>(prior, pidx, pscale, S0, p0, n0);
     S += S0;
     npos += p0;
     nneg += n0;
     if (WRITE_VF) {
-#pragma unroll
-        for (int u = 0; u < NV; u++)
-            if (e[u] != kSentinel) vf[e[u]] = excl_msg<T>(S, npos, nneg, x[u]);
+        for (uint32_t k = lane; k < deg; k += 32) {
+            const uint32_t e = en[k];
+            if (e != kSentinel) vf[e] = excl_msg<T>(S, npos, nneg, x[k]);
+        }
     }
-    return (lane == 0) ? var_finish<BMODE>(a, v, S, npos, nneg, tol, a.belief[v], cnt) : 0.0;
+    return (lane == 0) ? var_finish<BMODE>(a, v, S, npos, nneg, tol, (BMODE == 1 || BMODE == 2) ? a.belief[v] : 0.0, cnt)
+                       : 0.0;
 }
 
 // Larger variables: lanes stride over the entries, reading them twice.
@@ -877,17 +903,14 @@ __device__ __noinline__ double var_warp_loop(const VarArgs &a, uint32_t v, uint3
     return (lane == 0) ? var_finish<BMODE>(a, v, S, npos, nneg, tol, a.belief[v], cnt) : 0.0;
 }
 
-// Large variable b (internal index nv_sell + b), one warp.
+// Big variable b (internal index nv_sell + b) too large for a tile, one warp.
 template <typename T, int BMODE, bool WRITE_VF, bool DAMP>
 __device__ __forceinline__ double var_warp(const VarArgs &a, uint32_t b, int lane, const T *__restrict__ fv,
                                            T *__restrict__ vf, T *__restrict__ fvd, T d, double pscale, double tol,
                                            unsigned long long &cnt) {
-    const uint32_t v = a.nv_sell + b;
-    const uint32_t k0 = a.vb_off[b], k1 = a.vb_off[b + 1], n = k1 - k0;
-    if (n <= 32) return var_warp_nv<T, BMODE, WRITE_VF, DAMP, 1>(a, v, k0, n, lane, fv, vf, fvd, d, pscale, tol, cnt);
-    if (n <= 64) return var_warp_nv<T, BMODE, WRITE_VF, DAMP, 2>(a, v, k0, n, lane, fv, vf, fvd, d, pscale, tol, cnt);
-    if (n <= 128) return var_warp_nv<T, BMODE, WRITE_VF, DAMP, 4>(a, v, k0, n, lane, fv, vf, fvd, d, pscale, tol, cnt);
-    return var_warp_loop<T, BMODE, WRITE_VF, DAMP>(a, v, k0, k1, lane, fv, vf, fvd, d, pscale, tol, cnt);
+    const uint32_t k0 = a.vb_off[b];
+    return var_warp_loop<T, BMODE, WRITE_VF, DAMP>(a, a.nv_sell + b, k0, k0 + a.vb_deg[b], lane, fv, vf, fvd, d, pscale,
+                                                   tol, cnt);
 }
 
 __device__ __forceinline__ double warp_max(double x) {
@@ -949,8 +972,9 @@ static __device__ void stop_rules(Ctl *ctl) {
 // previous damped messages (with damping), priors and (with a residual)
 // previous beliefs; consumer warp j takes group j, one variable per lane:
 // the FP64 sum of its incoming messages with +-inf counts and its prior,
-// belief and residual, then the leave-one-out messages scattered to vf.
-// Blocks [n_tile_blocks, grid) take the large variables. With BMODE 1/2 the
+// belief and residual, then the leave-one-out messages scattered to vf; a
+// big variable of a big tile takes the whole warp. Variables too large for a
+// tile are taken first, one per warp. With BMODE 1/2 the
 // block maxima of |belief change| are combined with an atomic max and the
 // last block to finish applies the stop rules. DAMP mixes each new message
 // with the previous damped one (fvd) and stores the result back to fvd.
@@ -968,8 +992,7 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
     const double tol = ctl->tol;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const uint32_t n_tiles = a.n_tiles, nb = a.n_tile_blocks;
-    const bool tile_block = blockIdx.x < nb;
-    const uint32_t my_tiles = (tile_block && blockIdx.x < n_tiles) ? (n_tiles - blockIdx.x + nb - 1) / nb : 0;
+    const uint32_t my_tiles = (blockIdx.x < n_tiles) ? (n_tiles - blockIdx.x + nb - 1) / nb : 0;
     const T inf = Num<T>::inf();
     double dmax = 0.0;
     unsigned long long cnt = 0;
@@ -981,12 +1004,7 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    if (!tile_block) {  // large variables
-        const uint32_t warp = (blockIdx.x - nb) * (blockDim.x >> 5) + wid;
-        const uint32_t nwarps = (gridDim.x - nb) * (blockDim.x >> 5);
-        for (uint32_t b = warp; b < a.nv_big; b += nwarps)
-            dmax = fmax(dmax, var_warp<T, BMODE, WRITE_VF, DAMP>(a, b, lane, fv, vf, fvd, d, pscale, tol, cnt));
-    } else if (wid == kConsumerWarps) {  // producer warp
+    if (wid == kConsumerWarps) {  // producer warp
         if (lane == 0) {
             TileHdr h;
             if (my_tiles) h.load(a.thdr + (size_t)(kHdrWords / 4) * blockIdx.x);
@@ -1002,26 +1020,34 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
                 unsigned char *st = smem + (size_t)s * VS::bytes;
                 uint32_t *gb = reinterpret_cast<uint32_t *>(st + VS::hdr);
                 h.store(gb);
-                const uint32_t g0 = gb[0], n = gb[1];
+                const uint32_t g0 = gb[0], n = gb[1] & ~kBigTileFlag;
                 const uint32_t ns = gb[2 + n] - gb[2];
-                const uint32_t items = 32u * n;
-                mbar_arrive_expect_tx(&full[s], ns * (4u + (DAMP ? 2u : 1u) * (uint32_t)sizeof(T)) + psz * items +
-                                                    (RESID ? 8u * items : 0u));
+                const uint32_t mbytes = ns * (4u + (DAMP ? 2u : 1u) * (uint32_t)sizeof(T));
+                if (gb[1] & kBigTileFlag) {  // big variables: entry counts and priors from the tile's constants
+                    const size_t bt = gb[kHdrWords - 1];
+                    mbar_arrive_expect_tx(&full[s], mbytes + psz * kTileGroups + 4u * kTileGroups);
+                    bulk_g2s(st + VS::prior, reinterpret_cast<const unsigned char *>(a.bt_prior) + psz * kTileGroups * bt,
+                             psz * kTileGroups, &full[s]);
+                    bulk_g2s(st + VS::bold, a.bt_deg + kTileGroups * bt, 4u * kTileGroups, &full[s]);
+                } else {
+                    const uint32_t items = 32u * n;
+                    mbar_arrive_expect_tx(&full[s], mbytes + psz * items + (RESID ? 8u * items : 0u));
+                    bulk_g2s(st + VS::prior, reinterpret_cast<const unsigned char *>(a.prior) + 32ull * g0 * psz,
+                             psz * items, &full[s]);
+                    if (RESID) bulk_g2s(st + VS::bold, a.belief + 32ull * g0, 8u * items, &full[s]);
+                }
                 if (ns) {
                     bulk_g2s(st + VS::ent, a.v_ent + gb[2], ns * 4u, &full[s]);
                     bulk_g2s(st + VS::x, fv + gb[2], ns * (uint32_t)sizeof(T), &full[s]);
                     if (DAMP) bulk_g2s(st + VS::xo, fvd + gb[2], ns * (uint32_t)sizeof(T), &full[s]);
                 }
-                bulk_g2s(st + VS::prior, reinterpret_cast<const unsigned char *>(a.prior) + 32ull * g0 * psz,
-                         psz * items, &full[s]);
-                if (RESID) bulk_g2s(st + VS::bold, a.belief + 32ull * g0, 8u * items, &full[s]);
                 if (it + 1 < my_tiles) h.load(a.thdr + (size_t)(kHdrWords / 4) * (blockIdx.x + (size_t)(it + 1) * nb));
             }
         }
-    } else {  // consumer warps (large variables first when no blocks are dedicated to them)
-        if (nb == gridDim.x) {
+    } else {  // consumer warps: variables too large for a tile first
+        {
             const uint32_t warp = blockIdx.x * kConsumerWarps + wid, nwarps = gridDim.x * kConsumerWarps;
-            for (uint32_t b = warp; b < a.nv_big; b += nwarps)
+            for (uint32_t b = warp; b < a.nv_huge; b += nwarps)
                 dmax = fmax(dmax, var_warp<T, BMODE, WRITE_VF, DAMP>(a, b, lane, fv, vf, fvd, d, pscale, tol, cnt));
         }
         for (uint32_t it = 0; it < my_tiles; it++) {
@@ -1032,7 +1058,17 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
             }
             unsigned char *st = smem + (size_t)s * VS::bytes;
             const uint32_t *gb = reinterpret_cast<const uint32_t *>(st + VS::hdr);
-            if ((uint32_t)wid < gb[1]) {
+            if (gb[1] & kBigTileFlag) {  // one big variable per warp
+                if ((uint32_t)wid < (gb[1] & ~kBigTileFlag)) {
+                    const uint32_t base = gb[2 + wid] - gb[2];
+                    dmax = fmax(dmax, var_tile_big<T, BMODE, WRITE_VF, DAMP>(
+                                          a, a.nv_sell + gb[0] + wid, reinterpret_cast<const uint32_t *>(st + VS::bold)[wid],
+                                          reinterpret_cast<const uint32_t *>(st + VS::ent) + base,
+                                          reinterpret_cast<T *>(st + VS::x) + base,
+                                          reinterpret_cast<const T *>(st + VS::xo) + base, fvd + gb[2] + base,
+                                          st + VS::prior, wid, lane, vf, d, pscale, tol, cnt));
+                }
+            } else if ((uint32_t)wid < gb[1]) {
                 const uint32_t base = gb[2 + wid] - gb[2];
                 const int w = (int)((gb[3 + wid] - gb[2 + wid]) >> 5);
                 const uint32_t t = 32u * wid + lane, v = 32u * gb[0] + t;

@@ -198,12 +198,15 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err) {
         if (next < UINT32_MAX) {
             L.fg_base[ng] = (uint32_t)next;
             L.fb_off.assign((size_t)nf_big + 1, 0);
+            L.fb_deg.assign(nf_big, 0);
             for (uint32_t b = 0; b < nf_big && next < UINT32_MAX; b++) {
                 const int64_t I = fact_of_int[nf_sell + b];
                 L.fb_off[b] = (uint32_t)next;
+                L.fb_deg[b] = (uint32_t)(off[I + 1] - off[I]);
                 dev_slot[g.factor_head[I]] = (uint32_t)next++;
                 for (int64_t e = off[I]; e < off[I + 1]; e++)
                     if (e != g.factor_head[I]) dev_slot[e] = (uint32_t)next++;
+                next = (next + kRunAlign - 1) & ~(uint64_t)(kRunAlign - 1);  // 16-byte aligned runs
             }
         }
         if (next >= UINT32_MAX) {
@@ -280,17 +283,19 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err) {
             nent += 32ull * w;
         }
         uint64_t nbig = 0;
-        for (uint32_t iv = nv_sell; iv < (uint32_t)V; iv++) nbig += vdeg[order[iv]];
+        for (uint32_t iv = nv_sell; iv < (uint32_t)V; iv++) nbig += (vdeg[order[iv]] + kRunAlign - 1) & ~(kRunAlign - 1);
         if (nent + nbig >= UINT32_MAX) {
             err = "graph exceeds 2^32-1 variable entries";
             return FLBP_ERR_LIMIT;
         }
         L.vg_base[ng] = (uint32_t)nent;
         L.vb_off.assign((size_t)L.nv_big + 1, 0);
+        L.vb_deg.assign(L.nv_big, 0);
         uint64_t pos = nent;
         for (uint32_t b = 0; b < L.nv_big; b++) {
             L.vb_off[b] = (uint32_t)pos;
-            pos += vdeg[order[nv_sell + b]];
+            L.vb_deg[b] = vdeg[order[nv_sell + b]];
+            pos = (pos + L.vb_deg[b] + kRunAlign - 1) & ~(uint64_t)(kRunAlign - 1);  // 16-byte aligned runs
         }
         L.vb_off[L.nv_big] = (uint32_t)pos;
         // first entry position and stride of every variable
@@ -305,7 +310,7 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err) {
                 estride[v] = 1;
             }
         }
-        L.v_ent.assign(nent + nbig, kSentinel);
+        L.v_ent.assign(pos, kSentinel);
         L.f_pos.assign(L.n_slots, kSentinel);  // slot -> entry receiving its f->v message
         for (uint64_t sl = 0; sl < L.n_slots; sl++) {
             const uint32_t v = var_of_dev[sl];
@@ -317,24 +322,77 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err) {
         }
     }
 
-    // --- tiles: up to kTileGroupsHost groups within kTileSlotsHost slots ----------------
-    auto make_tiles = [](const std::vector<uint32_t> &base, std::vector<uint32_t> &tiles) {
-        tiles.clear();
+    // --- tiles and their headers ------------------------------------------------------
+    // Large items that fit a tile come first (a warp per item, staged like the
+    // sliced-ELL groups); the sliced-ELL tiles follow. Items too large for a
+    // tile (the first ones, by decreasing degree) are left to the warp path.
+    L.nf_huge = 0;
+    while (L.nf_huge < L.nf_big && L.fb_deg[L.nf_huge] - 1 > kBigFactorBody) L.nf_huge++;
+    L.nv_huge = 0;
+    while (L.nv_huge < L.nv_big && L.vb_deg[L.nv_huge] > kTileSlotsHost) L.nv_huge++;
+    auto push_hdr = [](std::vector<uint32_t> &h, uint32_t first, uint32_t nflag, const uint32_t *offs, uint32_t n,
+                       uint32_t ordinal) {
+        const size_t at = h.size();
+        h.push_back(first);
+        h.push_back(nflag);
+        for (uint32_t j = 0; j + 2 < kHdrWordsHost; j++) h.push_back(offs[std::min(j, n)]);
+        if (nflag & kBigTileFlag) h[at + kHdrWordsHost - 1] = ordinal;
+    };
+    auto big_tiles = [&](const std::vector<uint32_t> &boff, const std::vector<uint32_t> &bdeg, uint32_t b0,
+                         uint32_t nb, std::vector<uint32_t> &hdr, std::vector<uint32_t> &firsts) -> uint32_t {
+        uint32_t nt = 0, b = b0;
+        while (b < nb) {
+            const uint32_t start = b;
+            do b++;  // every item fits a tile by itself (larger ones are left to the warp path)
+            while (b < nb && b - start < kTileGroupsHost && boff[b + 1] - boff[start] <= kTileSlotsHost);
+            push_hdr(hdr, start, (b - start) | kBigTileFlag, &boff[start], b - start, nt);
+            firsts.push_back(start);
+            nt++;
+        }
+        (void)bdeg;
+        return nt;
+    };
+    auto sell_tiles = [&](const std::vector<uint32_t> &base, std::vector<uint32_t> &hdr) -> uint32_t {
         const uint32_t ng = base.empty() ? 0 : (uint32_t)base.size() - 1;
-        uint32_t g = 0;
-        tiles.push_back(0);
+        uint32_t g = 0, nt = 0;
         while (g < ng) {
-            uint32_t n = 0, slots = 0;
-            while (g < ng && n < kTileGroupsHost && slots + (base[g + 1] - base[g]) <= kTileSlotsHost) {
+            const uint32_t g0 = g;
+            uint32_t slots = 0;
+            while (g < ng && g - g0 < kTileGroupsHost && slots + (base[g + 1] - base[g]) <= kTileSlotsHost) {
                 slots += base[g + 1] - base[g];
-                n++;
                 g++;
             }
-            tiles.push_back(g);
+            push_hdr(hdr, g0, g - g0, &base[g0], g - g0, 0);
+            nt++;
         }
+        return nt;
     };
-    make_tiles(L.fg_base, L.ftiles);
-    make_tiles(L.vg_base, L.vtiles);
+    L.fhdr.clear();
+    L.vhdr.clear();
+    std::vector<uint32_t> fbt_first, vbt_first;
+    L.n_fbtiles = big_tiles(L.fb_off, L.fb_deg, L.nf_huge, L.nf_big, L.fhdr, fbt_first);
+    L.n_ftiles = L.n_fbtiles + sell_tiles(L.fg_base, L.fhdr);
+    L.n_vbtiles = big_tiles(L.vb_off, L.vb_deg, L.nv_huge, L.nv_big, L.vhdr, vbt_first);
+    L.n_vtiles = L.n_vbtiles + sell_tiles(L.vg_base, L.vhdr);
+    // per large tile constants: degrees and kinds (factor side), degrees (variable side)
+    L.fbt_deg.assign((size_t)kTileGroupsHost * L.n_fbtiles, 0);
+    L.fbt_kind.assign((size_t)kTileGroupsHost * L.n_fbtiles, 0);
+    L.fbt_pq.assign((size_t)2 * kTileGroupsHost * L.n_fbtiles, 0.0);
+    for (uint32_t t = 0; t < L.n_fbtiles; t++) {
+        const uint32_t b0 = fbt_first[t], n = L.fhdr[(size_t)kHdrWordsHost * t + 1] & ~kBigTileFlag;
+        for (uint32_t j = 0; j < n; j++) {
+            const size_t k = (size_t)kTileGroupsHost * t + j, fi = (size_t)nf_sell + b0 + j;
+            L.fbt_deg[k] = L.fb_deg[b0 + j];
+            L.fbt_kind[k] = L.f_kind[fi];
+            L.fbt_pq[2 * k] = L.f_pq[2 * fi];
+            L.fbt_pq[2 * k + 1] = L.f_pq[2 * fi + 1];
+        }
+    }
+    L.vbt_deg.assign((size_t)kTileGroupsHost * L.n_vbtiles, 0);
+    for (uint32_t t = 0; t < L.n_vbtiles; t++) {
+        const uint32_t b0 = vbt_first[t], n = L.vhdr[(size_t)kHdrWordsHost * t + 1] & ~kBigTileFlag;
+        for (uint32_t j = 0; j < n; j++) L.vbt_deg[(size_t)kTileGroupsHost * t + j] = L.vb_deg[b0 + j];
+    }
 
     // --- priors ------------------------------------------------------------------
     L.prior_fin.assign(V, 0.0);

@@ -139,10 +139,12 @@ int flbp_get_fv_messages(flbp_engine *eng, double *m0, double *m1, int64_t n_slo
  * variable's message all the same). */
 int flbp_get_vf_messages(flbp_engine *eng, double *m0, double *m1, int64_t n_slots);
 
-/* Layout statistics: counts[0..9] = vars, factors, slots, active factors,
+/* Layout statistics: counts[0..13] = vars, factors, slots, active factors,
  * active slots, factors handled warp-wide, variables handled warp-wide,
  * bytes of device memory held, host->device bytes copied by create, engine
- * kernels launched so far. */
+ * kernels launched so far, warp-wide factors too large for a tile, likewise
+ * variables, tiles of warp-wide factors, tiles of warp-wide variables.
+ * Entries past n_counts are not written. */
 int flbp_engine_stats(flbp_engine *eng, int64_t *counts, int64_t n_counts);
 
 /* Per-pass timing mode (for measurement): while enabled, sweeps are launched

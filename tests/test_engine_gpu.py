@@ -161,3 +161,63 @@ def test_repeat_runs_continue_iteration_count():
     info = eng.run_tol(1e-6, 1000, 100.0)
     assert info["total_sweeps"] == bp.iters
     assert np.max(np.abs(eng.beliefs() - bp.beliefs())) <= 1e-9
+
+
+def _large_item_graph(seed):
+    """Factors of every large-item size class (bodies of 17 to 1000 slots, on
+    both sides of the 32/64/128/256 register splits and of the tile limit)
+    and variables with more entries than a tile holds."""
+    rng = np.random.default_rng(seed)
+    n_in = 1200
+    kind, head, off, body, p, q = [], [], [0], [], [], []
+
+    def add(k, h, b, pp, qq):
+        kind.append(k)
+        head.append(h)
+        body.extend(int(x) for x in b)
+        off.append(len(body))
+        p.append(pp)
+        q.append(qq)
+
+    for v in range(n_in):  # input priors
+        add(workloads.SINGLETON, v, [], float(rng.uniform(0.05, 0.95)), 0.0)
+    nxt = n_in
+    for size in (17, 20, 33, 40, 64, 65, 100, 128, 129, 200, 255, 256, 257, 300, 1000):
+        for k in (workloads.AND, workloads.OR):
+            b = rng.choice(n_in, size=size, replace=False)
+            qq = 0.0 if rng.random() < 0.5 else float(rng.uniform(0.0, 0.1))
+            add(k, nxt, b, float(rng.uniform(0.6, 0.99)), qq)
+            nxt += 1
+    hub = nxt  # a variable in the bodies of 2100 rules: more entries than a tile holds
+    add(workloads.SINGLETON, hub, [], 0.7, 0.0)
+    nxt += 1
+    for i in range(2100):
+        add(workloads.AND, nxt, [hub, int(rng.integers(n_in))], float(rng.uniform(0.6, 0.99)), 0.0)
+        nxt += 1
+    mid = nxt  # and one with a few hundred entries (a big-tile variable)
+    add(workloads.SINGLETON, mid, [], 0.4, 0.0)
+    nxt += 1
+    for i in range(300):
+        add(workloads.OR, nxt, [mid, int(rng.integers(n_in)), int(rng.integers(n_in))], 1.0, 0.0)
+        nxt += 1
+    k, h, o, b, pp, qq = workloads._append_auto_singletons(
+        np.array(kind, np.int32), np.array(head, np.int64), np.array(off, np.int64), np.array(body, np.int64),
+        workloads._quant(np.array(p)), workloads._quant(np.array(q)))
+    return workloads.FactorList(k, h, o, b, pp, qq)
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+@pytest.mark.parametrize("damping", [0.0, 0.15])
+def test_large_items(prec, damping):
+    fl = _large_item_graph(11)
+    clamps = {1200 + 3: 1, 1200 + 7: 0, 5: 1}  # clamp two big factors' heads and one input
+    g, og = _pair(fl, clamps)
+    eng = Engine.from_graph(g, precision=prec, damping=damping)
+    st = eng.stats()
+    assert st["huge_factors"] > 0 and st["huge_vars"] > 0 and st["big_factor_tiles"] > 0 and st["big_var_tiles"] > 0
+    bp = O.OracleBP(og, damping=damping)
+    bp.init()
+    bp.run_fixed(1e-6, 40, 1)
+    eng.init()
+    eng.run_fixed(40)
+    assert np.max(np.abs(eng.beliefs() - bp.beliefs())) <= TOL[prec]

@@ -1,0 +1,72 @@
+"""FastLBP's own example drivers as drop-in clients of this library.
+
+The CPU test compiles examples/fl_wrapper.cu, bingo_wrapper.cu, example_ext.cu
+and example_ext_clamp.cu from the FastLBP sources, unchanged, against this
+repository's include/ and links them to libfastlbp_b200.so (bingo_wrapper
+also to NVML, as FastLBP's own build does). It needs the FastLBP sources and
+is skipped without them.
+
+The GPU test runs fl_wrapper built that way (oracle/_ref/examples, made by
+`make -C oracle examples`) on a golden case whose beliefs FastLBP's own code
+produced - the same graph, clamps and fixed 500 PARALL sweeps - and checks the
+printed beliefs within the FP32 tolerance (1e-5 absolute).
+"""
+
+import concurrent.futures as cf
+import gzip
+import json
+import os
+import shutil
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_EXAMPLES = os.path.join(os.environ.get("FASTLBP_REF", "/root/reference"), "examples")
+EXAMPLES = ["fl_wrapper", "bingo_wrapper", "example_ext", "example_ext_clamp"]
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_EXAMPLES) or shutil.which("nvcc") is None,
+                    reason="FastLBP example sources or nvcc not available")
+def test_reference_examples_compile_unchanged(tmp_path):
+    lib = os.path.join(ROOT, "fastlbp_b200", "libfastlbp_b200.so")
+    assert os.path.exists(lib)
+
+    def compile_one(name):
+        cmd = ["nvcc", "-std=c++17", "-O0", "-w", "-gencode", "arch=compute_100a,code=sm_100a",
+               "-I" + os.path.join(ROOT, "include"), os.path.join(REF_EXAMPLES, name + ".cu"),
+               "-L" + os.path.dirname(lib), "-lfastlbp_b200", "-L/usr/local/cuda/lib64/stubs", "-lnvidia-ml",
+               "-o", str(tmp_path / name)]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        return name, r.returncode, r.stderr[-2000:]
+
+    with cf.ThreadPoolExecutor(4) as ex:
+        for name, rc, err in ex.map(compile_one, EXAMPLES):
+            assert rc == 0, (name, err)
+            assert os.path.exists(tmp_path / name)
+
+
+@pytest.mark.gpu
+def test_fl_wrapper_reproduces_reference_beliefs(tmp_path):
+    exe = os.path.join(ROOT, "oracle", "_ref", "examples", "fl_wrapper")
+    if not os.path.exists(exe):
+        pytest.skip("oracle/_ref/examples/fl_wrapper not built (needs the FastLBP sources at build time)")
+    name = "cfg0_s0_clamped_fixed500"
+    rec = json.load(open(os.path.join(GOLDEN, name + ".json")))
+    assert rec["mode"][0] == "fixed" and int(rec["mode"][1]) == 500  # fl_wrapper's own schedule
+    graph = tmp_path / "g.causal_fg"
+    with gzip.open(os.path.join(GOLDEN, name + ".causal_fg.gz"), "rt") as f:
+        graph.write_text(f.read())
+    obs = tmp_path / "obs.txt"
+    obs.write_text("".join("%s %s\n" % (k, "true" if int(v) else "false") for k, v in rec["clamps"].items()))
+    r = subprocess.run([exe, str(graph), str(obs)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = {}
+    for line in r.stdout.splitlines():
+        k, v = line.split()
+        got[int(k)] = float(v)
+    want = {int(k): float(v) for k, v in rec["beliefs"].items()}
+    assert set(want) <= set(got)
+    err = max(abs(got[k] - want[k]) for k in want)
+    assert err <= 1e-5, err

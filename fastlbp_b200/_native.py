@@ -104,6 +104,9 @@ def lib():
         "flbp_fg_construct": [_vp, _i64p, _i64p, _i64p, _i64p, _i64p],
         "flbp_engine_create_from_fg": [_vp, P(EngineOpts), P(_vp)],
         "flbp_run_fixed_device_noalloc": [P(DeviceGraph), C.c_int64, C.c_double, _vp, _vp],
+        "flbp_batch_create": [P(GraphDesc), C.c_int64, P(EngineOpts), P(_vp)],
+        "flbp_batch_info": [_vp, P(C.c_int64), _i64p],
+        "flbp_batch_run_tol": [_vp, C.c_double, C.c_int64, C.c_double, _i64p, _i32p, P(RunInfo)],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -128,4 +131,5 @@ EXPORTED = ["flbp_last_error", "flbp_version", "flbp_engine_create", "flbp_engin
             "flbp_engine_stats", "flbp_last_run_ms", "flbp_set_kernel_timing", "flbp_kernel_times", "flbp_fg_read_file", "flbp_fg_read_string",
             "flbp_fg_from_factors", "flbp_fg_destroy", "flbp_fg_clamp", "flbp_fg_rebuild", "flbp_fg_sizes",
             "flbp_fg_var_labels", "flbp_fg_factors", "flbp_fg_neighbors", "flbp_fg_construct",
-            "flbp_engine_create_from_fg", "flbp_run_fixed_device_noalloc"]
+            "flbp_engine_create_from_fg", "flbp_run_fixed_device_noalloc", "flbp_batch_create", "flbp_batch_info",
+            "flbp_batch_run_tol"]

@@ -287,6 +287,43 @@ class Engine:
         return v.value
 
 
+class BatchEngine(Engine):
+    """Many independent graphs in one engine (flbp_batch_*): one sweep is one
+    pass over all of them; each graph stops on its own tolerance rule and is
+    frozen from then on. beliefs() covers all graphs in order;
+    beliefs_of(g) is graph g's part."""
+
+    def __init__(self, graphs: Sequence[Dict[str, np.ndarray]], precision: int = 32, damping: float = 0.0,
+                 stream: Optional[int] = None, device: int = -1):
+        keep = []
+        descs = (N.GraphDesc * len(graphs))()
+        for i, a in enumerate(graphs):
+            descs[i] = _desc_from_arrays(a, keep)
+        opts = N.EngineOpts(int(precision), int(device), float(damping), stream)
+        h = C.c_void_p()
+        check(lib().flbp_batch_create(descs, len(graphs), C.byref(opts), C.byref(h)))
+        self._h = h
+        self.n_graphs = len(graphs)
+        self.var_off = np.zeros(self.n_graphs + 1, np.int64)
+        ng = C.c_int64()
+        check(lib().flbp_batch_info(h, C.byref(ng), self.var_off))
+        self.n_vars = int(self.var_off[-1])
+        self.n_slots = int(sum(int(d.n_slots) for d in descs))
+        self.info = None
+
+    def run_batch_tol(self, tol=1e-6, maxiter=500, maxtime=1e9):
+        """Per-graph sweeps and stop reasons (0 converged, 2 iteration/time limit)."""
+        sweeps = np.zeros(self.n_graphs, np.int64)
+        reasons = np.zeros(self.n_graphs, np.int32)
+        check(lib().flbp_batch_run_tol(self._h, float(tol), int(maxiter), float(maxtime), sweeps, reasons,
+                                       self._info()))
+        return sweeps, reasons
+
+    def beliefs_of(self, g: int, all_beliefs: Optional[np.ndarray] = None) -> np.ndarray:
+        b = self.beliefs() if all_beliefs is None else all_beliefs
+        return b[self.var_off[g]:self.var_off[g + 1]]
+
+
 class CausalBP:
     """CausalBP(fg, opts) with the reference's run semantics (include/ext/causal_bp.h:167-193)."""
 

@@ -58,6 +58,11 @@ struct flbp_engine {
     void *d_fbt_pq = nullptr;                             // per big tile: (p, q) of its factors
     void *d_vbt_prior = nullptr;                          // per big tile: priors of its variables
     uint32_t f_tile_blocks = 0, v_tile_blocks = 0;
+    // Batched solves: the engine holds the disjoint union of n_graphs graphs.
+    uint32_t n_graphs = 0;
+    std::vector<int64_t> graph_var_off;  // n_graphs + 1: variable ranges in the union's order
+    uint32_t *d_f_graph = nullptr, *d_v_graph = nullptr;  // internal factor / variable -> graph
+    int *d_gstate = nullptr;  // [4][n_graphs]: stopped, moved, sweeps, stop reason
     uint8_t *d_f_kind = nullptr, *d_f_deg = nullptr;
     void *d_prior = nullptr;
     double *d_belief = nullptr, *d_lowpass = nullptr, *d_hist = nullptr;
@@ -110,6 +115,8 @@ FactorArgs factor_args(flbp_engine *e) {
     a.thdr = reinterpret_cast<const uint4 *>(e->d_ftiles);
     a.n_tiles = e->L.n_ftiles;
     a.n_tile_blocks = e->f_tile_blocks;
+    a.f_graph = nullptr;
+    a.gdone = nullptr;
     return a;
 }
 
@@ -134,6 +141,9 @@ VarArgs var_args(flbp_engine *e) {
     a.n_tiles = e->L.n_vtiles;
     a.n_tile_blocks = e->v_tile_blocks;
     a.hist_len = e->hist_cap;
+    a.v_graph = nullptr;
+    a.gstate = nullptr;
+    a.n_graphs = 0;
     return a;
 }
 
@@ -171,6 +181,8 @@ cudaError_t configure_kernels(bool damp, int *fb, int *vb) {
     set((const void *)var_pass_kernel<T, 0, true, true, kStages>, var_smem<T, true>());
     set((const void *)var_pass_kernel<T, 1, true, true, kStages>, var_smem<T, true>());
     set((const void *)var_pass_kernel<T, 2, true, true, kStages>, var_smem<T, true>());
+    set((const void *)var_pass_kernel<T, 4, true, false, kStages>, var_smem<T, false>());
+    set((const void *)var_pass_kernel<T, 4, true, true, kStages>, var_smem<T, true>());
     set((const void *)var_pass_kernel<T, 3, false, false, kStages>, var_smem<T, false>());
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(fb, factor_pass_kernel<T, kStages>, kBlockThreads, factor_smem<T>());
     if (damp)
@@ -192,20 +204,31 @@ template <typename T, bool DAMP>
 void launch_var_mode(flbp_engine *e, const VarArgs &va, int mode) {
     if (mode == 0) launch_var<T, 0, DAMP>(e, va);
     else if (mode == 1) launch_var<T, 1, DAMP>(e, va);
-    else launch_var<T, 2, DAMP>(e, va);
+    else if (mode == 2) launch_var<T, 2, DAMP>(e, va);
+    else launch_var<T, 4, DAMP>(e, va);
 }
 
-// mode 0: bare sweep; 1: tolerance loop sweep; 2: low-pass loop sweep.
+// mode 0: bare sweep; 1: tolerance loop sweep; 2: low-pass loop sweep;
+// 3: batched tolerance sweep (stopped graphs frozen, per-graph stop rules).
 // which: bit 0 launches the factor pass, bit 1 the variable pass.
 template <typename T>
 void launch_sweep(flbp_engine *e, int mode, int which = 3) {
     if (which & 1) {
-        const FactorArgs fa = factor_args<T>(e);
+        FactorArgs fa = factor_args<T>(e);
+        if (mode == 3) {
+            fa.f_graph = e->d_f_graph;
+            fa.gdone = e->d_gstate;
+        }
         factor_pass_kernel<T, kStages><<<e->factor_grid, kBlockThreads, factor_smem<T>(), e->stream>>>(
             fa, (const T *)e->d_vf, (T *)e->d_fv, e->d_ctl);
     }
     if (!(which & 2)) return;
-    const VarArgs va = var_args(e);
+    VarArgs va = var_args(e);
+    if (mode == 3) {
+        va.v_graph = e->d_v_graph;
+        va.gstate = e->d_gstate;
+        va.n_graphs = e->n_graphs;
+    }
     if (e->damping != 0.0) launch_var_mode<T, true>(e, va, mode);
     else launch_var_mode<T, false>(e, va, mode);
 }
@@ -406,7 +429,30 @@ const char *flbp_last_error(void) { return g_last_error.c_str(); }
 
 const char *flbp_version(void) { return "fastlbp_b200 0.1 (sm_100a)"; }
 
-int flbp_engine_create(const flbp_graph_desc *graph, const flbp_engine_opts *opts, flbp_engine **out) {
+}  // extern "C"
+
+namespace {
+
+// Graph of every reference factor and variable of a batched engine (the
+// concatenation order of its graphs); null for a single graph.
+struct BatchSpec {
+    std::vector<uint32_t> factor_graph, var_graph;
+    std::vector<int64_t> var_off;
+};
+
+int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, flbp_engine **out,
+                  const BatchSpec *batch);
+
+}  // namespace
+
+extern "C" int flbp_engine_create(const flbp_graph_desc *graph, const flbp_engine_opts *opts, flbp_engine **out) {
+    return create_engine(graph, opts, out, nullptr);
+}
+
+namespace {
+
+int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, flbp_engine **out,
+                  const BatchSpec *batch) {
     if (!graph || !out) {
         set_error("null argument");
         return FLBP_ERR_INVALID;
@@ -582,9 +628,26 @@ int flbp_engine_create(const flbp_graph_desc *graph, const flbp_engine_opts *opt
         set_error(std::string("device initialisation failed: ") + cudaGetErrorString(ce));
         return fail(FLBP_ERR_CUDA);
     }
+    if (batch) {  // graph ids in the kernels' orders, padded like the per-item arrays
+        e->n_graphs = (uint32_t)(batch->var_off.size() - 1);
+        e->graph_var_off = batch->var_off;
+        std::vector<uint32_t> fg(nf_pad, 0), vg(std::max<size_t>(1, nv_pad), 0);
+        for (uint32_t f = 0; f < nf; f++) fg[f] = batch->factor_graph[L.factor_of_internal[f]];
+        for (uint32_t iv = 0; iv < (uint32_t)L.V; iv++) vg[iv] = batch->var_graph[L.var_of_internal[iv]];
+        if ((rc = dalloc(e, &e->d_f_graph, fg.size())) || (rc = dalloc(e, &e->d_v_graph, vg.size())) ||
+            (rc = dalloc(e, &e->d_gstate, 4 * (size_t)e->n_graphs)) || (rc = upload(e, e->d_f_graph, fg)) ||
+            (rc = upload(e, e->d_v_graph, vg)))
+            return fail(rc);
+        FLBP_CUDA(cudaMemsetAsync(e->d_gstate, 0, 4 * sizeof(int) * std::max<size_t>(1, e->n_graphs), e->stream));
+        FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    }
     *out = e;
     return FLBP_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 int flbp_engine_destroy(flbp_engine *e) {
     if (!e) return FLBP_OK;
@@ -596,7 +659,7 @@ int flbp_engine_destroy(flbp_engine *e) {
                     e->d_f_deg,  e->d_vg_base,  e->d_vb_off, e->d_v_ent,     e->d_prior,      e->d_belief,
                     e->d_lowpass, e->d_hist,    e->d_hist_next, e->d_hist_count, e->d_ctl,    e->d_scratch,
                     e->d_ftiles, e->d_vtiles,  e->d_fb_deg, e->d_vb_deg, e->d_fbt_deg, e->d_vbt_deg,
-                    e->d_fbt_kind, e->d_fbt_pq, e->d_vbt_prior};
+                    e->d_fbt_kind, e->d_fbt_pq, e->d_vbt_prior, e->d_f_graph, e->d_v_graph, e->d_gstate};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (e->h_ctl) cudaFreeHost(e->h_ctl);
@@ -926,6 +989,127 @@ int flbp_last_run_ms(flbp_engine *e, double *ms) {
         return FLBP_ERR_INVALID;
     }
     *ms = e->last_ms;
+    return FLBP_OK;
+}
+
+// ------------------------------------------------------------------ batched solves
+
+int flbp_batch_create(const flbp_graph_desc *graphs, int64_t n_graphs, const flbp_engine_opts *opts,
+                      flbp_engine **out) {
+    if (!graphs || !out || n_graphs <= 0) {
+        set_error("batch needs at least one graph");
+        return FLBP_ERR_INVALID;
+    }
+    *out = nullptr;
+    int64_t V = 0, F = 0, E = 0;
+    for (int64_t g = 0; g < n_graphs; g++) {
+        const flbp_graph_desc &d = graphs[g];
+        if (d.n_vars < 0 || d.n_factors < 0 || d.n_slots < 0 || (d.n_factors > 0 && !d.factor_offsets)) {
+            set_error("graph " + std::to_string(g) + " of the batch is malformed");
+            return FLBP_ERR_INVALID;
+        }
+        if (d.n_factors > 0 && (d.factor_offsets[0] != 0 || d.factor_offsets[d.n_factors] != d.n_slots)) {
+            set_error("graph " + std::to_string(g) + ": factor_offsets must start at 0 and end at n_slots");
+            return FLBP_ERR_INVALID;
+        }
+        if ((d.n_factors > 0 || d.n_slots > 0) &&
+            (!d.slot_var || !d.factor_head || !d.factor_type || !d.factor_p || !d.factor_q)) {
+            set_error("graph " + std::to_string(g) + " of the batch lacks an array");
+            return FLBP_ERR_INVALID;
+        }
+        V += d.n_vars;
+        F += d.n_factors;
+        E += d.n_slots;
+    }
+    if (V >= (int64_t)UINT32_MAX || E >= (int64_t)UINT32_MAX || n_graphs >= (int64_t)INT32_MAX) {
+        set_error("batch exceeds 2^32-1 variables or edge slots");
+        return FLBP_ERR_LIMIT;
+    }
+    // the disjoint union, graphs in order
+    std::vector<int64_t> off(F + 1, 0), sv(E), head(F);
+    std::vector<int32_t> type(F), clamped(F, 0);
+    std::vector<double> p(F), q(F), m0(F, 1.0), m1(F, 1.0);
+    BatchSpec spec;
+    spec.factor_graph.resize(F);
+    spec.var_graph.resize(V);
+    spec.var_off.assign(n_graphs + 1, 0);
+    int64_t vo = 0, fo = 0, so = 0;
+    for (int64_t g = 0; g < n_graphs; g++) {
+        const flbp_graph_desc &d = graphs[g];
+        for (int64_t I = 0; I < d.n_factors; I++) {
+            off[fo + I + 1] = so + d.factor_offsets[I + 1];
+            head[fo + I] = so + d.factor_head[I];
+            type[fo + I] = d.factor_type[I];
+            p[fo + I] = d.factor_p[I];
+            q[fo + I] = d.factor_q[I];
+            if (d.factor_head_clamped) clamped[fo + I] = d.factor_head_clamped[I];
+            if (d.factor_mask0) m0[fo + I] = d.factor_mask0[I];
+            if (d.factor_mask1) m1[fo + I] = d.factor_mask1[I];
+            spec.factor_graph[fo + I] = (uint32_t)g;
+        }
+        for (int64_t e = 0; e < d.n_slots; e++) {
+            if (d.slot_var[e] < 0 || d.slot_var[e] >= d.n_vars) {
+                set_error("graph " + std::to_string(g) + ": slot_var out of range at slot " + std::to_string(e));
+                return FLBP_ERR_INVALID;
+            }
+            sv[so + e] = vo + d.slot_var[e];
+        }
+        for (int64_t i = 0; i < d.n_vars; i++) spec.var_graph[vo + i] = (uint32_t)g;
+        vo += d.n_vars;
+        fo += d.n_factors;
+        so += d.n_slots;
+        spec.var_off[g + 1] = vo;
+    }
+    flbp_graph_desc u{V, F, E, off.data(), sv.data(), head.data(), type.data(), p.data(), q.data(),
+                      clamped.data(), m0.data(), m1.data()};
+    return create_engine(&u, opts, out, &spec);
+}
+
+int flbp_batch_info(flbp_engine *e, int64_t *n_graphs, int64_t *var_off) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    if (n_graphs) *n_graphs = e->n_graphs;
+    if (var_off)
+        for (size_t g = 0; g < e->graph_var_off.size(); g++) var_off[g] = e->graph_var_off[g];
+    return FLBP_OK;
+}
+
+int flbp_batch_run_tol(flbp_engine *e, double tol, int64_t maxiter, double maxtime, int64_t *sweeps, int32_t *reasons,
+                       flbp_run_info *info) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    if (e->n_graphs == 0) {
+        set_error("not a batched engine (create it with flbp_batch_create)");
+        return FLBP_ERR_INVALID;
+    }
+    const uint32_t G = e->n_graphs;
+    const long long l0 = e->launches;
+    FLBP_CUDA(cudaMemsetAsync(e->d_gstate, 0, 4 * sizeof(int) * G, e->stream));
+    reset_ctl_for_run(e, 3);
+    Ctl &c = *e->h_ctl;
+    c.iters0 = 0;  // every graph's sweep count starts at this call
+    c.tol = tol;
+    c.maxiter = maxiter;
+    c.maxtime_ns = maxtime * 1e9;
+    c.maxdiff = INFINITY;
+    if ((rc = record_start(e))) return rc;
+    long long done_sweeps = 0;
+    if (maxiter > 0 && maxtime > 0.0) {
+        if ((rc = upload_ctl(e)) || (rc = run_loop(e, 3, maxiter))) return rc;
+        if ((rc = download_ctl(e))) return rc;
+        done_sweeps = e->h_ctl->run_sweeps;
+    }
+    if ((rc = record_stop(e))) return rc;
+    std::vector<int> st(4 * (size_t)G);
+    FLBP_CUDA(cudaMemcpyAsync(st.data(), e->d_gstate, st.size() * sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+    FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    for (uint32_t g = 0; g < G; g++) {
+        if (sweeps) sweeps[g] = st[2 * (size_t)G + g];
+        if (reasons) reasons[g] = st[g] ? st[3 * (size_t)G + g] : FLBP_DIVERGED;
+    }
+    e->t += done_sweeps;
+    e->iters += done_sweeps;
+    fill_info(e, info, done_sweeps, l0);
     return FLBP_OK;
 }
 

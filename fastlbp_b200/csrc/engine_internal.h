@@ -78,6 +78,7 @@ struct HostLayout {
     std::vector<double> prior_fin;     // per internal variable: finite constant log-odds (damping-scaled)
     std::vector<uint32_t> prior_cnt;   // per internal variable: (#+inf) | (#-inf << 16)
     std::vector<uint32_t> var_of_internal;  // internal variable -> reference variable
+    std::vector<uint32_t> factor_of_internal;  // internal (active) factor -> reference factor
     std::vector<uint32_t> internal_of_var;  // reference variable -> internal variable
     uint64_t n_active_slots = 0;       // real (non-padding) slots of active factors
 

@@ -114,8 +114,8 @@ __device__ __forceinline__ T log_sigmoid(T x) {
 template <typename T>
 __device__ __forceinline__ T head_out(T lo, T p, T q, T lp) {
     const T P = Num<T>::exp(lo), R = -Num<T>::expm1(lo);
-    const T B = (T(1) - p) * P + (T(1) - q) * R;
-    const T la = (q == T(0)) ? lp + lo : Num<T>::log(p * P + q * R);
+    const T B = fma(T(1) - p, P, (T(1) - q) * R);
+    const T la = (q == T(0)) ? lp + lo : Num<T>::log(fma(p, P, q * R));
     return la - Num<T>::log(B);
 }
 
@@ -158,7 +158,8 @@ __device__ __forceinline__ BodyDen<T> body_den(T lh, T p, T q) {
 // Body output from the pair (Po, Ro = 1 - Po) of the other body slots.
 template <typename T>
 __device__ __forceinline__ T body_out_pr(T Po, T Ro, T p, T q, const BodyDen<T> &D) {
-    const T a = p * Po + q * Ro, b = (T(1) - p) * Po + (T(1) - q) * Ro;
+    // explicit fused forms: the result must not depend on how a caller's code is contracted
+    const T a = fma(p, Po, q * Ro), b = fma(T(1) - p, Po, (T(1) - q) * Ro);
     const T u = D.pos ? a : b, w = D.pos ? b : a;
     const T lnum = Num<T>::log(u == T(0) ? w : fma(D.r, w, u)) - (u == T(0) ? D.alh : T(0));
     return (D.lden == -Num<T>::inf()) ? D.zero_out : lnum - D.lden;
@@ -180,7 +181,7 @@ __device__ __forceinline__ T damp_mix(T nw, T old, T d) {
         if (ni && oi) return (nw == old) ? nw : T(0);
         return ni ? nw : old;
     }
-    return (T(1) - d) * nw + d * old;
+    return fma(T(1) - d, nw, d * old);
 }
 
 struct FactorArgs {
@@ -195,6 +196,8 @@ struct FactorArgs {
     const uint8_t *bt_kind;   // per big tile: kTileGroups kinds
     const void *bt_pq;        // per big tile: kTileGroups (p, q), T
     const uint4 *thdr;        // kHdrWords-word header per tile (see TileHdr)
+    const uint32_t *f_graph;  // batched solves: graph of every internal factor, else null
+    const int *gdone;         // batched solves: per graph, nonzero once it has stopped
     uint32_t nf_sell, nf_big, nf_huge, n_fgroups, n_tiles, n_tile_blocks;
 };
 
@@ -214,6 +217,12 @@ struct VarArgs {
     const uint4 *thdr;        // kHdrWords-word header per tile (see TileHdr)
     uint32_t nv_sell, nv_big, nv_huge, n_vgroups, n_tiles, n_tile_blocks;
     uint32_t hist_len;
+    // Batched solves (BMODE 4): graph of every internal variable and the
+    // per-graph state gstate[4][n_graphs] = stopped flag, "some belief moved
+    // by more than tol this sweep" flag, sweeps, stop reason.
+    const uint32_t *v_graph;
+    int *gstate;
+    uint32_t n_graphs;
 };
 
 template <typename T>
@@ -332,7 +341,8 @@ struct FactorStage {
     static constexpr size_t deg = pos + 4 * kTileSlots;                // uint8[kTileItems]
     static constexpr size_t kind = deg + kTileItems;                   // uint8[kTileItems]
     static constexpr size_t pq = kind + kTileItems;                    // T[2 * kTileItems]
-    static constexpr size_t bytes = (pq + 2 * sizeof(T) * kTileItems + 127) & ~(size_t)127;
+    static constexpr size_t gid = pq + 2 * sizeof(T) * kTileItems;     // uint32[kTileItems]: graph (batched solves)
+    static constexpr size_t bytes = (gid + 4 * kTileItems + 127) & ~(size_t)127;
 };
 
 // Shared-memory layout of one variable-pass stage.
@@ -344,7 +354,8 @@ struct VarStage {
     static constexpr size_t xo = x + sizeof(T) * kTileSlots;                     // T[kTileSlots]: previous damped fv
     static constexpr size_t prior = xo + (DAMP ? sizeof(T) * kTileSlots : 0);   // uint2 / uint4 [kTileItems]
     static constexpr size_t bold = prior + (sizeof(T) == 4 ? 8 : 16) * kTileItems;  // double[kTileItems]
-    static constexpr size_t bytes = bold + 8 * kTileItems;
+    static constexpr size_t gid = bold + 8 * kTileItems;                        // uint32[kTileItems]: graph (batched)
+    static constexpr size_t bytes = gid + 4 * kTileItems;
 };
 
 // sigma(x) and 1 - sigma(x) without cancellation, from e = exp(-|x|):
@@ -417,7 +428,8 @@ __device__ __forceinline__ void factor_reg(const T *vb, const uint32_t *ps, int 
             R = fma(sg[k], R, ta[k]);
             P = sg[k] * P;
         }
-        if ((kind & HEAD_MASK) == HEAD_FREE) put_fv<T>(fv, ps[lane], sgn * head_from_pair<T>(P, R, p, q, logP));
+        (void)P;
+        (void)R;
         const BodyDen<T> D = body_den<T>(lh, p, q);
         T Pp = T(1), Rp = T(0);
 #pragma unroll
@@ -427,6 +439,9 @@ __device__ __forceinline__ void factor_reg(const T *vb, const uint32_t *ps, int 
             Rp = fma(Pp, ta[k], Rp);
             Pp = Pp * sg[k];
         }
+        // the head from the forward product, as in the wider form below, so that a
+        // factor's outputs do not depend on the width of the group it lands in
+        if ((kind & HEAD_MASK) == HEAD_FREE) put_fv<T>(fv, ps[lane], sgn * head_from_pair<T>(Pp, Rp, p, q, logP));
     } else {
         T pP[W], pR[W];
         T P = T(1), R = T(0);
@@ -603,6 +618,7 @@ template <typename T>
 __device__ __forceinline__ void factor_warp(const FactorArgs &a, uint32_t b, int lane, const T *__restrict__ vf,
                                             T *__restrict__ fv) {
     const uint32_t fi = a.nf_sell + b;
+    if (a.f_graph && a.gdone[a.f_graph[fi]]) return;  // batched solve: its graph has stopped
     const uint32_t s0 = a.fb_off[b], s1 = s0 + a.fb_deg[b];
     const T *pq = reinterpret_cast<const T *>(a.f_pq);
     factor_warp_loop<T>(a, s0, s1, a.f_kind[fi], pq[2 * fi], pq[2 * fi + 1], lane, vf, fv);
@@ -686,11 +702,12 @@ __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArg
                          2u * kTileGroups * (uint32_t)sizeof(T), &full[s]);
             } else {
                 const uint32_t items = 32u * n;
-                mbar_arrive_expect_tx(&full[s],
-                                      ns * (uint32_t)(sizeof(T) + 4) + 2u * items + 2u * items * (uint32_t)sizeof(T));
+                mbar_arrive_expect_tx(&full[s], ns * (uint32_t)(sizeof(T) + 4) + 2u * items +
+                                                    2u * items * (uint32_t)sizeof(T) + (a.f_graph ? 4u * items : 0u));
                 bulk_g2s(st + FS::deg, a.f_deg + 32ull * g0, items, &full[s]);
                 bulk_g2s(st + FS::kind, a.f_kind + 32ull * g0, items, &full[s]);
                 bulk_g2s(st + FS::pq, pq_g + 64ull * g0, 2u * items * (uint32_t)sizeof(T), &full[s]);
+                if (a.f_graph) bulk_g2s(st + FS::gid, a.f_graph + 32ull * g0, 4u * items, &full[s]);
             }
             if (ns) {
                 bulk_g2s(st + FS::vbuf, vf + gb[2], ns * (uint32_t)sizeof(T), &full[s]);
@@ -720,7 +737,8 @@ __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArg
         const unsigned char *st = smem + (size_t)s * FS::bytes;
         const uint32_t *gb = reinterpret_cast<const uint32_t *>(st + FS::hdr);
         if (gb[1] & kBigTileFlag) {  // one big factor per warp
-            if ((uint32_t)wid < (gb[1] & ~kBigTileFlag)) {
+            if ((uint32_t)wid < (gb[1] & ~kBigTileFlag) &&
+                !(a.f_graph && a.gdone[a.f_graph[a.nf_sell + gb[0] + wid]])) {
                 const uint32_t base = gb[2 + wid] - gb[2];
                 const T *pq = reinterpret_cast<const T *>(st + FS::pq);
                 factor_tile_item<T>(reinterpret_cast<const T *>(st + FS::vbuf) + base,
@@ -731,7 +749,8 @@ __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArg
         } else if ((uint32_t)wid < gb[1]) {
             const uint32_t base = gb[2 + wid] - gb[2], f = 32u * wid + lane;
             const int w = (int)((gb[3 + wid] - gb[2 + wid]) >> 5);
-            const int deg = st[FS::deg + f];
+            int deg = st[FS::deg + f];
+            if (a.f_graph && a.gdone[reinterpret_cast<const uint32_t *>(st + FS::gid)[f]]) deg = 0;  // stopped graph
             const T *pq = reinterpret_cast<const T *>(st + FS::pq);
             if (deg > 0)
                 factor_group<T>(w, reinterpret_cast<const T *>(st + FS::vbuf) + base,
@@ -768,14 +787,15 @@ __device__ __forceinline__ double belief_of(double S, int npos, int nneg) {
 }
 
 // BMODE: 0 no beliefs; 1 beliefs + residual; 2 beliefs + residual + count +
-// history; 3 beliefs only (no residual, no history).
+// history; 3 beliefs only (no residual, no history); 4 beliefs + residual of
+// a batched solve (per-graph stop rules).
 template <int BMODE>
 __device__ __forceinline__ double var_finish(const VarArgs &a, uint32_t v, double S, int npos, int nneg, double tol,
                                              double bold, unsigned long long &cnt) {
     double diff = 0.0;
     if (BMODE != 0) {
         const double b = belief_of(S, npos, nneg);
-        if (BMODE == 1 || BMODE == 2) {
+        if (BMODE == 1 || BMODE == 2 || BMODE == 4) {
             const double dd = fabs(bold - b);
             diff = dd;
             if (BMODE == 2) {
@@ -859,8 +879,8 @@ __device__ __forceinline__ double var_tile_big(const VarArgs &a, uint32_t v, uin
             if (e != kSentinel) vf[e] = excl_msg<T>(S, npos, nneg, x[k]);
         }
     }
-    return (lane == 0) ? var_finish<BMODE>(a, v, S, npos, nneg, tol, (BMODE == 1 || BMODE == 2) ? a.belief[v] : 0.0, cnt)
-                       : 0.0;
+    constexpr bool RESID = (BMODE == 1 || BMODE == 2 || BMODE == 4);
+    return (lane == 0) ? var_finish<BMODE>(a, v, S, npos, nneg, tol, RESID ? a.belief[v] : 0.0, cnt) : 0.0;
 }
 
 // Larger variables: lanes stride over the entries, reading them twice.
@@ -967,6 +987,46 @@ static __device__ void stop_rules(Ctl *ctl) {
     }
 }
 
+// Per-graph stop rules of a batched tolerance solve (the rule of stop_rules
+// mode 1 applied to each graph: it stops after the sweep in which no belief
+// moved by more than tol, or after maxiter sweeps; it is then frozen), run by
+// every thread of the last block of the variable pass. The run ends when all
+// graphs have stopped, or at maxtime.
+static __device__ void batch_stop_rules(Ctl *ctl, const VarArgs &a) {
+    __shared__ int s_open;
+    if (threadIdx.x == 0) s_open = 0;
+    __syncthreads();
+    const uint32_t G = a.n_graphs;
+    int *done = a.gstate, *moved = a.gstate + G, *iters = a.gstate + 2 * G, *reason = a.gstate + 3 * G;
+    int open = 0;
+    for (uint32_t g = threadIdx.x; g < G; g += blockDim.x) {
+        if (done[g]) continue;
+        iters[g] += 1;
+        if (!moved[g]) {
+            done[g] = 1;
+            reason[g] = FLBP_ALL_CONVERGED;
+        } else if (ctl->iters0 + iters[g] >= ctl->maxiter) {
+            done[g] = 1;
+            reason[g] = FLBP_DIVERGED;
+        } else {
+            open++;
+        }
+        moved[g] = 0;
+    }
+    if (open) atomicAdd(&s_open, open);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ctl->maxdiff = __longlong_as_double((long long)ctl->maxdiff_bits);
+        unsigned long long now;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+        if (ctl->status != 0 || s_open == 0 || (double)(now - ctl->t_start_ns) >= ctl->maxtime_ns) {
+            ctl->done = 1;
+            ctl->reason = (s_open == 0 && ctl->status == 0) ? FLBP_ALL_CONVERGED : FLBP_DIVERGED;
+        }
+        __threadfence();
+    }
+}
+
 // Variable pass, warp-specialised like the factor pass: the producer warp
 // bulk-loads each tile's entries (factor-side slots), incoming messages, the
 // previous damped messages (with damping), priors and (with a residual)
@@ -985,7 +1045,7 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES];
     typedef VarStage<T, DAMP> VS;
-    constexpr bool RESID = (BMODE == 1 || BMODE == 2);
+    constexpr bool RESID = (BMODE == 1 || BMODE == 2 || BMODE == 4);
     constexpr uint32_t psz = sizeof(T) == 4 ? 8u : 16u;
     if (*(volatile int *)&ctl->done) return;
     const double pscale = ctl->pscale;
@@ -1031,10 +1091,12 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
                     bulk_g2s(st + VS::bold, a.bt_deg + kTileGroups * bt, 4u * kTileGroups, &full[s]);
                 } else {
                     const uint32_t items = 32u * n;
-                    mbar_arrive_expect_tx(&full[s], mbytes + psz * items + (RESID ? 8u * items : 0u));
+                    mbar_arrive_expect_tx(&full[s], mbytes + psz * items + (RESID ? 8u * items : 0u) +
+                                                        (a.v_graph ? 4u * items : 0u));
                     bulk_g2s(st + VS::prior, reinterpret_cast<const unsigned char *>(a.prior) + 32ull * g0 * psz,
                              psz * items, &full[s]);
                     if (RESID) bulk_g2s(st + VS::bold, a.belief + 32ull * g0, 8u * items, &full[s]);
+                    if (a.v_graph) bulk_g2s(st + VS::gid, a.v_graph + 32ull * g0, 4u * items, &full[s]);
                 }
                 if (ns) {
                     bulk_g2s(st + VS::ent, a.v_ent + gb[2], ns * 4u, &full[s]);
@@ -1047,8 +1109,13 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
     } else {  // consumer warps: variables too large for a tile first
         {
             const uint32_t warp = blockIdx.x * kConsumerWarps + wid, nwarps = gridDim.x * kConsumerWarps;
-            for (uint32_t b = warp; b < a.nv_huge; b += nwarps)
-                dmax = fmax(dmax, var_warp<T, BMODE, WRITE_VF, DAMP>(a, b, lane, fv, vf, fvd, d, pscale, tol, cnt));
+            for (uint32_t b = warp; b < a.nv_huge; b += nwarps) {
+                const uint32_t g = a.v_graph ? a.v_graph[a.nv_sell + b] : 0;
+                if (a.v_graph && a.gstate[g]) continue;  // stopped graph (batched solve)
+                const double dd = var_warp<T, BMODE, WRITE_VF, DAMP>(a, b, lane, fv, vf, fvd, d, pscale, tol, cnt);
+                dmax = fmax(dmax, dd);
+                if (BMODE == 4 && dd > tol) a.gstate[a.n_graphs + g] = 1;
+            }
         }
         for (uint32_t it = 0; it < my_tiles; it++) {
             const int s = (int)(it % STAGES);
@@ -1059,14 +1126,17 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
             unsigned char *st = smem + (size_t)s * VS::bytes;
             const uint32_t *gb = reinterpret_cast<const uint32_t *>(st + VS::hdr);
             if (gb[1] & kBigTileFlag) {  // one big variable per warp
-                if ((uint32_t)wid < (gb[1] & ~kBigTileFlag)) {
+                const uint32_t v = a.nv_sell + gb[0] + wid;
+                const uint32_t g = a.v_graph && (uint32_t)wid < (gb[1] & ~kBigTileFlag) ? a.v_graph[v] : 0;
+                if ((uint32_t)wid < (gb[1] & ~kBigTileFlag) && !(a.v_graph && a.gstate[g])) {
                     const uint32_t base = gb[2 + wid] - gb[2];
-                    dmax = fmax(dmax, var_tile_big<T, BMODE, WRITE_VF, DAMP>(
-                                          a, a.nv_sell + gb[0] + wid, reinterpret_cast<const uint32_t *>(st + VS::bold)[wid],
-                                          reinterpret_cast<const uint32_t *>(st + VS::ent) + base,
-                                          reinterpret_cast<T *>(st + VS::x) + base,
-                                          reinterpret_cast<const T *>(st + VS::xo) + base, fvd + gb[2] + base,
-                                          st + VS::prior, wid, lane, vf, d, pscale, tol, cnt));
+                    const double dd = var_tile_big<T, BMODE, WRITE_VF, DAMP>(
+                        a, v, reinterpret_cast<const uint32_t *>(st + VS::bold)[wid],
+                        reinterpret_cast<const uint32_t *>(st + VS::ent) + base, reinterpret_cast<T *>(st + VS::x) + base,
+                        reinterpret_cast<const T *>(st + VS::xo) + base, fvd + gb[2] + base, st + VS::prior, wid, lane,
+                        vf, d, pscale, tol, cnt);
+                    dmax = fmax(dmax, dd);
+                    if (BMODE == 4 && dd > tol) a.gstate[a.n_graphs + g] = 1;
                 }
             } else if ((uint32_t)wid < gb[1]) {
                 const uint32_t base = gb[2 + wid] - gb[2];
@@ -1075,10 +1145,13 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
                 const uint32_t *en = reinterpret_cast<const uint32_t *>(st + VS::ent) + base;
                 T *x = reinterpret_cast<T *>(st + VS::x) + base;
                 const T *xo = reinterpret_cast<const T *>(st + VS::xo) + base;
+                const uint32_t g = a.v_graph ? reinterpret_cast<const uint32_t *>(st + VS::gid)[t] : 0;
+                const bool live = !(a.v_graph && a.gstate[g]);  // stopped graph (batched solve): no work
+                const int wl = live ? w : 0;
                 double S = 0.0;
                 int npos = 0, nneg = 0;
                 if (v < a.nv_sell) decode_prior<T>(st + VS::prior, t, pscale, S, npos, nneg);
-                for (int k = 0; k < w; k++) {  // padding entries hold 0
+                for (int k = 0; k < wl; k++) {  // padding entries hold 0
                     const int i = 32 * k + lane;
                     T xv = x[i];
                     if (DAMP) {
@@ -1090,13 +1163,14 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
                     else if (xv == -inf) nneg++;
                     else S += (double)xv;
                 }
-                if (v < a.nv_sell)
-                    dmax = fmax(dmax, var_finish<BMODE>(a, v, S, npos, nneg, tol,
-                                                        RESID ? reinterpret_cast<const double *>(st + VS::bold)[t]
-                                                              : 0.0,
-                                                        cnt));
+                if (v < a.nv_sell && live) {
+                    const double dd = var_finish<BMODE>(
+                        a, v, S, npos, nneg, tol, RESID ? reinterpret_cast<const double *>(st + VS::bold)[t] : 0.0, cnt);
+                    dmax = fmax(dmax, dd);
+                    if (BMODE == 4 && dd > tol) a.gstate[a.n_graphs + g] = 1;
+                }
                 if (WRITE_VF) {
-                    for (int k = 0; k < w; k++) {
+                    for (int k = 0; k < wl; k++) {
                         const int i = 32 * k + lane;
                         const uint32_t e = en[i];
                         if (e != kSentinel) vf[e] = excl_msg<T>(S, npos, nneg, x[i]);
@@ -1117,6 +1191,7 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
             s_max[wid] = dmax;
             s_cnt[wid] = cnt;
         }
+        if (BMODE == 4) __threadfence();  // this thread's per-graph flags before the block's arrival
         __syncthreads();
         if (threadIdx.x == 0) {
             double m = 0.0;
@@ -1132,9 +1207,10 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
             s_last = (prev == gridDim.x - 1);
         }
         __syncthreads();
-        if (s_last && threadIdx.x == 0) {
+        if (s_last) {
             __threadfence();
-            stop_rules(ctl);
+            if (BMODE == 4) batch_stop_rules(ctl, a);  // the whole block
+            else if (threadIdx.x == 0) stop_rules(ctl);
         }
     }
 }

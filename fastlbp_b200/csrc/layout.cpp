@@ -160,6 +160,7 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err) {
                          [&](int64_t x, int64_t y) { return off[x + 1] - off[x] > off[y + 1] - off[y]; });
     }
     const uint32_t nf = nf_sell + nf_big;
+    L.factor_of_internal.assign(fact_of_int.begin(), fact_of_int.end());
     L.nf_sell = nf_sell;
     L.nf_big = nf_big;
     L.f_kind.assign(nf, 0);

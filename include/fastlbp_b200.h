@@ -262,6 +262,31 @@ int flbp_fg_construct(const flbp_fg *fg, int64_t *factor_offsets, int64_t *slot_
 /* Engine straight from a graph-model handle (what CausalBP's constructor does). */
 int flbp_engine_create_from_fg(const flbp_fg *fg, const flbp_engine_opts *opts, flbp_engine **out);
 
+/* ---- batched solves (no counterpart in the reference: it solves one graph
+ * per CausalBP object, csrc/ext/causal_bp.cu:858-910) ----
+ *
+ * One engine over n_graphs independent graphs (their disjoint union, graphs
+ * in order): every sweep is one pass over all of them, and each graph stops
+ * by itself under the reference's tolerance rule, after which its messages
+ * and beliefs stay frozen. A graph's results are those of solving it alone
+ * with flbp_run_tol from init(). flbp_get_beliefs returns the beliefs of all
+ * graphs, graph g's variables at [var_off[g], var_off[g+1]). */
+int flbp_batch_create(const flbp_graph_desc *graphs, int64_t n_graphs, const flbp_engine_opts *opts,
+                      flbp_engine **out);
+
+/* Number of graphs and their variable ranges (var_off: n_graphs + 1 entries,
+ * may be NULL). */
+int flbp_batch_info(flbp_engine *eng, int64_t *n_graphs, int64_t *var_off);
+
+/* Tolerance run of every graph from the current messages (call flbp_init
+ * first for a fresh solve): graph g stops after the first sweep in which no
+ * belief moved by more than tol, or after maxiter sweeps; the call returns
+ * when all graphs have stopped or maxtime seconds have passed. Per graph:
+ * sweeps[g] (NULL allowed) and reasons[g] (FLBP_ALL_CONVERGED or
+ * FLBP_DIVERGED; NULL allowed). */
+int flbp_batch_run_tol(flbp_engine *eng, double tol, int64_t maxiter, double maxtime, int64_t *sweeps,
+                       int32_t *reasons, flbp_run_info *info);
+
 #ifdef __cplusplus
 }
 #endif

@@ -63,6 +63,7 @@ struct flbp_engine {
     std::vector<int64_t> graph_var_off;  // n_graphs + 1: variable ranges in the union's order
     uint32_t *d_f_graph = nullptr, *d_v_graph = nullptr;  // internal factor / variable -> graph
     int *d_gstate = nullptr;  // [4][n_graphs]: stopped, moved, sweeps, stop reason
+    uint2 *d_ftrange = nullptr, *d_vtrange = nullptr;  // per tile: range of its items' graphs
     uint8_t *d_f_kind = nullptr, *d_f_deg = nullptr;
     void *d_prior = nullptr;
     double *d_belief = nullptr, *d_lowpass = nullptr, *d_hist = nullptr;
@@ -117,6 +118,8 @@ FactorArgs factor_args(flbp_engine *e) {
     a.n_tile_blocks = e->f_tile_blocks;
     a.f_graph = nullptr;
     a.gdone = nullptr;
+    a.trange = nullptr;
+    a.n_graphs = 0;
     return a;
 }
 
@@ -143,6 +146,7 @@ VarArgs var_args(flbp_engine *e) {
     a.hist_len = e->hist_cap;
     a.v_graph = nullptr;
     a.gstate = nullptr;
+    a.trange = nullptr;
     a.n_graphs = 0;
     return a;
 }
@@ -218,6 +222,8 @@ void launch_sweep(flbp_engine *e, int mode, int which = 3) {
         if (mode == 3) {
             fa.f_graph = e->d_f_graph;
             fa.gdone = e->d_gstate;
+            fa.trange = e->d_ftrange;
+            fa.n_graphs = e->n_graphs;
         }
         factor_pass_kernel<T, kStages><<<e->factor_grid, kBlockThreads, factor_smem<T>(), e->stream>>>(
             fa, (const T *)e->d_vf, (T *)e->d_fv, e->d_ctl);
@@ -227,6 +233,7 @@ void launch_sweep(flbp_engine *e, int mode, int which = 3) {
     if (mode == 3) {
         va.v_graph = e->d_v_graph;
         va.gstate = e->d_gstate;
+        va.trange = e->d_vtrange;
         va.n_graphs = e->n_graphs;
     }
     if (e->damping != 0.0) launch_var_mode<T, true>(e, va, mode);
@@ -474,7 +481,9 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
         return FLBP_ERR_NOMEM;
     }
     std::string err;
-    int rc = build_layout(*graph, e->L, err);
+    GraphIds ids{0, nullptr, nullptr};
+    if (batch) ids = GraphIds{(uint32_t)(batch->var_off.size() - 1), batch->factor_graph.data(), batch->var_graph.data()};
+    int rc = build_layout(*graph, e->L, err, batch ? &ids : nullptr);
     if (rc) {
         set_error(err);
         delete e;
@@ -634,9 +643,18 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
         std::vector<uint32_t> fg(nf_pad, 0), vg(std::max<size_t>(1, nv_pad), 0);
         for (uint32_t f = 0; f < nf; f++) fg[f] = batch->factor_graph[L.factor_of_internal[f]];
         for (uint32_t iv = 0; iv < (uint32_t)L.V; iv++) vg[iv] = batch->var_graph[L.var_of_internal[iv]];
+        auto ranges = [](const std::vector<uint32_t> &hdr, uint32_t nt) {
+            std::vector<uint2> r(std::max<uint32_t>(1, nt));
+            for (uint32_t t = 0; t < nt; t++)
+                r[t] = make_uint2(hdr[(size_t)kHdrWordsHost * t + kHdrGraphLo], hdr[(size_t)kHdrWordsHost * t + kHdrGraphHi]);
+            return r;
+        };
+        const std::vector<uint2> fr = ranges(L.fhdr, L.n_ftiles), vr = ranges(L.vhdr, L.n_vtiles);
         if ((rc = dalloc(e, &e->d_f_graph, fg.size())) || (rc = dalloc(e, &e->d_v_graph, vg.size())) ||
             (rc = dalloc(e, &e->d_gstate, 4 * (size_t)e->n_graphs)) || (rc = upload(e, e->d_f_graph, fg)) ||
-            (rc = upload(e, e->d_v_graph, vg)))
+            (rc = upload(e, e->d_v_graph, vg)) || (rc = dalloc(e, &e->d_ftrange, fr.size())) ||
+            (rc = dalloc(e, &e->d_vtrange, vr.size())) || (rc = upload(e, e->d_ftrange, fr)) ||
+            (rc = upload(e, e->d_vtrange, vr)))
             return fail(rc);
         FLBP_CUDA(cudaMemsetAsync(e->d_gstate, 0, 4 * sizeof(int) * std::max<size_t>(1, e->n_graphs), e->stream));
         FLBP_CUDA(cudaStreamSynchronize(e->stream));
@@ -659,7 +677,7 @@ int flbp_engine_destroy(flbp_engine *e) {
                     e->d_f_deg,  e->d_vg_base,  e->d_vb_off, e->d_v_ent,     e->d_prior,      e->d_belief,
                     e->d_lowpass, e->d_hist,    e->d_hist_next, e->d_hist_count, e->d_ctl,    e->d_scratch,
                     e->d_ftiles, e->d_vtiles,  e->d_fb_deg, e->d_vb_deg, e->d_fbt_deg, e->d_vbt_deg,
-                    e->d_fbt_kind, e->d_fbt_pq, e->d_vbt_prior, e->d_f_graph, e->d_v_graph, e->d_gstate};
+                    e->d_fbt_kind, e->d_fbt_pq, e->d_vbt_prior, e->d_f_graph, e->d_v_graph, e->d_gstate, e->d_ftrange, e->d_vtrange};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (e->h_ctl) cudaFreeHost(e->h_ctl);

@@ -31,6 +31,7 @@ constexpr uint32_t kHdrWordsHost = 32;       // words per tile header
 constexpr uint32_t kBigTileFlag = 0x80000000u;  // header word 1: a tile of large items
 constexpr uint32_t kBigFactorBody = 256;     // body slots of the largest factor evaluated from a tile
 constexpr uint32_t kRunAlign = 4;            // large items' slot / entry runs start on 4-element boundaries
+constexpr uint32_t kHdrGraphLo = 29, kHdrGraphHi = 30;  // tile header words: graph range (batched engines)
 
 // Host-built device layout.
 //
@@ -118,8 +119,18 @@ struct HostLayout {
     uint32_t n_vgroups() const { return vg_base.empty() ? 0 : (uint32_t)vg_base.size() - 1; }
 };
 
+// Graph of every reference factor and variable of a batched engine (the
+// disjoint union of n_graphs graphs).
+struct GraphIds {
+    uint32_t n_graphs;
+    const uint32_t *factor_graph;
+    const uint32_t *var_graph;
+};
+
 // Builds the layout; returns FLBP_OK or an error code with `err` filled in.
-int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err);
+// With `graphs`, items are ordered graph by graph and every tile header also
+// names the range of graphs its items belong to (words kHdrGraphLo/Hi).
+int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, const GraphIds *graphs = nullptr);
 
 // Fills the variable-major export maps of L (idempotent).
 void build_export_maps(HostLayout &L);

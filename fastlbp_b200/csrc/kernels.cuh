@@ -198,6 +198,8 @@ struct FactorArgs {
     const uint4 *thdr;        // kHdrWords-word header per tile (see TileHdr)
     const uint32_t *f_graph;  // batched solves: graph of every internal factor, else null
     const int *gdone;         // batched solves: per graph, nonzero once it has stopped
+    const uint2 *trange;      // batched solves: per tile, the range of its items' graphs
+    uint32_t n_graphs;        // batched solves: number of graphs
     uint32_t nf_sell, nf_big, nf_huge, n_fgroups, n_tiles, n_tile_blocks;
 };
 
@@ -222,6 +224,7 @@ struct VarArgs {
     // by more than tol this sweep" flag, sweeps, stop reason.
     const uint32_t *v_graph;
     int *gstate;
+    const uint2 *trange;      // per tile, the range of its items' graphs
     uint32_t n_graphs;
 };
 
@@ -331,6 +334,93 @@ struct TileHdr {
         for (int i = 0; i < kHdrWords / 4; i++) d[i] = w[i];
     }
 };
+
+constexpr uint32_t kEndTile = 0x40000000u;  // header word 1 of the stage that ends a block's tiles
+constexpr int kDoneWords = 128;              // graphs whose stopped flag is cached in shared memory, / 32
+
+// Batched solves: stopped flags of graphs [0, 32 kDoneWords) as bits in
+// shared memory, taken at kernel entry (they change only between launches).
+__device__ __forceinline__ void load_done_bits(uint32_t *s_done, const int *gdone, uint32_t n_graphs, int lane,
+                                               int wid, int nwarps) {
+    const uint32_t words = min((n_graphs + 31) / 32, (uint32_t)kDoneWords);
+    for (uint32_t w = wid; w < words; w += nwarps) {
+        const uint32_t g = 32 * w + lane;
+        const uint32_t bits = __ballot_sync(0xffffffffu, g < n_graphs && gdone[g] != 0);
+        if (lane == 0) s_done[w] = bits;
+    }
+}
+
+__device__ __forceinline__ bool graph_done(const uint32_t *s_done, const int *gdone, uint32_t g) {
+    return g < 32u * kDoneWords ? ((s_done[g >> 5] >> (g & 31)) & 1u) != 0 : gdone[g] != 0;
+}
+
+// Producer warp of a pass: walks the block's tiles (blockIdx.x + i nb),
+// leaves out those whose graphs have all stopped (batched solves: the lanes
+// test 32 tiles at once), fills one stage per remaining tile with
+// fill(stage, header in shared memory, full barrier) and closes with a stage
+// whose header word 1 is kEndTile. All lanes call it; lane 0 issues the
+// copies. After a timeout it records FLBP_ERR_TIMEOUT, lets its own copies
+// land and returns false.
+template <int STAGES, typename Fill>
+__device__ bool produce_tiles(const uint4 *thdr, const uint2 *trange, const uint32_t *s_done, const int *gdone,
+                              uint32_t my_tiles, uint32_t nb, unsigned char *smem, size_t stage_bytes,
+                              uint64_t *full, uint64_t *empty, int lane, Ctl *ctl, Fill fill) {
+    uint32_t issued = 0;
+    bool ok = true;
+    auto tile_of = [&](uint32_t i) { return (size_t)blockIdx.x + (size_t)i * nb; };
+    for (uint32_t base = 0; base < my_tiles && ok; base += 32) {
+        const uint32_t i = base + lane;
+        bool act = i < my_tiles;
+        if (act && trange) {  // active unless every graph of the tile has stopped
+            const uint2 r = trange[tile_of(i)];
+            bool stopped = r.y >= r.x && r.y - r.x <= 32;
+            for (uint32_t g = r.x; stopped && g <= r.y; g++) stopped = graph_done(s_done, gdone, g);
+            act = !stopped;
+        }
+        uint32_t bits = __ballot_sync(0xffffffffu, act);
+        if (lane == 0 && bits) {
+            TileHdr h;
+            int j = __ffs(bits) - 1;
+            h.load(thdr + (size_t)(kHdrWords / 4) * tile_of(base + j));
+            while (true) {
+                bits &= bits - 1;
+                const int s = (int)(issued % STAGES);
+                if (issued >= (uint32_t)STAGES && !mbar_wait_bounded(&empty[s], ((issued / STAGES) - 1) & 1u)) {
+                    ok = false;
+                    break;
+                }
+                unsigned char *st = smem + (size_t)s * stage_bytes;
+                uint32_t *gb = reinterpret_cast<uint32_t *>(st);
+                h.store(gb);
+                fill(st, gb, &full[s]);
+                issued++;
+                if (!bits) break;
+                j = __ffs(bits) - 1;
+                h.load(thdr + (size_t)(kHdrWords / 4) * tile_of(base + j));
+            }
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+    }
+    if (lane == 0) {
+        if (ok) {  // end marker
+            const int s = (int)(issued % STAGES);
+            if (issued >= (uint32_t)STAGES && !mbar_wait_bounded(&empty[s], ((issued / STAGES) - 1) & 1u)) {
+                ok = false;
+            } else {
+                reinterpret_cast<uint32_t *>(smem + (size_t)s * stage_bytes)[1] = kEndTile;
+                mbar_arrive_expect_tx(&full[s], 0);
+                issued++;
+            }
+        }
+        if (!ok) {
+            record_timeout(ctl);
+            // let this block's own loads in flight land before the block moves on
+            for (uint32_t k = issued > (uint32_t)STAGES ? issued - STAGES : 0; k < issued; k++)
+                mbar_wait_bounded(&full[k % STAGES], (k / STAGES) & 1u);
+        }
+    }
+    return __shfl_sync(0xffffffffu, ok, 0);
+}
 
 // Shared-memory layout of one factor-pass stage.
 template <typename T>
@@ -665,6 +755,8 @@ __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArg
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const uint32_t n_tiles = a.n_tiles, nb = a.n_tile_blocks;
     const uint32_t my_tiles = (blockIdx.x < n_tiles) ? (n_tiles - blockIdx.x + nb - 1) / nb : 0;
+    __shared__ uint32_t s_done[kDoneWords];  // batched solves: stopped graphs
+    if (a.f_graph) load_done_bits(s_done, a.gdone, a.n_graphs, lane, wid, blockDim.x >> 5);
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; s++) {
             mbar_init(&full[s], 1);
@@ -675,52 +767,34 @@ __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArg
     __syncthreads();
 
     if (wid == kConsumerWarps) {  // producer warp
-        if (lane != 0) return;
         const T *pq_g = reinterpret_cast<const T *>(a.f_pq);
-        bool ok = true;
-        uint32_t issued = 0;
-        TileHdr h;
-        if (my_tiles) h.load(a.thdr + (size_t)(kHdrWords / 4) * blockIdx.x);
-        for (uint32_t it = 0; it < my_tiles; it++, issued++) {
-            const int s = (int)(it % STAGES);
-            if (it >= (uint32_t)STAGES && !mbar_wait_bounded(&empty[s], ((it / STAGES) - 1) & 1u)) {
-                ok = false;
-                break;
-            }
-            unsigned char *st = smem + (size_t)s * FS::bytes;
-            uint32_t *gb = reinterpret_cast<uint32_t *>(st + FS::hdr);
-            h.store(gb);
+        auto fill = [&](unsigned char *st, uint32_t *gb, uint64_t *bar) {
             const uint32_t g0 = gb[0], n = gb[1] & ~kBigTileFlag;
             const uint32_t ns = gb[2 + n] - gb[2];
             if (gb[1] & kBigTileFlag) {  // big factors: degrees, kinds and (p, q) from the tile's constants
                 const size_t bt = gb[kHdrWords - 1];
                 constexpr uint32_t cbytes = 4u * kTileGroups + kTileGroups + 2u * kTileGroups * (uint32_t)sizeof(T);
-                mbar_arrive_expect_tx(&full[s], ns * (uint32_t)(sizeof(T) + 4) + cbytes);
-                bulk_g2s(st + FS::deg, a.bt_deg + kTileGroups * bt, 4u * kTileGroups, &full[s]);
-                bulk_g2s(st + FS::kind, a.bt_kind + kTileGroups * bt, kTileGroups, &full[s]);
+                mbar_arrive_expect_tx(bar, ns * (uint32_t)(sizeof(T) + 4) + cbytes);
+                bulk_g2s(st + FS::deg, a.bt_deg + kTileGroups * bt, 4u * kTileGroups, bar);
+                bulk_g2s(st + FS::kind, a.bt_kind + kTileGroups * bt, kTileGroups, bar);
                 bulk_g2s(st + FS::pq, reinterpret_cast<const T *>(a.bt_pq) + 2 * kTileGroups * bt,
-                         2u * kTileGroups * (uint32_t)sizeof(T), &full[s]);
+                         2u * kTileGroups * (uint32_t)sizeof(T), bar);
             } else {
                 const uint32_t items = 32u * n;
-                mbar_arrive_expect_tx(&full[s], ns * (uint32_t)(sizeof(T) + 4) + 2u * items +
-                                                    2u * items * (uint32_t)sizeof(T) + (a.f_graph ? 4u * items : 0u));
-                bulk_g2s(st + FS::deg, a.f_deg + 32ull * g0, items, &full[s]);
-                bulk_g2s(st + FS::kind, a.f_kind + 32ull * g0, items, &full[s]);
-                bulk_g2s(st + FS::pq, pq_g + 64ull * g0, 2u * items * (uint32_t)sizeof(T), &full[s]);
-                if (a.f_graph) bulk_g2s(st + FS::gid, a.f_graph + 32ull * g0, 4u * items, &full[s]);
+                mbar_arrive_expect_tx(bar, ns * (uint32_t)(sizeof(T) + 4) + 2u * items +
+                                               2u * items * (uint32_t)sizeof(T) + (a.f_graph ? 4u * items : 0u));
+                bulk_g2s(st + FS::deg, a.f_deg + 32ull * g0, items, bar);
+                bulk_g2s(st + FS::kind, a.f_kind + 32ull * g0, items, bar);
+                bulk_g2s(st + FS::pq, pq_g + 64ull * g0, 2u * items * (uint32_t)sizeof(T), bar);
+                if (a.f_graph) bulk_g2s(st + FS::gid, a.f_graph + 32ull * g0, 4u * items, bar);
             }
             if (ns) {
-                bulk_g2s(st + FS::vbuf, vf + gb[2], ns * (uint32_t)sizeof(T), &full[s]);
-                bulk_g2s(st + FS::pos, a.f_pos + gb[2], ns * 4u, &full[s]);
+                bulk_g2s(st + FS::vbuf, vf + gb[2], ns * (uint32_t)sizeof(T), bar);
+                bulk_g2s(st + FS::pos, a.f_pos + gb[2], ns * 4u, bar);
             }
-            if (it + 1 < my_tiles) h.load(a.thdr + (size_t)(kHdrWords / 4) * (blockIdx.x + (size_t)(it + 1) * nb));
-        }
-        if (!ok) {
-            record_timeout(ctl);
-            // let this block's own loads in flight land before the block exits
-            for (uint32_t k = issued > (uint32_t)STAGES ? issued - STAGES : 0; k < issued; k++)
-                mbar_wait_bounded(&full[k % STAGES], (k / STAGES) & 1u);
-        }
+        };
+        produce_tiles<STAGES>(a.thdr, a.f_graph ? a.trange : nullptr, s_done, a.gdone, my_tiles, nb, smem, FS::bytes,
+                              full, empty, lane, ctl, fill);
         return;
     }
 
@@ -728,7 +802,7 @@ __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArg
         const uint32_t warp = blockIdx.x * kConsumerWarps + wid, nwarps = gridDim.x * kConsumerWarps;
         for (uint32_t b = warp; b < a.nf_huge; b += nwarps) factor_warp<T>(a, b, lane, vf, fv);
     }
-    for (uint32_t it = 0; it < my_tiles; it++) {
+    for (uint32_t it = 0;; it++) {
         const int s = (int)(it % STAGES);
         if (!warp_wait_stage(&full[s], (it / STAGES) & 1u)) {
             if (lane == 0) record_timeout(ctl);
@@ -736,9 +810,10 @@ __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArg
         }
         const unsigned char *st = smem + (size_t)s * FS::bytes;
         const uint32_t *gb = reinterpret_cast<const uint32_t *>(st + FS::hdr);
+        if (gb[1] == kEndTile) break;
         if (gb[1] & kBigTileFlag) {  // one big factor per warp
             if ((uint32_t)wid < (gb[1] & ~kBigTileFlag) &&
-                !(a.f_graph && a.gdone[a.f_graph[a.nf_sell + gb[0] + wid]])) {
+                !(a.f_graph && graph_done(s_done, a.gdone, a.f_graph[a.nf_sell + gb[0] + wid]))) {
                 const uint32_t base = gb[2 + wid] - gb[2];
                 const T *pq = reinterpret_cast<const T *>(st + FS::pq);
                 factor_tile_item<T>(reinterpret_cast<const T *>(st + FS::vbuf) + base,
@@ -750,7 +825,8 @@ __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArg
             const uint32_t base = gb[2 + wid] - gb[2], f = 32u * wid + lane;
             const int w = (int)((gb[3 + wid] - gb[2 + wid]) >> 5);
             int deg = st[FS::deg + f];
-            if (a.f_graph && a.gdone[reinterpret_cast<const uint32_t *>(st + FS::gid)[f]]) deg = 0;  // stopped graph
+            if (a.f_graph && graph_done(s_done, a.gdone, reinterpret_cast<const uint32_t *>(st + FS::gid)[f]))
+                deg = 0;  // stopped graph
             const T *pq = reinterpret_cast<const T *>(st + FS::pq);
             if (deg > 0)
                 factor_group<T>(w, reinterpret_cast<const T *>(st + FS::vbuf) + base,
@@ -1027,6 +1103,20 @@ static __device__ void batch_stop_rules(Ctl *ctl, const VarArgs &a) {
     }
 }
 
+// Batched solves: graph g had a belief move by more than tol this sweep.
+// Graphs below kMovedWords * 32 are collected in a shared-memory bit set and
+// written out once per block at the end of the pass (a store per graph and
+// block instead of one per variable, which would all hit a few addresses).
+constexpr int kMovedWords = 128;
+__device__ __forceinline__ void mark_moved(uint32_t *s_moved, const VarArgs &a, uint32_t g) {
+    if (g < 32u * kMovedWords) {
+        const uint32_t bit = 1u << (g & 31);
+        if (!(s_moved[g >> 5] & bit)) atomicOr(&s_moved[g >> 5], bit);
+    } else {
+        a.gstate[a.n_graphs + g] = 1;
+    }
+}
+
 // Variable pass, warp-specialised like the factor pass: the producer warp
 // bulk-loads each tile's entries (factor-side slots), incoming messages, the
 // previous damped messages (with damping), priors and (with a residual)
@@ -1056,6 +1146,11 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
     const T inf = Num<T>::inf();
     double dmax = 0.0;
     unsigned long long cnt = 0;
+    __shared__ uint32_t s_moved[BMODE == 4 ? kMovedWords : 1];  // batched: graphs with a belief moved > tol
+    __shared__ uint32_t s_done[kDoneWords];                      // batched: stopped graphs
+    if (BMODE == 4)
+        for (int w = threadIdx.x; w < kMovedWords; w += blockDim.x) s_moved[w] = 0u;
+    if (a.v_graph) load_done_bits(s_done, a.gstate, a.n_graphs, lane, wid, blockDim.x >> 5);
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; s++) {
             mbar_init(&full[s], 1);
@@ -1065,59 +1160,44 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
     }
     __syncthreads();
     if (wid == kConsumerWarps) {  // producer warp
-        if (lane == 0) {
-            TileHdr h;
-            if (my_tiles) h.load(a.thdr + (size_t)(kHdrWords / 4) * blockIdx.x);
-            for (uint32_t it = 0; it < my_tiles; it++) {
-                const int s = (int)(it % STAGES);
-                if (it >= (uint32_t)STAGES && !mbar_wait_bounded(&empty[s], ((it / STAGES) - 1) & 1u)) {
-                    record_timeout(ctl);
-                    // let this block's own loads in flight land before the block moves on
-                    for (uint32_t k = it > (uint32_t)STAGES ? it - STAGES : 0; k < it; k++)
-                        mbar_wait_bounded(&full[k % STAGES], (k / STAGES) & 1u);
-                    break;
-                }
-                unsigned char *st = smem + (size_t)s * VS::bytes;
-                uint32_t *gb = reinterpret_cast<uint32_t *>(st + VS::hdr);
-                h.store(gb);
-                const uint32_t g0 = gb[0], n = gb[1] & ~kBigTileFlag;
-                const uint32_t ns = gb[2 + n] - gb[2];
-                const uint32_t mbytes = ns * (4u + (DAMP ? 2u : 1u) * (uint32_t)sizeof(T));
-                if (gb[1] & kBigTileFlag) {  // big variables: entry counts and priors from the tile's constants
-                    const size_t bt = gb[kHdrWords - 1];
-                    mbar_arrive_expect_tx(&full[s], mbytes + psz * kTileGroups + 4u * kTileGroups);
-                    bulk_g2s(st + VS::prior, reinterpret_cast<const unsigned char *>(a.bt_prior) + psz * kTileGroups * bt,
-                             psz * kTileGroups, &full[s]);
-                    bulk_g2s(st + VS::bold, a.bt_deg + kTileGroups * bt, 4u * kTileGroups, &full[s]);
-                } else {
-                    const uint32_t items = 32u * n;
-                    mbar_arrive_expect_tx(&full[s], mbytes + psz * items + (RESID ? 8u * items : 0u) +
-                                                        (a.v_graph ? 4u * items : 0u));
-                    bulk_g2s(st + VS::prior, reinterpret_cast<const unsigned char *>(a.prior) + 32ull * g0 * psz,
-                             psz * items, &full[s]);
-                    if (RESID) bulk_g2s(st + VS::bold, a.belief + 32ull * g0, 8u * items, &full[s]);
-                    if (a.v_graph) bulk_g2s(st + VS::gid, a.v_graph + 32ull * g0, 4u * items, &full[s]);
-                }
-                if (ns) {
-                    bulk_g2s(st + VS::ent, a.v_ent + gb[2], ns * 4u, &full[s]);
-                    bulk_g2s(st + VS::x, fv + gb[2], ns * (uint32_t)sizeof(T), &full[s]);
-                    if (DAMP) bulk_g2s(st + VS::xo, fvd + gb[2], ns * (uint32_t)sizeof(T), &full[s]);
-                }
-                if (it + 1 < my_tiles) h.load(a.thdr + (size_t)(kHdrWords / 4) * (blockIdx.x + (size_t)(it + 1) * nb));
+        auto fill = [&](unsigned char *st, uint32_t *gb, uint64_t *bar) {
+            const uint32_t g0 = gb[0], n = gb[1] & ~kBigTileFlag;
+            const uint32_t ns = gb[2 + n] - gb[2];
+            const uint32_t mbytes = ns * (4u + (DAMP ? 2u : 1u) * (uint32_t)sizeof(T));
+            if (gb[1] & kBigTileFlag) {  // big variables: entry counts and priors from the tile's constants
+                const size_t bt = gb[kHdrWords - 1];
+                mbar_arrive_expect_tx(bar, mbytes + psz * kTileGroups + 4u * kTileGroups);
+                bulk_g2s(st + VS::prior, reinterpret_cast<const unsigned char *>(a.bt_prior) + psz * kTileGroups * bt,
+                         psz * kTileGroups, bar);
+                bulk_g2s(st + VS::bold, a.bt_deg + kTileGroups * bt, 4u * kTileGroups, bar);
+            } else {
+                const uint32_t items = 32u * n;
+                mbar_arrive_expect_tx(bar, mbytes + psz * items + (RESID ? 8u * items : 0u) + (a.v_graph ? 4u * items : 0u));
+                bulk_g2s(st + VS::prior, reinterpret_cast<const unsigned char *>(a.prior) + 32ull * g0 * psz,
+                         psz * items, bar);
+                if (RESID) bulk_g2s(st + VS::bold, a.belief + 32ull * g0, 8u * items, bar);
+                if (a.v_graph) bulk_g2s(st + VS::gid, a.v_graph + 32ull * g0, 4u * items, bar);
             }
-        }
+            if (ns) {
+                bulk_g2s(st + VS::ent, a.v_ent + gb[2], ns * 4u, bar);
+                bulk_g2s(st + VS::x, fv + gb[2], ns * (uint32_t)sizeof(T), bar);
+                if (DAMP) bulk_g2s(st + VS::xo, fvd + gb[2], ns * (uint32_t)sizeof(T), bar);
+            }
+        };
+        produce_tiles<STAGES>(a.thdr, a.v_graph ? a.trange : nullptr, s_done, a.gstate, my_tiles, nb, smem,
+                              VS::bytes, full, empty, lane, ctl, fill);
     } else {  // consumer warps: variables too large for a tile first
         {
             const uint32_t warp = blockIdx.x * kConsumerWarps + wid, nwarps = gridDim.x * kConsumerWarps;
             for (uint32_t b = warp; b < a.nv_huge; b += nwarps) {
                 const uint32_t g = a.v_graph ? a.v_graph[a.nv_sell + b] : 0;
-                if (a.v_graph && a.gstate[g]) continue;  // stopped graph (batched solve)
+                if (a.v_graph && graph_done(s_done, a.gstate, g)) continue;  // stopped graph (batched solve)
                 const double dd = var_warp<T, BMODE, WRITE_VF, DAMP>(a, b, lane, fv, vf, fvd, d, pscale, tol, cnt);
                 dmax = fmax(dmax, dd);
-                if (BMODE == 4 && dd > tol) a.gstate[a.n_graphs + g] = 1;
+                if (BMODE == 4 && dd > tol) mark_moved(s_moved, a, g);
             }
         }
-        for (uint32_t it = 0; it < my_tiles; it++) {
+        for (uint32_t it = 0;; it++) {
             const int s = (int)(it % STAGES);
             if (!warp_wait_stage(&full[s], (it / STAGES) & 1u)) {
                 if (lane == 0) record_timeout(ctl);
@@ -1125,10 +1205,11 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
             }
             unsigned char *st = smem + (size_t)s * VS::bytes;
             const uint32_t *gb = reinterpret_cast<const uint32_t *>(st + VS::hdr);
+            if (gb[1] == kEndTile) break;
             if (gb[1] & kBigTileFlag) {  // one big variable per warp
                 const uint32_t v = a.nv_sell + gb[0] + wid;
                 const uint32_t g = a.v_graph && (uint32_t)wid < (gb[1] & ~kBigTileFlag) ? a.v_graph[v] : 0;
-                if ((uint32_t)wid < (gb[1] & ~kBigTileFlag) && !(a.v_graph && a.gstate[g])) {
+                if ((uint32_t)wid < (gb[1] & ~kBigTileFlag) && !(a.v_graph && graph_done(s_done, a.gstate, g))) {
                     const uint32_t base = gb[2 + wid] - gb[2];
                     const double dd = var_tile_big<T, BMODE, WRITE_VF, DAMP>(
                         a, v, reinterpret_cast<const uint32_t *>(st + VS::bold)[wid],
@@ -1136,7 +1217,7 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
                         reinterpret_cast<const T *>(st + VS::xo) + base, fvd + gb[2] + base, st + VS::prior, wid, lane,
                         vf, d, pscale, tol, cnt);
                     dmax = fmax(dmax, dd);
-                    if (BMODE == 4 && dd > tol) a.gstate[a.n_graphs + g] = 1;
+                    if (BMODE == 4 && dd > tol) mark_moved(s_moved, a, g);
                 }
             } else if ((uint32_t)wid < gb[1]) {
                 const uint32_t base = gb[2 + wid] - gb[2];
@@ -1146,7 +1227,7 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
                 T *x = reinterpret_cast<T *>(st + VS::x) + base;
                 const T *xo = reinterpret_cast<const T *>(st + VS::xo) + base;
                 const uint32_t g = a.v_graph ? reinterpret_cast<const uint32_t *>(st + VS::gid)[t] : 0;
-                const bool live = !(a.v_graph && a.gstate[g]);  // stopped graph (batched solve): no work
+                const bool live = !(a.v_graph && graph_done(s_done, a.gstate, g));  // stopped graph: no work
                 const int wl = live ? w : 0;
                 double S = 0.0;
                 int npos = 0, nneg = 0;
@@ -1167,7 +1248,7 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
                     const double dd = var_finish<BMODE>(
                         a, v, S, npos, nneg, tol, RESID ? reinterpret_cast<const double *>(st + VS::bold)[t] : 0.0, cnt);
                     dmax = fmax(dmax, dd);
-                    if (BMODE == 4 && dd > tol) a.gstate[a.n_graphs + g] = 1;
+                    if (BMODE == 4 && dd > tol) mark_moved(s_moved, a, g);
                 }
                 if (WRITE_VF) {
                     for (int k = 0; k < wl; k++) {
@@ -1191,8 +1272,20 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
             s_max[wid] = dmax;
             s_cnt[wid] = cnt;
         }
-        if (BMODE == 4) __threadfence();  // this thread's per-graph flags before the block's arrival
         __syncthreads();
+        if (BMODE == 4) {  // the block's per-graph flags, one store per graph
+            const uint32_t words = min((a.n_graphs + 31) / 32, (uint32_t)kMovedWords);
+            for (uint32_t w = threadIdx.x; w < words; w += blockDim.x) {
+                uint32_t bits = s_moved[w];
+                while (bits) {
+                    const int b = __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    a.gstate[a.n_graphs + 32 * w + b] = 1;
+                }
+            }
+            __threadfence();
+            __syncthreads();
+        }
         if (threadIdx.x == 0) {
             double m = 0.0;
             unsigned long long c = 0;

@@ -36,7 +36,7 @@ inline double logit(double p) { return std::log(p) - std::log1p(-p); }
 
 }  // namespace
 
-int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err) {
+int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, const GraphIds *graphs) {
     const int64_t V = g.n_vars, F = g.n_factors, E = g.n_slots;
     if (V < 0 || F < 0 || E < 0) {
         err = "negative graph size";
@@ -134,30 +134,42 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err) {
         active[I] = 1;
     }
 
-    // --- internal factor order: sliced-ELL factors by degree, then big ones ---------
+    // --- internal factor order: sliced-ELL factors by (graph, degree), then big ones ---
+    // Batched engines (graph ids given) keep each graph's items together so
+    // that the tiles of a graph that has stopped can be skipped; a single
+    // graph is graph 0 throughout.
+    const uint32_t G = graphs ? graphs->n_graphs : 1;
+    auto fgraph = [&](int64_t I) -> uint32_t { return graphs ? graphs->factor_graph[I] : 0u; };
+    auto vgraph = [&](int64_t i) -> uint32_t { return graphs ? graphs->var_graph[i] : 0u; };
     std::vector<int64_t> fact_of_int;
     uint32_t nf_sell = 0, nf_big = 0;
     {
-        std::vector<uint32_t> cnt(kSellFactorDegree + 1, 0);
+        constexpr uint32_t D = kSellFactorDegree + 1;
+        std::vector<uint64_t> pos((size_t)G * D + 1, 0);
         for (int64_t I = 0; I < F; I++) {
             if (!active[I]) continue;
             const uint64_t d = (uint64_t)(off[I + 1] - off[I]);
-            if (d <= kSellFactorDegree) cnt[d]++, nf_sell++;
+            if (d <= kSellFactorDegree) pos[(size_t)fgraph(I) * D + d + 1]++, nf_sell++;
             else nf_big++;
         }
-        std::vector<uint32_t> pos(kSellFactorDegree + 1, 0);
-        for (uint32_t d = 1; d <= kSellFactorDegree; d++) pos[d] = pos[d - 1] + cnt[d - 1];
+        for (size_t k = 1; k < pos.size(); k++) pos[k] += pos[k - 1];
         fact_of_int.assign((size_t)nf_sell + nf_big, 0);
         uint32_t b = nf_sell;
         for (int64_t I = 0; I < F; I++) {
             if (!active[I]) continue;
             const uint64_t d = (uint64_t)(off[I + 1] - off[I]);
-            if (d <= kSellFactorDegree) fact_of_int[pos[d]++] = I;
+            if (d <= kSellFactorDegree) fact_of_int[pos[(size_t)fgraph(I) * D + d]++] = I;
             else fact_of_int[b++] = I;
         }
-        // large factors by decreasing degree: warps deal them round-robin, largest first
-        std::stable_sort(fact_of_int.begin() + nf_sell, fact_of_int.end(),
-                         [&](int64_t x, int64_t y) { return off[x + 1] - off[x] > off[y + 1] - off[y]; });
+        // large factors: those too large for a tile first, then by (graph, decreasing
+        // degree); warps deal them round-robin, largest first
+        auto deg = [&](int64_t I) { return off[I + 1] - off[I]; };
+        std::stable_sort(fact_of_int.begin() + nf_sell, fact_of_int.end(), [&](int64_t x, int64_t y) {
+            const bool hx = deg(x) - 1 > (int64_t)kBigFactorBody, hy = deg(y) - 1 > (int64_t)kBigFactorBody;
+            if (hx != hy) return hx;
+            if (!hx && fgraph(x) != fgraph(y)) return fgraph(x) < fgraph(y);
+            return deg(x) > deg(y);
+        });
     }
     const uint32_t nf = nf_sell + nf_big;
     L.factor_of_internal.assign(fact_of_int.begin(), fact_of_int.end());
@@ -238,31 +250,37 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err) {
     }
     L.n_active_slots = n_act;
 
-    // Internal variable order: sliced-ELL variables by degree and, within a
-    // degree, by their first device slot (so that variables reached from
-    // neighbouring factors sit together), then the large ones by decreasing
-    // degree. One scan over the device slots in increasing order finds every
-    // variable's first slot.
+    // Internal variable order: sliced-ELL variables by (graph, degree) and,
+    // within that, by their first device slot (so that variables reached from
+    // neighbouring factors sit together), then the large ones: those too large
+    // for a tile first, the rest by (graph, decreasing degree). One scan over
+    // the device slots in increasing order finds every variable's first slot.
     uint32_t nv_sell = 0;
     std::vector<uint32_t> order(V);
     {
-        std::vector<uint64_t> pos(kSellVarDegree + 2, 0);
+        constexpr uint32_t D = kSellVarDegree + 1;
+        std::vector<uint64_t> pos((size_t)G * D + 1, 0);
         for (int64_t i = 0; i < V; i++)
-            if (vdeg[i] <= kSellVarDegree) pos[vdeg[i] + 1]++, nv_sell++;
-        for (uint32_t d = 1; d <= kSellVarDegree + 1; d++) pos[d] += pos[d - 1];
+            if (vdeg[i] <= kSellVarDegree) pos[(size_t)vgraph(i) * D + vdeg[i] + 1]++, nv_sell++;
+        for (size_t k = 1; k < pos.size(); k++) pos[k] += pos[k - 1];
         for (int64_t i = 0; i < V; i++)
-            if (vdeg[i] == 0) order[pos[0]++] = (uint32_t)i;
+            if (vdeg[i] == 0) order[pos[(size_t)vgraph(i) * D]++] = (uint32_t)i;
         std::vector<uint8_t> seen(V, 0);
         for (uint64_t sl = 0; sl < L.n_slots; sl++) {
             const uint32_t v = var_of_dev[sl];
             if (v == UINT32_MAX || seen[v]) continue;
             seen[v] = 1;
-            if (vdeg[v] <= kSellVarDegree) order[pos[vdeg[v]]++] = v;
+            if (vdeg[v] <= kSellVarDegree) order[pos[(size_t)vgraph(v) * D + vdeg[v]]++] = v;
         }
         uint32_t b = nv_sell;
         for (int64_t i = 0; i < V; i++)
             if (vdeg[i] > kSellVarDegree) order[b++] = (uint32_t)i;
-        std::stable_sort(order.begin() + nv_sell, order.end(), [&](uint32_t x, uint32_t y) { return vdeg[x] > vdeg[y]; });
+        std::stable_sort(order.begin() + nv_sell, order.end(), [&](uint32_t x, uint32_t y) {
+            const bool hx = vdeg[x] > kTileSlotsHost, hy = vdeg[y] > kTileSlotsHost;
+            if (hx != hy) return hx;
+            if (!hx && vgraph(x) != vgraph(y)) return vgraph(x) < vgraph(y);
+            return vdeg[x] > vdeg[y];
+        });
     }
     L.nv_sell = nv_sell;
     L.nv_big = (uint32_t)V - nv_sell;
@@ -375,6 +393,32 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err) {
     L.n_ftiles = L.n_fbtiles + sell_tiles(L.fg_base, L.fhdr);
     L.n_vbtiles = big_tiles(L.vb_off, L.vb_deg, L.nv_huge, L.nv_big, L.vhdr, vbt_first);
     L.n_vtiles = L.n_vbtiles + sell_tiles(L.vg_base, L.vhdr);
+    // batched engines: the range of graphs of every tile's items
+    if (graphs) {
+        auto stamp = [&](std::vector<uint32_t> &hdr, uint32_t nt, uint32_t n_sell_items, auto item_graph) {
+            for (uint32_t t = 0; t < nt; t++) {
+                uint32_t *h = &hdr[(size_t)kHdrWordsHost * t];
+                const bool big = h[1] & kBigTileFlag;
+                const uint32_t n = h[1] & ~kBigTileFlag;
+                uint32_t lo = UINT32_MAX, hi = 0;
+                auto see = [&](uint32_t item) {
+                    const uint32_t gr = item_graph(item);
+                    lo = std::min(lo, gr);
+                    hi = std::max(hi, gr);
+                };
+                if (big) {
+                    for (uint32_t j = 0; j < n; j++) see(n_sell_items + h[0] + j);
+                } else {
+                    for (uint32_t i = 32 * h[0]; i < std::min(n_sell_items, 32 * (h[0] + n)); i++) see(i);
+                }
+                h[kHdrGraphLo] = lo;
+                h[kHdrGraphHi] = hi;
+            }
+        };
+        stamp(L.fhdr, L.n_ftiles, nf_sell, [&](uint32_t f) { return fgraph(fact_of_int[f]); });
+        stamp(L.vhdr, L.n_vtiles, nv_sell, [&](uint32_t iv) { return vgraph(order[iv]); });
+    }
+
     // per large tile constants: degrees and kinds (factor side), degrees (variable side)
     L.fbt_deg.assign((size_t)kTileGroupsHost * L.n_fbtiles, 0);
     L.fbt_kind.assign((size_t)kTileGroupsHost * L.n_fbtiles, 0);

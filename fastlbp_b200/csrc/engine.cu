@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstddef>
 #include <cstring>
 #include <limits>
 #include <map>
@@ -252,6 +253,8 @@ void launch_beliefs_only_t(flbp_engine *e, double *dst) {
     VarArgs a = var_args(e);
     a.belief = dst;
     const T *src = (const T *)(e->damping != 0.0 ? e->d_fvd : e->d_fv);
+    // the tile counter of the variable pass is reset by the factor pass; none ran since the last one
+    cudaMemsetAsync(reinterpret_cast<char *>(e->d_ctl) + offsetof(Ctl, vnext), 0, sizeof(unsigned int), e->stream);
     var_pass_kernel<T, 3, false, false, kStages><<<e->var_grid, kBlockThreads, var_smem<T, false>(), e->stream>>>(
         a, src, (T *)e->d_vf, nullptr, (T)0, e->d_ctl);
 }

@@ -57,6 +57,8 @@ struct Ctl {
     long long n_vars;
     double damping;
     double pscale;                    // 1 - damping^t: weight of the finite constant priors
+    unsigned int fnext, vnext;        // next chunk of tiles of the factor / variable pass (reset by the other pass)
+    unsigned int pad2[2];
 };
 
 template <typename T>
@@ -354,35 +356,51 @@ __device__ __forceinline__ bool graph_done(const uint32_t *s_done, const int *gd
     return g < 32u * kDoneWords ? ((s_done[g >> 5] >> (g & 31)) & 1u) != 0 : gdone[g] != 0;
 }
 
-// Producer warp of a pass: walks the block's tiles (blockIdx.x + i nb),
-// leaves out those whose graphs have all stopped (batched solves: the lanes
-// test 32 tiles at once), fills one stage per remaining tile with
-// fill(stage, header in shared memory, full barrier) and closes with a stage
-// whose header word 1 is kEndTile. All lanes call it; lane 0 issues the
-// copies. After a timeout it records FLBP_ERR_TIMEOUT, lets its own copies
-// land and returns false.
+// Producer warp of a pass. A single graph's pass walks the block's tiles
+// blockIdx.x + i gridDim.x in order (neighbouring blocks work on neighbouring
+// tiles at any moment, which keeps the scattered stores of a pass close
+// together). A batched solve instead takes chunks of kChunkTiles consecutive
+// tiles from the pass's counter, so that blocks whose tiles belong to stopped
+// graphs take more, and leaves out tiles whose graphs have all stopped. One
+// stage per remaining tile is filled with fill(stage, header in shared
+// memory, full barrier); a stage whose header word 1 is kEndTile closes the
+// stream. All lanes call it; lane 0 issues the copies. After a timeout it
+// records FLBP_ERR_TIMEOUT, lets its own copies land and returns false.
+constexpr uint32_t kChunkTiles = 4;
+
 template <int STAGES, typename Fill>
 __device__ bool produce_tiles(const uint4 *thdr, const uint2 *trange, const uint32_t *s_done, const int *gdone,
-                              uint32_t my_tiles, uint32_t nb, unsigned char *smem, size_t stage_bytes,
+                              uint32_t n_tiles, unsigned int *counter, unsigned char *smem, size_t stage_bytes,
                               uint64_t *full, uint64_t *empty, int lane, Ctl *ctl, Fill fill) {
     uint32_t issued = 0;
     bool ok = true;
-    auto tile_of = [&](uint32_t i) { return (size_t)blockIdx.x + (size_t)i * nb; };
-    for (uint32_t base = 0; base < my_tiles && ok; base += 32) {
-        const uint32_t i = base + lane;
-        bool act = i < my_tiles;
-        if (act && trange) {  // active unless every graph of the tile has stopped
-            const uint2 r = trange[tile_of(i)];
+    const bool dynamic = trange != nullptr;
+    // round r covers tiles tile_at(r, 0..width-1)
+    const uint32_t width = dynamic ? kChunkTiles : 32u;
+    const uint32_t nb = gridDim.x;
+    uint32_t round = dynamic ? __shfl_sync(0xffffffffu, lane == 0 ? atomicAdd(counter, 1u) : 0u, 0) : 0u;
+    auto tile_at = [&](uint32_t r, uint32_t k) -> uint32_t {  // n_tiles when out of range
+        const uint64_t t = dynamic ? (uint64_t)r * width + k : (uint64_t)blockIdx.x + ((uint64_t)r * width + k) * nb;
+        return t < n_tiles ? (uint32_t)t : n_tiles;
+    };
+    TileHdr h;
+    bool have_h = false;  // h holds the header of tile_at(round, 0)
+    while (ok && tile_at(round, 0) < n_tiles) {
+        const uint32_t next = dynamic ? __shfl_sync(0xffffffffu, lane == 0 ? atomicAdd(counter, 1u) : 0u, 0)
+                                      : round + 1;
+        const uint32_t t = (uint32_t)lane < width ? tile_at(round, lane) : n_tiles;
+        bool act = t < n_tiles;
+        if (act && dynamic) {  // active unless every graph of the tile has stopped
+            const uint2 r = trange[t];
             bool stopped = r.y >= r.x && r.y - r.x <= 32;
             for (uint32_t g = r.x; stopped && g <= r.y; g++) stopped = graph_done(s_done, gdone, g);
             act = !stopped;
         }
         uint32_t bits = __ballot_sync(0xffffffffu, act);
-        if (lane == 0 && bits) {
-            TileHdr h;
-            int j = __ffs(bits) - 1;
-            h.load(thdr + (size_t)(kHdrWords / 4) * tile_of(base + j));
-            while (true) {
+        if (lane == 0) {
+            int j = bits ? __ffs(bits) - 1 : -1;
+            if (j > 0 || (j == 0 && !have_h)) h.load(thdr + (size_t)(kHdrWords / 4) * tile_at(round, j));
+            while (j >= 0) {
                 bits &= bits - 1;
                 const int s = (int)(issued % STAGES);
                 if (issued >= (uint32_t)STAGES && !mbar_wait_bounded(&empty[s], ((issued / STAGES) - 1) & 1u)) {
@@ -394,12 +412,15 @@ __device__ bool produce_tiles(const uint4 *thdr, const uint2 *trange, const uint
                 h.store(gb);
                 fill(st, gb, &full[s]);
                 issued++;
-                if (!bits) break;
-                j = __ffs(bits) - 1;
-                h.load(thdr + (size_t)(kHdrWords / 4) * tile_of(base + j));
+                j = bits ? __ffs(bits) - 1 : -1;
+                if (j >= 0) h.load(thdr + (size_t)(kHdrWords / 4) * tile_at(round, j));
             }
+            // the first header of the next round, while the stages are busy
+            have_h = tile_at(next, 0) < n_tiles;
+            if (ok && have_h) h.load(thdr + (size_t)(kHdrWords / 4) * tile_at(next, 0));
         }
         ok = __shfl_sync(0xffffffffu, ok, 0);
+        round = next;
     }
     if (lane == 0) {
         if (ok) {  // end marker
@@ -751,10 +772,10 @@ __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArg
         ctl->maxdiff_bits = 0ull;
         ctl->nonconv = 0ull;
         ctl->arrive = 0u;
+        ctl->vnext = 0u;  // the variable pass of this sweep starts after this kernel
     }
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const uint32_t n_tiles = a.n_tiles, nb = a.n_tile_blocks;
-    const uint32_t my_tiles = (blockIdx.x < n_tiles) ? (n_tiles - blockIdx.x + nb - 1) / nb : 0;
+    const uint32_t n_tiles = a.n_tiles;
     __shared__ uint32_t s_done[kDoneWords];  // batched solves: stopped graphs
     if (a.f_graph) load_done_bits(s_done, a.gdone, a.n_graphs, lane, wid, blockDim.x >> 5);
     if (threadIdx.x == 0) {
@@ -793,8 +814,8 @@ __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArg
                 bulk_g2s(st + FS::pos, a.f_pos + gb[2], ns * 4u, bar);
             }
         };
-        produce_tiles<STAGES>(a.thdr, a.f_graph ? a.trange : nullptr, s_done, a.gdone, my_tiles, nb, smem, FS::bytes,
-                              full, empty, lane, ctl, fill);
+        produce_tiles<STAGES>(a.thdr, a.f_graph ? a.trange : nullptr, s_done, a.gdone, n_tiles, &ctl->fnext, smem,
+                              FS::bytes, full, empty, lane, ctl, fill);
         return;
     }
 
@@ -1138,11 +1159,11 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
     constexpr bool RESID = (BMODE == 1 || BMODE == 2 || BMODE == 4);
     constexpr uint32_t psz = sizeof(T) == 4 ? 8u : 16u;
     if (*(volatile int *)&ctl->done) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->fnext = 0u;  // the next factor pass starts after this kernel
     const double pscale = ctl->pscale;
     const double tol = ctl->tol;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const uint32_t n_tiles = a.n_tiles, nb = a.n_tile_blocks;
-    const uint32_t my_tiles = (blockIdx.x < n_tiles) ? (n_tiles - blockIdx.x + nb - 1) / nb : 0;
+    const uint32_t n_tiles = a.n_tiles;
     const T inf = Num<T>::inf();
     double dmax = 0.0;
     unsigned long long cnt = 0;
@@ -1184,7 +1205,7 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
                 if (DAMP) bulk_g2s(st + VS::xo, fvd + gb[2], ns * (uint32_t)sizeof(T), bar);
             }
         };
-        produce_tiles<STAGES>(a.thdr, a.v_graph ? a.trange : nullptr, s_done, a.gstate, my_tiles, nb, smem,
+        produce_tiles<STAGES>(a.thdr, a.v_graph ? a.trange : nullptr, s_done, a.gstate, n_tiles, &ctl->vnext, smem,
                               VS::bytes, full, empty, lane, ctl, fill);
     } else {  // consumer warps: variables too large for a tile first
         {

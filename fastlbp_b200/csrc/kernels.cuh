@@ -309,6 +309,9 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
 
 __device__ __forceinline__ void record_timeout(Ctl *ctl) { atomicExch(&ctl->status, FLBP_ERR_TIMEOUT); }
 
+// Barrier among the consumer threads only (the producer warp never joins).
+__device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kConsumers) : "memory"); }
+
 
 // Waits for a stage on every lane of a warp; true on all lanes, or false on
 // all lanes when any of them gave up.
@@ -694,17 +697,25 @@ __device__ __forceinline__ void factor_tile_big(const T *vb, const uint32_t *ps,
     }
 }
 
-// Larger factors: lanes stride over the body, reading it twice.
+// A factor too large for a tile (big factor b, internal index nf_sell + b),
+// spread over all consumer threads of a block (called by all of them): a
+// log-sigmoid sum of the body in FP64 with a count of -inf terms, reduced
+// over the block in a fixed order, then every slot removes its own term.
 template <typename T>
-__device__ __noinline__ void factor_warp_loop(const FactorArgs &a, uint32_t s0, uint32_t s1, uint8_t kind, T p, T q,
-                                              int lane, const T *__restrict__ vf, T *__restrict__ fv) {
+__device__ void factor_block_huge(const FactorArgs &a, uint32_t b, int tid, const T *__restrict__ vf,
+                                  T *__restrict__ fv, double *s_l, int *s_nz) {
+    const uint32_t fi = a.nf_sell + b;
+    if (a.f_graph && a.gdone[a.f_graph[fi]]) return;  // batched solve: its graph has stopped (same for all)
+    const uint32_t s0 = a.fb_off[b], s1 = s0 + a.fb_deg[b];
+    const uint8_t kind = a.f_kind[fi];
+    const T *pq = reinterpret_cast<const T *>(a.f_pq);
+    const T p = pq[2 * fi], q = pq[2 * fi + 1];
     const T s = (kind & KIND_OR) ? T(-1) : T(1);
     const T inf = Num<T>::inf();
-    const bool free_head = (kind & HEAD_MASK) == HEAD_FREE;
-    const T lh = s * head_effective<T>(kind, vf[s0]);
+    const int lane = tid & 31, wid = tid >> 5;
     double L = 0.0;
     int nz = 0;
-    for (uint32_t k = s0 + 1 + lane; k < s1; k += 32) {
+    for (uint32_t k = s0 + 1 + tid; k < s1; k += kConsumers) {
         const T ls = log_sigmoid<T>(s * vf[k]);
         if (ls == -inf) nz++;
         else L += (double)ls;
@@ -714,25 +725,27 @@ __device__ __noinline__ void factor_warp_loop(const FactorArgs &a, uint32_t s0, 
         L += __shfl_xor_sync(0xffffffffu, L, o);
         nz += __shfl_xor_sync(0xffffffffu, nz, o);
     }
-    if (free_head && lane == 0) put_fv<T>(fv, a.f_pos[s0], s * head_out<T>(nz ? -inf : (T)L, p, q, Num<T>::log(p)));
-    const BodyDen<T> D = body_den<T>(lh, p, q);
-    for (uint32_t k = s0 + 1 + lane; k < s1; k += 32) {
+    if (lane == 0) {
+        s_l[wid] = L;
+        s_nz[wid] = nz;
+    }
+    consumer_sync();
+    L = 0.0;
+    nz = 0;
+    for (int w = 0; w < kConsumerWarps; w++) {
+        L += s_l[w];
+        nz += s_nz[w];
+    }
+    consumer_sync();  // the partials are reused by the next factor
+    if ((kind & HEAD_MASK) == HEAD_FREE && tid == 0)
+        put_fv<T>(fv, a.f_pos[s0], s * head_out<T>(nz ? -inf : (T)L, p, q, Num<T>::log(p)));
+    const BodyDen<T> D = body_den<T>(s * head_effective<T>(kind, vf[s0]), p, q);
+    for (uint32_t k = s0 + 1 + tid; k < s1; k += kConsumers) {
         const T ls = log_sigmoid<T>(s * vf[k]);
         const bool z = (ls == -inf);
         const T lo = (nz - (int)z) ? -inf : (T)(z ? L : L - (double)ls);
         put_fv<T>(fv, a.f_pos[k], s * body_out<T>(lo, p, q, D));
     }
-}
-
-// Big factor b (internal index nf_sell + b) too large for a tile, one warp.
-template <typename T>
-__device__ __forceinline__ void factor_warp(const FactorArgs &a, uint32_t b, int lane, const T *__restrict__ vf,
-                                            T *__restrict__ fv) {
-    const uint32_t fi = a.nf_sell + b;
-    if (a.f_graph && a.gdone[a.f_graph[fi]]) return;  // batched solve: its graph has stopped
-    const uint32_t s0 = a.fb_off[b], s1 = s0 + a.fb_deg[b];
-    const T *pq = reinterpret_cast<const T *>(a.f_pq);
-    factor_warp_loop<T>(a, s0, s1, a.f_kind[fi], pq[2 * fi], pq[2 * fi + 1], lane, vf, fv);
 }
 
 // Item `wid` of a staged big tile: dispatch on its body size.
@@ -819,9 +832,11 @@ __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArg
         return;
     }
 
-    {  // factors too large for a tile first, while the producer's first loads are in flight
-        const uint32_t warp = blockIdx.x * kConsumerWarps + wid, nwarps = gridDim.x * kConsumerWarps;
-        for (uint32_t b = warp; b < a.nf_huge; b += nwarps) factor_warp<T>(a, b, lane, vf, fv);
+    {  // factors too large for a tile first, one per block, while the producer's first loads are in flight
+        __shared__ double s_l[kConsumerWarps];
+        __shared__ int s_nz[kConsumerWarps];
+        for (uint32_t b = blockIdx.x; b < a.nf_huge; b += gridDim.x)
+            factor_block_huge<T>(a, b, threadIdx.x, vf, fv, s_l, s_nz);
     }
     for (uint32_t it = 0;; it++) {
         const int s = (int)(it % STAGES);
@@ -980,16 +995,23 @@ __device__ __forceinline__ double var_tile_big(const VarArgs &a, uint32_t v, uin
     return (lane == 0) ? var_finish<BMODE>(a, v, S, npos, nneg, tol, RESID ? a.belief[v] : 0.0, cnt) : 0.0;
 }
 
-// Larger variables: lanes stride over the entries, reading them twice.
+// A variable too large for a tile (big variable b, internal index
+// nv_sell + b), spread over all consumer threads of a block (called by all
+// of them): FP64 sum with +-inf counts reduced over the block in a fixed
+// order, then every entry's leave-one-out message. Returns the belief change
+// on thread 0 (0 elsewhere).
 template <typename T, int BMODE, bool WRITE_VF, bool DAMP>
-__device__ __noinline__ double var_warp_loop(const VarArgs &a, uint32_t v, uint32_t k0, uint32_t k1, int lane,
-                                             const T *__restrict__ fv, T *__restrict__ vf, T *__restrict__ fvd, T d,
-                                             double pscale, double tol, unsigned long long &cnt) {
+__device__ double var_block_huge(const VarArgs &a, uint32_t b, int tid, const T *__restrict__ fv,
+                                 T *__restrict__ vf, T *__restrict__ fvd, T d, double pscale, double tol,
+                                 unsigned long long &cnt, double *s_s, int *s_np, int *s_nn) {
+    constexpr bool RESID = (BMODE == 1 || BMODE == 2 || BMODE == 4);
+    const uint32_t v = a.nv_sell + b, k0 = a.vb_off[b], k1 = k0 + a.vb_deg[b];
     const T inf = Num<T>::inf();
     const T *src = DAMP ? fvd : fv;  // after the first loop, fvd holds the messages in use
+    const int lane = tid & 31, wid = tid >> 5;
     double S = 0.0;
     int npos = 0, nneg = 0;
-    for (uint32_t k = k0 + lane; k < k1; k += 32) {
+    for (uint32_t k = k0 + tid; k < k1; k += kConsumers) {
         T x = fv[k];
         if (DAMP) {
             x = take_fv<T, DAMP>(x, fvd[k], d);
@@ -1005,6 +1027,20 @@ __device__ __noinline__ double var_warp_loop(const VarArgs &a, uint32_t v, uint3
         npos += __shfl_xor_sync(0xffffffffu, npos, o);
         nneg += __shfl_xor_sync(0xffffffffu, nneg, o);
     }
+    if (lane == 0) {
+        s_s[wid] = S;
+        s_np[wid] = npos;
+        s_nn[wid] = nneg;
+    }
+    consumer_sync();
+    S = 0.0;
+    npos = nneg = 0;
+    for (int w = 0; w < kConsumerWarps; w++) {
+        S += s_s[w];
+        npos += s_np[w];
+        nneg += s_nn[w];
+    }
+    consumer_sync();  // the partials are reused by the next variable
     double S0;
     int p0, n0;
     decode_prior<T>(a.prior, v, pscale, S0, p0, n0);
@@ -1012,22 +1048,12 @@ __device__ __noinline__ double var_warp_loop(const VarArgs &a, uint32_t v, uint3
     npos += p0;
     nneg += n0;
     if (WRITE_VF) {
-        for (uint32_t k = k0 + lane; k < k1; k += 32) {
+        for (uint32_t k = k0 + tid; k < k1; k += kConsumers) {
             const uint32_t e = a.v_ent[k];
             if (e != kSentinel) vf[e] = excl_msg<T>(S, npos, nneg, src[k]);
         }
     }
-    return (lane == 0) ? var_finish<BMODE>(a, v, S, npos, nneg, tol, a.belief[v], cnt) : 0.0;
-}
-
-// Big variable b (internal index nv_sell + b) too large for a tile, one warp.
-template <typename T, int BMODE, bool WRITE_VF, bool DAMP>
-__device__ __forceinline__ double var_warp(const VarArgs &a, uint32_t b, int lane, const T *__restrict__ fv,
-                                           T *__restrict__ vf, T *__restrict__ fvd, T d, double pscale, double tol,
-                                           unsigned long long &cnt) {
-    const uint32_t k0 = a.vb_off[b];
-    return var_warp_loop<T, BMODE, WRITE_VF, DAMP>(a, a.nv_sell + b, k0, k0 + a.vb_deg[b], lane, fv, vf, fvd, d, pscale,
-                                                   tol, cnt);
+    return (tid == 0) ? var_finish<BMODE>(a, v, S, npos, nneg, tol, RESID ? a.belief[v] : 0.0, cnt) : 0.0;
 }
 
 __device__ __forceinline__ double warp_max(double x) {
@@ -1208,12 +1234,14 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
         produce_tiles<STAGES>(a.thdr, a.v_graph ? a.trange : nullptr, s_done, a.gstate, n_tiles, &ctl->vnext, smem,
                               VS::bytes, full, empty, lane, ctl, fill);
     } else {  // consumer warps: variables too large for a tile first
-        {
-            const uint32_t warp = blockIdx.x * kConsumerWarps + wid, nwarps = gridDim.x * kConsumerWarps;
-            for (uint32_t b = warp; b < a.nv_huge; b += nwarps) {
+        {  // one per block
+            __shared__ double s_s[kConsumerWarps];
+            __shared__ int s_np[kConsumerWarps], s_nn[kConsumerWarps];
+            for (uint32_t b = blockIdx.x; b < a.nv_huge; b += gridDim.x) {
                 const uint32_t g = a.v_graph ? a.v_graph[a.nv_sell + b] : 0;
                 if (a.v_graph && graph_done(s_done, a.gstate, g)) continue;  // stopped graph (batched solve)
-                const double dd = var_warp<T, BMODE, WRITE_VF, DAMP>(a, b, lane, fv, vf, fvd, d, pscale, tol, cnt);
+                const double dd = var_block_huge<T, BMODE, WRITE_VF, DAMP>(a, b, threadIdx.x, fv, vf, fvd, d, pscale,
+                                                                           tol, cnt, s_s, s_np, s_nn);
                 dmax = fmax(dmax, dd);
                 if (BMODE == 4 && dd > tol) mark_moved(s_moved, a, g);
             }

@@ -221,3 +221,32 @@ def test_large_items(prec, damping):
     eng.init()
     eng.run_fixed(40)
     assert np.max(np.abs(eng.beliefs() - bp.beliefs())) <= TOL[prec]
+
+
+def test_fault_localisation_statement_ranking():
+    """cfg2 shape at reduced size: tolerance run (tol 1e-6, maxiter 500) in
+    FP32 against the FP64 oracle. Beliefs within the FP32 tolerance, and the
+    ranking of the statements (the input tuples) by belief agrees: Spearman
+    correlation >= 0.999, and every pair of statements whose oracle beliefs
+    differ by more than twice the tolerance is ordered the same way."""
+    from scipy.stats import spearmanr
+
+    fl, cl = workloads.config2(seed=6, scale=0.02)
+    g, og = _pair(fl, cl)
+    eng = Engine.from_graph(g, precision=32)
+    eng.init()
+    info = eng.run_tol(1e-6, 500, 1e9)
+    bp = O.OracleBP(og)
+    bp.init()
+    bp.run(1e-6, 500, 1e9)
+    b, bo = eng.beliefs(), bp.beliefs()
+    assert np.max(np.abs(b - bo)) <= TOL[32]
+    assert abs(info["sweeps"] - bp.iters) <= 2
+    labels = g.var_labels()
+    stm = np.nonzero(labels < fl.info["n_inputs"])[0]
+    assert stm.size > 20
+    assert spearmanr(b[stm], bo[stm]).statistic >= 0.999
+    d_o = bo[stm][:, None] - bo[stm][None, :]
+    d_e = b[stm][:, None] - b[stm][None, :]
+    sure = np.abs(d_o) > 2 * TOL[32]
+    assert np.all(np.sign(d_e[sure]) == np.sign(d_o[sure]))

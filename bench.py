@@ -240,6 +240,16 @@ def run_fl(args, rank, world, local):
     bp.run(1e-6, 500, 1e9)
     t_cpu = time.perf_counter() - t0
     bo = bp.beliefs()
+    # the same comparison after a few sweeps, before any chaotic growth of rounding differences
+    e10 = Engine(arr, precision=args.precision)
+    e10.init()
+    e10.run_fixed(10)
+    b10 = e10.beliefs()
+    e10.close()
+    bp10 = O.OracleBP(og, threads=os.cpu_count() or 1)
+    bp10.init()
+    bp10.run_fixed(1e-6, 10, 1)
+    err10 = float(np.nanmax(np.abs(b10 - bp10.lowpass())))
     labels = g.var_labels()
     stm = np.searchsorted(labels, np.arange(int(fl.info["n_inputs"])))
     stm = stm[(stm < labels.size)]
@@ -262,6 +272,8 @@ def run_fl(args, rank, world, local):
             "max_belief_error_vs_fp64_oracle": float(np.nanmax(np.abs(b - bo))),
             "belief_error_quantiles": {str(qq): float(np.nanquantile(np.abs(b - bo), qq)) for qq in (0.5, 0.99, 0.999)},
             "vars_off_by_more_than_1e-5": int(np.sum(np.abs(b - bo) > 1e-5)),
+            "max_belief_error_after_10_sweeps": err10,
+            "oracle_final_residual_converged": bool(bp.iters < 500),
             "nan_beliefs": {"engine": int(np.isnan(b).sum()), "oracle": int(np.isnan(bo).sum()),
                             "same_positions": bool(np.array_equal(np.isnan(b), np.isnan(bo)))},
             "ranking": dict(statements=int(stm.size), spearman=rho, **top),

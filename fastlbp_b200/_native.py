@@ -107,6 +107,9 @@ def lib():
         "flbp_batch_create": [P(GraphDesc), C.c_int64, P(EngineOpts), P(_vp)],
         "flbp_batch_info": [_vp, P(C.c_int64), _i64p],
         "flbp_batch_run_tol": [_vp, C.c_double, C.c_int64, C.c_double, _i64p, _i32p, P(RunInfo)],
+        "flbp_adjoint_forward": [_vp, C.c_int64, C.c_int64, _f64p, C.c_int64],
+        "flbp_adjoint_backward": [_vp, _f64p, _f64p, _f64p],
+        "flbp_set_factor_probs": [_vp, _f64p, _f64p],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -132,4 +135,4 @@ EXPORTED = ["flbp_last_error", "flbp_version", "flbp_engine_create", "flbp_engin
             "flbp_fg_from_factors", "flbp_fg_destroy", "flbp_fg_clamp", "flbp_fg_rebuild", "flbp_fg_sizes",
             "flbp_fg_var_labels", "flbp_fg_factors", "flbp_fg_neighbors", "flbp_fg_construct",
             "flbp_engine_create_from_fg", "flbp_run_fixed_device_noalloc", "flbp_batch_create", "flbp_batch_info",
-            "flbp_batch_run_tol"]
+            "flbp_batch_run_tol", "flbp_adjoint_forward", "flbp_adjoint_backward", "flbp_set_factor_probs"]

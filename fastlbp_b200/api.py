@@ -203,6 +203,7 @@ class Engine:
         self._h = h
         self.n_vars = int(desc.n_vars)
         self.n_slots = int(desc.n_slots)
+        self.n_factors = int(desc.n_factors)
         self.info = None
 
     @classmethod
@@ -272,6 +273,25 @@ class Engine:
                 "h2d_bytes", "launches", "huge_factors", "huge_vars", "big_factor_tiles", "big_var_tiles"]
         return dict(zip(keys, (int(x) for x in c)))
 
+    # gradients through unrolled sweeps --------------------------------------
+    def adjoint_forward(self, sweeps: int, every: int) -> np.ndarray:
+        """init() and `sweeps` sweeps with checkpoints every `every`; the beliefs."""
+        out = np.zeros(self.n_vars)
+        check(lib().flbp_adjoint_forward(self._h, int(sweeps), int(every), out, out.size))
+        return out
+
+    def adjoint_backward(self, grad_beliefs: np.ndarray):
+        """dL/dp and dL/dq of every factor (reference order) for dL/dbeliefs."""
+        g = np.ascontiguousarray(grad_beliefs, np.float64)
+        gp = np.zeros(self.n_factors)
+        gq = np.zeros(self.n_factors)
+        check(lib().flbp_adjoint_backward(self._h, g, gp, gq))
+        return gp, gq
+
+    def set_factor_probs(self, p: np.ndarray, q: np.ndarray) -> None:
+        check(lib().flbp_set_factor_probs(self._h, np.ascontiguousarray(p, np.float64),
+                                          np.ascontiguousarray(q, np.float64)))
+
     def set_kernel_timing(self, enable: bool) -> None:
         check(lib().flbp_set_kernel_timing(self._h, 1 if enable else 0))
 
@@ -309,6 +329,7 @@ class BatchEngine(Engine):
         check(lib().flbp_batch_info(h, C.byref(ng), self.var_off))
         self.n_vars = int(self.var_off[-1])
         self.n_slots = int(sum(int(d.n_slots) for d in descs))
+        self.n_factors = int(sum(int(d.n_factors) for d in descs))
         self.info = None
 
     def run_batch_tol(self, tol=1e-6, maxiter=500, maxtime=1e9):

@@ -16,6 +16,7 @@
 
 #include "engine_internal.h"
 #include "kernels.cuh"
+#include "adjoint.cuh"
 
 namespace flbp {
 
@@ -65,6 +66,14 @@ struct flbp_engine {
     uint32_t *d_f_graph = nullptr, *d_v_graph = nullptr;  // internal factor / variable -> graph
     int *d_gstate = nullptr;  // [4][n_graphs]: stopped, moved, sweeps, stop reason
     uint2 *d_ftrange = nullptr, *d_vtrange = nullptr;  // per tile: range of its items' graphs
+    // Adjoint: checkpoints of vf every adj_k sweeps of the last adjoint forward
+    // run (adj_t sweeps), per-sweep states of one segment, and derivatives.
+    long long adj_t = 0, adj_k = 0;
+    void *d_ckpt = nullptr, *d_seg_vf = nullptr, *d_seg_fv = nullptr;
+    double *d_lam = nullptr, *d_lam2 = nullptr, *d_mu = nullptr, *d_gp = nullptr, *d_gq = nullptr;
+    double *d_gprior = nullptr, *d_gs = nullptr;
+    size_t adj_ckpt_n = 0, adj_seg_n = 0;
+    std::vector<double> factor_p_host;  // every reference factor's p (for derivatives of folded constants)
     uint8_t *d_f_kind = nullptr, *d_f_deg = nullptr;
     void *d_prior = nullptr;
     double *d_belief = nullptr, *d_lowpass = nullptr, *d_hist = nullptr;
@@ -461,6 +470,35 @@ extern "C" int flbp_engine_create(const flbp_graph_desc *graph, const flbp_engin
 
 namespace {
 
+// Device words of the per-variable priors (finite part, +-inf counts) and of
+// the big-tile copies of them.
+void packed_priors(const flbp_engine *e, size_t nv_pad, std::vector<uint32_t> &prior, std::vector<uint32_t> &bt_prior) {
+    const HostLayout &L = e->L;
+    const size_t psz = e->prec == 64 ? 16 : 8;
+    prior.assign(std::max<size_t>(1, nv_pad) * (psz / 4), 0u);
+    for (int64_t i = 0; i < L.V; i++) {
+        if (e->prec == 64) {
+            std::memcpy(&prior[4 * i], &L.prior_fin[i], 8);
+            prior[4 * i + 2] = L.prior_cnt[i];
+        } else {
+            const float f = (float)L.prior_fin[i];
+            std::memcpy(&prior[2 * i], &f, 4);
+            prior[2 * i + 1] = L.prior_cnt[i];
+        }
+    }
+    // priors of the variables of every big tile, in tile order
+    bt_prior.assign(std::max<size_t>(1, L.vbt_deg.size()) * (psz / 4), 0u);
+    for (uint32_t t = 0; t < L.n_vbtiles; t++) {
+        const uint32_t *h = &L.vhdr[(size_t)kHdrWordsHost * t];
+        const uint32_t b0 = h[0], n = h[1] & ~kBigTileFlag;
+        for (uint32_t j = 0; j < n; j++) {
+            const size_t k = (size_t)kTileGroupsHost * t + j, iv = (size_t)L.nv_sell + b0 + j;
+            std::copy(&prior[iv * (psz / 4)], &prior[(iv + 1) * (psz / 4)], &bt_prior[k * (psz / 4)]);
+        }
+    }
+    bt_prior.resize(L.vbt_deg.size() * (psz / 4));
+}
+
 int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, flbp_engine **out,
                   const BatchSpec *batch) {
     if (!graph || !out) {
@@ -492,6 +530,7 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
         delete e;
         return rc;
     }
+    if (graph->n_factors > 0 && graph->factor_p) e->factor_p_host.assign(graph->factor_p, graph->factor_p + graph->n_factors);
     e->prec = o.precision;
     e->tsize = o.precision == 64 ? 8 : 4;
     e->damping = o.damping;
@@ -584,28 +623,8 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
         return fail(FLBP_ERR_NOMEM);
     }
     std::memset(e->h_ctl, 0, sizeof(Ctl));
-    std::vector<uint32_t> prior(std::max<size_t>(1, nv_pad) * (psz / 4), 0u);
-    for (int64_t i = 0; i < L.V; i++) {
-        if (e->prec == 64) {
-            std::memcpy(&prior[4 * i], &L.prior_fin[i], 8);
-            prior[4 * i + 2] = L.prior_cnt[i];
-        } else {
-            const float f = (float)L.prior_fin[i];
-            std::memcpy(&prior[2 * i], &f, 4);
-            prior[2 * i + 1] = L.prior_cnt[i];
-        }
-    }
-    // priors of the variables of every big tile, in tile order
-    std::vector<uint32_t> bt_prior(std::max<size_t>(1, L.vbt_deg.size()) * (psz / 4), 0u);
-    for (uint32_t t = 0; t < L.n_vbtiles; t++) {
-        const uint32_t *h = &L.vhdr[(size_t)kHdrWordsHost * t];
-        const uint32_t b0 = h[0], n = h[1] & ~kBigTileFlag;
-        for (uint32_t j = 0; j < n; j++) {
-            const size_t k = (size_t)kTileGroupsHost * t + j, iv = (size_t)L.nv_sell + b0 + j;
-            std::copy(&prior[iv * (psz / 4)], &prior[(iv + 1) * (psz / 4)], &bt_prior[k * (psz / 4)]);
-        }
-    }
-    bt_prior.resize(L.vbt_deg.size() * (psz / 4));
+    std::vector<uint32_t> prior, bt_prior;
+    packed_priors(e, nv_pad, prior, bt_prior);
     std::vector<uint8_t> kind_pad(nf_pad, 0), deg_pad(nf_pad, 0);
     std::copy(L.f_kind.begin(), L.f_kind.end(), kind_pad.begin());
     std::copy(L.f_deg.begin(), L.f_deg.end(), deg_pad.begin());
@@ -680,7 +699,9 @@ int flbp_engine_destroy(flbp_engine *e) {
                     e->d_f_deg,  e->d_vg_base,  e->d_vb_off, e->d_v_ent,     e->d_prior,      e->d_belief,
                     e->d_lowpass, e->d_hist,    e->d_hist_next, e->d_hist_count, e->d_ctl,    e->d_scratch,
                     e->d_ftiles, e->d_vtiles,  e->d_fb_deg, e->d_vb_deg, e->d_fbt_deg, e->d_vbt_deg,
-                    e->d_fbt_kind, e->d_fbt_pq, e->d_vbt_prior, e->d_f_graph, e->d_v_graph, e->d_gstate, e->d_ftrange, e->d_vtrange};
+                    e->d_fbt_kind, e->d_fbt_pq, e->d_vbt_prior, e->d_f_graph, e->d_v_graph, e->d_gstate, e->d_ftrange, e->d_vtrange,
+                    e->d_ckpt, e->d_seg_vf, e->d_seg_fv, e->d_lam, e->d_lam2, e->d_mu, e->d_gp, e->d_gq,
+                    e->d_gprior, e->d_gs};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (e->h_ctl) cudaFreeHost(e->h_ctl);
@@ -1131,6 +1152,233 @@ int flbp_batch_run_tol(flbp_engine *e, double tol, int64_t maxiter, double maxti
     e->t += done_sweeps;
     e->iters += done_sweeps;
     fill_info(e, info, done_sweeps, l0);
+    return FLBP_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ adjoint
+
+namespace {
+
+AdjArgs adj_args(flbp_engine *e) {
+    AdjArgs a;
+    a.fg_base = e->d_fg_base;
+    a.fb_off = e->d_fb_off;
+    a.fb_deg = e->d_fb_deg;
+    a.f_pos = e->d_f_pos;
+    a.f_kind = e->d_f_kind;
+    a.f_deg = e->d_f_deg;
+    a.f_pq = e->d_f_pq;
+    a.nf_sell = e->L.nf_sell;
+    a.nf_big = e->L.nf_big;
+    a.vg_base = e->d_vg_base;
+    a.vb_off = e->d_vb_off;
+    a.vb_deg = e->d_vb_deg;
+    a.v_ent = e->d_v_ent;
+    a.prior = e->d_prior;
+    a.nv_sell = e->L.nv_sell;
+    a.nv_big = e->L.nv_big;
+    return a;
+}
+
+template <typename T>
+void launch_adjoint_step(flbp_engine *e, const void *vf, const void *fv, const double *lam_next, const double *gs,
+                         double *lam) {
+    const AdjArgs a = adj_args(e);
+    const uint32_t nv = a.nv_sell + a.nv_big;
+    if (nv) var_adjoint_kernel<T><<<(nv + 127) / 128, 128, 0, e->stream>>>(a, (const T *)fv, lam_next, gs, e->d_mu,
+                                                                           e->d_gprior);
+    cudaMemsetAsync(lam, 0, std::max<uint64_t>(1, e->L.n_slots) * sizeof(double), e->stream);
+    if (a.nf_sell)
+        factor_adjoint_sell_kernel<T><<<(a.nf_sell + 127) / 128, 128, 0, e->stream>>>(a, (const T *)vf, e->d_mu, lam,
+                                                                                       e->d_gp, e->d_gq);
+    if (a.nf_big)
+        factor_adjoint_big_kernel<T><<<(a.nf_big + 3) / 4, 128, 0, e->stream>>>(a, (const T *)vf, e->d_mu, lam, e->d_gp,
+                                                                                 e->d_gq);
+    e->launches += 2 + (a.nf_big ? 1 : 0);
+}
+
+}  // namespace
+
+extern "C" {
+
+int flbp_adjoint_forward(flbp_engine *e, int64_t sweeps, int64_t every, double *beliefs, int64_t n) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    if (e->damping != 0.0) {
+        set_error("the adjoint needs an engine without damping");
+        return FLBP_ERR_INVALID;
+    }
+    if (sweeps < 1 || every < 1) {
+        set_error("sweeps and checkpoint interval must be positive");
+        return FLBP_ERR_INVALID;
+    }
+    const size_t ns = std::max<uint64_t>(1, e->L.n_slots), ne = e->n_ent;
+    const size_t nck = (size_t)((sweeps + every - 1) / every);
+    const size_t nseg = (size_t)std::min<int64_t>(every, sweeps);
+    if (nck > e->adj_ckpt_n) {
+        if (e->d_ckpt) cudaFree(e->d_ckpt);
+        e->d_ckpt = nullptr;
+        if ((rc = dalloc(e, (char **)&e->d_ckpt, nck * ns * e->tsize))) return rc;
+        e->adj_ckpt_n = nck;
+    }
+    if (nseg > e->adj_seg_n) {
+        if (e->d_seg_vf) cudaFree(e->d_seg_vf);
+        if (e->d_seg_fv) cudaFree(e->d_seg_fv);
+        e->d_seg_vf = e->d_seg_fv = nullptr;
+        if ((rc = dalloc(e, (char **)&e->d_seg_vf, nseg * ns * e->tsize)) ||
+            (rc = dalloc(e, (char **)&e->d_seg_fv, nseg * ne * e->tsize)))
+            return rc;
+        e->adj_seg_n = nseg;
+    }
+    if ((rc = flbp_init(e))) return rc;
+    reset_ctl_for_run(e, 0);
+    if ((rc = upload_ctl(e))) return rc;
+    for (size_t c = 0; c < nck; c++) {
+        FLBP_CUDA(cudaMemcpyAsync((char *)e->d_ckpt + c * ns * e->tsize, e->d_vf, ns * e->tsize,
+                                  cudaMemcpyDeviceToDevice, e->stream));
+        const long long n1 = std::min<long long>(every, sweeps - (long long)c * every);
+        if ((rc = launch_sweeps(e, 0, n1))) return rc;
+    }
+    launch_beliefs_only(e, e->d_belief);
+    if ((rc = download_ctl(e))) return rc;
+    e->t += sweeps;
+    e->iters += sweeps;
+    e->adj_t = sweeps;
+    e->adj_k = every;
+    if (beliefs) return fetch_internal(e, e->d_belief, beliefs, n);
+    return FLBP_OK;
+}
+
+int flbp_adjoint_backward(flbp_engine *e, const double *grad_beliefs, double *grad_p, double *grad_q) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    if (e->adj_t == 0) {
+        set_error("no adjoint forward run to differentiate (call flbp_adjoint_forward first)");
+        return FLBP_ERR_INVALID;
+    }
+    const HostLayout &L = e->L;
+    const size_t ns = std::max<uint64_t>(1, L.n_slots), ne = e->n_ent, nv = std::max<int64_t>(1, L.V);
+    const size_t nf = std::max<size_t>(1, (size_t)L.nf_sell + L.nf_big);
+    if (!e->d_lam &&
+        ((rc = dalloc(e, &e->d_lam, ns)) || (rc = dalloc(e, &e->d_lam2, ns)) || (rc = dalloc(e, &e->d_mu, ne)) ||
+         (rc = dalloc(e, &e->d_gp, nf)) || (rc = dalloc(e, &e->d_gq, nf)) || (rc = dalloc(e, &e->d_gprior, nv)) ||
+         (rc = dalloc(e, &e->d_gs, nv))))
+        return rc;
+    // dL/dS_v = dL/db_v * b (1 - b) at the final beliefs
+    std::vector<double> b(nv, 0.0), gs(nv, 0.0);
+    if (L.V) {
+        FLBP_CUDA(cudaMemcpyAsync(b.data(), e->d_belief, (size_t)L.V * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+        FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    }
+    for (int64_t i = 0; i < L.V; i++) {
+        const uint32_t iv = L.internal_of_var[i];
+        const double g = grad_beliefs ? grad_beliefs[i] : 0.0;
+        gs[iv] = std::isfinite(b[iv]) ? g * b[iv] * (1.0 - b[iv]) : 0.0;
+    }
+    if ((rc = upload(e, e->d_gs, gs))) return rc;
+    FLBP_CUDA(cudaMemsetAsync(e->d_gp, 0, nf * sizeof(double), e->stream));
+    FLBP_CUDA(cudaMemsetAsync(e->d_gq, 0, nf * sizeof(double), e->stream));
+    FLBP_CUDA(cudaMemsetAsync(e->d_gprior, 0, nv * sizeof(double), e->stream));
+    FLBP_CUDA(cudaMemsetAsync(e->d_lam, 0, ns * sizeof(double), e->stream));
+    reset_ctl_for_run(e, 0);
+    if ((rc = upload_ctl(e))) return rc;
+    const long long T = e->adj_t, K = e->adj_k;
+    const long long nck = (T + K - 1) / K;
+    double *lam_next = e->d_lam, *lam_cur = e->d_lam2;
+    for (long long c = nck - 1; c >= 0; c--) {
+        const long long t0 = c * K, n1 = std::min<long long>(K, T - t0);
+        // recompute the segment's states from its checkpoint
+        FLBP_CUDA(cudaMemcpyAsync(e->d_vf, (char *)e->d_ckpt + (size_t)c * ns * e->tsize, ns * e->tsize,
+                                  cudaMemcpyDeviceToDevice, e->stream));
+        for (long long i = 0; i < n1; i++) {
+            FLBP_CUDA(cudaMemcpyAsync((char *)e->d_seg_vf + (size_t)i * ns * e->tsize, e->d_vf, ns * e->tsize,
+                                      cudaMemcpyDeviceToDevice, e->stream));
+            launch_sweep_any(e, 0, 1);
+            FLBP_CUDA(cudaMemcpyAsync((char *)e->d_seg_fv + (size_t)i * ne * e->tsize, e->d_fv, ne * e->tsize,
+                                      cudaMemcpyDeviceToDevice, e->stream));
+            launch_sweep_any(e, 0, 2);
+            e->launches += 2;
+        }
+        for (long long i = n1 - 1; i >= 0; i--) {
+            const void *vf = (char *)e->d_seg_vf + (size_t)i * ns * e->tsize;
+            const void *fv = (char *)e->d_seg_fv + (size_t)i * ne * e->tsize;
+            const double *gsp = (t0 + i == T - 1) ? e->d_gs : nullptr;
+            if (e->prec == 64) launch_adjoint_step<double>(e, vf, fv, lam_next, gsp, lam_cur);
+            else launch_adjoint_step<float>(e, vf, fv, lam_next, gsp, lam_cur);
+            std::swap(lam_next, lam_cur);
+        }
+    }
+    FLBP_CUDA(cudaGetLastError());
+    if ((rc = download_ctl(e))) return rc;
+    std::vector<double> gp(nf), gq(nf), gpr(nv);
+    FLBP_CUDA(cudaMemcpyAsync(gp.data(), e->d_gp, nf * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    FLBP_CUDA(cudaMemcpyAsync(gq.data(), e->d_gq, nf * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    FLBP_CUDA(cudaMemcpyAsync(gpr.data(), e->d_gprior, nv * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    for (int64_t I = 0; I < L.F; I++) {
+        if (grad_p) grad_p[I] = 0.0;
+        if (grad_q) grad_q[I] = 0.0;
+    }
+    for (uint32_t f = 0; f < L.nf_sell + L.nf_big; f++) {
+        const uint32_t I = L.factor_of_internal[f];
+        if (grad_p) grad_p[I] += gp[f];
+        if (grad_q) grad_q[I] += gq[f];
+    }
+    // folded constants sign * logit(p): d/dp = sign / (p (1 - p))
+    for (size_t k = 0; k < L.prior_factor.size(); k++) {
+        const uint32_t I = L.prior_factor[k];
+        const double p = e->factor_p_host.empty() ? 0.5 : e->factor_p_host[I];
+        if (grad_p && p > 0.0 && p < 1.0) grad_p[I] += gpr[L.prior_var[k]] * L.prior_sign[k] / (p * (1.0 - p));
+    }
+    return FLBP_OK;
+}
+
+int flbp_set_factor_probs(flbp_engine *e, const double *p, const double *q) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    HostLayout &L = e->L;
+    for (int64_t I = 0; I < L.F; I++) {
+        if (!(p[I] >= 0.0 && p[I] <= 1.0) || !(q[I] >= 0.0 && q[I] <= 1.0)) {
+            set_error("factor probabilities must lie in [0,1] (factor " + std::to_string(I) + ")");
+            return FLBP_ERR_INVALID;
+        }
+    }
+    e->factor_p_host.assign(p, p + L.F);
+    const uint32_t nf = L.nf_sell + L.nf_big;
+    for (uint32_t f = 0; f < nf; f++) {
+        L.f_pq[2 * f] = p[L.factor_of_internal[f]];
+        L.f_pq[2 * f + 1] = q[L.factor_of_internal[f]];
+    }
+    for (uint32_t t = 0; t < L.n_fbtiles; t++) {
+        const uint32_t *h = &L.fhdr[(size_t)kHdrWordsHost * t];
+        for (uint32_t j = 0; j < (h[1] & ~kBigTileFlag); j++) {
+            const size_t k = (size_t)kTileGroupsHost * t + j, fi = (size_t)L.nf_sell + h[0] + j;
+            L.fbt_pq[2 * k] = L.f_pq[2 * fi];
+            L.fbt_pq[2 * k + 1] = L.f_pq[2 * fi + 1];
+        }
+    }
+    std::fill(L.prior_fin.begin(), L.prior_fin.end(), 0.0);
+    for (size_t k = 0; k < L.prior_factor.size(); k++) {
+        const double pk = p[L.prior_factor[k]];
+        L.prior_fin[L.prior_var[k]] += L.prior_sign[k] * (std::log(pk) - std::log1p(-pk));
+    }
+    const size_t nf_pad = std::max<size_t>(nf, 32ull * L.n_fgroups());
+    const size_t nv_pad = std::max<size_t>((size_t)L.V, 32ull * L.n_vgroups());
+    std::vector<double> pq64(2 * nf_pad, 0.0);
+    std::copy(L.f_pq.begin(), L.f_pq.end(), pq64.begin());
+    if (e->prec == 64) {
+        if ((rc = upload(e, (double *)e->d_f_pq, pq64)) || (rc = upload(e, (double *)e->d_fbt_pq, L.fbt_pq))) return rc;
+    } else {
+        std::vector<float> a(pq64.begin(), pq64.end()), b(L.fbt_pq.begin(), L.fbt_pq.end());
+        if ((rc = upload(e, (float *)e->d_f_pq, a)) || (rc = upload(e, (float *)e->d_fbt_pq, b))) return rc;
+    }
+    std::vector<uint32_t> prior, bt_prior;
+    packed_priors(e, nv_pad, prior, bt_prior);
+    if ((rc = upload(e, (uint32_t *)e->d_prior, prior)) || (rc = upload(e, (uint32_t *)e->d_vbt_prior, bt_prior)))
+        return rc;
+    FLBP_CUDA(cudaStreamSynchronize(e->stream));
     return FLBP_OK;
 }
 

@@ -78,6 +78,10 @@ struct HostLayout {
     std::vector<uint32_t> f_pos;       // per slot: entry of its f->v message (kSentinel: none)
     std::vector<double> prior_fin;     // per internal variable: finite constant log-odds (damping-scaled)
     std::vector<uint32_t> prior_cnt;   // per internal variable: (#+inf) | (#-inf << 16)
+    // The finite constant messages folded into prior_fin: reference factor,
+    // internal variable and sign (the constant is sign * logit(p)).
+    std::vector<uint32_t> prior_factor, prior_var;
+    std::vector<int8_t> prior_sign;
     std::vector<uint32_t> var_of_internal;  // internal variable -> reference variable
     std::vector<uint32_t> factor_of_internal;  // internal (active) factor -> reference factor
     std::vector<uint32_t> internal_of_var;  // reference variable -> internal variable

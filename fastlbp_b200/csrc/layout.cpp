@@ -454,6 +454,10 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
                 if ((L.prior_cnt[iv] >> 16) != 0xffffu) L.prior_cnt[iv] += 1u << 16;
             } else {
                 fin[iv] += c;
+                // finite constant: +-logit(p) of a singleton or of an AND/OR factor reduced to its head
+                L.prior_factor.push_back((uint32_t)I);
+                L.prior_var.push_back(iv);
+                L.prior_sign.push_back(g.factor_type[I] == FLBP_OR ? -1 : 1);
             }
         }
         L.prior_fin = fin;

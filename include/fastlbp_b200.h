@@ -287,6 +287,25 @@ int flbp_batch_info(flbp_engine *eng, int64_t *n_graphs, int64_t *var_off);
 int flbp_batch_run_tol(flbp_engine *eng, double tol, int64_t maxiter, double maxtime, int64_t *sweeps,
                        int32_t *reasons, flbp_run_info *info);
 
+/* ---- gradients through unrolled sweeps (no counterpart in the reference) ----
+ *
+ * flbp_adjoint_forward: init() and `sweeps` synchronous sweeps (engines
+ * without damping), keeping the v->f messages every `every` sweeps; writes
+ * the beliefs after the last sweep (n = number of variables; may be NULL).
+ * flbp_adjoint_backward: given dL/dbelief for every variable, the gradient
+ * of L with respect to every factor's p and q (reference factor order; NULL
+ * allowed), by reversing the sweeps of the last forward run: each segment
+ * between checkpoints is recomputed, then the adjoint kernels run backwards
+ * through it. Singleton priors and AND/OR factors reduced to their head get
+ * their p gradient through the folded constant logit(p). */
+int flbp_adjoint_forward(flbp_engine *eng, int64_t sweeps, int64_t every, double *beliefs, int64_t n);
+int flbp_adjoint_backward(flbp_engine *eng, const double *grad_beliefs, double *grad_p, double *grad_q);
+
+/* New p and q for every factor (reference order) of an existing engine, e.g.
+ * after a learning step: constants folded into priors follow. The graph's
+ * structure (which factors are singletons, clamped or reduced) stays. */
+int flbp_set_factor_probs(flbp_engine *eng, const double *p, const double *q);
+
 #ifdef __cplusplus
 }
 #endif

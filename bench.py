@@ -55,10 +55,14 @@ def parse():
     ap.add_argument("--scale", type=float, default=1.0, help="graph size factor (1.0 = the 1M-variable graph)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "fl"],
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "fl", "adjoint"],
                     help="single: the 1M-variable graph (default); batch: many uneven graphs solved together; "
-                         "fl: the fault-localisation graph with its statement ranking against the FP64 oracle")
-    ap.add_argument("--graphs", type=int, default=512, help="batch workload: number of graphs")
+                         "fl: the fault-localisation graph with its statement ranking against the FP64 oracle; "
+                         "adjoint: gradients through unrolled sweeps on 64 graphs of 50k tuples "
+                         "(use --sweeps 100 --damping 0 --graphs 64)")
+    ap.add_argument("--graphs", type=int, default=512, help="batch / adjoint workloads: number of graphs")
+    ap.add_argument("--every", type=int, default=10, help="adjoint workload: checkpoint interval")
+    ap.add_argument("--fd-params", type=int, default=1000, help="adjoint workload: parameters checked by differences")
     return ap.parse_args()
 
 
@@ -194,6 +198,186 @@ def run_batch(args, rank, world, local):
     for e in plain:
         e.close()
     return line
+
+
+def adjoint_graph_arrays(i):
+    """Reference-order arrays of graph i of the gradient set, with the
+    variable indices and labels of its labelled alarms (cached)."""
+    from fastlbp_b200 import CausalFactorGraph, workloads
+
+    cache = os.path.join(tempfile.gettempdir(), "fastlbp_b200_cfg4_s4_g%d.npz" % i)
+    if os.path.exists(cache):
+        z = np.load(cache)
+        return {k: z[k] for k in z.files}
+    fl, alarms, y = workloads.config4_graph(i)
+    g = CausalFactorGraph.from_factors(fl)
+    a = g.graph_arrays()
+    a["n_vars"] = np.int64(a["n_vars"])
+    a["label_vars"] = np.array([g.findVar(int(t)) for t in alarms], np.int64)
+    a["labels"] = y
+    np.savez(cache, **a)
+    return a
+
+
+def bce_and_grad(b, idx, y):
+    """Binary cross-entropy of the beliefs b[idx] against labels y, and dL/db."""
+    bb = np.clip(b[idx], 1e-300, 1.0 - 1e-16)
+    loss = float(-(y * np.log(bb) + (1 - y) * np.log1p(-bb)).sum())
+    g = np.zeros_like(b)
+    np.add.at(g, idx, -y / bb + (1 - y) / (1 - bb))
+    return loss, g
+
+
+def run_adjoint(args, rank, world, local):
+    """Gradient through unrolled sweeps: 64 graphs of 50 k tuples (config-0
+    laws, ~75 k rules each), T = 100 sweeps from init(), checkpoints every
+    10, FP32 messages; loss = binary cross-entropy of the beliefs of 200
+    labelled alarms per graph (labels Bernoulli(0.3)); gradient with
+    respect to every factor's p (rule firing probabilities and input
+    priors). All graphs sit in one BatchEngine.
+
+    Timed per step, device-resident (beliefs and gradients in CUDA tensors):
+    a forward solve (init + T sweeps + beliefs) and a gradient (checkpointed
+    forward + beliefs + the loss gradient in torch + the adjoint backward);
+    the same two through the host-buffer calls (beliefs and gradients copied
+    to numpy arrays). On rank 0, graph 0 alone is checked in FP64 against
+    central differences (eps 1e-6) on sampled parameters, and the FP32
+    gradient against the FP64 one."""
+    import torch
+
+    from fastlbp_b200 import BatchEngine
+    from fastlbp_b200.shard import partition
+
+    T, K, n_graphs = args.sweeps, args.every, args.graphs
+    mine = partition(np.ones(n_graphs), world)[rank]
+    arrays = [adjoint_graph_arrays(i) for i in mine]
+    be = BatchEngine(arrays, precision=args.precision)
+    idx = np.concatenate([be.var_off[k] + a["label_vars"] for k, a in enumerate(arrays)])
+    y = np.concatenate([a["labels"] for a in arrays])
+    E = int(sum(int(a["factor_offsets"][-1]) for a in arrays))
+    dev = torch.device("cuda", local)
+    idx_d = torch.as_tensor(idx, device=dev)
+    y_d = torch.as_tensor(y, device=dev)
+    b_d = torch.empty(be.n_vars, dtype=torch.float64, device=dev)
+    gp_d = torch.empty(be.n_factors, dtype=torch.float64, device=dev)
+
+    def forward_dev():
+        be.init()
+        be.run_fixed(T)
+        be.beliefs_device(b_d)
+
+    def gradient_dev():
+        be.adjoint_forward(T, K, fetch=False)
+        be.beliefs_device(b_d)
+        bb = b_d[idx_d].clamp(1e-300, 1.0 - 1e-16)
+        g = torch.zeros_like(b_d)
+        g.index_put_((idx_d,), -y_d / bb + (1 - y_d) / (1 - bb), accumulate=True)
+        be.adjoint_backward_device(g, gp_d)
+
+    def forward_host():
+        be.init()
+        be.run_fixed(T)
+        return be.beliefs()
+
+    def gradient_host():
+        b = be.adjoint_forward(T, K)
+        loss, g = bce_and_grad(b, idx, y)
+        gp, _ = be.adjoint_backward(g, want_q=False)
+        return loss, gp
+
+    def timed(fn):
+        barrier(world)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, out
+
+    for _ in range(max(1, args.warmup)):
+        forward_dev()
+        gradient_dev()
+        forward_host()
+        gradient_host()
+    torch.cuda.synchronize()
+    tf, tg, tfh, tgh = [], [], [], []
+    for _ in range(args.steps):
+        tf.append(timed(forward_dev)[0])
+        tg.append(timed(gradient_dev)[0])
+        tfh.append(timed(forward_host)[0])
+        t, (loss, gp_host) = timed(gradient_host)
+        tgh.append(t)
+    med = lambda xs: allreduce_max(statistics.median(xs), world)  # noqa: E731
+    t_f, t_g, t_fh, t_gh = med(tf), med(tg), med(tfh), med(tgh)
+    same = float(np.max(np.abs(gp_d.cpu().numpy() - gp_host))) if be.n_factors else 0.0
+    line = {"metric": "adjoint time (gradient of the loss w.r.t. every p)", "value": t_g, "unit": "s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+            "scaling": "strong", "dtype": "f32" if args.precision == 32 else "f64",
+            "data": "synthetic (seeded Bingo-style generator)",
+            "config": {"workload": "%d graphs x 50k tuples (config-0 laws, 1.5 rules/tuple), T=%d sweeps from init, "
+                                   "checkpoint every %d, BCE on 200 labelled alarms per graph" % (n_graphs, T, K),
+                       "graphs_this_rank": len(mine), "vars_this_rank": be.n_vars,
+                       "factors_this_rank": be.n_factors, "edge_slots_this_rank": E},
+            "seconds": {"forward_solve": t_f, "gradient": t_g, "forward_solve_host_buffers": t_fh,
+                        "gradient_host_buffers": t_gh},
+            "gradient_over_forward": t_g / t_f,
+            "gradient_over_forward_host_buffers": t_gh / t_fh,
+            "forward_updates_per_s": 2.0 * E * T * world / t_f,
+            "loss": loss,
+            "device_vs_host_gradient_max_abs_diff": same}
+    be.close()
+    if rank == 0 and args.fd_params > 0:
+        line["checks"] = adjoint_checks(arrays[0], T, K, args.fd_params)
+    return line
+
+
+def adjoint_checks(a, T, K, n_params):
+    """Graph 0 alone: FP64 adjoint against central differences (eps 1e-6) on
+    n_params sampled rule probabilities and input priors, and the FP32
+    adjoint against the FP64 one."""
+    from fastlbp_b200 import Engine
+
+    idx, y = a["label_vars"], a["labels"]
+    p0, q0 = np.asarray(a["factor_p"], np.float64).copy(), np.asarray(a["factor_q"], np.float64)
+    grads = {}
+    for prec in (64, 32):
+        e = Engine(a, precision=prec)
+        _, g = bce_and_grad(e.adjoint_forward(T, K), idx, y)
+        grads[prec] = e.adjoint_backward(g)[0]
+        if prec == 32:
+            e.close()
+        else:
+            e64 = e
+    g64, g32 = grads[64], grads[32]
+    rng = np.random.default_rng(5)
+    cand = np.nonzero((p0 > 1e-3) & (p0 < 1 - 1e-3))[0]
+    sample = np.sort(rng.choice(cand, size=min(n_params, cand.size), replace=False))
+    eps = 1e-6
+
+    def loss(p):
+        e64.set_factor_probs(p, q0)
+        return bce_and_grad(e64.adjoint_forward(T, K), idx, y)[0]
+
+    t0 = time.perf_counter()
+    fd = np.zeros(sample.size)
+    for j, I in enumerate(sample):
+        pp, pm = p0.copy(), p0.copy()
+        pp[I] += eps
+        pm[I] -= eps
+        fd[j] = (loss(pp) - loss(pm)) / (2 * eps)
+    t_fd = time.perf_counter() - t0
+    e64.close()
+    ga = g64[sample]
+    scale = float(np.max(np.abs(g64)))
+    floor = 1e-3 * scale
+    rel = np.abs(fd - ga) / np.maximum(np.abs(ga), floor)
+    big = np.abs(ga) >= floor
+    return {"fd": {"params": int(sample.size), "eps": eps, "within_1e-4": int((rel <= 1e-4).sum()),
+                   "max_rel_err": float(rel.max()),
+                   "max_rel_err_where_grad_ge_1e-3_max": float(rel[big].max()) if big.any() else None,
+                   "params_with_grad_ge_1e-3_max": int(big.sum()), "seconds": t_fd,
+                   "note": "relative error |fd - g| / max(|g|, 1e-3 max|g|), FP64 engine, graph 0"},
+            "fp32_vs_fp64_rel_l2": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64)),
+            "grad_max_abs": scale}
 
 
 def run_fl(args, rank, world, local):
@@ -515,6 +699,8 @@ def main():
         line = run_batch(args, rank, world, local)
     elif args.workload == "fl":
         line = run_fl(args, rank, world, local)
+    elif args.workload == "adjoint":
+        line = run_adjoint(args, rank, world, local)
     else:
         line = run_ours(args, rank, world, local)
     if rank == 0 and line is not None:

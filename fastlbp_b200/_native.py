@@ -24,6 +24,14 @@ _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 _vp = C.c_void_p
 
 
+class _F64OrNull:
+    """A C-contiguous float64 array, or None for a NULL pointer."""
+
+    @classmethod
+    def from_param(cls, obj):
+        return None if obj is None else _f64p.from_param(obj)
+
+
 class GraphDesc(C.Structure):
     _fields_ = [("n_vars", C.c_int64), ("n_factors", C.c_int64), ("n_slots", C.c_int64),
                 ("factor_offsets", _vp), ("slot_var", _vp), ("factor_head", _vp), ("factor_type", _vp),
@@ -107,8 +115,10 @@ def lib():
         "flbp_batch_create": [P(GraphDesc), C.c_int64, P(EngineOpts), P(_vp)],
         "flbp_batch_info": [_vp, P(C.c_int64), _i64p],
         "flbp_batch_run_tol": [_vp, C.c_double, C.c_int64, C.c_double, _i64p, _i32p, P(RunInfo)],
-        "flbp_adjoint_forward": [_vp, C.c_int64, C.c_int64, _f64p, C.c_int64],
-        "flbp_adjoint_backward": [_vp, _f64p, _f64p, _f64p],
+        "flbp_adjoint_forward": [_vp, C.c_int64, C.c_int64, _F64OrNull, C.c_int64],
+        "flbp_adjoint_backward": [_vp, _f64p, _F64OrNull, _F64OrNull],
+        "flbp_adjoint_backward_device": [_vp, _vp, _vp, _vp],
+        "flbp_get_beliefs_device": [_vp, _vp, C.c_int64],
         "flbp_set_factor_probs": [_vp, _f64p, _f64p],
     }
     for name, args in sig.items():
@@ -135,4 +145,5 @@ EXPORTED = ["flbp_last_error", "flbp_version", "flbp_engine_create", "flbp_engin
             "flbp_fg_from_factors", "flbp_fg_destroy", "flbp_fg_clamp", "flbp_fg_rebuild", "flbp_fg_sizes",
             "flbp_fg_var_labels", "flbp_fg_factors", "flbp_fg_neighbors", "flbp_fg_construct",
             "flbp_engine_create_from_fg", "flbp_run_fixed_device_noalloc", "flbp_batch_create", "flbp_batch_info",
-            "flbp_batch_run_tol", "flbp_adjoint_forward", "flbp_adjoint_backward", "flbp_set_factor_probs"]
+            "flbp_batch_run_tol", "flbp_adjoint_forward", "flbp_adjoint_backward", "flbp_set_factor_probs",
+            "flbp_adjoint_backward_device", "flbp_get_beliefs_device"]

@@ -163,6 +163,14 @@ class CausalFactorGraph:
                 self.clamp(i, clamps[lab])
 
 
+def _check_device_tensor(t, n: int, name: str) -> None:
+    import torch
+
+    if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()
+            and t.numel() == n):
+        raise ValueError("%s must be a contiguous float64 CUDA tensor of %d elements" % (name, n))
+
+
 def _desc_from_arrays(a: Dict[str, np.ndarray], keep: list) -> N.GraphDesc:
     def ptr(name, dt):
         v = a.get(name)
@@ -274,17 +282,40 @@ class Engine:
         return dict(zip(keys, (int(x) for x in c)))
 
     # gradients through unrolled sweeps --------------------------------------
-    def adjoint_forward(self, sweeps: int, every: int) -> np.ndarray:
-        """init() and `sweeps` sweeps with checkpoints every `every`; the beliefs."""
-        out = np.zeros(self.n_vars)
-        check(lib().flbp_adjoint_forward(self._h, int(sweeps), int(every), out, out.size))
+    def adjoint_forward(self, sweeps: int, every: int, fetch: bool = True) -> Optional[np.ndarray]:
+        """init() and `sweeps` sweeps with checkpoints every `every`; the
+        beliefs (None with fetch=False: they stay on the device, see
+        beliefs_device)."""
+        out = np.zeros(self.n_vars) if fetch else None
+        check(lib().flbp_adjoint_forward(self._h, int(sweeps), int(every), out, self.n_vars))
         return out
 
-    def adjoint_backward(self, grad_beliefs: np.ndarray):
-        """dL/dp and dL/dq of every factor (reference order) for dL/dbeliefs."""
+    def beliefs_device(self, out) -> None:
+        """Beliefs of the last run into `out`, a contiguous float64 CUDA tensor
+        of n_vars elements on the engine's device."""
+        _check_device_tensor(out, self.n_vars, "out")
+        check(lib().flbp_get_beliefs_device(self._h, C.c_void_p(out.data_ptr()), self.n_vars))
+
+    def adjoint_backward_device(self, grad_beliefs, grad_p, grad_q=None) -> None:
+        """adjoint_backward on contiguous float64 CUDA tensors (grad_q may be
+        None). Waits for the current torch stream before reading grad_beliefs."""
+        import torch
+
+        _check_device_tensor(grad_beliefs, self.n_vars, "grad_beliefs")
+        _check_device_tensor(grad_p, self.n_factors, "grad_p")
+        if grad_q is not None:
+            _check_device_tensor(grad_q, self.n_factors, "grad_q")
+        torch.cuda.current_stream(grad_beliefs.device).synchronize()
+        check(lib().flbp_adjoint_backward_device(self._h, C.c_void_p(grad_beliefs.data_ptr()),
+                                                 C.c_void_p(grad_p.data_ptr()),
+                                                 None if grad_q is None else C.c_void_p(grad_q.data_ptr())))
+
+    def adjoint_backward(self, grad_beliefs: np.ndarray, want_q: bool = True):
+        """dL/dp and dL/dq of every factor (reference order) for dL/dbeliefs
+        (dL/dq None, and not accumulated, with want_q=False)."""
         g = np.ascontiguousarray(grad_beliefs, np.float64)
         gp = np.zeros(self.n_factors)
-        gq = np.zeros(self.n_factors)
+        gq = np.zeros(self.n_factors) if want_q else None
         check(lib().flbp_adjoint_backward(self._h, g, gp, gq))
         return gp, gq
 

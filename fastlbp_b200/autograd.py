@@ -8,7 +8,10 @@ input prior). The forward pass runs the CUDA engine with checkpoints every
 (flbp_adjoint_backward) backwards through the sweeps, recomputing each
 segment from its checkpoint. The engine keeps the state of its last forward
 call, so each forward must be followed by its backward before the next
-forward on the same engine.
+forward on the same engine. With p on the engine's CUDA device, beliefs and
+gradients stay on the device (flbp_get_beliefs_device,
+flbp_adjoint_backward_device); p itself goes to the host for
+flbp_set_factor_probs.
 """
 
 from __future__ import annotations
@@ -23,14 +26,24 @@ class UnrolledBeliefs(torch.autograd.Function):
     @staticmethod
     def forward(ctx, p: torch.Tensor, engine: Engine, q: np.ndarray, sweeps: int, every: int):
         engine.set_factor_probs(p.detach().to("cpu", torch.float64).numpy(), q)
-        b = engine.adjoint_forward(int(sweeps), int(every))
         ctx.engine = engine
-        return torch.from_numpy(b).to(p.device)
+        ctx.on_device = p.is_cuda
+        if p.is_cuda:
+            engine.adjoint_forward(int(sweeps), int(every), fetch=False)
+            b = torch.empty(engine.n_vars, dtype=torch.float64, device=p.device)
+            engine.beliefs_device(b)
+            return b
+        return torch.from_numpy(engine.adjoint_forward(int(sweeps), int(every)))
 
     @staticmethod
     def backward(ctx, grad_b: torch.Tensor):
-        gp, _ = ctx.engine.adjoint_backward(grad_b.detach().to("cpu", torch.float64).numpy())
-        return torch.from_numpy(gp).to(grad_b.device), None, None, None, None
+        if ctx.on_device:
+            g = grad_b.detach().to(torch.float64).contiguous()
+            gp = torch.empty(ctx.engine.n_factors, dtype=torch.float64, device=g.device)
+            ctx.engine.adjoint_backward_device(g, gp)
+            return gp, None, None, None, None
+        gp, _ = ctx.engine.adjoint_backward(grad_b.detach().to("cpu", torch.float64).numpy(), want_q=False)
+        return torch.from_numpy(gp), None, None, None, None
 
 
 def unrolled_beliefs(p: torch.Tensor, engine: Engine, q, sweeps: int, every: int) -> torch.Tensor:

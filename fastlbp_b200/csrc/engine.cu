@@ -70,9 +70,18 @@ struct flbp_engine {
     // run (adj_t sweeps), per-sweep states of one segment, and derivatives.
     long long adj_t = 0, adj_k = 0;
     void *d_ckpt = nullptr, *d_seg_vf = nullptr, *d_seg_fv = nullptr;
-    double *d_lam = nullptr, *d_lam2 = nullptr, *d_mu = nullptr, *d_gp = nullptr, *d_gq = nullptr;
-    double *d_gprior = nullptr, *d_gs = nullptr;
+    // in the message type: lambdas per entry (two), mu per slot, dL/dp and
+    // dL/dq per internal factor, dL/dprior and dL/dS per internal variable
+    void *d_lam = nullptr, *d_lam2 = nullptr, *d_mu = nullptr, *d_gp = nullptr, *d_gq = nullptr;
+    void *d_gprior = nullptr, *d_gs = nullptr;
     size_t adj_ckpt_n = 0, adj_seg_n = 0;
+    uint32_t *d_int_of_var = nullptr, *d_f_of_int = nullptr;  // caller variable -> internal; internal factor -> caller
+    uint32_t *d_pri_fac = nullptr, *d_pri_var = nullptr;      // folded constants: caller factor, internal variable
+    double *d_pri_coef = nullptr;                             // their d(constant)/dp
+    bool pri_coef_valid = false;
+    double *d_adj_in = nullptr, *d_adj_out = nullptr;         // staging of the host-buffer backward call
+    uint32_t *d_adj_groups = nullptr;  // sliced-ELL group ids by width class (see adj_group_n)
+    uint32_t adj_group_n[4] = {0, 0, 0, 0};
     std::vector<double> factor_p_host;  // every reference factor's p (for derivatives of folded constants)
     uint8_t *d_f_kind = nullptr, *d_f_deg = nullptr;
     void *d_prior = nullptr;
@@ -476,14 +485,19 @@ void packed_priors(const flbp_engine *e, size_t nv_pad, std::vector<uint32_t> &p
     const HostLayout &L = e->L;
     const size_t psz = e->prec == 64 ? 16 : 8;
     prior.assign(std::max<size_t>(1, nv_pad) * (psz / 4), 0u);
+    // bit 31 of the count word: the variable has a folded finite constant
+    // (its dL/dprior feeds a factor's dL/dp)
+    std::vector<uint8_t> folded((size_t)L.V, 0);
+    for (uint32_t v : L.prior_var) folded[v] = 1;
     for (int64_t i = 0; i < L.V; i++) {
+        const uint32_t cnt = L.prior_cnt[i] | (folded[i] ? 0x80000000u : 0u);
         if (e->prec == 64) {
             std::memcpy(&prior[4 * i], &L.prior_fin[i], 8);
-            prior[4 * i + 2] = L.prior_cnt[i];
+            prior[4 * i + 2] = cnt;
         } else {
             const float f = (float)L.prior_fin[i];
             std::memcpy(&prior[2 * i], &f, 4);
-            prior[2 * i + 1] = L.prior_cnt[i];
+            prior[2 * i + 1] = cnt;
         }
     }
     // priors of the variables of every big tile, in tile order
@@ -701,7 +715,8 @@ int flbp_engine_destroy(flbp_engine *e) {
                     e->d_ftiles, e->d_vtiles,  e->d_fb_deg, e->d_vb_deg, e->d_fbt_deg, e->d_vbt_deg,
                     e->d_fbt_kind, e->d_fbt_pq, e->d_vbt_prior, e->d_f_graph, e->d_v_graph, e->d_gstate, e->d_ftrange, e->d_vtrange,
                     e->d_ckpt, e->d_seg_vf, e->d_seg_fv, e->d_lam, e->d_lam2, e->d_mu, e->d_gp, e->d_gq,
-                    e->d_gprior, e->d_gs};
+                    e->d_gprior, e->d_gs, e->d_int_of_var, e->d_f_of_int, e->d_pri_fac, e->d_pri_var, e->d_pri_coef,
+                    e->d_adj_in, e->d_adj_out, e->d_adj_groups};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (e->h_ctl) cudaFreeHost(e->h_ctl);
@@ -1182,21 +1197,192 @@ AdjArgs adj_args(flbp_engine *e) {
     return a;
 }
 
+unsigned int blocks_for(uint64_t threads, unsigned int per_block) {
+    return (unsigned int)std::max<uint64_t>(1, (threads + per_block - 1) / per_block);
+}
+
+// One backward step: lam_next = dL/dvf_{t+1} -> lam = dL/dvf_t, with the
+// parameter gradients of sweep t accumulated (dL/dq only with want_q).
 template <typename T>
-void launch_adjoint_step(flbp_engine *e, const void *vf, const void *fv, const double *lam_next, const double *gs,
-                         double *lam) {
+void launch_adjoint_step(flbp_engine *e, const void *vf, const void *fv, const void *lam_next, const void *gs,
+                         void *lam, bool want_q) {
     const AdjArgs a = adj_args(e);
-    const uint32_t nv = a.nv_sell + a.nv_big;
-    if (nv) var_adjoint_kernel<T><<<(nv + 127) / 128, 128, 0, e->stream>>>(a, (const T *)fv, lam_next, gs, e->d_mu,
-                                                                           e->d_gprior);
-    cudaMemsetAsync(lam, 0, std::max<uint64_t>(1, e->L.n_slots) * sizeof(double), e->stream);
-    if (a.nf_sell)
-        factor_adjoint_sell_kernel<T><<<(a.nf_sell + 127) / 128, 128, 0, e->stream>>>(a, (const T *)vf, e->d_mu, lam,
-                                                                                       e->d_gp, e->d_gq);
-    if (a.nf_big)
-        factor_adjoint_big_kernel<T><<<(a.nf_big + 3) / 4, 128, 0, e->stream>>>(a, (const T *)vf, e->d_mu, lam, e->d_gp,
-                                                                                 e->d_gq);
-    e->launches += 2 + (a.nf_big ? 1 : 0);
+    T *mu = (T *)e->d_mu, *gp = (T *)e->d_gp, *gq = want_q ? (T *)e->d_gq : nullptr, *gprior = (T *)e->d_gprior;
+    const uint32_t *gl = e->d_adj_groups;
+    const uint32_t *c = e->adj_group_n;  // narrow var, wide var, narrow factor, wide factor groups
+    const uint32_t o1 = c[0], o2 = o1 + c[1], o3 = o2 + c[2];
+    int n = 0;
+    auto go = [&](uint32_t cnt) { n += cnt ? 1 : 0; return cnt != 0; };
+    if (go(c[0]))
+        var_adjoint_kernel<T, false><<<blocks_for(32ull * c[0], 128), 128, 0, e->stream>>>(
+            a, gl, c[0], (const T *)fv, (const T *)lam_next, (const T *)gs, mu, gprior);
+    if (go(c[1]))
+        var_adjoint_kernel<T, true><<<blocks_for(32ull * c[1], 128), 128, 0, e->stream>>>(
+            a, gl + o1, c[1], (const T *)fv, (const T *)lam_next, (const T *)gs, mu, gprior);
+    if (go(a.nv_big))
+        var_adjoint_big_kernel<T><<<blocks_for((uint64_t)kBigVarLanes * a.nv_big, 128), 128, 0, e->stream>>>(
+            a, (const T *)fv, (const T *)lam_next, (const T *)gs, mu, gprior);
+    if (go(c[2]))
+        factor_adjoint_sell_kernel<T, false><<<blocks_for(32ull * c[2], 128), 128, 0, e->stream>>>(
+            a, gl + o2, c[2], (const T *)vf, mu, (T *)lam, gp, gq);
+    if (go(c[3]))
+        factor_adjoint_sell_kernel<T, true><<<blocks_for(32ull * c[3], 128), 128, 0, e->stream>>>(
+            a, gl + o3, c[3], (const T *)vf, mu, (T *)lam, gp, gq);
+    if (go(a.nf_big))
+        factor_adjoint_big_kernel<T><<<blocks_for(32ull * a.nf_big, 128), 128, 0, e->stream>>>(a, (const T *)vf, mu,
+                                                                                                (T *)lam, gp, gq);
+    e->launches += n;
+}
+
+// Undamped sweep halves on explicit message arrays (the recomputation of a
+// segment writes each sweep's states straight into the segment buffers).
+template <typename T>
+void launch_factor_pass_on(flbp_engine *e, const void *vf, void *fv) {
+    const FactorArgs fa = factor_args<T>(e);
+    factor_pass_kernel<T, kStages><<<e->factor_grid, kBlockThreads, factor_smem<T>(), e->stream>>>(
+        fa, (const T *)vf, (T *)fv, e->d_ctl);
+    e->launches += 1;
+}
+
+template <typename T>
+void launch_var_pass_on(flbp_engine *e, const void *fv, void *vf) {
+    const VarArgs va = var_args(e);
+    var_pass_kernel<T, 0, true, false, kStages><<<e->var_grid, kBlockThreads, var_smem<T, false>(), e->stream>>>(
+        va, (const T *)fv, (T *)vf, nullptr, (T)0, e->d_ctl);
+    e->launches += 1;
+}
+
+template <typename T>
+void launch_adjoint_seed(flbp_engine *e, const double *grad_b) {
+    const int64_t V = e->L.V;
+    if (V)
+        adjoint_seed_kernel<T><<<blocks_for(V, 256), 256, 0, e->stream>>>(grad_b, e->d_int_of_var, e->d_belief, V,
+                                                                          (T *)e->d_gs);
+    e->launches += V ? 1 : 0;
+}
+
+template <typename T>
+void launch_adjoint_out(flbp_engine *e, double *gp_out, double *gq_out) {
+    const uint32_t nf = e->L.nf_sell + e->L.nf_big, np = (uint32_t)e->L.prior_factor.size();
+    if (nf)
+        adjoint_factor_out_kernel<T><<<blocks_for(nf, 256), 256, 0, e->stream>>>(
+            (const T *)e->d_gp, (const T *)e->d_gq, e->d_f_of_int, nf, gp_out, gq_out);
+    if (np && gp_out)
+        adjoint_prior_out_kernel<T><<<blocks_for(np, 256), 256, 0, e->stream>>>(
+            (const T *)e->d_gprior, e->d_pri_fac, e->d_pri_var, e->d_pri_coef, np, gp_out);
+    e->launches += (nf ? 1 : 0) + ((np && gp_out) ? 1 : 0);
+}
+
+// Device maps between the caller's order and the internal one, and the
+// coefficients of the folded constants, for the adjoint (built on first use;
+// the coefficients again after flbp_set_factor_probs).
+int ensure_adjoint_maps(flbp_engine *e) {
+    int rc;
+    const HostLayout &L = e->L;
+    if (!e->d_int_of_var) {
+        // sliced-ELL groups by width class: narrow var, wide var, narrow factor, wide factor
+        std::vector<uint32_t> lists[4];
+        for (uint32_t g = 0; g < L.n_vgroups(); g++)
+            lists[(L.vg_base[g + 1] - L.vg_base[g]) / 32 > kNarrowWidth ? 1 : 0].push_back(g);
+        for (uint32_t g = 0; g < L.n_fgroups(); g++)
+            lists[(L.fg_base[g + 1] - L.fg_base[g]) / 32 > kNarrowWidth ? 3 : 2].push_back(g);
+        std::vector<uint32_t> all;
+        for (int k = 0; k < 4; k++) {
+            e->adj_group_n[k] = (uint32_t)lists[k].size();
+            all.insert(all.end(), lists[k].begin(), lists[k].end());
+        }
+        if ((rc = dalloc(e, &e->d_adj_groups, all.size())) || (rc = upload(e, e->d_adj_groups, all))) return rc;
+        const uint32_t nf = L.nf_sell + L.nf_big;
+        std::vector<uint32_t> iov(L.internal_of_var.begin(), L.internal_of_var.end());
+        std::vector<uint32_t> foi(L.factor_of_internal.begin(), L.factor_of_internal.begin() + nf);
+        if ((rc = dalloc(e, &e->d_int_of_var, iov.size())) || (rc = upload(e, e->d_int_of_var, iov)) ||
+            (rc = dalloc(e, &e->d_f_of_int, foi.size())) || (rc = upload(e, e->d_f_of_int, foi)) ||
+            (rc = dalloc(e, &e->d_pri_fac, L.prior_factor.size())) || (rc = upload(e, e->d_pri_fac, L.prior_factor)) ||
+            (rc = dalloc(e, &e->d_pri_var, L.prior_var.size())) || (rc = upload(e, e->d_pri_var, L.prior_var)) ||
+            (rc = dalloc(e, &e->d_pri_coef, L.prior_factor.size())))
+            return rc;
+        e->pri_coef_valid = false;
+    }
+    if (!e->pri_coef_valid) {
+        std::vector<double> coef(L.prior_factor.size(), 0.0);
+        for (size_t k = 0; k < coef.size(); k++) {
+            const double p = e->factor_p_host[L.prior_factor[k]];
+            if (p > 0.0 && p < 1.0) coef[k] = L.prior_sign[k] / (p * (1.0 - p));
+        }
+        if ((rc = upload(e, e->d_pri_coef, coef))) return rc;
+        e->pri_coef_valid = true;
+    }
+    return FLBP_OK;
+}
+
+// The backward pass on device buffers in the caller's orders: dL/dbeliefs
+// in, dL/dp and dL/dq out (either may be null). Leaves the work queued on
+// the engine's stream.
+template <typename T>
+int adjoint_backward_t(flbp_engine *e, const double *grad_b, double *gp_out, double *gq_out) {
+    int rc;
+    const HostLayout &L = e->L;
+    const size_t ts = sizeof(T);
+    const size_t ns = std::max<uint64_t>(1, L.n_slots), ne = std::max<size_t>(1, e->n_ent);
+    const size_t nv = std::max<int64_t>(1, L.V), nf = std::max<size_t>(1, (size_t)L.nf_sell + L.nf_big);
+    if ((rc = ensure_adjoint_maps(e))) return rc;
+    if (!e->d_lam && ((rc = dalloc(e, (char **)&e->d_lam, ne * ts)) || (rc = dalloc(e, (char **)&e->d_lam2, ne * ts)) ||
+                      (rc = dalloc(e, (char **)&e->d_mu, ns * ts)) || (rc = dalloc(e, (char **)&e->d_gp, nf * ts)) ||
+                      (rc = dalloc(e, (char **)&e->d_gq, nf * ts)) ||
+                      (rc = dalloc(e, (char **)&e->d_gprior, nv * ts)) || (rc = dalloc(e, (char **)&e->d_gs, nv * ts))))
+        return rc;
+    FLBP_CUDA(cudaMemsetAsync(e->d_gp, 0, nf * ts, e->stream));
+    if (gq_out) FLBP_CUDA(cudaMemsetAsync(e->d_gq, 0, nf * ts, e->stream));
+    FLBP_CUDA(cudaMemsetAsync(e->d_gprior, 0, nv * ts, e->stream));
+    FLBP_CUDA(cudaMemsetAsync(e->d_lam, 0, ne * ts, e->stream));
+    FLBP_CUDA(cudaMemsetAsync(e->d_lam2, 0, ne * ts, e->stream));
+    FLBP_CUDA(cudaMemsetAsync(e->d_mu, 0, ns * ts, e->stream));
+    launch_adjoint_seed<T>(e, grad_b);
+    reset_ctl_for_run(e, 0);
+    if ((rc = upload_ctl(e))) return rc;
+    const long long T_ = e->adj_t, K = e->adj_k;
+    const long long nck = (T_ + K - 1) / K;
+    auto seg_vf = [&](long long i) { return (char *)e->d_seg_vf + (size_t)i * ns * ts; };
+    auto seg_fv = [&](long long i) { return (char *)e->d_seg_fv + (size_t)i * e->n_ent * ts; };
+    // Entries and slots that no pass writes hold constants: give every
+    // segment buffer the current arrays once, then only the passes write.
+    for (long long i = 0; i < (long long)e->adj_seg_n; i++) {
+        FLBP_CUDA(cudaMemcpyAsync(seg_vf(i), e->d_vf, ns * ts, cudaMemcpyDeviceToDevice, e->stream));
+        if (e->n_ent)
+            FLBP_CUDA(cudaMemcpyAsync(seg_fv(i), e->d_fv, e->n_ent * ts, cudaMemcpyDeviceToDevice, e->stream));
+    }
+    void *lam_next = e->d_lam, *lam_cur = e->d_lam2;
+    for (long long c = nck - 1; c >= 0; c--) {
+        const long long t0 = c * K, n1 = std::min<long long>(K, T_ - t0);
+        // recompute the segment's states from its checkpoint: vf_i in seg_vf(i), fv_i in seg_fv(i)
+        FLBP_CUDA(cudaMemcpyAsync(seg_vf(0), (char *)e->d_ckpt + (size_t)c * ns * ts, ns * ts,
+                                  cudaMemcpyDeviceToDevice, e->stream));
+        for (long long i = 0; i < n1; i++) {
+            launch_factor_pass_on<T>(e, seg_vf(i), seg_fv(i));
+            if (i + 1 < n1) launch_var_pass_on<T>(e, seg_fv(i), seg_vf(i + 1));
+        }
+        for (long long i = n1 - 1; i >= 0; i--) {
+            const void *gsp = (t0 + i == T_ - 1) ? e->d_gs : nullptr;
+            launch_adjoint_step<T>(e, seg_vf(i), seg_fv(i), lam_next, gsp, lam_cur, gq_out != nullptr);
+            std::swap(lam_next, lam_cur);
+        }
+    }
+    launch_adjoint_out<T>(e, gp_out, gq_out);
+    FLBP_CUDA(cudaGetLastError());
+    return download_ctl(e);  // synchronises; reports a timed-out pass
+}
+
+int adjoint_backward_dev(flbp_engine *e, const double *grad_b, double *gp_out, double *gq_out) {
+    if (e->adj_t == 0) {
+        set_error("no adjoint forward run to differentiate (call flbp_adjoint_forward first)");
+        return FLBP_ERR_INVALID;
+    }
+    if (e->L.F) {
+        if (gp_out) FLBP_CUDA(cudaMemsetAsync(gp_out, 0, (size_t)e->L.F * sizeof(double), e->stream));
+        if (gq_out) FLBP_CUDA(cudaMemsetAsync(gq_out, 0, (size_t)e->L.F * sizeof(double), e->stream));
+    }
+    if (e->prec == 64) return adjoint_backward_t<double>(e, grad_b, gp_out, gq_out);
+    return adjoint_backward_t<float>(e, grad_b, gp_out, gq_out);
 }
 
 }  // namespace
@@ -1214,12 +1400,17 @@ int flbp_adjoint_forward(flbp_engine *e, int64_t sweeps, int64_t every, double *
         set_error("sweeps and checkpoint interval must be positive");
         return FLBP_ERR_INVALID;
     }
-    const size_t ns = std::max<uint64_t>(1, e->L.n_slots), ne = e->n_ent;
+    if (beliefs && n != e->L.V) {
+        set_error("output length must equal the number of variables");
+        return FLBP_ERR_INVALID;
+    }
+    const size_t ns = std::max<uint64_t>(1, e->L.n_slots), ne = std::max<size_t>(1, e->n_ent);
     const size_t nck = (size_t)((sweeps + every - 1) / every);
     const size_t nseg = (size_t)std::min<int64_t>(every, sweeps);
     if (nck > e->adj_ckpt_n) {
         if (e->d_ckpt) cudaFree(e->d_ckpt);
         e->d_ckpt = nullptr;
+        e->adj_ckpt_n = 0;
         if ((rc = dalloc(e, (char **)&e->d_ckpt, nck * ns * e->tsize))) return rc;
         e->adj_ckpt_n = nck;
     }
@@ -1227,6 +1418,7 @@ int flbp_adjoint_forward(flbp_engine *e, int64_t sweeps, int64_t every, double *
         if (e->d_seg_vf) cudaFree(e->d_seg_vf);
         if (e->d_seg_fv) cudaFree(e->d_seg_fv);
         e->d_seg_vf = e->d_seg_fv = nullptr;
+        e->adj_seg_n = 0;
         if ((rc = dalloc(e, (char **)&e->d_seg_vf, nseg * ns * e->tsize)) ||
             (rc = dalloc(e, (char **)&e->d_seg_fv, nseg * ne * e->tsize)))
             return rc;
@@ -1254,84 +1446,53 @@ int flbp_adjoint_forward(flbp_engine *e, int64_t sweeps, int64_t every, double *
 int flbp_adjoint_backward(flbp_engine *e, const double *grad_beliefs, double *grad_p, double *grad_q) {
     int rc = begin_call(e);
     if (rc) return rc;
-    if (e->adj_t == 0) {
-        set_error("no adjoint forward run to differentiate (call flbp_adjoint_forward first)");
+    const HostLayout &L = e->L;
+    const size_t nv = std::max<int64_t>(1, L.V), nF = std::max<int64_t>(1, L.F);
+    if (!e->d_adj_in && ((rc = dalloc(e, &e->d_adj_in, nv)) || (rc = dalloc(e, &e->d_adj_out, 2 * nF)))) return rc;
+    if (L.V) {
+        if (grad_beliefs)
+            FLBP_CUDA(cudaMemcpyAsync(e->d_adj_in, grad_beliefs, (size_t)L.V * sizeof(double), cudaMemcpyHostToDevice,
+                                      e->stream));
+        else
+            FLBP_CUDA(cudaMemsetAsync(e->d_adj_in, 0, (size_t)L.V * sizeof(double), e->stream));
+    }
+    if ((rc = adjoint_backward_dev(e, e->d_adj_in, e->d_adj_out, e->d_adj_out + nF))) return rc;
+    if (L.F) {
+        if (grad_p)
+            FLBP_CUDA(cudaMemcpyAsync(grad_p, e->d_adj_out, (size_t)L.F * sizeof(double), cudaMemcpyDeviceToHost,
+                                      e->stream));
+        if (grad_q)
+            FLBP_CUDA(cudaMemcpyAsync(grad_q, e->d_adj_out + nF, (size_t)L.F * sizeof(double), cudaMemcpyDeviceToHost,
+                                      e->stream));
+    }
+    FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    return FLBP_OK;
+}
+
+int flbp_adjoint_backward_device(flbp_engine *e, const double *grad_beliefs, double *grad_p, double *grad_q) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    if (!grad_beliefs && e->L.V) {
+        set_error("grad_beliefs is required");
         return FLBP_ERR_INVALID;
     }
-    const HostLayout &L = e->L;
-    const size_t ns = std::max<uint64_t>(1, L.n_slots), ne = e->n_ent, nv = std::max<int64_t>(1, L.V);
-    const size_t nf = std::max<size_t>(1, (size_t)L.nf_sell + L.nf_big);
-    if (!e->d_lam &&
-        ((rc = dalloc(e, &e->d_lam, ns)) || (rc = dalloc(e, &e->d_lam2, ns)) || (rc = dalloc(e, &e->d_mu, ne)) ||
-         (rc = dalloc(e, &e->d_gp, nf)) || (rc = dalloc(e, &e->d_gq, nf)) || (rc = dalloc(e, &e->d_gprior, nv)) ||
-         (rc = dalloc(e, &e->d_gs, nv))))
-        return rc;
-    // dL/dS_v = dL/db_v * b (1 - b) at the final beliefs
-    std::vector<double> b(nv, 0.0), gs(nv, 0.0);
-    if (L.V) {
-        FLBP_CUDA(cudaMemcpyAsync(b.data(), e->d_belief, (size_t)L.V * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
-        FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    return adjoint_backward_dev(e, grad_beliefs, grad_p, grad_q);
+}
+
+int flbp_get_beliefs_device(flbp_engine *e, double *out, int64_t n) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    if (n != e->L.V) {
+        set_error("output length must equal the number of variables");
+        return FLBP_ERR_INVALID;
     }
-    for (int64_t i = 0; i < L.V; i++) {
-        const uint32_t iv = L.internal_of_var[i];
-        const double g = grad_beliefs ? grad_beliefs[i] : 0.0;
-        gs[iv] = std::isfinite(b[iv]) ? g * b[iv] * (1.0 - b[iv]) : 0.0;
-    }
-    if ((rc = upload(e, e->d_gs, gs))) return rc;
-    FLBP_CUDA(cudaMemsetAsync(e->d_gp, 0, nf * sizeof(double), e->stream));
-    FLBP_CUDA(cudaMemsetAsync(e->d_gq, 0, nf * sizeof(double), e->stream));
-    FLBP_CUDA(cudaMemsetAsync(e->d_gprior, 0, nv * sizeof(double), e->stream));
-    FLBP_CUDA(cudaMemsetAsync(e->d_lam, 0, ns * sizeof(double), e->stream));
-    reset_ctl_for_run(e, 0);
-    if ((rc = upload_ctl(e))) return rc;
-    const long long T = e->adj_t, K = e->adj_k;
-    const long long nck = (T + K - 1) / K;
-    double *lam_next = e->d_lam, *lam_cur = e->d_lam2;
-    for (long long c = nck - 1; c >= 0; c--) {
-        const long long t0 = c * K, n1 = std::min<long long>(K, T - t0);
-        // recompute the segment's states from its checkpoint
-        FLBP_CUDA(cudaMemcpyAsync(e->d_vf, (char *)e->d_ckpt + (size_t)c * ns * e->tsize, ns * e->tsize,
-                                  cudaMemcpyDeviceToDevice, e->stream));
-        for (long long i = 0; i < n1; i++) {
-            FLBP_CUDA(cudaMemcpyAsync((char *)e->d_seg_vf + (size_t)i * ns * e->tsize, e->d_vf, ns * e->tsize,
-                                      cudaMemcpyDeviceToDevice, e->stream));
-            launch_sweep_any(e, 0, 1);
-            FLBP_CUDA(cudaMemcpyAsync((char *)e->d_seg_fv + (size_t)i * ne * e->tsize, e->d_fv, ne * e->tsize,
-                                      cudaMemcpyDeviceToDevice, e->stream));
-            launch_sweep_any(e, 0, 2);
-            e->launches += 2;
-        }
-        for (long long i = n1 - 1; i >= 0; i--) {
-            const void *vf = (char *)e->d_seg_vf + (size_t)i * ns * e->tsize;
-            const void *fv = (char *)e->d_seg_fv + (size_t)i * ne * e->tsize;
-            const double *gsp = (t0 + i == T - 1) ? e->d_gs : nullptr;
-            if (e->prec == 64) launch_adjoint_step<double>(e, vf, fv, lam_next, gsp, lam_cur);
-            else launch_adjoint_step<float>(e, vf, fv, lam_next, gsp, lam_cur);
-            std::swap(lam_next, lam_cur);
-        }
+    if ((rc = ensure_adjoint_maps(e))) return rc;
+    if (n) {
+        gather_vars_kernel<<<blocks_for(n, 256), 256, 0, e->stream>>>(e->d_belief, e->d_int_of_var, n, out);
+        e->launches += 1;
     }
     FLBP_CUDA(cudaGetLastError());
-    if ((rc = download_ctl(e))) return rc;
-    std::vector<double> gp(nf), gq(nf), gpr(nv);
-    FLBP_CUDA(cudaMemcpyAsync(gp.data(), e->d_gp, nf * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
-    FLBP_CUDA(cudaMemcpyAsync(gq.data(), e->d_gq, nf * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
-    FLBP_CUDA(cudaMemcpyAsync(gpr.data(), e->d_gprior, nv * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
     FLBP_CUDA(cudaStreamSynchronize(e->stream));
-    for (int64_t I = 0; I < L.F; I++) {
-        if (grad_p) grad_p[I] = 0.0;
-        if (grad_q) grad_q[I] = 0.0;
-    }
-    for (uint32_t f = 0; f < L.nf_sell + L.nf_big; f++) {
-        const uint32_t I = L.factor_of_internal[f];
-        if (grad_p) grad_p[I] += gp[f];
-        if (grad_q) grad_q[I] += gq[f];
-    }
-    // folded constants sign * logit(p): d/dp = sign / (p (1 - p))
-    for (size_t k = 0; k < L.prior_factor.size(); k++) {
-        const uint32_t I = L.prior_factor[k];
-        const double p = e->factor_p_host.empty() ? 0.5 : e->factor_p_host[I];
-        if (grad_p && p > 0.0 && p < 1.0) grad_p[I] += gpr[L.prior_var[k]] * L.prior_sign[k] / (p * (1.0 - p));
-    }
     return FLBP_OK;
 }
 
@@ -1346,6 +1507,7 @@ int flbp_set_factor_probs(flbp_engine *e, const double *p, const double *q) {
         }
     }
     e->factor_p_host.assign(p, p + L.F);
+    e->pri_coef_valid = false;
     const uint32_t nf = L.nf_sell + L.nf_big;
     for (uint32_t f = 0; f < nf; f++) {
         L.f_pq[2 * f] = p[L.factor_of_internal[f]];

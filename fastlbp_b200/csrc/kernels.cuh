@@ -940,7 +940,7 @@ __device__ __forceinline__ void decode_prior(const void *pr, uint32_t i, double 
         cnt = x.z;
     }
     npos = (int)(cnt & 0xffffu);
-    nneg = (int)(cnt >> 16);
+    nneg = (int)((cnt >> 16) & 0x7fffu);  // bit 31: the variable has a folded finite constant (adjoint)
 }
 
 

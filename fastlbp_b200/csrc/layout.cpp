@@ -451,7 +451,7 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
             if (c == kInf) {
                 if ((L.prior_cnt[iv] & 0xffffu) != 0xffffu) L.prior_cnt[iv] += 1u;
             } else if (c == -kInf) {
-                if ((L.prior_cnt[iv] >> 16) != 0xffffu) L.prior_cnt[iv] += 1u << 16;
+                if (((L.prior_cnt[iv] >> 16) & 0x7fffu) != 0x7fffu) L.prior_cnt[iv] += 1u << 16;
             } else {
                 fin[iv] += c;
                 // finite constant: +-logit(p) of a singleton or of an AND/OR factor reduced to its head

@@ -294,6 +294,20 @@ def config3_graph(index: int, seed: int = 3):
     return fl, dict(zip(al.tolist(), vals.tolist()))
 
 
+def config4_graph(index: int, seed: int = 4, n_tuples: int = 50_000, n_labels: int = 200):
+    """Graph ``index`` of the gradient set: config-0 laws at ``n_tuples``
+    tuples (rules = 1.5 x tuples, 5 % inputs at 0.99, AND fan-in 2-4, OR
+    fan-in 1-6, 10 % back edges, p ~ U[0.85, 0.99]) with ``n_labels``
+    labelled alarm tuples, labels Bernoulli(0.3). Returns (factors, alarm
+    labels, labels)."""
+    rng = np.random.default_rng([seed, index])
+    fl = bingo_graph(n_tuples, int(1.5 * n_tuples), max(10, n_tuples // 20), uniform_int(2, 4), uniform_int(1, 6),
+                     int(rng.integers(1 << 31)), n_layers=8, back_frac=0.10, p_lo=0.85, p_hi=0.99,
+                     input_prior=0.99, n_alarms=n_labels)
+    y = (rng.random(fl.alarms.size) < 0.3).astype(np.float64)
+    return fl, fl.alarms.copy(), y
+
+
 def config3_sizes(n_graphs: int = 512, seed: int = 3) -> np.ndarray:
     return np.array([int(math.exp(np.random.default_rng([seed, i]).uniform(math.log(1000), math.log(200_000))))
                      for i in range(n_graphs)])

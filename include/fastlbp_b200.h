@@ -294,12 +294,22 @@ int flbp_batch_run_tol(flbp_engine *eng, double tol, int64_t maxiter, double max
  * the beliefs after the last sweep (n = number of variables; may be NULL).
  * flbp_adjoint_backward: given dL/dbelief for every variable, the gradient
  * of L with respect to every factor's p and q (reference factor order; NULL
- * allowed), by reversing the sweeps of the last forward run: each segment
+ * allowed, and a NULL grad_q also skips accumulating dL/dq), by reversing
+ * the sweeps of the last forward run: each segment
  * between checkpoints is recomputed, then the adjoint kernels run backwards
  * through it. Singleton priors and AND/OR factors reduced to their head get
  * their p gradient through the folded constant logit(p). */
 int flbp_adjoint_forward(flbp_engine *eng, int64_t sweeps, int64_t every, double *beliefs, int64_t n);
 int flbp_adjoint_backward(flbp_engine *eng, const double *grad_beliefs, double *grad_p, double *grad_q);
+
+/* flbp_adjoint_backward on device buffers of the engine's device, in the
+ * same orders (grad_p / grad_q may be NULL). The caller's writes to
+ * grad_beliefs must be complete before the call; the gradients are complete
+ * when it returns. */
+int flbp_adjoint_backward_device(flbp_engine *eng, const double *grad_beliefs, double *grad_p, double *grad_q);
+
+/* flbp_get_beliefs into a device buffer of the engine's device. */
+int flbp_get_beliefs_device(flbp_engine *eng, double *out, int64_t n_vars);
 
 /* New p and q for every factor (reference order) of an existing engine, e.g.
  * after a learning step: constants folded into priors follow. The graph's

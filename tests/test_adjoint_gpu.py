@@ -7,7 +7,9 @@ sweeps; gradient with respect to every factor's p (rule firing
 probabilities, input priors). Tolerances: FP64 adjoint against the torch
 reference 1e-7 relative (both exact up to rounding), against central
 differences (eps 1e-6) 1e-4 relative; the FP32 engine's adjoint (FP32
-states, FP64 derivative arithmetic) against the FP64 one 2e-3 relative.
+states and derivative arithmetic) against the FP64 one 2e-3 relative (L2).
+The device-buffer entry points give the host-buffer results bit for bit,
+and a batch engine's gradient is its graphs' gradients side by side.
 """
 
 import numpy as np
@@ -15,7 +17,7 @@ import pytest
 import torch
 
 import torch_bp
-from fastlbp_b200 import CausalFactorGraph, Engine, workloads
+from fastlbp_b200 import BatchEngine, CausalFactorGraph, Engine, workloads
 from fastlbp_b200.autograd import unrolled_beliefs
 from test_engine_gpu import _large_item_graph
 
@@ -102,3 +104,60 @@ def test_fp32_adjoint_close_to_fp64():
         grads[prec] = p.grad.numpy()
     g64, g32 = grads[64], grads[32]
     assert np.linalg.norm(g32 - g64) <= 2e-3 * np.linalg.norm(g64)
+
+
+def test_device_entry_points_match_host():
+    a = _graph("large")
+    T, K = 10, 3
+    idx, y = _labels(a, seed=4)
+    eng = Engine(a, precision=32)
+    b_host = eng.adjoint_forward(T, K)
+    bd = torch.empty(eng.n_vars, dtype=torch.float64, device="cuda")
+    eng.beliefs_device(bd)
+    assert np.array_equal(bd.cpu().numpy(), b_host)
+    g = np.zeros(eng.n_vars)
+    g[idx] = np.random.default_rng(5).standard_normal(idx.size)
+    gp_h, gq_h = eng.adjoint_backward(g)
+    gp = torch.empty(eng.n_factors, dtype=torch.float64, device="cuda")
+    gq = torch.empty_like(gp)
+    eng.adjoint_backward_device(torch.as_tensor(g, device="cuda"), gp, gq)
+    assert np.array_equal(gp.cpu().numpy(), gp_h) and np.array_equal(gq.cpu().numpy(), gq_h)
+    assert np.max(np.abs(gp_h)) > 0
+    gp_only, none = eng.adjoint_backward(g, want_q=False)  # dL/dq not accumulated: dL/dp unchanged
+    assert none is None and np.array_equal(gp_only, gp_h)
+    # the autograd bridge on CUDA tensors against the host path (labels on
+    # variables whose beliefs are not exactly 0 or 1, where the loss is finite)
+    keep = (b_host[idx] > 0) & (b_host[idx] < 1)
+    yt, it = torch.as_tensor(y[keep]), torch.as_tensor(idx[keep])
+    p = torch.tensor(np.asarray(a["factor_p"], np.float64), requires_grad=True)
+    _bce(unrolled_beliefs(p, eng, a["factor_q"], T, K), it, yt).backward()
+    pd = torch.tensor(np.asarray(a["factor_p"], np.float64), device="cuda", requires_grad=True)
+    _bce(unrolled_beliefs(pd, eng, a["factor_q"], T, K), it.cuda(), yt.cuda()).backward()
+    want, got = p.grad.numpy(), pd.grad.cpu().numpy()
+    assert np.max(np.abs(got - want)) <= 1e-12 * np.max(np.abs(want))
+
+
+def test_batch_gradient_is_per_graph_gradients():
+    graphs = [_graph("bingo"), _graph("large")]
+    T, K = 12, 4
+    labels = [_labels(a, seed=6 + k) for k, a in enumerate(graphs)]
+    want_p, want_q = [], []
+    for a, (idx, y) in zip(graphs, labels):
+        e = Engine(a, precision=64)
+        b = e.adjoint_forward(T, K)
+        g = np.zeros(e.n_vars)
+        g[idx] = -y / b[idx] + (1 - y) / (1 - b[idx])
+        gp, gq = e.adjoint_backward(g)
+        want_p.append(gp)
+        want_q.append(gq)
+        e.close()
+    be = BatchEngine(graphs, precision=64)
+    b = be.adjoint_forward(T, K)
+    g = np.zeros(be.n_vars)
+    for k, (idx, y) in enumerate(labels):
+        j = be.var_off[k] + idx
+        g[j] = -y / b[j] + (1 - y) / (1 - b[j])
+    gp, gq = be.adjoint_backward(g)
+    wp, wq = np.concatenate(want_p), np.concatenate(want_q)
+    assert np.max(np.abs(gp - wp)) <= 1e-9 * np.max(np.abs(wp))
+    assert np.max(np.abs(gq - wq)) <= 1e-9 * max(np.max(np.abs(wq)), 1e-300)

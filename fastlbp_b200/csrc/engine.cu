@@ -69,6 +69,7 @@ struct flbp_engine {
     // Adjoint: checkpoints of vf every adj_k sweeps of the last adjoint forward
     // run (adj_t sweeps), per-sweep states of one segment, and derivatives.
     long long adj_t = 0, adj_k = 0;
+    bool adj_last_seg = false;  // the segment buffers hold the last segment's states (from the forward run)
     void *d_ckpt = nullptr, *d_seg_vf = nullptr, *d_seg_fv = nullptr;
     // in the message type: lambdas per entry (two), mu per slot, dL/dp and
     // dL/dq per internal factor, dL/dprior and dL/dS per internal variable
@@ -1252,6 +1253,46 @@ void launch_var_pass_on(flbp_engine *e, const void *fv, void *vf) {
     e->launches += 1;
 }
 
+// State buffers of the checkpointed runs: checkpoint c (vf at sweep c K),
+// and sweep i of the segment being differentiated (vf_i: the checkpoint for
+// i = 0, else segment slot i; fv_i: segment slot i).
+char *adj_ckpt(flbp_engine *e, long long c) {
+    return (char *)e->d_ckpt + (size_t)c * std::max<uint64_t>(1, e->L.n_slots) * e->tsize;
+}
+char *adj_seg_vf(flbp_engine *e, long long c, long long i) {
+    return i == 0 ? adj_ckpt(e, c) : (char *)e->d_seg_vf + (size_t)i * std::max<uint64_t>(1, e->L.n_slots) * e->tsize;
+}
+char *adj_seg_fv(flbp_engine *e, long long i) {
+    return (char *)e->d_seg_fv + (size_t)i * std::max<size_t>(1, e->n_ent) * e->tsize;
+}
+
+// The checkpointed forward run on explicit buffers: each segment's sweeps
+// start from its checkpoint, the last sweep of a segment writes the next
+// checkpoint, and the last segment keeps every state in the segment buffers
+// (its final variable pass writes the engine's vf, and fv_{T-1} is copied
+// to the engine's fv, so the engine state is that of T plain sweeps).
+template <typename T>
+int adjoint_forward_t(flbp_engine *e, long long T_, long long K) {
+    const size_t ns = std::max<uint64_t>(1, e->L.n_slots);
+    const long long nck = (T_ + K - 1) / K;
+    FLBP_CUDA(cudaMemsetAsync(adj_ckpt(e, 0), 0, ns * e->tsize, e->stream));  // the state after init()
+    for (long long c = 0; c < nck; c++) {
+        const long long n1 = std::min<long long>(K, T_ - c * K);
+        const bool last = c == nck - 1;
+        for (long long i = 0; i < n1; i++) {
+            const void *vin = i == 0 ? adj_ckpt(e, c) : (last ? adj_seg_vf(e, c, i) : e->d_vf);
+            void *fout = last ? adj_seg_fv(e, i) : e->d_fv;
+            void *vout = i + 1 < n1 ? (last ? adj_seg_vf(e, c, i + 1) : e->d_vf) : (last ? e->d_vf : adj_ckpt(e, c + 1));
+            launch_factor_pass_on<T>(e, vin, fout);
+            launch_var_pass_on<T>(e, fout, vout);
+        }
+        if (last && e->n_ent)
+            FLBP_CUDA(cudaMemcpyAsync(e->d_fv, adj_seg_fv(e, n1 - 1), e->n_ent * e->tsize, cudaMemcpyDeviceToDevice,
+                                      e->stream));
+    }
+    return FLBP_OK;
+}
+
 template <typename T>
 void launch_adjoint_seed(flbp_engine *e, const double *grad_b) {
     const int64_t V = e->L.V;
@@ -1342,28 +1383,22 @@ int adjoint_backward_t(flbp_engine *e, const double *grad_b, double *gp_out, dou
     if ((rc = upload_ctl(e))) return rc;
     const long long T_ = e->adj_t, K = e->adj_k;
     const long long nck = (T_ + K - 1) / K;
-    auto seg_vf = [&](long long i) { return (char *)e->d_seg_vf + (size_t)i * ns * ts; };
-    auto seg_fv = [&](long long i) { return (char *)e->d_seg_fv + (size_t)i * e->n_ent * ts; };
-    // Entries and slots that no pass writes hold constants: give every
-    // segment buffer the current arrays once, then only the passes write.
-    for (long long i = 0; i < (long long)e->adj_seg_n; i++) {
-        FLBP_CUDA(cudaMemcpyAsync(seg_vf(i), e->d_vf, ns * ts, cudaMemcpyDeviceToDevice, e->stream));
-        if (e->n_ent)
-            FLBP_CUDA(cudaMemcpyAsync(seg_fv(i), e->d_fv, e->n_ent * ts, cudaMemcpyDeviceToDevice, e->stream));
-    }
     void *lam_next = e->d_lam, *lam_cur = e->d_lam2;
     for (long long c = nck - 1; c >= 0; c--) {
         const long long t0 = c * K, n1 = std::min<long long>(K, T_ - t0);
-        // recompute the segment's states from its checkpoint: vf_i in seg_vf(i), fv_i in seg_fv(i)
-        FLBP_CUDA(cudaMemcpyAsync(seg_vf(0), (char *)e->d_ckpt + (size_t)c * ns * ts, ns * ts,
-                                  cudaMemcpyDeviceToDevice, e->stream));
-        for (long long i = 0; i < n1; i++) {
-            launch_factor_pass_on<T>(e, seg_vf(i), seg_fv(i));
-            if (i + 1 < n1) launch_var_pass_on<T>(e, seg_fv(i), seg_vf(i + 1));
+        // the segment's states: vf_i = adj_seg_vf(c, i), fv_i in seg_fv(i), recomputed
+        // from the checkpoint unless the forward run left them (last segment)
+        if (!(c == nck - 1 && e->adj_last_seg)) {
+            for (long long i = 0; i < n1; i++) {
+                launch_factor_pass_on<T>(e, adj_seg_vf(e, c, i), adj_seg_fv(e, i));
+                if (i + 1 < n1) launch_var_pass_on<T>(e, adj_seg_fv(e, i), adj_seg_vf(e, c, i + 1));
+            }
         }
+        e->adj_last_seg = false;  // the segment buffers are reused from here on
         for (long long i = n1 - 1; i >= 0; i--) {
             const void *gsp = (t0 + i == T_ - 1) ? e->d_gs : nullptr;
-            launch_adjoint_step<T>(e, seg_vf(i), seg_fv(i), lam_next, gsp, lam_cur, gq_out != nullptr);
+            launch_adjoint_step<T>(e, adj_seg_vf(e, c, i), adj_seg_fv(e, i), lam_next, gsp, lam_cur,
+                                   gq_out != nullptr);
             std::swap(lam_next, lam_cur);
         }
     }
@@ -1422,23 +1457,26 @@ int flbp_adjoint_forward(flbp_engine *e, int64_t sweeps, int64_t every, double *
         if ((rc = dalloc(e, (char **)&e->d_seg_vf, nseg * ns * e->tsize)) ||
             (rc = dalloc(e, (char **)&e->d_seg_fv, nseg * ne * e->tsize)))
             return rc;
+        // positions that no pass writes (padding) keep the value init() gives the
+        // engine's own arrays, zero; the segment recomputation writes the rest
+        FLBP_CUDA(cudaMemsetAsync(e->d_seg_vf, 0, nseg * ns * e->tsize, e->stream));
+        FLBP_CUDA(cudaMemsetAsync(e->d_seg_fv, 0, nseg * ne * e->tsize, e->stream));
         e->adj_seg_n = nseg;
     }
     if ((rc = flbp_init(e))) return rc;
+    e->adj_t = 0;
+    e->adj_last_seg = false;
     reset_ctl_for_run(e, 0);
     if ((rc = upload_ctl(e))) return rc;
-    for (size_t c = 0; c < nck; c++) {
-        FLBP_CUDA(cudaMemcpyAsync((char *)e->d_ckpt + c * ns * e->tsize, e->d_vf, ns * e->tsize,
-                                  cudaMemcpyDeviceToDevice, e->stream));
-        const long long n1 = std::min<long long>(every, sweeps - (long long)c * every);
-        if ((rc = launch_sweeps(e, 0, n1))) return rc;
-    }
+    if ((rc = e->prec == 64 ? adjoint_forward_t<double>(e, sweeps, every) : adjoint_forward_t<float>(e, sweeps, every)))
+        return rc;
     launch_beliefs_only(e, e->d_belief);
     if ((rc = download_ctl(e))) return rc;
     e->t += sweeps;
     e->iters += sweeps;
     e->adj_t = sweeps;
     e->adj_k = every;
+    e->adj_last_seg = true;
     if (beliefs) return fetch_internal(e, e->d_belief, beliefs, n);
     return FLBP_OK;
 }

@@ -161,3 +161,28 @@ def test_batch_gradient_is_per_graph_gradients():
     wp, wq = np.concatenate(want_p), np.concatenate(want_q)
     assert np.max(np.abs(gp - wp)) <= 1e-9 * np.max(np.abs(wp))
     assert np.max(np.abs(gq - wq)) <= 1e-9 * max(np.max(np.abs(wq)), 1e-300)
+
+
+@pytest.mark.parametrize("prec", [32, 64])
+def test_checkpointed_forward_is_the_plain_run(prec):
+    """adjoint_forward leaves the engine exactly where T plain sweeps do, and
+    a second backward (segment buffers reused) repeats the first."""
+    a = _graph("large")
+    T, K = 13, 4
+    eng = Engine(a, precision=prec)
+    b_ck = eng.adjoint_forward(T, K)
+    eng.sweep(3)
+    b_more = eng.compute_beliefs()
+    ref = Engine(a, precision=prec)
+    ref.init()
+    ref.run_fixed(T)
+    assert np.array_equal(b_ck, ref.beliefs())
+    ref.sweep(3)
+    assert np.array_equal(b_more, ref.compute_beliefs())
+    idx, y = _labels(a, seed=8)
+    g = np.zeros(eng.n_vars)
+    g[idx] = y - 0.5
+    eng.adjoint_forward(T, K)
+    g1 = eng.adjoint_backward(g)
+    g2 = eng.adjoint_backward(g)
+    assert np.array_equal(g1[0], g2[0]) and np.array_equal(g1[1], g2[1])

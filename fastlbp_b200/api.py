@@ -224,7 +224,11 @@ class Engine:
             lib().flbp_engine_destroy(h)
             self._h = None
 
-    __del__ = close
+    def __del__(self):
+        try:
+            self.close()
+        except (AttributeError, TypeError, ImportError):  # interpreter shutdown: modules already torn down
+            pass
 
     def init(self):
         check(lib().flbp_init(self._h))

@@ -24,6 +24,7 @@ SOURCES = ["engine.cu", "layout.cpp", "model.cpp", "causal_bp.cpp", "fg_capi.cpp
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "nvcc")
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-ccbin", "g++", "-Xcompiler", "-fPIC", "-I" + INCLUDE]
+OPENMP = ["-Xcompiler", "-fopenmp"]  # the host layout build runs on all host threads
 
 
 def _obj(src: str) -> str:
@@ -46,7 +47,7 @@ def _headers():
 
 def _compile(src: str, verbose: bool) -> str:
     path = os.path.join(CSRC, src)
-    cmd = [NVCC] + COMMON + ARCH + ["-c", path, "-o", _obj(src)]
+    cmd = [NVCC] + COMMON + OPENMP + ARCH + ["-c", path, "-o", _obj(src)]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
@@ -63,7 +64,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
             list(ex.map(lambda s: _compile(s, verbose), todo))
     objs = [_obj(s) for s in SOURCES]
     if force or todo or _needs(LIB, objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-ccbin", "g++", "-o", LIB] + objs
+        cmd = [NVCC] + ARCH + ["-shared", "-ccbin", "g++", "-o", LIB] + objs + ["-lgomp"]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)

@@ -82,6 +82,7 @@ struct flbp_engine {
     bool pri_coef_valid = false;
     double *d_adj_in = nullptr, *d_adj_out = nullptr;         // staging of the host-buffer backward call
     uint32_t *d_adj_groups = nullptr;  // sliced-ELL group ids by width class (see adj_group_n)
+    double *d_ref_out = nullptr;       // per-variable results in the caller's order (readback staging)
     uint32_t adj_group_n[4] = {0, 0, 0, 0};
     std::vector<double> factor_p_host;  // every reference factor's p (for derivatives of folded constants)
     uint8_t *d_f_kind = nullptr, *d_f_deg = nullptr;
@@ -379,8 +380,8 @@ int dalloc(flbp_engine *e, X **p, size_t n) {
     return FLBP_OK;
 }
 
-template <typename X>
-int upload(flbp_engine *e, X *dst, const std::vector<X> &src) {
+template <typename X, typename A>
+int upload(flbp_engine *e, X *dst, const std::vector<X, A> &src) {
     if (src.empty()) return FLBP_OK;
     FLBP_CUDA(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(X), cudaMemcpyHostToDevice, e->stream));
     e->h2d_bytes += src.size() * sizeof(X);
@@ -490,6 +491,7 @@ void packed_priors(const flbp_engine *e, size_t nv_pad, std::vector<uint32_t> &p
     // (its dL/dprior feeds a factor's dL/dp)
     std::vector<uint8_t> folded((size_t)L.V, 0);
     for (uint32_t v : L.prior_var) folded[v] = 1;
+#pragma omp parallel for if (L.V >= (1 << 15))
     for (int64_t i = 0; i < L.V; i++) {
         const uint32_t cnt = L.prior_cnt[i] | (folded[i] ? 0x80000000u : 0u);
         if (e->prec == 64) {
@@ -643,16 +645,23 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
     std::vector<uint8_t> kind_pad(nf_pad, 0), deg_pad(nf_pad, 0);
     std::copy(L.f_kind.begin(), L.f_kind.end(), kind_pad.begin());
     std::copy(L.f_deg.begin(), L.f_deg.end(), deg_pad.begin());
-    std::vector<double> pq64(2 * nf_pad, 0.0);
-    std::copy(L.f_pq.begin(), L.f_pq.end(), pq64.begin());
-    std::vector<float> pq32, bpq32;
+    // (p, q) of every factor in the message type, padded with zeros
+    auto padded_pq = [&](auto zero) {
+        using X = decltype(zero);
+        hvec<X> v(2 * nf_pad);
+        const int64_t n = (int64_t)v.size(), nr = (int64_t)L.f_pq.size();
+#pragma omp parallel for if (n >= (1 << 15))
+        for (int64_t i = 0; i < n; i++) v[i] = i < nr ? (X)L.f_pq[i] : X(0);
+        return v;
+    };
     if (e->prec == 64) {
-        if ((rc = upload(e, (double *)e->d_f_pq, pq64)) || (rc = upload(e, (double *)e->d_fbt_pq, L.fbt_pq)))
+        if ((rc = upload(e, (double *)e->d_f_pq, padded_pq(0.0))) ||
+            (rc = upload(e, (double *)e->d_fbt_pq, L.fbt_pq)))
             return fail(rc);
     } else {
-        pq32.assign(pq64.begin(), pq64.end());
-        bpq32.assign(L.fbt_pq.begin(), L.fbt_pq.end());
-        if ((rc = upload(e, (float *)e->d_f_pq, pq32)) || (rc = upload(e, (float *)e->d_fbt_pq, bpq32))) return fail(rc);
+        std::vector<float> bpq32(L.fbt_pq.begin(), L.fbt_pq.end());
+        if ((rc = upload(e, (float *)e->d_f_pq, padded_pq(0.0f))) || (rc = upload(e, (float *)e->d_fbt_pq, bpq32)))
+            return fail(rc);
     }
     if ((rc = upload(e, e->d_fg_base, L.fg_base)) || (rc = upload(e, e->d_fb_off, L.fb_off)) ||
         (rc = upload(e, e->d_f_pos, L.f_pos)) ||
@@ -662,7 +671,9 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
         (rc = upload(e, e->d_ftiles, L.fhdr)) || (rc = upload(e, e->d_vtiles, L.vhdr)) ||
         (rc = upload(e, e->d_fb_deg, L.fb_deg)) || (rc = upload(e, e->d_vb_deg, L.vb_deg)) ||
         (rc = upload(e, e->d_fbt_deg, L.fbt_deg)) || (rc = upload(e, e->d_vbt_deg, L.vbt_deg)) ||
-        (rc = upload(e, e->d_fbt_kind, L.fbt_kind)) || (rc = upload(e, (uint32_t *)e->d_vbt_prior, bt_prior)))
+        (rc = upload(e, e->d_fbt_kind, L.fbt_kind)) || (rc = upload(e, (uint32_t *)e->d_vbt_prior, bt_prior)) ||
+        (rc = dalloc(e, &e->d_int_of_var, L.internal_of_var.size())) ||
+        (rc = upload(e, e->d_int_of_var, L.internal_of_var)) || (rc = dalloc(e, &e->d_ref_out, (size_t)L.V)))
         return fail(rc);
     cudaError_t ce = cudaSuccess;
     if ((ce = cudaStreamSynchronize(e->stream)) != cudaSuccess ||
@@ -680,7 +691,7 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
         std::vector<uint32_t> fg(nf_pad, 0), vg(std::max<size_t>(1, nv_pad), 0);
         for (uint32_t f = 0; f < nf; f++) fg[f] = batch->factor_graph[L.factor_of_internal[f]];
         for (uint32_t iv = 0; iv < (uint32_t)L.V; iv++) vg[iv] = batch->var_graph[L.var_of_internal[iv]];
-        auto ranges = [](const std::vector<uint32_t> &hdr, uint32_t nt) {
+        auto ranges = [](const hvec<uint32_t> &hdr, uint32_t nt) {
             std::vector<uint2> r(std::max<uint32_t>(1, nt));
             for (uint32_t t = 0; t < nt; t++)
                 r[t] = make_uint2(hdr[(size_t)kHdrWordsHost * t + kHdrGraphLo], hdr[(size_t)kHdrWordsHost * t + kHdrGraphHi]);
@@ -717,7 +728,7 @@ int flbp_engine_destroy(flbp_engine *e) {
                     e->d_fbt_kind, e->d_fbt_pq, e->d_vbt_prior, e->d_f_graph, e->d_v_graph, e->d_gstate, e->d_ftrange, e->d_vtrange,
                     e->d_ckpt, e->d_seg_vf, e->d_seg_fv, e->d_lam, e->d_lam2, e->d_mu, e->d_gp, e->d_gq,
                     e->d_gprior, e->d_gs, e->d_int_of_var, e->d_f_of_int, e->d_pri_fac, e->d_pri_var, e->d_pri_coef,
-                    e->d_adj_in, e->d_adj_out, e->d_adj_groups};
+                    e->d_adj_in, e->d_adj_out, e->d_adj_groups, e->d_ref_out};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (e->h_ctl) cudaFreeHost(e->h_ctl);
@@ -869,17 +880,25 @@ int flbp_run_lowpass(flbp_engine *e, double tol, int64_t min_iters, int64_t max_
     return FLBP_OK;
 }
 
+// A per-variable device array in the caller's variable order, gathered on
+// the device and copied straight into `out`.
 static int fetch_internal(flbp_engine *e, const double *dsrc, double *out, int64_t n) {
     if (n != e->L.V) {
         set_error("output length must equal the number of variables");
         return FLBP_ERR_INVALID;
     }
-    std::vector<double> tmp((size_t)n);
-    if (n) {
-        FLBP_CUDA(cudaMemcpyAsync(tmp.data(), dsrc, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
-        FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    if (!n) return FLBP_OK;
+    int rc;
+    if (!e->d_int_of_var) {
+        std::vector<uint32_t> iov(e->L.internal_of_var.begin(), e->L.internal_of_var.end());
+        if ((rc = dalloc(e, &e->d_int_of_var, iov.size())) || (rc = upload(e, e->d_int_of_var, iov))) return rc;
     }
-    for (int64_t i = 0; i < n; i++) out[i] = tmp[e->L.internal_of_var[i]];
+    if (!e->d_ref_out && (rc = dalloc(e, &e->d_ref_out, (size_t)n))) return rc;
+    gather_vars_kernel<<<(unsigned)((n + 255) / 256), 256, 0, e->stream>>>(dsrc, e->d_int_of_var, n, e->d_ref_out);
+    e->launches += 1;
+    FLBP_CUDA(cudaGetLastError());
+    FLBP_CUDA(cudaMemcpyAsync(out, e->d_ref_out, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    FLBP_CUDA(cudaStreamSynchronize(e->stream));
     return FLBP_OK;
 }
 
@@ -1320,7 +1339,7 @@ void launch_adjoint_out(flbp_engine *e, double *gp_out, double *gq_out) {
 int ensure_adjoint_maps(flbp_engine *e) {
     int rc;
     const HostLayout &L = e->L;
-    if (!e->d_int_of_var) {
+    if (!e->d_adj_groups) {
         // sliced-ELL groups by width class: narrow var, wide var, narrow factor, wide factor
         std::vector<uint32_t> lists[4];
         for (uint32_t g = 0; g < L.n_vgroups(); g++)
@@ -1334,10 +1353,8 @@ int ensure_adjoint_maps(flbp_engine *e) {
         }
         if ((rc = dalloc(e, &e->d_adj_groups, all.size())) || (rc = upload(e, e->d_adj_groups, all))) return rc;
         const uint32_t nf = L.nf_sell + L.nf_big;
-        std::vector<uint32_t> iov(L.internal_of_var.begin(), L.internal_of_var.end());
         std::vector<uint32_t> foi(L.factor_of_internal.begin(), L.factor_of_internal.begin() + nf);
-        if ((rc = dalloc(e, &e->d_int_of_var, iov.size())) || (rc = upload(e, e->d_int_of_var, iov)) ||
-            (rc = dalloc(e, &e->d_f_of_int, foi.size())) || (rc = upload(e, e->d_f_of_int, foi)) ||
+        if ((rc = dalloc(e, &e->d_f_of_int, foi.size())) || (rc = upload(e, e->d_f_of_int, foi)) ||
             (rc = dalloc(e, &e->d_pri_fac, L.prior_factor.size())) || (rc = upload(e, e->d_pri_fac, L.prior_factor)) ||
             (rc = dalloc(e, &e->d_pri_var, L.prior_var.size())) || (rc = upload(e, e->d_pri_var, L.prior_var)) ||
             (rc = dalloc(e, &e->d_pri_coef, L.prior_factor.size())))

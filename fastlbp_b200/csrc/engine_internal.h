@@ -2,13 +2,63 @@
 // the CUDA engine (engine.cu). Not part of the public interface.
 #pragma once
 
+#include <sys/mman.h>
+
 #include <cstdint>
+#include <cstdlib>
+#include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/fastlbp_b200.h"
 
 namespace flbp {
+
+// Allocator of the host layout's arrays: blocks of 2 MiB and more are
+// 2 MiB-aligned and hinted for transparent huge pages, and elements are
+// default-initialised (resize() writes nothing), so that large arrays are
+// first touched by the parallel loops that fill them instead of being
+// zeroed page by page by one thread.
+template <class T>
+struct HostAlloc {
+    using value_type = T;
+    static constexpr size_t kHuge = size_t(2) << 20;
+    HostAlloc() = default;
+    template <class U>
+    HostAlloc(const HostAlloc<U> &) {}
+    T *allocate(size_t n) {
+        const size_t bytes = n * sizeof(T);
+        if (bytes < kHuge) return static_cast<T *>(::operator new(bytes));
+        const size_t al = (bytes + kHuge - 1) & ~(kHuge - 1);
+        void *p = std::aligned_alloc(kHuge, al);
+        if (!p) throw std::bad_alloc();
+        madvise(p, al, MADV_HUGEPAGE);
+        return static_cast<T *>(p);
+    }
+    void deallocate(T *p, size_t n) {
+        if (n * sizeof(T) < kHuge) ::operator delete(p);
+        else std::free(p);
+    }
+    template <class U>
+    void construct(U *p) noexcept {
+        ::new (static_cast<void *>(p)) U;
+    }
+    template <class U, class... A>
+    void construct(U *p, A &&...a) {
+        ::new (static_cast<void *>(p)) U(std::forward<A>(a)...);
+    }
+};
+template <class T, class U>
+bool operator==(const HostAlloc<T> &, const HostAlloc<U> &) {
+    return true;
+}
+template <class T, class U>
+bool operator!=(const HostAlloc<T> &, const HostAlloc<U> &) {
+    return false;
+}
+template <class T>
+using hvec = std::vector<T, HostAlloc<T>>;
 
 // Kind byte of an active AND/OR factor.
 enum : uint8_t {
@@ -60,64 +110,64 @@ struct HostLayout {
     int64_t V = 0, F = 0, E = 0;  // reference sizes
 
     uint32_t nf_sell = 0, nf_big = 0;  // active factors per path
-    std::vector<uint32_t> fg_base;     // n_fgroups + 1
-    std::vector<uint32_t> fb_off;      // nf_big + 1 (absolute slot ids; runs padded to kRunAlign)
-    std::vector<uint32_t> fb_deg;      // per big factor: degree (head included)
+    hvec<uint32_t> fg_base;     // n_fgroups + 1
+    hvec<uint32_t> fb_off;      // nf_big + 1 (absolute slot ids; runs padded to kRunAlign)
+    hvec<uint32_t> fb_deg;      // per big factor: degree (head included)
     uint32_t nf_huge = 0;              // big factors [0, nf_huge) are too large for a tile
-    std::vector<uint8_t> f_kind;       // per active factor (internal order)
-    std::vector<uint8_t> f_deg;        // per sell factor
-    std::vector<double> f_pq;          // 2 per active factor: p, q
+    hvec<uint8_t> f_kind;       // per active factor (internal order)
+    hvec<uint8_t> f_deg;        // per sell factor
+    hvec<double> f_pq;          // 2 per active factor: p, q
     uint64_t n_slots = 0;              // slots incl. padding
 
     uint32_t nv_sell = 0, nv_big = 0;
-    std::vector<uint32_t> vg_base;     // n_vgroups + 1 (entry ids)
-    std::vector<uint32_t> vb_off;      // nv_big + 1 (entry ids; runs padded to kRunAlign)
-    std::vector<uint32_t> vb_deg;      // per big variable: number of entries
+    hvec<uint32_t> vg_base;     // n_vgroups + 1 (entry ids)
+    hvec<uint32_t> vb_off;      // nv_big + 1 (entry ids; runs padded to kRunAlign)
+    hvec<uint32_t> vb_deg;      // per big variable: number of entries
     uint32_t nv_huge = 0;              // big variables [0, nv_huge) are too large for a tile
-    std::vector<uint32_t> v_ent;       // entries incl. padding
-    std::vector<uint32_t> f_pos;       // per slot: entry of its f->v message (kSentinel: none)
-    std::vector<double> prior_fin;     // per internal variable: finite constant log-odds (damping-scaled)
-    std::vector<uint32_t> prior_cnt;   // per internal variable: (#+inf) | (#-inf << 16)
+    hvec<uint32_t> v_ent;       // entries incl. padding
+    hvec<uint32_t> f_pos;       // per slot: entry of its f->v message (kSentinel: none)
+    hvec<double> prior_fin;     // per internal variable: finite constant log-odds (damping-scaled)
+    hvec<uint32_t> prior_cnt;   // per internal variable: (#+inf) | (#-inf << 16)
     // The finite constant messages folded into prior_fin: reference factor,
     // internal variable and sign (the constant is sign * logit(p)).
-    std::vector<uint32_t> prior_factor, prior_var;
-    std::vector<int8_t> prior_sign;
-    std::vector<uint32_t> var_of_internal;  // internal variable -> reference variable
-    std::vector<uint32_t> factor_of_internal;  // internal (active) factor -> reference factor
-    std::vector<uint32_t> internal_of_var;  // reference variable -> internal variable
+    hvec<uint32_t> prior_factor, prior_var;
+    hvec<int8_t> prior_sign;
+    hvec<uint32_t> var_of_internal;  // internal variable -> reference variable
+    hvec<uint32_t> factor_of_internal;  // internal (active) factor -> reference factor
+    hvec<uint32_t> internal_of_var;  // reference variable -> internal variable
     uint64_t n_active_slots = 0;       // real (non-padding) slots of active factors
 
     // Reference order, kept for message export: factor offsets, slot ->
     // variable, slot -> fv entry of its message (kSentinel: constant message),
     // factor -> its constant message.
-    std::vector<int64_t> ref_off;
-    std::vector<uint32_t> ref_slot_var;
-    std::vector<uint32_t> ref_ent;
-    std::vector<double> ref_fconst;
+    hvec<int64_t> ref_off;
+    hvec<uint32_t> ref_slot_var;
+    hvec<uint32_t> ref_ent;
+    hvec<double> ref_fconst;
     // Built by build_export_maps() on first use. Reference variable-major
     // slot (row_ptr_fv order) -> source of its f->v message: >= 0 fv entry;
     // -1 constant finite (value in ref_const, damping-scaled); -2 constant
     // +inf; -3 constant -inf.
     bool export_ready = false;
-    std::vector<int64_t> ref_fv_src;
-    std::vector<double> ref_const;
-    std::vector<int64_t> row_ptr_fv;  // reference variable-major CSR (V+1)
-    std::vector<int64_t> fm_to_vm;    // reference factor-major slot -> variable-major position
-    std::vector<int64_t> vm_var;      // variable-major position -> reference variable
+    hvec<int64_t> ref_fv_src;
+    hvec<double> ref_const;
+    hvec<int64_t> row_ptr_fv;  // reference variable-major CSR (V+1)
+    hvec<int64_t> fm_to_vm;    // reference factor-major slot -> variable-major position
+    hvec<int64_t> vm_var;      // variable-major position -> reference variable
 
     // Tiles: kHdrWordsHost-word headers. Word 0: first group (sliced ELL) or
     // first big item; word 1: item count n, | kBigTileFlag for a tile of big
     // items; words 2..2+n: slot (entry) offsets of the items and the end; the
     // remaining words repeat the end offset, except that word 31 of a big
     // tile holds its ordinal among the big tiles. Big tiles come first.
-    std::vector<uint32_t> fhdr, vhdr;
+    hvec<uint32_t> fhdr, vhdr;
     uint32_t n_ftiles = 0, n_vtiles = 0, n_fbtiles = 0, n_vbtiles = 0;
     // per big tile, kTileGroupsHost entries each: degree, kind, (p, q) of its factors;
     // number of entries of its variables
-    std::vector<uint32_t> fbt_deg;
-    std::vector<uint8_t> fbt_kind;
-    std::vector<double> fbt_pq;
-    std::vector<uint32_t> vbt_deg;
+    hvec<uint32_t> fbt_deg;
+    hvec<uint8_t> fbt_kind;
+    hvec<double> fbt_pq;
+    hvec<uint32_t> vbt_deg;
 
     uint32_t n_fgroups() const { return fg_base.empty() ? 0 : (uint32_t)fg_base.size() - 1; }
     uint32_t n_vgroups() const { return vg_base.empty() ? 0 : (uint32_t)vg_base.size() - 1; }

@@ -14,6 +14,12 @@
 //   degree with coalesced loads and no divergence; the head of every factor
 //   is its slot 0.
 // * All offsets and indices are 32-bit.
+//
+// The build runs on all host threads (OpenMP) and gives the same layout as
+// a sequential build: parallel counting sorts keep items in index order
+// within each class, and every per-item result is written by one thread.
+
+#include <omp.h>
 
 #include <algorithm>
 #include <cmath>
@@ -33,6 +39,114 @@ namespace {
 constexpr double kInf = std::numeric_limits<double>::infinity();
 
 inline double logit(double p) { return std::log(p) - std::log1p(-p); }
+
+// Items [0, n) cut into T contiguous chunks (T = 1 for small n), one per
+// parallel iteration, so that per-chunk results combine in index order.
+constexpr int64_t kParMin = 1 << 15;
+
+struct Chunks {
+    int T;
+    int64_t n, len;
+    int64_t lo(int t) const { return std::min(n, (int64_t)t * len); }
+    int64_t hi(int t) const { return std::min(n, (int64_t)(t + 1) * len); }
+};
+
+Chunks chunks(int64_t n, size_t nk = 1) {
+    int T = n >= kParMin ? omp_get_max_threads() : 1;
+    // per-chunk class counters stay below 32 M words
+    T = (int)std::max<int64_t>(1, std::min<int64_t>(T, (int64_t)(32u << 20) / (int64_t)std::max<size_t>(1, nk)));
+    return {T, n, std::max<int64_t>(1, (n + T - 1) / T)};
+}
+
+// Counting sort in two steps. class_counts: per chunk, the number of items
+// of each class k < nk (key(i) >= nk: not placed). class_place: put(i, pos)
+// for every placed item, pos = start[k] + the number of items of class k
+// before i, i.e. classes at the given starts, items of a class in index
+// order.
+template <typename Key>
+std::vector<uint64_t> class_counts(const Chunks &c, size_t nk, Key key) {
+    std::vector<uint64_t> cnt((size_t)c.T * nk, 0);
+#pragma omp parallel for schedule(static, 1) if (c.T > 1)
+    for (int t = 0; t < c.T; t++) {
+        uint64_t *h = &cnt[(size_t)t * nk];
+        for (int64_t i = c.lo(t); i < c.hi(t); i++) {
+            const size_t k = key(i);
+            if (k < nk) h[k]++;
+        }
+    }
+    return cnt;
+}
+
+template <typename Key, typename Put>
+void class_place(const Chunks &c, size_t nk, const std::vector<uint64_t> &cnt, const std::vector<uint64_t> &start,
+                 Key key, Put put) {
+    std::vector<uint64_t> at((size_t)c.T * nk);
+    for (size_t k = 0; k < nk; k++) {
+        uint64_t p = start[k];
+        for (int t = 0; t < c.T; t++) {
+            at[(size_t)t * nk + k] = p;
+            p += cnt[(size_t)t * nk + k];
+        }
+    }
+#pragma omp parallel for schedule(static, 1) if (c.T > 1)
+    for (int t = 0; t < c.T; t++) {
+        uint64_t *a = &at[(size_t)t * nk];
+        for (int64_t i = c.lo(t); i < c.hi(t); i++) {
+            const size_t k = key(i);
+            if (k < nk) put(i, a[k]++);
+        }
+    }
+}
+
+// Sizes of the classes (summed over chunks) and their starts from `base`.
+std::vector<uint64_t> class_starts(const Chunks &c, size_t nk, const std::vector<uint64_t> &cnt, uint64_t base,
+                                   std::vector<uint64_t> *sizes = nullptr) {
+    std::vector<uint64_t> start(nk + 1, base);
+    for (size_t k = 0; k < nk; k++) {
+        uint64_t sz = 0;
+        for (int t = 0; t < c.T; t++) sz += cnt[(size_t)t * nk + k];
+        start[k + 1] = start[k] + sz;
+    }
+    if (sizes) {
+        sizes->resize(nk);
+        for (size_t k = 0; k < nk; k++) (*sizes)[k] = start[k + 1] - start[k];
+    }
+    return start;
+}
+
+inline void atomic_min_u32(uint32_t *p, uint32_t v) {
+    uint32_t cur = __atomic_load_n(p, __ATOMIC_RELAXED);
+    while (v < cur && !__atomic_compare_exchange_n(p, &cur, v, true, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+    }
+}
+
+// v = n copies of x, filled by all threads (first touch spread over them).
+template <class T, class X>
+void par_assign(hvec<T> &v, size_t n, const X &x) {
+    hvec<T>().swap(v);
+    v.resize(n);  // default-initialised: nothing written yet
+    T *d = v.data();
+    const T val = (T)x;
+#pragma omp parallel for if ((int64_t)n >= kParMin)
+    for (int64_t i = 0; i < (int64_t)n; i++) d[i] = val;
+}
+
+template <class T, class X>
+hvec<T> par_vec(size_t n, const X &x) {
+    hvec<T> v;
+    par_assign(v, n, x);
+    return v;
+}
+
+// v = the range [first, first + n), copied by all threads.
+template <class T, class S>
+void par_copy(hvec<T> &v, const S *first, size_t n) {
+    hvec<T>().swap(v);
+    v.resize(n);
+    T *d = v.data();
+#pragma omp parallel for if ((int64_t)n >= kParMin)
+    for (int64_t i = 0; i < (int64_t)n; i++) d[i] = (T)first[i];
+}
 
 }  // namespace
 
@@ -60,15 +174,20 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
         err = "edge slots without factors";
         return FLBP_ERR_INVALID;
     }
-    for (int64_t I = 0; I < F; I++) {
-        if (off[I + 1] < off[I]) {
-            err = "factor_offsets not monotone at factor " + std::to_string(I);
+    {  // first offending index, as a sequential scan reports it
+        int64_t bad_f = F, bad_e = E;
+#pragma omp parallel for reduction(min : bad_f) if (F >= kParMin)
+        for (int64_t I = 0; I < F; I++)
+            if (off[I + 1] < off[I]) bad_f = std::min(bad_f, I);
+        if (bad_f < F) {
+            err = "factor_offsets not monotone at factor " + std::to_string(bad_f);
             return FLBP_ERR_INVALID;
         }
-    }
-    for (int64_t e = 0; e < E; e++) {
-        if (g.slot_var[e] < 0 || g.slot_var[e] >= V) {
-            err = "slot_var out of range at slot " + std::to_string(e);
+#pragma omp parallel for reduction(min : bad_e) if (E >= kParMin)
+        for (int64_t e = 0; e < E; e++)
+            if (g.slot_var[e] < 0 || g.slot_var[e] >= V) bad_e = std::min(bad_e, e);
+        if (bad_e < E) {
+            err = "slot_var out of range at slot " + std::to_string(bad_e);
             return FLBP_ERR_INVALID;
         }
     }
@@ -79,46 +198,37 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
     L.E = E;
 
     // --- classify factors -------------------------------------------------
-    std::vector<uint8_t> active(F, 0);
-    std::vector<uint8_t> head_state(F, HEAD_FREE);
-    std::vector<double> fconst(F, 0.0);  // constant message of non-active factors / clamped heads
-    for (int64_t I = 0; I < F; I++) {
+    hvec<uint8_t> active = par_vec<uint8_t>(F, 0);
+    hvec<uint8_t> head_state = par_vec<uint8_t>(F, HEAD_FREE);
+    hvec<double> fconst = par_vec<double>(F, 0.0);  // constant message of non-active factors / clamped heads
+    // classify factor I; false (with the message in *msg when given) for a malformed factor
+    auto classify = [&](int64_t I, std::string *msg) -> bool {
+        auto fail = [&](const std::string &m) {
+            if (msg) *msg = m;
+            return false;
+        };
         const int64_t d = off[I + 1] - off[I];
         const int32_t t = g.factor_type[I];
         const double p = g.factor_p[I], q = g.factor_q[I];
-        if (t != FLBP_SINGLETON && t != FLBP_AND && t != FLBP_OR) {
-            err = "unknown factor type at factor " + std::to_string(I);
-            return FLBP_ERR_INVALID;
-        }
-        if (!(p >= 0.0 && p <= 1.0) || !(q >= 0.0 && q <= 1.0)) {
-            err = "factor probabilities must lie in [0,1] (factor " + std::to_string(I) + ")";
-            return FLBP_ERR_INVALID;
-        }
-        if (d < 1) {
-            err = "factor without variables at factor " + std::to_string(I);
-            return FLBP_ERR_INVALID;
-        }
+        if (t != FLBP_SINGLETON && t != FLBP_AND && t != FLBP_OR)
+            return fail("unknown factor type at factor " + std::to_string(I));
+        if (!(p >= 0.0 && p <= 1.0) || !(q >= 0.0 && q <= 1.0))
+            return fail("factor probabilities must lie in [0,1] (factor " + std::to_string(I) + ")");
+        if (d < 1) return fail("factor without variables at factor " + std::to_string(I));
         const int64_t h = g.factor_head[I];
-        if (h < off[I] || h >= off[I + 1]) {
-            err = "factor_head outside the factor's slots at factor " + std::to_string(I);
-            return FLBP_ERR_INVALID;
-        }
+        if (h < off[I] || h >= off[I + 1])
+            return fail("factor_head outside the factor's slots at factor " + std::to_string(I));
         if (t == FLBP_SINGLETON) {
-            if (d != 1) {
-                err = "singleton factor with more than one variable at factor " + std::to_string(I);
-                return FLBP_ERR_INVALID;
-            }
+            if (d != 1) return fail("singleton factor with more than one variable at factor " + std::to_string(I));
             fconst[I] = logit(p);  // (1-p, p), causal_bp_parall.cu:110-112
-            continue;
+            return true;
         }
         bool clamped = g.factor_head_clamped && g.factor_head_clamped[I];
         if (clamped) {
             const double m0 = g.factor_mask0 ? g.factor_mask0[I] : 1.0;
             const double m1 = g.factor_mask1 ? g.factor_mask1[I] : 1.0;
-            if (!((m0 == 0.0 || m0 == 1.0) && (m1 == 0.0 || m1 == 1.0))) {
-                err = "head_mask entries must be 0 or 1 (factor " + std::to_string(I) + ")";
-                return FLBP_ERR_INVALID;
-            }
+            if (!((m0 == 0.0 || m0 == 1.0) && (m1 == 0.0 || m1 == 1.0)))
+                return fail("head_mask entries must be 0 or 1 (factor " + std::to_string(I) + ")");
             if (m0 == 1.0 && m1 == 1.0) {
                 clamped = false;  // multiplying by (1,1) changes nothing
             } else {
@@ -129,9 +239,20 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
         }
         if (d == 1) {
             if (!clamped) fconst[I] = (t == FLBP_AND) ? logit(p) : -logit(p);  // :115-117, :154-156
-            continue;
+            return true;
         }
         active[I] = 1;
+        return true;
+    };
+    {
+        int64_t bad = F;
+#pragma omp parallel for reduction(min : bad) if (F >= kParMin)
+        for (int64_t I = 0; I < F; I++)
+            if (!classify(I, nullptr)) bad = std::min(bad, I);
+        if (bad < F) {
+            classify(bad, &err);
+            return FLBP_ERR_INVALID;
+        }
     }
 
     // --- internal factor order: sliced-ELL factors by (graph, degree), then big ones ---
@@ -141,26 +262,24 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
     const uint32_t G = graphs ? graphs->n_graphs : 1;
     auto fgraph = [&](int64_t I) -> uint32_t { return graphs ? graphs->factor_graph[I] : 0u; };
     auto vgraph = [&](int64_t i) -> uint32_t { return graphs ? graphs->var_graph[i] : 0u; };
-    std::vector<int64_t> fact_of_int;
+    hvec<int64_t> fact_of_int;
     uint32_t nf_sell = 0, nf_big = 0;
     {
+        // classes (graph, degree) of the sliced-ELL factors, then one class of the large ones
         constexpr uint32_t D = kSellFactorDegree + 1;
-        std::vector<uint64_t> pos((size_t)G * D + 1, 0);
-        for (int64_t I = 0; I < F; I++) {
-            if (!active[I]) continue;
+        const size_t nk = (size_t)G * D + 1;
+        auto key = [&](int64_t I) -> size_t {
+            if (!active[I]) return nk;
             const uint64_t d = (uint64_t)(off[I + 1] - off[I]);
-            if (d <= kSellFactorDegree) pos[(size_t)fgraph(I) * D + d + 1]++, nf_sell++;
-            else nf_big++;
-        }
-        for (size_t k = 1; k < pos.size(); k++) pos[k] += pos[k - 1];
-        fact_of_int.assign((size_t)nf_sell + nf_big, 0);
-        uint32_t b = nf_sell;
-        for (int64_t I = 0; I < F; I++) {
-            if (!active[I]) continue;
-            const uint64_t d = (uint64_t)(off[I + 1] - off[I]);
-            if (d <= kSellFactorDegree) fact_of_int[pos[(size_t)fgraph(I) * D + d]++] = I;
-            else fact_of_int[b++] = I;
-        }
+            return d <= kSellFactorDegree ? (size_t)fgraph(I) * D + d : nk - 1;
+        };
+        const Chunks c = chunks(F, nk);
+        const std::vector<uint64_t> cnt = class_counts(c, nk, key);
+        const std::vector<uint64_t> start = class_starts(c, nk, cnt, 0);
+        nf_sell = (uint32_t)start[nk - 1];
+        nf_big = (uint32_t)(start[nk] - start[nk - 1]);
+        fact_of_int.resize((size_t)nf_sell + nf_big);  // every position is placed below
+        class_place(c, nk, cnt, start, key, [&](int64_t I, uint64_t at) { fact_of_int[at] = I; });
         // large factors: those too large for a tile first, then by (graph, decreasing
         // degree); warps deal them round-robin, largest first
         auto deg = [&](int64_t I) { return off[I + 1] - off[I]; };
@@ -172,12 +291,13 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
         });
     }
     const uint32_t nf = nf_sell + nf_big;
-    L.factor_of_internal.assign(fact_of_int.begin(), fact_of_int.end());
+    par_copy(L.factor_of_internal, fact_of_int.data(), fact_of_int.size());
     L.nf_sell = nf_sell;
     L.nf_big = nf_big;
-    L.f_kind.assign(nf, 0);
-    L.f_deg.assign(nf_sell, 0);
-    L.f_pq.assign(2 * (size_t)nf, 0.0);
+    par_assign(L.f_kind, nf, 0);
+    par_assign(L.f_deg, nf_sell, 0);
+    par_assign(L.f_pq, 2 * (size_t)nf, 0.0);
+#pragma omp parallel for if (nf >= kParMin)
     for (uint32_t f = 0; f < nf; f++) {
         const int64_t I = fact_of_int[f];
         L.f_kind[f] = (uint8_t)((g.factor_type[I] == FLBP_OR ? KIND_OR : 0) | head_state[I]);
@@ -187,56 +307,60 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
     }
 
     // --- device slots --------------------------------------------------------------
-    std::vector<uint32_t> dev_slot(E, UINT32_MAX);  // reference slot -> device slot
+    hvec<uint32_t> dev_slot = par_vec<uint32_t>(E, UINT32_MAX);  // reference slot -> device slot
     {
-        uint64_t next = 0;
+        // group widths and bases, then the big runs (sizes first, 64-bit), then the slots
         const uint32_t ng = (nf_sell + 31) / 32;
-        L.fg_base.assign(ng + 1, 0);
+        std::vector<uint64_t> gbase((size_t)ng + 1, 0);
+#pragma omp parallel for if (ng >= kParMin / 32)
         for (uint32_t gi = 0; gi < ng; gi++) {
-            const uint32_t f0 = gi * 32, f1 = std::min(nf_sell, gi * 32 + 32);
             uint32_t w = 0;
-            for (uint32_t f = f0; f < f1; f++) w = std::max<uint32_t>(w, L.f_deg[f]);
-            L.fg_base[gi] = (uint32_t)next;
-            for (uint32_t f = f0; f < f1; f++) {
-                const int64_t I = fact_of_int[f];
-                const uint32_t lane = f - f0;
-                uint64_t k = 0;
-                dev_slot[g.factor_head[I]] = (uint32_t)(next + lane);
-                for (int64_t e = off[I]; e < off[I + 1]; e++)
-                    if (e != g.factor_head[I]) dev_slot[e] = (uint32_t)(next + 32ull * (++k) + lane);
-            }
-            next += 32ull * w;
-            if (next >= UINT32_MAX) break;
+            for (uint32_t f = gi * 32; f < std::min(nf_sell, gi * 32 + 32); f++) w = std::max<uint32_t>(w, L.f_deg[f]);
+            gbase[gi + 1] = 32ull * w;
         }
-        if (next < UINT32_MAX) {
-            L.fg_base[ng] = (uint32_t)next;
-            L.fb_off.assign((size_t)nf_big + 1, 0);
-            L.fb_deg.assign(nf_big, 0);
-            for (uint32_t b = 0; b < nf_big && next < UINT32_MAX; b++) {
-                const int64_t I = fact_of_int[nf_sell + b];
-                L.fb_off[b] = (uint32_t)next;
-                L.fb_deg[b] = (uint32_t)(off[I + 1] - off[I]);
-                dev_slot[g.factor_head[I]] = (uint32_t)next++;
-                for (int64_t e = off[I]; e < off[I + 1]; e++)
-                    if (e != g.factor_head[I]) dev_slot[e] = (uint32_t)next++;
-                next = (next + kRunAlign - 1) & ~(uint64_t)(kRunAlign - 1);  // 16-byte aligned runs
-            }
+        for (uint32_t gi = 0; gi < ng; gi++) gbase[gi + 1] += gbase[gi];
+        std::vector<uint64_t> boff((size_t)nf_big + 1, gbase[ng]);
+        for (uint32_t b = 0; b < nf_big; b++) {
+            const int64_t I = fact_of_int[nf_sell + b];
+            boff[b + 1] = (boff[b] + (uint64_t)(off[I + 1] - off[I]) + kRunAlign - 1) & ~(uint64_t)(kRunAlign - 1);
         }
+        const uint64_t next = boff[nf_big];
         if (next >= UINT32_MAX) {
             err = "graph exceeds 2^32-1 device slots";
             return FLBP_ERR_LIMIT;
         }
-        L.fb_off[nf_big] = (uint32_t)next;
+        par_copy(L.fg_base, gbase.data(), gbase.size());
+        par_copy(L.fb_off, boff.data(), boff.size());
+        L.fb_deg.assign(nf_big, 0);
+#pragma omp parallel for if (nf_sell >= kParMin)
+        for (uint32_t f = 0; f < nf_sell; f++) {
+            const int64_t I = fact_of_int[f];
+            const uint64_t base = gbase[f / 32] + (f % 32);
+            uint64_t k = 0;
+            dev_slot[g.factor_head[I]] = (uint32_t)base;
+            for (int64_t e = off[I]; e < off[I + 1]; e++)
+                if (e != g.factor_head[I]) dev_slot[e] = (uint32_t)(base + 32ull * (++k));
+        }
+#pragma omp parallel for if (nf_big >= kParMin / 64)
+        for (uint32_t b = 0; b < nf_big; b++) {
+            const int64_t I = fact_of_int[nf_sell + b];
+            uint64_t at = boff[b];
+            L.fb_deg[b] = (uint32_t)(off[I + 1] - off[I]);
+            dev_slot[g.factor_head[I]] = (uint32_t)at++;
+            for (int64_t e = off[I]; e < off[I + 1]; e++)
+                if (e != g.factor_head[I]) dev_slot[e] = (uint32_t)at++;
+        }
         L.n_slots = next;
     }
 
     // --- variable entries ----------------------------------------------------------
     // A reference slot reaches its variable through the engine when it is an
     // active body slot or the head slot of an active factor with a free head.
-    std::vector<uint8_t> entry(E, 0);
-    std::vector<uint32_t> vdeg(V, 0);
-    std::vector<uint32_t> var_of_dev(L.n_slots, UINT32_MAX);  // device slot -> variable of its entry
+    hvec<uint8_t> entry = par_vec<uint8_t>(E, 0);
+    hvec<uint32_t> vdeg = par_vec<uint32_t>(V, 0);
+    hvec<uint32_t> var_of_dev = par_vec<uint32_t>(L.n_slots, UINT32_MAX);  // device slot -> variable of its entry
     uint64_t n_act = 0;
+#pragma omp parallel for reduction(+ : n_act) if (F >= kParMin)
     for (int64_t I = 0; I < F; I++) {
         if (!active[I]) continue;
         n_act += (uint64_t)(off[I + 1] - off[I]);
@@ -244,7 +368,7 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
             if (e == g.factor_head[I] && head_state[I] != HEAD_FREE) continue;
             entry[e] = 1;
             const uint32_t v = (uint32_t)g.slot_var[e];
-            vdeg[v]++;
+            __atomic_fetch_add(&vdeg[v], 1u, __ATOMIC_RELAXED);
             var_of_dev[dev_slot[e]] = v;
         }
     }
@@ -256,25 +380,39 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
     // for a tile first, the rest by (graph, decreasing degree). One scan over
     // the device slots in increasing order finds every variable's first slot.
     uint32_t nv_sell = 0;
-    std::vector<uint32_t> order(V);
+    hvec<uint32_t> order(V);  // every position is placed below
     {
+        // classes (graph, degree) of the sliced-ELL variables, then one class of the large ones
         constexpr uint32_t D = kSellVarDegree + 1;
-        std::vector<uint64_t> pos((size_t)G * D + 1, 0);
-        for (int64_t i = 0; i < V; i++)
-            if (vdeg[i] <= kSellVarDegree) pos[(size_t)vgraph(i) * D + vdeg[i] + 1]++, nv_sell++;
-        for (size_t k = 1; k < pos.size(); k++) pos[k] += pos[k - 1];
-        for (int64_t i = 0; i < V; i++)
-            if (vdeg[i] == 0) order[pos[(size_t)vgraph(i) * D]++] = (uint32_t)i;
-        std::vector<uint8_t> seen(V, 0);
-        for (uint64_t sl = 0; sl < L.n_slots; sl++) {
+        const size_t nk = (size_t)G * D + 1;
+        auto vkey = [&](int64_t i) -> size_t {
+            return vdeg[i] <= kSellVarDegree ? (size_t)vgraph(i) * D + vdeg[i] : nk - 1;
+        };
+        const Chunks cv = chunks(V, nk);
+        const std::vector<uint64_t> start = class_starts(cv, nk, class_counts(cv, nk, vkey), 0);
+        nv_sell = (uint32_t)start[nk - 1];
+        // variables without entries and the large ones in index order
+        auto key0 = [&](int64_t i) -> size_t {
+            const size_t k = vkey(i);
+            return (vdeg[i] == 0 || k == nk - 1) ? k : nk;
+        };
+        class_place(cv, nk, class_counts(cv, nk, key0), start, key0,
+                    [&](int64_t i, uint64_t at) { order[at] = (uint32_t)i; });
+        // the others in the order of their first device slot
+        hvec<uint32_t> first = par_vec<uint32_t>(V, UINT32_MAX);
+#pragma omp parallel for if (L.n_slots >= (uint64_t)kParMin)
+        for (int64_t sl = 0; sl < (int64_t)L.n_slots; sl++) {
             const uint32_t v = var_of_dev[sl];
-            if (v == UINT32_MAX || seen[v]) continue;
-            seen[v] = 1;
-            if (vdeg[v] <= kSellVarDegree) order[pos[(size_t)vgraph(v) * D + vdeg[v]]++] = v;
+            if (v != UINT32_MAX) atomic_min_u32(&first[v], (uint32_t)sl);
         }
-        uint32_t b = nv_sell;
-        for (int64_t i = 0; i < V; i++)
-            if (vdeg[i] > kSellVarDegree) order[b++] = (uint32_t)i;
+        auto skey = [&](int64_t sl) -> size_t {
+            const uint32_t v = var_of_dev[sl];
+            if (v == UINT32_MAX || first[v] != (uint32_t)sl || vdeg[v] > kSellVarDegree) return nk;
+            return (size_t)vgraph(v) * D + vdeg[v];
+        };
+        const Chunks cs = chunks((int64_t)L.n_slots, nk);
+        class_place(cs, nk, class_counts(cs, nk, skey), start, skey,
+                    [&](int64_t sl, uint64_t at) { order[at] = var_of_dev[sl]; });
         std::stable_sort(order.begin() + nv_sell, order.end(), [&](uint32_t x, uint32_t y) {
             const bool hx = vdeg[x] > kTileSlotsHost, hy = vdeg[y] > kTileSlotsHost;
             if (hx != hy) return hx;
@@ -284,30 +422,33 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
     }
     L.nv_sell = nv_sell;
     L.nv_big = (uint32_t)V - nv_sell;
-    L.var_of_internal.assign(order.begin(), order.end());
-    L.internal_of_var.assign(V, 0);
-    for (uint32_t iv = 0; iv < (uint32_t)V; iv++) L.internal_of_var[order[iv]] = iv;
+    par_copy(L.var_of_internal, order.data(), order.size());
+    L.internal_of_var.resize(V);  // a permutation: every position is written below
+#pragma omp parallel for if (V >= kParMin)
+    for (int64_t iv = 0; iv < V; iv++) L.internal_of_var[order[iv]] = (uint32_t)iv;
 
     // Entry positions: group base + 32 k + lane for sliced-ELL variables, a
     // contiguous run for large ones; entry k of a variable is its k-th device
     // slot in increasing order.
     {
         const uint32_t ng = (nv_sell + 31) / 32;
-        L.vg_base.assign(ng + 1, 0);
-        uint64_t nent = 0;
+        std::vector<uint64_t> gbase((size_t)ng + 1, 0);
+#pragma omp parallel for if (ng >= kParMin / 32)
         for (uint32_t gi = 0; gi < ng; gi++) {
             uint32_t w = 0;
             for (uint32_t iv = gi * 32; iv < std::min(nv_sell, gi * 32 + 32); iv++) w = std::max(w, vdeg[order[iv]]);
-            L.vg_base[gi] = (uint32_t)nent;
-            nent += 32ull * w;
+            gbase[gi + 1] = 32ull * w;
         }
+        for (uint32_t gi = 0; gi < ng; gi++) gbase[gi + 1] += gbase[gi];
+        const uint64_t nent = gbase[ng];
+        L.vg_base.assign(ng + 1, 0);
         uint64_t nbig = 0;
         for (uint32_t iv = nv_sell; iv < (uint32_t)V; iv++) nbig += (vdeg[order[iv]] + kRunAlign - 1) & ~(kRunAlign - 1);
         if (nent + nbig >= UINT32_MAX) {
             err = "graph exceeds 2^32-1 variable entries";
             return FLBP_ERR_LIMIT;
         }
-        L.vg_base[ng] = (uint32_t)nent;
+        std::copy(gbase.begin(), gbase.end(), L.vg_base.begin());
         L.vb_off.assign((size_t)L.nv_big + 1, 0);
         L.vb_deg.assign(L.nv_big, 0);
         uint64_t pos = nent;
@@ -318,8 +459,9 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
         }
         L.vb_off[L.nv_big] = (uint32_t)pos;
         // first entry position and stride of every variable
-        std::vector<uint32_t> epos(V), estride(V);
-        for (uint32_t iv = 0; iv < (uint32_t)V; iv++) {
+        hvec<uint32_t> epos(V), estride(V);  // written for every variable below
+#pragma omp parallel for if (V >= kParMin)
+        for (int64_t iv = 0; iv < V; iv++) {
             const uint32_t v = order[iv];
             if (iv < nv_sell) {
                 epos[v] = L.vg_base[iv / 32] + (iv % 32);
@@ -329,14 +471,61 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
                 estride[v] = 1;
             }
         }
-        L.v_ent.assign(pos, kSentinel);
-        L.f_pos.assign(L.n_slots, kSentinel);  // slot -> entry receiving its f->v message
-        for (uint64_t sl = 0; sl < L.n_slots; sl++) {
-            const uint32_t v = var_of_dev[sl];
-            if (v == UINT32_MAX) continue;
-            const uint32_t ep = epos[v];
-            epos[v] += estride[v];
-            L.v_ent[ep] = (uint32_t)sl;
+        par_assign(L.v_ent, pos, kSentinel);
+        par_assign(L.f_pos, L.n_slots, kSentinel);  // slot -> entry receiving its f->v message
+        // The (variable, device slot) pairs in slot order, stably radix-sorted
+        // by variable (11-bit digits): each variable's slots end up together
+        // in increasing order, and entry k of a variable gets its k-th.
+        hvec<uint32_t> kv, ks, kv2, ks2;  // variable, slot
+        {
+            constexpr int kBits = 11;
+            constexpr size_t nk = size_t(1) << kBits;
+            int passes = 1;
+            while (passes * kBits < 32 && ((uint64_t)V - 1) >> (passes * kBits)) passes++;
+            uint64_t n_ent = 0;
+            for (int64_t i = 0; i < V; i++) n_ent += vdeg[i];
+            kv.resize(n_ent);
+            ks.resize(n_ent);
+            kv2.resize(n_ent);
+            ks2.resize(n_ent);
+            for (int ps = 0; ps < passes; ps++) {
+                const int sh = ps * kBits;
+                if (ps == 0) {  // straight from the slots
+                    const Chunks c = chunks((int64_t)L.n_slots, nk);
+                    auto key = [&](int64_t sl) -> size_t {
+                        const uint32_t v = var_of_dev[sl];
+                        return v == UINT32_MAX ? nk : (v & (nk - 1));
+                    };
+                    const std::vector<uint64_t> cnt = class_counts(c, nk, key);
+                    class_place(c, nk, cnt, class_starts(c, nk, cnt, 0), key, [&](int64_t sl, uint64_t at) {
+                        kv2[at] = var_of_dev[sl];
+                        ks2[at] = (uint32_t)sl;
+                    });
+                } else {
+                    const Chunks c = chunks((int64_t)n_ent, nk);
+                    auto key = [&](int64_t i) -> size_t { return (kv[i] >> sh) & (nk - 1); };
+                    const std::vector<uint64_t> cnt = class_counts(c, nk, key);
+                    class_place(c, nk, cnt, class_starts(c, nk, cnt, 0), key, [&](int64_t i, uint64_t at) {
+                        kv2[at] = kv[i];
+                        ks2[at] = ks[i];
+                    });
+                }
+                kv.swap(kv2);
+                ks.swap(ks2);
+            }
+            hvec<uint32_t>().swap(kv2);
+            hvec<uint32_t>().swap(ks2);
+        }
+        // run starts: the first pair of every variable
+        hvec<uint64_t> vstart((size_t)V);
+#pragma omp parallel for if ((int64_t)kv.size() >= kParMin)
+        for (int64_t i = 0; i < (int64_t)kv.size(); i++)
+            if (i == 0 || kv[i - 1] != kv[i]) vstart[kv[i]] = (uint64_t)i;
+#pragma omp parallel for if ((int64_t)kv.size() >= kParMin)
+        for (int64_t i = 0; i < (int64_t)kv.size(); i++) {
+            const uint32_t v = kv[i], k = (uint32_t)(i - vstart[v]), sl = ks[i];
+            const uint32_t ep = epos[v] + k * estride[v];
+            L.v_ent[ep] = sl;
             L.f_pos[sl] = ep;
         }
     }
@@ -349,7 +538,7 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
     while (L.nf_huge < L.nf_big && L.fb_deg[L.nf_huge] - 1 > kBigFactorBody) L.nf_huge++;
     L.nv_huge = 0;
     while (L.nv_huge < L.nv_big && L.vb_deg[L.nv_huge] > kTileSlotsHost) L.nv_huge++;
-    auto push_hdr = [](std::vector<uint32_t> &h, uint32_t first, uint32_t nflag, const uint32_t *offs, uint32_t n,
+    auto push_hdr = [](hvec<uint32_t> &h, uint32_t first, uint32_t nflag, const uint32_t *offs, uint32_t n,
                        uint32_t ordinal) {
         const size_t at = h.size();
         h.push_back(first);
@@ -357,8 +546,8 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
         for (uint32_t j = 0; j + 2 < kHdrWordsHost; j++) h.push_back(offs[std::min(j, n)]);
         if (nflag & kBigTileFlag) h[at + kHdrWordsHost - 1] = ordinal;
     };
-    auto big_tiles = [&](const std::vector<uint32_t> &boff, const std::vector<uint32_t> &bdeg, uint32_t b0,
-                         uint32_t nb, std::vector<uint32_t> &hdr, std::vector<uint32_t> &firsts) -> uint32_t {
+    auto big_tiles = [&](const hvec<uint32_t> &boff, const hvec<uint32_t> &bdeg, uint32_t b0, uint32_t nb,
+                         hvec<uint32_t> &hdr, std::vector<uint32_t> &firsts) -> uint32_t {
         uint32_t nt = 0, b = b0;
         while (b < nb) {
             const uint32_t start = b;
@@ -371,7 +560,7 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
         (void)bdeg;
         return nt;
     };
-    auto sell_tiles = [&](const std::vector<uint32_t> &base, std::vector<uint32_t> &hdr) -> uint32_t {
+    auto sell_tiles = [&](const hvec<uint32_t> &base, hvec<uint32_t> &hdr) -> uint32_t {
         const uint32_t ng = base.empty() ? 0 : (uint32_t)base.size() - 1;
         uint32_t g = 0, nt = 0;
         while (g < ng) {
@@ -395,7 +584,7 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
     L.n_vtiles = L.n_vbtiles + sell_tiles(L.vg_base, L.vhdr);
     // batched engines: the range of graphs of every tile's items
     if (graphs) {
-        auto stamp = [&](std::vector<uint32_t> &hdr, uint32_t nt, uint32_t n_sell_items, auto item_graph) {
+        auto stamp = [&](hvec<uint32_t> &hdr, uint32_t nt, uint32_t n_sell_items, auto item_graph) {
             for (uint32_t t = 0; t < nt; t++) {
                 uint32_t *h = &hdr[(size_t)kHdrWordsHost * t];
                 const bool big = h[1] & kBigTileFlag;
@@ -440,13 +629,18 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
     }
 
     // --- priors ------------------------------------------------------------------
-    L.prior_fin.assign(V, 0.0);
-    L.prior_cnt.assign(V, 0);
+    par_assign(L.prior_fin, V, 0.0);
+    par_assign(L.prior_cnt, V, 0);
     {
-        std::vector<double> fin(V, 0.0);
-        for (int64_t I = 0; I < F; I++) {
-            if (active[I] && head_state[I] == HEAD_FREE) continue;
-            const uint32_t iv = L.internal_of_var[g.slot_var[g.factor_head[I]]];
+        hvec<double> fin = par_vec<double>(V, 0.0);
+        hvec<uint32_t> head_iv(F);  // internal variable of every folded factor's head (all written below)
+#pragma omp parallel for if (F >= kParMin)
+        for (int64_t I = 0; I < F; I++)
+            head_iv[I] = (active[I] && head_state[I] == HEAD_FREE) ? UINT32_MAX
+                                                                   : L.internal_of_var[g.slot_var[g.factor_head[I]]];
+        for (int64_t I = 0; I < F; I++) {  // in factor order: the sums and lists are order-dependent
+            if (head_iv[I] == UINT32_MAX) continue;
+            const uint32_t iv = head_iv[I];
             const double c = fconst[I];
             if (c == kInf) {
                 if ((L.prior_cnt[iv] & 0xffffu) != 0xffffu) L.prior_cnt[iv] += 1u;
@@ -460,13 +654,14 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
                 L.prior_sign.push_back(g.factor_type[I] == FLBP_OR ? -1 : 1);
             }
         }
-        L.prior_fin = fin;
+        L.prior_fin.swap(fin);
     }
 
     // --- reference-order data for message export (maps built on first use) ----------
-    L.ref_off.assign(off, off + F + 1);
-    L.ref_slot_var.resize(E);
+    par_copy(L.ref_off, off, (size_t)F + 1);
+    L.ref_slot_var.resize(E);  // both written for every slot below
     L.ref_ent.resize(E);
+#pragma omp parallel for if (E >= kParMin)
     for (int64_t e = 0; e < E; e++) {
         L.ref_slot_var[e] = (uint32_t)g.slot_var[e];
         L.ref_ent[e] = entry[e] ? L.f_pos[dev_slot[e]] : kSentinel;
@@ -485,7 +680,7 @@ void build_export_maps(HostLayout &L) {
     L.ref_const.assign(E, 0.0);
     L.fm_to_vm.assign(E, 0);
     L.vm_var.assign(E, 0);
-    std::vector<int64_t> cur(L.row_ptr_fv.begin(), L.row_ptr_fv.end() - 1);
+    hvec<int64_t> cur(L.row_ptr_fv.begin(), L.row_ptr_fv.end() - 1);
     for (int64_t I = 0; I < F; I++) {
         for (int64_t e = L.ref_off[I]; e < L.ref_off[I + 1]; e++) {
             const int64_t pos = cur[L.ref_slot_var[e]]++;

@@ -386,8 +386,10 @@ __device__ bool produce_tiles(const uint4 *thdr, const uint2 *trange, const uint
         const uint64_t t = dynamic ? (uint64_t)r * width + k : (uint64_t)blockIdx.x + ((uint64_t)r * width + k) * nb;
         return t < n_tiles ? (uint32_t)t : n_tiles;
     };
-    TileHdr h;
-    bool have_h = false;  // h holds the header of tile_at(round, 0)
+    // The round's tile headers, one per lane, loaded by the whole warp at
+    // once, so that lane 0 issues every stage's copies without waiting for a
+    // header load.
+    __shared__ uint4 s_hdr[32][kHdrWords / 4];
     while (ok && tile_at(round, 0) < n_tiles) {
         const uint32_t next = dynamic ? __shfl_sync(0xffffffffu, lane == 0 ? atomicAdd(counter, 1u) : 0u, 0)
                                       : round + 1;
@@ -400,9 +402,17 @@ __device__ bool produce_tiles(const uint4 *thdr, const uint2 *trange, const uint
             act = !stopped;
         }
         uint32_t bits = __ballot_sync(0xffffffffu, act);
+        if (act) {  // global -> shared without registers (16 B asynchronous copies)
+            const uint4 *src = thdr + (size_t)(kHdrWords / 4) * t;
+            const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&s_hdr[lane][0]);
+#pragma unroll
+            for (int i = 0; i < kHdrWords / 4; i++)
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + 16u * i), "l"(src + i) : "memory");
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncwarp();
         if (lane == 0) {
             int j = bits ? __ffs(bits) - 1 : -1;
-            if (j > 0 || (j == 0 && !have_h)) h.load(thdr + (size_t)(kHdrWords / 4) * tile_at(round, j));
             while (j >= 0) {
                 bits &= bits - 1;
                 const int s = (int)(issued % STAGES);
@@ -412,16 +422,14 @@ __device__ bool produce_tiles(const uint4 *thdr, const uint2 *trange, const uint
                 }
                 unsigned char *st = smem + (size_t)s * stage_bytes;
                 uint32_t *gb = reinterpret_cast<uint32_t *>(st);
-                h.store(gb);
+#pragma unroll
+                for (int i = 0; i < kHdrWords / 4; i++) reinterpret_cast<uint4 *>(gb)[i] = s_hdr[j][i];
                 fill(st, gb, &full[s]);
                 issued++;
                 j = bits ? __ffs(bits) - 1 : -1;
-                if (j >= 0) h.load(thdr + (size_t)(kHdrWords / 4) * tile_at(round, j));
             }
-            // the first header of the next round, while the stages are busy
-            have_h = tile_at(next, 0) < n_tiles;
-            if (ok && have_h) h.load(thdr + (size_t)(kHdrWords / 4) * tile_at(next, 0));
         }
+        __syncwarp();  // s_hdr is rewritten next round
         ok = __shfl_sync(0xffffffffu, ok, 0);
         round = next;
     }

@@ -172,12 +172,15 @@ VarArgs var_args(flbp_engine *e) {
     return a;
 }
 
-constexpr int kStages = 3;                        // bulk-copy pipeline depth of both passes
+constexpr int kStages = 3;  // bulk-copy pipeline depth of the variable pass (and of the FP64 factor pass)
+// FP32 factor-pass stages are small enough for a fourth with two blocks per SM
+template <typename T>
+constexpr int kFactorStages = sizeof(T) == 4 ? 4 : 3;
 constexpr int kBlockThreads = kBlockThreadsDev;  // 16 consumer warps + 1 producer warp
 
 template <typename T>
 constexpr size_t factor_smem() {
-    return (size_t)kStages * FactorStage<T>::bytes;
+    return (size_t)kFactorStages<T> * FactorStage<T>::bytes;
 }
 
 template <typename T, bool DAMP>
@@ -199,7 +202,7 @@ cudaError_t configure_kernels(bool damp, int *fb, int *vb) {
         cudaError_t e2 = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         if (e2 != cudaSuccess) err = e2;
     };
-    set((const void *)factor_pass_kernel<T, kStages>, factor_smem<T>());
+    set((const void *)factor_pass_kernel<T, kFactorStages<T>>, factor_smem<T>());
     set((const void *)var_pass_kernel<T, 0, true, false, kStages>, var_smem<T, false>());
     set((const void *)var_pass_kernel<T, 1, true, false, kStages>, var_smem<T, false>());
     set((const void *)var_pass_kernel<T, 2, true, false, kStages>, var_smem<T, false>());
@@ -209,7 +212,7 @@ cudaError_t configure_kernels(bool damp, int *fb, int *vb) {
     set((const void *)var_pass_kernel<T, 4, true, false, kStages>, var_smem<T, false>());
     set((const void *)var_pass_kernel<T, 4, true, true, kStages>, var_smem<T, true>());
     set((const void *)var_pass_kernel<T, 3, false, false, kStages>, var_smem<T, false>());
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(fb, factor_pass_kernel<T, kStages>, kBlockThreads, factor_smem<T>());
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(fb, factor_pass_kernel<T, kFactorStages<T>>, kBlockThreads, factor_smem<T>());
     if (damp)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(vb, var_pass_kernel<T, 2, true, true, kStages>, kBlockThreads,
                                                       var_smem<T, true>());
@@ -246,7 +249,7 @@ void launch_sweep(flbp_engine *e, int mode, int which = 3) {
             fa.trange = e->d_ftrange;
             fa.n_graphs = e->n_graphs;
         }
-        factor_pass_kernel<T, kStages><<<e->factor_grid, kBlockThreads, factor_smem<T>(), e->stream>>>(
+        factor_pass_kernel<T, kFactorStages<T>><<<e->factor_grid, kBlockThreads, factor_smem<T>(), e->stream>>>(
             fa, (const T *)e->d_vf, (T *)e->d_fv, e->d_ctl);
     }
     if (!(which & 2)) return;
@@ -1259,7 +1262,7 @@ void launch_adjoint_step(flbp_engine *e, const void *vf, const void *fv, const v
 template <typename T>
 void launch_factor_pass_on(flbp_engine *e, const void *vf, void *fv) {
     const FactorArgs fa = factor_args<T>(e);
-    factor_pass_kernel<T, kStages><<<e->factor_grid, kBlockThreads, factor_smem<T>(), e->stream>>>(
+    factor_pass_kernel<T, kFactorStages<T>><<<e->factor_grid, kBlockThreads, factor_smem<T>(), e->stream>>>(
         fa, (const T *)vf, (T *)fv, e->d_ctl);
     e->launches += 1;
 }

@@ -323,6 +323,16 @@ class Engine:
         check(lib().flbp_adjoint_backward(self._h, g, gp, gq))
         return gp, gq
 
+    def clamp(self, variables, values) -> None:
+        """Clamp variables (graph order) to 0/1 in place (flbp_clamp_vars): the
+        same solution as clamping the factor graph and building a new engine,
+        without the rebuild; takes effect from the next init()/run."""
+        v = np.ascontiguousarray(np.atleast_1d(variables), np.int64)
+        x = np.ascontiguousarray(np.atleast_1d(values), np.int32)
+        if v.shape != x.shape:
+            raise ValueError("one value per clamped variable")
+        check(lib().flbp_clamp_vars(self._h, v.size, v, x))
+
     def set_factor_probs(self, p: np.ndarray, q: np.ndarray) -> None:
         check(lib().flbp_set_factor_probs(self._h, np.ascontiguousarray(p, np.float64),
                                           np.ascontiguousarray(q, np.float64)))

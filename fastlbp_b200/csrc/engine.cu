@@ -85,6 +85,12 @@ struct flbp_engine {
     double *d_ref_out = nullptr;       // per-variable results in the caller's order (readback staging)
     uint32_t adj_group_n[4] = {0, 0, 0, 0};
     std::vector<double> factor_p_host;  // every reference factor's p (for derivatives of folded constants)
+    std::vector<int8_t> clamp_state;    // per reference variable: -1 free, else the value it is clamped to
+    // (slot, value) of every slot of a clamped variable: its v->f message is
+    // +-inf from init() on, as if the variable had left the factor
+    std::vector<uint32_t> clamp_slots;
+    uint32_t *d_clamp_slots = nullptr;
+    size_t clamp_slots_cap = 0;
     uint8_t *d_f_kind = nullptr, *d_f_deg = nullptr;
     void *d_prior = nullptr;
     double *d_belief = nullptr, *d_lowpass = nullptr, *d_hist = nullptr;
@@ -714,6 +720,25 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
     return FLBP_OK;
 }
 
+// The v->f messages of clamped variables: +inf (clamped to 1) or -inf (0).
+template <typename T>
+__global__ void clamp_slots_kernel(const uint32_t *__restrict__ pairs, uint32_t n, T *vf) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) vf[pairs[2 * i]] = pairs[2 * i + 1] ? Num<T>::inf() : -Num<T>::inf();
+}
+
+int apply_clamp_slots(flbp_engine *e) {
+    const uint32_t n = (uint32_t)(e->clamp_slots.size() / 2);
+    if (!n) return FLBP_OK;
+    if (e->prec == 64)
+        clamp_slots_kernel<double><<<(n + 255) / 256, 256, 0, e->stream>>>(e->d_clamp_slots, n, (double *)e->d_vf);
+    else
+        clamp_slots_kernel<float><<<(n + 255) / 256, 256, 0, e->stream>>>(e->d_clamp_slots, n, (float *)e->d_vf);
+    e->launches += 1;
+    FLBP_CUDA(cudaGetLastError());
+    return FLBP_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -731,7 +756,7 @@ int flbp_engine_destroy(flbp_engine *e) {
                     e->d_fbt_kind, e->d_fbt_pq, e->d_vbt_prior, e->d_f_graph, e->d_v_graph, e->d_gstate, e->d_ftrange, e->d_vtrange,
                     e->d_ckpt, e->d_seg_vf, e->d_seg_fv, e->d_lam, e->d_lam2, e->d_mu, e->d_gp, e->d_gq,
                     e->d_gprior, e->d_gs, e->d_int_of_var, e->d_f_of_int, e->d_pri_fac, e->d_pri_var, e->d_pri_coef,
-                    e->d_adj_in, e->d_adj_out, e->d_adj_groups, e->d_ref_out};
+                    e->d_adj_in, e->d_adj_out, e->d_adj_groups, e->d_ref_out, e->d_clamp_slots};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (e->h_ctl) cudaFreeHost(e->h_ctl);
@@ -749,6 +774,7 @@ int flbp_init(flbp_engine *e) {
     FLBP_CUDA(cudaMemsetAsync(e->d_vf, 0, ns * e->tsize, e->stream));
     FLBP_CUDA(cudaMemsetAsync(e->d_fv, 0, e->n_ent * e->tsize, e->stream));
     if (e->d_fvd) FLBP_CUDA(cudaMemsetAsync(e->d_fvd, 0, e->n_ent * e->tsize, e->stream));
+    if ((rc = apply_clamp_slots(e))) return rc;
     e->t = 0;
     e->lowpass_valid = false;
     return FLBP_OK;
@@ -1297,7 +1323,8 @@ template <typename T>
 int adjoint_forward_t(flbp_engine *e, long long T_, long long K) {
     const size_t ns = std::max<uint64_t>(1, e->L.n_slots);
     const long long nck = (T_ + K - 1) / K;
-    FLBP_CUDA(cudaMemsetAsync(adj_ckpt(e, 0), 0, ns * e->tsize, e->stream));  // the state after init()
+    FLBP_CUDA(cudaMemcpyAsync(adj_ckpt(e, 0), e->d_vf, ns * e->tsize, cudaMemcpyDeviceToDevice,
+                              e->stream));  // the state after init()
     for (long long c = 0; c < nck; c++) {
         const long long n1 = std::min<long long>(K, T_ - c * K);
         const bool last = c == nck - 1;
@@ -1599,6 +1626,181 @@ int flbp_set_factor_probs(flbp_engine *e, const double *p, const double *q) {
     if ((rc = upload(e, (uint32_t *)e->d_prior, prior)) || (rc = upload(e, (uint32_t *)e->d_vbt_prior, bt_prior)))
         return rc;
     FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    return FLBP_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------ incremental clamping
+
+namespace {
+
+// Applies a clamp batch: zero the listed f->v entries (and their damped
+// copies), mark the listed slots as sending to no entry, and write the
+// listed prior count words (engine priors and big-tile copies).
+template <typename T>
+__global__ void clamp_apply_kernel(const uint32_t *__restrict__ ents, uint32_t n_e, const uint32_t *__restrict__ pw,
+                                   uint32_t n_p, const uint32_t *__restrict__ bw, uint32_t n_b, T *fv, T *fvd,
+                                   uint32_t *f_pos, uint32_t *prior_words, uint32_t *bt_prior_words) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n_e) {
+        fv[ents[2 * i]] = T(0);
+        if (fvd) fvd[ents[2 * i]] = T(0);
+        f_pos[ents[2 * i + 1]] = kSentinel;
+    }
+    if (i < n_p) prior_words[pw[2 * i]] = pw[2 * i + 1];
+    if (i < n_b) bt_prior_words[bw[2 * i]] = bw[2 * i + 1];
+}
+
+}  // namespace
+
+extern "C" {
+
+int flbp_clamp_vars(flbp_engine *e, int64_t n, const int64_t *vars, const int32_t *values) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    HostLayout &L = e->L;
+    if (n < 0 || (n > 0 && (!vars || !values))) {
+        set_error("clamp list is malformed");
+        return FLBP_ERR_INVALID;
+    }
+    if (e->clamp_state.empty()) e->clamp_state.assign((size_t)L.V, -1);
+    for (int64_t k = 0; k < n; k++) {
+        if (vars[k] < 0 || vars[k] >= L.V) {
+            set_error("clamped variable out of range: " + std::to_string(vars[k]));
+            return FLBP_ERR_INVALID;
+        }
+        if (values[k] != 0 && values[k] != 1) {
+            set_error("clamp value must be 0 or 1 (variable " + std::to_string(vars[k]) + ")");
+            return FLBP_ERR_INVALID;
+        }
+        const int8_t st = e->clamp_state[vars[k]];
+        if (st >= 0 && st != values[k]) {
+            set_error("variable " + std::to_string(vars[k]) + " is already clamped to the other value");
+            return FLBP_ERR_INVALID;
+        }
+        for (int64_t j = 0; j < k; j++)
+            if (vars[j] == vars[k] && values[j] != values[k]) {
+                set_error("variable " + std::to_string(vars[k]) + " is clamped to both values");
+                return FLBP_ERR_INVALID;
+            }
+    }
+    std::vector<uint8_t> folded((size_t)L.V, 0);
+    for (uint32_t v : L.prior_var) folded[v] = 1;
+    const size_t pwords = e->prec == 64 ? 4 : 2, cword = e->prec == 64 ? 2 : 1;
+    std::vector<uint32_t> ents, pw, bw;  // (entry, slot), (word, value), (word, value)
+    for (int64_t k = 0; k < n; k++) {
+        if (e->clamp_state[vars[k]] >= 0) continue;  // clamping again to the same value changes nothing
+        e->clamp_state[vars[k]] = (int8_t)values[k];
+        const uint32_t iv = L.internal_of_var[vars[k]];
+        // the clamp: one exact-zero count in the variable's prior
+        uint32_t &cnt = L.prior_cnt[iv];
+        if (values[k]) {
+            if ((cnt & 0xffffu) != 0xffffu) cnt += 1u;
+        } else if (((cnt >> 16) & 0x7fffu) != 0x7fffu) {
+            cnt += 1u << 16;
+        }
+        const uint32_t word = cnt | (folded[iv] ? 0x80000000u : 0u);
+        pw.push_back((uint32_t)(pwords * iv + cword));
+        pw.push_back(word);
+        // its entries: no factor's message reaches it any more; its v->f
+        // messages are +-inf from init() on (it leaves every body it is in);
+        // a factor it kills (0 in an AND body, 1 in an OR body) leaves its
+        // other body variables too
+        auto cut = [&](uint32_t sl) {  // no message from slot sl any more
+            const uint32_t en = L.f_pos[sl];
+            if (en == kSentinel) return;
+            ents.push_back(en);
+            ents.push_back(sl);
+            L.f_pos[sl] = kSentinel;
+        };
+        auto entry = [&](uint32_t en) {
+            const uint32_t sl = L.v_ent[en];
+            if (sl == kSentinel) return;
+            cut(sl);
+            e->clamp_slots.push_back(sl);
+            e->clamp_slots.push_back((uint32_t)values[k]);
+            // the factor of slot sl, and sl's position in it (0 = head)
+            uint32_t f, pos, base, stride, deg;
+            if (sl < L.fg_base.back()) {
+                const uint32_t g = (uint32_t)(std::upper_bound(L.fg_base.begin(), L.fg_base.end(), sl) - L.fg_base.begin()) - 1;
+                const uint32_t off = sl - L.fg_base[g];
+                f = 32u * g + off % 32u;
+                pos = off / 32u;
+                base = L.fg_base[g] + off % 32u;
+                stride = 32;
+                deg = L.f_deg[f];
+            } else {
+                const uint32_t b = (uint32_t)(std::upper_bound(L.fb_off.begin(), L.fb_off.end(), sl) - L.fb_off.begin()) - 1;
+                f = L.nf_sell + b;
+                pos = sl - L.fb_off[b];
+                base = L.fb_off[b];
+                stride = 1;
+                deg = L.fb_deg[b];
+            }
+            const bool is_or = L.f_kind[f] & KIND_OR;
+            if (pos > 0 && ((values[k] == 0 && !is_or) || (values[k] == 1 && is_or)))
+                for (uint32_t j = 1; j < deg; j++)
+                    if (j != pos) cut(base + stride * j);
+        };
+        if (iv < L.nv_sell) {
+            const uint32_t g = iv / 32, lane = iv % 32, w = (L.vg_base[g + 1] - L.vg_base[g]) / 32;
+            for (uint32_t j = 0; j < w; j++) entry(L.vg_base[g] + 32u * j + lane);
+        } else {
+            const uint32_t b = iv - L.nv_sell;
+            for (uint32_t j = 0; j < L.vb_deg[b]; j++) entry(L.vb_off[b] + j);
+            for (uint32_t t = 0; t < L.n_vbtiles; t++) {  // the big-tile copy of its prior
+                const uint32_t *h = &L.vhdr[(size_t)kHdrWordsHost * t];
+                const uint32_t b0 = h[0], nb = h[1] & ~kBigTileFlag;
+                if (b >= b0 && b < b0 + nb) {
+                    bw.push_back((uint32_t)(pwords * ((size_t)kTileGroupsHost * t + (b - b0)) + cword));
+                    bw.push_back(word);
+                    break;
+                }
+            }
+        }
+    }
+    const uint32_t n_e = (uint32_t)(ents.size() / 2), n_p = (uint32_t)(pw.size() / 2), n_b = (uint32_t)(bw.size() / 2);
+    const uint32_t m = std::max(n_e, std::max(n_p, n_b));
+    if (m == 0) return FLBP_OK;
+    if (e->clamp_slots.size() > e->clamp_slots_cap) {  // the device copy of the clamped slots
+        if (e->d_clamp_slots) cudaFree(e->d_clamp_slots);
+        e->d_clamp_slots = nullptr;
+        e->clamp_slots_cap = 0;
+        if ((rc = dalloc(e, &e->d_clamp_slots, 2 * e->clamp_slots.size()))) return rc;
+        e->clamp_slots_cap = 2 * e->clamp_slots.size();
+    }
+    if ((rc = upload(e, e->d_clamp_slots, e->clamp_slots)) || (rc = apply_clamp_slots(e))) return rc;
+    uint32_t *d = nullptr;
+    FLBP_CUDA(cudaMalloc((void **)&d, (ents.size() + pw.size() + bw.size()) * sizeof(uint32_t)));
+    cudaError_t ce = cudaSuccess;
+    auto put = [&](const std::vector<uint32_t> &v, size_t at) {
+        if (!v.empty() && ce == cudaSuccess)
+            ce = cudaMemcpyAsync(d + at, v.data(), v.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, e->stream);
+    };
+    put(ents, 0);
+    put(pw, ents.size());
+    put(bw, ents.size() + pw.size());
+    if (ce == cudaSuccess) {
+        const unsigned blocks = (m + 255) / 256;
+        uint32_t *pwords_d = reinterpret_cast<uint32_t *>(e->d_prior), *bw_d = reinterpret_cast<uint32_t *>(e->d_vbt_prior);
+        if (e->prec == 64)
+            clamp_apply_kernel<double><<<blocks, 256, 0, e->stream>>>(
+                d, n_e, d + ents.size(), n_p, d + ents.size() + pw.size(), n_b, (double *)e->d_fv, (double *)e->d_fvd,
+                e->d_f_pos, pwords_d, bw_d);
+        else
+            clamp_apply_kernel<float><<<blocks, 256, 0, e->stream>>>(
+                d, n_e, d + ents.size(), n_p, d + ents.size() + pw.size(), n_b, (float *)e->d_fv, (float *)e->d_fvd,
+                e->d_f_pos, pwords_d, bw_d);
+        e->launches += 1;
+        ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    cudaFree(d);
+    if (ce != cudaSuccess) {
+        set_error(std::string("clamp update failed: ") + cudaGetErrorString(ce));
+        return FLBP_ERR_CUDA;
+    }
     return FLBP_OK;
 }
 

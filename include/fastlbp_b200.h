@@ -311,6 +311,22 @@ int flbp_adjoint_backward_device(flbp_engine *eng, const double *grad_beliefs, d
 /* flbp_get_beliefs into a device buffer of the engine's device. */
 int flbp_get_beliefs_device(flbp_engine *eng, double *out, int64_t n_vars);
 
+/* ---- incremental evidence (the alarm-ranking loop) ----
+ *
+ * Clamps variables (graph variable order) to 0 or 1 on an existing engine,
+ * with the effect of CausalFactorGraph::clamp on every neighbouring factor
+ * followed by a rebuild and a new engine (csrc/ext/causal_factor.cpp:63-100,
+ * csrc/ext/causal_fg.cpp:17-26; fl_wrapper.cu:29-45 and bingo_wrapper.cu
+ * rebuild after every label), without the rebuild: the variable gets an
+ * exact-zero count in its prior and no factor's message reaches it any
+ * more. An input at +-inf leaves a noisy-AND/OR product unchanged or zeroes
+ * it, which is exactly the reference's removal of the variable from a body
+ * or its "killed" factor (p := q, empty body). Takes effect from the next
+ * init()/run. Clamping a variable again to the same value changes nothing;
+ * to the other value is rejected (FLBP_ERR_INVALID). Messages exported
+ * afterwards (flbp_get_fv_messages) keep the unclamped graph's slots. */
+int flbp_clamp_vars(flbp_engine *eng, int64_t n, const int64_t *vars, const int32_t *values);
+
 /* New p and q for every factor (reference order) of an existing engine, e.g.
  * after a learning step: constants folded into priors follow. The graph's
  * structure (which factors are singletons, clamped or reduced) stays. */

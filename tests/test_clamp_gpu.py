@@ -1,0 +1,108 @@
+"""Incremental evidence (flbp_clamp_vars) against FastLBP's own sequence:
+clamp the factor graph (CausalFactorGraph::clamp on every neighbouring
+factor, csrc/ext/causal_factor.cpp:63-100), rebuild it and build a new
+engine, as fl_wrapper.cu:29-45 and bingo_wrapper.cu do after every label.
+
+Both runs start from init(); beliefs agree to 1e-9 (FP64) / 1e-5 (FP32)
+after a fixed number of sweeps, and tolerance runs stop after the same
+number of sweeps. Covered: AND bodies clamped to 0 (the reference "kills"
+the factor: p := q, empty body) and to 1 (the variable leaves the body), OR
+bodies alike, clamped heads of AND/OR factors and singletons, variables of
+the sliced-ELL, big-tile and block-cooperative size classes, damping, and
+clamps given in two batches.
+"""
+
+import numpy as np
+import pytest
+
+from fastlbp_b200 import CausalFactorGraph, Engine, FlbpError, workloads
+from test_engine_gpu import _large_item_graph
+
+pytestmark = pytest.mark.gpu
+
+
+def _bingo():
+    return workloads.bingo_graph(600, 900, 40, workloads.uniform_int(2, 4), workloads.uniform_int(1, 6), 11,
+                                 n_layers=6, back_frac=0.10, p_lo=0.6, p_hi=0.97, input_prior=0.8, n_alarms=30)
+
+
+def _clamps(fl, n, seed, extra=()):
+    """n clamps on random labels of the graph (heads and bodies alike), plus `extra`."""
+    g = CausalFactorGraph.from_factors(fl)
+    labels = g.var_labels()
+    rng = np.random.default_rng(seed)
+    pick = rng.choice(labels, size=min(n, labels.size), replace=False).tolist() + list(extra)
+    return {int(lab): int(rng.integers(0, 2)) for lab in pick}
+
+
+def _rebuilt(fl, clamps):
+    g = CausalFactorGraph.from_factors(fl)
+    g.clamp_labels(clamps)
+    return g.rebuild().graph_arrays()
+
+
+def _incremental(fl, clamps, batches=1, **kw):
+    g = CausalFactorGraph.from_factors(fl)
+    eng = Engine(g.graph_arrays(), **kw)
+    items = sorted(clamps.items())
+    for part in np.array_split(np.arange(len(items)), batches):
+        eng.clamp([g.findVar(items[i][0]) for i in part], [items[i][1] for i in part])
+    return eng
+
+
+@pytest.mark.parametrize("prec,tol", [(64, 1e-9), (32, 1e-5)])
+@pytest.mark.parametrize("kind", ["bingo", "large"])
+def test_clamp_matches_rebuilt_graph(kind, prec, tol):
+    if kind == "bingo":
+        fl, n = _bingo(), 60
+        extra = ()
+    else:
+        fl, n = _large_item_graph(4), 80
+        hub = 1200 + 30  # after 1,200 inputs and 30 large factors: the 2100-entry variable
+        extra = (hub, hub + 1 + 2100, 7, 1201)  # the hub, the big-tile variable, an input, a large factor's head
+    clamps = _clamps(fl, n, seed=5, extra=extra)
+    ref = Engine(_rebuilt(fl, clamps), precision=prec)
+    ref.init()
+    ref.run_fixed(30)
+    eng = _incremental(fl, clamps, batches=2, precision=prec)
+    eng.init()
+    eng.run_fixed(30)
+    want, got = ref.beliefs(), eng.beliefs()
+    assert want.shape == got.shape
+    assert np.array_equal(np.isnan(want), np.isnan(got))
+    ok = ~np.isnan(want)
+    assert np.max(np.abs(got[ok] - want[ok])) <= tol
+    # the tolerance loop stops after the same number of sweeps
+    ref.init()
+    a = ref.run_tol(1e-6, 400, 1e9)
+    eng.init()
+    b = eng.run_tol(1e-6, 400, 1e9)
+    assert a["sweeps"] == b["sweeps"]
+    assert np.max(np.abs(eng.beliefs()[ok] - ref.beliefs()[ok])) <= max(tol, 1e-6)
+
+
+def test_clamp_with_damping():
+    fl = _bingo()
+    clamps = _clamps(fl, 40, seed=6)
+    ref = Engine(_rebuilt(fl, clamps), precision=32, damping=0.1)
+    ref.init()
+    ref.run_fixed(40)
+    eng = _incremental(fl, clamps, precision=32, damping=0.1)
+    eng.init()
+    eng.run_fixed(40)
+    assert np.max(np.abs(eng.beliefs() - ref.beliefs())) <= 1e-5
+
+
+def test_clamp_rejects_conflicts():
+    fl = _bingo()
+    eng = Engine(CausalFactorGraph.from_factors(fl).graph_arrays(), precision=32)
+    eng.clamp([3], [1])
+    eng.clamp([3], [1])  # the same value again: nothing changes
+    with pytest.raises(FlbpError):
+        eng.clamp([3], [0])
+    with pytest.raises(FlbpError):
+        eng.clamp([5, 5], [0, 1])
+    with pytest.raises(FlbpError):
+        eng.clamp([eng.n_vars], [0])
+    with pytest.raises(FlbpError):
+        eng.clamp([4], [2])

@@ -55,11 +55,12 @@ def parse():
     ap.add_argument("--scale", type=float, default=1.0, help="graph size factor (1.0 = the 1M-variable graph)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
     ap.add_argument("--e2e-steps", type=int, default=4)
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "fl", "adjoint"],
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "fl", "adjoint", "bingo"],
                     help="single: the 1M-variable graph (default); batch: many uneven graphs solved together; "
                          "fl: the fault-localisation graph with its statement ranking against the FP64 oracle; "
                          "adjoint: gradients through unrolled sweeps on 64 graphs of 50k tuples "
-                         "(use --sweeps 100 --damping 0 --graphs 64)")
+                         "(use --sweeps 100 --damping 0 --graphs 64); "
+                         "bingo: re-solving after each label, rebuild against incremental clamps")
     ap.add_argument("--graphs", type=int, default=512, help="batch / adjoint workloads: number of graphs")
     ap.add_argument("--every", type=int, default=10, help="adjoint workload: checkpoint interval")
     ap.add_argument("--fd-params", type=int, default=1000, help="adjoint workload: parameters checked by differences")
@@ -378,6 +379,75 @@ def adjoint_checks(a, T, K, n_params):
                    "note": "relative error |fd - g| / max(|g|, 1e-3 max|g|), FP64 engine, graph 0"},
             "fp32_vs_fp64_rel_l2": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64)),
             "grad_max_abs": scale}
+
+
+def run_bingo(args, rank, world, local):
+    """The alarm-ranking loop: after each label (an alarm clamped to its
+    value) the graph is solved again (init + tolerance run, tol 1e-6, maxiter
+    500, FP32, beliefs to the host). Graph: 50 k tuples with config-0 laws,
+    its first 30 labelled alarms in turn. Three forms, each over the same
+    label sequence: FastLBP's (clamp the factor graph, rebuild it, build a new
+    engine: fl_wrapper.cu:29-45, bingo_wrapper.cu), incremental clamps on one
+    engine (flbp_clamp_vars, same results), and incremental clamps with a
+    warm start (no init: the previous solution is the starting point).
+    Reported: labels/s of each and the largest belief difference to the
+    first form."""
+    if rank != 0:
+        return None
+    from fastlbp_b200 import CausalFactorGraph, Engine, workloads
+
+    tol, maxiter, n_labels = 1e-6, 500, 30
+    fl, alarms, y = workloads.config4_graph(0)
+    labels = [(int(a), int(v)) for a, v in zip(alarms[:n_labels], y[:n_labels])]
+
+    def rebuild_form():
+        g = CausalFactorGraph.from_factors(fl)
+        out = []
+        t0 = time.perf_counter()
+        for lab, val in labels:
+            g.clamp(g.findVar(lab), val)
+            e = Engine(g.rebuild().graph_arrays(), precision=32)
+            e.init()
+            info = e.run_tol(tol, maxiter, 1e9)
+            out.append((info["sweeps"], e.beliefs()))
+            e.close()
+        return time.perf_counter() - t0, out
+
+    def incremental_form(warm):
+        g = CausalFactorGraph.from_factors(fl)
+        idx = [g.findVar(lab) for lab, _ in labels]
+        e = Engine(g.graph_arrays(), precision=32)
+        out = []
+        t0 = time.perf_counter()
+        if warm:
+            e.init()
+        for i, (lab, val) in zip(idx, labels):
+            e.clamp([i], [val])
+            if not warm:
+                e.init()
+            info = e.run_tol(tol, maxiter, 1e9)
+            out.append((info["sweeps"], e.beliefs()))
+        dt = time.perf_counter() - t0
+        e.close()
+        return dt, out
+
+    for _ in range(max(1, args.warmup)):
+        incremental_form(False)
+    t_r, ref = rebuild_form()
+    t_i, inc = incremental_form(False)
+    t_w, warm = incremental_form(True)
+    diff = lambda a: max(float(np.max(np.abs(x[1] - r[1]))) for x, r in zip(a, ref))  # noqa: E731
+    return {"metric": "labels/s (re-solve after each label)", "value": n_labels / t_i, "unit": "labels/s",
+            "n_gpus": 1, "steps": 1, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "dtype": "f32", "data": "synthetic (seeded Bingo-style generator)",
+            "config": {"workload": "50k-tuple Bingo-style graph (config-0 laws), %d labels in turn, tol 1e-6, "
+                                   "maxiter 500, FP32, init + tolerance run after each label" % n_labels},
+            "forms": {"rebuild": {"labels_per_s": n_labels / t_r, "sweeps": [s for s, _ in ref]},
+                      "incremental": {"labels_per_s": n_labels / t_i, "sweeps": [s for s, _ in inc],
+                                      "max_belief_diff_vs_rebuild": diff(inc)},
+                      "incremental_warm": {"labels_per_s": n_labels / t_w, "sweeps": [s for s, _ in warm],
+                                           "max_belief_diff_vs_rebuild": diff(warm)}},
+            "incremental_over_rebuild": t_r / t_i}
 
 
 def run_fl(args, rank, world, local):
@@ -702,6 +772,8 @@ def main():
         line = run_fl(args, rank, world, local)
     elif args.workload == "adjoint":
         line = run_adjoint(args, rank, world, local)
+    elif args.workload == "bingo":
+        line = run_bingo(args, rank, world, local)
     else:
         line = run_ours(args, rank, world, local)
     if rank == 0 and line is not None:

@@ -1763,6 +1763,11 @@ int flbp_clamp_vars(flbp_engine *e, int64_t n, const int64_t *vars, const int32_
     const uint32_t n_e = (uint32_t)(ents.size() / 2), n_p = (uint32_t)(pw.size() / 2), n_b = (uint32_t)(bw.size() / 2);
     const uint32_t m = std::max(n_e, std::max(n_p, n_b));
     if (m == 0) return FLBP_OK;
+    // the run state a new engine starts with: no sweeps since construction (the
+    // reference's maxiter counts them) and previous beliefs 0 (its tolerance rule)
+    e->iters = 0;
+    e->lowpass_valid = false;
+    FLBP_CUDA(cudaMemsetAsync(e->d_belief, 0, (size_t)std::max<int64_t>(1, L.V) * sizeof(double), e->stream));
     if (e->clamp_slots.size() > e->clamp_slots_cap) {  // the device copy of the clamped slots
         if (e->d_clamp_slots) cudaFree(e->d_clamp_slots);
         e->d_clamp_slots = nullptr;

@@ -322,7 +322,10 @@ int flbp_get_beliefs_device(flbp_engine *eng, double *out, int64_t n_vars);
  * more. An input at +-inf leaves a noisy-AND/OR product unchanged or zeroes
  * it, which is exactly the reference's removal of the variable from a body
  * or its "killed" factor (p := q, empty body). Takes effect from the next
- * init()/run. Clamping a variable again to the same value changes nothing;
+ * init()/run; like a new engine, the engine then counts its sweeps against
+ * maxiter from zero and its tolerance rule starts from beliefs 0 (the
+ * reference resets both only when an engine is constructed,
+ * csrc/ext/causal_bp.cu:371). Clamping a variable again to the same value changes nothing;
  * to the other value is rejected (FLBP_ERR_INVALID). Messages exported
  * afterwards (flbp_get_fv_messages) keep the unclamped graph's slots. */
 int flbp_clamp_vars(flbp_engine *eng, int64_t n, const int64_t *vars, const int32_t *values);

@@ -163,6 +163,23 @@ class CausalFactorGraph:
                 self.clamp(i, clamps[lab])
 
 
+def layout_digest(arrays: Dict[str, np.ndarray], threads: int = 0, graph_of=None) -> int:
+    """Digest of the device layout built for reference-order graph arrays
+    (flbp_layout_digest; host only). graph_of: optional (factor_graph,
+    var_graph, n_graphs) of a batch."""
+    keep = []
+    desc = _desc_from_arrays(arrays, keep)
+    out = C.c_uint64()
+    if graph_of is None:
+        check(lib().flbp_layout_digest(C.byref(desc), None, None, 0, int(threads), C.byref(out)))
+    else:
+        fg = np.ascontiguousarray(graph_of[0], np.uint32)
+        vg = np.ascontiguousarray(graph_of[1], np.uint32)
+        check(lib().flbp_layout_digest(C.byref(desc), fg.ctypes.data_as(C.c_void_p), vg.ctypes.data_as(C.c_void_p),
+                                       int(graph_of[2]), int(threads), C.byref(out)))
+    return int(out.value)
+
+
 def _check_device_tensor(t, n: int, name: str) -> None:
     import torch
 

@@ -699,3 +699,46 @@ void build_export_maps(HostLayout &L) {
 }
 
 }  // namespace flbp
+
+// Digest of the host layout of a graph (no GPU needed): an FNV-1a hash over
+// every layout array and count, built with `threads` host threads (0: all).
+extern "C" int flbp_layout_digest(const flbp_graph_desc *graph, const uint32_t *factor_graph,
+                                  const uint32_t *var_graph, uint32_t n_graphs, int32_t threads, uint64_t *digest) {
+    using namespace flbp;
+    if (!graph || !digest || (n_graphs && (!factor_graph || !var_graph))) {
+        set_error("null argument");
+        return FLBP_ERR_INVALID;
+    }
+    const int saved = omp_get_max_threads();
+    if (threads > 0) omp_set_num_threads(threads);
+    HostLayout L;
+    std::string err;
+    const GraphIds ids{n_graphs, factor_graph, var_graph};
+    const int rc = build_layout(*graph, L, err, n_graphs ? &ids : nullptr);
+    omp_set_num_threads(saved);
+    if (rc) {
+        set_error(err);
+        return rc;
+    }
+    uint64_t h = 1469598103934665603ull;
+    auto bytes = [&](const void *p, size_t n) {
+        const unsigned char *c = static_cast<const unsigned char *>(p);
+        for (size_t i = 0; i < n; i++) h = (h ^ c[i]) * 1099511628211ull;
+    };
+    auto arr = [&](const auto &v) {
+        const uint64_t n = v.size();
+        bytes(&n, sizeof n);
+        if (n) bytes(v.data(), n * sizeof(v[0]));
+    };
+    arr(L.fg_base), arr(L.fb_off), arr(L.fb_deg), arr(L.f_kind), arr(L.f_deg), arr(L.f_pq), arr(L.vg_base);
+    arr(L.vb_off), arr(L.vb_deg), arr(L.v_ent), arr(L.f_pos), arr(L.prior_fin), arr(L.prior_cnt);
+    arr(L.prior_factor), arr(L.prior_var), arr(L.prior_sign), arr(L.var_of_internal), arr(L.factor_of_internal);
+    arr(L.internal_of_var), arr(L.ref_off), arr(L.ref_slot_var), arr(L.ref_ent), arr(L.ref_fconst), arr(L.fhdr);
+    arr(L.vhdr), arr(L.fbt_deg), arr(L.fbt_kind), arr(L.fbt_pq), arr(L.vbt_deg);
+    const uint64_t sc[] = {L.nf_sell, L.nf_big, L.nf_huge, L.nv_sell, L.nv_big, L.nv_huge, L.n_slots,
+                           L.n_active_slots, L.n_ftiles, L.n_vtiles, L.n_fbtiles, L.n_vbtiles};
+    bytes(sc, sizeof sc);
+    *digest = h;
+    return FLBP_OK;
+}
+

@@ -311,6 +311,14 @@ int flbp_adjoint_backward_device(flbp_engine *eng, const double *grad_beliefs, d
 /* flbp_get_beliefs into a device buffer of the engine's device. */
 int flbp_get_beliefs_device(flbp_engine *eng, double *out, int64_t n_vars);
 
+/* A digest (64-bit FNV-1a) of the device layout the engine would build for
+ * `graph` (no counterpart in the reference; needs no GPU), built on the host
+ * with `threads` threads (0: all). For batches, factor_graph / var_graph give
+ * every factor's and variable's graph (n_graphs > 0), else NULL and 0. The
+ * layout does not depend on the thread count; tests use this to check it. */
+int flbp_layout_digest(const flbp_graph_desc *graph, const uint32_t *factor_graph, const uint32_t *var_graph,
+                       uint32_t n_graphs, int32_t threads, uint64_t *digest);
+
 /* ---- incremental evidence (the alarm-ranking loop) ----
  *
  * Clamps variables (graph variable order) to 0 or 1 on an existing engine,

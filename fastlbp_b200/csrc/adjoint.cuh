@@ -173,6 +173,77 @@ __global__ void var_adjoint_kernel(AdjArgs a, const uint32_t *__restrict__ group
 }
 static_assert(kSellVarDegree == 16, "var_adjoint_kernel instantiates widths 1..16");
 
+// Wide sliced-ELL groups (9-16 entries), two warps per group: warp h of the
+// pair takes entries h, h + 2, ... of the group's 32 variables (one per
+// lane), the pair combines its partial sums in shared memory, and each warp
+// writes the mu of its own entries. Blocks of 128 threads hold two groups.
+template <typename T>
+__global__ void __launch_bounds__(128) var_adjoint_wide_kernel(AdjArgs a, const uint32_t *__restrict__ groups,
+                                                                uint32_t n, const T *__restrict__ fv,
+                                                                const T *__restrict__ lam, const T *gS,
+                                                                T *__restrict__ mu, T *__restrict__ gprior) {
+    __shared__ int s_cnt[4][32][2];
+    __shared__ T s_sum[4][32][3];
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31, h = warp & 1;
+    const uint32_t gi = 2 * blockIdx.x + (warp >> 1);
+    const bool live_g = gi < n;
+    const uint32_t g = live_g ? groups[gi] : 0u, iv = 32u * g + lane;
+    const bool live = live_g && iv < a.nv_sell;
+    const uint32_t base = live ? a.vg_base[g] : 0u;
+    const uint32_t w = live ? (a.vg_base[g + 1] - base) >> 5 : 0u, bl = base + lane;
+    constexpr int R = (kSellVarDegree + 1) / 2;  // entries per warp at most
+    T x[R], l[R];
+    uint32_t sl[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        const uint32_t k = h + 2u * r;
+        sl[r] = kSentinel;
+        if (k < w) {
+            sl[r] = a.v_ent[bl + 32u * k];
+            x[r] = fv[bl + 32u * k];
+            l[r] = lam[bl + 32u * k];
+        }
+    }
+    int npos = 0, nneg = 0;
+    T Lf = T(0), Lp = T(0), Ln = T(0);
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        if (sl[r] == kSentinel) continue;
+        if (x[r] == Num<T>::inf()) {
+            npos++;
+            Lp += l[r];
+        } else if (x[r] == -Num<T>::inf()) {
+            nneg++;
+            Ln += l[r];
+        } else {
+            Lf += l[r];
+        }
+    }
+    s_cnt[warp][lane][0] = npos;
+    s_cnt[warp][lane][1] = nneg;
+    s_sum[warp][lane][0] = Lf;
+    s_sum[warp][lane][1] = Lp;
+    s_sum[warp][lane][2] = Ln;
+    __syncthreads();
+    const uint32_t o = warp ^ 1u;  // the pair's other warp; entries added in the order (even, odd)
+    const int np = h ? s_cnt[o][lane][0] + npos : npos + s_cnt[o][lane][0];
+    const int nn = h ? s_cnt[o][lane][1] + nneg : nneg + s_cnt[o][lane][1];
+    const T lf = h ? s_sum[o][lane][0] + Lf : Lf + s_sum[o][lane][0];
+    const T lp = h ? s_sum[o][lane][1] + Lp : Lp + s_sum[o][lane][1];
+    const T ln = h ? s_sum[o][lane][2] + Ln : Ln + s_sum[o][lane][2];
+    if (!live) return;
+    int p0, n0;
+    const bool folded = prior_info<T>(a.prior, iv, p0, n0);
+    const int tp = np + p0, tn = nn + n0;
+    const bool fin = tp == 0 && tn == 0;
+    const T Lam = lambda_of<T>(tp, tn, lf, lp, ln);
+    const T gs = (gS && fin) ? gS[iv] : T(0);
+#pragma unroll
+    for (int r = 0; r < R; r++)
+        if (sl[r] != kSentinel) mu[sl[r]] = isfinite(x[r]) ? Lam - (fin ? l[r] : T(0)) + gs : T(0);
+    if (h == 0 && folded) gprior[iv] += Lam + gs;
+}
+
 // Variables too large for a sliced-ELL group, kBigVarLanes lanes each: lane
 // j of a variable takes entries e0 + j, e0 + j + kBigVarLanes, ..., the first
 // kBigVarRegs of them held in registers between the two passes.

@@ -1266,7 +1266,7 @@ void launch_adjoint_step(flbp_engine *e, const void *vf, const void *fv, const v
         var_adjoint_kernel<T, false><<<blocks_for(32ull * c[0], 128), 128, 0, e->stream>>>(
             a, gl, c[0], (const T *)fv, (const T *)lam_next, (const T *)gs, mu, gprior);
     if (go(c[1]))
-        var_adjoint_kernel<T, true><<<blocks_for(32ull * c[1], 128), 128, 0, e->stream>>>(
+        var_adjoint_wide_kernel<T><<<(unsigned)((c[1] + 1) / 2), 128, 0, e->stream>>>(
             a, gl + o1, c[1], (const T *)fv, (const T *)lam_next, (const T *)gs, mu, gprior);
     if (go(a.nv_big))
         var_adjoint_big_kernel<T><<<blocks_for((uint64_t)kBigVarLanes * a.nv_big, 128), 128, 0, e->stream>>>(

@@ -1,6 +1,7 @@
 // Graph-model half of the C ABI (flbp_fg_*): the CausalFactorGraph of the
 // C++ API behind an opaque handle, for callers without C++.
 
+#include <cstring>
 #include <fstream>
 #include <sstream>
 #include <stdexcept>
@@ -51,7 +52,7 @@ int flbp_fg_read_file(const char *path, flbp_fg **out) {
             flbp::set_error(std::string("Cannot read from file ") + path + ".");
             return FLBP_ERR_INVALID;
         }
-        auto *h = new flbp_fg{lbp::detail::parse_causal_fg(in)};
+        auto *h = new flbp_fg{lbp::detail::read_causal_fg_file(in)};
         *out = h;
         return FLBP_OK;
     });
@@ -64,8 +65,7 @@ int flbp_fg_read_string(const char *text, flbp_fg **out) {
     }
     *out = nullptr;
     return guarded([&] {
-        std::istringstream in(text);
-        *out = new flbp_fg{lbp::detail::parse_causal_fg(in)};
+        *out = new flbp_fg{lbp::detail::parse_causal_fg_text(text, std::strlen(text))};
         return FLBP_OK;
     });
 }

@@ -4,6 +4,12 @@
 // conversion of a CausalFactorGraph into the engine's reference-order arrays.
 
 #include <algorithm>
+#include <cctype>
+#include <cerrno>
+#include <climits>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
 #include <fstream>
 #include <iomanip>
 #include <map>
@@ -11,6 +17,7 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <string_view>
 #include <unordered_map>
 #include <vector>
 
@@ -260,26 +267,55 @@ std::ostream &operator<<(std::ostream &os, const CausalFactor &f) {
 // ---------------------------------------------------------- CausalFactorGraph
 
 void CausalFactorGraph::constructGraph(size_t nrEdges) {
+    // label -> variable index: a direct table when the labels are dense
+    // (the usual 0..V-1), else a hash map
+    const size_t V = _vars.size();
+    const size_t max_label = V ? _vars.back().label() : 0;  // _vars is sorted by label
+    std::vector<uint32_t> dense;
     std::unordered_map<size_t, size_t> idx;
-    idx.reserve(_vars.size() * 2 + 1);
-    for (size_t i = 0; i < _vars.size(); i++) idx[_vars[i].label()] = i;
+    const bool use_dense = V && V < UINT32_MAX && max_label < 4 * V + 1024;
+    if (use_dense) {
+        dense.assign(max_label + 1, UINT32_MAX);
+        for (size_t i = 0; i < V; i++) dense[_vars[i].label()] = (uint32_t)i;
+    } else {
+        idx.reserve(V * 2 + 1);
+        for (size_t i = 0; i < V; i++) idx[_vars[i].label()] = i;
+    }
     std::vector<Edge> edges;
     edges.reserve(nrEdges);
     for (size_t I = 0; I < _factors.size(); I++)
-        for (const auto &v : _factors[I].vars()) edges.push_back(Edge(idx[v.label()], I));
-    _G.construct(_vars.size(), _factors.size(), edges.begin(), edges.end(), false);
+        for (const auto &v : _factors[I].vars())
+            edges.push_back(Edge(use_dense ? (size_t)dense[v.label()] : idx[v.label()], I));
+    _G.construct(V, _factors.size(), edges.begin(), edges.end(), false);
 }
 
-CausalFactorGraph::CausalFactorGraph(const std::vector<CausalFactor> &P) {
-    std::set<Var> vs;
-    size_t nrEdges = 0;
-    _factors.reserve(P.size());
-    for (const auto &f : P) {
-        _factors.push_back(f);
-        vs.insert(f.vars().begin(), f.vars().end());
+CausalFactorGraph::CausalFactorGraph(const std::vector<CausalFactor> &P) : CausalFactorGraph(std::vector<CausalFactor>(P)) {}
+
+CausalFactorGraph::CausalFactorGraph(std::vector<CausalFactor> &&P) {
+    _factors = std::move(P);
+    size_t nrEdges = 0, max_label = 0;
+    for (const auto &f : _factors) {
         nrEdges += f.vars().size();
+        for (const auto &v : f.vars()) max_label = std::max(max_label, v.label());
     }
-    _vars.assign(vs.begin(), vs.end());
+    // the variables in ascending label order without repeats, each as first met
+    // (what inserting them all into a std::set<Var> keeps)
+    std::vector<Var> vs;
+    if (nrEdges && max_label < 4 * nrEdges + 1024) {  // dense labels: a table of first occurrences
+        std::vector<const Var *> first(max_label + 1, nullptr);
+        for (const auto &f : _factors)
+            for (const auto &v : f.vars())
+                if (!first[v.label()]) first[v.label()] = &v;
+        for (const Var *v : first)
+            if (v) vs.push_back(*v);
+    } else {
+        vs.reserve(nrEdges);
+        for (const auto &f : _factors) vs.insert(vs.end(), f.vars().begin(), f.vars().end());
+        std::stable_sort(vs.begin(), vs.end());
+        vs.erase(std::unique(vs.begin(), vs.end(), [](const Var &a, const Var &b) { return !(a < b) && !(b < a); }),
+                 vs.end());
+    }
+    _vars = std::move(vs);
     constructGraph(nrEdges);
 }
 
@@ -301,7 +337,7 @@ void CausalFactorGraph::ReadFromFile(const char *filename) {
     std::ifstream in(filename);
     if (!in.is_open()) LOG_FATAL("Cannot read from file %s.", filename);
     try {
-        *this = detail::parse_causal_fg(in);
+        *this = detail::read_causal_fg_file(in);
     } catch (const detail::BadFactorType &) {
         LOG_FATAL("Unreachable");
     }
@@ -318,67 +354,191 @@ std::istream &operator>>(std::istream &is, CausalFactorGraph &fg) {
 
 namespace detail {
 
+// Line sources of the reader, with the semantics of std::getline (false
+// when nothing could be read: the stream's failbit) and of peeking at the
+// next character.
+struct StreamLines {
+    std::istream &is;
+    std::string buf;
+    bool next(std::string_view &line) {
+        std::getline(is, buf);
+        line = buf;
+        return !is.fail();
+    }
+    bool peek_hash() { return is.peek() == '#'; }
+};
+
+struct BufferLines {
+    const char *p, *end;
+    bool next(std::string_view &line) {
+        if (p >= end) {
+            line = std::string_view();
+            return false;
+        }
+        const char *nl = static_cast<const char *>(std::memchr(p, '\n', (size_t)(end - p)));
+        const char *e = nl ? nl : end;
+        line = std::string_view(p, (size_t)(e - p));
+        p = nl ? nl + 1 : end;
+        return true;
+    }
+    bool peek_hash() { return p < end && *p == '#'; }
+};
+
+// std::stoi / std::stold on a line: the same conversion (strtol / strtold on
+// the line alone) and the same exceptions.
+int line_stoi(std::string_view s) {
+    char buf[64];
+    if (s.size() >= sizeof buf) return std::stoi(std::string(s));
+    std::memcpy(buf, s.data(), s.size());
+    buf[s.size()] = 0;
+    char *e = nullptr;
+    errno = 0;
+    const long v = std::strtol(buf, &e, 10);
+    if (e == buf) throw std::invalid_argument("stoi");
+    if (errno == ERANGE || v < INT_MIN || v > INT_MAX) throw std::out_of_range("stoi");
+    return (int)v;
+}
+
+long double line_stold(std::string_view s) {
+    char buf[128];
+    if (s.size() >= sizeof buf) return std::stold(std::string(s));
+    std::memcpy(buf, s.data(), s.size());
+    buf[s.size()] = 0;
+    char *e = nullptr;
+    errno = 0;
+    const long double v = std::strtold(buf, &e);
+    if (e == buf) throw std::invalid_argument("stold");
+    if (errno == ERANGE) throw std::out_of_range("stold");
+    return v;
+}
+
+// Successive `long` extractions from a line as an istringstream performs
+// them: leading white space skipped; after a failed extraction (no number,
+// or out of range: LONG_MAX / LONG_MIN) every later one yields 0.
+struct LongReader {
+    const char *p, *end;
+    bool ok = true;
+    long next() {
+        if (!ok) return 0;
+        while (p < end && std::isspace((unsigned char)*p)) p++;
+        const char *q = p;
+        bool neg = false;
+        if (q < end && (*q == '+' || *q == '-')) neg = *q++ == '-';
+        if (q >= end || !std::isdigit((unsigned char)*q)) {
+            ok = false;
+            return 0;
+        }
+        unsigned long long mag = 0;
+        bool over = false;
+        for (; q < end && std::isdigit((unsigned char)*q); q++) {
+            const unsigned d = (unsigned)(*q - '0');
+            if (mag > (ULLONG_MAX - d) / 10) over = true;
+            else mag = mag * 10 + d;
+        }
+        p = q;
+        const unsigned long long lim = neg ? (unsigned long long)LONG_MAX + 1ull : (unsigned long long)LONG_MAX;
+        if (over || mag > lim) {
+            ok = false;
+            return neg ? LONG_MIN : LONG_MAX;
+        }
+        return neg ? (long)(0ull - mag) : (long)mag;
+    }
+};
+
 // The .causal_fg grammar of csrc/ext/causal_fg.cpp:129-279: a factor count;
 // per factor a separating blank line, the head id, a type line ("I", or "*" /
 // "+" optionally followed by "p;q", defaults p=1, q=0), then for "I" the
 // probability, else the body length and the body ids on one line. Lines
 // starting with '#' directly after a consumed line are skipped. Variables
 // never used as a head get Singleton(0.5), appended in ascending label order.
-CausalFactorGraph parse_causal_fg(std::istream &is) {
+template <typename Lines>
+CausalFactorGraph parse_lines(Lines &in) {
     std::vector<CausalFactor> facs;
-    std::string line;
-    std::getline(is, line);
-    read_annotation(is, line);
-    const size_t nr = (size_t)std::stoi(line);
-    std::set<size_t> heads, all_vars;
+    std::string_view line;
+    auto skip_annotation = [&] {
+        std::string_view c;
+        while (in.peek_hash()) in.next(c);
+    };
+    in.next(line);
+    skip_annotation();
+    const size_t nr = (size_t)line_stoi(line);
+    std::vector<size_t> heads, all_vars;  // sorted and de-duplicated at the end
+    facs.reserve(nr);
+    heads.reserve(nr);
+    std::vector<Var> body_vars;
     for (size_t I = 0; I < nr; I++) {
-        std::getline(is, line);
-        if (is.fail() || line.size() > 0) LOG_ERROR("Expecting empty line");
-        std::getline(is, line);
-        read_annotation(is, line);
-        const size_t head_id = (size_t)std::stoi(line);
+        if (!in.next(line) || line.size() > 0) LOG_ERROR("Expecting empty line");
+        in.next(line);
+        skip_annotation();
+        const size_t head_id = (size_t)line_stoi(line);
         const Var head(head_id, 2);
-        heads.insert(head_id);
-        all_vars.insert(head_id);
-        std::getline(is, line);
-        read_annotation(is, line);
+        heads.push_back(head_id);
+        all_vars.push_back(head_id);
+        in.next(line);
+        skip_annotation();
         const char ch = line.empty() ? '\0' : line.front();
         if (ch != CausalFactor::Singleton && ch != CausalFactor::DefiniteAnd && ch != CausalFactor::DefiniteOr)
             throw BadFactorType();
         if (ch == CausalFactor::Singleton) {
-            std::getline(is, line);
-            read_annotation(is, line);
-            const Real prob = static_cast<Real>(std::stold(line));
+            in.next(line);
+            skip_annotation();
+            const Real prob = static_cast<Real>(line_stold(line));
             facs.emplace_back(head, prob);
             continue;
         }
         Real prob = 1, prob_default = 0;
         if (line.length() > 1) {
             const size_t sp = line.find(';');
-            if (sp > 1) prob = static_cast<Real>(std::stold(line.substr(1, sp - 1)));
-            if (sp != std::string::npos && sp + 1 != line.length())
-                prob_default = static_cast<Real>(std::stold(line.substr(sp + 1)));
+            if (sp > 1) prob = static_cast<Real>(line_stold(line.substr(1, sp - 1)));
+            if (sp != std::string_view::npos && sp + 1 != line.length())
+                prob_default = static_cast<Real>(line_stold(line.substr(sp + 1)));
         }
-        std::getline(is, line);
-        read_annotation(is, line);
-        const size_t blen = (size_t)std::stoi(line);
-        std::getline(is, line);
-        read_annotation(is, line);
-        std::istringstream ss(line);
-        std::vector<Var> body_vars;
+        in.next(line);
+        skip_annotation();
+        const size_t blen = (size_t)line_stoi(line);
+        in.next(line);
+        skip_annotation();
+        LongReader ids{line.data(), line.data() + line.size()};
+        body_vars.clear();
         body_vars.reserve(blen);
         for (size_t b = 0; b < blen; b++) {
-            long id = 0;
-            ss >> id;
+            const long id = ids.next();
             body_vars.emplace_back((size_t)id, 2);
-            all_vars.insert((size_t)id);
+            all_vars.push_back((size_t)id);
         }
         VarSet body(body_vars.begin(), body_vars.end(), body_vars.size());
         facs.emplace_back(head, body, ch == CausalFactor::DefiniteAnd, prob, prob_default);
     }
+    std::sort(heads.begin(), heads.end());
+    heads.erase(std::unique(heads.begin(), heads.end()), heads.end());
+    std::sort(all_vars.begin(), all_vars.end());
+    all_vars.erase(std::unique(all_vars.begin(), all_vars.end()), all_vars.end());
     for (size_t v : all_vars)
-        if (heads.find(v) == heads.end()) facs.emplace_back(Var(v, 2), 0.5);
-    return CausalFactorGraph(facs);
+        if (!std::binary_search(heads.begin(), heads.end(), v)) facs.emplace_back(Var(v, 2), 0.5);
+    return CausalFactorGraph(std::move(facs));
+}
+
+CausalFactorGraph parse_causal_fg(std::istream &is) {
+    StreamLines in{is, {}};
+    return parse_lines(in);
+}
+
+CausalFactorGraph parse_causal_fg_text(const char *text, size_t n) {
+    BufferLines in{text, text + n};
+    return parse_lines(in);
+}
+
+CausalFactorGraph read_causal_fg_file(std::ifstream &f) {
+    std::string buf;
+    f.seekg(0, std::ios::end);
+    const std::streamoff sz = f.tellg();
+    f.seekg(0, std::ios::beg);
+    if (sz > 0) {
+        buf.resize((size_t)sz);
+        f.read(&buf[0], sz);
+        buf.resize((size_t)f.gcount());
+    }
+    return parse_causal_fg_text(buf.data(), buf.size());
 }
 
 int build_arrays(const CausalFactorGraph &fg, GraphArrays &a, std::string &err) {

@@ -1,6 +1,7 @@
 // Internal helpers shared by the C++ API implementation and the graph-model C ABI.
 #pragma once
 
+#include <fstream>
 #include <istream>
 #include <string>
 #include <vector>
@@ -17,6 +18,9 @@ struct BadFactorType {};
 
 /// .causal_fg reader; throws BadFactorType or the std:: conversion errors.
 CausalFactorGraph parse_causal_fg(std::istream &is);
+/// The same reader on text in memory, and on a whole open file (read at once).
+CausalFactorGraph parse_causal_fg_text(const char *text, size_t n);
+CausalFactorGraph read_causal_fg_file(std::ifstream &f);
 
 /// A CausalFactorGraph as the engine's reference-order arrays.
 struct GraphArrays {

@@ -28,6 +28,7 @@ class CausalFactorGraph {
 public:
     CausalFactorGraph() = default;
     CausalFactorGraph(const std::vector<CausalFactor> &P);
+    CausalFactorGraph(std::vector<CausalFactor> &&P);
     ~CausalFactorGraph() = default;
 
     const Var &var(size_t i) const { return _vars[i]; }

@@ -24,6 +24,15 @@ public:
                    bool check = true) {
         _nb1.assign(nrNodes1, Neighbors());
         _nb2.assign(nrNodes2, Neighbors());
+        {  // room for every node's neighbours first (the edge order decides iter / dual as before)
+            std::vector<size_t> d1(nrNodes1, 0), d2(nrNodes2, 0);
+            for (EdgeInputIterator e = begin; e != end; ++e) {
+                if (e->first < nrNodes1) d1[e->first]++;
+                if (e->second < nrNodes2) d2[e->second]++;
+            }
+            for (size_t i = 0; i < nrNodes1; i++) _nb1[i].reserve(d1[i]);
+            for (size_t i = 0; i < nrNodes2; i++) _nb2[i].reserve(d2[i]);
+        }
         for (EdgeInputIterator e = begin; e != end; ++e) addEdge(e->first, e->second, check);
     }
 

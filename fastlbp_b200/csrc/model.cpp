@@ -543,9 +543,30 @@ CausalFactorGraph read_causal_fg_file(std::ifstream &f) {
 
 int build_arrays(const CausalFactorGraph &fg, GraphArrays &a, std::string &err) {
     const size_t V = fg.nrVars(), F = fg.nrFactors();
+    // label -> variable index: a direct table when the labels are dense, else a hash map
+    size_t max_label = 0;
+    for (size_t i = 0; i < V; i++) max_label = std::max(max_label, fg.var(i).label());
+    const bool use_dense = V && V < UINT32_MAX && max_label < 4 * V + 1024;
+    std::vector<uint32_t> dense;
     std::unordered_map<size_t, size_t> idx;
-    idx.reserve(V * 2 + 1);
-    for (size_t i = 0; i < V; i++) idx[fg.var(i).label()] = i;
+    if (use_dense) {
+        dense.assign(max_label + 1, UINT32_MAX);
+        for (size_t i = 0; i < V; i++) dense[fg.var(i).label()] = (uint32_t)i;
+    } else {
+        idx.reserve(V * 2 + 1);
+        for (size_t i = 0; i < V; i++) idx[fg.var(i).label()] = i;
+    }
+    auto index_of = [&](size_t label, size_t &out) {
+        if (use_dense) {
+            if (label > max_label || dense[label] == UINT32_MAX) return false;
+            out = dense[label];
+            return true;
+        }
+        auto it = idx.find(label);
+        if (it == idx.end()) return false;
+        out = it->second;
+        return true;
+    };
     a = GraphArrays();
     a.offsets.assign(F + 1, 0);
     a.head.assign(F, 0);
@@ -563,8 +584,8 @@ int build_arrays(const CausalFactorGraph &fg, GraphArrays &a, std::string &err) 
         const size_t hl = f.head().label();
         bool found = false;
         for (const auto &v : f.vars()) {
-            auto it = idx.find(v.label());
-            if (it == idx.end()) {
+            size_t vi = 0;
+            if (!index_of(v.label(), vi)) {
                 err = "factor " + std::to_string(I) + " uses variable x" + std::to_string(v.label()) +
                       " that is not in the graph";
                 return 1;
@@ -573,7 +594,7 @@ int build_arrays(const CausalFactorGraph &fg, GraphArrays &a, std::string &err) 
                 a.head[I] = (int64_t)a.slot_var.size();
                 found = true;
             }
-            a.slot_var.push_back((int64_t)it->second);
+            a.slot_var.push_back((int64_t)vi);
         }
         if (!found) {
             err = "factor " + std::to_string(I) + " does not contain its head";

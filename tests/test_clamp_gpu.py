@@ -129,3 +129,12 @@ def test_clamp_rejects_conflicts():
         eng.clamp([eng.n_vars], [0])
     with pytest.raises(FlbpError):
         eng.clamp([4], [2])
+
+
+def test_adjoint_refuses_clamped_engine():
+    """Gradients are taken on engines built from the clamped graph; an engine
+    with incremental clamps refuses the adjoint instead of giving them."""
+    fl = _bingo()
+    eng = _incremental(fl, _clamps(fl, 5, seed=12), precision=64)
+    with pytest.raises(FlbpError):
+        eng.adjoint_forward(10, 5)

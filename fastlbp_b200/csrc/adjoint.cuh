@@ -332,7 +332,8 @@ __device__ __forceinline__ void factor_adjoint_reg(const AdjArgs &a, uint32_t ba
     }
     const T gp0 = *gp, gq0 = gq ? *gq : T(0);
     const T sgn = (kind & KIND_OR) ? T(-1) : T(1);
-    const T lh = hs == HEAD_FREE ? sgn * y[0] : (hs == HEAD_ONE ? Num<T>::inf() : -Num<T>::inf());
+    // the head's log-odds in the factor's orientation, as the forward pass takes it
+    const T lh = sgn * (hs == HEAD_FREE ? y[0] : (hs == HEAD_ONE ? Num<T>::inf() : -Num<T>::inf()));
     T sh, th;
     sig_pair<T>(lh, sh, th);
     auto mu_of = [&](int k) { return sgn * m[k]; };
@@ -439,7 +440,7 @@ __global__ void factor_adjoint_big_kernel(AdjArgs a, const T *__restrict__ vf, c
     const T *pqa = reinterpret_cast<const T *>(a.f_pq);
     const T p = pqa[2 * f], q = pqa[2 * f + 1];
     const T sgn = (kind & KIND_OR) ? T(-1) : T(1);
-    const T lh = hs == HEAD_FREE ? sgn * vf[s0] : (hs == HEAD_ONE ? Num<T>::inf() : -Num<T>::inf());
+    const T lh = sgn * (hs == HEAD_FREE ? vf[s0] : (hs == HEAD_ONE ? Num<T>::inf() : -Num<T>::inf()));
     T sh, th;
     sig_pair<T>(lh, sh, th);
     auto mu_of = [&](uint32_t s) { return sgn * mu[s]; };

@@ -1478,10 +1478,6 @@ int flbp_adjoint_forward(flbp_engine *e, int64_t sweeps, int64_t every, double *
         set_error("the adjoint needs an engine without damping");
         return FLBP_ERR_INVALID;
     }
-    if (!e->clamp_slots.empty()) {
-        set_error("the adjoint needs an engine without incremental clamps (build one from the clamped graph)");
-        return FLBP_ERR_INVALID;
-    }
     if (sweeps < 1 || every < 1) {
         set_error("sweeps and checkpoint interval must be positive");
         return FLBP_ERR_INVALID;

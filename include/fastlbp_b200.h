@@ -290,9 +290,7 @@ int flbp_batch_run_tol(flbp_engine *eng, double tol, int64_t maxiter, double max
 /* ---- gradients through unrolled sweeps (no counterpart in the reference) ----
  *
  * flbp_adjoint_forward: init() and `sweeps` synchronous sweeps (engines
- * without damping and without flbp_clamp_vars clamps: differentiate an
- * engine built from the clamped graph), keeping the v->f messages every
- * `every` sweeps; writes
+ * without damping), keeping the v->f messages every `every` sweeps; writes
  * the beliefs after the last sweep (n = number of variables; may be NULL).
  * flbp_adjoint_backward: given dL/dbelief for every variable, the gradient
  * of L with respect to every factor's p and q (reference factor order; NULL
@@ -337,8 +335,7 @@ int flbp_layout_digest(const flbp_graph_desc *graph, const uint32_t *factor_grap
  * reference resets both only when an engine is constructed,
  * csrc/ext/causal_bp.cu:371). Clamping a variable again to the same value changes nothing;
  * to the other value is rejected (FLBP_ERR_INVALID). Messages exported
- * afterwards (flbp_get_fv_messages) keep the unclamped graph's slots, and
- * the engine refuses flbp_adjoint_forward. */
+ * afterwards (flbp_get_fv_messages) keep the unclamped graph's slots. */
 int flbp_clamp_vars(flbp_engine *eng, int64_t n, const int64_t *vars, const int32_t *values);
 
 /* New p and q for every factor (reference order) of an existing engine, e.g.

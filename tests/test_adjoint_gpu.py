@@ -6,7 +6,8 @@ Loss: binary cross-entropy of the beliefs of labelled variables after T
 sweeps; gradient with respect to every factor's p (rule firing
 probabilities, input priors). Tolerances: FP64 adjoint against the torch
 reference 1e-7 relative (both exact up to rounding), against central
-differences (eps 1e-6) 1e-4 relative; the FP32 engine's adjoint (FP32
+differences (eps 1e-6) 1e-4 relative, also on a graph with clamped AND and
+OR heads; the FP32 engine's adjoint (FP32
 states and derivative arithmetic) against the FP64 one 2e-3 relative (L2).
 The device-buffer entry points give the host-buffer results bit for bit,
 and a batch engine's gradient is its graphs' gradients side by side.
@@ -186,3 +187,41 @@ def test_checkpointed_forward_is_the_plain_run(prec):
     g1 = eng.adjoint_backward(g)
     g2 = eng.adjoint_backward(g)
     assert np.array_equal(g1[0], g2[0]) and np.array_equal(g1[1], g2[1])
+
+
+def test_adjoint_on_clamped_graph_matches_central_differences():
+    """Head-clamped AND and OR factors (a clamped graph, rebuilt): the
+    adjoint against central differences (eps 1e-6) of the FP64 engine."""
+    fl = workloads.bingo_graph(300, 450, 20, workloads.uniform_int(2, 4), workloads.uniform_int(1, 6), 9,
+                               n_layers=6, back_frac=0.10, p_lo=0.6, p_hi=0.95, input_prior=0.8, n_alarms=30)
+    g = CausalFactorGraph.from_factors(fl)
+    labels = g.var_labels()
+    rng = np.random.default_rng(21)
+    g.clamp_labels({int(l): int(rng.integers(0, 2)) for l in rng.choice(labels, 25, replace=False)})
+    a = g.rebuild().graph_arrays()
+    assert np.asarray(a["factor_head_clamped"]).any()
+    T, K, eps = 12, 4, 1e-6
+    eng = Engine(a, precision=64)
+    p0, q0 = np.asarray(a["factor_p"], np.float64).copy(), np.asarray(a["factor_q"], np.float64)
+    b0 = eng.adjoint_forward(T, K)
+    idx = np.array([i for i in rng.choice(eng.n_vars, 50, replace=False) if 0 < b0[i] < 1])
+    y = (rng.random(idx.size) < 0.3).astype(np.float64)
+
+    def loss(p):
+        eng.set_factor_probs(p, q0)
+        return float(_bce(torch.as_tensor(eng.adjoint_forward(T, K)), idx, torch.as_tensor(y)))
+
+    eng.set_factor_probs(p0, q0)
+    b = torch.as_tensor(eng.adjoint_forward(T, K), dtype=torch.float64).requires_grad_(True)
+    _bce(b, idx, torch.as_tensor(y)).backward()
+    gp, _ = eng.adjoint_backward(b.grad.numpy())
+    cand = np.nonzero((p0 > 1e-3) & (p0 < 1 - 1e-3))[0]
+    sample = rng.choice(cand, size=min(60, cand.size), replace=False)
+    scale = np.max(np.abs(gp))
+    assert scale > 0
+    for I in sample:
+        pp, pm = p0.copy(), p0.copy()
+        pp[I] += eps
+        pm[I] -= eps
+        fd = (loss(pp) - loss(pm)) / (2 * eps)
+        assert abs(fd - gp[I]) <= 1e-4 * max(abs(gp[I]), 1e-3 * scale), (I, fd, gp[I])

@@ -12,6 +12,8 @@
 #include <map>
 #include <new>
 #include <string>
+#include <unordered_set>
+#include <utility>
 #include <vector>
 
 #include "engine_internal.h"
@@ -727,8 +729,7 @@ __global__ void clamp_slots_kernel(const uint32_t *__restrict__ pairs, uint32_t 
     if (i < n) vf[pairs[2 * i]] = pairs[2 * i + 1] ? Num<T>::inf() : -Num<T>::inf();
 }
 
-int apply_clamp_slots(flbp_engine *e) {
-    const uint32_t n = (uint32_t)(e->clamp_slots.size() / 2);
+int launch_clamp_slots(flbp_engine *e, uint32_t n) {
     if (!n) return FLBP_OK;
     if (e->prec == 64)
         clamp_slots_kernel<double><<<(n + 255) / 256, 256, 0, e->stream>>>(e->d_clamp_slots, n, (double *)e->d_vf);
@@ -738,6 +739,8 @@ int apply_clamp_slots(flbp_engine *e) {
     FLBP_CUDA(cudaGetLastError());
     return FLBP_OK;
 }
+
+int apply_clamp_slots(flbp_engine *e) { return launch_clamp_slots(e, (uint32_t)(e->clamp_slots.size() / 2)); }
 
 }  // namespace
 
@@ -1688,18 +1691,27 @@ int flbp_clamp_vars(flbp_engine *e, int64_t n, const int64_t *vars, const int32_
     std::vector<uint8_t> folded((size_t)L.V, 0);
     for (uint32_t v : L.prior_var) folded[v] = 1;
     const size_t pwords = e->prec == 64 ? 4 : 2, cword = e->prec == 64 ? 2 : 1;
+    // Every change is staged and the engine's host state is updated only once
+    // the device has taken them.
     std::vector<uint32_t> ents, pw, bw;  // (entry, slot), (word, value), (word, value)
+    std::vector<std::pair<int64_t, int8_t>> new_state;
+    std::vector<std::pair<uint32_t, uint32_t>> new_cnt;  // (internal variable, count word)
+    std::vector<uint32_t> cut_slots, slots = e->clamp_slots;
+    std::unordered_set<int64_t> in_call;
+    std::unordered_set<uint32_t> cut_now;
     for (int64_t k = 0; k < n; k++) {
-        if (e->clamp_state[vars[k]] >= 0) continue;  // clamping again to the same value changes nothing
-        e->clamp_state[vars[k]] = (int8_t)values[k];
+        // clamping again to the same value changes nothing
+        if (e->clamp_state[vars[k]] >= 0 || !in_call.insert(vars[k]).second) continue;
+        new_state.push_back({vars[k], (int8_t)values[k]});
         const uint32_t iv = L.internal_of_var[vars[k]];
         // the clamp: one exact-zero count in the variable's prior
-        uint32_t &cnt = L.prior_cnt[iv];
+        uint32_t cnt = L.prior_cnt[iv];
         if (values[k]) {
             if ((cnt & 0xffffu) != 0xffffu) cnt += 1u;
         } else if (((cnt >> 16) & 0x7fffu) != 0x7fffu) {
             cnt += 1u << 16;
         }
+        new_cnt.push_back({iv, cnt});
         const uint32_t word = cnt | (folded[iv] ? 0x80000000u : 0u);
         pw.push_back((uint32_t)(pwords * iv + cword));
         pw.push_back(word);
@@ -1709,17 +1721,17 @@ int flbp_clamp_vars(flbp_engine *e, int64_t n, const int64_t *vars, const int32_
         // other body variables too
         auto cut = [&](uint32_t sl) {  // no message from slot sl any more
             const uint32_t en = L.f_pos[sl];
-            if (en == kSentinel) return;
+            if (en == kSentinel || !cut_now.insert(sl).second) return;
             ents.push_back(en);
             ents.push_back(sl);
-            L.f_pos[sl] = kSentinel;
+            cut_slots.push_back(sl);
         };
         auto entry = [&](uint32_t en) {
             const uint32_t sl = L.v_ent[en];
             if (sl == kSentinel) return;
             cut(sl);
-            e->clamp_slots.push_back(sl);
-            e->clamp_slots.push_back((uint32_t)values[k]);
+            slots.push_back(sl);
+            slots.push_back((uint32_t)values[k]);
             // the factor of slot sl, and sl's position in it (0 = head)
             uint32_t f, pos, base, stride, deg;
             if (sl < L.fg_base.back()) {
@@ -1763,19 +1775,18 @@ int flbp_clamp_vars(flbp_engine *e, int64_t n, const int64_t *vars, const int32_
     const uint32_t n_e = (uint32_t)(ents.size() / 2), n_p = (uint32_t)(pw.size() / 2), n_b = (uint32_t)(bw.size() / 2);
     const uint32_t m = std::max(n_e, std::max(n_p, n_b));
     if (m == 0) return FLBP_OK;
-    // the run state a new engine starts with: no sweeps since construction (the
-    // reference's maxiter counts them) and previous beliefs 0 (its tolerance rule)
-    e->iters = 0;
-    e->lowpass_valid = false;
-    FLBP_CUDA(cudaMemsetAsync(e->d_belief, 0, (size_t)std::max<int64_t>(1, L.V) * sizeof(double), e->stream));
-    if (e->clamp_slots.size() > e->clamp_slots_cap) {  // the device copy of the clamped slots
+    // the device side: the clamped slots' list, the run state a new engine
+    // starts with (previous beliefs 0, for the tolerance rule), the updates
+    if (slots.size() > e->clamp_slots_cap) {
         if (e->d_clamp_slots) cudaFree(e->d_clamp_slots);
         e->d_clamp_slots = nullptr;
         e->clamp_slots_cap = 0;
-        if ((rc = dalloc(e, &e->d_clamp_slots, 2 * e->clamp_slots.size()))) return rc;
-        e->clamp_slots_cap = 2 * e->clamp_slots.size();
+        if ((rc = dalloc(e, &e->d_clamp_slots, 2 * slots.size()))) return rc;
+        e->clamp_slots_cap = 2 * slots.size();
     }
-    if ((rc = upload(e, e->d_clamp_slots, e->clamp_slots)) || (rc = apply_clamp_slots(e))) return rc;
+    if ((rc = upload(e, e->d_clamp_slots, slots)) || (rc = launch_clamp_slots(e, (uint32_t)(slots.size() / 2))))
+        return rc;
+    FLBP_CUDA(cudaMemsetAsync(e->d_belief, 0, (size_t)std::max<int64_t>(1, L.V) * sizeof(double), e->stream));
     uint32_t *d = nullptr;
     FLBP_CUDA(cudaMalloc((void **)&d, (ents.size() + pw.size() + bw.size()) * sizeof(uint32_t)));
     cudaError_t ce = cudaSuccess;
@@ -1806,6 +1817,14 @@ int flbp_clamp_vars(flbp_engine *e, int64_t n, const int64_t *vars, const int32_
         set_error(std::string("clamp update failed: ") + cudaGetErrorString(ce));
         return FLBP_ERR_CUDA;
     }
+    // the host side, now that the device holds the update; like a new engine,
+    // no sweeps since construction (the reference's maxiter counts them)
+    for (const auto &st : new_state) e->clamp_state[st.first] = st.second;
+    for (const auto &c : new_cnt) L.prior_cnt[c.first] = c.second;
+    for (uint32_t sl : cut_slots) L.f_pos[sl] = kSentinel;
+    e->clamp_slots.swap(slots);
+    e->iters = 0;
+    e->lowpass_valid = false;
     return FLBP_OK;
 }
 

@@ -122,6 +122,11 @@ def lib():
         "flbp_clamp_vars": [_vp, C.c_int64, _i64p, _i32p],
         "flbp_layout_digest": [P(GraphDesc), _vp, _vp, C.c_uint32, C.c_int32, P(C.c_uint64)],
         "flbp_set_factor_probs": [_vp, _f64p, _f64p],
+        "flbp_update_seq": [P(GraphDesc), C.c_int32, _vp, _i64p],
+        "flbp_shuffled_factors": [C.c_int64, C.c_uint32, _i32p],
+        "flbp_seq_batches": [P(GraphDesc), _i64p, C.c_int64, _vp, P(C.c_int64)],
+        "flbp_set_update_seq": [_vp, _vp, C.c_int64],
+        "flbp_update_info": [_vp, P(C.c_int32), P(C.c_int64)],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -148,4 +153,5 @@ EXPORTED = ["flbp_last_error", "flbp_version", "flbp_engine_create", "flbp_engin
             "flbp_fg_var_labels", "flbp_fg_factors", "flbp_fg_neighbors", "flbp_fg_construct",
             "flbp_engine_create_from_fg", "flbp_run_fixed_device_noalloc", "flbp_batch_create", "flbp_batch_info",
             "flbp_batch_run_tol", "flbp_adjoint_forward", "flbp_adjoint_backward", "flbp_set_factor_probs",
-            "flbp_adjoint_backward_device", "flbp_get_beliefs_device", "flbp_clamp_vars", "flbp_layout_digest"]
+            "flbp_adjoint_backward_device", "flbp_get_beliefs_device", "flbp_clamp_vars", "flbp_layout_digest",
+            "flbp_update_seq", "flbp_shuffled_factors", "flbp_seq_batches", "flbp_set_update_seq", "flbp_update_info"]

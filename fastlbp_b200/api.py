@@ -10,7 +10,7 @@ Names and argument meanings follow FastLBP's C++ classes
 from __future__ import annotations
 
 import ctypes as C
-from typing import Dict, Optional, Sequence
+from typing import Dict, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -180,6 +180,47 @@ def layout_digest(arrays: Dict[str, np.ndarray], threads: int = 0, graph_of=None
     return int(out.value)
 
 
+UPDATES = {"PARALL": 0, "SEQFIX": 1, "TOPO": 2}
+
+
+def update_seq(arrays: Dict[str, np.ndarray], updates: str = "SEQFIX", seed: int = 42,
+               factor_order=None) -> np.ndarray:
+    """The update sequence of a sequential schedule as factor-major slots
+    (flbp_update_seq). SEQFIX takes the factors in `factor_order`, by default
+    0..F-1 shuffled by std::mt19937(seed) as the reference's first CausalBP of
+    a thread does (csrc/ext/causal_bp.cu:116, 186-201); TOPO ranks edges by a
+    breadth-first order (:203-304)."""
+    if updates not in ("SEQFIX", "TOPO"):
+        raise ValueError("updates must be SEQFIX or TOPO")
+    keep = []
+    desc = _desc_from_arrays(arrays, keep)
+    seq = np.zeros(max(1, desc.n_slots), np.int64)
+    order = None
+    if updates == "SEQFIX":
+        if factor_order is None:
+            order = np.zeros(max(1, desc.n_factors), np.int32)
+            check(lib().flbp_shuffled_factors(int(desc.n_factors), int(seed) & 0xffffffff, order))
+        else:
+            order = np.ascontiguousarray(factor_order, np.int32)
+            if order.size != desc.n_factors:
+                raise ValueError("factor_order must list every factor once")
+    check(lib().flbp_update_seq(C.byref(desc), UPDATES[updates],
+                                None if order is None else order.ctypes.data_as(C.c_void_p), seq))
+    return seq[:desc.n_slots]
+
+
+def seq_batches(arrays: Dict[str, np.ndarray], seq) -> Tuple[np.ndarray, int]:
+    """(batch of every factor-major slot, number of batches) of an update
+    sequence (flbp_seq_batches; host only)."""
+    keep = []
+    desc = _desc_from_arrays(arrays, keep)
+    sq = np.ascontiguousarray(seq, np.int64)
+    out = np.zeros(max(1, desc.n_slots), np.int64)
+    nb = C.c_int64()
+    check(lib().flbp_seq_batches(C.byref(desc), sq, sq.size, out.ctypes.data_as(C.c_void_p), C.byref(nb)))
+    return out[:desc.n_slots], int(nb.value)
+
+
 def _check_device_tensor(t, n: int, name: str) -> None:
     import torch
 
@@ -219,7 +260,11 @@ class Engine:
     """The C-ABI engine over reference-order graph arrays (flbp_engine_*)."""
 
     def __init__(self, arrays: Dict[str, np.ndarray], precision: int = 32, damping: float = 0.0,
-                 stream: Optional[int] = None, device: int = -1):
+                 stream: Optional[int] = None, device: int = -1, updates: str = "PARALL", seed: int = 42):
+        """updates: "PARALL" (default), or "SEQFIX" / "TOPO" to run the
+        reference's sequential schedule (update_seq(arrays, updates, seed))."""
+        if updates not in UPDATES:
+            raise ValueError("updates must be one of PARALL, SEQFIX, TOPO")
         keep = []
         desc = _desc_from_arrays(arrays, keep)
         opts = N.EngineOpts(int(precision), int(device), float(damping), stream)
@@ -230,6 +275,23 @@ class Engine:
         self.n_slots = int(desc.n_slots)
         self.n_factors = int(desc.n_factors)
         self.info = None
+        if updates != "PARALL":
+            self.set_update_seq(update_seq(arrays, updates, seed))
+
+    def set_update_seq(self, seq) -> None:
+        """Run the sweeps in the conflict-free batches of an update sequence
+        (None: PARALL again); messages return to the init() state."""
+        if seq is None:
+            check(lib().flbp_set_update_seq(self._h, None, 0))
+            return
+        sq = np.ascontiguousarray(seq, np.int64)
+        check(lib().flbp_set_update_seq(self._h, sq.ctypes.data_as(C.c_void_p), sq.size))
+
+    def update_info(self) -> Tuple[bool, int]:
+        """(runs a sequential schedule, batches per sweep)."""
+        a, b = C.c_int32(), C.c_int64()
+        check(lib().flbp_update_info(self._h, C.byref(a), C.byref(b)))
+        return bool(a.value), int(b.value)
 
     @classmethod
     def from_graph(cls, fg: CausalFactorGraph, **kw) -> "Engine":
@@ -416,10 +478,15 @@ class CausalBP:
         self.tol = float(get("tol", 1e-9))
         self.maxiter = int(get("maxiter", 10000))
         self.maxtime = float(get("maxtime", 10.0))
-        self.updates = get("updates", "SEQFIX")
+        self.updates = str(get("updates", "SEQFIX"))
+        if self.updates not in UPDATES:
+            self.updates = "SEQFIX"  # unknown names fall back to SEQFIX (csrc/ext/causal_bp.cu:173-178)
         prec = str(get("precision", "FP32")).upper()
+        # SEQFIX shuffles the factors with std::mt19937("seed", 42 by default): the
+        # order of the reference's first CausalBP of a thread
         self.engine = Engine.from_graph(fg, precision=64 if prec == "FP64" else 32,
-                                        damping=float(get("damping", 0.0)))
+                                        damping=float(get("damping", 0.0)), updates=self.updates,
+                                        seed=int(get("seed", 42)))
         self._beliefs = np.zeros(self.engine.n_vars)
         self._lowpass = None
         self._iters = 0

@@ -1,9 +1,12 @@
 // CausalBP of the drop-in C++ API: property parsing, construction of the
-// GPU engine through the C ABI, and the three run entry points of
+// GPU engine through the C ABI (with the SEQFIX / TOPO update sequence of
+// csrc/ext/causal_bp.cu:186-304 when asked for), and the three run entry points of
 // csrc/ext/causal_bp.cu (run() :858-910, run(tol,maxIters,hist) :912-1004,
 // run(tol,minIters,maxIters,hist) :1006-1143).
 
+#include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <iostream>
 #include <string>
 #include <vector>
@@ -45,15 +48,6 @@ void CausalBP::setProperties(const PropertySet &opts) {
         else if (p == "FP32" || p == "fp32") props.precision = 32;
         else std::cerr << "CausalBP: unknown precision '" << p << "', using FP32" << std::endl;
     }
-    if (props.updates != Properties::UpdateType::PARALL) {
-        static bool warned = false;
-        if (!warned) {
-            std::cerr << "CausalBP: updates="
-                      << (props.updates == Properties::UpdateType::TOPO ? "TOPO" : "SEQFIX")
-                      << " runs the synchronous PARALL schedule on this engine" << std::endl;
-            warned = true;
-        }
-    }
     if (props.logdomain) {
         static bool warned = false;
         if (!warned) {
@@ -73,6 +67,22 @@ void CausalBP::construct() {
     o.damping = props.damping;
     o.stream = nullptr;
     check(flbp_engine_create(&a.desc, &o, &_engine), "flbp_engine_create");
+    if (props.updates != Properties::UpdateType::PARALL) {
+        // buildFixedUpdateSeq / buildTopoUpdateSeq (csrc/ext/causal_bp.cu:186-304): SEQFIX draws
+        // its factor order from the thread's rnd_gen, once per construction, as the reference does
+        std::vector<int32_t> order;
+        int32_t kind = FLBP_UPDATES_TOPO;
+        if (props.updates == Properties::UpdateType::SEQFIX) {
+            std::vector<int> numbers(nrFactors());
+            for (int i = 0; i < (int)numbers.size(); ++i) numbers[i] = i;
+            std::shuffle(numbers.begin(), numbers.end(), rnd_gen);
+            order.assign(numbers.begin(), numbers.end());
+            kind = FLBP_UPDATES_SEQFIX;
+        }
+        std::vector<int64_t> seq((size_t)a.desc.n_slots);
+        check(flbp_update_seq(&a.desc, kind, order.data(), seq.data()), "flbp_update_seq");
+        check(flbp_set_update_seq(_engine, seq.data(), (int64_t)seq.size()), "flbp_set_update_seq");
+    }
     _beliefsV.assign(nrVars(), 0.0);
 }
 

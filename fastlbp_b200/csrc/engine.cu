@@ -19,6 +19,7 @@
 #include "engine_internal.h"
 #include "kernels.cuh"
 #include "adjoint.cuh"
+#include "seq.cuh"
 
 namespace flbp {
 
@@ -87,6 +88,17 @@ struct flbp_engine {
     double *d_ref_out = nullptr;       // per-variable results in the caller's order (readback staging)
     uint32_t adj_group_n[4] = {0, 0, 0, 0};
     std::vector<double> factor_p_host;  // every reference factor's p (for derivatives of folded constants)
+    std::vector<double> factor_q_host;  // every reference factor's q
+    std::vector<int64_t> ref_head;      // every reference factor's head slot
+    // Sequential schedule (updates=SEQFIX / TOPO): its layout and device state.
+    bool seq = false;
+    SeqLayout SQ;
+    uint32_t *d_sq_foff = nullptr, *d_sq_var = nullptr, *d_sq_items = nullptr, *d_sq_tgt = nullptr;
+    uint32_t *d_sq_iota = nullptr;
+    uint8_t *d_sq_kind = nullptr;
+    void *d_sq_cst = nullptr, *d_sq_pq = nullptr, *d_sq_fv = nullptr, *d_sq_vf = nullptr, *d_sq_nw = nullptr;
+    double *d_sq_S = nullptr;
+    int2 *d_sq_cnt = nullptr;
     std::vector<int8_t> clamp_state;    // per reference variable: -1 free, else the value it is clamped to
     // (slot, value) of every slot of a clamped variable: its v->f message is
     // +-inf from init() on, as if the variable had left the factor
@@ -178,6 +190,63 @@ VarArgs var_args(flbp_engine *e) {
     a.trange = nullptr;
     a.n_graphs = 0;
     return a;
+}
+
+SeqArgs seq_args(flbp_engine *e) {
+    SeqArgs a;
+    a.foff = e->d_sq_foff;
+    a.var = e->d_sq_var;
+    a.kind = e->d_sq_kind;
+    a.cst = e->d_sq_cst;
+    a.pq = e->d_sq_pq;
+    a.items = e->d_sq_items;
+    a.tgt = e->d_sq_tgt;
+    a.iota = e->d_sq_iota;
+    a.fv = e->d_sq_fv;
+    a.vf = e->d_sq_vf;
+    a.nw = e->d_sq_nw;
+    a.S = e->d_sq_S;
+    a.cnt = e->d_sq_cnt;
+    return a;
+}
+
+unsigned int seq_belief_grid(const flbp_engine *e) {
+    const uint64_t b = ((uint64_t)e->L.V + 255) / 256;
+    return (unsigned int)std::max<uint64_t>(1, std::min<uint64_t>(b, 148ull * 8));
+}
+
+// Kernels of one sequential sweep: `which` bit 0 the batches (with the
+// sweep's opening kernel), bit 1 the beliefs of the tolerance / low-pass loops.
+long long seq_sweep_launches(const flbp_engine *e, int mode, int which) {
+    return ((which & 1) ? 1 + 2LL * e->SQ.n_batches : 0) + (((which & 2) && (mode == 1 || mode == 2)) ? 1 : 0);
+}
+
+template <typename T>
+void launch_seq_sweep(flbp_engine *e, int mode, int which) {
+    const SeqArgs a = seq_args(e);
+    const SeqLayout &Q = e->SQ;
+    if (which & 1) {
+        seq_begin_kernel<<<1, 1, 0, e->stream>>>(e->d_ctl);
+        for (uint32_t b = 0; b < Q.n_batches; b++) {
+            const uint32_t i0 = Q.ioff[b], i1 = Q.ioff[b + 1], t0 = Q.toff[b], t1 = Q.toff[b + 1];
+            seq_factor_kernel<T><<<(i1 - i0 + kSeqWarps - 1) / kSeqWarps, 32 * kSeqWarps, 0, e->stream>>>(a, i0, i1,
+                                                                                                      e->d_ctl);
+            if (e->damping != 0.0)
+                seq_apply_kernel<T, true><<<(t1 - t0 + 255) / 256, 256, 0, e->stream>>>(a, t0, t1, (T)e->damping,
+                                                                                       e->d_ctl);
+            else
+                seq_apply_kernel<T, false><<<(t1 - t0 + 255) / 256, 256, 0, e->stream>>>(a, t0, t1, (T)0, e->d_ctl);
+        }
+    }
+    if ((which & 2) && (mode == 1 || mode == 2)) {
+        const VarArgs va = var_args(e);
+        if (mode == 1)
+            seq_belief_kernel<1><<<seq_belief_grid(e), 256, 0, e->stream>>>(va, e->d_sq_S, e->d_sq_cnt,
+                                                                            (uint32_t)e->L.V, e->d_ctl);
+        else
+            seq_belief_kernel<2><<<seq_belief_grid(e), 256, 0, e->stream>>>(va, e->d_sq_S, e->d_sq_cnt,
+                                                                            (uint32_t)e->L.V, e->d_ctl);
+    }
 }
 
 constexpr int kStages = 3;  // bulk-copy pipeline depth of the variable pass (and of the FP64 factor pass)
@@ -273,6 +342,11 @@ void launch_sweep(flbp_engine *e, int mode, int which = 3) {
 }
 
 void launch_sweep_any(flbp_engine *e, int mode, int which = 3) {
+    if (e->seq) {
+        if (e->prec == 64) launch_seq_sweep<double>(e, mode, which);
+        else launch_seq_sweep<float>(e, mode, which);
+        return;
+    }
     if (e->prec == 64) launch_sweep<double>(e, mode, which);
     else launch_sweep<float>(e, mode, which);
 }
@@ -291,7 +365,12 @@ void launch_beliefs_only_t(flbp_engine *e, double *dst) {
 }
 
 void launch_beliefs_only(flbp_engine *e, double *dst) {
-    if (e->prec == 64) launch_beliefs_only_t<double>(e, dst);
+    if (e->seq) {
+        VarArgs va = var_args(e);
+        va.belief = dst;
+        seq_belief_kernel<3><<<seq_belief_grid(e), 256, 0, e->stream>>>(va, e->d_sq_S, e->d_sq_cnt, (uint32_t)e->L.V,
+                                                                        e->d_ctl);
+    } else if (e->prec == 64) launch_beliefs_only_t<double>(e, dst);
     else launch_beliefs_only_t<float>(e, dst);
     e->launches += 1;
 }
@@ -320,9 +399,14 @@ int sweep_graph(flbp_engine *e, int mode, int n, cudaGraphExec_t *out) {
     return FLBP_OK;
 }
 
-// Launch n sweeps as power-of-two graph chunks.
+// Launch n sweeps as power-of-two graph chunks (of at most 64 sweeps, and for
+// a sequential schedule of about 2048 kernels).
 int launch_sweeps(flbp_engine *e, int mode, long long n) {
     if (e->L.nf_sell + e->L.nf_big == 0 && e->L.V == 0) return FLBP_OK;
+    const long long per = e->seq ? seq_sweep_launches(e, mode, 3) : 2;
+    int kmax = 64;
+    if (e->seq)
+        while (kmax > 1 && (long long)kmax * per > 2048) kmax /= 2;
     if (e->ktime) {  // no graphs: events around each pass
         for (long long i = 0; i < n; i++) {
             while (e->kev.size() < e->kev_used + 3) {
@@ -337,18 +421,18 @@ int launch_sweeps(flbp_engine *e, int mode, long long n) {
             FLBP_CUDA(cudaEventRecord(ev[1], e->stream));
             launch_sweep_any(e, mode, 2);
             FLBP_CUDA(cudaEventRecord(ev[2], e->stream));
-            e->launches += 2;
+            e->launches += per;
         }
         return FLBP_OK;
     }
     while (n > 0) {
         int k = 1;
-        while ((long long)k * 2 <= n && k < 64) k *= 2;
+        while ((long long)k * 2 <= n && k < kmax) k *= 2;
         cudaGraphExec_t x;
         int rc = sweep_graph(e, mode, k, &x);
         if (rc) return rc;
         FLBP_CUDA(cudaGraphLaunch(x, e->stream));
-        e->launches += 2LL * k;
+        e->launches += per * k;
         n -= k;
     }
     return FLBP_OK;
@@ -406,6 +490,13 @@ int begin_call(flbp_engine *e) {
     }
     FLBP_CUDA(cudaSetDevice(e->device));
     return FLBP_OK;
+}
+
+// Entry points of the PARALL layout that a sequential schedule does not support.
+int refuse_seq(flbp_engine *e, const char *what) {
+    if (!e->seq) return FLBP_OK;
+    set_error(std::string(what) + " is not available with a sequential update schedule");
+    return FLBP_ERR_STATE;
 }
 
 int record_start(flbp_engine *e) {
@@ -559,6 +650,8 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
         return rc;
     }
     if (graph->n_factors > 0 && graph->factor_p) e->factor_p_host.assign(graph->factor_p, graph->factor_p + graph->n_factors);
+    if (graph->n_factors > 0 && graph->factor_q) e->factor_q_host.assign(graph->factor_q, graph->factor_q + graph->n_factors);
+    if (graph->n_factors > 0) e->ref_head.assign(graph->factor_head, graph->factor_head + graph->n_factors);
     e->prec = o.precision;
     e->tsize = o.precision == 64 ? 8 : 4;
     e->damping = o.damping;
@@ -759,7 +852,9 @@ int flbp_engine_destroy(flbp_engine *e) {
                     e->d_fbt_kind, e->d_fbt_pq, e->d_vbt_prior, e->d_f_graph, e->d_v_graph, e->d_gstate, e->d_ftrange, e->d_vtrange,
                     e->d_ckpt, e->d_seg_vf, e->d_seg_fv, e->d_lam, e->d_lam2, e->d_mu, e->d_gp, e->d_gq,
                     e->d_gprior, e->d_gs, e->d_int_of_var, e->d_f_of_int, e->d_pri_fac, e->d_pri_var, e->d_pri_coef,
-                    e->d_adj_in, e->d_adj_out, e->d_adj_groups, e->d_ref_out, e->d_clamp_slots};
+                    e->d_adj_in, e->d_adj_out, e->d_adj_groups, e->d_ref_out, e->d_clamp_slots,
+                    e->d_sq_foff, e->d_sq_var, e->d_sq_items, e->d_sq_tgt, e->d_sq_iota, e->d_sq_kind,
+                    e->d_sq_cst, e->d_sq_pq, e->d_sq_fv, e->d_sq_vf, e->d_sq_nw, e->d_sq_S, e->d_sq_cnt};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (e->h_ctl) cudaFreeHost(e->h_ctl);
@@ -777,6 +872,11 @@ int flbp_init(flbp_engine *e) {
     FLBP_CUDA(cudaMemsetAsync(e->d_vf, 0, ns * e->tsize, e->stream));
     FLBP_CUDA(cudaMemsetAsync(e->d_fv, 0, e->n_ent * e->tsize, e->stream));
     if (e->d_fvd) FLBP_CUDA(cudaMemsetAsync(e->d_fvd, 0, e->n_ent * e->tsize, e->stream));
+    if (e->seq) {  // every message (1, 1): log-odds 0; totals and counts 0 (causal_bp.cu:824-856)
+        FLBP_CUDA(cudaMemsetAsync(e->d_sq_fv, 0, std::max<size_t>(1, (size_t)e->L.E) * e->tsize, e->stream));
+        FLBP_CUDA(cudaMemsetAsync(e->d_sq_S, 0, std::max<size_t>(1, (size_t)e->L.V) * sizeof(double), e->stream));
+        FLBP_CUDA(cudaMemsetAsync(e->d_sq_cnt, 0, std::max<size_t>(1, (size_t)e->L.V) * sizeof(int2), e->stream));
+    }
     if ((rc = apply_clamp_slots(e))) return rc;
     e->t = 0;
     e->lowpass_valid = false;
@@ -964,6 +1064,22 @@ int flbp_compute_beliefs(flbp_engine *e, double *out, int64_t n) {
 static int fv_lambda(flbp_engine *e, std::vector<double> &lam) {
     build_export_maps(e->L);
     const HostLayout &L = e->L;
+    if (e->seq) {  // one message per edge, in device-slot order
+        const size_t ne = std::max<size_t>(1, (size_t)L.E);
+        std::vector<double> m(ne);
+        if (e->prec == 64) {
+            FLBP_CUDA(cudaMemcpyAsync(m.data(), e->d_sq_fv, ne * 8, cudaMemcpyDeviceToHost, e->stream));
+        } else {
+            std::vector<float> f(ne);
+            FLBP_CUDA(cudaMemcpyAsync(f.data(), e->d_sq_fv, ne * 4, cudaMemcpyDeviceToHost, e->stream));
+            FLBP_CUDA(cudaStreamSynchronize(e->stream));
+            for (size_t i = 0; i < ne; i++) m[i] = f[i];
+        }
+        FLBP_CUDA(cudaStreamSynchronize(e->stream));
+        lam.assign((size_t)L.E, 0.0);
+        for (int64_t r = 0; r < L.E; r++) lam[L.fm_to_vm[r]] = m[e->SQ.dslot[r]];
+        return FLBP_OK;
+    }
     const size_t ne = L.v_ent.size();
     const void *src = e->d_fvd ? e->d_fvd : e->d_fv;
     std::vector<double> ent(ne);
@@ -1476,7 +1592,7 @@ extern "C" {
 
 int flbp_adjoint_forward(flbp_engine *e, int64_t sweeps, int64_t every, double *beliefs, int64_t n) {
     int rc = begin_call(e);
-    if (rc) return rc;
+    if (rc || (rc = refuse_seq(e, "the adjoint"))) return rc;
     if (e->damping != 0.0) {
         set_error("the adjoint needs an engine without damping");
         return FLBP_ERR_INVALID;
@@ -1533,7 +1649,7 @@ int flbp_adjoint_forward(flbp_engine *e, int64_t sweeps, int64_t every, double *
 
 int flbp_adjoint_backward(flbp_engine *e, const double *grad_beliefs, double *grad_p, double *grad_q) {
     int rc = begin_call(e);
-    if (rc) return rc;
+    if (rc || (rc = refuse_seq(e, "the adjoint"))) return rc;
     const HostLayout &L = e->L;
     const size_t nv = std::max<int64_t>(1, L.V), nF = std::max<int64_t>(1, L.F);
     if (!e->d_adj_in && ((rc = dalloc(e, &e->d_adj_in, nv)) || (rc = dalloc(e, &e->d_adj_out, 2 * nF)))) return rc;
@@ -1559,7 +1675,7 @@ int flbp_adjoint_backward(flbp_engine *e, const double *grad_beliefs, double *gr
 
 int flbp_adjoint_backward_device(flbp_engine *e, const double *grad_beliefs, double *grad_p, double *grad_q) {
     int rc = begin_call(e);
-    if (rc) return rc;
+    if (rc || (rc = refuse_seq(e, "the adjoint"))) return rc;
     if (!grad_beliefs && e->L.V) {
         set_error("grad_beliefs is required");
         return FLBP_ERR_INVALID;
@@ -1586,7 +1702,7 @@ int flbp_get_beliefs_device(flbp_engine *e, double *out, int64_t n) {
 
 int flbp_set_factor_probs(flbp_engine *e, const double *p, const double *q) {
     int rc = begin_call(e);
-    if (rc) return rc;
+    if (rc || (rc = refuse_seq(e, "flbp_set_factor_probs"))) return rc;
     HostLayout &L = e->L;
     for (int64_t I = 0; I < L.F; I++) {
         if (!(p[I] >= 0.0 && p[I] <= 1.0) || !(q[I] >= 0.0 && q[I] <= 1.0)) {
@@ -1661,7 +1777,7 @@ extern "C" {
 
 int flbp_clamp_vars(flbp_engine *e, int64_t n, const int64_t *vars, const int32_t *values) {
     int rc = begin_call(e);
-    if (rc) return rc;
+    if (rc || (rc = refuse_seq(e, "flbp_clamp_vars"))) return rc;
     HostLayout &L = e->L;
     if (n < 0 || (n > 0 && (!vars || !values))) {
         set_error("clamp list is malformed");
@@ -1825,6 +1941,115 @@ int flbp_clamp_vars(flbp_engine *e, int64_t n, const int64_t *vars, const int32_
     e->clamp_slots.swap(slots);
     e->iters = 0;
     e->lowpass_valid = false;
+    return FLBP_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ sequential schedules
+
+namespace {
+
+void free_seq(flbp_engine *e) {
+    void *bufs[] = {e->d_sq_foff, e->d_sq_var, e->d_sq_items, e->d_sq_tgt, e->d_sq_iota, e->d_sq_kind, e->d_sq_cst,
+                    e->d_sq_pq,   e->d_sq_fv,  e->d_sq_vf,    e->d_sq_nw,  e->d_sq_S,    e->d_sq_cnt};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    e->d_sq_foff = e->d_sq_var = e->d_sq_items = e->d_sq_tgt = e->d_sq_iota = nullptr;
+    e->d_sq_kind = nullptr;
+    e->d_sq_cst = e->d_sq_pq = e->d_sq_fv = e->d_sq_vf = e->d_sq_nw = nullptr;
+    e->d_sq_S = nullptr;
+    e->d_sq_cnt = nullptr;
+    e->SQ = SeqLayout();
+    e->seq = false;
+}
+
+template <typename T>
+int upload_seq_consts(flbp_engine *e) {
+    const SeqLayout &Q = e->SQ;
+    std::vector<T> cst(Q.cst.begin(), Q.cst.end()), pq(Q.pq.begin(), Q.pq.end());
+    int rc;
+    if ((rc = dalloc(e, (T **)&e->d_sq_cst, cst.size())) || (rc = dalloc(e, (T **)&e->d_sq_pq, pq.size())) ||
+        (rc = upload(e, (T *)e->d_sq_cst, cst)) || (rc = upload(e, (T *)e->d_sq_pq, pq)))
+        return rc;
+    const size_t ne = std::max<size_t>(1, (size_t)e->L.E);
+    if ((rc = dalloc(e, (T **)&e->d_sq_fv, ne)) || (rc = dalloc(e, (T **)&e->d_sq_vf, ne)) ||
+        (rc = dalloc(e, (T **)&e->d_sq_nw, ne)))
+        return rc;
+    FLBP_CUDA(cudaStreamSynchronize(e->stream));  // the host vectors above go out of scope
+    return FLBP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int flbp_set_update_seq(flbp_engine *e, const int64_t *seq, int64_t n) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    if (e->n_graphs > 0) {
+        set_error("sequential update schedules are not available on batched engines");
+        return FLBP_ERR_STATE;
+    }
+    for (int8_t st : e->clamp_state)
+        if (st >= 0) {
+            set_error("sequential update schedules are not available after flbp_clamp_vars");
+            return FLBP_ERR_STATE;
+        }
+    const HostLayout &L = e->L;
+    SeqLayout Q;
+    if (seq) {  // build before touching the engine, so that a bad sequence leaves it as it was
+        std::vector<int64_t> slot_var(L.ref_slot_var.begin(), L.ref_slot_var.end());
+        flbp_graph_desc g{};
+        g.n_vars = L.V;
+        g.n_factors = L.F;
+        g.n_slots = L.E;
+        g.factor_offsets = L.ref_off.data();
+        g.slot_var = slot_var.data();
+        g.factor_head = e->ref_head.data();
+        g.factor_p = e->factor_p_host.data();
+        g.factor_q = e->factor_q_host.data();
+        std::string err;
+        if ((rc = build_seq_layout(g, L, seq, n, Q, err))) {
+            set_error(err);
+            return rc;
+        }
+    }
+    FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    for (auto &kv : e->graphs) cudaGraphExecDestroy(kv.second);  // captured for the previous schedule
+    e->graphs.clear();
+    free_seq(e);
+    if (seq) {
+        e->SQ = std::move(Q);
+        const SeqLayout &S = e->SQ;
+        const size_t nv = std::max<size_t>(1, (size_t)L.V), ne = std::max<size_t>(1, (size_t)L.E);
+        std::vector<uint32_t> iota(ne);
+        for (size_t k = 0; k < ne; k++) iota[k] = (uint32_t)k;
+        if ((rc = dalloc(e, &e->d_sq_foff, S.foff.size())) || (rc = upload(e, e->d_sq_foff, S.foff)) ||
+            (rc = dalloc(e, &e->d_sq_var, S.var.size())) || (rc = upload(e, e->d_sq_var, S.var)) ||
+            (rc = dalloc(e, &e->d_sq_kind, S.kind.size())) || (rc = upload(e, e->d_sq_kind, S.kind)) ||
+            (rc = dalloc(e, &e->d_sq_items, S.items.size())) || (rc = upload(e, e->d_sq_items, S.items)) ||
+            (rc = dalloc(e, &e->d_sq_tgt, S.tgt.size())) || (rc = upload(e, e->d_sq_tgt, S.tgt)) ||
+            (rc = dalloc(e, &e->d_sq_iota, ne)) || (rc = upload(e, e->d_sq_iota, iota)) ||
+            (rc = dalloc(e, &e->d_sq_S, nv)) || (rc = dalloc(e, &e->d_sq_cnt, nv)) ||
+            (rc = (e->prec == 64 ? upload_seq_consts<double>(e) : upload_seq_consts<float>(e)))) {
+            free_seq(e);
+            return rc;
+        }
+        e->seq = true;
+    }
+    if ((rc = flbp_init(e))) return rc;
+    FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    return FLBP_OK;
+}
+
+int flbp_update_info(flbp_engine *e, int32_t *sequential, int64_t *n_batches) {
+    if (!e) {
+        set_error("null engine handle");
+        return FLBP_ERR_INVALID;
+    }
+    if (sequential) *sequential = e->seq ? 1 : 0;
+    if (n_batches) *n_batches = e->seq ? (int64_t)e->SQ.n_batches : 1;
     return FLBP_OK;
 }
 

@@ -181,6 +181,35 @@ struct GraphIds {
     const uint32_t *var_graph;
 };
 
+// Sequential schedule (updates=SEQFIX / TOPO) of one engine. Every edge is a
+// message of its own here, constants included, because the reference folds
+// a message into its variable's product only when the edge's turn comes.
+// Device slots are the reference's factor-major slots with each factor's
+// head moved to the front (the order the factor kernels read).
+constexpr uint8_t kSeqConst = 0x80;  // kind flag: the factor sends one constant message
+struct SeqLayout {
+    uint32_t n_batches = 0;
+    uint32_t max_items = 0, max_tgt = 0;  // largest batch
+    hvec<uint32_t> foff;   // per reference factor: first device slot (F + 1)
+    hvec<uint32_t> dslot;  // reference factor-major slot -> device slot
+    hvec<uint32_t> var;    // per device slot: internal variable
+    hvec<uint8_t> kind;    // per reference factor: active factors' kind, else kSeqConst
+    hvec<double> cst;      // per reference factor: its constant message (a clamped head's output)
+    hvec<double> pq;       // per reference factor: p, q
+    hvec<uint32_t> ioff, items;  // per batch: its factors
+    hvec<uint32_t> toff, tgt;    // per batch: its target device slots
+};
+
+// Conflict-free batches of an update sequence (every factor-major slot once):
+// the batch of every slot and the number of batches.
+int seq_batches(const flbp_graph_desc &g, const int64_t *seq, int64_t n, std::vector<uint32_t> &slot_batch,
+                uint32_t &n_batches, std::string &err);
+// The TOPO update sequence.
+int topo_seq(const flbp_graph_desc &g, std::vector<int64_t> &seq, std::string &err);
+// The device layout of a sequential schedule over an engine's layout L.
+int build_seq_layout(const flbp_graph_desc &g, const HostLayout &L, const int64_t *seq, int64_t n, SeqLayout &S,
+                     std::string &err);
+
 // Builds the layout; returns FLBP_OK or an error code with `err` filled in.
 // With `graphs`, items are ordered graph by graph and every tile header also
 // names the range of graphs its items belong to (words kHdrGraphLo/Hi).

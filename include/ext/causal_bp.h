@@ -4,8 +4,9 @@
 ///
 /// Properties read from the PropertySet (exact value types, as in the
 /// reference): "tol" (Real, 1e-9), "maxiter" (size_t, 10000), "maxtime"
-/// (Real seconds, 10), "updates" (std::string: PARALL; SEQFIX and TOPO are
-/// accepted and run the PARALL schedule, with a warning), "logdomain"
+/// (Real seconds, 10), "updates" (std::string: PARALL, SEQFIX or TOPO;
+/// SEQFIX, the default, shuffles the factor order with rnd_gen at
+/// construction as the reference does), "logdomain"
 /// (bool), "verbose" (size_t). Added by this engine: "damping" (Real in
 /// [0,1), 0) and "precision" (std::string "FP32" or "FP64", "FP32").
 ///

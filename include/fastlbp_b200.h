@@ -41,6 +41,11 @@ extern "C" {
 #define FLBP_BIG_FRAC_CONVERGED 1
 #define FLBP_DIVERGED 2 /* iteration or time limit reached */
 
+/* Update schedules (the "updates" property, csrc/ext/causal_bp.cu:144-184) */
+#define FLBP_UPDATES_PARALL 0
+#define FLBP_UPDATES_SEQFIX 1
+#define FLBP_UPDATES_TOPO 2
+
 /* A causal factor graph in the reference's factor-major edge order: the
  * arrays CausalBP::construct() derives (csrc/ext/causal_bp.cu:310-407).
  * Factor I owns edge slots [factor_offsets[I], factor_offsets[I+1]) holding
@@ -342,6 +347,43 @@ int flbp_clamp_vars(flbp_engine *eng, int64_t n, const int64_t *vars, const int3
  * after a learning step: constants folded into priors follow. The graph's
  * structure (which factors are singletons, clamped or reduced) stays. */
 int flbp_set_factor_probs(flbp_engine *eng, const double *p, const double *q);
+
+/* ---- Sequential schedules (updates=SEQFIX / TOPO) ----------------------
+ * An update sequence lists every edge once, as its factor-major slot
+ * (factor_offsets[I] + position in the factor). */
+
+/* The update sequence of a schedule. FLBP_UPDATES_SEQFIX: the slots of
+ * factor_order[0], then of factor_order[1], ... (a permutation of the
+ * factors; buildFixedUpdateSeq, csrc/ext/causal_bp.cu:186-201, shuffles it
+ * with the thread's std::mt19937). FLBP_UPDATES_TOPO: edges ranked by a
+ * breadth-first order over variables and factors (buildTopoUpdateSeq,
+ * csrc/ext/causal_bp.cu:203-304); factor_order is ignored. seq_out holds
+ * n_slots entries. */
+int flbp_update_seq(const flbp_graph_desc *graph, int32_t kind, const int32_t *factor_order, int64_t *seq_out);
+
+/* 0..n-1 shuffled by std::shuffle with std::mt19937(seed): the SEQFIX factor
+ * order of the first CausalBP a thread constructs after seeding rnd_gen. */
+int flbp_shuffled_factors(int64_t n, uint32_t seed, int32_t *order);
+
+/* The conflict-free batches the engine runs a sequence in
+ * (putUpdateSeqToKernelFused, csrc/ext/causal_bp.cu:583-722): batch of every
+ * slot (n_slots entries, may be NULL) and their number. Host only. */
+int flbp_seq_batches(const flbp_graph_desc *graph, const int64_t *seq, int64_t n, int64_t *slot_batch,
+                     int64_t *n_batches);
+
+/* Run this engine's sweeps in the batches of `seq` (n == n_slots), one batch
+ * after the other: the batch's v->f messages from the current variable
+ * totals, then its f->v messages, each folded into its variable's total at
+ * once (calcNewMessageFused, csrc/ext/causal_bp.cu:446-476, and
+ * csrc/kernel/causal_bp_seq.cu). seq == NULL returns to PARALL. Resets the
+ * messages to the init() state. Not available on batched engines, after
+ * flbp_clamp_vars, or together with the adjoint and flbp_set_factor_probs
+ * (FLBP_ERR_STATE). */
+int flbp_set_update_seq(flbp_engine *eng, const int64_t *seq, int64_t n);
+
+/* Whether the engine runs an installed sequence (1) or PARALL (0), and its
+ * number of batches per sweep (1 for PARALL). Either pointer may be NULL. */
+int flbp_update_info(flbp_engine *eng, int32_t *sequential, int64_t *n_batches);
 
 #ifdef __cplusplus
 }

@@ -17,6 +17,9 @@
 //   * v->f kernel .............. csrc/kernel/causal_bp_parall.cu:55-92
 //   * beliefs .................. csrc/kernel/causal_bp_seq.cu:102-111, csrc/ext/causal_bp.cu:483-515
 //   * run loops ................ csrc/ext/causal_bp.cu:858-910, 912-1004, 1006-1143 (+ HostBeliefHistory :28-78)
+//   * SEQFIX / TOPO orders ..... csrc/ext/causal_bp.cu:186-201, 203-304
+//   * conflict-free batches .... csrc/ext/causal_bp.cu:583-722
+//   * sequential sweep ......... csrc/kernel/causal_bp_seq.cu:13-83, 113-459, csrc/ext/causal_bp.cu:446-476
 //
 // Damping is not part of the reference. It is defined here once, for the
 // oracle and the GPU engine alike: after the f->v sweep each new f->v message
@@ -39,6 +42,8 @@
 #include <iostream>
 #include <limits>
 #include <map>
+#include <queue>
+#include <random>
 #include <set>
 #include <sstream>
 #include <stdexcept>
@@ -320,14 +325,36 @@ OLayout construct(const OGraph &g) {
 
 // ------------------------------------------------------------------ kernels
 
-inline void scale2(double &x, double &y) {  // csrc/kernel/causal_bp_parall.cu:14-18
+inline void scale_parall(double &x, double &y) {  // csrc/kernel/causal_bp_parall.cu:14-18
     double m = std::fmax(x, y);
     x /= m;
     y /= m;
 }
 
-// One f->v message, csrc/kernel/causal_bp_parall.cu:102-397.
-void fv_message(const ORec &r, const double *vf0, const double *vf1, double &out0, double &out1) {
+// csrc/kernel/causal_bp_seq.cu:13-23: the sequential kernels' rescaling; it
+// differs from the PARALL one only for two equal values (both become 1, so
+// (0, 0) gives (1, 1) instead of NaN).
+inline void scale_seq(double &x, double &y) {
+    if (x < y) {
+        x = x / y;
+        y = 1.0;
+    } else if (y < x) {
+        y = y / x;
+        x = 1.0;
+    } else {
+        x = y = 1.0;
+    }
+}
+
+// One f->v message, csrc/kernel/causal_bp_parall.cu:102-397 (PARALL) and
+// csrc/kernel/causal_bp_seq.cu:162-452 (SEQ): the same formulas, with the
+// rescaling of the schedule's kernels.
+template <bool SEQ>
+void fv_message_t(const ORec &r, const double *vf0, const double *vf1, double &out0, double &out1) {
+    auto scale2 = [](double &x, double &y) {
+        if (SEQ) scale_seq(x, y);
+        else scale_parall(x, y);
+    };
     const size_t type = r.type, src = r.src, h = r.head, s = r.start, e = r.end;
     const double p0 = r.q, p1 = r.p, mask0 = r.m0, mask1 = r.m1;
     double marg0 = 0.0, marg1 = 0.0;
@@ -487,6 +514,10 @@ void fv_message(const ORec &r, const double *vf0, const double *vf1, double &out
     out1 = marg1;
 }
 
+void fv_message(const ORec &r, const double *vf0, const double *vf1, double &out0, double &out1) {
+    fv_message_t<false>(r, vf0, vf1, out0, out1);
+}
+
 double now_s() {
     struct timeval tv;
     gettimeofday(&tv, nullptr);
@@ -508,6 +539,13 @@ struct OBP {
     size_t iters = 0;
     double maxdiff_member = 0.0;
     bool logdomain = false;
+    // sequential schedule (updates=SEQFIX / TOPO): per batch its v->f records
+    // and its f->v records (indices into L.rec); empty for PARALL
+    bool seq = false;
+    std::vector<std::vector<OVfRec>> seq_vf;
+    std::vector<std::vector<size_t>> seq_fv;
+    std::vector<size_t> seq_slots;   // the update sequence as factor-major slots
+    std::vector<size_t> slot_batch;  // batch of every factor-major slot
 };
 
 void bp_init(OBP &b) {  // csrc/ext/causal_bp.cu:824-856
@@ -529,7 +567,7 @@ inline double powz(double x, double a) {  // x^a with 0^0 = 1 and 0^a = 0 for a 
 }
 
 // csrc/ext/causal_bp.cu:409-444: f->v, per-variable product, v->f.
-void bp_sweep(OBP &b) {
+void bp_sweep_parall(OBP &b) {
     const long E = (long)b.E, V = (long)b.V;
     const double d = b.damping;
     const ORec *rec = b.L.rec.data();
@@ -562,7 +600,7 @@ void bp_sweep(OBP &b) {
             else pr0 *= m0;
             if (m1 == 0) z1++;
             else pr1 *= m1;
-            scale2(pr0, pr1);
+            scale_parall(pr0, pr1);
         }
         b.prod0[i] = pr0;
         b.prod1[i] = pr1;
@@ -585,6 +623,209 @@ void bp_sweep(OBP &b) {
         b.vf0[x.ind] = pr0 / pr;
         b.vf1[x.ind] = pr1 / pr;
     }
+}
+
+// ------------------------------------------------------ sequential schedules
+
+using OEdge = std::pair<size_t, size_t>;  // (variable, dual): Edge of include/ext/causal_bp.h
+
+// csrc/ext/causal_bp.cu:186-201: factors in an order shuffled by the
+// thread-local std::mt19937 (seeded 42 at start-up, csrc/ext/causal_bp.cu:116),
+// every factor's edges in its neighbour order.
+std::vector<OEdge> seqfix_order(const OGraph &g, uint32_t seed) {
+    std::mt19937 rng(seed);
+    std::vector<int> numbers(g.factors.size());
+    for (int i = 0; i < (int)numbers.size(); ++i) numbers[i] = i;
+    std::shuffle(numbers.begin(), numbers.end(), rng);
+    std::vector<OEdge> seq;
+    for (size_t I = 0; I < numbers.size(); I++)
+        for (const ONb &n : g.nbF[numbers[I]]) seq.push_back({n.node, n.dual});
+    return seq;
+}
+
+// csrc/ext/causal_bp.cu:203-304: breadth-first order over variables (nodes
+// 0..V-1) and factors (V..V+F-1), roots in node order, neighbours in node
+// order; edges ranked by (later endpoint, earlier endpoint, factor, variable,
+// dual).
+std::vector<OEdge> topo_order(const OGraph &g) {
+    const size_t V = g.vars.size(), F = g.factors.size(), N = V + F;
+    std::vector<std::vector<size_t>> adj(N);
+    for (size_t I = 0; I < F; I++)
+        for (const ONb &n : g.nbF[I]) {
+            adj[V + I].push_back(n.node);
+            adj[n.node].push_back(V + I);
+        }
+    for (auto &a : adj) {
+        std::sort(a.begin(), a.end());
+        a.erase(std::unique(a.begin(), a.end()), a.end());
+    }
+    std::vector<size_t> order(N, N);
+    size_t next = 0;
+    std::queue<size_t> ready;
+    for (size_t r = 0; r < N; r++) {
+        if (order[r] != N) continue;
+        ready.push(r);
+        order[r] = next++;
+        while (!ready.empty()) {
+            const size_t i = ready.front();
+            ready.pop();
+            for (size_t x : adj[i]) {
+                if (order[x] != N) continue;
+                order[x] = next++;
+                ready.push(x);
+            }
+        }
+    }
+    struct Ranked {
+        size_t rank, src, factor, var, dual;
+    };
+    std::vector<Ranked> rs;
+    for (size_t I = 0; I < F; I++)
+        for (const ONb &n : g.nbF[I]) {
+            const size_t a = order[V + I], c = order[n.node];
+            rs.push_back({std::max(a, c), std::min(a, c), I, n.node, n.dual});
+        }
+    std::stable_sort(rs.begin(), rs.end(), [](const Ranked &x, const Ranked &y) {
+        if (x.rank != y.rank) return x.rank < y.rank;
+        if (x.src != y.src) return x.src < y.src;
+        if (x.factor != y.factor) return x.factor < y.factor;
+        if (x.var != y.var) return x.var < y.var;
+        return x.dual < y.dual;
+    });
+    std::vector<OEdge> seq;
+    for (const Ranked &r : rs) seq.push_back({r.var, r.dual});
+    return seq;
+}
+
+// csrc/ext/causal_bp.cu:583-722: cut the sequence into batches. An edge
+// (i, I) opens a new batch when a v->f message of I it needs is not yet in
+// the batch while its variable already receives a batch f->v message from
+// another factor (for TOPO only if that edge precedes it in the sequence),
+// or when i itself already receives one. Every batch records its new v->f
+// messages (factor-major) and its f->v records.
+void seq_batches(OBP &b, const std::vector<OEdge> &seq, bool respect_preorder) {
+    const OGraph &g = b.g;
+    std::map<OEdge, size_t> rank;
+    for (size_t k = 0; k < seq.size(); k++) rank[seq[k]] = k;
+    b.seq_vf.clear();
+    b.seq_fv.clear();
+    b.seq_slots.clear();
+    b.slot_batch.assign(b.E, 0);
+    std::set<OEdge> fv_set, vf_set;
+    std::set<size_t> v_set;
+    std::vector<OVfRec> cur_vf;
+    std::vector<size_t> cur_fv;
+    for (const OEdge &e : seq) {
+        const size_t i = e.first;
+        const size_t I = g.nbV[i][e.second].node;
+        bool conflict = false;
+        for (const ONb &j : g.nbF[I]) {
+            if (j.node == i) continue;
+            if (vf_set.find({I, j.iter}) == vf_set.end()) {
+                for (const ONb &J : g.nbV[j.node]) {
+                    if (J.node == I) continue;
+                    const OEdge fv_e(j.node, J.iter);
+                    if (fv_set.find(fv_e) != fv_set.end() && (!respect_preorder || rank[fv_e] < rank[e])) {
+                        conflict = true;
+                        break;
+                    }
+                }
+            }
+            if (conflict) break;
+        }
+        if (!conflict && v_set.find(i) != v_set.end()) conflict = true;
+        if (conflict) {
+            b.seq_vf.push_back(cur_vf);
+            b.seq_fv.push_back(cur_fv);
+            v_set.clear();
+            fv_set.clear();
+            vf_set.clear();
+            cur_vf.clear();
+            cur_fv.clear();
+        }
+        v_set.insert(i);
+        fv_set.insert(e);
+        cur_fv.push_back(b.L.row_ptr_fv[i] + e.second);
+        const size_t slot = b.L.row_ptr_vf[I] + g.nbV[i][e.second].dual;
+        b.seq_slots.push_back(slot);
+        b.slot_batch[slot] = b.seq_fv.size();
+        for (const ONb &j : g.nbF[I]) {
+            if (j.node == i || vf_set.find({I, j.iter}) != vf_set.end()) continue;
+            vf_set.insert({I, j.iter});
+            cur_vf.push_back({b.L.row_ptr_vf[I] + j.iter, j.node, b.L.row_ptr_fv[j.node] + j.dual});
+        }
+    }
+    b.seq_vf.push_back(cur_vf);
+    b.seq_fv.push_back(cur_fv);
+}
+
+// csrc/kernel/causal_bp_seq.cu:34-83: replace one f->v message and update
+// its variable's product and zero counts in place.
+void update_message(OBP &b, size_t ind, size_t v, double marg0, double marg1) {
+    const double old0 = b.fv0[ind], old1 = b.fv1[ind];
+    double p0 = b.prod0[v], p1 = b.prod1[v];
+    size_t z0 = b.nz0[v], z1 = b.nz1[v];
+    if (old0 == 0) z0--;
+    else p0 /= old0;
+    if (marg0 == 0) z0++;
+    else p0 *= marg0;
+    if (old1 == 0) z1--;
+    else p1 /= old1;
+    if (marg1 == 0) z1++;
+    else p1 *= marg1;
+    scale_seq(p0, p1);
+    b.prod0[v] = p0;
+    b.prod1[v] = p1;
+    b.nz0[v] = z0;
+    b.nz1[v] = z1;
+    b.fv0[ind] = marg0;
+    b.fv1[ind] = marg1;
+}
+
+// One sequential sweep (csrc/ext/causal_bp.cu:446-476 for every batch in
+// order): the batch's v->f messages from the current products
+// (causal_bp_seq.cu:113-147), then its f->v messages, each folded into its
+// variable's product at once (:149-459). The f->v records of a batch have
+// distinct variables, so their order inside the batch does not matter.
+// Damping (not in the reference) mixes each new message with the one it
+// replaces, as in the PARALL sweep.
+void bp_sweep_seq(OBP &b) {
+    const double d = b.damping;
+    for (size_t k = 0; k < b.seq_fv.size(); k++) {
+        for (const OVfRec &x : b.seq_vf[k]) {
+            const size_t c0 = b.nz0[x.v], c1 = b.nz1[x.v];
+            const double ms0 = b.fv0[x.src], ms1 = b.fv1[x.src];
+            double pr0 = b.prod0[x.v], pr1 = b.prod1[x.v];
+            if (c0 >= 2 || (c0 == 1 && ms0 != 0)) pr0 = 0.0;
+            else if (ms0 != 0) pr0 = pr0 / ms0;
+            if (c1 >= 2 || (c1 == 1 && ms1 != 0)) pr1 = 0.0;
+            else if (ms1 != 0) pr1 = pr1 / ms1;
+            const double pr = pr0 + pr1;
+            b.vf0[x.ind] = pr0 / pr;
+            b.vf1[x.ind] = pr1 / pr;
+        }
+        for (size_t r : b.seq_fv[k]) {
+            double o0, o1;
+            fv_message_t<true>(b.L.rec[r], b.vf0.data(), b.vf1.data(), o0, o1);
+            if (d != 0.0) {
+                double n0 = powz(o0, 1.0 - d) * powz(b.fv0[r], d);
+                double n1 = powz(o1, 1.0 - d) * powz(b.fv1[r], d);
+                if (n0 == 0 && n1 == 0) {
+                    n0 = 0.5;
+                    n1 = 0.5;
+                }
+                const double s = n0 + n1;
+                o0 = n0 / s;
+                o1 = n1 / s;
+            }
+            update_message(b, r, b.L.rec[r].v, o0, o1);
+        }
+    }
+}
+
+void bp_sweep(OBP &b) {
+    if (b.seq) bp_sweep_seq(b);
+    else bp_sweep_parall(b);
 }
 
 // csrc/ext/causal_bp.cu:483-515 with getBeliefsV (causal_bp_seq.cu:102-111).
@@ -945,6 +1186,25 @@ void orc_bp_messages(void *b, double *fv0, double *fv1, double *vf0, double *vf1
         vf0[k] = B.vf0[k];
         vf1[k] = B.vf1[k];
     }
+}
+
+// Switch to a sequential schedule: kind 1 SEQFIX with the factor order
+// shuffled by std::mt19937(seed), kind 2 TOPO. Returns the number of batches.
+int64_t orc_bp_set_schedule(void *b, int kind, uint32_t seed) {
+    auto &B = *(OBP *)b;
+    if (kind == 1) seq_batches(B, seqfix_order(B.g, seed), false);
+    else if (kind == 2) seq_batches(B, topo_order(B.g), true);
+    else return -1;
+    B.seq = true;
+    return (int64_t)B.seq_fv.size();
+}
+
+// The update sequence as factor-major slots (row_ptr_vf[I] + iter) and the
+// batch of every slot.
+void orc_bp_schedule(void *b, int64_t *seq_slots, int64_t *slot_batch) {
+    auto &B = *(OBP *)b;
+    for (size_t k = 0; k < B.seq_slots.size(); k++) seq_slots[k] = (int64_t)B.seq_slots[k];
+    for (size_t k = 0; k < B.slot_batch.size(); k++) slot_batch[k] = (int64_t)B.slot_batch[k];
 }
 
 // Overwrite v->f messages (factor-major); lets tests drive single f->v evaluations.

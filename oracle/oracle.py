@@ -90,6 +90,9 @@ def lib():
         L.orc_bp_current_beliefs.argtypes = [_vp, _f64p]
         L.orc_bp_messages.argtypes = [_vp, _f64p, _f64p, _f64p, _f64p]
         L.orc_bp_set_vf.argtypes = [_vp, _f64p, _f64p]
+        L.orc_bp_set_schedule.argtypes = [_vp, C.c_int, C.c_uint32]
+        L.orc_bp_set_schedule.restype = C.c_int64
+        L.orc_bp_schedule.argtypes = [_vp, _i64p, _i64p]
         _lib = L
     return _lib
 
@@ -227,7 +230,8 @@ class RefGraph(_GraphBase):
 
 
 class OracleBP:
-    """FP64 CausalBP restatement (updates=PARALL) over an OracleGraph."""
+    """FP64 CausalBP restatement over an OracleGraph: updates=PARALL, or after
+    set_schedule() the sequential SEQFIX / TOPO schedules."""
 
     def __init__(self, g: OracleGraph, damping: float = 0.0, threads: int = 1, logdomain: bool = False):
         self.L = lib()
@@ -282,6 +286,22 @@ class OracleBP:
         a = [np.zeros(self.E) for _ in range(4)]
         self.L.orc_bp_messages(self.h, *a)
         return a  # fv0, fv1 (variable-major), vf0, vf1 (factor-major)
+
+    def set_schedule(self, updates: str, seed: int = 42) -> int:
+        """Switch to updates="SEQFIX" (factor order shuffled by std::mt19937(seed),
+        as the reference's first CausalBP of a thread) or "TOPO"; returns the
+        number of batches."""
+        kind = {"SEQFIX": 1, "TOPO": 2}[updates]
+        n = int(self.L.orc_bp_set_schedule(self.h, kind, int(seed)))
+        self.n_batches = n
+        return n
+
+    def schedule(self):
+        """(update sequence as factor-major slots, batch of every slot)."""
+        seq = np.zeros(self.E, np.int64)
+        batch = np.zeros(self.E, np.int64)
+        self.L.orc_bp_schedule(self.h, seq, batch)
+        return seq, batch
 
     def set_vf(self, vf0, vf1):
         self.L.orc_bp_set_vf(self.h, np.ascontiguousarray(vf0, np.float64), np.ascontiguousarray(vf1, np.float64))

@@ -1,6 +1,7 @@
 // Command-line driver over the FastLBP reference's public API, compiled with
 // the reference sources into oracle/_ref/ref_bp by oracle/Makefile. It runs
-// the reference's own GPU FP64 CausalBP (updates=PARALL) the way
+// the reference's own GPU FP64 CausalBP (updates=PARALL, or the schedule in
+// the environment variable REF_BP_UPDATES: SEQFIX or TOPO) the way
 // examples/fl_wrapper.cu does: read the graph, clamp by label, rebuild the
 // graph from its factors, construct, init, run.
 //
@@ -80,7 +81,8 @@ int main(int argc, char **argv) {
     opts.set("maxtime", Real(57600));
     opts.set("tol", Real(tol));
     opts.set("verbose", (size_t)(getenv("REF_BP_VERBOSE") ? 1 : 0));
-    opts.set("updates", std::string("PARALL"));
+    const char *upd = getenv("REF_BP_UPDATES");
+    opts.set("updates", std::string(upd ? upd : "PARALL"));
     opts.set("logdomain", false);
 
     double best_construct = 1e30, best_run = 1e30, best_run_ev = 1e30;

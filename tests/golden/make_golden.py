@@ -3,10 +3,14 @@
 Runs oracle/_ref/ref_bp (the reference sources compiled by oracle/Makefile,
 driven through the reference's public API the way examples/fl_wrapper.cu
 does) on seeded graphs and stores, per case, the graph file (gzip), the
-clamps, the run parameters and the reference's beliefs at 17 significant
-digits. Needs a CUDA GPU; the outputs are committed under tests/golden/.
+clamps, the update schedule, the run parameters and the reference's beliefs
+at 17 significant digits. Needs a CUDA GPU; the outputs are committed under
+tests/golden/.
 
-    python tests/golden/make_golden.py --out tests/golden
+    python tests/golden/make_golden.py --out tests/golden [--only REGEX]
+
+With --only, just the matching cases are run and the existing index in --out
+is extended.
 """
 
 import argparse
@@ -47,16 +51,31 @@ def cases():
         labels = sorted(set(t.head.tolist()) | set(t.body.tolist()))
         clt = {int(l): int(rng.integers(0, 2)) for l in labels if rng.random() < 0.2}
         yield "tree_%d_fixed60" % s, t, clt, ["fixed", "60"]
+    # sequential schedules (the SEQFIX order of the process's first CausalBP)
+    yield "seqfix_cfg0_s0_fixed100", fl, {}, ["fixed", "100"], "SEQFIX"
+    yield "seqfix_cfg0_s1_clamped_tol", fl1, cl1, ["tol", "1e-6", "1000"], "SEQFIX"
+    yield "seqfix_cfg0_s1_clamped_lowpass", fl1, cl1, ["lowpass", "1e-6", "20", "60", "10"], "SEQFIX"
+    yield "topo_cfg0_s0_clamped_fixed20", fl, cl, ["fixed", "20"], "TOPO"
+    t = trees.random_tree(1003, n_factors=6, extreme=0.2)
+    yield "seqfix_tree_3_fixed60", t, {}, ["fixed", "60"], "SEQFIX"
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
+    ap.add_argument("--only", default=None, help="regex: run only the matching cases, extend the index")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     tmp = tempfile.mkdtemp()
     index = []
-    for name, fl, cl, mode in cases():
+    ipath = os.path.join(args.out, "index.json")
+    if args.only and os.path.exists(ipath):
+        index = json.load(open(ipath))
+    for case in cases():
+        name, fl, cl, mode = case[:4]
+        updates = case[4] if len(case) > 4 else "PARALL"
+        if args.only and not re.search(args.only, name):
+            continue
         gpath = os.path.join(tmp, name + ".causal_fg")
         fl.write(gpath)
         cpath = os.path.join(tmp, name + ".clamps")
@@ -64,7 +83,7 @@ def main():
             for k in sorted(cl):
                 f.write("%d %d\n" % (k, cl[k]))
         opath = os.path.join(tmp, name + ".out")
-        env = dict(os.environ, REF_BP_VERBOSE="1")
+        env = dict(os.environ, REF_BP_VERBOSE="1", REF_BP_UPDATES=updates)
         r = subprocess.run([REF_BP, gpath, cpath, opath] + mode, capture_output=True, text=True, env=env)
         if r.returncode != 0:
             raise SystemExit("ref_bp failed on %s: %s %s" % (name, r.stdout, r.stderr))
@@ -80,9 +99,12 @@ def main():
             f.write(fl.text())
         rec = dict(name=name, mode=mode, clamps={str(k): v for k, v in sorted(cl.items())}, ref=meta,
                    ref_sweeps=sweeps, beliefs=beliefs)
+        if updates != "PARALL":
+            rec["updates"] = updates
         with open(os.path.join(args.out, name + ".json"), "w") as f:
             json.dump(rec, f, indent=0)
-        index.append(name)
+        if name not in index:
+            index.append(name)
         print(name, meta)
     with open(os.path.join(args.out, "index.json"), "w") as f:
         json.dump(index, f)

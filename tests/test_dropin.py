@@ -70,3 +70,31 @@ def test_fl_wrapper_reproduces_reference_beliefs(tmp_path):
     assert set(want) <= set(got)
     err = max(abs(got[k] - want[k]) for k in want)
     assert err <= 1e-5, err
+
+
+@pytest.mark.gpu
+def test_example_ext_clamp_runs_seqfix(tmp_path):
+    """example_ext_clamp.cu asks for updates=SEQFIX and the low-pass run
+    run(1e-6, 500, 1000, 100); built unchanged against this library it runs
+    the sequential schedule with the factor order drawn from rnd_gen (seed
+    42), and its yetToConverge fraction is the oracle's for that schedule."""
+    import oracle as O
+    from fastlbp_b200 import workloads as W
+
+    exe = os.path.join(ROOT, "oracle", "_ref", "examples", "example_ext_clamp")
+    if not os.path.exists(exe):
+        pytest.skip("oracle/_ref/examples/example_ext_clamp not built (needs the FastLBP sources at build time)")
+    fl = W.config0(2)
+    graph = tmp_path / "g.causal_fg"
+    fl.write(str(graph))
+    r = subprocess.run([exe, str(graph)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = [x for x in r.stdout.splitlines() if x.startswith("yetToConverge:")]
+    assert len(line) == 1, r.stdout[-2000:]
+    got = float(line[0].split()[1])
+    og = O.OracleGraph.from_factors(fl)
+    bp = O.OracleBP(og)
+    bp.set_schedule("SEQFIX", 42)
+    bp.init()
+    frac, _, _ = bp.run_lowpass(1e-6, 500, 1000, 100)
+    assert abs(got - frac) <= 1e-5 * max(1.0, abs(frac)), (got, frac)

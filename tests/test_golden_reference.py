@@ -33,6 +33,8 @@ def oracle_run(rec, text):
     g.clamp_labels({int(k): int(v) for k, v in rec["clamps"].items()})
     g = g.rebuild()
     bp = O.OracleBP(g)
+    if rec.get("updates", "PARALL") != "PARALL":
+        bp.set_schedule(rec["updates"], 42)
     bp.init()
     mode = rec["mode"]
     out = {}
@@ -71,3 +73,42 @@ def test_golden_graphs_match_generator():
 
     rec, text = load_case("cfg0_s0_tol")
     assert text == W.config0(0).text()
+
+
+# The high-fan-in case parts from the reference from sweep 4 on: its FP64
+# probability products underflow to exact zeros, the engine's log-odds do not
+# (a documented deviation; the oracle reproduces the reference's underflow).
+ENGINE_SKIP = {"cfg2_small_clamped_fixed100"}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", [c for c in CASES if c not in ENGINE_SKIP])
+def test_engine_matches_reference_binary(name):
+    """The FP64 engine (PARALL or the case's sequential schedule) against the
+    reference's own beliefs."""
+    from fastlbp_b200 import CausalFactorGraph, Engine
+
+    rec, text = load_case(name)
+    g = CausalFactorGraph.from_text(text)
+    g.clamp_labels({int(k): int(v) for k, v in rec["clamps"].items()})
+    g = g.rebuild()
+    eng = Engine.from_graph(g, precision=64, updates=rec.get("updates", "PARALL"), seed=42)
+    eng.init()
+    mode = rec["mode"]
+    if mode[0] == "fixed":
+        eng.run_fixed(int(mode[1]))
+        b = eng.lowpass()
+    elif mode[0] == "tol":
+        info = eng.run_tol(float(mode[1]), int(mode[2]), 57600.0)
+        if rec.get("ref_sweeps") is not None:
+            assert info["total_sweeps"] == rec["ref_sweeps"]
+        b = eng.beliefs()
+    else:
+        info = eng.run_lowpass(float(mode[1]), int(mode[2]), int(mode[3]), int(mode[4]))
+        assert abs(info["frac"] - rec["ref"]["ret"]) <= 1e-12
+        b = eng.lowpass()
+    got = dict(zip(g.var_labels().tolist(), b.tolist()))
+    ref = {int(k): float(v) for k, v in rec["beliefs"].items()}
+    assert set(ref) == set(got)
+    err = max(abs(got[k] - ref[k]) for k in ref)
+    assert err <= 1e-9, (name, err)

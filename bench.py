@@ -55,12 +55,13 @@ def parse():
     ap.add_argument("--scale", type=float, default=1.0, help="graph size factor (1.0 = the 1M-variable graph)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
     ap.add_argument("--e2e-steps", type=int, default=4)
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "fl", "adjoint", "bingo"],
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "fl", "adjoint", "bingo", "seq"],
                     help="single: the 1M-variable graph (default); batch: many uneven graphs solved together; "
                          "fl: the fault-localisation graph with its statement ranking against the FP64 oracle; "
                          "adjoint: gradients through unrolled sweeps on 64 graphs of 50k tuples "
                          "(use --sweeps 100 --damping 0 --graphs 64); "
-                         "bingo: re-solving after each label, rebuild against incremental clamps")
+                         "bingo: re-solving after each label, rebuild against incremental clamps; "
+                         "seq: the sequential SEQFIX / TOPO schedules against the reference's own")
     ap.add_argument("--graphs", type=int, default=512, help="batch / adjoint workloads: number of graphs")
     ap.add_argument("--every", type=int, default=10, help="adjoint workload: checkpoint interval")
     ap.add_argument("--fd-params", type=int, default=1000, help="adjoint workload: parameters checked by differences")
@@ -450,6 +451,78 @@ def run_bingo(args, rank, world, local):
             "incremental_over_rebuild": t_r / t_i}
 
 
+def run_seq(args, rank, world, local):
+    """The sequential schedules (updates=SEQFIX / TOPO): fixed sweeps from
+    init() on Bingo-style graphs with config-1 laws, SEQFIX on 100 k tuples
+    (50 sweeps), TOPO on 10 k tuples (5 sweeps; its batches hold about three
+    edges each), each with the factor order of the first CausalBP of a
+    thread. Ours: FP32 and FP64 engines timed with CUDA events around
+    run_fixed (kernels only, the graph resident). The reference's own code
+    (oracle/_ref/ref_bp, REF_BP_UPDATES) runs the same schedule on the same
+    graph in FP64, timed around its run(); its beliefs are compared with the
+    FP64 engine's."""
+    if rank != 0:
+        return None
+    import torch
+
+    from fastlbp_b200 import CausalFactorGraph, Engine, workloads
+
+    ref_bp = os.path.join(ROOT, "oracle", "_ref", "ref_bp")
+    forms = {}
+    for updates, scale, sweeps in (("SEQFIX", 0.1, 50), ("TOPO", 0.01, 5)):
+        fl = workloads.config1(args.seed, scale=scale)
+        g = CausalFactorGraph.from_factors(fl)
+        a = g.graph_arrays()
+        E = int(a["factor_offsets"][-1])
+        rec = {"tuples": int(round(1_000_000 * scale)), "edge_slots": E, "sweeps": sweeps}
+        b64 = None
+        for prec in (32, 64):
+            e = Engine(a, precision=prec, updates=updates)
+            rec["batches"] = e.update_info()[1]
+            ts = []
+            for rep in range(max(1, args.warmup) + 2):
+                e.init()
+                info = e.run_fixed(sweeps)
+                if rep >= max(1, args.warmup):
+                    ts.append(e.last_run_ms() / 1e3)
+            rec["fp%d_updates_per_s" % prec] = 2.0 * E * sweeps / statistics.median(ts)
+            rec["fp%d_ms_per_sweep" % prec] = statistics.median(ts) / sweeps * 1e3
+            rec["fp%d_launches_per_sweep" % prec] = info["launches"] / sweeps
+            if prec == 64:
+                b64 = dict(zip(g.var_labels().tolist(), e.lowpass().tolist()))
+            e.close()
+        if os.path.exists(ref_bp) and torch.cuda.is_available():
+            path = os.path.join(tempfile.gettempdir(), "fastlbp_seq_%s_x%g.causal_fg" % (updates, scale))
+            fl.write(path)
+            out = path + ".out"
+            r = subprocess.run([ref_bp, path, "-", out, "fixed", str(sweeps), "repeat", "2"], capture_output=True,
+                               text=True, timeout=1200, env=dict(os.environ, REF_BP_UPDATES=updates))
+            if r.returncode == 0:
+                d = json.loads(r.stdout.strip().splitlines()[-1])
+                t = d["run_event_all_s"][-1]
+                rec["reference_updates_per_s"] = 2.0 * E * sweeps / t
+                rec["reference_ms_per_sweep"] = t / sweeps * 1e3
+                rec["reference_construct_s"] = d["construct_all_s"][-1]
+                rec["fp32_over_reference"] = rec["fp32_updates_per_s"] / rec["reference_updates_per_s"]
+                ref = {}
+                with open(out) as f:
+                    for line in f:
+                        k, v = line.split()
+                        ref[int(k)] = float(v)
+                rec["fp64_max_belief_diff_vs_reference"] = max(abs(b64[k] - ref[k]) for k in ref)
+            else:
+                rec["reference_unavailable"] = (r.stderr or r.stdout)[-200:]
+        forms[updates] = rec
+    s0 = forms["SEQFIX"]
+    return {"metric": METRIC, "value": s0["fp32_updates_per_s"], "unit": UNIT, "n_gpus": 1, "steps": 2,
+            "warmup": args.warmup, "ms_per_step": s0["fp32_ms_per_sweep"] * s0["sweeps"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Bingo-style generator)",
+            "config": {"workload": "sequential schedules: SEQFIX on a 100k-tuple graph (50 sweeps), TOPO on a "
+                                   "10k-tuple graph (5 sweeps), fixed sweeps from init, kernels only",
+                       "l2": "inputs smaller than L2; every sweep rewrites all messages"},
+            "forms": forms}
+
+
 def run_fl(args, rank, world, local):
     """Fault-localisation graph (200 k tuples, OR fan-in log-uniform 1-4096,
     2 % of tuples clamped as test outcomes), tolerance run tol 1e-6, maxiter
@@ -774,6 +847,8 @@ def main():
         line = run_adjoint(args, rank, world, local)
     elif args.workload == "bingo":
         line = run_bingo(args, rank, world, local)
+    elif args.workload == "seq":
+        line = run_seq(args, rank, world, local)
     else:
         line = run_ours(args, rank, world, local)
     if rank == 0 and line is not None:

@@ -457,7 +457,9 @@ def run_seq(args, rank, world, local):
     (50 sweeps), TOPO on 10 k tuples (5 sweeps; its batches hold about three
     edges each), each with the factor order of the first CausalBP of a
     thread. Ours: FP32 and FP64 engines timed with CUDA events around
-    run_fixed (kernels only, the graph resident). The reference's own code
+    run_fixed (kernels only, the graph resident), with the engine's choice of
+    launch form and with each form forced (two launches per batch; the whole
+    sweep on one thread-block cluster). The reference's own code
     (oracle/_ref/ref_bp, REF_BP_UPDATES) runs the same schedule on the same
     graph in FP64, timed around its run(); its beliefs are compared with the
     FP64 engine's."""
@@ -479,16 +481,22 @@ def run_seq(args, rank, world, local):
         for prec in (32, 64):
             e = Engine(a, precision=prec, updates=updates)
             rec["batches"] = e.update_info()[1]
-            ts = []
-            for rep in range(max(1, args.warmup) + 2):
-                e.init()
-                info = e.run_fixed(sweeps)
-                if rep >= max(1, args.warmup):
-                    ts.append(e.last_run_ms() / 1e3)
-            rec["fp%d_updates_per_s" % prec] = 2.0 * E * sweeps / statistics.median(ts)
-            rec["fp%d_ms_per_sweep" % prec] = statistics.median(ts) / sweeps * 1e3
-            rec["fp%d_launches_per_sweep" % prec] = info["launches"] / sweeps
+            # 0: the engine's choice, 1: two launches per batch, 2: one cluster per sweep
+            for kernel, tag in ((0, ""), (1, "_launches"), (2, "_cluster")):
+                e.set_seq_kernel(kernel)
+                ts = []
+                for rep in range(max(1, args.warmup) + 2):
+                    e.init()
+                    info = e.run_fixed(sweeps)
+                    if rep >= max(1, args.warmup):
+                        ts.append(e.last_run_ms() / 1e3)
+                rec["fp%d%s_updates_per_s" % (prec, tag)] = 2.0 * E * sweeps / statistics.median(ts)
+                rec["fp%d%s_ms_per_sweep" % (prec, tag)] = statistics.median(ts) / sweeps * 1e3
+                rec["fp%d%s_launches_per_sweep" % (prec, tag)] = info["launches"] / sweeps
             if prec == 64:
+                e.set_seq_kernel(0)
+                e.init()
+                e.run_fixed(sweeps)
                 b64 = dict(zip(g.var_labels().tolist(), e.lowpass().tolist()))
             e.close()
         if os.path.exists(ref_bp) and torch.cuda.is_available():

@@ -127,6 +127,7 @@ def lib():
         "flbp_seq_batches": [P(GraphDesc), _i64p, C.c_int64, _vp, P(C.c_int64)],
         "flbp_set_update_seq": [_vp, _vp, C.c_int64],
         "flbp_update_info": [_vp, P(C.c_int32), P(C.c_int64)],
+        "flbp_set_seq_kernel": [_vp, C.c_int32],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -154,4 +155,5 @@ EXPORTED = ["flbp_last_error", "flbp_version", "flbp_engine_create", "flbp_engin
             "flbp_engine_create_from_fg", "flbp_run_fixed_device_noalloc", "flbp_batch_create", "flbp_batch_info",
             "flbp_batch_run_tol", "flbp_adjoint_forward", "flbp_adjoint_backward", "flbp_set_factor_probs",
             "flbp_adjoint_backward_device", "flbp_get_beliefs_device", "flbp_clamp_vars", "flbp_layout_digest",
-            "flbp_update_seq", "flbp_shuffled_factors", "flbp_seq_batches", "flbp_set_update_seq", "flbp_update_info"]
+            "flbp_update_seq", "flbp_shuffled_factors", "flbp_seq_batches", "flbp_set_update_seq", "flbp_update_info",
+            "flbp_set_seq_kernel"]

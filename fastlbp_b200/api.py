@@ -287,6 +287,11 @@ class Engine:
         sq = np.ascontiguousarray(seq, np.int64)
         check(lib().flbp_set_update_seq(self._h, sq.ctypes.data_as(C.c_void_p), sq.size))
 
+    def set_seq_kernel(self, kind: int) -> None:
+        """Sequential sweeps: 0 choose, 1 two launches per batch, 2 one cluster
+        per sweep (flbp_set_seq_kernel)."""
+        check(lib().flbp_set_seq_kernel(self._h, int(kind)))
+
     def update_info(self) -> Tuple[bool, int]:
         """(runs a sequential schedule, batches per sweep)."""
         a, b = C.c_int32(), C.c_int64()

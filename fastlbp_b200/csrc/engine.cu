@@ -94,7 +94,9 @@ struct flbp_engine {
     bool seq = false;
     SeqLayout SQ;
     uint32_t *d_sq_foff = nullptr, *d_sq_var = nullptr, *d_sq_items = nullptr, *d_sq_tgt = nullptr;
-    uint32_t *d_sq_iota = nullptr;
+    uint32_t *d_sq_iota = nullptr, *d_sq_irec = nullptr, *d_sq_tvar = nullptr, *d_sq_bo = nullptr;
+    int seq_kernel = 0;        // 0: choose, 1: two launches per batch, 2: one cluster per sweep
+    bool seq_cluster = false;  // the sweep runs as one cluster kernel
     uint8_t *d_sq_kind = nullptr;
     void *d_sq_cst = nullptr, *d_sq_pq = nullptr, *d_sq_fv = nullptr, *d_sq_vf = nullptr, *d_sq_nw = nullptr;
     double *d_sq_S = nullptr;
@@ -194,6 +196,9 @@ VarArgs var_args(flbp_engine *e) {
 
 SeqArgs seq_args(flbp_engine *e) {
     SeqArgs a;
+    a.irec = reinterpret_cast<const uint4 *>(e->d_sq_irec);
+    a.tvar = e->d_sq_tvar;
+    a.bo = reinterpret_cast<const uint2 *>(e->d_sq_bo);
     a.foff = e->d_sq_foff;
     a.var = e->d_sq_var;
     a.kind = e->d_sq_kind;
@@ -218,14 +223,33 @@ unsigned int seq_belief_grid(const flbp_engine *e) {
 // Kernels of one sequential sweep: `which` bit 0 the batches (with the
 // sweep's opening kernel), bit 1 the beliefs of the tolerance / low-pass loops.
 long long seq_sweep_launches(const flbp_engine *e, int mode, int which) {
-    return ((which & 1) ? 1 + 2LL * e->SQ.n_batches : 0) + (((which & 2) && (mode == 1 || mode == 2)) ? 1 : 0);
+    const long long batches = e->seq_cluster ? 1 : 1 + 2LL * e->SQ.n_batches;
+    return ((which & 1) ? batches : 0) + (((which & 2) && (mode == 1 || mode == 2)) ? 1 : 0);
+}
+
+// One cluster per sweep where batches hold a few factors on average (TOPO's
+// hold two or three: a batch then takes 3.3 us on the cluster against 3.9 us
+// as two launches on a B200), else two launches per batch over the whole GPU
+// (SEQFIX's batches of a few hundred factors: 5.4 against 6.2 us).
+bool choose_seq_cluster(const flbp_engine *e) {
+    if (e->seq_kernel == 1) return false;
+    if (e->seq_kernel == 2) return true;
+    const SeqLayout &Q = e->SQ;
+    return Q.n_batches > 0 && Q.items.size() <= (size_t)Q.n_batches * 32;
 }
 
 template <typename T>
 void launch_seq_sweep(flbp_engine *e, int mode, int which) {
     const SeqArgs a = seq_args(e);
     const SeqLayout &Q = e->SQ;
-    if (which & 1) {
+    if ((which & 1) && e->seq_cluster) {
+        if (e->damping != 0.0)
+            seq_sweep_cluster_kernel<T, true><<<kSeqClusterCtas, 32 * kSeqClusterWarps, 0, e->stream>>>(
+                a, Q.n_batches, (T)e->damping, e->d_ctl);
+        else
+            seq_sweep_cluster_kernel<T, false><<<kSeqClusterCtas, 32 * kSeqClusterWarps, 0, e->stream>>>(
+                a, Q.n_batches, (T)0, e->d_ctl);
+    } else if (which & 1) {
         seq_begin_kernel<<<1, 1, 0, e->stream>>>(e->d_ctl);
         for (uint32_t b = 0; b < Q.n_batches; b++) {
             const uint32_t i0 = Q.ioff[b], i1 = Q.ioff[b + 1], t0 = Q.toff[b], t1 = Q.toff[b + 1];
@@ -1952,10 +1976,13 @@ namespace {
 
 void free_seq(flbp_engine *e) {
     void *bufs[] = {e->d_sq_foff, e->d_sq_var, e->d_sq_items, e->d_sq_tgt, e->d_sq_iota, e->d_sq_kind, e->d_sq_cst,
-                    e->d_sq_pq,   e->d_sq_fv,  e->d_sq_vf,    e->d_sq_nw,  e->d_sq_S,    e->d_sq_cnt};
+                    e->d_sq_pq,   e->d_sq_fv,  e->d_sq_vf,    e->d_sq_nw,  e->d_sq_S,    e->d_sq_cnt, e->d_sq_irec,
+                    e->d_sq_tvar, e->d_sq_bo};
     for (void *b : bufs)
         if (b) cudaFree(b);
     e->d_sq_foff = e->d_sq_var = e->d_sq_items = e->d_sq_tgt = e->d_sq_iota = nullptr;
+    e->d_sq_irec = e->d_sq_tvar = e->d_sq_bo = nullptr;
+    e->seq_cluster = false;
     e->d_sq_kind = nullptr;
     e->d_sq_cst = e->d_sq_pq = e->d_sq_fv = e->d_sq_vf = e->d_sq_nw = nullptr;
     e->d_sq_S = nullptr;
@@ -2031,15 +2058,34 @@ int flbp_set_update_seq(flbp_engine *e, const int64_t *seq, int64_t n) {
             (rc = dalloc(e, &e->d_sq_items, S.items.size())) || (rc = upload(e, e->d_sq_items, S.items)) ||
             (rc = dalloc(e, &e->d_sq_tgt, S.tgt.size())) || (rc = upload(e, e->d_sq_tgt, S.tgt)) ||
             (rc = dalloc(e, &e->d_sq_iota, ne)) || (rc = upload(e, e->d_sq_iota, iota)) ||
+            (rc = dalloc(e, &e->d_sq_irec, S.irec.size())) || (rc = upload(e, e->d_sq_irec, S.irec)) ||
+            (rc = dalloc(e, &e->d_sq_tvar, S.tvar.size())) || (rc = upload(e, e->d_sq_tvar, S.tvar)) ||
+            (rc = dalloc(e, &e->d_sq_bo, S.bo.size())) || (rc = upload(e, e->d_sq_bo, S.bo)) ||
             (rc = dalloc(e, &e->d_sq_S, nv)) || (rc = dalloc(e, &e->d_sq_cnt, nv)) ||
             (rc = (e->prec == 64 ? upload_seq_consts<double>(e) : upload_seq_consts<float>(e)))) {
             free_seq(e);
             return rc;
         }
         e->seq = true;
+        e->seq_cluster = choose_seq_cluster(e);
     }
     if ((rc = flbp_init(e))) return rc;
     FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    return FLBP_OK;
+}
+
+int flbp_set_seq_kernel(flbp_engine *e, int32_t kind) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    if (kind < 0 || kind > 2) {
+        set_error("kind must be 0 (choose), 1 (two launches per batch) or 2 (one cluster per sweep)");
+        return FLBP_ERR_INVALID;
+    }
+    FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    for (auto &kv : e->graphs) cudaGraphExecDestroy(kv.second);
+    e->graphs.clear();
+    e->seq_kernel = kind;
+    e->seq_cluster = e->seq && choose_seq_cluster(e);
     return FLBP_OK;
 }
 

@@ -198,6 +198,9 @@ struct SeqLayout {
     hvec<double> pq;       // per reference factor: p, q
     hvec<uint32_t> ioff, items;  // per batch: its factors
     hvec<uint32_t> toff, tgt;    // per batch: its target device slots
+    hvec<uint32_t> irec;         // per item: first device slot, degree, kind, factor (4 words)
+    hvec<uint32_t> tvar;         // per target: its internal variable
+    hvec<uint32_t> bo;           // per batch and the end: first item, first target (2 words)
 };
 
 // Conflict-free batches of an update sequence (every factor-major slot once):

@@ -236,6 +236,21 @@ int build_seq_layout(const flbp_graph_desc &g, const HostLayout &L, const int64_
         }
         S.ioff[b + 1] = (uint32_t)S.items.size();
     }
+    S.irec.resize(4 * S.items.size());
+    for (size_t it = 0; it < S.items.size(); it++) {
+        const uint32_t I = S.items[it];
+        S.irec[4 * it] = S.foff[I];
+        S.irec[4 * it + 1] = S.foff[I + 1] - S.foff[I];
+        S.irec[4 * it + 2] = S.kind[I];
+        S.irec[4 * it + 3] = I;
+    }
+    S.tvar.resize((size_t)E);
+    for (int64_t k = 0; k < E; k++) S.tvar[k] = S.var[S.tgt[k]];
+    S.bo.resize(2 * ((size_t)nb + 1));
+    for (uint32_t b = 0; b <= nb; b++) {
+        S.bo[2 * b] = S.ioff[b];
+        S.bo[2 * b + 1] = S.toff[b];
+    }
     S.max_items = S.max_tgt = 0;
     for (uint32_t b = 0; b < nb; b++) {
         S.max_items = std::max(S.max_items, S.ioff[b + 1] - S.ioff[b]);

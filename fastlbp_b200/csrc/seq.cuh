@@ -1,6 +1,6 @@
 // Kernels of the sequential schedules (updates=SEQFIX / TOPO).
 //
-// A sweep runs the schedule's batches in order, each as two launches:
+// A sweep runs the schedule's batches in order, each in two phases:
 //   seq_factor_kernel  one warp per factor of the batch: the v->f message of
 //                      every slot from the current variable totals (the
 //                      reference's calcMessageVFKernel, causal_bp_seq.cu:
@@ -15,6 +15,14 @@
 // outputs to slots that are not targets of the batch are staged but not
 // applied. seq_begin_kernel opens a sweep; seq_belief_kernel closes it with
 // the beliefs, residuals and stop rules of the run loops.
+//
+// seq_sweep_cluster_kernel runs all batches of a sweep in one launch on one
+// cluster of kSeqClusterCtas blocks: the two phases of a batch are
+// separated by cluster barriers (release / acquire) instead of kernel
+// boundaries. Every thread passes exactly two barriers per batch and none
+// leaves early, so the barriers cannot wait for a thread that is gone. State
+// that other blocks write (totals, counts, messages, staged messages) is
+// read with ld.global.cg, from L2, never from a stale L1 line.
 #pragma once
 
 #include "kernels.cuh"
@@ -22,6 +30,9 @@
 namespace flbp {
 
 struct SeqArgs {
+    const uint4 *irec;      // per item: first device slot, degree, kind, factor
+    const uint32_t *tvar;   // per target: its variable
+    const uint2 *bo;        // per batch: (first item, first target), n_batches + 1
     const uint32_t *foff;   // per factor: first device slot (F + 1)
     const uint32_t *var;    // per device slot: internal variable
     const uint8_t *kind;    // per factor
@@ -37,7 +48,9 @@ struct SeqArgs {
     int2 *cnt;              // per internal variable: (+inf count, -inf count)
 };
 
-constexpr int kSeqWarps = 8;  // warps per block of the factor kernel
+constexpr int kSeqWarps = 8;           // warps per block of the factor kernel
+constexpr int kSeqClusterCtas = 8;     // blocks of the one-cluster sweep kernel (portable cluster size)
+constexpr int kSeqClusterWarps = 16;   // warps per block of that kernel (FP64 item code: ~92 registers)
 
 static __global__ void seq_begin_kernel(Ctl *ctl) {
     if (*(volatile int *)&ctl->done) return;
@@ -82,16 +95,14 @@ __device__ void seq_factor_huge(const T *vb, uint32_t nbody, uint8_t kind, T p, 
     }
 }
 
-// Items [i0, i1) of the batches' item list: one warp per factor.
+// Item `it` of the batches' item list, one whole warp: every v->f message of
+// the factor from the current totals, then all its outputs into the staging
+// array.
 template <typename T>
-__global__ void __launch_bounds__(32 * kSeqWarps) seq_factor_kernel(SeqArgs a, uint32_t i0, uint32_t i1, Ctl *ctl) {
-    if (*(volatile int *)&ctl->done) return;
-    const int lane = threadIdx.x & 31;
-    const uint32_t it = i0 + blockIdx.x * kSeqWarps + (threadIdx.x >> 5);
-    if (it >= i1) return;  // whole warps leave together
-    const uint32_t f = a.items[it];
-    const uint32_t s0 = a.foff[f], deg = a.foff[f + 1] - s0;
-    const uint8_t kind = a.kind[f];
+__device__ __forceinline__ void seq_factor_item(const SeqArgs &a, uint32_t it, int lane) {
+    const uint4 r = a.irec[it];  // first slot, degree, kind, factor
+    const uint32_t s0 = r.x, deg = r.y, f = r.w;
+    const uint8_t kind = (uint8_t)r.z;
     T *nw = reinterpret_cast<T *>(a.nw);
     const T c = reinterpret_cast<const T *>(a.cst)[f];
     if (kind & kSeqConst) {  // singleton, or an AND/OR factor reduced to its head
@@ -102,8 +113,9 @@ __global__ void __launch_bounds__(32 * kSeqWarps) seq_factor_kernel(SeqArgs a, u
     T *vf = reinterpret_cast<T *>(a.vf);
     for (uint32_t k = lane; k < deg; k += 32) {
         const uint32_t s = s0 + k, v = a.var[s];
-        const int2 n = a.cnt[v];
-        vf[s] = excl_msg<T>(a.S[v], n.x, n.y, fv[s]);
+        const T x = __ldcg(fv + s);
+        const int2 n = __ldcg(a.cnt + v);
+        vf[s] = excl_msg<T>(__ldcg(a.S + v), n.x, n.y, x);
     }
     __syncwarp();  // orders the v->f stores before the other lanes' loads
     const T *pq = reinterpret_cast<const T *>(a.pq);
@@ -113,20 +125,18 @@ __global__ void __launch_bounds__(32 * kSeqWarps) seq_factor_kernel(SeqArgs a, u
     if ((kind & HEAD_MASK) != HEAD_FREE && lane == 0) nw[s0] = c;  // a clamped head's constant
 }
 
-// Targets [t0, t1) of the batches' target list.
+// Target k of the batches' target list: its staged message replaces the old
+// one in its variable's total and counts.
 template <typename T, bool DAMP>
-__global__ void seq_apply_kernel(SeqArgs a, uint32_t t0, uint32_t t1, T d, Ctl *ctl) {
-    if (*(volatile int *)&ctl->done) return;
-    const uint32_t k = t0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= t1) return;
-    const uint32_t s = a.tgt[k], v = a.var[s];
+__device__ __forceinline__ void seq_apply_one(const SeqArgs &a, uint32_t k, T d) {
+    const uint32_t s = a.tgt[k], v = a.tvar[k];
     T *fv = reinterpret_cast<T *>(a.fv);
-    const T old = fv[s];
-    T x = reinterpret_cast<const T *>(a.nw)[s];
+    const T old = __ldcg(fv + s);
+    T x = __ldcg(reinterpret_cast<const T *>(a.nw) + s);
+    double S = __ldcg(a.S + v);
+    int2 n = __ldcg(a.cnt + v);
     if (DAMP) x = damp_mix<T>(x, old, d);
     const T inf = Num<T>::inf();
-    double S = a.S[v];
-    int2 n = a.cnt[v];
     if (old == inf) n.x--;
     else if (old == -inf) n.y--;
     else S -= (double)old;
@@ -136,6 +146,57 @@ __global__ void seq_apply_kernel(SeqArgs a, uint32_t t0, uint32_t t1, T d, Ctl *
     a.S[v] = S;
     a.cnt[v] = n;
     fv[s] = x;
+}
+
+// Items [i0, i1) of the batches' item list: one warp per factor.
+template <typename T>
+__global__ void __launch_bounds__(32 * kSeqWarps) seq_factor_kernel(SeqArgs a, uint32_t i0, uint32_t i1, Ctl *ctl) {
+    if (*(volatile int *)&ctl->done) return;
+    const uint32_t it = i0 + blockIdx.x * kSeqWarps + (threadIdx.x >> 5);
+    if (it >= i1) return;  // whole warps leave together
+    seq_factor_item<T>(a, it, threadIdx.x & 31);
+}
+
+// Targets [t0, t1) of the batches' target list.
+template <typename T, bool DAMP>
+__global__ void seq_apply_kernel(SeqArgs a, uint32_t t0, uint32_t t1, T d, Ctl *ctl) {
+    if (*(volatile int *)&ctl->done) return;
+    const uint32_t k = t0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= t1) return;
+    seq_apply_one<T, DAMP>(a, k, d);
+}
+
+__device__ __forceinline__ void cluster_barrier() {
+    asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+}
+
+// One whole sweep (its opening included) on one cluster; grid = one cluster.
+template <typename T, bool DAMP>
+__global__ void __cluster_dims__(kSeqClusterCtas, 1, 1) __launch_bounds__(32 * kSeqClusterWarps, 1)
+    seq_sweep_cluster_kernel(SeqArgs a, uint32_t n_batches, T d, Ctl *ctl) {
+    if (*(volatile int *)&ctl->done) return;  // the same for every thread: only earlier launches write it
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        unsigned long long now;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+        if (ctl->run_sweeps == 0) ctl->t_start_ns = now;
+        ctl->t += 1;
+        ctl->run_sweeps += 1;
+        ctl->maxdiff_bits = 0ull;
+        ctl->nonconv = 0ull;
+        ctl->arrive = 0u;
+    }
+    const int lane = threadIdx.x & 31;
+    const uint32_t gw = blockIdx.x * kSeqClusterWarps + (threadIdx.x >> 5), nwarps = gridDim.x * kSeqClusterWarps;
+    const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+    uint2 lo = a.bo[0];
+    for (uint32_t b = 0; b < n_batches; b++) {
+        const uint2 hi = a.bo[b + 1];
+        for (uint32_t it = lo.x + gw; it < hi.x; it += nwarps) seq_factor_item<T>(a, it, lane);
+        cluster_barrier();
+        for (uint32_t k = lo.y + gt; k < hi.y; k += nthreads) seq_apply_one<T, DAMP>(a, k, d);
+        cluster_barrier();
+        lo = hi;
+    }
 }
 
 // Beliefs of every internal variable from its total and counts, with the

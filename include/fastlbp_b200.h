@@ -381,6 +381,12 @@ int flbp_seq_batches(const flbp_graph_desc *graph, const int64_t *seq, int64_t n
  * (FLBP_ERR_STATE). */
 int flbp_set_update_seq(flbp_engine *eng, const int64_t *seq, int64_t n);
 
+/* How sequential sweeps are launched: 0 chooses (the default: one cluster per
+ * sweep when batches are small, else two launches per batch), 1 two kernel
+ * launches per batch over the whole GPU, 2 the whole sweep as one launch on
+ * one thread-block cluster. Results are the same. */
+int flbp_set_seq_kernel(flbp_engine *eng, int32_t kind);
+
 /* Whether the engine runs an installed sequence (1) or PARALL (0), and its
  * number of batches per sweep (1 for PARALL). Either pointer may be NULL. */
 int flbp_update_info(flbp_engine *eng, int32_t *sequential, int64_t *n_batches);

@@ -35,18 +35,21 @@ def _clamped_cfg0(seed):
     return _pair(fl, cl)
 
 
+@pytest.mark.parametrize("kernel", [1, 2])
 @pytest.mark.parametrize("prec", [64, 32])
 @pytest.mark.parametrize("updates,sweeps", [("SEQFIX", 60), ("TOPO", 20)])
-def test_fixed_sweeps(updates, sweeps, prec):
+def test_fixed_sweeps(updates, sweeps, prec, kernel):
+    """kernel 1: two launches per batch; 2: the sweep on one cluster."""
     g, og = _clamped_cfg0(0)
     bp, nb = _oracle(og, updates)
     bp.run_fixed(1e-6, sweeps, 1)
     eng = Engine.from_graph(g, precision=prec, updates=updates)
     assert eng.update_info() == (True, nb)
+    eng.set_seq_kernel(kernel)
     eng.init()
     info = eng.run_fixed(sweeps)
     assert info["sweeps"] == sweeps
-    assert info["launches"] == sweeps * (1 + 2 * nb) + 1
+    assert info["launches"] == sweeps * (1 + 2 * nb if kernel == 1 else 1) + 1
     assert np.max(np.abs(eng.beliefs() - bp.beliefs())) <= TOL[prec]
     assert np.max(np.abs(eng.lowpass() - bp.lowpass())) <= TOL[prec]
 
@@ -82,16 +85,22 @@ def test_lowpass_run():
 @pytest.mark.parametrize("damping", [0.0, 0.15])
 def test_large_items(prec, damping):
     """Factors with bodies of 17 to 1000 slots (the warp forms on both sides
-    of 256 body slots), a variable in 2100 factors, clamped heads."""
+    of 256 body slots), a variable in 2100 factors, clamped heads; both
+    launch forms give the same bits."""
     fl = _large_item_graph(11)
     clamps = {1200 + 3: 1, 1200 + 7: 0, 5: 1}
     g, og = _pair(fl, clamps)
     bp, _ = _oracle(og, "SEQFIX", damping)
     bp.run_fixed(1e-6, 15, 1)
     eng = Engine.from_graph(g, precision=prec, damping=damping, updates="SEQFIX")
-    eng.init()
-    eng.run_fixed(15)
-    assert np.max(np.abs(eng.beliefs() - bp.beliefs())) <= TOL[prec]
+    out = []
+    for kernel in (1, 2):
+        eng.set_seq_kernel(kernel)
+        eng.init()
+        eng.run_fixed(15)
+        out.append(eng.beliefs())
+    assert np.max(np.abs(out[0] - bp.beliefs())) <= TOL[prec]
+    assert np.array_equal(out[0], out[1])
 
 
 def test_trees_exact_marginals():

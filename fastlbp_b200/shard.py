@@ -6,6 +6,13 @@ Graphs are dealt largest first to the rank with the least work so far
 (longest-processing-time order), which keeps the slowest rank within one
 graph of the mean. The partition is a pure function of the weights, so every
 rank computes the same one without communicating.
+
+When graphs share parameters (the same analysis rules instantiated in many
+graphs, each with its own evidence and labels), learning needs one exchange
+per step: every rank sums the adjoint's per-factor gradients of its graphs
+into the shared rules, and one all-reduce sums them over the ranks
+(shared_gradient); the updated rule probabilities go back to every factor
+that instantiates them (expand_shared).
 """
 
 from __future__ import annotations
@@ -39,4 +46,36 @@ def gather_results(local: dict, world: int) -> dict:
     out = {}
     for p in parts:
         out.update(p)
+    return out
+
+
+def shared_gradient(grad_p, rule_of_factor, n_rules: int, world: int = 1):
+    """dL/d(shared rule probabilities), summed over every rank's graphs.
+
+    grad_p: per-factor dL/dp of this rank's graphs (float64 tensor, e.g. the
+    adjoint's output for a BatchEngine); rule_of_factor: the rule each
+    factor instantiates, -1 for a factor with a parameter of its own (int64
+    tensor on the same device). Returns a float64 tensor of n_rules entries,
+    the same on every rank: one all-reduce (sum) over the process group, on
+    NCCL for CUDA tensors and gloo for CPU ones."""
+    import torch
+
+    if grad_p.shape != rule_of_factor.shape:
+        raise ValueError("grad_p and rule_of_factor must have one entry per factor")
+    g = torch.zeros(int(n_rules), dtype=torch.float64, device=grad_p.device)
+    m = rule_of_factor >= 0
+    g.index_add_(0, rule_of_factor[m], grad_p[m].to(torch.float64))
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(g, op=dist.ReduceOp.SUM)
+    return g
+
+
+def expand_shared(p_rules, rule_of_factor, p_factor):
+    """Per-factor probabilities after a learning step: the shared rule's value
+    where a factor instantiates one, the factor's own elsewhere."""
+    out = p_factor.clone()
+    m = rule_of_factor >= 0
+    out[m] = p_rules[rule_of_factor[m]].to(out.dtype)
     return out

@@ -225,3 +225,51 @@ def test_adjoint_on_clamped_graph_matches_central_differences():
         pm[I] -= eps
         fd = (loss(pp) - loss(pm)) / (2 * eps)
         assert abs(fd - gp[I]) <= 1e-4 * max(abs(gp[I]), 1e-3 * scale), (I, fd, gp[I])
+
+
+def test_shared_rule_gradient_matches_central_differences():
+    """Three copies of one graph, each with its own labels, share every
+    factor's p (the same rules analysed under different evidence). The
+    shared gradient - the adjoint's per-factor gradients of a BatchEngine
+    summed into their rules (fastlbp_b200.shard.shared_gradient, the
+    reduction a multi-GPU learning step all-reduces) - against central
+    differences of the summed loss, each rule moved in every copy at once
+    (expand_shared)."""
+    from fastlbp_b200.shard import expand_shared, shared_gradient
+
+    a = _graph("bingo")
+    T, K, eps = 20, 4, 1e-6
+    copies = 3
+    labels = [_labels(a, seed=20 + c) for c in range(copies)]
+    be = BatchEngine([a] * copies, precision=64)
+    F0 = len(a["factor_p"])
+    rule_of = torch.as_tensor(np.tile(np.arange(F0), copies))
+    p_rules = torch.as_tensor(np.asarray(a["factor_p"], np.float64))
+    q_all = np.tile(np.asarray(a["factor_q"], np.float64), copies)
+    base = torch.as_tensor(np.tile(np.asarray(a["factor_p"], np.float64), copies))
+
+    def loss_and_grad(pr):
+        be.set_factor_probs(expand_shared(pr, rule_of, base).numpy(), q_all)
+        b = be.adjoint_forward(T, K)
+        total, g = 0.0, np.zeros(be.n_vars)
+        for c, (idx, y) in enumerate(labels):
+            j = be.var_off[c] + idx
+            total += float(_bce(torch.as_tensor(b), torch.as_tensor(j), torch.as_tensor(y)))
+            g[j] += -y / b[j] + (1 - y) / (1 - b[j])
+        return total, g
+
+    _, g = loss_and_grad(p_rules)
+    gp, _ = be.adjoint_backward(g, want_q=False)
+    shared = shared_gradient(torch.as_tensor(gp), rule_of, F0).numpy()
+    per_copy = gp.reshape(copies, F0)
+    assert np.max(np.abs(shared - per_copy.sum(0))) <= 1e-12 * np.max(np.abs(shared))
+    rng = np.random.default_rng(7)
+    p0 = p_rules.numpy()
+    cand = np.nonzero((p0 > 1e-3) & (p0 < 1 - 1e-3))[0]
+    scale = np.max(np.abs(shared))
+    for r in rng.choice(cand, size=min(25, cand.size), replace=False):
+        pp, pm = p_rules.clone(), p_rules.clone()
+        pp[r] += eps
+        pm[r] -= eps
+        fd = (loss_and_grad(pp)[0] - loss_and_grad(pm)[0]) / (2 * eps)
+        assert abs(fd - shared[r]) <= 1e-4 * max(abs(shared[r]), 1e-3 * scale), (r, fd, shared[r])

@@ -12,7 +12,7 @@ import pytest
 import torch.multiprocessing as mp
 
 from fastlbp_b200 import workloads
-from fastlbp_b200.shard import gather_results, partition
+from fastlbp_b200.shard import expand_shared, gather_results, partition, shared_gradient
 
 N_GRAPHS = 10
 
@@ -86,3 +86,72 @@ def test_two_gloo_ranks_match_one_process(tmp_path):
     got = np.load(out, allow_pickle=True)
     for i in range(N_GRAPHS):
         assert np.array_equal(np.array(got[i]), np.array(_solve(i)))
+
+
+N_RULES = 40
+
+
+def _grad_of(i):
+    """A graph's per-factor gradient and rule map (seeded stand-ins for the
+    adjoint's output: this test covers the reduction, not the gradient)."""
+    rng = np.random.default_rng(100 + i)
+    nf = 50 + 7 * i
+    rules = rng.integers(-1, N_RULES, nf)  # -1: a parameter of the factor's own
+    return rng.standard_normal(nf), rules
+
+
+def _grad_rank(rank, world, port, out_path):
+    import torch
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    mine = partition([50 + 7 * i for i in range(N_GRAPHS)], world)[rank]
+    gp = torch.tensor(np.concatenate([_grad_of(i)[0] for i in mine]))
+    rf = torch.tensor(np.concatenate([_grad_of(i)[1] for i in mine]))
+    g = shared_gradient(gp, rf, N_RULES, world)
+    allg = [torch.zeros(N_RULES, dtype=torch.float64) for _ in range(world)]
+    dist.all_gather(allg, g)
+    if rank == 0:
+        np.save(out_path, torch.stack(allg).numpy())
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_shared_rule_gradient_allreduce_two_gloo_ranks(tmp_path):
+    """Two ranks, each with its share of the graphs, end with the same shared
+    gradient, equal to summing every graph's gradient in one process."""
+    import torch
+
+    out = str(tmp_path / "g.npy")
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_grad_rank, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=240)
+        if p.is_alive():
+            p.kill()
+            pytest.fail("gloo rank did not finish")
+        assert p.exitcode == 0
+    got = np.load(out)
+    want = np.zeros(N_RULES)
+    for i in range(N_GRAPHS):
+        gp, rf = _grad_of(i)
+        np.add.at(want, rf[rf >= 0], gp[rf >= 0])
+    assert np.array_equal(got[0], got[1])
+    assert np.max(np.abs(got[0] - want)) <= 1e-12 * max(1.0, np.max(np.abs(want)))
+    one = shared_gradient(torch.tensor(np.concatenate([_grad_of(i)[0] for i in range(N_GRAPHS)])),
+                          torch.tensor(np.concatenate([_grad_of(i)[1] for i in range(N_GRAPHS)])), N_RULES)
+    assert np.max(np.abs(one.numpy() - want)) <= 1e-12 * max(1.0, np.max(np.abs(want)))
+
+
+def test_expand_shared():
+    import torch
+
+    rf = torch.tensor([2, -1, 0, 2, -1])
+    p = expand_shared(torch.tensor([0.1, 0.2, 0.3], dtype=torch.float64), rf,
+                      torch.tensor([0.9, 0.8, 0.7, 0.6, 0.5], dtype=torch.float64))
+    assert p.tolist() == [0.3, 0.8, 0.1, 0.3, 0.5]

@@ -481,8 +481,9 @@ def run_seq(args, rank, world, local):
         for prec in (32, 64):
             e = Engine(a, precision=prec, updates=updates)
             rec["batches"] = e.update_info()[1]
-            # 0: the engine's choice, 1: two launches per batch, 2: one cluster per sweep
-            for kernel, tag in ((0, ""), (1, "_launches"), (2, "_cluster")):
+            # 0: the engine's choice, 1: two launches per batch, 2: one cluster per sweep,
+            # 3: two launches per batch with programmatic dependent launch
+            for kernel, tag in ((0, ""), (1, "_launches"), (2, "_cluster"), (3, "_pdl")):
                 e.set_seq_kernel(kernel)
                 ts = []
                 for rep in range(max(1, args.warmup) + 2):

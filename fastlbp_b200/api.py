@@ -289,7 +289,8 @@ class Engine:
 
     def set_seq_kernel(self, kind: int) -> None:
         """Sequential sweeps: 0 choose, 1 two launches per batch, 2 one cluster
-        per sweep (flbp_set_seq_kernel)."""
+        per sweep, 3 as 1 with programmatic dependent launch
+        (flbp_set_seq_kernel)."""
         check(lib().flbp_set_seq_kernel(self._h, int(kind)))
 
     def update_info(self) -> Tuple[bool, int]:

@@ -95,7 +95,8 @@ struct flbp_engine {
     SeqLayout SQ;
     uint32_t *d_sq_foff = nullptr, *d_sq_var = nullptr, *d_sq_items = nullptr, *d_sq_tgt = nullptr;
     uint32_t *d_sq_iota = nullptr, *d_sq_irec = nullptr, *d_sq_tvar = nullptr, *d_sq_bo = nullptr;
-    int seq_kernel = 0;        // 0: choose, 1: two launches per batch, 2: one cluster per sweep
+    int seq_kernel = 0;        // 0: choose, 1: two launches per batch, 2: one cluster per sweep, 3: as 1 with
+                               // programmatic dependent launch
     bool seq_cluster = false;  // the sweep runs as one cluster kernel
     uint8_t *d_sq_kind = nullptr;
     void *d_sq_cst = nullptr, *d_sq_pq = nullptr, *d_sq_fv = nullptr, *d_sq_vf = nullptr, *d_sq_nw = nullptr;
@@ -232,16 +233,33 @@ long long seq_sweep_launches(const flbp_engine *e, int mode, int which) {
 // as two launches on a B200), else two launches per batch over the whole GPU
 // (SEQFIX's batches of a few hundred factors: 5.4 against 6.2 us).
 bool choose_seq_cluster(const flbp_engine *e) {
-    if (e->seq_kernel == 1) return false;
+    if (e->seq_kernel == 1 || e->seq_kernel == 3) return false;
     if (e->seq_kernel == 2) return true;
     const SeqLayout &Q = e->SQ;
     return Q.n_batches > 0 && Q.items.size() <= (size_t)Q.n_batches * 32;
+}
+
+// A kernel launch on the engine's stream, with programmatic dependent launch
+// when asked for (the kernels wait for their predecessor in pdl_enter).
+template <typename... K, typename... A>
+void launch_seq(flbp_engine *e, bool pdl, void (*kern)(K...), unsigned grid, unsigned block, A... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.stream = e->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kern, args...);
 }
 
 template <typename T>
 void launch_seq_sweep(flbp_engine *e, int mode, int which) {
     const SeqArgs a = seq_args(e);
     const SeqLayout &Q = e->SQ;
+    const bool pdl = (e->seq_kernel == 3);
     if ((which & 1) && e->seq_cluster) {
         if (e->damping != 0.0)
             seq_sweep_cluster_kernel<T, true><<<kSeqClusterCtas, 32 * kSeqClusterWarps, 0, e->stream>>>(
@@ -250,26 +268,27 @@ void launch_seq_sweep(flbp_engine *e, int mode, int which) {
             seq_sweep_cluster_kernel<T, false><<<kSeqClusterCtas, 32 * kSeqClusterWarps, 0, e->stream>>>(
                 a, Q.n_batches, (T)0, e->d_ctl);
     } else if (which & 1) {
-        seq_begin_kernel<<<1, 1, 0, e->stream>>>(e->d_ctl);
+        launch_seq(e, pdl, seq_begin_kernel, 1, 1, e->d_ctl);
+        const T d = (T)e->damping;
         for (uint32_t b = 0; b < Q.n_batches; b++) {
             const uint32_t i0 = Q.ioff[b], i1 = Q.ioff[b + 1], t0 = Q.toff[b], t1 = Q.toff[b + 1];
-            seq_factor_kernel<T><<<(i1 - i0 + kSeqWarps - 1) / kSeqWarps, 32 * kSeqWarps, 0, e->stream>>>(a, i0, i1,
-                                                                                                      e->d_ctl);
+            launch_seq(e, pdl, seq_factor_kernel<T>, (i1 - i0 + kSeqWarps - 1) / kSeqWarps, 32 * kSeqWarps, a, i0, i1,
+                       e->d_ctl);
             if (e->damping != 0.0)
-                seq_apply_kernel<T, true><<<(t1 - t0 + 255) / 256, 256, 0, e->stream>>>(a, t0, t1, (T)e->damping,
-                                                                                       e->d_ctl);
+                launch_seq(e, pdl, seq_apply_kernel<T, true>, (t1 - t0 + 255) / 256, 256, a, t0, t1, d, e->d_ctl);
             else
-                seq_apply_kernel<T, false><<<(t1 - t0 + 255) / 256, 256, 0, e->stream>>>(a, t0, t1, (T)0, e->d_ctl);
+                launch_seq(e, pdl, seq_apply_kernel<T, false>, (t1 - t0 + 255) / 256, 256, a, t0, t1, d, e->d_ctl);
         }
     }
     if ((which & 2) && (mode == 1 || mode == 2)) {
         const VarArgs va = var_args(e);
+        const uint32_t V = (uint32_t)e->L.V;
         if (mode == 1)
-            seq_belief_kernel<1><<<seq_belief_grid(e), 256, 0, e->stream>>>(va, e->d_sq_S, e->d_sq_cnt,
-                                                                            (uint32_t)e->L.V, e->d_ctl);
+            launch_seq(e, pdl, seq_belief_kernel<1>, seq_belief_grid(e), 256, va, (const double *)e->d_sq_S,
+                       (const int2 *)e->d_sq_cnt, V, e->d_ctl);
         else
-            seq_belief_kernel<2><<<seq_belief_grid(e), 256, 0, e->stream>>>(va, e->d_sq_S, e->d_sq_cnt,
-                                                                            (uint32_t)e->L.V, e->d_ctl);
+            launch_seq(e, pdl, seq_belief_kernel<2>, seq_belief_grid(e), 256, va, (const double *)e->d_sq_S,
+                       (const int2 *)e->d_sq_cnt, V, e->d_ctl);
     }
 }
 
@@ -2077,8 +2096,9 @@ int flbp_set_update_seq(flbp_engine *e, const int64_t *seq, int64_t n) {
 int flbp_set_seq_kernel(flbp_engine *e, int32_t kind) {
     int rc = begin_call(e);
     if (rc) return rc;
-    if (kind < 0 || kind > 2) {
-        set_error("kind must be 0 (choose), 1 (two launches per batch) or 2 (one cluster per sweep)");
+    if (kind < 0 || kind > 3) {
+        set_error("kind must be 0 (choose), 1 (two launches per batch), 2 (one cluster per sweep) or 3 (two "
+                  "launches per batch with programmatic dependent launch)");
         return FLBP_ERR_INVALID;
     }
     FLBP_CUDA(cudaStreamSynchronize(e->stream));

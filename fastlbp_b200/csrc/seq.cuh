@@ -48,11 +48,21 @@ struct SeqArgs {
     int2 *cnt;              // per internal variable: (+inf count, -inf count)
 };
 
+// Programmatic dependent launch: a kernel lets the next one in the stream
+// launch at once and waits (in hardware) for the previous one to finish and
+// its memory to be visible before it reads any state. Both are no-ops for a
+// kernel launched without the attribute.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 constexpr int kSeqWarps = 8;           // warps per block of the factor kernel
 constexpr int kSeqClusterCtas = 8;     // blocks of the one-cluster sweep kernel (portable cluster size)
 constexpr int kSeqClusterWarps = 16;   // warps per block of that kernel (FP64 item code: ~92 registers)
 
 static __global__ void seq_begin_kernel(Ctl *ctl) {
+    pdl_enter();
     if (*(volatile int *)&ctl->done) return;
     unsigned long long now;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
@@ -151,6 +161,7 @@ __device__ __forceinline__ void seq_apply_one(const SeqArgs &a, uint32_t k, T d)
 // Items [i0, i1) of the batches' item list: one warp per factor.
 template <typename T>
 __global__ void __launch_bounds__(32 * kSeqWarps) seq_factor_kernel(SeqArgs a, uint32_t i0, uint32_t i1, Ctl *ctl) {
+    pdl_enter();
     if (*(volatile int *)&ctl->done) return;
     const uint32_t it = i0 + blockIdx.x * kSeqWarps + (threadIdx.x >> 5);
     if (it >= i1) return;  // whole warps leave together
@@ -160,6 +171,7 @@ __global__ void __launch_bounds__(32 * kSeqWarps) seq_factor_kernel(SeqArgs a, u
 // Targets [t0, t1) of the batches' target list.
 template <typename T, bool DAMP>
 __global__ void seq_apply_kernel(SeqArgs a, uint32_t t0, uint32_t t1, T d, Ctl *ctl) {
+    pdl_enter();
     if (*(volatile int *)&ctl->done) return;
     const uint32_t k = t0 + blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= t1) return;
@@ -206,6 +218,7 @@ template <int BMODE>
 __global__ void __launch_bounds__(256) seq_belief_kernel(VarArgs va, const double *S, const int2 *cnt, uint32_t V,
                                                          Ctl *ctl) {
     constexpr bool RESID = (BMODE == 1 || BMODE == 2);
+    pdl_enter();
     if (BMODE != 3 && *(volatile int *)&ctl->done) return;
     const double tol = ctl->tol;
     double dmax = 0.0;

@@ -384,7 +384,8 @@ int flbp_set_update_seq(flbp_engine *eng, const int64_t *seq, int64_t n);
 /* How sequential sweeps are launched: 0 chooses (the default: one cluster per
  * sweep when batches are small, else two launches per batch), 1 two kernel
  * launches per batch over the whole GPU, 2 the whole sweep as one launch on
- * one thread-block cluster. Results are the same. */
+ * one thread-block cluster, 3 as 1 with programmatic dependent launch.
+ * Results are the same. */
 int flbp_set_seq_kernel(flbp_engine *eng, int32_t kind);
 
 /* Whether the engine runs an installed sequence (1) or PARALL (0), and its

@@ -35,11 +35,12 @@ def _clamped_cfg0(seed):
     return _pair(fl, cl)
 
 
-@pytest.mark.parametrize("kernel", [1, 2])
+@pytest.mark.parametrize("kernel", [1, 2, 3])
 @pytest.mark.parametrize("prec", [64, 32])
 @pytest.mark.parametrize("updates,sweeps", [("SEQFIX", 60), ("TOPO", 20)])
 def test_fixed_sweeps(updates, sweeps, prec, kernel):
-    """kernel 1: two launches per batch; 2: the sweep on one cluster."""
+    """kernel 1: two launches per batch; 2: the sweep on one cluster; 3: as 1
+    with programmatic dependent launch."""
     g, og = _clamped_cfg0(0)
     bp, nb = _oracle(og, updates)
     bp.run_fixed(1e-6, sweeps, 1)
@@ -49,17 +50,19 @@ def test_fixed_sweeps(updates, sweeps, prec, kernel):
     eng.init()
     info = eng.run_fixed(sweeps)
     assert info["sweeps"] == sweeps
-    assert info["launches"] == sweeps * (1 + 2 * nb if kernel == 1 else 1) + 1
+    assert info["launches"] == sweeps * (1 if kernel == 2 else 1 + 2 * nb) + 1
     assert np.max(np.abs(eng.beliefs() - bp.beliefs())) <= TOL[prec]
     assert np.max(np.abs(eng.lowpass() - bp.lowpass())) <= TOL[prec]
 
 
 @pytest.mark.parametrize("prec", [64, 32])
-def test_tolerance_run(prec):
+@pytest.mark.parametrize("kernel", [0, 3])
+def test_tolerance_run(prec, kernel):
     g, og = _pair(workloads.config0(1))
     bp, _ = _oracle(og, "SEQFIX")
     bp.run(1e-6, 1000, 100.0)
     eng = Engine.from_graph(g, precision=prec, updates="SEQFIX")
+    eng.set_seq_kernel(kernel)
     eng.init()
     info = eng.run_tol(1e-6, 1000, 100.0)
     assert np.max(np.abs(eng.beliefs() - bp.beliefs())) <= TOL[prec]
@@ -94,13 +97,13 @@ def test_large_items(prec, damping):
     bp.run_fixed(1e-6, 15, 1)
     eng = Engine.from_graph(g, precision=prec, damping=damping, updates="SEQFIX")
     out = []
-    for kernel in (1, 2):
+    for kernel in (1, 2, 3):
         eng.set_seq_kernel(kernel)
         eng.init()
         eng.run_fixed(15)
         out.append(eng.beliefs())
     assert np.max(np.abs(out[0] - bp.beliefs())) <= TOL[prec]
-    assert np.array_equal(out[0], out[1])
+    assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
 
 
 def test_trees_exact_marginals():

@@ -1,4 +1,5 @@
-"""B200-native causal loopy belief propagation (drop-in for FastLBP's CausalBP PARALL path).
+"""B200-native causal loopy belief propagation (drop-in for FastLBP's CausalBP: the PARALL
+sweep, and the SEQFIX / TOPO schedules).
 
 The product is the shared library libfastlbp_b200.so (CUDA sm_100a kernels,
 the C ABI of include/fastlbp_b200.h and the libDAI-style C++ API of

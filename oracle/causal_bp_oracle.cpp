@@ -1,4 +1,5 @@
-// FP64 CPU restatement of FastLBP's causal loopy-BP PARALL path.
+// FP64 CPU restatement of FastLBP's causal loopy-BP path: the PARALL sweep and
+// the sequential SEQFIX / TOPO schedules.
 //
 // TEST INFRASTRUCTURE ONLY. This file is the correctness oracle: only the
 // tests, the smoke check and the CPU-baseline leg of the benchmark may load

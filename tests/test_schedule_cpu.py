@@ -81,3 +81,33 @@ def test_malformed_sequences_are_rejected():
     F = np.asarray(a["factor_offsets"]).size - 1
     with pytest.raises(FlbpError):
         update_seq(a, "SEQFIX", factor_order=np.zeros(F, np.int32))
+
+
+def test_schedule_entry_points_reject_bad_arguments():
+    import ctypes as C
+
+    from fastlbp_b200 import _native as N
+    from fastlbp_b200.api import _desc_from_arrays
+
+    g = CausalFactorGraph.from_factors(workloads.config0(0))
+    a = g.graph_arrays()
+    keep = []
+    desc = _desc_from_arrays(a, keep)
+    seq = np.zeros(desc.n_slots, np.int64)
+    assert N.lib().flbp_update_seq(C.byref(desc), 7, None, seq) == 1      # unknown kind
+    assert N.lib().flbp_update_seq(C.byref(desc), 1, None, seq) == 1      # SEQFIX without an order
+    order = np.zeros(4, np.int32)
+    assert N.lib().flbp_shuffled_factors(-1, 0, order) == 1
+    assert N.lib().flbp_shuffled_factors(4, 0, order) == 0
+    assert sorted(order.tolist()) == [0, 1, 2, 3]
+    nb = C.c_int64()
+    assert N.lib().flbp_seq_batches(None, seq, seq.size, None, C.byref(nb)) == 1
+    # a factor listing a variable twice is refused (the batching assumes distinct variables)
+    bad = dict(a)
+    sv = np.asarray(a["slot_var"]).copy()
+    off = np.asarray(a["factor_offsets"])
+    I = int(np.nonzero(np.diff(off) >= 2)[0][0])
+    sv[off[I] + 1] = sv[off[I]]
+    bad["slot_var"] = sv
+    with pytest.raises(FlbpError):
+        update_seq(bad, "TOPO")

@@ -111,3 +111,33 @@ def test_schedule_entry_points_reject_bad_arguments():
     bad["slot_var"] = sv
     with pytest.raises(FlbpError):
         update_seq(bad, "TOPO")
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_random_graphs_and_orders_match_oracle(seed):
+    """Seeded random graphs (sizes, fan-ins, back edges, clamps) and SEQFIX
+    seeds: the library's sequences and batches equal the oracle's."""
+    rng = np.random.default_rng(1000 + seed)
+    nt = int(rng.integers(20, 400))
+    fl = workloads.bingo_graph(nt, int(nt * rng.uniform(1.0, 2.0)), max(3, nt // 15),
+                               workloads.uniform_int(1, int(rng.integers(2, 7))),
+                               workloads.uniform_int(1, int(rng.integers(2, 12))), int(rng.integers(1 << 30)),
+                               n_layers=int(rng.integers(2, 9)), back_frac=float(rng.uniform(0.0, 0.3)),
+                               n_alarms=max(2, nt // 20))
+    g = CausalFactorGraph.from_factors(fl)
+    og = O.OracleGraph.from_factors(fl)
+    labels = g.var_labels()
+    cl = {int(l): int(rng.integers(0, 2)) for l in rng.choice(labels, size=min(5, labels.size), replace=False)}
+    g.clamp_labels(cl)
+    og.clamp_labels(cl)
+    g, og = g.rebuild(), og.rebuild()
+    a = g.graph_arrays()
+    for updates in ("SEQFIX", "TOPO"):
+        s = int(rng.integers(1 << 31))
+        bp = O.OracleBP(og)
+        nb = bp.set_schedule(updates, s)
+        oseq, obatch = bp.schedule()
+        seq = update_seq(a, updates, s)
+        assert np.array_equal(seq, oseq)
+        sb, n = seq_batches(a, seq)
+        assert n == nb and np.array_equal(sb, obatch)

@@ -65,7 +65,32 @@ def parse():
     ap.add_argument("--graphs", type=int, default=512, help="batch / adjoint workloads: number of graphs")
     ap.add_argument("--every", type=int, default=10, help="adjoint workload: checkpoint interval")
     ap.add_argument("--fd-params", type=int, default=1000, help="adjoint workload: parameters checked by differences")
+    ap.add_argument("--extras", default="batched,adjoint",
+                    help="sub-records of the default line: comma-separated subset of batched,adjoint, or none")
+    ap.add_argument("--plan-only", action="store_true",
+                    help="start the ranks, deal the batched graphs to them and print the plan; no GPU work")
     return ap.parse_args()
+
+
+def maybe_spawn(args):
+    """`--gpus N` with N > 1 and no launcher: run this script again under
+    torch.distributed.run with N processes on this node, one per GPU (rank r
+    on local device r). Under a launcher (WORLD_SIZE set) nothing happens."""
+    if args.gpus <= 1 or "WORLD_SIZE" in os.environ:
+        return
+    import socket
+
+    import torch
+
+    if not args.plan_only and torch.cuda.device_count() < args.gpus:
+        raise SystemExit("bench.py --gpus %d: only %d CUDA devices are visible" % (args.gpus, torch.cuda.device_count()))
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=%d" % args.gpus,
+           "--master-addr=127.0.0.1", "--master-port=%d" % port, os.path.abspath(__file__)] + sys.argv[1:]
+    sys.stdout.flush()
+    os.execv(sys.executable, cmd)
 
 
 def dist_setup(args):
@@ -75,11 +100,15 @@ def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if torch.cuda.is_available():
+    if world != args.gpus and not (world == 1 and args.gpus == 1):
+        raise SystemExit("bench.py: %d ranks were started for --gpus %d" % (world, args.gpus))
+    gpu = torch.cuda.is_available() and not args.plan_only
+    if gpu:
+        if torch.cuda.device_count() <= local:
+            raise SystemExit("bench.py: rank %d has no CUDA device %d" % (rank, local))
         torch.cuda.set_device(local)
     if world > 1 and not dist.is_initialized():
-        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
-                                timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group("nccl" if gpu else "gloo", timeout=datetime.timedelta(seconds=300))
     return rank, world, local
 
 
@@ -94,9 +123,25 @@ def allreduce_max(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def run_plan(args, rank, world):
+    """--plan-only: every rank takes its share of the batched-serving graphs
+    (dealt by size, as the batched sub-record and --workload batch do); rank
+    0 prints the plan with the ranks' shares gathered. No GPU work."""
+    from fastlbp_b200 import workloads
+    from fastlbp_b200.shard import gather_results, partition
+
+    sizes = workloads.config3_sizes(args.graphs)
+    mine = partition(sizes, world)[rank]
+    plan = gather_results({rank: {"graphs": mine, "tuples": int(sum(sizes[i] for i in mine))}}, world)
+    t = allreduce_max(float(len(mine)), world)
+    return {"plan": {str(r): plan[r] for r in sorted(plan)}, "n_gpus": world, "graphs": args.graphs,
+            "max_graphs_per_rank": int(t)}
 
 
 def graph_arrays(args):
@@ -680,9 +725,11 @@ def ncu_traffic():
     return out
 
 
-def cpu_baseline(fl, args):
-    """FP64 oracle (CPU restatement of the reference's PARALL math), OpenMP over
-    all host cores, timed on a bounded number of sweeps of the same graph."""
+def oracle_leg(fl, args, sweeps):
+    """The FP64 oracle (CPU restatement of the reference's PARALL arithmetic),
+    OpenMP over all host cores, on the same graph: init + `sweeps` sweeps with
+    the run's damping, then beliefs. Its time is the CPU baseline; its
+    beliefs are the parity reference of the engine's FP32 ones."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
@@ -692,37 +739,26 @@ def cpu_baseline(fl, args):
     bp.init()
     E = bp.E
     t0 = time.perf_counter()
-    bp.sweep()
-    one = time.perf_counter() - t0
-    n = max(1, int(args.cpu_seconds / max(one, 1e-3)))
-    t0 = time.perf_counter()
-    for _ in range(n):
-        bp.sweep()
+    bp.run_fixed(1e-9, sweeps, 1)
     dt = time.perf_counter() - t0
-    return {"value": 2.0 * E * n / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": "%d FP64 sweeps of the same graph (damping %g) by the oracle's OpenMP loop, %.1f s" % (n, args.damping, dt)}
+    base = {"value": 2.0 * E * sweeps / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "%d FP64 sweeps of the same graph (damping %g) from init by the oracle's OpenMP loop, %.1f s"
+                      % (sweeps, args.damping, dt)}
+    return base, bp.lowpass()
 
 
-def run_ours(args, rank, world, local):
+def sweep_timing(eng, args, stream, flush, world):
+    """Device time of `steps` steps (init + run_fixed(sweeps) + beliefs) with
+    CUDA events on the engine stream, L2 flushed before every step; max over
+    ranks. Returns (total ms, launches, clock record)."""
     import torch
-
-    from fastlbp_b200 import Engine
-
-    fl, arr = graph_arrays(args)
-    E = int(arr["factor_offsets"][-1])
-    F = int(arr["factor_offsets"].size - 1)
-    V = int(arr["n_vars"])
-    stream = torch.cuda.current_stream()
-    eng = Engine(arr, precision=args.precision, damping=args.damping, stream=stream.cuda_stream)
-    st = eng.stats()
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     for _ in range(args.warmup):
         eng.init()
         eng.run_fixed(args.sweeps)
     torch.cuda.synchronize()
     barrier(world)
-    clocks = Clocks(local)
+    clocks = Clocks(torch.cuda.current_device())
     clocks.start()
     times, launches = [], 0
     for _ in range(args.steps):
@@ -737,21 +773,47 @@ def run_ours(args, rank, world, local):
     torch.cuda.synchronize()
     barrier(world)
     clk = clocks.stop()
-    total_ms = sum(s.elapsed_time(e) for s, e in times)
-    total_ms = allreduce_max(total_ms, world)
-    updates = 2.0 * E * args.sweeps * args.steps * world
-    value = updates / (total_ms / 1e3)
+    total_ms = allreduce_max(sum(s.elapsed_time(e) for s, e in times), world)
+    return total_ms, launches, clk
 
-    # Per-pass durations: the same steps again with CUDA events around each pass.
+
+def pass_timing(eng, args, flush):
+    """Average device time of each pass (ms) with the sweeps replayed from
+    CUDA graphs: the engine's timing mode records CUDA events by event nodes
+    of the captured graph around every factor and variable pass."""
+    import torch
+
     eng.set_kernel_timing(True)
-    for _ in range(args.steps):
+    for _ in range(max(1, min(args.steps, 3))):
         flush.zero_()
         eng.init()
         eng.run_fixed(args.sweeps)
     torch.cuda.synchronize()
     f_ms, v_ms, f_n, v_n = eng.kernel_times()
     eng.set_kernel_timing(False)
-    per = {"factor_pass": f_ms / max(f_n, 1), "var_pass": v_ms / max(v_n, 1)}
+    return {"factor_pass": f_ms / max(f_n, 1), "var_pass": v_ms / max(v_n, 1)}
+
+
+def run_ours(args, rank, world, local):
+    import torch
+
+    from fastlbp_b200 import Engine
+
+    fl, arr = graph_arrays(args)
+    E = int(arr["factor_offsets"][-1])
+    F = int(arr["factor_offsets"].size - 1)
+    V = int(arr["n_vars"])
+    stream = torch.cuda.current_stream()
+    eng = Engine(arr, precision=args.precision, damping=args.damping, stream=stream.cuda_stream)
+    tuned = eng.autotune(args.sweeps) if hasattr(eng, "autotune") else None
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    total_ms, launches, clk = sweep_timing(eng, args, stream, flush, world)
+    updates = 2.0 * E * args.sweeps * args.steps * world
+    value = updates / (total_ms / 1e3)
+    b_engine = eng.beliefs()  # after init + the last step's sweeps
+
+    per = pass_timing(eng, args, flush)
     # Algorithmic bytes per launch (per-unit figures x units): factor pass
     # 12 B per edge slot + 16 B per factor; variable pass 12 B per slot + 12 B per variable.
     alg = {"factor_pass": 12.0 * E + 16.0 * F, "var_pass": 12.0 * E + 12.0 * V}
@@ -759,10 +821,14 @@ def run_ours(args, rank, world, local):
     peak, peak_kind = peaks()
     achieved = alg[dom] / (per[dom] / 1e3) / 1e9
     traffic = ncu_traffic().get(dom)
+    sweep_ms = total_ms / (args.steps * args.sweeps)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                 "traffic": traffic, "alg_bytes_per_launch": alg[dom],
-                "launch_ms": {k: round(v, 5) for k, v in per.items()}}
+                "launch_ms": {k: round(v, 5) for k, v in per.items()},
+                "timing": "CUDA events from event nodes of the graph-replayed sweeps (engine timing mode)",
+                "sweep_ms_graph_replay": round(sweep_ms, 5),
+                "sweep_frac": round((24.0 * E + 16.0 * F + 12.0 * V) / (sweep_ms / 1e3) / 1e9 / peak, 4)}
 
     # End to end through the C ABI with host arrays.
     e2e_ms, h2d = [], 0
@@ -773,6 +839,8 @@ def run_ours(args, rank, world, local):
         s.record(stream)
         t0 = time.perf_counter()
         eng2 = Engine(arr, precision=args.precision, damping=args.damping, stream=stream.cuda_stream)
+        if tuned:
+            eng2.set_tuning(tuned["factor_form"], tuned["var_form"])
         eng2.init()
         eng2.run_fixed(args.sweeps)
         out = eng2.beliefs()
@@ -787,6 +855,21 @@ def run_ours(args, rank, world, local):
     e2e_mean = statistics.median(e2e_ms) if e2e_ms else float("nan")  # --e2e-steps 0: profiling runs only
     e2e_val = 2.0 * E * args.sweeps * world / (allreduce_max(e2e_mean, world) / 1e3)
 
+    # Like for like with the reference arm (which has no damping): the same
+    # sweeps undamped, in FP32 and in FP64 (the reference's own precision).
+    undamped = {}
+    if args.damping != 0.0:
+        for prec in (32, 64):
+            e0 = Engine(arr, precision=prec, damping=0.0, stream=stream.cuda_stream)
+            if tuned and prec == args.precision:
+                e0.set_tuning(tuned["factor_form"], tuned["var_form"])
+            a0 = argparse.Namespace(**vars(args))
+            a0.steps = max(3, min(args.steps, 5))
+            ms0, _, _ = sweep_timing(e0, a0, stream, flush, world)
+            undamped["fp%d" % prec] = {"value": 2.0 * E * args.sweeps * a0.steps * world / (ms0 / 1e3),
+                                       "ms_per_step": ms0 / a0.steps}
+            e0.close()
+
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == 32 else "f64",
@@ -794,14 +877,179 @@ def run_ours(args, rank, world, local):
             "config": {"workload": "1M-tuple Bingo-style graph, 200 PARALL sweeps, damping 0.1, FP32 log-odds",
                        "vars": V, "factors": F, "edge_slots": E, "sweeps": args.sweeps, "damping": args.damping,
                        "seed": args.seed, "scale": args.scale, "replicas": world,
-                       "l2": "256 MB buffer written between timed steps; working set > L2"},
+                       "l2": "256 MB buffer written between timed steps; working set > L2",
+                       "kernel_forms": eng.tuning(), "autotune": tuned},
             "roofline": roofline, "clocks": clk, "gpu_launches": launches,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": V * 8,
-                    "ms_per_step": e2e_mean}}
-    if rank == 0 and world == 1:
-        line["cpu_baseline"] = cpu_baseline(fl, args)
+                    "ms_per_step": e2e_mean},
+            "undamped": undamped}
     eng.close()
+    if rank == 0 and world == 1 and args.cpu_seconds > 0:
+        base, b_oracle = oracle_leg(fl, args, args.sweeps)
+        line["cpu_baseline"] = base
+        nan_same = bool(np.array_equal(np.isnan(b_engine), np.isnan(b_oracle)))
+        err = float(np.nanmax(np.abs(b_engine - b_oracle)))
+        line["parity"] = {"belief_error_vs_fp64_oracle": err, "tolerance": 1e-5, "within": bool(err <= 1e-5 and nan_same),
+                          "vars_compared": V, "nan_positions_equal": nan_same,
+                          "oracle": "reference arithmetic, FP64, init + %d sweeps, damping %g" % (args.sweeps, args.damping)}
+    extras = [x for x in args.extras.split(",") if x and x != "none"]
+    for name in extras:
+        try:
+            line[name] = {"batched": batched_record, "adjoint": adjoint_record}[name](args, rank, world, local)
+        except Exception as ex:  # a sub-record must not cost the main line
+            line[name] = {"error": "%s: %s" % (type(ex).__name__, ex)}
     return line
+
+
+def _make_arrays(job):
+    kind, i = job
+    (batch_graph_arrays if kind == "batch" else adjoint_graph_arrays)(i)
+    return i
+
+
+def arrays_parallel(kind, indices):
+    """Graph arrays of the batched-serving (kind "batch") or gradient
+    ("adjoint") sets, generated on all host cores (a spawn-started process
+    pool: no worker inherits a CUDA context) and cached in the temp dir."""
+    import multiprocessing as mp
+
+    todo = [i for i in indices if not os.path.exists(os.path.join(
+        tempfile.gettempdir(), ("fastlbp_b200_cfg3_s3_g%d.npz" if kind == "batch" else "fastlbp_b200_cfg4_s4_g%d.npz") % i))]
+    if len(todo) > 1:
+        with mp.get_context("spawn").Pool(min(len(todo), os.cpu_count() or 1)) as pool:
+            pool.map(_make_arrays, [(kind, i) for i in todo], chunksize=1)
+    load = batch_graph_arrays if kind == "batch" else adjoint_graph_arrays
+    return [load(i) for i in indices]
+
+
+def batched_record(args, rank, world, local):
+    """Sub-record of the default line: batched serving (512 uneven Bingo-style
+    graphs, 1 k-200 k tuples, 1-50 clamps each, per-graph tol 1e-6, maxiter
+    500, FP32) in one BatchEngine against the plain form (one engine per
+    graph, solved in turn) on the same graphs; graphs dealt to ranks by size.
+    Median of 5 steps of each, device work timed by the wall clock around
+    whole solves (init + run, results on the device), max over ranks."""
+    import torch
+
+    from fastlbp_b200 import BatchEngine, Engine, workloads
+    from fastlbp_b200.shard import partition
+
+    tol, maxiter, steps = 1e-6, 500, 5
+    sizes = workloads.config3_sizes(args.graphs)
+    mine = partition(sizes, world)[rank]
+    arrays = arrays_parallel("batch", mine)
+    be = BatchEngine(arrays, precision=32)
+    plain = [Engine(a, precision=32) for a in arrays]
+    tuned = be.autotune_batch(tol, maxiter) if hasattr(be, "autotune_batch") else None
+    for e in plain:
+        if tuned:
+            e.set_tuning(tuned["factor_form"], tuned["var_form"])
+    be.init()
+    be.run_batch_tol(tol, maxiter)  # captures the sweep graphs
+    for e in plain:
+        e.init()
+        e.run_tol(tol, maxiter, 1e9)
+    torch.cuda.synchronize()
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    tb, tp = [], []
+    for _ in range(steps):
+        barrier(world)
+        t0 = time.perf_counter()
+        be.init()
+        sweeps, reasons = be.run_batch_tol(tol, maxiter)
+        tb.append(time.perf_counter() - t0)
+        barrier(world)
+        t0 = time.perf_counter()
+        psweeps = []
+        for e in plain:
+            e.init()
+            psweeps.append(e.run_tol(tol, maxiter, 1e9)["sweeps"])
+        tp.append(time.perf_counter() - t0)
+    clk = clocks.stop()
+    allb = be.beliefs()
+    diff = max((float(np.max(np.abs(be.beliefs_of(k, allb) - e.beliefs()))) if e.n_vars else 0.0
+                for k, e in enumerate(plain)), default=0.0)
+    t_b = allreduce_max(statistics.median(tb), world)
+    t_p = allreduce_max(statistics.median(tp), world)
+    E = float(sum(int(a["factor_offsets"][-1]) for a in arrays))
+    rec = {"metric": "graphs/s (batched, per-graph tol 1e-6)", "value": args.graphs / t_b, "unit": "graphs/s",
+           "plain": args.graphs / t_p, "batched_over_plain": t_p / t_b, "steps": steps, "statistic": "median",
+           "graphs": args.graphs, "graphs_this_rank": len(mine), "edge_slots_this_rank": E,
+           "sweeps": {"min": int(sweeps.min()), "median": float(np.median(sweeps)), "max": int(sweeps.max()),
+                      "same_as_plain": bool(sweeps.tolist() == psweeps)},
+           "max_belief_diff_batched_vs_plain": diff, "seconds": {"batched": t_b, "plain": t_p},
+           "kernel_forms": be.tuning(), "autotune": tuned, "clocks": clk,
+           "scaling": "strong: the graphs are dealt to the ranks"}
+    be.close()
+    for e in plain:
+        e.close()
+    return rec
+
+
+def adjoint_record(args, rank, world, local):
+    """Sub-record of the default line: gradient through T = 100 undamped
+    sweeps from init (checkpoints every 10, FP32) of the BCE loss on 200
+    labelled alarms per graph, 64 graphs of 50 k tuples in one BatchEngine
+    (graphs dealt to ranks), against a forward solve (init + 100 sweeps +
+    beliefs) of the same engine; device buffers. Median of 5 steps, max over
+    ranks. The gradient is checked against central differences by
+    --workload adjoint and the tests."""
+    import torch
+
+    from fastlbp_b200 import BatchEngine
+    from fastlbp_b200.shard import partition
+
+    T, K, n_graphs, steps = 100, 10, 64, 5
+    mine = partition(np.ones(n_graphs), world)[rank]
+    arrays = arrays_parallel("adjoint", mine)
+    be = BatchEngine(arrays, precision=32)
+    idx = np.concatenate([be.var_off[k] + a["label_vars"] for k, a in enumerate(arrays)])
+    y = np.concatenate([a["labels"] for a in arrays])
+    dev = torch.device("cuda", local)
+    idx_d, y_d = torch.as_tensor(idx, device=dev), torch.as_tensor(y, device=dev)
+    b_d = torch.empty(be.n_vars, dtype=torch.float64, device=dev)
+    gp_d = torch.empty(be.n_factors, dtype=torch.float64, device=dev)
+
+    def forward():
+        be.init()
+        be.run_fixed(T)
+        be.beliefs_device(b_d)
+
+    def gradient():
+        be.adjoint_forward(T, K, fetch=False)
+        be.beliefs_device(b_d)
+        bb = b_d[idx_d].clamp(1e-300, 1.0 - 1e-16)
+        g = torch.zeros_like(b_d)
+        g.index_put_((idx_d,), -y_d / bb + (1 - y_d) / (1 - bb), accumulate=True)
+        be.adjoint_backward_device(g, gp_d)
+
+    def timed(fn):
+        barrier(world)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0
+
+    forward()
+    gradient()
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    tf, tg = [], []
+    for _ in range(steps):
+        tf.append(timed(forward))
+        tg.append(timed(gradient))
+    clk = clocks.stop()
+    t_f = allreduce_max(statistics.median(tf), world)
+    t_g = allreduce_max(statistics.median(tg), world)
+    rec = {"metric": "gradient time / forward-solve time", "value": t_g / t_f, "unit": "ratio",
+           "higher_is_better": False, "target": 3.0, "steps": steps, "statistic": "median",
+           "seconds": {"forward_solve": t_f, "gradient": t_g}, "graphs": n_graphs, "graphs_this_rank": len(mine),
+           "sweeps": T, "checkpoint_every": K, "finite_gradient": bool(torch.isfinite(gp_d).all().item()),
+           "clocks": clk}
+    be.close()
+    return rec
 
 
 def run_reference(args, rank, world):
@@ -810,14 +1058,17 @@ def run_reference(args, rank, world):
     so it runs the same sweep count undamped."""
     if rank != 0:
         return None
-    fl, arr = graph_arrays(args)
-    E = int(arr["factor_offsets"][-1])
+    # The graph file comes from the seeded generator alone (plain Python and
+    # numpy): nothing of this repository's library is loaded in this arm.
+    from fastlbp_b200 import workloads
+
+    fl = workloads.config1(args.seed, scale=args.scale)
     ref_bp = os.path.join(ROOT, "oracle", "_ref", "ref_bp")
     base = {"metric": METRIC, "unit": UNIT, "impl": "reference", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "data": "synthetic (seeded Bingo-style generator)",
             "config": {"workload": "1M-tuple Bingo-style graph, 200 PARALL sweeps, FP64 (reference has no damping)",
-                       "edge_slots": E, "sweeps": args.sweeps, "seed": args.seed, "scale": args.scale}}
+                       "sweeps": args.sweeps, "seed": args.seed, "scale": args.scale}}
     import torch
     if not (os.path.exists(ref_bp) and torch.cuda.is_available()):
         return dict(base, unavailable="oracle/_ref/ref_bp not built on this machine")
@@ -830,23 +1081,35 @@ def run_reference(args, rank, world):
     if r.returncode != 0:
         return dict(base, unavailable="reference run failed: " + (r.stderr or r.stdout)[-200:])
     d = json.loads(r.stdout.strip().splitlines()[-1])
+    E = int(d["slots"])
+    base["config"]["edge_slots"] = E
     runs = d["run_event_all_s"][args.warmup:]
     cons = d["construct_all_s"][args.warmup:]
     value = 2.0 * E * args.sweeps / statistics.mean(runs)
+    # end to end as a FastLBP user pays it per solve: construct (host edge
+    # records + H2D) + run; the file read is reported apart
+    e2e_s = statistics.mean(runs) + statistics.mean(cons)
     line = dict(base, value=value, ms_per_step=statistics.mean(runs) * 1e3, dtype="f64",
                 reference_construct_s=statistics.mean(cons), reference_read_s=d["read_s"])
     line["cpu_baseline"] = {"value": value, "unit": UNIT, "kind": "reference", "cores": 1,
                             "sample": "FastLBP CausalBP (updates=PARALL) built from its sources, run(tol, %d, 1) "
                                       "on the B200 from one host thread; its path has no CPU implementation" % args.sweeps}
-    line["e2e"] = {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    line["e2e"] = {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                   "excludes": "CausalBP construction (host edge records + their copy to the device) and the "
+                               "file read; see e2e_with_construct"}
+    line["e2e_with_construct"] = {"value": 2.0 * E * args.sweeps / e2e_s, "unit": UNIT, "ms_per_step": e2e_s * 1e3,
+                                  "includes": "CausalBP construction + run(tol, %d, 1), per solve" % args.sweeps}
     line["gpu_launches"] = None
     return line
 
 
 def main():
     args = parse()
+    maybe_spawn(args)
     rank, world, local = dist_setup(args)
-    if args.impl == "reference":
+    if args.plan_only:
+        line = run_plan(args, rank, world)
+    elif args.impl == "reference":
         line = run_reference(args, rank, world)
     elif args.workload == "batch":
         line = run_batch(args, rank, world, local)

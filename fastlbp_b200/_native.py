@@ -54,6 +54,12 @@ class DeviceGraph(C.Structure):
 NOALLOC_MAX_SLOTS = 1 << 19
 
 
+class Tuning(C.Structure):
+    """flbp_tuning: form of each sweep pass (0 staged, 1/2 direct) and the blocks it launches."""
+    _fields_ = [("factor_form", C.c_int32), ("var_form", C.c_int32), ("factor_blocks", C.c_int32),
+                ("var_blocks", C.c_int32)]
+
+
 class RunInfo(C.Structure):
     _fields_ = [("sweeps", C.c_int64), ("total_sweeps", C.c_int64), ("maxdiff", C.c_double), ("frac", C.c_double),
                 ("reason", C.c_int32), ("status", C.c_int32), ("launches", C.c_int64)]
@@ -128,6 +134,8 @@ def lib():
         "flbp_set_update_seq": [_vp, _vp, C.c_int64],
         "flbp_update_info": [_vp, P(C.c_int32), P(C.c_int64)],
         "flbp_set_seq_kernel": [_vp, C.c_int32],
+        "flbp_set_tuning": [_vp, P(Tuning)],
+        "flbp_get_tuning": [_vp, P(Tuning)],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -156,4 +164,4 @@ EXPORTED = ["flbp_last_error", "flbp_version", "flbp_engine_create", "flbp_engin
             "flbp_batch_run_tol", "flbp_adjoint_forward", "flbp_adjoint_backward", "flbp_set_factor_probs",
             "flbp_adjoint_backward_device", "flbp_get_beliefs_device", "flbp_clamp_vars", "flbp_layout_digest",
             "flbp_update_seq", "flbp_shuffled_factors", "flbp_seq_batches", "flbp_set_update_seq", "flbp_update_info",
-            "flbp_set_seq_kernel"]
+            "flbp_set_seq_kernel", "flbp_set_tuning", "flbp_get_tuning"]

@@ -431,6 +431,16 @@ class Engine:
         check(lib().flbp_kernel_times(self._h, ms, n))
         return float(ms[0]), float(ms[1]), int(n[0]), int(n[1])
 
+    def set_tuning(self, factor_form: int, var_form: int) -> None:
+        """Form of each sweep pass: 0 staged, 1 or 2 direct (flbp_set_tuning)."""
+        t = N.Tuning(int(factor_form), int(var_form), 0, 0)
+        N.check(N.lib().flbp_set_tuning(self.h, C.byref(t)))
+
+    def tuning(self) -> Dict[str, int]:
+        t = N.Tuning()
+        N.check(N.lib().flbp_get_tuning(self.h, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in t._fields_}
+
     def last_run_ms(self) -> float:
         v = C.c_double()
         check(lib().flbp_last_run_ms(self._h, C.byref(v)))

@@ -1,0 +1,27 @@
+// Host launchers of the direct-load sweep passes (direct.cu). Forms: 1 = at
+// most 64 registers per thread (two 16-warp blocks per SM), 2 = at most 40
+// (three blocks per SM; the widest groups spill).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "kernels.cuh"
+
+namespace flbp {
+
+template <typename T>
+cudaError_t direct_factor_launch(int form, unsigned grid, const FactorArgs &a, const T *vf, T *fv, Ctl *ctl,
+                                 cudaStream_t st);
+
+// bmode: the variable pass's belief mode (0 none, 1 residual, 2 residual +
+// count + history, 4 batched residual); always writes vf.
+template <typename T>
+cudaError_t direct_var_launch(int form, int bmode, bool damp, unsigned grid, const VarArgs &a, const T *fv, T *vf,
+                              T *fvd, T d, Ctl *ctl, cudaStream_t st);
+
+// Resident 16-warp blocks per SM of a form's factor (var = false) or
+// variable pass.
+template <typename T>
+int direct_blocks_per_sm(int form, bool var, bool damp);
+
+}  // namespace flbp

@@ -19,6 +19,7 @@
 #include "engine_internal.h"
 #include "kernels.cuh"
 #include "adjoint.cuh"
+#include "direct_launch.h"
 #include "seq.cuh"
 
 namespace flbp {
@@ -118,6 +119,10 @@ struct flbp_engine {
     Ctl *h_ctl = nullptr;  // pinned mirror
 
     int factor_grid = 1, var_grid = 1;
+    // Form of each pass (flbp_tuning): 0 staged, 1/2 direct; grids of the direct forms.
+    int f_form = 0, v_form = 0;
+    int f_grid_direct = 1, v_grid_direct = 1;
+    int sms = 148;
     std::map<std::pair<int, int>, cudaGraphExec_t> graphs;  // (mode, sweeps) -> executable graph
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float last_ms = 0.f;
@@ -134,6 +139,7 @@ struct flbp_engine {
     bool ktime = false;
     std::vector<cudaEvent_t> kev;
     size_t kev_used = 0;
+    std::vector<cudaGraphExec_t> kgraphs;  // timing-mode graphs of the current call
     double kt_ms[2] = {0.0, 0.0};
     long long kt_n[2] = {0, 0};
 };
@@ -344,8 +350,24 @@ cudaError_t configure_kernels(bool damp, int *fb, int *vb) {
 
 template <typename T, int BMODE, bool DAMP>
 void launch_var(flbp_engine *e, const VarArgs &va) {
+    if (e->v_form) {
+        direct_var_launch<T>(e->v_form, BMODE, DAMP, (unsigned)e->v_grid_direct, va, (const T *)e->d_fv, (T *)e->d_vf,
+                             (T *)e->d_fvd, (T)e->damping, e->d_ctl, e->stream);
+        return;
+    }
     var_pass_kernel<T, BMODE, true, DAMP, kStages><<<e->var_grid, kBlockThreads, var_smem<T, DAMP>(), e->stream>>>(
         va, (const T *)e->d_fv, (T *)e->d_vf, (T *)e->d_fvd, (T)e->damping, e->d_ctl);
+}
+
+template <typename T>
+void launch_factor(flbp_engine *e, const FactorArgs &fa, const void *vf, void *fv) {
+    if (e->f_form) {
+        direct_factor_launch<T>(e->f_form, (unsigned)e->f_grid_direct, fa, (const T *)vf, (T *)fv, e->d_ctl,
+                                e->stream);
+        return;
+    }
+    factor_pass_kernel<T, kFactorStages<T>><<<e->factor_grid, kBlockThreads, factor_smem<T>(), e->stream>>>(
+        fa, (const T *)vf, (T *)fv, e->d_ctl);
 }
 
 template <typename T, bool DAMP>
@@ -369,8 +391,7 @@ void launch_sweep(flbp_engine *e, int mode, int which = 3) {
             fa.trange = e->d_ftrange;
             fa.n_graphs = e->n_graphs;
         }
-        factor_pass_kernel<T, kFactorStages<T>><<<e->factor_grid, kBlockThreads, factor_smem<T>(), e->stream>>>(
-            fa, (const T *)e->d_vf, (T *)e->d_fv, e->d_ctl);
+        launch_factor<T>(e, fa, e->d_vf, e->d_fv);
     }
     if (!(which & 2)) return;
     VarArgs va = var_args(e);
@@ -450,21 +471,39 @@ int launch_sweeps(flbp_engine *e, int mode, long long n) {
     int kmax = 64;
     if (e->seq)
         while (kmax > 1 && (long long)kmax * per > 2048) kmax /= 2;
-    if (e->ktime) {  // no graphs: events around each pass
-        for (long long i = 0; i < n; i++) {
-            while (e->kev.size() < e->kev_used + 3) {
+    if (e->ktime) {
+        // Events around each pass, recorded by event nodes of a captured graph,
+        // so that the passes run back to back as in the graph-replayed sweeps.
+        while (n > 0) {
+            const long long k = std::min<long long>(n, kmax);
+            while (e->kev.size() < e->kev_used + 3 * (size_t)k) {
                 cudaEvent_t ev;
                 FLBP_CUDA(cudaEventCreate(&ev));
                 e->kev.push_back(ev);
             }
-            cudaEvent_t *ev = &e->kev[e->kev_used];
-            e->kev_used += 3;
-            FLBP_CUDA(cudaEventRecord(ev[0], e->stream));
-            launch_sweep_any(e, mode, 1);
-            FLBP_CUDA(cudaEventRecord(ev[1], e->stream));
-            launch_sweep_any(e, mode, 2);
-            FLBP_CUDA(cudaEventRecord(ev[2], e->stream));
-            e->launches += per;
+            cudaGraph_t g = nullptr;
+            FLBP_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+            for (long long i = 0; i < k; i++) {
+                cudaEvent_t *ev = &e->kev[e->kev_used];
+                e->kev_used += 3;
+                cudaEventRecordWithFlags(ev[0], e->stream, cudaEventRecordExternal);
+                launch_sweep_any(e, mode, 1);
+                cudaEventRecordWithFlags(ev[1], e->stream, cudaEventRecordExternal);
+                launch_sweep_any(e, mode, 2);
+                cudaEventRecordWithFlags(ev[2], e->stream, cudaEventRecordExternal);
+            }
+            FLBP_CUDA(cudaStreamEndCapture(e->stream, &g));
+            cudaGraphExec_t x = nullptr;
+            cudaError_t err = cudaGraphInstantiateWithFlags(&x, g, 0);
+            cudaGraphDestroy(g);
+            if (err != cudaSuccess) {
+                set_error(std::string("CUDA graph instantiation failed: ") + cudaGetErrorString(err));
+                return FLBP_ERR_CUDA;
+            }
+            e->kgraphs.push_back(x);
+            FLBP_CUDA(cudaGraphLaunch(x, e->stream));
+            e->launches += per * k;
+            n -= k;
         }
         return FLBP_OK;
     }
@@ -563,6 +602,8 @@ int record_stop(flbp_engine *e) {
         e->kt_n[1]++;
     }
     e->kev_used = 0;
+    for (auto x : e->kgraphs) cudaGraphExecDestroy(x);
+    e->kgraphs.clear();
     return FLBP_OK;
 }
 
@@ -736,6 +777,7 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
     const size_t ns = std::max<uint64_t>(1, L.n_slots);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
+    e->sms = sms;
     // One full wave of resident blocks; the kernels stride over tiles and large items.
     int fb = 1, vb = 1;
     const bool damp = e->damping != 0.0;
@@ -858,6 +900,27 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
     return FLBP_OK;
 }
 
+// Installs the forms of the two passes (0 staged, 1/2 direct) with one wave
+// of resident blocks for a direct form; captured sweep graphs are dropped.
+int apply_forms(flbp_engine *e, int ff, int vf) {
+    const bool damp = e->damping != 0.0;
+    const HostLayout &L = e->L;
+    auto grid = [&](int form, bool var, uint64_t items, uint64_t huge) -> int {
+        const int bps = e->prec == 64 ? direct_blocks_per_sm<double>(form, var, damp)
+                                      : direct_blocks_per_sm<float>(form, var, damp);
+        const uint64_t need = std::max<uint64_t>((items + kConsumerWarps - 1) / kConsumerWarps, huge);
+        return (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)e->sms * (uint64_t)bps, need));
+    };
+    if (ff) e->f_grid_direct = grid(ff, false, (uint64_t)(L.nf_big - L.nf_huge) + L.n_fgroups(), L.nf_huge);
+    if (vf) e->v_grid_direct = grid(vf, true, (uint64_t)(L.nv_big - L.nv_huge) + L.n_vgroups(), L.nv_huge);
+    FLBP_CUDA(cudaGetLastError());
+    e->f_form = ff;
+    e->v_form = vf;
+    for (auto &kv : e->graphs) cudaGraphExecDestroy(kv.second);
+    e->graphs.clear();
+    return FLBP_OK;
+}
+
 // The v->f messages of clamped variables: +inf (clamped to 1) or -inf (0).
 template <typename T>
 __global__ void clamp_slots_kernel(const uint32_t *__restrict__ pairs, uint32_t n, T *vf) {
@@ -888,6 +951,7 @@ int flbp_engine_destroy(flbp_engine *e) {
     if (e->stream) cudaStreamSynchronize(e->stream);
     for (auto &kv : e->graphs) cudaGraphExecDestroy(kv.second);
     for (auto ev : e->kev) cudaEventDestroy(ev);
+    for (auto x : e->kgraphs) cudaGraphExecDestroy(x);
     void *bufs[] = {e->d_vf,     e->d_fv,       e->d_fvd,    e->d_f_pos,     e->d_f_pq,   e->d_fg_base,   e->d_fb_off,     e->d_f_kind,
                     e->d_f_deg,  e->d_vg_base,  e->d_vb_off, e->d_v_ent,     e->d_prior,      e->d_belief,
                     e->d_lowpass, e->d_hist,    e->d_hist_next, e->d_hist_count, e->d_ctl,    e->d_scratch,
@@ -1251,6 +1315,28 @@ int flbp_kernel_times(flbp_engine *e, double *ms, int64_t *counts) {
     return FLBP_OK;
 }
 
+int flbp_set_tuning(flbp_engine *e, const flbp_tuning *t) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    if (!t || t->factor_form < 0 || t->factor_form > 2 || t->var_form < 0 || t->var_form > 2) {
+        set_error("flbp_set_tuning: forms must be 0 (staged), 1 or 2 (direct)");
+        return FLBP_ERR_INVALID;
+    }
+    return apply_forms(e, t->factor_form, t->var_form);
+}
+
+int flbp_get_tuning(flbp_engine *e, flbp_tuning *t) {
+    if (!e || !t) {
+        set_error("null argument");
+        return FLBP_ERR_INVALID;
+    }
+    t->factor_form = e->f_form;
+    t->var_form = e->v_form;
+    t->factor_blocks = e->f_form ? e->f_grid_direct : e->factor_grid;
+    t->var_blocks = e->v_form ? e->v_grid_direct : e->var_grid;
+    return FLBP_OK;
+}
+
 int flbp_last_run_ms(flbp_engine *e, double *ms) {
     if (!e || !ms) {
         set_error("null argument");
@@ -1450,16 +1536,19 @@ void launch_adjoint_step(flbp_engine *e, const void *vf, const void *fv, const v
 template <typename T>
 void launch_factor_pass_on(flbp_engine *e, const void *vf, void *fv) {
     const FactorArgs fa = factor_args<T>(e);
-    factor_pass_kernel<T, kFactorStages<T>><<<e->factor_grid, kBlockThreads, factor_smem<T>(), e->stream>>>(
-        fa, (const T *)vf, (T *)fv, e->d_ctl);
+    launch_factor<T>(e, fa, vf, fv);
     e->launches += 1;
 }
 
 template <typename T>
 void launch_var_pass_on(flbp_engine *e, const void *fv, void *vf) {
     const VarArgs va = var_args(e);
-    var_pass_kernel<T, 0, true, false, kStages><<<e->var_grid, kBlockThreads, var_smem<T, false>(), e->stream>>>(
-        va, (const T *)fv, (T *)vf, nullptr, (T)0, e->d_ctl);
+    if (e->v_form)
+        direct_var_launch<T>(e->v_form, 0, false, (unsigned)e->v_grid_direct, va, (const T *)fv, (T *)vf, nullptr,
+                             (T)0, e->d_ctl, e->stream);
+    else
+        var_pass_kernel<T, 0, true, false, kStages><<<e->var_grid, kBlockThreads, var_smem<T, false>(), e->stream>>>(
+            va, (const T *)fv, (T *)vf, nullptr, (T)0, e->d_ctl);
     e->launches += 1;
 }
 

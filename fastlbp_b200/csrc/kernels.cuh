@@ -507,8 +507,9 @@ __device__ __forceinline__ T head_from_pair(T P, T R, T p, T q, LogP lP) {
 }
 
 // One factor of a sliced-ELL group of width W, one lane, all in registers:
-// slot k of the factor at vb[32 k + lane] (head at k = 0), the fv position
-// of its output at ps[32 k + lane]. With sigma_k, tau_k = 1 - sigma_k of the
+// vb(k) is the message of slot k of the factor (head at k = 0) and ps(k) the
+// fv position of its output, read from a staged tile in shared memory or
+// from registers that the direct form loaded. With sigma_k, tau_k = 1 - sigma_k of the
 // body messages (AND orientation), pairs combine as
 //   (P1, R1) o (P2, R2) = (P1 P2, R1 + P1 R2),
 // a product and its complement: every term is non-negative, so P and 1 - P
@@ -518,24 +519,23 @@ __device__ __forceinline__ T head_from_pair(T P, T R, T p, T q, LogP lP) {
 // 341-366 in log-odds; OR = AND on negated log-odds). Widths up to 8 keep
 // sigma, tau and the suffix pairs of every slot (4 W registers); wider
 // groups keep only the prefix pairs and evaluate sigma again on the way back.
-template <typename T, int W>
-__device__ __forceinline__ void factor_reg(const T *vb, const uint32_t *ps, int deg, uint8_t kind, T p, T q, int lane,
-                                           T *__restrict__ fv) {
+template <typename T, int W, typename VB, typename PS>
+__device__ __forceinline__ void factor_reg(VB vb, PS ps, int deg, uint8_t kind, T p, T q, T *__restrict__ fv) {
     const T sgn = (kind & KIND_OR) ? T(-1) : T(1);
     auto logP = [&]() {
         T l = T(0);
 #pragma unroll
         for (int k = 1; k < W; k++)
-            if (k < deg) l += log_sigmoid<T>(sgn * vb[32 * k + lane]);
+            if (k < deg) l += log_sigmoid<T>(sgn * vb(k));
         return l;
     };
-    const T lh = sgn * head_effective<T>(kind, vb[lane]);
+    const T lh = sgn * head_effective<T>(kind, vb(0));
     if constexpr (W <= 8) {
         T sg[W], ta[W];
 #pragma unroll
         for (int k = 1; k < W; k++) {
             if (k < deg) {
-                sig_pair<T>(sgn * vb[32 * k + lane], sg[k], ta[k]);
+                sig_pair<T>(sgn * vb(k), sg[k], ta[k]);
             } else {  // padding slot: the identity pair
                 sg[k] = T(1);
                 ta[k] = T(0);
@@ -557,13 +557,13 @@ __device__ __forceinline__ void factor_reg(const T *vb, const uint32_t *ps, int 
 #pragma unroll
         for (int k = 1; k < W; k++) {
             if (k < deg)
-                put_fv<T>(fv, ps[32 * k + lane], sgn * body_out_pr<T>(Pp * sP[k], fma(Pp, sR[k], Rp), p, q, D));
+                put_fv<T>(fv, ps(k), sgn * body_out_pr<T>(Pp * sP[k], fma(Pp, sR[k], Rp), p, q, D));
             Rp = fma(Pp, ta[k], Rp);
             Pp = Pp * sg[k];
         }
         // the head from the forward product, as in the wider form below, so that a
         // factor's outputs do not depend on the width of the group it lands in
-        if ((kind & HEAD_MASK) == HEAD_FREE) put_fv<T>(fv, ps[lane], sgn * head_from_pair<T>(Pp, Rp, p, q, logP));
+        if ((kind & HEAD_MASK) == HEAD_FREE) put_fv<T>(fv, ps(0), sgn * head_from_pair<T>(Pp, Rp, p, q, logP));
     } else {
         T pP[W], pR[W];
         T P = T(1), R = T(0);
@@ -573,20 +573,20 @@ __device__ __forceinline__ void factor_reg(const T *vb, const uint32_t *ps, int 
             pR[k] = R;
             if (k < deg) {
                 T sk, tk;
-                sig_pair<T>(sgn * vb[32 * k + lane], sk, tk);
+                sig_pair<T>(sgn * vb(k), sk, tk);
                 R = fma(P, tk, R);
                 P = P * sk;
             }
         }
-        if ((kind & HEAD_MASK) == HEAD_FREE) put_fv<T>(fv, ps[lane], sgn * head_from_pair<T>(P, R, p, q, logP));
+        if ((kind & HEAD_MASK) == HEAD_FREE) put_fv<T>(fv, ps(0), sgn * head_from_pair<T>(P, R, p, q, logP));
         const BodyDen<T> D = body_den<T>(lh, p, q);
         T Ps = T(1), Rs = T(0);
 #pragma unroll
         for (int k = W - 1; k >= 1; k--) {
             if (k < deg) {
                 T sk, tk;
-                sig_pair<T>(sgn * vb[32 * k + lane], sk, tk);
-                put_fv<T>(fv, ps[32 * k + lane], sgn * body_out_pr<T>(pP[k] * Ps, fma(pP[k], Rs, pR[k]), p, q, D));
+                sig_pair<T>(sgn * vb(k), sk, tk);
+                put_fv<T>(fv, ps(k), sgn * body_out_pr<T>(pP[k] * Ps, fma(pP[k], Rs, pR[k]), p, q, D));
                 Rs = fma(sk, Rs, tk);
                 Ps = sk * Ps;
             }
@@ -599,7 +599,10 @@ __device__ __forceinline__ void factor_group(int w, const T *vb, const uint32_t 
                                              int lane, T *__restrict__ fv) {
     switch (w) {
 #define FLBP_W(N) \
-    case N: factor_reg<T, N>(vb, ps, deg, kind, p, q, lane, fv); break;
+    case N:                                                                                           \
+        factor_reg<T, N>([&](int k) { return vb[32 * k + lane]; }, [&](int k) { return ps[32 * k + lane]; }, deg, \
+                         kind, p, q, fv);                                                                     \
+        break;
         FLBP_W(2) FLBP_W(3) FLBP_W(4) FLBP_W(5) FLBP_W(6) FLBP_W(7) FLBP_W(8) FLBP_W(9) FLBP_W(10) FLBP_W(11)
         FLBP_W(12) FLBP_W(13) FLBP_W(14) FLBP_W(15) FLBP_W(16)
 #undef FLBP_W
@@ -768,6 +771,21 @@ __device__ __forceinline__ void factor_tile_item(const T *vb, const uint32_t *ps
 }
 static_assert(kBigFactorBody == 256, "factor_tile_item covers bodies of up to 256 slots");
 
+// Opens a sweep (thread 0 of block 0 of the factor pass, either form): sweep
+// counters, damping weight of the constant priors, residual reset.
+__device__ __forceinline__ void sweep_open(Ctl *ctl) {
+    unsigned long long now;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+    if (ctl->run_sweeps == 0) ctl->t_start_ns = now;
+    ctl->t += 1;
+    ctl->run_sweeps += 1;
+    ctl->pscale = (ctl->damping == 0.0) ? 1.0 : 1.0 - pow(ctl->damping, (double)ctl->t);
+    ctl->maxdiff_bits = 0ull;
+    ctl->nonconv = 0ull;
+    ctl->arrive = 0u;
+    ctl->vnext = 0u;  // the variable pass of this sweep starts after this kernel
+}
+
 // Factor pass. Every block runs a STAGES-deep pipeline over its tiles (tile
 // blockIdx.x + i gridDim.x): warp kConsumerWarps (one lane) is the producer -
 // it waits until the consumer warps have released a stage and bulk-loads the
@@ -783,18 +801,7 @@ __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArg
     __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES];
     typedef FactorStage<T> FS;
     if (*(volatile int *)&ctl->done) return;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        unsigned long long now;
-        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
-        if (ctl->run_sweeps == 0) ctl->t_start_ns = now;
-        ctl->t += 1;
-        ctl->run_sweeps += 1;
-        ctl->pscale = (ctl->damping == 0.0) ? 1.0 : 1.0 - pow(ctl->damping, (double)ctl->t);
-        ctl->maxdiff_bits = 0ull;
-        ctl->nonconv = 0ull;
-        ctl->arrive = 0u;
-        ctl->vnext = 0u;  // the variable pass of this sweep starts after this kernel
-    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) sweep_open(ctl);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const uint32_t n_tiles = a.n_tiles;
     __shared__ uint32_t s_done[kDoneWords];  // batched solves: stopped graphs
@@ -1172,6 +1179,57 @@ __device__ __forceinline__ void mark_moved(uint32_t *s_moved, const VarArgs &a, 
     }
 }
 
+// End of a variable pass with a residual (BMODE 1, 2, 4), called by every
+// thread of the block: the block's maximum belief change (and count of
+// changes above tol) into the control block, the batched per-graph flags,
+// and in the last block to finish, the run's stop rules.
+template <int BMODE>
+__device__ __forceinline__ void var_close(const VarArgs &a, Ctl *ctl, double dmax, unsigned long long cnt,
+                                          const uint32_t *s_moved, int lane, int wid) {
+    __shared__ double s_max[kConsumerWarps + 1];
+    __shared__ unsigned long long s_cnt[kConsumerWarps + 1];
+    __shared__ bool s_last;
+    dmax = warp_max(dmax);
+    cnt = warp_sum(cnt);
+    if (lane == 0) {
+        s_max[wid] = dmax;
+        s_cnt[wid] = cnt;
+    }
+    __syncthreads();
+    if (BMODE == 4) {  // the block's per-graph flags, one store per graph
+        const uint32_t words = min((a.n_graphs + 31) / 32, (uint32_t)kMovedWords);
+        for (uint32_t w = threadIdx.x; w < words; w += blockDim.x) {
+            uint32_t bits = s_moved[w];
+            while (bits) {
+                const int b = __ffs(bits) - 1;
+                bits &= bits - 1;
+                a.gstate[a.n_graphs + 32 * w + b] = 1;
+            }
+        }
+        __threadfence();
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        unsigned long long c = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); i++) {
+            m = fmax(m, s_max[i]);
+            c += s_cnt[i];
+        }
+        atomicMax(&ctl->maxdiff_bits, (unsigned long long)__double_as_longlong(m));
+        if (BMODE == 2) atomicAdd(&ctl->nonconv, c);
+        __threadfence();
+        const unsigned int prev = atomicAdd(&ctl->arrive, 1u);
+        s_last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        if (BMODE == 4) batch_stop_rules(ctl, a);  // the whole block
+        else if (threadIdx.x == 0) stop_rules(ctl);
+    }
+}
+
 // Variable pass, warp-specialised like the factor pass: the producer warp
 // bulk-loads each tile's entries (factor-side slots), incoming messages, the
 // previous damped messages (with damping), priors and (with a residual)
@@ -1319,50 +1377,7 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
             if (lane == 0) mbar_arrive(&empty[s]);
         }
     }
-    if (RESID) {
-        __shared__ double s_max[kConsumerWarps + 1];
-        __shared__ unsigned long long s_cnt[kConsumerWarps + 1];
-        __shared__ bool s_last;
-        dmax = warp_max(dmax);
-        cnt = warp_sum(cnt);
-        if (lane == 0) {
-            s_max[wid] = dmax;
-            s_cnt[wid] = cnt;
-        }
-        __syncthreads();
-        if (BMODE == 4) {  // the block's per-graph flags, one store per graph
-            const uint32_t words = min((a.n_graphs + 31) / 32, (uint32_t)kMovedWords);
-            for (uint32_t w = threadIdx.x; w < words; w += blockDim.x) {
-                uint32_t bits = s_moved[w];
-                while (bits) {
-                    const int b = __ffs(bits) - 1;
-                    bits &= bits - 1;
-                    a.gstate[a.n_graphs + 32 * w + b] = 1;
-                }
-            }
-            __threadfence();
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) {
-            double m = 0.0;
-            unsigned long long c = 0;
-            for (int i = 0; i < (int)(blockDim.x >> 5); i++) {
-                m = fmax(m, s_max[i]);
-                c += s_cnt[i];
-            }
-            atomicMax(&ctl->maxdiff_bits, (unsigned long long)__double_as_longlong(m));
-            if (BMODE == 2) atomicAdd(&ctl->nonconv, c);
-            __threadfence();
-            const unsigned int prev = atomicAdd(&ctl->arrive, 1u);
-            s_last = (prev == gridDim.x - 1);
-        }
-        __syncthreads();
-        if (s_last) {
-            __threadfence();
-            if (BMODE == 4) batch_stop_rules(ctl, a);  // the whole block
-            else if (threadIdx.x == 0) stop_rules(ctl);
-        }
-    }
+    if (RESID) var_close<BMODE>(a, ctl, dmax, cnt, s_moved, lane, wid);
 }
 
 // Low-pass belief mean, oldest to newest, then one division

@@ -53,7 +53,8 @@ __global__ void noalloc_factor(flbp_device_graph g, const float *__restrict__ vf
             continue;
         }
         const float sg = (type == FLBP_OR) ? -1.f : 1.f;
-        if (hs) {  // head-clamped: one-hot head output
+        if (hs) {  // head-clamped: the mask's one-hot fallback; a (0,0) mask gives (0, 1) like a 1-clamp
+                   // (causal_bp_parall.cu:222-238, 271-287), as the engine folds it
             put(h, (hs == 2) ? -inf : inf);
         } else if (s1 - s0 == 1) {  // reduced to its head: (1-p, p) for AND, (p, 1-p) for OR
             put(h, sg * (logf(p) - log1pf(-p)));
@@ -149,8 +150,9 @@ extern "C" int flbp_run_fixed_device_noalloc(const flbp_device_graph *g, int64_t
                   " (use flbp_engine_create for larger graphs)");
         return FLBP_ERR_LIMIT;
     }
-    if ((g->n_factors > 0 && (!g->factor_offsets || !g->slot_var || !g->factor_head || !g->factor_type ||
-                              !g->factor_p || !g->factor_q)) ||
+    // slot_var is not read here (var_offsets / var_slots give the variable side) and may be NULL
+    if ((g->n_factors > 0 && (!g->factor_offsets || !g->factor_head || !g->factor_type || !g->factor_p ||
+                              !g->factor_q)) ||
         (g->n_vars > 0 && (!g->var_offsets || (g->n_slots > 0 && !g->var_slots)))) {
         set_error("flbp_run_fixed_device_noalloc: missing device array");
         return FLBP_ERR_INVALID;

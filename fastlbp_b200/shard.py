@@ -62,6 +62,10 @@ def shared_gradient(grad_p, rule_of_factor, n_rules: int, world: int = 1):
 
     if grad_p.shape != rule_of_factor.shape:
         raise ValueError("grad_p and rule_of_factor must have one entry per factor")
+    # An index outside [-1, n_rules) would make index_add_ raise a device-side
+    # assert on a CUDA tensor, which poisons the CUDA context: check first.
+    if rule_of_factor.numel() and (int(rule_of_factor.min()) < -1 or int(rule_of_factor.max()) >= int(n_rules)):
+        raise ValueError("rule_of_factor entries must lie in [-1, n_rules)")
     g = torch.zeros(int(n_rules), dtype=torch.float64, device=grad_p.device)
     m = rule_of_factor >= 0
     g.index_add_(0, rule_of_factor[m], grad_p[m].to(torch.float64))
@@ -75,6 +79,8 @@ def shared_gradient(grad_p, rule_of_factor, n_rules: int, world: int = 1):
 def expand_shared(p_rules, rule_of_factor, p_factor):
     """Per-factor probabilities after a learning step: the shared rule's value
     where a factor instantiates one, the factor's own elsewhere."""
+    if rule_of_factor.numel() and (int(rule_of_factor.min()) < -1 or int(rule_of_factor.max()) >= p_rules.shape[0]):
+        raise ValueError("rule_of_factor entries must lie in [-1, number of rules)")
     out = p_factor.clone()
     m = rule_of_factor >= 0
     out[m] = p_rules[rule_of_factor[m]].to(out.dtype)

@@ -152,14 +152,38 @@ int flbp_get_vf_messages(flbp_engine *eng, double *m0, double *m1, int64_t n_slo
  * Entries past n_counts are not written. */
 int flbp_engine_stats(flbp_engine *eng, int64_t *counts, int64_t n_counts);
 
-/* Per-pass timing mode (for measurement): while enabled, sweeps are launched
- * one kernel at a time with CUDA events around the factor and variable
- * passes instead of as CUDA graphs. Enabling resets the accumulators. */
+/* Per-pass timing mode (for measurement): while enabled, every sweep is
+ * launched from a CUDA graph captured for the call that also records CUDA
+ * events (event nodes) around the factor and the variable pass, so the
+ * passes run back to back as in the normal graph-replayed sweeps. Enabling
+ * resets the accumulators. */
 int flbp_set_kernel_timing(flbp_engine *eng, int32_t enable);
 
 /* Accumulated device time (ms) and launch counts of the factor pass [0] and
  * the variable pass [1] recorded in timing mode. */
 int flbp_kernel_times(flbp_engine *eng, double *ms, int64_t *counts);
+
+/* ---- kernel configuration of the PARALL sweep ----
+ *
+ * FastLBP launches every sweep kernel with a fixed kCudaThreadsNum = 128
+ * threads per block, one thread per edge or variable
+ * (include/utils/cuda_utils.h:23-27, csrc/kernel/causal_bp_parall.cu:400-467).
+ * Here each of the two passes of a sweep has two forms with identical
+ * results: 0 = staged (persistent blocks in which a producer warp bulk-copies
+ * tiles of items into a shared-memory ring for 16 consumer warps) and direct
+ * (every warp of a persistent grid loads its own items straight into
+ * registers; 1 = up to 64 registers per thread, two 16-warp blocks per SM,
+ * 2 = up to 40 registers, three blocks per SM). Which is faster depends on
+ * the graph; new engines start with both passes staged. */
+typedef struct flbp_tuning {
+    int32_t factor_form; /* 0 staged, 1 or 2 direct */
+    int32_t var_form;    /* 0 staged, 1 or 2 direct */
+    int32_t factor_blocks; /* flbp_get_tuning: blocks launched per factor pass (ignored when set) */
+    int32_t var_blocks;    /* flbp_get_tuning: blocks launched per variable pass (ignored when set) */
+} flbp_tuning;
+
+int flbp_set_tuning(flbp_engine *eng, const flbp_tuning *tuning);
+int flbp_get_tuning(flbp_engine *eng, flbp_tuning *tuning);
 
 /* ------------------------------------------------------------------------
  * Allocation-free solve. No counterpart in FastLBP.
@@ -184,6 +208,13 @@ int flbp_kernel_times(flbp_engine *eng, double *ms, int64_t *counts);
  *   the scratch and give wrong results: order them.
  * - Work is launched on `stream` (NULL: the legacy default stream); the
  *   call returns without waiting for it.
+ * - The device arrays are trusted, not checked (that would need a device
+ *   pass and a read-back): the graph must be well formed - factor_offsets
+ *   non-decreasing from 0 to n_slots; factor_head[I] inside factor I's
+ *   slots; var_offsets non-decreasing from 0 to n_slots; var_slots a
+ *   permutation of 0..n_slots-1 grouped by variable; factor types 0-2 with
+ *   singletons of one slot; p, q in [0,1]. A malformed graph makes the
+ *   kernels read and write outside the arrays and the scratch.
  * ---------------------------------------------------------------------- */
 #define FLBP_NOALLOC_MAX_SLOTS (1 << 19)
 
@@ -192,7 +223,7 @@ int flbp_kernel_times(flbp_engine *eng, double *ms, int64_t *counts);
 typedef struct flbp_device_graph {
     int32_t n_vars, n_factors, n_slots;
     const int32_t *factor_offsets;     /* n_factors + 1: factor-major slot offsets (row_ptr_vf) */
-    const int32_t *slot_var;           /* n_slots: variable of each slot (col_ind_vf) */
+    const int32_t *slot_var;           /* n_slots: variable of each slot (col_ind_vf); not read, may be NULL */
     const int32_t *factor_head;        /* n_factors: absolute slot of each factor's head */
     const int32_t *factor_type;        /* n_factors: FLBP_SINGLETON / FLBP_AND / FLBP_OR */
     const uint8_t *factor_head_state;  /* n_factors or NULL: 0 free, 1 head clamped to 1, 2 to 0, 3 mask (0,0) */

@@ -32,6 +32,25 @@
 // Built with -ffp-contract=off so results are deterministic; expect agreement
 // with the reference GPU binary to ~1e-12, not bit-exactly (nvcc contracts
 // multiply-adds into FMAs by default).
+//
+// Two arithmetic modes. The default restates the reference's arithmetic:
+// message pairs in probability space, rescaled by their larger component
+// after every product (causal_bp_parall.cu:14-18) and exact zeros counted
+// (:36-45, 74-83). Once the smaller component of a pair falls below the
+// double range (log-odds beyond about +-745) it becomes an exact zero, which
+// the zero-count rules then treat as hard evidence. The log-odds mode
+// ("lodds") runs the same PARALL recurrence - the same case split of the nine
+// factor/clamp/direction types, the same zero-count and fallback rules,
+// damping and run loops - with every message held as an FP64 log-odds value
+// and every product taken as a sum of logs, so nothing underflows: exact
+// zeros arise only where the reference's arithmetic gives them with exact
+// inputs (a p or q of 0 or 1, a clamp). On graphs whose messages stay in
+// range both modes agree to rounding. With underflow tracking on, the
+// default mode also marks every message and belief that depends on an
+// underflow: a message whose probability-space result has an exact zero (or
+// a product that reached zero without an exact-zero input) where the
+// log-odds evaluation of the same inputs is finite, and everything computed
+// from it in later sweeps.
 
 #include <algorithm>
 #include <cmath>
@@ -519,6 +538,111 @@ void fv_message(const ORec &r, const double *vf0, const double *vf1, double &out
     fv_message_t<false>(r, vf0, vf1, out0, out1);
 }
 
+// --------------------------------------------------------- log-odds mode
+//
+// A message (m0, m1), normalised, is held as lambda = log m1 - log m0:
+// +inf is (0, 1), -inf is (1, 0), 0 is (0.5, 0.5), NaN is the reference's
+// NaN pair.
+
+constexpr double kInfD = std::numeric_limits<double>::infinity();
+
+// log sigmoid(x) = log of the normalised m1 of lambda x; +inf -> 0, -inf -> -inf.
+inline double lsig(double x) {
+    if (std::isnan(x)) return x;
+    return x >= 0 ? -std::log1p(std::exp(-x)) : x - std::log1p(std::exp(x));
+}
+
+// log(e^a + e^b), exact zeros (-inf) allowed.
+inline double lae(double a, double b) {
+    if (a == -kInfD) return b;
+    if (b == -kInfD) return a;
+    const double m = std::fmax(a, b);
+    return m + std::log1p(std::exp(-std::fabs(a - b)));
+}
+
+// log(1 - e^x) for x <= 0.
+inline double log1mexp(double x) {
+    if (x == -kInfD) return 0.0;
+    if (x == 0.0) return -kInfD;
+    return x > -M_LN2 ? std::log(-std::expm1(x)) : std::log1p(-std::exp(x));
+}
+
+inline double lmask(double m) { return m == 0.0 ? -kInfD : 0.0; }  // masks are 0 or 1
+
+// Pair (log a, log b) of a noisy-AND over a body whose product of sigma is
+// e^lP: a = p P + q (1 - P), b = (1 - p) P + (1 - q)(1 - P).
+inline void and_pair(double lP, double p, double q, double &la, double &lb) {
+    const double l1 = log1mexp(lP);
+    la = lae(std::log(p) + lP, std::log(q) + l1);
+    lb = lae(std::log1p(-p) + lP, std::log1p(-q) + l1);
+}
+
+// One f->v message in log-odds: the nine types of
+// csrc/kernel/causal_bp_parall.cu:102-397 with every product taken as a sum
+// of logs. OR factors are AND factors with the states swapped.
+double fv_message_lodds(const ORec &r, const double *lvf) {
+    const size_t type = r.type, src = r.src, h = r.head, s = r.start, e = r.end;
+    const double p = r.p, q = r.q;
+    if (type == 0) return std::log(p) - std::log1p(-p);  // (1-p, p), :110-112
+    if (type <= 4) {  // into the head: AND 1 / 3, OR 2 / 4 (:113-288)
+        const bool is_or = (type == 2 || type == 4);
+        const double sg = is_or ? -1.0 : 1.0;
+        double lP = 0.0;  // log product of the body's sigma (AND orientation)
+        for (size_t j = s; j < e; j++)
+            if (j != src) lP += lsig(sg * lvf[j]);
+        double la, lb;
+        and_pair(lP, p, q, la, lb);
+        // AND: (marg0, marg1) = (b, a); OR: (a, b)
+        double l0 = is_or ? la : lb, l1 = is_or ? lb : la;
+        if (type >= 3) {
+            l0 += lmask(r.m0);
+            l1 += lmask(r.m1);
+        }
+        if (l0 == -kInfD && l1 == -kInfD) {  // marg == 0: the mask's one-hot fallback, else (0.5, 0.5)
+            if (type >= 3 && r.m0 == 0.0) return kInfD;
+            if (type >= 3 && r.m1 == 0.0) return -kInfD;
+            return 0.0;
+        }
+        return l1 - l0;
+    }
+    // into a body slot: AND 5 / 7, OR 6 / 8 (:289-393), in AND orientation
+    const bool is_or = (type == 6 || type == 8);
+    const double sg = is_or ? -1.0 : 1.0;
+    double lh1 = lsig(sg * lvf[h]), lh0 = lsig(-sg * lvf[h]);  // head message, oriented
+    if (type >= 7) {
+        lh1 += lmask(is_or ? r.m0 : r.m1);
+        lh0 += lmask(is_or ? r.m1 : r.m0);
+    }
+    // prod_10 = q m1h + (1 - q) m0h; the reference skips its loop when it is 0
+    const double lden = lae(std::log(q) + lh1, std::log1p(-q) + lh0);
+    if (lden == -kInfD) {
+        // scale() of (prod_1, 0): (1, 0) if prod_1 = (p - q)(m1h - m0h) > 0, else NaN
+        const double dh = (lh1 > lh0) ? 1.0 : (lh1 < lh0) ? -1.0 : 0.0;
+        return ((p - q) * dh > 0.0) ? sg * kInfD : std::numeric_limits<double>::quiet_NaN();
+    }
+    double lPo = 0.0;  // the other body slots
+    for (size_t j = s; j < e; j++)
+        if (j != src && j != h) lPo += lsig(sg * lvf[j]);
+    double la, lb;
+    and_pair(lPo, p, q, la, lb);
+    const double lnum = lae(lh1 + la, lh0 + lb);  // prod_10 + prod_1 = m1h a + m0h b
+    return sg * (lnum - lden);
+}
+
+// Damping in log-odds: (1 - d) new + d old, with exact zeros dominating and
+// opposite zeros giving (0.5, 0.5) - the probability-space rule of the
+// default mode.
+inline double damp_lodds(double nw, double old, double d) {
+    const bool ni = std::isinf(nw), oi = std::isinf(old);
+    if (ni || oi) {
+        if (ni && oi) return (nw == old) ? nw : 0.0;
+        return ni ? nw : old;
+    }
+    return (1.0 - d) * nw + d * old;
+}
+
+inline double lodds_of(double m0, double m1) { return std::log(m1) - std::log(m0); }
+
 double now_s() {
     struct timeval tv;
     gettimeofday(&tv, nullptr);
@@ -540,6 +664,14 @@ struct OBP {
     size_t iters = 0;
     double maxdiff_member = 0.0;
     bool logdomain = false;
+    // log-odds mode: f->v (variable-major) and v->f (factor-major) log-odds,
+    // per-variable finite sums; nz0 / nz1 count the +inf / -inf inputs
+    bool lodds = false;
+    std::vector<double> lfv, lvf, lS;
+    // underflow tracking (default mode): per message / variable, 1 = depends on an underflow
+    bool track = false;
+    std::vector<uint8_t> t_fv, t_vf, t_var;
+    size_t underflow_events = 0;
     // sequential schedule (updates=SEQFIX / TOPO): per batch its v->f records
     // and its f->v records (indices into L.rec); empty for PARALL
     bool seq = false;
@@ -550,6 +682,17 @@ struct OBP {
 };
 
 void bp_init(OBP &b) {  // csrc/ext/causal_bp.cu:824-856
+    if (b.lodds) {  // every message (1, 1): log-odds 0
+        b.lfv.assign(b.E, 0.0);
+        b.lvf.assign(b.E, 0.0);
+        b.lS.assign(b.V, 0.0);
+    }
+    if (b.track) {
+        b.t_fv.assign(b.E, 0);
+        b.t_vf.assign(b.E, 0);
+        b.t_var.assign(b.V, 0);
+        b.underflow_events = 0;
+    }
     double c = b.logdomain ? 0.0 : 1.0;
     std::fill(b.fv0.begin(), b.fv0.end(), c);
     std::fill(b.fv1.begin(), b.fv1.end(), c);
@@ -567,15 +710,98 @@ inline double powz(double x, double a) {  // x^a with 0^0 = 1 and 0^a = 0 for a 
     return std::pow(x, a);
 }
 
-// csrc/ext/causal_bp.cu:409-444: f->v, per-variable product, v->f.
-void bp_sweep_parall(OBP &b) {
+// Underflow tracking, f->v side: the message at variable-major position i
+// depends on an underflow if an input v->f message does, or if its
+// probability-space result (o0, o1) differs in kind (an exact zero, NaN)
+// from the log-odds evaluation of the same inputs, or by more than 1e-9 in
+// log-odds (denormal products). Inputs are the v->f messages of the factor's
+// other slots.
+uint8_t fv_taint(const OBP &b, const ORec &r, double o0, double o1, std::vector<double> &scratch) {
+    uint8_t t = 0;
+    if (r.type != 0)
+        for (size_t j = r.start; j < r.end; j++)
+            if (j != r.src) t |= b.t_vf[j];
+    if (t) return 1;
+    if (r.type == 0) return 0;
+    // log-odds of the same inputs (only the factor's own slots are read)
+    if (scratch.size() < b.E) scratch.resize(b.E);
+    for (size_t j = r.start; j < r.end; j++) scratch[j] = lodds_of(b.vf0[j], b.vf1[j]);
+    const double want = fv_message_lodds(r, scratch.data());
+    const double got = lodds_of(o0, o1);
+    if (std::isnan(want) || std::isnan(got)) return (uint8_t)(std::isnan(want) != std::isnan(got));
+    if (std::isinf(want) || std::isinf(got)) return (uint8_t)(want != got);
+    return (uint8_t)(std::fabs(want - got) > 1e-9 * std::fmax(1.0, std::fabs(want)));
+}
+
+// csrc/ext/causal_bp.cu:409-444 in log-odds (see fv_message_lodds): f->v,
+// per-variable sums with +-inf counts, v->f.
+void bp_sweep_parall_lodds(OBP &b) {
     const long E = (long)b.E, V = (long)b.V;
     const double d = b.damping;
     const ORec *rec = b.L.rec.data();
 #pragma omp parallel for schedule(dynamic, 4096) num_threads(b.nthreads)
     for (long i = 0; i < E; i++) {
+        double o = fv_message_lodds(rec[i], b.lvf.data());
+        if (d != 0.0) o = damp_lodds(o, b.lfv[i], d);
+        b.lfv[i] = o;
+    }
+    const size_t *rp = b.L.row_ptr_fv.data();
+#pragma omp parallel for schedule(dynamic, 4096) num_threads(b.nthreads)
+    for (long i = 0; i < V; i++) {  // csrc/kernel/causal_bp_parall.cu:30-52
+        double S = 0.0;
+        size_t z0 = 0, z1 = 0;
+        for (size_t j = rp[i]; j < rp[i + 1]; j++) {
+            const double x = b.lfv[j];
+            if (x == kInfD) z0++;        // m0 == 0
+            else if (x == -kInfD) z1++;  // m1 == 0
+            else S += x;                 // NaN stays NaN, as the reference's product
+        }
+        b.lS[i] = S;
+        b.nz0[i] = z0;
+        b.nz1[i] = z1;
+    }
+    const OVfRec *vr = b.L.vf.data();
+#pragma omp parallel for schedule(dynamic, 4096) num_threads(b.nthreads)
+    for (long k = 0; k < E; k++) {  // csrc/kernel/causal_bp_parall.cu:67-91
+        const OVfRec &x = vr[k];
+        const double ms = b.lfv[x.src];
+        const bool zero0 = b.nz0[x.v] - (size_t)(ms == kInfD) > 0;
+        const bool zero1 = b.nz1[x.v] - (size_t)(ms == -kInfD) > 0;
+        double o;
+        if (zero0 && zero1) o = 0.0;  // (0.5, 0.5)
+        else if (zero0) o = kInfD;
+        else if (zero1) o = -kInfD;
+        else o = b.lS[x.v] - (std::isinf(ms) ? 0.0 : ms);
+        b.lvf[x.ind] = o;
+    }
+}
+
+// csrc/ext/causal_bp.cu:409-444: f->v, per-variable product, v->f.
+void bp_sweep_parall(OBP &b) {
+    if (b.lodds) {
+        bp_sweep_parall_lodds(b);
+        return;
+    }
+    const long E = (long)b.E, V = (long)b.V;
+    const double d = b.damping;
+    const ORec *rec = b.L.rec.data();
+    std::vector<uint8_t> t_fv_new(b.track ? b.E : 0);
+    size_t events = 0;
+#pragma omp parallel for schedule(dynamic, 4096) num_threads(b.nthreads) reduction(+ : events)
+    for (long i = 0; i < E; i++) {
         double o0, o1;
         fv_message(rec[i], b.vf0.data(), b.vf1.data(), o0, o1);
+        if (b.track) {
+            thread_local std::vector<double> scratch;
+            const uint8_t t = fv_taint(b, rec[i], o0, o1, scratch);
+            t_fv_new[i] = t | (d != 0.0 ? b.t_fv[i] : 0);
+            if (t && rec[i].type != 0) {
+                bool in = false;
+                for (size_t j = rec[i].start; j < rec[i].end; j++)
+                    if (j != rec[i].src) in |= b.t_vf[j] != 0;
+                events += in ? 0 : 1;
+            }
+        }
         if (d != 0.0) {
             double n0 = powz(o0, 1.0 - d) * powz(b.fv0[i], d);
             double n1 = powz(o1, 1.0 - d) * powz(b.fv1[i], d);
@@ -590,8 +816,9 @@ void bp_sweep_parall(OBP &b) {
         b.fv0[i] = o0;
         b.fv1[i] = o1;
     }
+    if (b.track) b.t_fv.swap(t_fv_new);
     const size_t *rp = b.L.row_ptr_fv.data();
-#pragma omp parallel for schedule(dynamic, 4096) num_threads(b.nthreads)
+#pragma omp parallel for schedule(dynamic, 4096) num_threads(b.nthreads) reduction(+ : events)
     for (long i = 0; i < V; i++) {  // csrc/kernel/causal_bp_parall.cu:30-52
         double pr0 = 1.0, pr1 = 1.0;
         size_t z0 = 0, z1 = 0;
@@ -607,7 +834,16 @@ void bp_sweep_parall(OBP &b) {
         b.prod1[i] = pr1;
         b.nz0[i] = z0;
         b.nz1[i] = z1;
+        if (b.track) {  // the variable's totals depend on every incoming message; a product that
+                        // reached zero without an exact-zero input underflowed here
+            uint8_t t = 0;
+            for (size_t j = rp[i]; j < rp[i + 1]; j++) t |= b.t_fv[j];
+            const bool uf = (pr0 == 0 && z0 == 0) || (pr1 == 0 && z1 == 0);
+            events += (uf && !t) ? 1 : 0;
+            b.t_var[i] = t | (uint8_t)uf;
+        }
     }
+    if (b.track) b.underflow_events += events;
     const OVfRec *vr = b.L.vf.data();
 #pragma omp parallel for schedule(dynamic, 4096) num_threads(b.nthreads)
     for (long k = 0; k < E; k++) {  // csrc/kernel/causal_bp_parall.cu:67-91
@@ -623,6 +859,7 @@ void bp_sweep_parall(OBP &b) {
         double pr = pr0 + pr1;
         b.vf0[x.ind] = pr0 / pr;
         b.vf1[x.ind] = pr1 / pr;
+        if (b.track) b.t_vf[x.ind] = b.t_var[x.v];
     }
 }
 
@@ -825,6 +1062,7 @@ void bp_sweep_seq(OBP &b) {
 }
 
 void bp_sweep(OBP &b) {
+    if (b.seq && (b.lodds || b.track)) throw std::runtime_error("the log-odds mode and underflow tracking are PARALL only");
     if (b.seq) bp_sweep_seq(b);
     else bp_sweep_parall(b);
 }
@@ -832,6 +1070,17 @@ void bp_sweep(OBP &b) {
 // csrc/ext/causal_bp.cu:483-515 with getBeliefsV (causal_bp_seq.cu:102-111).
 void bp_beliefs(const OBP &b, std::vector<double> &out) {
     out.resize(b.V);
+    if (b.lodds) {  // b_s = P_s [zeros_s == 0], belief = b1 / (b0 + b1), from the log-odds sum
+        for (size_t i = 0; i < b.V; i++) {
+            const bool z0 = b.nz0[i] != 0, z1 = b.nz1[i] != 0;
+            const double S = b.lS[i];
+            out[i] = (z0 && z1) ? std::numeric_limits<double>::quiet_NaN()
+                     : z0       ? 1.0
+                     : z1       ? 0.0
+                     : (S >= 0 ? 1.0 / (1.0 + std::exp(-S)) : std::exp(S) / (1.0 + std::exp(S)));
+        }
+        return;
+    }
     for (size_t i = 0; i < b.V; i++) {
         double x = b.prod0[i] * (double)(!b.nz0[i]);
         double y = b.prod1[i] * (double)(!b.nz1[i]);
@@ -1133,6 +1382,27 @@ void *orc_bp_create(void *g, double damping, int nthreads, int logdomain) {
     b->logdomain = logdomain != 0;
     return b;
 }
+
+// Arithmetic mode (takes effect at the next init): 0 the reference's
+// probability-space arithmetic, 1 log-odds (no underflow), 2 the reference's
+// arithmetic with underflow tracking.
+int orc_bp_set_mode(void *b, int mode) {
+    auto &B = *(OBP *)b;
+    if (mode < 0 || mode > 2) return -1;
+    B.lodds = mode == 1;
+    B.track = mode == 2;
+    return 0;
+}
+
+// Underflow tracking: per variable 1 if its belief depends on an underflow;
+// returns the number of underflow events since init (messages or totals that
+// underflowed from inputs that did not).
+int64_t orc_bp_underflow(void *b, uint8_t *var_taint) {
+    auto &B = *(OBP *)b;
+    if (!B.track) return -1;
+    for (size_t i = 0; i < B.V; i++) var_taint[i] = B.t_var.empty() ? 0 : B.t_var[i];
+    return (int64_t)B.underflow_events;
+}
 void orc_bp_free(void *b) { delete (OBP *)b; }
 int64_t orc_bp_nr_vars(void *b) { return (int64_t)((OBP *)b)->V; }
 int64_t orc_bp_nr_slots(void *b) { return (int64_t)((OBP *)b)->E; }
@@ -1181,6 +1451,21 @@ void orc_bp_current_beliefs(void *b, double *out) {
 // Messages: f->v in variable-major order, v->f in factor-major order.
 void orc_bp_messages(void *b, double *fv0, double *fv1, double *vf0, double *vf1) {
     auto &B = *(OBP *)b;
+    if (B.lodds) {  // normalised pairs of the log-odds
+        auto pair = [](double l, double &m0, double &m1) {
+            if (std::isnan(l)) {
+                m0 = m1 = l;
+                return;
+            }
+            m1 = std::exp(lsig(l));
+            m0 = std::exp(lsig(-l));
+        };
+        for (size_t k = 0; k < B.E; k++) {
+            pair(B.lfv[k], fv0[k], fv1[k]);
+            pair(B.lvf[k], vf0[k], vf1[k]);
+        }
+        return;
+    }
     for (size_t k = 0; k < B.E; k++) {
         fv0[k] = B.fv0[k];
         fv1[k] = B.fv1[k];

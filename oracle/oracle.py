@@ -93,6 +93,10 @@ def lib():
         L.orc_bp_set_schedule.argtypes = [_vp, C.c_int, C.c_uint32]
         L.orc_bp_set_schedule.restype = C.c_int64
         L.orc_bp_schedule.argtypes = [_vp, _i64p, _i64p]
+        L.orc_bp_set_mode.argtypes = [_vp, C.c_int]
+        L.orc_bp_set_mode.restype = C.c_int
+        L.orc_bp_underflow.argtypes = [_vp, np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")]
+        L.orc_bp_underflow.restype = C.c_int64
         _lib = L
     return _lib
 
@@ -231,13 +235,35 @@ class RefGraph(_GraphBase):
 
 class OracleBP:
     """FP64 CausalBP restatement over an OracleGraph: updates=PARALL, or after
-    set_schedule() the sequential SEQFIX / TOPO schedules."""
+    set_schedule() the sequential SEQFIX / TOPO schedules.
 
-    def __init__(self, g: OracleGraph, damping: float = 0.0, threads: int = 1, logdomain: bool = False):
+    arith: "reference" (the reference's probability-space arithmetic, which
+    underflows to exact zeros beyond log-odds of about +-745), "lodds" (the
+    same PARALL recurrence in FP64 log-odds: no underflow) or "track" (the
+    reference's arithmetic, marking every belief that depends on an
+    underflow; see underflow()). `logdomain` is the reference's own property
+    of that name (messages initialised to (0, 0))."""
+
+    ARITH = {"reference": 0, "lodds": 1, "track": 2}
+
+    def __init__(self, g: OracleGraph, damping: float = 0.0, threads: int = 1, logdomain: bool = False,
+                 arith: str = "reference"):
         self.L = lib()
         self.h = self.L.orc_bp_create(g.h, float(damping), int(threads), 1 if logdomain else 0)
         self.V = int(self.L.orc_bp_nr_vars(self.h))
         self.E = int(self.L.orc_bp_nr_slots(self.h))
+        if self.L.orc_bp_set_mode(self.h, self.ARITH[arith]) != 0:
+            raise ValueError("unknown arithmetic mode " + arith)
+        self.arith = arith
+
+    def underflow(self):
+        """(per-variable flags: the belief depends on an underflow, number of
+        underflow events since init()) of a "track" run."""
+        t = np.zeros(self.V, np.uint8)
+        n = int(self.L.orc_bp_underflow(self.h, t))
+        if n < 0:
+            raise RuntimeError("underflow tracking needs arith='track'")
+        return t.astype(bool), n
 
     def __del__(self):
         if getattr(self, "h", None):

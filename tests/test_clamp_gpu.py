@@ -162,3 +162,35 @@ def test_gradient_after_clamps_matches_rebuilt_graph():
     scale = max(np.max(np.abs(gp_ref[same])), 1e-300)
     assert scale > 0
     assert np.max(np.abs(gp_eng[same] - gp_ref[same])) <= 1e-8 * scale
+
+
+@pytest.mark.parametrize("prec,tol", [(64, 1e-9), (32, 1e-5)])
+def test_clamp_matches_oracle(prec, tol):
+    """The incremental clamp against the FP64 oracle run on the clamped and
+    rebuilt graph (CausalFactorGraph::clamp on every neighbouring factor, then
+    a new graph from its factors, as fl_wrapper.cu:29-45 does): beliefs after
+    a fixed run, and the tolerance loop's sweep count and beliefs."""
+    import oracle as O
+
+    fl = _bingo()
+    clamps = _clamps(fl, 60, seed=12)
+    og = O.OracleGraph.from_factors(fl)
+    og.clamp_labels(clamps)
+    og = og.rebuild()
+    eng = _incremental(fl, clamps, batches=3, precision=prec)
+    ref = O.OracleBP(og)
+    ref.init()
+    ref.run_fixed(1e-9, 30, 1)
+    eng.init()
+    eng.run_fixed(30)
+    want, got = ref.beliefs(), eng.beliefs()
+    assert np.array_equal(np.isnan(want), np.isnan(got))
+    ok = ~np.isnan(want)
+    assert np.max(np.abs(got[ok] - want[ok])) <= tol
+    ref.init()
+    ref.run(1e-6, 400, 1e9)
+    eng.init()
+    info = eng.run_tol(1e-6, 400, 1e9)
+    # FP32 rounding may move the last residual across tol by one sweep
+    assert abs(info["sweeps"] - ref.iters) <= (0 if prec == 64 else 1)
+    assert np.max(np.abs(eng.beliefs()[ok] - ref.beliefs()[ok])) <= max(tol, 1e-6)

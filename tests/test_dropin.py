@@ -1,10 +1,13 @@
 """FastLBP's own example drivers as drop-in clients of this library.
 
 The CPU test compiles examples/fl_wrapper.cu, bingo_wrapper.cu, example_ext.cu
-and example_ext_clamp.cu from the FastLBP sources, unchanged, against this
-repository's include/ and links them to libfastlbp_b200.so (bingo_wrapper
-also to NVML, as FastLBP's own build does). It needs the FastLBP sources and
-is skipped without them.
+and example_ext_clamp.cu from the FastLBP sources (the directory named by the
+FASTLBP_REF environment variable), unchanged, against this repository's
+include/ and links them to libfastlbp_b200.so (bingo_wrapper also to NVML, as
+FastLBP's own build does). Without FASTLBP_REF it checks the same four
+programs as the build step made them (oracle/_ref/examples, by
+`make -C oracle examples` from the unchanged sources): present, and linked
+to libfastlbp_b200.so. Without either it is skipped.
 
 The GPU test runs fl_wrapper built that way (oracle/_ref/examples, made by
 `make -C oracle examples`) on a golden case whose beliefs FastLBP's own code
@@ -22,13 +25,24 @@ import subprocess
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_EXAMPLES = os.path.join(os.environ.get("FASTLBP_REF", "/root/reference"), "examples")
+REF_EXAMPLES = os.path.join(os.environ["FASTLBP_REF"], "examples") if os.environ.get("FASTLBP_REF") else ""
+BUILT_EXAMPLES = os.path.join(ROOT, "oracle", "_ref", "examples")
 EXAMPLES = ["fl_wrapper", "bingo_wrapper", "example_ext", "example_ext_clamp"]
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_EXAMPLES) or shutil.which("nvcc") is None,
-                    reason="FastLBP example sources or nvcc not available")
+@pytest.mark.skipif(bool(REF_EXAMPLES) or not all(os.path.exists(os.path.join(BUILT_EXAMPLES, n)) for n in EXAMPLES)
+                    or shutil.which("readelf") is None,
+                    reason="FASTLBP_REF is set (the sources are compiled below) or the build step made no examples")
+def test_built_examples_link_this_library():
+    for name in EXAMPLES:
+        r = subprocess.run(["readelf", "-d", os.path.join(BUILT_EXAMPLES, name)], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        assert "[libfastlbp_b200.so]" in r.stdout, name
+
+
+@pytest.mark.skipif(not REF_EXAMPLES or not os.path.isdir(REF_EXAMPLES) or shutil.which("nvcc") is None,
+                    reason="FASTLBP_REF (FastLBP sources) or nvcc not available")
 def test_reference_examples_compile_unchanged(tmp_path):
     lib = os.path.join(ROOT, "fastlbp_b200", "libfastlbp_b200.so")
     assert os.path.exists(lib)

@@ -155,3 +155,17 @@ def test_expand_shared():
     p = expand_shared(torch.tensor([0.1, 0.2, 0.3], dtype=torch.float64), rf,
                       torch.tensor([0.9, 0.8, 0.7, 0.6, 0.5], dtype=torch.float64))
     assert p.tolist() == [0.3, 0.8, 0.1, 0.3, 0.5]
+
+
+def test_rule_indices_out_of_range_are_rejected():
+    """A rule index outside [-1, n_rules) raises ValueError on the host before
+    any index_add_ (on a CUDA tensor that would be a device-side assert)."""
+    import torch
+
+    g = torch.ones(3, dtype=torch.float64)
+    for bad in ([0, 3, -1], [0, -2, 1]):
+        with pytest.raises(ValueError):
+            shared_gradient(g, torch.tensor(bad), 3)
+        with pytest.raises(ValueError):
+            expand_shared(torch.zeros(3, dtype=torch.float64), torch.tensor(bad), g)
+    assert shared_gradient(g, torch.tensor([0, 2, -1]), 3).tolist() == [1.0, 0.0, 1.0]

@@ -10,7 +10,8 @@ here does not hide the other tests; it passes alone or after them.
 Checks: two calls in a row, on different graphs and settings, each agree
 with the regular engine (flbp_engine_create + flbp_run_fixed) within the
 FP32 tolerance of the other tests, and the second call leaves the device's
-free memory unchanged.
+free memory unchanged; the solve agrees with the FP64 oracle on a clamped
+graph and with the engine on a head clamped both ways.
 """
 
 import ctypes as C
@@ -102,3 +103,45 @@ def test_oversized_graph_is_rejected():
     rc = _native.lib().flbp_run_fixed_device_noalloc(C.byref(d), 1, 0.0, C.c_void_p(C.addressof(out)), None)
     assert rc == 5
     assert b"at most" in _native.lib().flbp_last_error()
+
+
+def test_against_the_oracle_and_a_doubly_clamped_head():
+    """The allocation-free solve against the FP64 oracle on a clamped graph
+    (1e-5), and against the engine on a graph whose head is clamped both
+    ways (head mask (0,0), state 3): the reference's head fallback gives
+    (0, 1) there and its body messages are NaN (0/0); NaN patterns and the
+    finite beliefs must agree."""
+    torch = pytest.importorskip("torch")
+    import oracle as O
+
+    fl = workloads.config0(3)
+    clamps = {int(x): (i + 1) % 2 for i, x in enumerate(fl.alarms)}
+    g = CausalFactorGraph.from_factors(fl)
+    g.clamp_labels(clamps)
+    g = g.rebuild()
+    og = O.OracleGraph.from_factors(fl)
+    og.clamp_labels(clamps)
+    og = og.rebuild()
+    d, keep, _ = device_graph(g, torch)
+    got = solve_noalloc(d, 60, 0.0, torch)
+    ref = O.OracleBP(og)
+    ref.init()
+    ref.run_fixed(1e-9, 60, 1)
+    want = ref.beliefs()
+    assert np.array_equal(np.isnan(got), np.isnan(want))
+    ok = ~np.isnan(want)
+    assert np.max(np.abs(got[ok] - want[ok])) <= TOL32
+
+    g2 = CausalFactorGraph.from_factors(fl)
+    head = g2.findVar(int(fl.alarms[0]))
+    g2.clamp(head, 0)
+    g2.clamp(head, 1)
+    g2 = g2.rebuild()
+    info = g2.factor_info()
+    assert ((info["mask0"] == 0) & (info["mask1"] == 0)).any()
+    d2, keep2, a2 = device_graph(g2, torch)
+    got2 = solve_noalloc(d2, 4, 0.0, torch)
+    want2 = solve_engine(a2, 4, 0.0)
+    assert np.array_equal(np.isnan(got2), np.isnan(want2))
+    ok2 = ~np.isnan(want2)
+    assert ok2.any() and np.max(np.abs(got2[ok2] - want2[ok2])) <= TOL32

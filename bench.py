@@ -805,7 +805,7 @@ def run_ours(args, rank, world, local):
     V = int(arr["n_vars"])
     stream = torch.cuda.current_stream()
     eng = Engine(arr, precision=args.precision, damping=args.damping, stream=stream.cuda_stream)
-    tuned = eng.autotune(args.sweeps) if hasattr(eng, "autotune") else None
+    tuned = eng.autotune(args.sweeps)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     total_ms, launches, clk = sweep_timing(eng, args, stream, flush, world)
@@ -940,10 +940,10 @@ def batched_record(args, rank, world, local):
     arrays = arrays_parallel("batch", mine)
     be = BatchEngine(arrays, precision=32)
     plain = [Engine(a, precision=32) for a in arrays]
-    tuned = be.autotune_batch(tol, maxiter) if hasattr(be, "autotune_batch") else None
-    for e in plain:
-        if tuned:
-            e.set_tuning(tuned["factor_form"], tuned["var_form"])
+    tuned = be.autotune_batch(tol, maxiter)
+    for e in plain:  # each plain engine takes the tuner's choice for its size class (timed once per class)
+        e.autotune(maxiter, tol=tol, reps=2)
+    plain_forms = sorted({(e.tuning()["factor_form"], e.tuning()["var_form"]) for e in plain})
     be.init()
     be.run_batch_tol(tol, maxiter)  # captures the sweep graphs
     for e in plain:
@@ -979,7 +979,7 @@ def batched_record(args, rank, world, local):
            "sweeps": {"min": int(sweeps.min()), "median": float(np.median(sweeps)), "max": int(sweeps.max()),
                       "same_as_plain": bool(sweeps.tolist() == psweeps)},
            "max_belief_diff_batched_vs_plain": diff, "seconds": {"batched": t_b, "plain": t_p},
-           "kernel_forms": be.tuning(), "autotune": tuned, "clocks": clk,
+           "kernel_forms": be.tuning(), "plain_kernel_forms": [list(x) for x in plain_forms], "clocks": clk,
            "scaling": "strong: the graphs are dealt to the ranks"}
     be.close()
     for e in plain:

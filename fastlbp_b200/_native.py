@@ -136,6 +136,7 @@ def lib():
         "flbp_set_seq_kernel": [_vp, C.c_int32],
         "flbp_set_tuning": [_vp, P(Tuning)],
         "flbp_get_tuning": [_vp, P(Tuning)],
+        "flbp_autotune": [_vp, C.c_int32, C.c_int64, C.c_double, C.c_int32, P(Tuning)],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -164,4 +165,4 @@ EXPORTED = ["flbp_last_error", "flbp_version", "flbp_engine_create", "flbp_engin
             "flbp_batch_run_tol", "flbp_adjoint_forward", "flbp_adjoint_backward", "flbp_set_factor_probs",
             "flbp_adjoint_backward_device", "flbp_get_beliefs_device", "flbp_clamp_vars", "flbp_layout_digest",
             "flbp_update_seq", "flbp_shuffled_factors", "flbp_seq_batches", "flbp_set_update_seq", "flbp_update_info",
-            "flbp_set_seq_kernel", "flbp_set_tuning", "flbp_get_tuning"]
+            "flbp_set_seq_kernel", "flbp_set_tuning", "flbp_get_tuning", "flbp_autotune"]

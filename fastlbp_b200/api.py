@@ -364,10 +364,11 @@ class Engine:
         return m0, m1
 
     def stats(self) -> Dict[str, int]:
-        c = np.zeros(14, np.int64)
+        c = np.zeros(18, np.int64)
         check(lib().flbp_engine_stats(self._h, c, c.size))
         keys = ["vars", "factors", "slots", "active_factors", "active_slots", "warp_factors", "warp_vars", "bytes",
-                "h2d_bytes", "launches", "huge_factors", "huge_vars", "big_factor_tiles", "big_var_tiles"]
+                "h2d_bytes", "launches", "huge_factors", "huge_vars", "big_factor_tiles", "big_var_tiles",
+                "create_us_layout", "create_us_alloc", "create_us_upload", "create_us_rest"]
         return dict(zip(keys, (int(x) for x in c)))
 
     # gradients through unrolled sweeps --------------------------------------
@@ -435,6 +436,18 @@ class Engine:
         """Form of each sweep pass: 0 staged, 1 or 2 direct (flbp_set_tuning)."""
         t = N.Tuning(int(factor_form), int(var_form), 0, 0)
         N.check(N.lib().flbp_set_tuning(self.h, C.byref(t)))
+
+    def autotune(self, sweeps: int = 200, tol: Optional[float] = None, reps: int = 3) -> Dict[str, int]:
+        """Time the pass forms on this graph and keep the fastest (flbp_autotune):
+        whole fixed-sweep runs, or whole tolerance runs when tol is given."""
+        t = N.Tuning()
+        check(lib().flbp_autotune(self._h, 0 if tol is None else 1, int(sweeps), float(tol or 0.0), int(reps),
+                                  C.byref(t)))
+        return {k: getattr(t, k) for k, _ in t._fields_}
+
+    def autotune_batch(self, tol: float = 1e-6, maxiter: int = 500, reps: int = 2) -> Dict[str, int]:
+        """autotune over whole batched tolerance runs (flbp_batch_run_tol)."""
+        return self.autotune(maxiter, tol=tol, reps=reps)
 
     def tuning(self) -> Dict[str, int]:
         t = N.Tuning()

@@ -4,13 +4,16 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstddef>
 #include <cstring>
 #include <limits>
 #include <map>
+#include <mutex>
 #include <new>
+#include <tuple>
 #include <string>
 #include <unordered_set>
 #include <utility>
@@ -133,6 +136,9 @@ struct flbp_engine {
     bool lowpass_valid = false;
     size_t bytes = 0;
     size_t h2d_bytes = 0;  // host->device bytes copied by create
+    // wall time (us) of the phases of create: host layout, device allocation,
+    // host->device copies (with the host-side packing they need), the rest
+    int64_t create_us[4] = {0, 0, 0, 0};
 
     // Per-kernel timing mode: sweeps are launched without graphs, with events
     // around each pass; collect_kernel_times() folds them into kt_ms / kt_n.
@@ -704,6 +710,11 @@ void packed_priors(const flbp_engine *e, size_t nv_pad, std::vector<uint32_t> &p
 
 int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, flbp_engine **out,
                   const BatchSpec *batch) {
+    auto clk = [] { return std::chrono::steady_clock::now(); };
+    auto us = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+        return (int64_t)std::chrono::duration_cast<std::chrono::microseconds>(b - a).count();
+    };
+    const auto t_begin = clk();
     if (!graph || !out) {
         set_error("null argument");
         return FLBP_ERR_INVALID;
@@ -727,7 +738,9 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
     std::string err;
     GraphIds ids{0, nullptr, nullptr};
     if (batch) ids = GraphIds{(uint32_t)(batch->var_off.size() - 1), batch->factor_graph.data(), batch->var_graph.data()};
+    auto tc0 = clk();
     int rc = build_layout(*graph, e->L, err, batch ? &ids : nullptr);
+    e->create_us[0] = us(tc0, clk());
     if (rc) {
         set_error(err);
         delete e;
@@ -808,6 +821,7 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
     const size_t psz = e->prec == 64 ? 16 : 8;
     e->n_ent = std::max<size_t>(1, L.v_ent.size());
     const size_t ne = e->n_ent;
+    auto tc1 = clk();
     if ((rc = dalloc(e, (char **)&e->d_vf, ns * e->tsize)) || (rc = dalloc(e, (char **)&e->d_fv, ne * e->tsize)) ||
         (damp && (rc = dalloc(e, (char **)&e->d_fvd, ne * e->tsize))) || (rc = dalloc(e, &e->d_f_pos, ns)) ||
         (rc = dalloc(e, (char **)&e->d_f_pq, 2 * nf_pad * e->tsize)) ||
@@ -829,6 +843,8 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
         return fail(FLBP_ERR_NOMEM);
     }
     std::memset(e->h_ctl, 0, sizeof(Ctl));
+    auto tc2 = clk();
+    e->create_us[1] = us(tc1, tc2);
     std::vector<uint32_t> prior, bt_prior;
     packed_priors(e, nv_pad, prior, bt_prior);
     std::vector<uint8_t> kind_pad(nf_pad, 0), deg_pad(nf_pad, 0);
@@ -865,8 +881,12 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
         (rc = upload(e, e->d_int_of_var, L.internal_of_var)) || (rc = dalloc(e, &e->d_ref_out, (size_t)L.V)))
         return fail(rc);
     cudaError_t ce = cudaSuccess;
-    if ((ce = cudaStreamSynchronize(e->stream)) != cudaSuccess ||
-        (ce = cudaMemsetAsync(e->d_belief, 0, std::max<size_t>(1, nv_pad) * sizeof(double), e->stream)) != cudaSuccess ||
+    if ((ce = cudaStreamSynchronize(e->stream)) != cudaSuccess) {
+        set_error(std::string("device initialisation failed: ") + cudaGetErrorString(ce));
+        return fail(FLBP_ERR_CUDA);
+    }
+    e->create_us[2] = us(tc2, clk());
+    if ((ce = cudaMemsetAsync(e->d_belief, 0, std::max<size_t>(1, nv_pad) * sizeof(double), e->stream)) != cudaSuccess ||
         (ce = cudaMemsetAsync(e->d_vf, 0, ns * e->tsize, e->stream)) != cudaSuccess ||
         (ce = cudaMemsetAsync(e->d_fv, 0, ne * e->tsize, e->stream)) != cudaSuccess ||
         (damp && (ce = cudaMemsetAsync(e->d_fvd, 0, ne * e->tsize, e->stream)) != cudaSuccess) ||
@@ -896,6 +916,7 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
         FLBP_CUDA(cudaMemsetAsync(e->d_gstate, 0, 4 * sizeof(int) * std::max<size_t>(1, e->n_graphs), e->stream));
         FLBP_CUDA(cudaStreamSynchronize(e->stream));
     }
+    e->create_us[3] = us(t_begin, clk()) - e->create_us[0] - e->create_us[1] - e->create_us[2];
     *out = e;
     return FLBP_OK;
 }
@@ -1283,12 +1304,13 @@ int flbp_engine_stats(flbp_engine *e, int64_t *c, int64_t n) {
         set_error("null argument");
         return FLBP_ERR_INVALID;
     }
-    const int64_t v[14] = {e->L.V, e->L.F, e->L.E, (int64_t)(e->L.nf_sell + e->L.nf_big),
+    const int64_t v[18] = {e->L.V, e->L.F, e->L.E, (int64_t)(e->L.nf_sell + e->L.nf_big),
                            (int64_t)e->L.n_active_slots, (int64_t)e->L.nf_big, (int64_t)e->L.nv_big,
                            (int64_t)e->bytes, (int64_t)e->h2d_bytes, (int64_t)e->launches,
                            (int64_t)e->L.nf_huge, (int64_t)e->L.nv_huge, (int64_t)e->L.n_fbtiles,
-                           (int64_t)e->L.n_vbtiles};
-    for (int64_t i = 0; i < n && i < 14; i++) c[i] = v[i];
+                           (int64_t)e->L.n_vbtiles, e->create_us[0], e->create_us[1], e->create_us[2],
+                           e->create_us[3]};
+    for (int64_t i = 0; i < n && i < 18; i++) c[i] = v[i];
     return FLBP_OK;
 }
 
@@ -1334,6 +1356,122 @@ int flbp_get_tuning(flbp_engine *e, flbp_tuning *t) {
     t->var_form = e->v_form;
     t->factor_blocks = e->f_form ? e->f_grid_direct : e->factor_grid;
     t->var_blocks = e->v_form ? e->v_grid_direct : e->var_grid;
+    return FLBP_OK;
+}
+
+// ---- autotuner: the form of each pass, timed on the engine's own graph ----
+
+namespace {
+
+struct TuneKey {
+    int prec, damped, batched, kind, lv, le, big;
+    bool operator<(const TuneKey &o) const {
+        return std::tie(prec, damped, batched, kind, lv, le, big) <
+               std::tie(o.prec, o.damped, o.batched, o.kind, o.lv, o.le, o.big);
+    }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, std::pair<int, int>> g_tune_cache;
+
+int ilog2(uint64_t x) {
+    int r = 0;
+    while (x > 1) {
+        x >>= 1;
+        r++;
+    }
+    return r;
+}
+
+// Size class of the graph: log2 of variables and slots, and the share of
+// slots held by items too wide for a lane (the fan-in histogram's tail) in
+// eighths.
+TuneKey tune_key(const flbp_engine *e, int kind) {
+    const HostLayout &L = e->L;
+    uint64_t wide = 0;
+    for (uint32_t b = 0; b < L.nf_big; b++) wide += L.fb_deg[b];
+    for (uint32_t b = 0; b < L.nv_big; b++) wide += L.vb_deg[b];
+    const uint64_t tot = std::max<uint64_t>(1, 2 * L.n_active_slots);
+    return TuneKey{e->prec, e->damping != 0.0 ? 1 : 0, e->n_graphs ? 1 : 0, kind, ilog2((uint64_t)L.V + 1),
+                   ilog2((uint64_t)L.E + 1), (int)std::min<uint64_t>(8, (8 * wide + tot - 1) / tot)};
+}
+
+}  // namespace
+
+int flbp_autotune(flbp_engine *e, int32_t kind, int64_t sweeps, double tol, int32_t reps, flbp_tuning *chosen) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    if ((rc = refuse_seq(e, "flbp_autotune"))) return rc;
+    if (kind < 0 || kind > 1 || sweeps < 1 || reps < 1) {
+        set_error("flbp_autotune: kind must be 0 (fixed sweeps) or 1 (tolerance run), sweeps and reps positive");
+        return FLBP_ERR_INVALID;
+    }
+    const TuneKey key = tune_key(e, kind);
+    std::pair<int, int> best{-1, -1};
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) best = it->second;
+    }
+    if (best.first < 0) {
+        // Keep what a run changes: the sweep counts and the previous beliefs
+        // of the tolerance rule (device), restored after the timing runs.
+        const long long iters0 = e->iters, t0 = e->t;
+        const bool lp0 = e->lowpass_valid;
+        const size_t nb = std::max<size_t>((size_t)e->L.V, 32ull * e->L.n_vgroups());
+        double *saved = nullptr;
+        FLBP_CUDA(cudaMalloc((void **)&saved, std::max<size_t>(1, nb) * sizeof(double)));
+        FLBP_CUDA(cudaMemcpyAsync(saved, e->d_belief, std::max<size_t>(1, nb) * sizeof(double), cudaMemcpyDeviceToDevice,
+                                  e->stream));
+        auto time_one = [&](int ff, int vf, double *ms) -> int {
+            int r = apply_forms(e, ff, vf);
+            if (r) return r;
+            std::vector<double> ts;
+            for (int i = 0; i <= reps; i++) {  // the first run captures the sweep graphs
+                if ((r = flbp_init(e))) return r;
+                e->iters = 0;
+                if (kind == 0) r = flbp_run_fixed(e, sweeps, nullptr);
+                else if (e->n_graphs) r = flbp_batch_run_tol(e, tol, sweeps, 1e9, nullptr, nullptr, nullptr);
+                else r = flbp_run_tol(e, tol, sweeps, 1e9, nullptr);
+                if (r) return r;
+                if (i > 0) ts.push_back(e->last_ms);
+            }
+            std::sort(ts.begin(), ts.end());
+            *ms = ts[ts.size() / 2];
+            return FLBP_OK;
+        };
+        // coordinate descent: the factor pass's form with the variable pass
+        // staged, then the variable pass's form with that factor form
+        double bms = 0.0, ms = 0.0;
+        int bf = 0, bv = 0;
+        rc = time_one(0, 0, &bms);
+        for (int ff = 1; ff <= 2 && !rc; ff++) {
+            rc = time_one(ff, 0, &ms);
+            if (!rc && ms < bms) bms = ms, bf = ff;
+        }
+        for (int vf = 1; vf <= 2 && !rc; vf++) {
+            rc = time_one(bf, vf, &ms);
+            if (!rc && ms < bms) bms = ms, bv = vf;
+        }
+        e->iters = iters0;
+        e->t = t0;
+        e->lowpass_valid = lp0;
+        cudaMemcpyAsync(e->d_belief, saved, std::max<size_t>(1, nb) * sizeof(double), cudaMemcpyDeviceToDevice,
+                        e->stream);
+        cudaStreamSynchronize(e->stream);
+        cudaFree(saved);
+        if (rc) return rc;
+        best = {bf, bv};
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tune_cache[key] = best;
+    }
+    if ((rc = apply_forms(e, best.first, best.second))) return rc;
+    if ((rc = flbp_init(e))) return rc;
+    if (chosen) {
+        chosen->factor_form = e->f_form;
+        chosen->var_form = e->v_form;
+        chosen->factor_blocks = e->f_form ? e->f_grid_direct : e->factor_grid;
+        chosen->var_blocks = e->v_form ? e->v_grid_direct : e->var_grid;
+    }
     return FLBP_OK;
 }
 

@@ -144,11 +144,14 @@ int flbp_get_fv_messages(flbp_engine *eng, double *m0, double *m1, int64_t n_slo
  * variable's message all the same). */
 int flbp_get_vf_messages(flbp_engine *eng, double *m0, double *m1, int64_t n_slots);
 
-/* Layout statistics: counts[0..13] = vars, factors, slots, active factors,
+/* Layout statistics: counts[0..17] = vars, factors, slots, active factors,
  * active slots, factors handled warp-wide, variables handled warp-wide,
  * bytes of device memory held, host->device bytes copied by create, engine
  * kernels launched so far, warp-wide factors too large for a tile, likewise
- * variables, tiles of warp-wide factors, tiles of warp-wide variables.
+ * variables, tiles of warp-wide factors, tiles of warp-wide variables, and
+ * the wall time (microseconds) of create's phases: host layout, device
+ * allocation, host->device copies (with their host-side packing), and the
+ * rest (device and stream set-up, kernel configuration, initial state).
  * Entries past n_counts are not written. */
 int flbp_engine_stats(flbp_engine *eng, int64_t *counts, int64_t n_counts);
 
@@ -184,6 +187,21 @@ typedef struct flbp_tuning {
 
 int flbp_set_tuning(flbp_engine *eng, const flbp_tuning *tuning);
 int flbp_get_tuning(flbp_engine *eng, flbp_tuning *tuning);
+
+/* Autotuner: times the forms of the two passes on this engine's own graph
+ * and installs the fastest (coordinate descent: the factor pass's form
+ * first, then the variable pass's). kind 0 times whole fixed-sweep runs
+ * (init + `sweeps` sweeps + beliefs); kind 1 whole tolerance runs (tol,
+ * maxiter = sweeps; batched engines: flbp_batch_run_tol, whose cost changes
+ * as graphs stop, which is why whole runs are timed). Each candidate runs
+ * once to capture its graphs, then `reps` timed runs; the median decides.
+ * The choice is cached in the process by precision, damping, batching,
+ * kind and a size class of the graph (log2 of variables and slots, share of
+ * slots in warp-wide items), and later engines of the same class take it
+ * without timing. The engine is left as flbp_init leaves it, with its sweep
+ * count and previous beliefs as before the call. No counterpart in FastLBP
+ * (it hard-codes kCudaThreadsNum = 128, include/utils/cuda_utils.h:23). */
+int flbp_autotune(flbp_engine *eng, int32_t kind, int64_t sweeps, double tol, int32_t reps, flbp_tuning *chosen);
 
 /* ------------------------------------------------------------------------
  * Allocation-free solve. No counterpart in FastLBP.

@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(kDirectThreads, MINB) factor_direct_kernel(Fac
     if (blockIdx.x == 0 && threadIdx.x == 0) sweep_open(ctl);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     {
-        __shared__ double s_l[kConsumerWarps];
+        __shared__ typename WideAcc<T>::type s_l[kConsumerWarps];
         __shared__ int s_nz[kConsumerWarps];
         for (uint32_t b = blockIdx.x; b < a.nf_huge; b += gridDim.x)
             factor_block_huge<T>(a, b, threadIdx.x, vf, fv, s_l, s_nz);
@@ -175,7 +175,8 @@ __device__ __forceinline__ double var_group_direct(const VarArgs &a, const T *__
         for (int k = 0; k < W; k++) en[k] = ld_stream(a.v_ent + base + 32u * k + lane);
     }
     const bool real = v < a.nv_sell;
-    double S = 0.0;
+    typedef typename NarrowAcc<T>::type A;
+    A S = AccOps<A>::zero();
     int npos = 0, nneg = 0;
     if (real) decode_prior<T>(a.prior, v, pscale, S, npos, nneg);
     const double bold = (RESID && real) ? a.belief[v] : 0.0;
@@ -190,10 +191,10 @@ __device__ __forceinline__ double var_group_direct(const VarArgs &a, const T *__
         }
         if (xv == inf) npos++;
         else if (xv == -inf) nneg++;
-        else S += (double)xv;
+        else AccOps<A>::add(S, xv);
     }
     double dd = 0.0;
-    if (real) dd = var_finish<BMODE>(a, v, S, npos, nneg, tol, bold, cnt);
+    if (real) dd = var_finish<BMODE>(a, v, AccOps<A>::value(S), npos, nneg, tol, bold, cnt);
     if (WRITE_VF) {
 #pragma unroll
         for (int k = 0; k < W; k++)
@@ -229,7 +230,9 @@ __device__ __forceinline__ double var_warp_direct(const VarArgs &a, uint32_t b, 
     const uint32_t v = a.nv_sell + b, k0 = __ldcs(a.vb_off + b), k1 = k0 + __ldcs(a.vb_deg + b);
     const T inf = Num<T>::inf();
     const T *src = DAMP ? fvd : fv;  // after the first loop, fvd holds the messages in use
-    double S = 0.0;
+    typedef typename WideAcc<T>::type A;
+    typedef AccOps<A> O;
+    A S = O::zero();
     int npos = 0, nneg = 0;
     for (uint32_t k = k0 + lane; k < k1; k += 32) {
         T x = fv[k];
@@ -239,18 +242,18 @@ __device__ __forceinline__ double var_warp_direct(const VarArgs &a, uint32_t b, 
         }
         if (x == inf) npos++;
         else if (x == -inf) nneg++;
-        else S += (double)x;
+        else O::add(S, x);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        S += __shfl_xor_sync(0xffffffffu, S, o);
+        O::combine(S, O::shfl_xor(S, o));
         npos += __shfl_xor_sync(0xffffffffu, npos, o);
         nneg += __shfl_xor_sync(0xffffffffu, nneg, o);
     }
-    double S0;
+    A S0;
     int p0, n0;
     decode_prior<T>(a.prior, v, pscale, S0, p0, n0);
-    S += S0;
+    O::combine(S, S0);
     npos += p0;
     nneg += n0;
     if (WRITE_VF) {
@@ -259,7 +262,7 @@ __device__ __forceinline__ double var_warp_direct(const VarArgs &a, uint32_t b, 
             if (e != kSentinel) vf[e] = excl_msg<T>(S, npos, nneg, src[k]);
         }
     }
-    return (lane == 0) ? var_finish<BMODE>(a, v, S, npos, nneg, tol, RESID ? a.belief[v] : 0.0, cnt) : 0.0;
+    return (lane == 0) ? var_finish<BMODE>(a, v, O::value(S), npos, nneg, tol, RESID ? a.belief[v] : 0.0, cnt) : 0.0;
 }
 
 // Variable pass, direct form: variables too large for a warp first (one per
@@ -285,7 +288,7 @@ __global__ void __launch_bounds__(kDirectThreads, MINB) var_direct_kernel(VarArg
     if (a.v_graph) load_done_bits(s_done, a.gstate, a.n_graphs, lane, wid, blockDim.x >> 5);
     __syncthreads();
     {
-        __shared__ double s_s[kConsumerWarps];
+        __shared__ typename WideAcc<T>::type s_s[kConsumerWarps];
         __shared__ int s_np[kConsumerWarps], s_nn[kConsumerWarps];
         for (uint32_t b = blockIdx.x; b < a.nv_huge; b += gridDim.x) {
             const uint32_t g = a.v_graph ? a.v_graph[a.nv_sell + b] : 0;

@@ -230,6 +230,90 @@ struct VarArgs {
     uint32_t n_graphs;
 };
 
+// ------------------------------------------------------------ accumulators
+//
+// Sums of log-odds (a variable's incoming messages and prior) and of
+// log-sigmoids (a large factor's body). FP64 engines sum in double. FP32
+// engines keep the sweep in FP32: a plain float sum where at most 16 terms
+// meet (the sliced-ELL variables), and a compensated two-float sum
+// (Neumaier's variant of Kahan summation) for wider items, whose error does
+// not grow with the number of terms. FP64 then appears in an FP32 sweep only
+// in the residual and in the belief normalisation (belief_of).
+struct F2 {
+    float hi, lo;  // value = hi + lo
+};
+
+template <typename A>
+struct AccOps;
+
+template <>
+struct AccOps<double> {
+    static __device__ __forceinline__ double zero() { return 0.0; }
+    static __device__ __forceinline__ double of(double x) { return x; }
+    static __device__ __forceinline__ void add(double &s, double x) { s += x; }
+    static __device__ __forceinline__ void combine(double &s, double o) { s += o; }
+    static __device__ __forceinline__ double value(double s) { return s; }
+    // s - x rounded once to the message type
+    template <typename T>
+    static __device__ __forceinline__ T excl(double s, T x) {
+        return (T)(s - (double)x);
+    }
+    static __device__ __forceinline__ double shfl_xor(double s, int o) { return __shfl_xor_sync(0xffffffffu, s, o); }
+};
+
+template <>
+struct AccOps<float> {
+    static __device__ __forceinline__ float zero() { return 0.f; }
+    static __device__ __forceinline__ float of(float x) { return x; }
+    static __device__ __forceinline__ void add(float &s, float x) { s += x; }
+    static __device__ __forceinline__ void combine(float &s, float o) { s += o; }
+    static __device__ __forceinline__ double value(float s) { return (double)s; }
+    template <typename T>
+    static __device__ __forceinline__ T excl(float s, T x) {
+        return (T)(s - (float)x);
+    }
+    static __device__ __forceinline__ float shfl_xor(float s, int o) { return __shfl_xor_sync(0xffffffffu, s, o); }
+};
+
+template <>
+struct AccOps<F2> {
+    static __device__ __forceinline__ F2 zero() { return F2{0.f, 0.f}; }
+    static __device__ __forceinline__ F2 of(float x) { return F2{x, 0.f}; }
+    static __device__ __forceinline__ void add(F2 &s, float x) {  // Neumaier: the error of hi + x into lo
+        const float t = s.hi + x;
+        s.lo += (fabsf(s.hi) >= fabsf(x)) ? (s.hi - t) + x : (x - t) + s.hi;
+        s.hi = t;
+    }
+    static __device__ __forceinline__ void combine(F2 &s, F2 o) {
+        add(s, o.hi);
+        s.lo += o.lo;
+    }
+    static __device__ __forceinline__ double value(F2 s) { return (double)s.hi + (double)s.lo; }
+    template <typename T>
+    static __device__ __forceinline__ T excl(F2 s, T x) {
+        return (T)((s.hi - (float)x) + s.lo);
+    }
+    static __device__ __forceinline__ F2 shfl_xor(F2 s, int o) {
+        return F2{__shfl_xor_sync(0xffffffffu, s.hi, o), __shfl_xor_sync(0xffffffffu, s.lo, o)};
+    }
+};
+
+// Accumulator of the sliced-ELL variables (<= 16 terms) and of wider items.
+template <typename T>
+struct NarrowAcc {
+    typedef T type;
+};
+template <typename T>
+struct WideAcc;
+template <>
+struct WideAcc<float> {
+    typedef F2 type;
+};
+template <>
+struct WideAcc<double> {
+    typedef double type;
+};
+
 template <typename T>
 __device__ __forceinline__ T head_effective(uint8_t kind, T vf_head) {
     const uint8_t hs = kind & HEAD_MASK;
@@ -678,11 +762,12 @@ __device__ __forceinline__ void factor_tile_big(const T *vb, const uint32_t *ps,
     if (lane == 31) xP = T(1), xR = T(0);
     if ((kind & HEAD_MASK) == HEAD_FREE) {
         auto logP = [&]() {  // rare: whole-body log-sigmoid sum, by the whole warp
-            double l = 0.0;
-            for (uint32_t k = lane; k < nbody; k += 32) l += (double)log_sigmoid<T>(sgn * vb[1 + k]);
+            typedef AccOps<typename WideAcc<T>::type> O;
+            typename WideAcc<T>::type l = O::zero();
+            for (uint32_t k = lane; k < nbody; k += 32) O::add(l, log_sigmoid<T>(sgn * vb[1 + k]));
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
-            return (T)l;
+            for (int o = 16; o > 0; o >>= 1) O::combine(l, O::shfl_xor(l, o));
+            return (T)O::value(l);
         };
         const T o = sgn * head_from_pair<T>(P, R, p, q, logP);
         if (lane == 0) put_fv<T>(fv, ps[0], o);
@@ -710,11 +795,13 @@ __device__ __forceinline__ void factor_tile_big(const T *vb, const uint32_t *ps,
 
 // A factor too large for a tile (big factor b, internal index nf_sell + b),
 // spread over all consumer threads of a block (called by all of them): a
-// log-sigmoid sum of the body in FP64 with a count of -inf terms, reduced
+// log-sigmoid sum of the body (WideAcc) with a count of -inf terms, reduced
 // over the block in a fixed order, then every slot removes its own term.
 template <typename T>
 __device__ void factor_block_huge(const FactorArgs &a, uint32_t b, int tid, const T *__restrict__ vf,
-                                  T *__restrict__ fv, double *s_l, int *s_nz) {
+                                  T *__restrict__ fv, typename WideAcc<T>::type *s_l, int *s_nz) {
+    typedef typename WideAcc<T>::type A;
+    typedef AccOps<A> O;
     const uint32_t fi = a.nf_sell + b;
     if (a.f_graph && a.gdone[a.f_graph[fi]]) return;  // batched solve: its graph has stopped (same for all)
     const uint32_t s0 = a.fb_off[b], s1 = s0 + a.fb_deg[b];
@@ -724,16 +811,16 @@ __device__ void factor_block_huge(const FactorArgs &a, uint32_t b, int tid, cons
     const T s = (kind & KIND_OR) ? T(-1) : T(1);
     const T inf = Num<T>::inf();
     const int lane = tid & 31, wid = tid >> 5;
-    double L = 0.0;
+    A L = O::zero();
     int nz = 0;
     for (uint32_t k = s0 + 1 + tid; k < s1; k += kConsumers) {
         const T ls = log_sigmoid<T>(s * vf[k]);
         if (ls == -inf) nz++;
-        else L += (double)ls;
+        else O::add(L, ls);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        L += __shfl_xor_sync(0xffffffffu, L, o);
+        O::combine(L, O::shfl_xor(L, o));
         nz += __shfl_xor_sync(0xffffffffu, nz, o);
     }
     if (lane == 0) {
@@ -741,20 +828,20 @@ __device__ void factor_block_huge(const FactorArgs &a, uint32_t b, int tid, cons
         s_nz[wid] = nz;
     }
     consumer_sync();
-    L = 0.0;
+    L = O::zero();
     nz = 0;
     for (int w = 0; w < kConsumerWarps; w++) {
-        L += s_l[w];
+        O::combine(L, s_l[w]);
         nz += s_nz[w];
     }
     consumer_sync();  // the partials are reused by the next factor
     if ((kind & HEAD_MASK) == HEAD_FREE && tid == 0)
-        put_fv<T>(fv, a.f_pos[s0], s * head_out<T>(nz ? -inf : (T)L, p, q, Num<T>::log(p)));
+        put_fv<T>(fv, a.f_pos[s0], s * head_out<T>(nz ? -inf : (T)O::value(L), p, q, Num<T>::log(p)));
     const BodyDen<T> D = body_den<T>(s * head_effective<T>(kind, vf[s0]), p, q);
     for (uint32_t k = s0 + 1 + tid; k < s1; k += kConsumers) {
         const T ls = log_sigmoid<T>(s * vf[k]);
         const bool z = (ls == -inf);
-        const T lo = (nz - (int)z) ? -inf : (T)(z ? L : L - (double)ls);
+        const T lo = (nz - (int)z) ? -inf : (z ? (T)O::value(L) : O::template excl<T>(L, ls));
         put_fv<T>(fv, a.f_pos[k], s * body_out<T>(lo, p, q, D));
     }
 }
@@ -848,7 +935,7 @@ __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArg
     }
 
     {  // factors too large for a tile first, one per block, while the producer's first loads are in flight
-        __shared__ double s_l[kConsumerWarps];
+        __shared__ typename WideAcc<T>::type s_l[kConsumerWarps];
         __shared__ int s_nz[kConsumerWarps];
         for (uint32_t b = blockIdx.x; b < a.nf_huge; b += gridDim.x)
             factor_block_huge<T>(a, b, threadIdx.x, vf, fv, s_l, s_nz);
@@ -892,16 +979,16 @@ __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArg
 // Leave-one-out message of a variable to the factor of one entry: remove
 // `x` from (S, npos, nneg); both kinds of zero left -> (0.5,0.5); otherwise
 // the remaining zero wins (causal_bp_parall.cu:74-90).
-template <typename T>
-__device__ __forceinline__ T excl_msg(double S, int npos, int nneg, T x) {
+template <typename T, typename A>
+__device__ __forceinline__ T excl_msg(const A &S, int npos, int nneg, T x) {
     const T inf = Num<T>::inf();
+    const bool fin = !(x == inf || x == -inf);
     if (x == inf) npos--;
     else if (x == -inf) nneg--;
-    else S -= (double)x;
     if (npos > 0 && nneg > 0) return T(0);
     if (npos > 0) return inf;
     if (nneg > 0) return -inf;
-    return (T)S;
+    return fin ? AccOps<A>::template excl<T>(S, x) : (T)AccOps<A>::value(S);
 }
 
 // Belief P(x=1): b_s = prod_s * [zeros_s == 0], belief = b1 / (b0 + b1)
@@ -941,17 +1028,19 @@ __device__ __forceinline__ double var_finish(const VarArgs &a, uint32_t v, doubl
     return diff;
 }
 
-template <typename T>
-__device__ __forceinline__ void decode_prior(const void *pr, uint32_t i, double pscale, double &S, int &npos,
-                                             int &nneg) {
+// Prior of internal variable i: its finite constant log-odds times the
+// damping weight pscale (FP32 engines: in float; an accumulator A of a
+// wider type receives it exactly), and its +-inf counts.
+template <typename T, typename A>
+__device__ __forceinline__ void decode_prior(const void *pr, uint32_t i, double pscale, A &S, int &npos, int &nneg) {
     uint32_t cnt;
     if (sizeof(T) == 4) {
         const uint2 x = reinterpret_cast<const uint2 *>(pr)[i];
-        S = (double)__uint_as_float(x.x) * pscale;
+        S = AccOps<A>::of(__uint_as_float(x.x) * (float)pscale);
         cnt = x.y;
     } else {
         const uint4 x = reinterpret_cast<const uint4 *>(pr)[i];
-        S = __hiloint2double((int)x.y, (int)x.x) * pscale;
+        S = AccOps<A>::of(__hiloint2double((int)x.y, (int)x.x) * pscale);
         cnt = x.z;
     }
     npos = (int)(cnt & 0xffffu);
@@ -974,8 +1063,10 @@ __device__ __forceinline__ double var_tile_big(const VarArgs &a, uint32_t v, uin
                                                const T *xo, T *__restrict__ fvd_run, const void *prior, uint32_t pidx,
                                                int lane, T *__restrict__ vf, T d, double pscale, double tol,
                                                unsigned long long &cnt) {
+    typedef typename WideAcc<T>::type A;
+    typedef AccOps<A> O;
     const T inf = Num<T>::inf();
-    double S = 0.0;
+    A S = O::zero();
     int npos = 0, nneg = 0;
     for (uint32_t k = lane; k < deg; k += 32) {
         T xv = x[k];
@@ -986,18 +1077,18 @@ __device__ __forceinline__ double var_tile_big(const VarArgs &a, uint32_t v, uin
         }
         if (xv == inf) npos++;
         else if (xv == -inf) nneg++;
-        else S += (double)xv;
+        else O::add(S, xv);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        S += __shfl_xor_sync(0xffffffffu, S, o);
+        O::combine(S, O::shfl_xor(S, o));
         npos += __shfl_xor_sync(0xffffffffu, npos, o);
         nneg += __shfl_xor_sync(0xffffffffu, nneg, o);
     }
-    double S0;
+    A S0;
     int p0, n0;
     decode_prior<T>(prior, pidx, pscale, S0, p0, n0);
-    S += S0;
+    O::combine(S, S0);
     npos += p0;
     nneg += n0;
     if (WRITE_VF) {
@@ -1007,24 +1098,26 @@ __device__ __forceinline__ double var_tile_big(const VarArgs &a, uint32_t v, uin
         }
     }
     constexpr bool RESID = (BMODE == 1 || BMODE == 2 || BMODE == 4);
-    return (lane == 0) ? var_finish<BMODE>(a, v, S, npos, nneg, tol, RESID ? a.belief[v] : 0.0, cnt) : 0.0;
+    return (lane == 0) ? var_finish<BMODE>(a, v, O::value(S), npos, nneg, tol, RESID ? a.belief[v] : 0.0, cnt) : 0.0;
 }
 
 // A variable too large for a tile (big variable b, internal index
 // nv_sell + b), spread over all consumer threads of a block (called by all
-// of them): FP64 sum with +-inf counts reduced over the block in a fixed
+// of them): a WideAcc sum with +-inf counts reduced over the block in a fixed
 // order, then every entry's leave-one-out message. Returns the belief change
 // on thread 0 (0 elsewhere).
 template <typename T, int BMODE, bool WRITE_VF, bool DAMP>
 __device__ double var_block_huge(const VarArgs &a, uint32_t b, int tid, const T *__restrict__ fv,
                                  T *__restrict__ vf, T *__restrict__ fvd, T d, double pscale, double tol,
-                                 unsigned long long &cnt, double *s_s, int *s_np, int *s_nn) {
+                                 unsigned long long &cnt, typename WideAcc<T>::type *s_s, int *s_np, int *s_nn) {
+    typedef typename WideAcc<T>::type A;
+    typedef AccOps<A> O;
     constexpr bool RESID = (BMODE == 1 || BMODE == 2 || BMODE == 4);
     const uint32_t v = a.nv_sell + b, k0 = a.vb_off[b], k1 = k0 + a.vb_deg[b];
     const T inf = Num<T>::inf();
     const T *src = DAMP ? fvd : fv;  // after the first loop, fvd holds the messages in use
     const int lane = tid & 31, wid = tid >> 5;
-    double S = 0.0;
+    A S = O::zero();
     int npos = 0, nneg = 0;
     for (uint32_t k = k0 + tid; k < k1; k += kConsumers) {
         T x = fv[k];
@@ -1034,11 +1127,11 @@ __device__ double var_block_huge(const VarArgs &a, uint32_t b, int tid, const T 
         }
         if (x == inf) npos++;
         else if (x == -inf) nneg++;
-        else S += (double)x;
+        else O::add(S, x);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        S += __shfl_xor_sync(0xffffffffu, S, o);
+        O::combine(S, O::shfl_xor(S, o));
         npos += __shfl_xor_sync(0xffffffffu, npos, o);
         nneg += __shfl_xor_sync(0xffffffffu, nneg, o);
     }
@@ -1048,18 +1141,18 @@ __device__ double var_block_huge(const VarArgs &a, uint32_t b, int tid, const T 
         s_nn[wid] = nneg;
     }
     consumer_sync();
-    S = 0.0;
+    S = O::zero();
     npos = nneg = 0;
     for (int w = 0; w < kConsumerWarps; w++) {
-        S += s_s[w];
+        O::combine(S, s_s[w]);
         npos += s_np[w];
         nneg += s_nn[w];
     }
     consumer_sync();  // the partials are reused by the next variable
-    double S0;
+    A S0;
     int p0, n0;
     decode_prior<T>(a.prior, v, pscale, S0, p0, n0);
-    S += S0;
+    O::combine(S, S0);
     npos += p0;
     nneg += n0;
     if (WRITE_VF) {
@@ -1068,7 +1161,7 @@ __device__ double var_block_huge(const VarArgs &a, uint32_t b, int tid, const T 
             if (e != kSentinel) vf[e] = excl_msg<T>(S, npos, nneg, src[k]);
         }
     }
-    return (tid == 0) ? var_finish<BMODE>(a, v, S, npos, nneg, tol, RESID ? a.belief[v] : 0.0, cnt) : 0.0;
+    return (tid == 0) ? var_finish<BMODE>(a, v, O::value(S), npos, nneg, tol, RESID ? a.belief[v] : 0.0, cnt) : 0.0;
 }
 
 __device__ __forceinline__ double warp_max(double x) {
@@ -1301,7 +1394,7 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
                               VS::bytes, full, empty, lane, ctl, fill);
     } else {  // consumer warps: variables too large for a tile first
         {  // one per block
-            __shared__ double s_s[kConsumerWarps];
+            __shared__ typename WideAcc<T>::type s_s[kConsumerWarps];
             __shared__ int s_np[kConsumerWarps], s_nn[kConsumerWarps];
             for (uint32_t b = blockIdx.x; b < a.nv_huge; b += gridDim.x) {
                 const uint32_t g = a.v_graph ? a.v_graph[a.nv_sell + b] : 0;
@@ -1344,7 +1437,8 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
                 const uint32_t g = a.v_graph ? reinterpret_cast<const uint32_t *>(st + VS::gid)[t] : 0;
                 const bool live = !(a.v_graph && graph_done(s_done, a.gstate, g));  // stopped graph: no work
                 const int wl = live ? w : 0;
-                double S = 0.0;
+                typedef typename NarrowAcc<T>::type A;
+                A S = AccOps<A>::zero();
                 int npos = 0, nneg = 0;
                 if (v < a.nv_sell) decode_prior<T>(st + VS::prior, t, pscale, S, npos, nneg);
                 for (int k = 0; k < wl; k++) {  // padding entries hold 0
@@ -1357,11 +1451,11 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
                     }
                     if (xv == inf) npos++;
                     else if (xv == -inf) nneg++;
-                    else S += (double)xv;
+                    else AccOps<A>::add(S, xv);
                 }
                 if (v < a.nv_sell && live) {
                     const double dd = var_finish<BMODE>(
-                        a, v, S, npos, nneg, tol, RESID ? reinterpret_cast<const double *>(st + VS::bold)[t] : 0.0, cnt);
+                        a, v, AccOps<A>::value(S), npos, nneg, tol, RESID ? reinterpret_cast<const double *>(st + VS::bold)[t] : 0.0, cnt);
                     dmax = fmax(dmax, dd);
                     if (BMODE == 4 && dd > tol) mark_moved(s_moved, a, g);
                 }

@@ -163,6 +163,12 @@ class CausalFactorGraph:
                 self.clamp(i, clamps[lab])
 
 
+def set_layout_builder(mode: str) -> None:
+    """Where new engines build their layout: "auto" (GPU from 2^18 edge slots),
+    "host" or "device" (flbp_set_layout_builder; process-wide)."""
+    check(lib().flbp_set_layout_builder({"auto": 0, "host": 1, "device": 2}[mode]))
+
+
 def layout_digest(arrays: Dict[str, np.ndarray], threads: int = 0, graph_of=None) -> int:
     """Digest of the device layout built for reference-order graph arrays
     (flbp_layout_digest; host only). graph_of: optional (factor_graph,
@@ -435,7 +441,7 @@ class Engine:
     def set_tuning(self, factor_form: int, var_form: int) -> None:
         """Form of each sweep pass: 0 staged, 1 or 2 direct (flbp_set_tuning)."""
         t = N.Tuning(int(factor_form), int(var_form), 0, 0)
-        N.check(N.lib().flbp_set_tuning(self.h, C.byref(t)))
+        check(lib().flbp_set_tuning(self._h, C.byref(t)))
 
     def autotune(self, sweeps: int = 200, tol: Optional[float] = None, reps: int = 3) -> Dict[str, int]:
         """Time the pass forms on this graph and keep the fastest (flbp_autotune):
@@ -449,9 +455,15 @@ class Engine:
         """autotune over whole batched tolerance runs (flbp_batch_run_tol)."""
         return self.autotune(maxiter, tol=tol, reps=reps)
 
+    def layout_digest(self) -> Tuple[int, bool]:
+        """(digest of the engine's device layout, built on the GPU) - flbp_engine_layout_digest."""
+        d, on_dev = C.c_uint64(), C.c_int32()
+        check(lib().flbp_engine_layout_digest(self._h, C.byref(d), C.byref(on_dev)))
+        return int(d.value), bool(on_dev.value)
+
     def tuning(self) -> Dict[str, int]:
         t = N.Tuning()
-        N.check(N.lib().flbp_get_tuning(self.h, C.byref(t)))
+        check(lib().flbp_get_tuning(self._h, C.byref(t)))
         return {k: getattr(t, k) for k, _ in t._fields_}
 
     def last_run_ms(self) -> float:

@@ -20,7 +20,7 @@ INCLUDE = os.path.join(ROOT, "include")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libfastlbp_b200.so")
 
-SOURCES = ["engine.cu", "direct.cu", "layout.cpp", "model.cpp", "causal_bp.cpp", "fg_capi.cpp", "noalloc.cu", "schedule.cpp"]
+SOURCES = ["engine.cu", "direct.cu", "dlayout.cu", "layout.cpp", "model.cpp", "causal_bp.cpp", "fg_capi.cpp", "noalloc.cu", "schedule.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "nvcc")
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-ccbin", "g++", "-Xcompiler", "-fPIC", "-I" + INCLUDE]

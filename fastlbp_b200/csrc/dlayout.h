@@ -1,0 +1,53 @@
+// Construction of the engine's device layout on the GPU (dlayout.cu).
+//
+// The result equals the host build (build_layout, layout.cpp) bit for bit:
+// the same item orders, slots, entries, priors and tile headers. The device
+// arrays the sweep reads are built and left on the device; the host receives
+// only the layout's counts and its small arrays (group bases, large-item
+// runs, tile headers and per-tile constants), which is what the launch code
+// needs. The per-slot and per-item arrays that other host-side features read
+// (message export, gradients, clamps, schedules) are not filled here: the
+// engine builds the complete host layout from the graph when one of them is
+// first used.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "engine_internal.h"
+
+namespace flbp {
+
+// The caller's graph arrays, copied to the device (reference order).
+struct DevGraphIn {
+    const int64_t *off = nullptr, *slot_var = nullptr, *head = nullptr;
+    const int32_t *type = nullptr, *clamped = nullptr;
+    const double *p = nullptr, *q = nullptr, *mask0 = nullptr, *mask1 = nullptr;
+};
+
+// Device buffers of a layout (owned by the caller once built). Per-item
+// arrays are padded to whole groups of 32 like the host build's uploads.
+struct DevLayout {
+    uint32_t *f_pos = nullptr, *fg_base = nullptr, *fb_off = nullptr, *fb_deg = nullptr;
+    uint32_t *vg_base = nullptr, *vb_off = nullptr, *vb_deg = nullptr, *v_ent = nullptr;
+    uint32_t *ftiles = nullptr, *vtiles = nullptr, *fbt_deg = nullptr, *vbt_deg = nullptr, *int_of_var = nullptr;
+    uint8_t *f_kind = nullptr, *f_deg = nullptr, *fbt_kind = nullptr;
+    void *f_pq = nullptr, *fbt_pq = nullptr, *prior = nullptr, *vbt_prior = nullptr;
+    size_t bytes = 0;      // device memory held by these buffers
+    size_t nf_pad = 0, nv_pad = 0, n_ent = 0;
+};
+
+// Builds the layout of graph `g` (sizes and, on the host, the arrays that
+// the validation messages and the folded constants need) from its device
+// copy `in`, for messages of `prec` bits (32 / 64). Fills the counts and
+// small arrays of L (L.complete false) and the buffers of D. On a malformed
+// graph returns the host build's error code and message.
+int build_layout_device(const flbp_graph_desc &g, const DevGraphIn &in, int prec, HostLayout &L, DevLayout &D,
+                        std::string &err, cudaStream_t st);
+
+// Frees the buffers of D.
+void free_dev_layout(DevLayout &D);
+
+}  // namespace flbp

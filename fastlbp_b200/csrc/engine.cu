@@ -10,6 +10,7 @@
 #include <cstddef>
 #include <cstring>
 #include <limits>
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <new>
@@ -23,6 +24,7 @@
 #include "kernels.cuh"
 #include "adjoint.cuh"
 #include "direct_launch.h"
+#include "dlayout.h"
 #include "seq.cuh"
 
 namespace flbp {
@@ -136,6 +138,11 @@ struct flbp_engine {
     bool lowpass_valid = false;
     size_t bytes = 0;
     size_t h2d_bytes = 0;  // host->device bytes copied by create
+    // Layout built on the device (dlayout.h): the caller's graph arrays stay
+    // on the device until the complete host layout is first needed.
+    bool dev_layout = false;
+    DevGraphIn din;
+    void *d_in[9] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     // wall time (us) of the phases of create: host layout, device allocation,
     // host->device copies (with the host-side packing they need), the rest
     int64_t create_us[4] = {0, 0, 0, 0};
@@ -708,6 +715,95 @@ void packed_priors(const flbp_engine *e, size_t nv_pad, std::vector<uint32_t> &p
     bt_prior.resize(L.vbt_deg.size() * (psz / 4));
 }
 
+// Which builder makes a new engine's layout: 0 the device for graphs of at
+// least 2^18 edge slots (below that the host build is as fast), 1 always
+// the host, 2 always the device (flbp_set_layout_builder).
+std::atomic<int> g_layout_builder{0};
+
+bool use_device_layout(const flbp_graph_desc &g) {
+    const int mode = g_layout_builder.load();
+    if (mode == 1) return false;
+    const bool fits = g.n_slots < (1ll << 30) && g.n_factors < (1ll << 30) && g.n_vars < (1ll << 30);
+    return fits && (mode == 2 || g.n_slots >= (1ll << 18));
+}
+
+// The host copies of the caller's factor p, q and heads that later calls
+// (schedules, gradients, new probabilities) read.
+void keep_host_graph(flbp_engine *e, const flbp_graph_desc &g) {
+    if (g.n_factors > 0 && g.factor_p) e->factor_p_host.assign(g.factor_p, g.factor_p + g.n_factors);
+    if (g.n_factors > 0 && g.factor_q) e->factor_q_host.assign(g.factor_q, g.factor_q + g.n_factors);
+    if (g.n_factors > 0) e->ref_head.assign(g.factor_head, g.factor_head + g.n_factors);
+}
+
+// Device build of the layout: the caller's arrays are copied to the device
+// (and kept there for ensure_host_layout), then dlayout.cu builds the layout.
+int device_layout(flbp_engine *e, const flbp_graph_desc &g, DevLayout &D) {
+    std::string err;
+    int rc = check_graph_shape(g, err);
+    if (rc) {
+        set_error(err);
+        return rc;
+    }
+    const size_t F = (size_t)g.n_factors, E = (size_t)g.n_slots;
+    struct In {
+        const void *src;
+        size_t bytes;
+    };
+    const In ins[9] = {{g.factor_offsets, F ? (F + 1) * 8 : 0}, {g.slot_var, E * 8}, {g.factor_head, F * 8},
+                       {g.factor_type, F * 4}, {g.factor_p, F * 8}, {g.factor_q, F * 8},
+                       {g.factor_head_clamped, g.factor_head_clamped ? F * 4 : 0},
+                       {g.factor_mask0, g.factor_mask0 ? F * 8 : 0}, {g.factor_mask1, g.factor_mask1 ? F * 8 : 0}};
+    for (int k = 0; k < 9; k++) {
+        if (!ins[k].bytes || !ins[k].src) continue;
+        FLBP_CUDA(cudaMalloc(&e->d_in[k], ins[k].bytes));
+        FLBP_CUDA(cudaMemcpyAsync(e->d_in[k], ins[k].src, ins[k].bytes, cudaMemcpyHostToDevice, e->stream));
+        e->h2d_bytes += ins[k].bytes;
+    }
+    DevGraphIn &in = e->din;
+    in.off = (const int64_t *)e->d_in[0];
+    in.slot_var = (const int64_t *)e->d_in[1];
+    in.head = (const int64_t *)e->d_in[2];
+    in.type = (const int32_t *)e->d_in[3];
+    in.p = (const double *)e->d_in[4];
+    in.q = (const double *)e->d_in[5];
+    in.clamped = (const int32_t *)e->d_in[6];
+    in.mask0 = (const double *)e->d_in[7];
+    in.mask1 = (const double *)e->d_in[8];
+    rc = build_layout_device(g, in, e->prec, e->L, D, err, e->stream);
+    if (rc) {
+        free_dev_layout(D);
+        set_error(err);
+        return rc;
+    }
+    e->dev_layout = true;
+    return FLBP_OK;
+}
+
+void adopt_dev_layout(flbp_engine *e, DevLayout &D) {
+    e->d_f_pos = D.f_pos;
+    e->d_fg_base = D.fg_base;
+    e->d_fb_off = D.fb_off;
+    e->d_fb_deg = D.fb_deg;
+    e->d_vg_base = D.vg_base;
+    e->d_vb_off = D.vb_off;
+    e->d_vb_deg = D.vb_deg;
+    e->d_v_ent = D.v_ent;
+    e->d_ftiles = D.ftiles;
+    e->d_vtiles = D.vtiles;
+    e->d_fbt_deg = D.fbt_deg;
+    e->d_vbt_deg = D.vbt_deg;
+    e->d_int_of_var = D.int_of_var;
+    e->d_f_kind = D.f_kind;
+    e->d_f_deg = D.f_deg;
+    e->d_fbt_kind = D.fbt_kind;
+    e->d_f_pq = D.f_pq;
+    e->d_fbt_pq = D.fbt_pq;
+    e->d_prior = D.prior;
+    e->d_vbt_prior = D.vbt_prior;
+    e->bytes += D.bytes;
+    D = DevLayout();
+}
+
 int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, flbp_engine **out,
                   const BatchSpec *batch) {
     auto clk = [] { return std::chrono::steady_clock::now(); };
@@ -736,19 +832,24 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
         return FLBP_ERR_NOMEM;
     }
     std::string err;
-    GraphIds ids{0, nullptr, nullptr};
-    if (batch) ids = GraphIds{(uint32_t)(batch->var_off.size() - 1), batch->factor_graph.data(), batch->var_graph.data()};
-    auto tc0 = clk();
-    int rc = build_layout(*graph, e->L, err, batch ? &ids : nullptr);
-    e->create_us[0] = us(tc0, clk());
-    if (rc) {
-        set_error(err);
-        delete e;
-        return rc;
+    int rc = FLBP_OK;
+    // The host build runs first (a malformed graph is reported without a
+    // GPU); the device build needs the engine's device and stream.
+    const bool on_device = !batch && use_device_layout(*graph);
+    if (!on_device) {
+        GraphIds ids{0, nullptr, nullptr};
+        if (batch)
+            ids = GraphIds{(uint32_t)(batch->var_off.size() - 1), batch->factor_graph.data(), batch->var_graph.data()};
+        auto tc0 = clk();
+        rc = build_layout(*graph, e->L, err, batch ? &ids : nullptr);
+        e->create_us[0] = us(tc0, clk());
+        if (rc) {
+            set_error(err);
+            delete e;
+            return rc;
+        }
+        keep_host_graph(e, *graph);
     }
-    if (graph->n_factors > 0 && graph->factor_p) e->factor_p_host.assign(graph->factor_p, graph->factor_p + graph->n_factors);
-    if (graph->n_factors > 0 && graph->factor_q) e->factor_q_host.assign(graph->factor_q, graph->factor_q + graph->n_factors);
-    if (graph->n_factors > 0) e->ref_head.assign(graph->factor_head, graph->factor_head + graph->n_factors);
     e->prec = o.precision;
     e->tsize = o.precision == 64 ? 8 : 4;
     e->damping = o.damping;
@@ -785,6 +886,12 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
         set_error("event creation failed");
         return fail(FLBP_ERR_CUDA);
     }
+    DevLayout DL;
+    if (on_device) {
+        auto tc0 = clk();
+        if ((rc = device_layout(e, *graph, DL))) return fail(rc);
+        e->create_us[0] = us(tc0, clk());
+    }
     const HostLayout &L = e->L;
     const uint32_t nf = L.nf_sell + L.nf_big;
     const size_t ns = std::max<uint64_t>(1, L.n_slots);
@@ -819,67 +926,84 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
     const size_t nf_pad = std::max<size_t>(nf, 32ull * L.n_fgroups());
     const size_t nv_pad = std::max<size_t>((size_t)L.V, 32ull * L.n_vgroups());
     const size_t psz = e->prec == 64 ? 16 : 8;
-    e->n_ent = std::max<size_t>(1, L.v_ent.size());
+    e->n_ent = std::max<size_t>(1, e->dev_layout ? DL.n_ent : L.v_ent.size());
     const size_t ne = e->n_ent;
     auto tc1 = clk();
-    if ((rc = dalloc(e, (char **)&e->d_vf, ns * e->tsize)) || (rc = dalloc(e, (char **)&e->d_fv, ne * e->tsize)) ||
-        (damp && (rc = dalloc(e, (char **)&e->d_fvd, ne * e->tsize))) || (rc = dalloc(e, &e->d_f_pos, ns)) ||
-        (rc = dalloc(e, (char **)&e->d_f_pq, 2 * nf_pad * e->tsize)) ||
-        (rc = dalloc(e, &e->d_fg_base, L.fg_base.size())) || (rc = dalloc(e, &e->d_fb_off, L.fb_off.size())) ||
-        (rc = dalloc(e, &e->d_f_kind, nf_pad)) || (rc = dalloc(e, &e->d_f_deg, nf_pad)) ||
-        (rc = dalloc(e, &e->d_vg_base, L.vg_base.size())) || (rc = dalloc(e, &e->d_vb_off, L.vb_off.size())) ||
-        (rc = dalloc(e, &e->d_v_ent, L.v_ent.size())) || (rc = dalloc(e, &e->d_ftiles, L.fhdr.size())) ||
-        (rc = dalloc(e, &e->d_vtiles, L.vhdr.size())) || (rc = dalloc(e, &e->d_fb_deg, L.fb_deg.size())) ||
-        (rc = dalloc(e, &e->d_vb_deg, L.vb_deg.size())) || (rc = dalloc(e, &e->d_fbt_deg, L.fbt_deg.size())) ||
-        (rc = dalloc(e, &e->d_vbt_deg, L.vbt_deg.size())) || (rc = dalloc(e, &e->d_fbt_kind, L.fbt_kind.size())) ||
-        (rc = dalloc(e, (char **)&e->d_fbt_pq, L.fbt_pq.size() * e->tsize)) ||
-        (rc = dalloc(e, (char **)&e->d_vbt_prior, L.vbt_deg.size() * psz)) ||
-        (rc = dalloc(e, (char **)&e->d_prior, std::max<size_t>(1, nv_pad) * psz)) ||
-        (rc = dalloc(e, &e->d_belief, nv_pad)) || (rc = dalloc(e, &e->d_lowpass, (size_t)L.V)) ||
-        (rc = dalloc(e, &e->d_ctl, 1)))
-        return fail(rc);
-    if (cudaMallocHost((void **)&e->h_ctl, sizeof(Ctl)) != cudaSuccess) {
-        set_error("pinned allocation failed");
-        return fail(FLBP_ERR_NOMEM);
-    }
-    std::memset(e->h_ctl, 0, sizeof(Ctl));
-    auto tc2 = clk();
-    e->create_us[1] = us(tc1, tc2);
-    std::vector<uint32_t> prior, bt_prior;
-    packed_priors(e, nv_pad, prior, bt_prior);
-    std::vector<uint8_t> kind_pad(nf_pad, 0), deg_pad(nf_pad, 0);
-    std::copy(L.f_kind.begin(), L.f_kind.end(), kind_pad.begin());
-    std::copy(L.f_deg.begin(), L.f_deg.end(), deg_pad.begin());
-    // (p, q) of every factor in the message type, padded with zeros
-    auto padded_pq = [&](auto zero) {
-        using X = decltype(zero);
-        hvec<X> v(2 * nf_pad);
-        const int64_t n = (int64_t)v.size(), nr = (int64_t)L.f_pq.size();
-#pragma omp parallel for if (n >= (1 << 15))
-        for (int64_t i = 0; i < n; i++) v[i] = i < nr ? (X)L.f_pq[i] : X(0);
-        return v;
-    };
-    if (e->prec == 64) {
-        if ((rc = upload(e, (double *)e->d_f_pq, padded_pq(0.0))) ||
-            (rc = upload(e, (double *)e->d_fbt_pq, L.fbt_pq)))
+    auto tc2 = tc1;
+    if (e->dev_layout) {  // the layout's buffers are built; the run state's follow
+        adopt_dev_layout(e, DL);
+        if ((rc = dalloc(e, (char **)&e->d_vf, ns * e->tsize)) || (rc = dalloc(e, (char **)&e->d_fv, ne * e->tsize)) ||
+            (damp && (rc = dalloc(e, (char **)&e->d_fvd, ne * e->tsize))) || (rc = dalloc(e, &e->d_belief, nv_pad)) ||
+            (rc = dalloc(e, &e->d_lowpass, (size_t)L.V)) || (rc = dalloc(e, &e->d_ctl, 1)) ||
+            (rc = dalloc(e, &e->d_ref_out, (size_t)L.V)))
             return fail(rc);
+        if (cudaMallocHost((void **)&e->h_ctl, sizeof(Ctl)) != cudaSuccess) {
+            set_error("pinned allocation failed");
+            return fail(FLBP_ERR_NOMEM);
+        }
+        std::memset(e->h_ctl, 0, sizeof(Ctl));
+        tc2 = clk();
+        e->create_us[1] = us(tc1, tc2);
     } else {
-        std::vector<float> bpq32(L.fbt_pq.begin(), L.fbt_pq.end());
-        if ((rc = upload(e, (float *)e->d_f_pq, padded_pq(0.0f))) || (rc = upload(e, (float *)e->d_fbt_pq, bpq32)))
+        if ((rc = dalloc(e, (char **)&e->d_vf, ns * e->tsize)) || (rc = dalloc(e, (char **)&e->d_fv, ne * e->tsize)) ||
+            (damp && (rc = dalloc(e, (char **)&e->d_fvd, ne * e->tsize))) || (rc = dalloc(e, &e->d_f_pos, ns)) ||
+            (rc = dalloc(e, (char **)&e->d_f_pq, 2 * nf_pad * e->tsize)) ||
+            (rc = dalloc(e, &e->d_fg_base, L.fg_base.size())) || (rc = dalloc(e, &e->d_fb_off, L.fb_off.size())) ||
+            (rc = dalloc(e, &e->d_f_kind, nf_pad)) || (rc = dalloc(e, &e->d_f_deg, nf_pad)) ||
+            (rc = dalloc(e, &e->d_vg_base, L.vg_base.size())) || (rc = dalloc(e, &e->d_vb_off, L.vb_off.size())) ||
+            (rc = dalloc(e, &e->d_v_ent, L.v_ent.size())) || (rc = dalloc(e, &e->d_ftiles, L.fhdr.size())) ||
+            (rc = dalloc(e, &e->d_vtiles, L.vhdr.size())) || (rc = dalloc(e, &e->d_fb_deg, L.fb_deg.size())) ||
+            (rc = dalloc(e, &e->d_vb_deg, L.vb_deg.size())) || (rc = dalloc(e, &e->d_fbt_deg, L.fbt_deg.size())) ||
+            (rc = dalloc(e, &e->d_vbt_deg, L.vbt_deg.size())) || (rc = dalloc(e, &e->d_fbt_kind, L.fbt_kind.size())) ||
+            (rc = dalloc(e, (char **)&e->d_fbt_pq, L.fbt_pq.size() * e->tsize)) ||
+            (rc = dalloc(e, (char **)&e->d_vbt_prior, L.vbt_deg.size() * psz)) ||
+            (rc = dalloc(e, (char **)&e->d_prior, std::max<size_t>(1, nv_pad) * psz)) ||
+            (rc = dalloc(e, &e->d_belief, nv_pad)) || (rc = dalloc(e, &e->d_lowpass, (size_t)L.V)) ||
+            (rc = dalloc(e, &e->d_ctl, 1)))
+            return fail(rc);
+        if (cudaMallocHost((void **)&e->h_ctl, sizeof(Ctl)) != cudaSuccess) {
+            set_error("pinned allocation failed");
+            return fail(FLBP_ERR_NOMEM);
+        }
+        std::memset(e->h_ctl, 0, sizeof(Ctl));
+        tc2 = clk();
+        e->create_us[1] = us(tc1, tc2);
+        std::vector<uint32_t> prior, bt_prior;
+        packed_priors(e, nv_pad, prior, bt_prior);
+        std::vector<uint8_t> kind_pad(nf_pad, 0), deg_pad(nf_pad, 0);
+        std::copy(L.f_kind.begin(), L.f_kind.end(), kind_pad.begin());
+        std::copy(L.f_deg.begin(), L.f_deg.end(), deg_pad.begin());
+        // (p, q) of every factor in the message type, padded with zeros
+        auto padded_pq = [&](auto zero) {
+            using X = decltype(zero);
+            hvec<X> v(2 * nf_pad);
+            const int64_t n = (int64_t)v.size(), nr = (int64_t)L.f_pq.size();
+    #pragma omp parallel for if (n >= (1 << 15))
+            for (int64_t i = 0; i < n; i++) v[i] = i < nr ? (X)L.f_pq[i] : X(0);
+            return v;
+        };
+        if (e->prec == 64) {
+            if ((rc = upload(e, (double *)e->d_f_pq, padded_pq(0.0))) ||
+                (rc = upload(e, (double *)e->d_fbt_pq, L.fbt_pq)))
+                return fail(rc);
+        } else {
+            std::vector<float> bpq32(L.fbt_pq.begin(), L.fbt_pq.end());
+            if ((rc = upload(e, (float *)e->d_f_pq, padded_pq(0.0f))) || (rc = upload(e, (float *)e->d_fbt_pq, bpq32)))
+                return fail(rc);
+        }
+        if ((rc = upload(e, e->d_fg_base, L.fg_base)) || (rc = upload(e, e->d_fb_off, L.fb_off)) ||
+            (rc = upload(e, e->d_f_pos, L.f_pos)) ||
+            (rc = upload(e, e->d_f_kind, kind_pad)) || (rc = upload(e, e->d_f_deg, deg_pad)) ||
+            (rc = upload(e, e->d_vg_base, L.vg_base)) || (rc = upload(e, e->d_vb_off, L.vb_off)) ||
+            (rc = upload(e, e->d_v_ent, L.v_ent)) || (rc = upload(e, (uint32_t *)e->d_prior, prior)) ||
+            (rc = upload(e, e->d_ftiles, L.fhdr)) || (rc = upload(e, e->d_vtiles, L.vhdr)) ||
+            (rc = upload(e, e->d_fb_deg, L.fb_deg)) || (rc = upload(e, e->d_vb_deg, L.vb_deg)) ||
+            (rc = upload(e, e->d_fbt_deg, L.fbt_deg)) || (rc = upload(e, e->d_vbt_deg, L.vbt_deg)) ||
+            (rc = upload(e, e->d_fbt_kind, L.fbt_kind)) || (rc = upload(e, (uint32_t *)e->d_vbt_prior, bt_prior)) ||
+            (rc = dalloc(e, &e->d_int_of_var, L.internal_of_var.size())) ||
+            (rc = upload(e, e->d_int_of_var, L.internal_of_var)) || (rc = dalloc(e, &e->d_ref_out, (size_t)L.V)))
             return fail(rc);
     }
-    if ((rc = upload(e, e->d_fg_base, L.fg_base)) || (rc = upload(e, e->d_fb_off, L.fb_off)) ||
-        (rc = upload(e, e->d_f_pos, L.f_pos)) ||
-        (rc = upload(e, e->d_f_kind, kind_pad)) || (rc = upload(e, e->d_f_deg, deg_pad)) ||
-        (rc = upload(e, e->d_vg_base, L.vg_base)) || (rc = upload(e, e->d_vb_off, L.vb_off)) ||
-        (rc = upload(e, e->d_v_ent, L.v_ent)) || (rc = upload(e, (uint32_t *)e->d_prior, prior)) ||
-        (rc = upload(e, e->d_ftiles, L.fhdr)) || (rc = upload(e, e->d_vtiles, L.vhdr)) ||
-        (rc = upload(e, e->d_fb_deg, L.fb_deg)) || (rc = upload(e, e->d_vb_deg, L.vb_deg)) ||
-        (rc = upload(e, e->d_fbt_deg, L.fbt_deg)) || (rc = upload(e, e->d_vbt_deg, L.vbt_deg)) ||
-        (rc = upload(e, e->d_fbt_kind, L.fbt_kind)) || (rc = upload(e, (uint32_t *)e->d_vbt_prior, bt_prior)) ||
-        (rc = dalloc(e, &e->d_int_of_var, L.internal_of_var.size())) ||
-        (rc = upload(e, e->d_int_of_var, L.internal_of_var)) || (rc = dalloc(e, &e->d_ref_out, (size_t)L.V)))
-        return fail(rc);
     cudaError_t ce = cudaSuccess;
     if ((ce = cudaStreamSynchronize(e->stream)) != cudaSuccess) {
         set_error(std::string("device initialisation failed: ") + cudaGetErrorString(ce));
@@ -942,6 +1066,54 @@ int apply_forms(flbp_engine *e, int ff, int vf) {
     return FLBP_OK;
 }
 
+// The complete host layout of an engine whose layout was built on the device
+// (message export, gradients, clamps, schedules and new probabilities read
+// it): the caller's graph arrays come back from the device and the host
+// build runs on them; its result equals the device build's (tested).
+int ensure_host_layout(flbp_engine *e) {
+    if (e->L.complete) return FLBP_OK;
+    const size_t F = (size_t)e->L.F, E = (size_t)e->L.E;
+    std::vector<int64_t> off(F ? F + 1 : 0), sv(E), head(F);
+    std::vector<int32_t> type(F), clamped(e->d_in[6] ? F : 0);
+    std::vector<double> p(F), q(F), m0(e->d_in[7] ? F : 0), m1(e->d_in[8] ? F : 0);
+    void *dst[9] = {off.data(), sv.data(), head.data(), type.data(), p.data(), q.data(), clamped.data(), m0.data(),
+                    m1.data()};
+    const size_t bytes[9] = {off.size() * 8, E * 8, F * 8, F * 4, F * 8, F * 8, clamped.size() * 4, m0.size() * 8,
+                             m1.size() * 8};
+    for (int k = 0; k < 9; k++)
+        if (e->d_in[k] && bytes[k])
+            FLBP_CUDA(cudaMemcpyAsync(dst[k], e->d_in[k], bytes[k], cudaMemcpyDeviceToHost, e->stream));
+    FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    flbp_graph_desc g{};
+    g.n_vars = e->L.V;
+    g.n_factors = (int64_t)F;
+    g.n_slots = (int64_t)E;
+    g.factor_offsets = off.empty() ? nullptr : off.data();
+    g.slot_var = sv.data();
+    g.factor_head = head.data();
+    g.factor_type = type.data();
+    g.factor_p = p.data();
+    g.factor_q = q.data();
+    g.factor_head_clamped = clamped.empty() ? nullptr : clamped.data();
+    g.factor_mask0 = m0.empty() ? nullptr : m0.data();
+    g.factor_mask1 = m1.empty() ? nullptr : m1.data();
+    HostLayout L;
+    std::string err;
+    int rc = build_layout(g, L, err, nullptr);
+    if (rc) {
+        set_error("host layout of a device-built engine: " + err);
+        return rc;
+    }
+    keep_host_graph(e, g);
+    e->L = std::move(L);
+    for (void *&b : e->d_in)
+        if (b) {
+            cudaFree(b);
+            b = nullptr;
+        }
+    return FLBP_OK;
+}
+
 // The v->f messages of clamped variables: +inf (clamped to 1) or -inf (0).
 template <typename T>
 __global__ void clamp_slots_kernel(const uint32_t *__restrict__ pairs, uint32_t n, T *vf) {
@@ -984,6 +1156,8 @@ int flbp_engine_destroy(flbp_engine *e) {
                     e->d_sq_foff, e->d_sq_var, e->d_sq_items, e->d_sq_tgt, e->d_sq_iota, e->d_sq_kind,
                     e->d_sq_cst, e->d_sq_pq, e->d_sq_fv, e->d_sq_vf, e->d_sq_nw, e->d_sq_S, e->d_sq_cnt};
     for (void *b : bufs)
+        if (b) cudaFree(b);
+    for (void *b : e->d_in)
         if (b) cudaFree(b);
     if (e->h_ctl) cudaFreeHost(e->h_ctl);
     if (e->ev0) cudaEventDestroy(e->ev0);
@@ -1249,7 +1423,7 @@ static void pair_of(double lam, double &m0, double &m1) {
 
 int flbp_get_fv_messages(flbp_engine *e, double *m0, double *m1, int64_t n) {
     int rc = begin_call(e);
-    if (rc) return rc;
+    if (rc || (rc = ensure_host_layout(e))) return rc;
     if (n != e->L.E) {
         set_error("output length must equal the number of edge slots");
         return FLBP_ERR_INVALID;
@@ -1266,7 +1440,7 @@ int flbp_get_fv_messages(flbp_engine *e, double *m0, double *m1, int64_t n) {
 
 int flbp_get_vf_messages(flbp_engine *e, double *m0, double *m1, int64_t n) {
     int rc = begin_call(e);
-    if (rc) return rc;
+    if (rc || (rc = ensure_host_layout(e))) return rc;
     const HostLayout &L = e->L;
     if (n != L.E) {
         set_error("output length must equal the number of edge slots");
@@ -1472,6 +1646,61 @@ int flbp_autotune(flbp_engine *e, int32_t kind, int64_t sweeps, double tol, int3
         chosen->factor_blocks = e->f_form ? e->f_grid_direct : e->factor_grid;
         chosen->var_blocks = e->v_form ? e->v_grid_direct : e->var_grid;
     }
+    return FLBP_OK;
+}
+
+int flbp_set_layout_builder(int32_t mode) {
+    if (mode < 0 || mode > 2) {
+        set_error("flbp_set_layout_builder: mode must be 0 (choose by size), 1 (host) or 2 (device)");
+        return FLBP_ERR_INVALID;
+    }
+    g_layout_builder.store(mode);
+    return FLBP_OK;
+}
+
+int flbp_engine_layout_digest(flbp_engine *e, uint64_t *digest, int32_t *built_on_device) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    if (!digest) {
+        set_error("null argument");
+        return FLBP_ERR_INVALID;
+    }
+    const HostLayout &L = e->L;
+    const size_t psz = e->prec == 64 ? 16 : 8, nf = L.nf_sell + L.nf_big;
+    const size_t nf_pad = std::max<size_t>(nf, 32ull * L.n_fgroups());
+    const size_t nv_pad = std::max<size_t>((size_t)L.V, 32ull * L.n_vgroups());
+    uint64_t h = 1469598103934665603ull;
+    auto bytes = [&](const void *p, size_t n) {
+        const unsigned char *c = static_cast<const unsigned char *>(p);
+        for (size_t i = 0; i < n; i++) h = (h ^ c[i]) * 1099511628211ull;
+    };
+    std::vector<unsigned char> buf;
+    auto dev = [&](const void *p, size_t n) -> int {
+        const uint64_t len = n;
+        bytes(&len, sizeof len);
+        if (!n) return FLBP_OK;
+        buf.resize(n);
+        FLBP_CUDA(cudaMemcpyAsync(buf.data(), p, n, cudaMemcpyDeviceToHost, e->stream));
+        FLBP_CUDA(cudaStreamSynchronize(e->stream));
+        bytes(buf.data(), n);
+        return FLBP_OK;
+    };
+    if ((rc = dev(e->d_fg_base, L.fg_base.size() * 4)) || (rc = dev(e->d_fb_off, L.fb_off.size() * 4)) ||
+        (rc = dev(e->d_fb_deg, L.fb_deg.size() * 4)) || (rc = dev(e->d_f_kind, nf_pad)) ||
+        (rc = dev(e->d_f_deg, nf_pad)) || (rc = dev(e->d_f_pq, 2 * nf_pad * e->tsize)) ||
+        (rc = dev(e->d_vg_base, L.vg_base.size() * 4)) || (rc = dev(e->d_vb_off, L.vb_off.size() * 4)) ||
+        (rc = dev(e->d_vb_deg, L.vb_deg.size() * 4)) || (rc = dev(e->d_v_ent, e->n_ent * 4)) ||
+        (rc = dev(e->d_f_pos, std::max<uint64_t>(1, L.n_slots) * 4)) || (rc = dev(e->d_prior, nv_pad * psz)) ||
+        (rc = dev(e->d_ftiles, L.fhdr.size() * 4)) || (rc = dev(e->d_vtiles, L.vhdr.size() * 4)) ||
+        (rc = dev(e->d_fbt_deg, L.fbt_deg.size() * 4)) || (rc = dev(e->d_vbt_deg, L.vbt_deg.size() * 4)) ||
+        (rc = dev(e->d_fbt_kind, L.fbt_kind.size())) || (rc = dev(e->d_fbt_pq, L.fbt_pq.size() * e->tsize)) ||
+        (rc = dev(e->d_vbt_prior, L.vbt_deg.size() * psz)) || (rc = dev(e->d_int_of_var, (size_t)L.V * 4)))
+        return rc;
+    const uint64_t sc[] = {L.nf_sell, L.nf_big, L.nf_huge, L.nv_sell, L.nv_big, L.nv_huge, L.n_slots,
+                           L.n_active_slots, L.n_ftiles, L.n_vtiles, L.n_fbtiles, L.n_vbtiles, (uint64_t)e->n_ent};
+    bytes(sc, sizeof sc);
+    *digest = h;
+    if (built_on_device) *built_on_device = e->dev_layout ? 1 : 0;
     return FLBP_OK;
 }
 
@@ -1756,6 +1985,7 @@ void launch_adjoint_out(flbp_engine *e, double *gp_out, double *gq_out) {
 // coefficients of the folded constants, for the adjoint (built on first use;
 // the coefficients again after flbp_set_factor_probs).
 int ensure_adjoint_maps(flbp_engine *e) {
+    if (int rc0 = ensure_host_layout(e)) return rc0;
     int rc;
     const HostLayout &L = e->L;
     if (!e->d_adj_groups) {
@@ -1862,7 +2092,7 @@ extern "C" {
 
 int flbp_adjoint_forward(flbp_engine *e, int64_t sweeps, int64_t every, double *beliefs, int64_t n) {
     int rc = begin_call(e);
-    if (rc || (rc = refuse_seq(e, "the adjoint"))) return rc;
+    if (rc || (rc = refuse_seq(e, "the adjoint")) || (rc = ensure_host_layout(e))) return rc;
     if (e->damping != 0.0) {
         set_error("the adjoint needs an engine without damping");
         return FLBP_ERR_INVALID;
@@ -1919,7 +2149,7 @@ int flbp_adjoint_forward(flbp_engine *e, int64_t sweeps, int64_t every, double *
 
 int flbp_adjoint_backward(flbp_engine *e, const double *grad_beliefs, double *grad_p, double *grad_q) {
     int rc = begin_call(e);
-    if (rc || (rc = refuse_seq(e, "the adjoint"))) return rc;
+    if (rc || (rc = refuse_seq(e, "the adjoint")) || (rc = ensure_host_layout(e))) return rc;
     const HostLayout &L = e->L;
     const size_t nv = std::max<int64_t>(1, L.V), nF = std::max<int64_t>(1, L.F);
     if (!e->d_adj_in && ((rc = dalloc(e, &e->d_adj_in, nv)) || (rc = dalloc(e, &e->d_adj_out, 2 * nF)))) return rc;
@@ -1945,7 +2175,7 @@ int flbp_adjoint_backward(flbp_engine *e, const double *grad_beliefs, double *gr
 
 int flbp_adjoint_backward_device(flbp_engine *e, const double *grad_beliefs, double *grad_p, double *grad_q) {
     int rc = begin_call(e);
-    if (rc || (rc = refuse_seq(e, "the adjoint"))) return rc;
+    if (rc || (rc = refuse_seq(e, "the adjoint")) || (rc = ensure_host_layout(e))) return rc;
     if (!grad_beliefs && e->L.V) {
         set_error("grad_beliefs is required");
         return FLBP_ERR_INVALID;
@@ -1960,7 +2190,7 @@ int flbp_get_beliefs_device(flbp_engine *e, double *out, int64_t n) {
         set_error("output length must equal the number of variables");
         return FLBP_ERR_INVALID;
     }
-    if ((rc = ensure_adjoint_maps(e))) return rc;
+    if (!e->d_int_of_var && (rc = ensure_adjoint_maps(e))) return rc;
     if (n) {
         gather_vars_kernel<<<blocks_for(n, 256), 256, 0, e->stream>>>(e->d_belief, e->d_int_of_var, n, out);
         e->launches += 1;
@@ -1972,7 +2202,7 @@ int flbp_get_beliefs_device(flbp_engine *e, double *out, int64_t n) {
 
 int flbp_set_factor_probs(flbp_engine *e, const double *p, const double *q) {
     int rc = begin_call(e);
-    if (rc || (rc = refuse_seq(e, "flbp_set_factor_probs"))) return rc;
+    if (rc || (rc = refuse_seq(e, "flbp_set_factor_probs")) || (rc = ensure_host_layout(e))) return rc;
     HostLayout &L = e->L;
     for (int64_t I = 0; I < L.F; I++) {
         if (!(p[I] >= 0.0 && p[I] <= 1.0) || !(q[I] >= 0.0 && q[I] <= 1.0)) {
@@ -2047,7 +2277,7 @@ extern "C" {
 
 int flbp_clamp_vars(flbp_engine *e, int64_t n, const int64_t *vars, const int32_t *values) {
     int rc = begin_call(e);
-    if (rc || (rc = refuse_seq(e, "flbp_clamp_vars"))) return rc;
+    if (rc || (rc = refuse_seq(e, "flbp_clamp_vars")) || (rc = ensure_host_layout(e))) return rc;
     HostLayout &L = e->L;
     if (n < 0 || (n > 0 && (!vars || !values))) {
         set_error("clamp list is malformed");
@@ -2259,7 +2489,7 @@ extern "C" {
 
 int flbp_set_update_seq(flbp_engine *e, const int64_t *seq, int64_t n) {
     int rc = begin_call(e);
-    if (rc) return rc;
+    if (rc || (rc = ensure_host_layout(e))) return rc;
     if (e->n_graphs > 0) {
         set_error("sequential update schedules are not available on batched engines");
         return FLBP_ERR_STATE;

@@ -108,6 +108,9 @@ constexpr uint32_t kHdrGraphLo = 29, kHdrGraphHi = 30;  // tile header words: gr
 // both passes read contiguously and scatter their outputs.
 struct HostLayout {
     int64_t V = 0, F = 0, E = 0;  // reference sizes
+    // false: built on the device (dlayout.h); only the counts and the small
+    // arrays (group bases, large-item runs, tiles) are filled
+    bool complete = true;
 
     uint32_t nf_sell = 0, nf_big = 0;  // active factors per path
     hvec<uint32_t> fg_base;     // n_fgroups + 1
@@ -218,8 +221,28 @@ int build_seq_layout(const flbp_graph_desc &g, const HostLayout &L, const int64_
 // names the range of graphs its items belong to (words kHdrGraphLo/Hi).
 int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, const GraphIds *graphs = nullptr);
 
+// The checks of a graph's sizes and offsets that come before any per-factor
+// work (both layout builds).
+int check_graph_shape(const flbp_graph_desc &g, std::string &err);
+
 // Fills the variable-major export maps of L (idempotent).
 void build_export_maps(HostLayout &L);
+
+// One factor of a graph: whether it is evaluated every sweep (active), the
+// state of its head (HEAD_*) and the constant message of a folded factor or
+// clamped head. False, with the message in *msg when given, for a malformed
+// factor.
+bool classify_factor(const flbp_graph_desc &g, int64_t I, uint8_t &active, uint8_t &head_state, double &fconst,
+                     std::string *msg);
+
+// log(p) - log1p(-p): the log-odds of a folded constant (computed on the
+// host by both layout builds, so that they agree bit for bit).
+double folded_logit(double p);
+
+// Tiles and headers of both passes, and the large items' per-tile
+// constants, from L's group bases and large-item runs; big_kind / big_pq:
+// kind and (p, q) of every large factor in internal order.
+void build_tiles(HostLayout &L, const uint8_t *big_kind, const double *big_pq);
 
 void set_error(const std::string &msg);
 

@@ -150,7 +150,56 @@ void par_copy(hvec<T> &v, const S *first, size_t n) {
 
 }  // namespace
 
-int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, const GraphIds *graphs) {
+bool classify_factor(const flbp_graph_desc &g, int64_t I, uint8_t &active, uint8_t &head_state, double &fconst,
+                     std::string *msg) {
+    auto fail = [&](const std::string &m) {
+        if (msg) *msg = m;
+        return false;
+    };
+    const int64_t *off = g.factor_offsets;
+    active = 0;
+    head_state = HEAD_FREE;
+    fconst = 0.0;
+    const int64_t d = off[I + 1] - off[I];
+    const int32_t t = g.factor_type[I];
+    const double p = g.factor_p[I], q = g.factor_q[I];
+    if (t != FLBP_SINGLETON && t != FLBP_AND && t != FLBP_OR)
+        return fail("unknown factor type at factor " + std::to_string(I));
+    if (!(p >= 0.0 && p <= 1.0) || !(q >= 0.0 && q <= 1.0))
+        return fail("factor probabilities must lie in [0,1] (factor " + std::to_string(I) + ")");
+    if (d < 1) return fail("factor without variables at factor " + std::to_string(I));
+    const int64_t h = g.factor_head[I];
+    if (h < off[I] || h >= off[I + 1]) return fail("factor_head outside the factor's slots at factor " + std::to_string(I));
+    if (t == FLBP_SINGLETON) {
+        if (d != 1) return fail("singleton factor with more than one variable at factor " + std::to_string(I));
+        fconst = logit(p);  // (1-p, p), causal_bp_parall.cu:110-112
+        return true;
+    }
+    bool clamped = g.factor_head_clamped && g.factor_head_clamped[I];
+    if (clamped) {
+        const double m0 = g.factor_mask0 ? g.factor_mask0[I] : 1.0;
+        const double m1 = g.factor_mask1 ? g.factor_mask1[I] : 1.0;
+        if (!((m0 == 0.0 || m0 == 1.0) && (m1 == 0.0 || m1 == 1.0)))
+            return fail("head_mask entries must be 0 or 1 (factor " + std::to_string(I) + ")");
+        if (m0 == 1.0 && m1 == 1.0) {
+            clamped = false;  // multiplying by (1,1) changes nothing
+        } else {
+            // causal_bp_parall.cu:222-238 / 271-287: marg*mask normalised, else the mask fallback.
+            fconst = (m0 == 0.0) ? kInf : -kInf;
+            head_state = (m0 == 0.0 && m1 == 1.0) ? HEAD_ONE : (m0 == 1.0 && m1 == 0.0) ? HEAD_ZERO : HEAD_NONE;
+        }
+    }
+    if (d == 1) {
+        if (!clamped) fconst = (t == FLBP_AND) ? logit(p) : -logit(p);  // :115-117, :154-156
+        return true;
+    }
+    active = 1;
+    return true;
+}
+
+double folded_logit(double p) { return logit(p); }
+
+int check_graph_shape(const flbp_graph_desc &g, std::string &err) {
     const int64_t V = g.n_vars, F = g.n_factors, E = g.n_slots;
     if (V < 0 || F < 0 || E < 0) {
         err = "negative graph size";
@@ -174,6 +223,89 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
         err = "edge slots without factors";
         return FLBP_ERR_INVALID;
     }
+    return FLBP_OK;
+}
+
+// Tiles of both passes and their headers, and the per-tile constants of the
+// large items, from the layout's group bases and large-item runs; big_kind /
+// big_pq hold the kind and (p, q) of every large factor (internal order).
+// Large items that fit a tile come first (a warp per item, staged like the
+// sliced-ELL groups); the sliced-ELL tiles follow. Items too large for a
+// tile (the first ones, by decreasing degree) are left to the warp path.
+void build_tiles(HostLayout &L, const uint8_t *big_kind, const double *big_pq) {
+    L.nf_huge = 0;
+    while (L.nf_huge < L.nf_big && L.fb_deg[L.nf_huge] - 1 > kBigFactorBody) L.nf_huge++;
+    L.nv_huge = 0;
+    while (L.nv_huge < L.nv_big && L.vb_deg[L.nv_huge] > kTileSlotsHost) L.nv_huge++;
+    auto push_hdr = [](hvec<uint32_t> &h, uint32_t first, uint32_t nflag, const uint32_t *offs, uint32_t n,
+                       uint32_t ordinal) {
+        const size_t at = h.size();
+        h.push_back(first);
+        h.push_back(nflag);
+        for (uint32_t j = 0; j + 2 < kHdrWordsHost; j++) h.push_back(offs[std::min(j, n)]);
+        if (nflag & kBigTileFlag) h[at + kHdrWordsHost - 1] = ordinal;
+    };
+    auto big_tiles = [&](const hvec<uint32_t> &boff, const hvec<uint32_t> &bdeg, uint32_t b0, uint32_t nb,
+                         hvec<uint32_t> &hdr, std::vector<uint32_t> &firsts) -> uint32_t {
+        uint32_t nt = 0, b = b0;
+        while (b < nb) {
+            const uint32_t start = b;
+            do b++;  // every item fits a tile by itself (larger ones are left to the warp path)
+            while (b < nb && b - start < kTileGroupsHost && boff[b + 1] - boff[start] <= kTileSlotsHost);
+            push_hdr(hdr, start, (b - start) | kBigTileFlag, &boff[start], b - start, nt);
+            firsts.push_back(start);
+            nt++;
+        }
+        (void)bdeg;
+        return nt;
+    };
+    auto sell_tiles = [&](const hvec<uint32_t> &base, hvec<uint32_t> &hdr) -> uint32_t {
+        const uint32_t ng = base.empty() ? 0 : (uint32_t)base.size() - 1;
+        uint32_t g = 0, nt = 0;
+        while (g < ng) {
+            const uint32_t g0 = g;
+            uint32_t slots = 0;
+            while (g < ng && g - g0 < kTileGroupsHost && slots + (base[g + 1] - base[g]) <= kTileSlotsHost) {
+                slots += base[g + 1] - base[g];
+                g++;
+            }
+            push_hdr(hdr, g0, g - g0, &base[g0], g - g0, 0);
+            nt++;
+        }
+        return nt;
+    };
+    L.fhdr.clear();
+    L.vhdr.clear();
+    std::vector<uint32_t> fbt_first, vbt_first;
+    L.n_fbtiles = big_tiles(L.fb_off, L.fb_deg, L.nf_huge, L.nf_big, L.fhdr, fbt_first);
+    L.n_ftiles = L.n_fbtiles + sell_tiles(L.fg_base, L.fhdr);
+    L.n_vbtiles = big_tiles(L.vb_off, L.vb_deg, L.nv_huge, L.nv_big, L.vhdr, vbt_first);
+    L.n_vtiles = L.n_vbtiles + sell_tiles(L.vg_base, L.vhdr);
+    // per large tile constants: degrees and kinds (factor side), degrees (variable side)
+    L.fbt_deg.assign((size_t)kTileGroupsHost * L.n_fbtiles, 0);
+    L.fbt_kind.assign((size_t)kTileGroupsHost * L.n_fbtiles, 0);
+    L.fbt_pq.assign((size_t)2 * kTileGroupsHost * L.n_fbtiles, 0.0);
+    for (uint32_t t = 0; t < L.n_fbtiles; t++) {
+        const uint32_t b0 = fbt_first[t], n = L.fhdr[(size_t)kHdrWordsHost * t + 1] & ~kBigTileFlag;
+        for (uint32_t j = 0; j < n; j++) {
+            const size_t k = (size_t)kTileGroupsHost * t + j, fi = (size_t)L.nf_sell + b0 + j;
+            L.fbt_deg[k] = L.fb_deg[b0 + j];
+            L.fbt_kind[k] = big_kind[fi - L.nf_sell];
+            L.fbt_pq[2 * k] = big_pq[2 * (fi - L.nf_sell)];
+            L.fbt_pq[2 * k + 1] = big_pq[2 * (fi - L.nf_sell) + 1];
+        }
+    }
+    L.vbt_deg.assign((size_t)kTileGroupsHost * L.n_vbtiles, 0);
+    for (uint32_t t = 0; t < L.n_vbtiles; t++) {
+        const uint32_t b0 = vbt_first[t], n = L.vhdr[(size_t)kHdrWordsHost * t + 1] & ~kBigTileFlag;
+        for (uint32_t j = 0; j < n; j++) L.vbt_deg[(size_t)kTileGroupsHost * t + j] = L.vb_deg[b0 + j];
+    }
+}
+
+int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, const GraphIds *graphs) {
+    const int64_t V = g.n_vars, F = g.n_factors, E = g.n_slots;
+    if (int rc = check_graph_shape(g, err)) return rc;
+    const int64_t *off = g.factor_offsets;
     {  // first offending index, as a sequential scan reports it
         int64_t bad_f = F, bad_e = E;
 #pragma omp parallel for reduction(min : bad_f) if (F >= kParMin)
@@ -203,46 +335,13 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
     hvec<double> fconst = par_vec<double>(F, 0.0);  // constant message of non-active factors / clamped heads
     // classify factor I; false (with the message in *msg when given) for a malformed factor
     auto classify = [&](int64_t I, std::string *msg) -> bool {
-        auto fail = [&](const std::string &m) {
-            if (msg) *msg = m;
-            return false;
-        };
-        const int64_t d = off[I + 1] - off[I];
-        const int32_t t = g.factor_type[I];
-        const double p = g.factor_p[I], q = g.factor_q[I];
-        if (t != FLBP_SINGLETON && t != FLBP_AND && t != FLBP_OR)
-            return fail("unknown factor type at factor " + std::to_string(I));
-        if (!(p >= 0.0 && p <= 1.0) || !(q >= 0.0 && q <= 1.0))
-            return fail("factor probabilities must lie in [0,1] (factor " + std::to_string(I) + ")");
-        if (d < 1) return fail("factor without variables at factor " + std::to_string(I));
-        const int64_t h = g.factor_head[I];
-        if (h < off[I] || h >= off[I + 1])
-            return fail("factor_head outside the factor's slots at factor " + std::to_string(I));
-        if (t == FLBP_SINGLETON) {
-            if (d != 1) return fail("singleton factor with more than one variable at factor " + std::to_string(I));
-            fconst[I] = logit(p);  // (1-p, p), causal_bp_parall.cu:110-112
-            return true;
-        }
-        bool clamped = g.factor_head_clamped && g.factor_head_clamped[I];
-        if (clamped) {
-            const double m0 = g.factor_mask0 ? g.factor_mask0[I] : 1.0;
-            const double m1 = g.factor_mask1 ? g.factor_mask1[I] : 1.0;
-            if (!((m0 == 0.0 || m0 == 1.0) && (m1 == 0.0 || m1 == 1.0)))
-                return fail("head_mask entries must be 0 or 1 (factor " + std::to_string(I) + ")");
-            if (m0 == 1.0 && m1 == 1.0) {
-                clamped = false;  // multiplying by (1,1) changes nothing
-            } else {
-                // causal_bp_parall.cu:222-238 / 271-287: marg*mask normalised, else the mask fallback.
-                fconst[I] = (m0 == 0.0) ? kInf : -kInf;
-                head_state[I] = (m0 == 0.0 && m1 == 1.0) ? HEAD_ONE : (m0 == 1.0 && m1 == 0.0) ? HEAD_ZERO : HEAD_NONE;
-            }
-        }
-        if (d == 1) {
-            if (!clamped) fconst[I] = (t == FLBP_AND) ? logit(p) : -logit(p);  // :115-117, :154-156
-            return true;
-        }
-        active[I] = 1;
-        return true;
+        uint8_t act = 0, hs = HEAD_FREE;
+        double c = 0.0;
+        const bool ok = classify_factor(g, I, act, hs, c, msg);
+        active[I] = act;
+        head_state[I] = hs;
+        fconst[I] = c;
+        return ok;
     };
     {
         int64_t bad = F;
@@ -473,9 +572,12 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
         }
         par_assign(L.v_ent, pos, kSentinel);
         par_assign(L.f_pos, L.n_slots, kSentinel);  // slot -> entry receiving its f->v message
-        // The (variable, device slot) pairs in slot order, stably radix-sorted
-        // by variable (11-bit digits): each variable's slots end up together
-        // in increasing order, and entry k of a variable gets its k-th.
+        // The (variable, device slot) pairs in the reference's factor-major
+        // slot order, stably radix-sorted by variable (11-bit digits): each
+        // variable's slots end up together, and entry k of a variable is its
+        // k-th slot in the reference's order. That order belongs to the graph,
+        // not to the layout, so a variable sums its messages in the same order
+        // whether its graph is solved alone or in a batch.
         hvec<uint32_t> kv, ks, kv2, ks2;  // variable, slot
         {
             constexpr int kBits = 11;
@@ -490,16 +592,15 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
             ks2.resize(n_ent);
             for (int ps = 0; ps < passes; ps++) {
                 const int sh = ps * kBits;
-                if (ps == 0) {  // straight from the slots
-                    const Chunks c = chunks((int64_t)L.n_slots, nk);
-                    auto key = [&](int64_t sl) -> size_t {
-                        const uint32_t v = var_of_dev[sl];
-                        return v == UINT32_MAX ? nk : (v & (nk - 1));
+                if (ps == 0) {  // straight from the reference slots that are entries
+                    const Chunks c = chunks(E, nk);
+                    auto key = [&](int64_t e) -> size_t {
+                        return entry[e] ? ((uint32_t)g.slot_var[e] & (nk - 1)) : nk;
                     };
                     const std::vector<uint64_t> cnt = class_counts(c, nk, key);
-                    class_place(c, nk, cnt, class_starts(c, nk, cnt, 0), key, [&](int64_t sl, uint64_t at) {
-                        kv2[at] = var_of_dev[sl];
-                        ks2[at] = (uint32_t)sl;
+                    class_place(c, nk, cnt, class_starts(c, nk, cnt, 0), key, [&](int64_t e, uint64_t at) {
+                        kv2[at] = (uint32_t)g.slot_var[e];
+                        ks2[at] = dev_slot[e];
                     });
                 } else {
                     const Chunks c = chunks((int64_t)n_ent, nk);
@@ -530,58 +631,10 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
         }
     }
 
-    // --- tiles and their headers ------------------------------------------------------
-    // Large items that fit a tile come first (a warp per item, staged like the
-    // sliced-ELL groups); the sliced-ELL tiles follow. Items too large for a
-    // tile (the first ones, by decreasing degree) are left to the warp path.
-    L.nf_huge = 0;
-    while (L.nf_huge < L.nf_big && L.fb_deg[L.nf_huge] - 1 > kBigFactorBody) L.nf_huge++;
-    L.nv_huge = 0;
-    while (L.nv_huge < L.nv_big && L.vb_deg[L.nv_huge] > kTileSlotsHost) L.nv_huge++;
-    auto push_hdr = [](hvec<uint32_t> &h, uint32_t first, uint32_t nflag, const uint32_t *offs, uint32_t n,
-                       uint32_t ordinal) {
-        const size_t at = h.size();
-        h.push_back(first);
-        h.push_back(nflag);
-        for (uint32_t j = 0; j + 2 < kHdrWordsHost; j++) h.push_back(offs[std::min(j, n)]);
-        if (nflag & kBigTileFlag) h[at + kHdrWordsHost - 1] = ordinal;
-    };
-    auto big_tiles = [&](const hvec<uint32_t> &boff, const hvec<uint32_t> &bdeg, uint32_t b0, uint32_t nb,
-                         hvec<uint32_t> &hdr, std::vector<uint32_t> &firsts) -> uint32_t {
-        uint32_t nt = 0, b = b0;
-        while (b < nb) {
-            const uint32_t start = b;
-            do b++;  // every item fits a tile by itself (larger ones are left to the warp path)
-            while (b < nb && b - start < kTileGroupsHost && boff[b + 1] - boff[start] <= kTileSlotsHost);
-            push_hdr(hdr, start, (b - start) | kBigTileFlag, &boff[start], b - start, nt);
-            firsts.push_back(start);
-            nt++;
-        }
-        (void)bdeg;
-        return nt;
-    };
-    auto sell_tiles = [&](const hvec<uint32_t> &base, hvec<uint32_t> &hdr) -> uint32_t {
-        const uint32_t ng = base.empty() ? 0 : (uint32_t)base.size() - 1;
-        uint32_t g = 0, nt = 0;
-        while (g < ng) {
-            const uint32_t g0 = g;
-            uint32_t slots = 0;
-            while (g < ng && g - g0 < kTileGroupsHost && slots + (base[g + 1] - base[g]) <= kTileSlotsHost) {
-                slots += base[g + 1] - base[g];
-                g++;
-            }
-            push_hdr(hdr, g0, g - g0, &base[g0], g - g0, 0);
-            nt++;
-        }
-        return nt;
-    };
-    L.fhdr.clear();
-    L.vhdr.clear();
-    std::vector<uint32_t> fbt_first, vbt_first;
-    L.n_fbtiles = big_tiles(L.fb_off, L.fb_deg, L.nf_huge, L.nf_big, L.fhdr, fbt_first);
-    L.n_ftiles = L.n_fbtiles + sell_tiles(L.fg_base, L.fhdr);
-    L.n_vbtiles = big_tiles(L.vb_off, L.vb_deg, L.nv_huge, L.nv_big, L.vhdr, vbt_first);
-    L.n_vtiles = L.n_vbtiles + sell_tiles(L.vg_base, L.vhdr);
+    // --- tiles and their headers, per large tile constants ---------------------------
+    std::vector<uint8_t> big_kind(L.f_kind.begin() + nf_sell, L.f_kind.end());
+    std::vector<double> big_pq(L.f_pq.begin() + 2 * (size_t)nf_sell, L.f_pq.end());
+    build_tiles(L, big_kind.data(), big_pq.data());
     // batched engines: the range of graphs of every tile's items
     if (graphs) {
         auto stamp = [&](hvec<uint32_t> &hdr, uint32_t nt, uint32_t n_sell_items, auto item_graph) {
@@ -606,26 +659,6 @@ int build_layout(const flbp_graph_desc &g, HostLayout &L, std::string &err, cons
         };
         stamp(L.fhdr, L.n_ftiles, nf_sell, [&](uint32_t f) { return fgraph(fact_of_int[f]); });
         stamp(L.vhdr, L.n_vtiles, nv_sell, [&](uint32_t iv) { return vgraph(order[iv]); });
-    }
-
-    // per large tile constants: degrees and kinds (factor side), degrees (variable side)
-    L.fbt_deg.assign((size_t)kTileGroupsHost * L.n_fbtiles, 0);
-    L.fbt_kind.assign((size_t)kTileGroupsHost * L.n_fbtiles, 0);
-    L.fbt_pq.assign((size_t)2 * kTileGroupsHost * L.n_fbtiles, 0.0);
-    for (uint32_t t = 0; t < L.n_fbtiles; t++) {
-        const uint32_t b0 = fbt_first[t], n = L.fhdr[(size_t)kHdrWordsHost * t + 1] & ~kBigTileFlag;
-        for (uint32_t j = 0; j < n; j++) {
-            const size_t k = (size_t)kTileGroupsHost * t + j, fi = (size_t)nf_sell + b0 + j;
-            L.fbt_deg[k] = L.fb_deg[b0 + j];
-            L.fbt_kind[k] = L.f_kind[fi];
-            L.fbt_pq[2 * k] = L.f_pq[2 * fi];
-            L.fbt_pq[2 * k + 1] = L.f_pq[2 * fi + 1];
-        }
-    }
-    L.vbt_deg.assign((size_t)kTileGroupsHost * L.n_vbtiles, 0);
-    for (uint32_t t = 0; t < L.n_vbtiles; t++) {
-        const uint32_t b0 = vbt_first[t], n = L.vhdr[(size_t)kHdrWordsHost * t + 1] & ~kBigTileFlag;
-        for (uint32_t j = 0; j < n; j++) L.vbt_deg[(size_t)kTileGroupsHost * t + j] = L.vb_deg[b0 + j];
     }
 
     // --- priors ------------------------------------------------------------------

@@ -365,6 +365,23 @@ int flbp_adjoint_backward_device(flbp_engine *eng, const double *grad_beliefs, d
 /* flbp_get_beliefs into a device buffer of the engine's device. */
 int flbp_get_beliefs_device(flbp_engine *eng, double *out, int64_t n_vars);
 
+/* Where new engines build their device layout (process-wide; no counterpart
+ * in FastLBP, whose construct() builds its edge records on the host,
+ * csrc/ext/causal_bp.cu:310-407, 724-817): 0 (default) on the GPU for graphs
+ * of at least 2^18 edge slots and on the host below that, 1 always on the
+ * host, 2 always on the GPU. Both builds give the same layout bit for bit.
+ * A GPU-built engine keeps the caller's graph arrays in device memory and
+ * builds the complete host-side layout only when a call needs it (message
+ * export, gradients, clamps, schedules, new probabilities). Batched engines
+ * always build on the host. */
+int flbp_set_layout_builder(int32_t mode);
+
+/* Digest (64-bit FNV-1a) of an engine's device layout as its kernels read
+ * it: every layout buffer copied back, and the layout's counts; equal
+ * digests mean equal layouts. *built_on_device (may be NULL): 1 when the
+ * engine's layout was built on the GPU. */
+int flbp_engine_layout_digest(flbp_engine *eng, uint64_t *digest, int32_t *built_on_device);
+
 /* A digest (64-bit FNV-1a) of the device layout the engine would build for
  * `graph` (no counterpart in the reference; needs no GPU), built on the host
  * with `threads` threads (0: all). For batches, factor_graph / var_graph give

@@ -75,14 +75,8 @@ def test_golden_graphs_match_generator():
     assert text == W.config0(0).text()
 
 
-# The high-fan-in case parts from the reference from sweep 4 on: its FP64
-# probability products underflow to exact zeros, the engine's log-odds do not
-# (a documented deviation; the oracle reproduces the reference's underflow).
-ENGINE_SKIP = {"cfg2_small_clamped_fixed100"}
-
-
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", [c for c in CASES if c not in ENGINE_SKIP])
+@pytest.mark.parametrize("name", CASES)
 def test_engine_matches_reference_binary(name):
     """The FP64 engine (PARALL or the case's sequential schedule) against the
     reference's own beliefs."""

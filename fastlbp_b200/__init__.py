@@ -6,8 +6,9 @@ the C ABI of include/fastlbp_b200.h and the libDAI-style C++ API of
 include/ext/*.h). This package loads it with ctypes.
 """
 
-from .api import BatchEngine, CausalBP, CausalFactorGraph, Engine, PropertySet, seq_batches, update_seq  # noqa: F401
+from .api import (BatchEngine, CausalBP, CausalFactorGraph, Engine, PropertySet, SetsEngine, seq_batches,  # noqa: F401
+                  update_seq)
 from ._native import FlbpError, lib  # noqa: F401
 
-__all__ = ["BatchEngine", "CausalBP", "CausalFactorGraph", "Engine", "PropertySet", "FlbpError", "lib", "seq_batches",
-           "update_seq"]
+__all__ = ["BatchEngine", "CausalBP", "CausalFactorGraph", "Engine", "PropertySet", "SetsEngine", "FlbpError", "lib",
+           "seq_batches", "update_seq"]

@@ -510,6 +510,49 @@ class BatchEngine(Engine):
         return b[self.var_off[g]:self.var_off[g + 1]]
 
 
+class SetsEngine(Engine):
+    """Evidence sets on one graph (flbp_sets_*): the graph's layout once, per
+    set its own clamps, messages and beliefs; every set stops on its own
+    tolerance rule. beliefs() holds n_sets x n_vars values (set k in row k)."""
+
+    def __init__(self, arrays: Dict[str, np.ndarray], sets: Sequence[Dict[int, int]], precision: int = 32,
+                 damping: float = 0.0, stream: Optional[int] = None, device: int = -1):
+        """sets: one {graph variable index: 0/1} clamp map per evidence set."""
+        keep = []
+        desc = _desc_from_arrays(arrays, keep)
+        off = np.zeros(len(sets) + 1, np.int64)
+        vs, vl = [], []
+        for k, cl in enumerate(sets):
+            for v, x in sorted(cl.items()):
+                vs.append(int(v))
+                vl.append(int(x))
+            off[k + 1] = len(vs)
+        vs_a, vl_a = np.array(vs, np.int64), np.array(vl, np.int32)
+        opts = N.EngineOpts(int(precision), int(device), float(damping), stream)
+        h = C.c_void_p()
+        check(lib().flbp_sets_create(C.byref(desc), len(sets), off, vs_a.ctypes.data_as(C.c_void_p),
+                                     vl_a.ctypes.data_as(C.c_void_p), C.byref(opts), C.byref(h)))
+        self._h = h
+        self.n_sets = len(sets)
+        self.n_vars = int(desc.n_vars)
+        self.n_slots = int(desc.n_slots)
+        self.n_factors = int(desc.n_factors)
+        self.info = None
+
+    def run_sets_tol(self, tol=1e-6, maxiter=500, maxtime=1e9):
+        """Per-set sweeps and stop reasons (0 converged, 2 iteration/time limit)."""
+        sweeps = np.zeros(self.n_sets, np.int64)
+        reasons = np.zeros(self.n_sets, np.int32)
+        check(lib().flbp_sets_run_tol(self._h, float(tol), int(maxiter), float(maxtime), sweeps, reasons,
+                                      self._info()))
+        return sweeps, reasons
+
+    def beliefs(self) -> np.ndarray:
+        out = np.zeros(self.n_sets * self.n_vars)
+        check(lib().flbp_get_beliefs(self._h, out, out.size))
+        return out.reshape(self.n_sets, self.n_vars)
+
+
 class CausalBP:
     """CausalBP(fg, opts) with the reference's run semantics (include/ext/causal_bp.h:167-193)."""
 

@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "direct.cuh"
 #include "direct_launch.h"
 
@@ -71,6 +73,71 @@ cudaError_t direct_var_launch(int form, int bmode, bool damp, unsigned grid, con
     void *params[] = {&args, &fvp, &vfp, &fvdp, &dd, &ctl};
     return cudaLaunchKernel(var_kernel<T>(form, bmode, damp), dim3(grid), dim3(kDirectThreads), params, 0, st);
 }
+
+// Evidence sets: cut entries get no message (their f->v values are zeroed
+// after every factor pass), clamped variables' v->f messages start at +-inf.
+template <typename T>
+__global__ void sets_cut_kernel(const uint2 *__restrict__ cut, uint32_t n, T *fv, uint64_t fv_stride,
+                                const int *done) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint2 c = cut[i];  // (set, entry)
+        if (!done[c.x]) fv[c.x * fv_stride + c.y] = T(0);
+    }
+}
+
+template <typename T>
+__global__ void sets_slots_kernel(const uint4 *__restrict__ sl, uint32_t n, T *vf, uint64_t vf_stride) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint4 c = sl[i];  // (set, slot, value, -)
+        vf[c.x * vf_stride + c.y] = c.z ? Num<T>::inf() : -Num<T>::inf();
+    }
+}
+
+template <typename T>
+cudaError_t sets_factor_launch(unsigned gx, unsigned n_sets, const FactorArgs &a, const T *vf, T *fv, Ctl *ctl,
+                               const uint2 *cut, uint32_t n_cut, cudaStream_t st) {
+    FactorArgs args = a;
+    const T *vfp = vf;
+    T *fvp = fv;
+    void *params[] = {&args, &vfp, &fvp, &ctl};
+    cudaError_t e = cudaLaunchKernel((const void *)factor_direct_kernel<T, 2, true>, dim3(gx, n_sets),
+                                     dim3(kDirectThreads), params, 0, st);
+    if (e == cudaSuccess && n_cut)
+        sets_cut_kernel<T><<<std::min<uint32_t>((n_cut + 255) / 256, 4096), 256, 0, st>>>(cut, n_cut, fv,
+                                                                                          a.set_fv_stride, a.set_done);
+    return e == cudaSuccess ? cudaGetLastError() : e;
+}
+
+template <typename T>
+cudaError_t sets_var_launch(bool damp, unsigned gx, unsigned n_sets, const VarArgs &a, const T *fv, T *vf, T *fvd,
+                            T d, Ctl *ctl, cudaStream_t st) {
+    VarArgs args = a;
+    const T *fvp = fv;
+    T *vfp = vf, *fvdp = fvd;
+    T dd = d;
+    void *params[] = {&args, &fvp, &vfp, &fvdp, &dd, &ctl};
+    const void *fn = damp ? (const void *)var_direct_kernel<T, 4, true, true, 2, true>
+                          : (const void *)var_direct_kernel<T, 4, true, false, 2, true>;
+    return cudaLaunchKernel(fn, dim3(gx, n_sets), dim3(kDirectThreads), params, 0, st);
+}
+
+template <typename T>
+cudaError_t sets_init_slots(const uint4 *slots, uint32_t n, T *vf, uint64_t vf_stride, cudaStream_t st) {
+    if (!n) return cudaSuccess;
+    sets_slots_kernel<T><<<std::min<uint32_t>((n + 255) / 256, 4096), 256, 0, st>>>(slots, n, vf, vf_stride);
+    return cudaGetLastError();
+}
+
+template cudaError_t sets_factor_launch<float>(unsigned, unsigned, const FactorArgs &, const float *, float *, Ctl *,
+                                               const uint2 *, uint32_t, cudaStream_t);
+template cudaError_t sets_factor_launch<double>(unsigned, unsigned, const FactorArgs &, const double *, double *,
+                                                Ctl *, const uint2 *, uint32_t, cudaStream_t);
+template cudaError_t sets_var_launch<float>(bool, unsigned, unsigned, const VarArgs &, const float *, float *, float *,
+                                            float, Ctl *, cudaStream_t);
+template cudaError_t sets_var_launch<double>(bool, unsigned, unsigned, const VarArgs &, const double *, double *,
+                                             double *, double, Ctl *, cudaStream_t);
+template cudaError_t sets_init_slots<float>(const uint4 *, uint32_t, float *, uint64_t, cudaStream_t);
+template cudaError_t sets_init_slots<double>(const uint4 *, uint32_t, double *, uint64_t, cudaStream_t);
 
 template <typename T>
 int direct_blocks_per_sm(int form, bool var, bool damp) {

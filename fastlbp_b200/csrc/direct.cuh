@@ -117,12 +117,18 @@ __device__ __forceinline__ FItem<T> factor_item(const FactorArgs &a, uint32_t it
 // factors too large for a warp first (one per block), then every warp takes
 // items it = warp, warp + all warps, ... (neighbouring warps work on
 // neighbouring items, which keeps the scattered stores of a pass close
-// together).
-template <typename T, int MINB>
+// together). SETS: evidence set blockIdx.y of an engine of sets (its
+// messages at the set's strides; a stopped set does no work).
+template <typename T, int MINB, bool SETS = false>
 __global__ void __launch_bounds__(kDirectThreads, MINB) factor_direct_kernel(FactorArgs a, const T *__restrict__ vf,
                                                                              T *__restrict__ fv, Ctl *ctl) {
     if (*(volatile int *)&ctl->done) return;
-    if (blockIdx.x == 0 && threadIdx.x == 0) sweep_open(ctl);
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) sweep_open(ctl);
+    if (SETS) {
+        if (a.set_done[blockIdx.y]) return;
+        vf += blockIdx.y * a.set_vf_stride;
+        fv += blockIdx.y * a.set_fv_stride;
+    }
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     {
         __shared__ typename WideAcc<T>::type s_l[kConsumerWarps];
@@ -268,14 +274,18 @@ __device__ __forceinline__ double var_warp_direct(const VarArgs &a, uint32_t b, 
 // Variable pass, direct form: variables too large for a warp first (one per
 // block), then items it = warp, warp + all warps, ...: [0, nbig) the large
 // variables that fit a warp, then the sliced-ELL groups (lane = variable).
-// Residual, counts and stop rules as in the staged form (var_close).
-template <typename T, int BMODE, bool WRITE_VF, bool DAMP, int MINB>
+// Residual, counts and stop rules as in the staged form (var_close). SETS:
+// evidence set blockIdx.y of an engine of sets (BMODE 4 with the set as the
+// graph); the blocks of a stopped set do no work but still take part in
+// the end-of-pass count.
+template <typename T, int BMODE, bool WRITE_VF, bool DAMP, int MINB, bool SETS = false>
 __global__ void __launch_bounds__(kDirectThreads, MINB) var_direct_kernel(VarArgs a, const T *__restrict__ fv,
                                                                           T *__restrict__ vf, T *__restrict__ fvd, T d,
                                                                           Ctl *ctl) {
     constexpr bool RESID = (BMODE == 1 || BMODE == 2 || BMODE == 4);
     if (*(volatile int *)&ctl->done) return;
-    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->fnext = 0u;  // the next staged factor pass starts after this kernel
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
+        ctl->fnext = 0u;  // the next staged factor pass starts after this kernel
     const double pscale = ctl->pscale;
     const double tol = ctl->tol;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -286,40 +296,53 @@ __global__ void __launch_bounds__(kDirectThreads, MINB) var_direct_kernel(VarArg
     if (BMODE == 4)
         for (int w = threadIdx.x; w < kMovedWords; w += blockDim.x) s_moved[w] = 0u;
     if (a.v_graph) load_done_bits(s_done, a.gstate, a.n_graphs, lane, wid, blockDim.x >> 5);
-    __syncthreads();
-    {
-        __shared__ typename WideAcc<T>::type s_s[kConsumerWarps];
-        __shared__ int s_np[kConsumerWarps], s_nn[kConsumerWarps];
-        for (uint32_t b = blockIdx.x; b < a.nv_huge; b += gridDim.x) {
-            const uint32_t g = a.v_graph ? a.v_graph[a.nv_sell + b] : 0;
-            if (a.v_graph && graph_done(s_done, a.gstate, g)) continue;  // stopped graph (batched solve)
-            const double dd = var_block_huge<T, BMODE, WRITE_VF, DAMP>(a, b, threadIdx.x, fv, vf, fvd, d, pscale, tol,
-                                                                       cnt, s_s, s_np, s_nn);
-            dmax = fmax(dmax, dd);
-            if (BMODE == 4 && dd > tol) mark_moved(s_moved, a, g);
-        }
+    const uint32_t set = SETS ? blockIdx.y : 0u;
+    bool set_live = true;
+    if (SETS) {
+        set_live = a.gstate[set] == 0;
+        fv += set * a.set_fv_stride;
+        vf += set * a.set_vf_stride;
+        if (DAMP) fvd += set * a.set_fv_stride;
+        a.prior = reinterpret_cast<const unsigned char *>(a.prior) + set * a.set_prior_stride;
+        a.belief += set * a.set_belief_stride;
     }
-    const uint32_t nbig = a.nv_big - a.nv_huge;
-    const uint32_t n_items = nbig + a.n_vgroups;
-    const uint32_t stride = gridDim.x * (uint32_t)kConsumerWarps;
-    for (uint32_t it = blockIdx.x * (uint32_t)kConsumerWarps + wid; it < n_items; it += stride) {
-        if (it < nbig) {
-            const uint32_t b = a.nv_huge + it;
-            const uint32_t g = a.v_graph ? a.v_graph[a.nv_sell + b] : 0;
-            if (a.v_graph && graph_done(s_done, a.gstate, g)) continue;
-            const double dd = var_warp_direct<T, BMODE, WRITE_VF, DAMP>(a, b, fv, vf, fvd, d, pscale, tol, lane, cnt);
-            dmax = fmax(dmax, dd);
-            if (BMODE == 4 && dd > tol) mark_moved(s_moved, a, g);
-        } else {
-            const uint32_t grp = it - nbig;
-            const uint32_t base = __ldcs(a.vg_base + grp), end = __ldcs(a.vg_base + grp + 1);
-            const uint32_t v = 32u * grp + lane;
-            const uint32_t g = a.v_graph ? a.v_graph[v] : 0;
-            const bool live = !(a.v_graph && graph_done(s_done, a.gstate, g));
-            const double dd = var_group_direct_w<T, BMODE, WRITE_VF, DAMP>(
-                (int)((end - base) >> 5), a, fv, vf, fvd, d, base, v, live, pscale, tol, lane, cnt);
-            dmax = fmax(dmax, dd);
-            if (BMODE == 4 && dd > tol) mark_moved(s_moved, a, g);
+    __syncthreads();
+    if (set_live) {
+        {
+            __shared__ typename WideAcc<T>::type s_s[kConsumerWarps];
+            __shared__ int s_np[kConsumerWarps], s_nn[kConsumerWarps];
+            for (uint32_t b = blockIdx.x; b < a.nv_huge; b += gridDim.x) {
+                const uint32_t g = SETS ? set : a.v_graph ? a.v_graph[a.nv_sell + b] : 0;
+                if (a.v_graph && graph_done(s_done, a.gstate, g)) continue;  // stopped graph (batched solve)
+                const double dd = var_block_huge<T, BMODE, WRITE_VF, DAMP>(a, b, threadIdx.x, fv, vf, fvd, d, pscale,
+                                                                           tol, cnt, s_s, s_np, s_nn);
+                dmax = fmax(dmax, dd);
+                if (BMODE == 4 && dd > tol) mark_moved(s_moved, a, g);
+            }
+        }
+        const uint32_t nbig = a.nv_big - a.nv_huge;
+        const uint32_t n_items = nbig + a.n_vgroups;
+        const uint32_t stride = gridDim.x * (uint32_t)kConsumerWarps;
+        for (uint32_t it = blockIdx.x * (uint32_t)kConsumerWarps + wid; it < n_items; it += stride) {
+            if (it < nbig) {
+                const uint32_t b = a.nv_huge + it;
+                const uint32_t g = SETS ? set : a.v_graph ? a.v_graph[a.nv_sell + b] : 0;
+                if (a.v_graph && graph_done(s_done, a.gstate, g)) continue;
+                const double dd =
+                    var_warp_direct<T, BMODE, WRITE_VF, DAMP>(a, b, fv, vf, fvd, d, pscale, tol, lane, cnt);
+                dmax = fmax(dmax, dd);
+                if (BMODE == 4 && dd > tol) mark_moved(s_moved, a, g);
+            } else {
+                const uint32_t grp = it - nbig;
+                const uint32_t base = __ldcs(a.vg_base + grp), end = __ldcs(a.vg_base + grp + 1);
+                const uint32_t v = 32u * grp + lane;
+                const uint32_t g = SETS ? set : a.v_graph ? a.v_graph[v] : 0;
+                const bool live = !(a.v_graph && graph_done(s_done, a.gstate, g));
+                const double dd = var_group_direct_w<T, BMODE, WRITE_VF, DAMP>(
+                    (int)((end - base) >> 5), a, fv, vf, fvd, d, base, v, live, pscale, tol, lane, cnt);
+                dmax = fmax(dmax, dd);
+                if (BMODE == 4 && dd > tol) mark_moved(s_moved, a, g);
+            }
         }
     }
     if (RESID) var_close<BMODE>(a, ctl, dmax, cnt, s_moved, lane, wid);

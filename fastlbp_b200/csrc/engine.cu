@@ -138,6 +138,17 @@ struct flbp_engine {
     bool lowpass_valid = false;
     size_t bytes = 0;
     size_t h2d_bytes = 0;  // host->device bytes copied by create
+    // Evidence sets on one graph (flbp_sets_create): n_sets copies of the
+    // messages, priors and beliefs at these strides (elements); (set, entry)
+    // pairs that no message reaches, (set, slot, value, -) of the clamped
+    // variables' slots; the sweep's grid width.
+    uint32_t n_sets = 0;
+    uint64_t set_vs = 0, set_es = 0, set_nv = 0;
+    uint2 *d_set_cut = nullptr;
+    uint32_t n_set_cut = 0;
+    uint4 *d_set_slots = nullptr;
+    uint32_t n_set_slots = 0;
+    unsigned set_fgx = 1, set_vgx = 1;
     // Layout built on the device (dlayout.h): the caller's graph arrays stay
     // on the device until the complete host layout is first needed.
     bool dev_layout = false;
@@ -396,6 +407,28 @@ void launch_var_mode(flbp_engine *e, const VarArgs &va, int mode) {
 // which: bit 0 launches the factor pass, bit 1 the variable pass.
 template <typename T>
 void launch_sweep(flbp_engine *e, int mode, int which = 3) {
+    if (e->n_sets) {  // evidence sets: the direct form over grid.y = set, per-set stop rules
+        if (which & 1) {
+            FactorArgs fa = factor_args<T>(e);
+            fa.set_done = e->d_gstate;
+            fa.set_vf_stride = e->set_vs;
+            fa.set_fv_stride = e->set_es;
+            sets_factor_launch<T>(e->set_fgx, e->n_sets, fa, (const T *)e->d_vf, (T *)e->d_fv, e->d_ctl, e->d_set_cut,
+                                  e->n_set_cut, e->stream);
+        }
+        if (which & 2) {
+            VarArgs va = var_args(e);
+            va.gstate = e->d_gstate;
+            va.n_graphs = e->n_sets;
+            va.set_vf_stride = e->set_vs;
+            va.set_fv_stride = e->set_es;
+            va.set_prior_stride = e->set_nv * (e->prec == 64 ? 16 : 8);
+            va.set_belief_stride = e->set_nv;
+            sets_var_launch<T>(e->damping != 0.0, e->set_vgx, e->n_sets, va, (const T *)e->d_fv, (T *)e->d_vf,
+                               (T *)e->d_fvd, (T)e->damping, e->d_ctl, e->stream);
+        }
+        return;
+    }
     if (which & 1) {
         FactorArgs fa = factor_args<T>(e);
         if (mode == 3) {
@@ -480,7 +513,7 @@ int sweep_graph(flbp_engine *e, int mode, int n, cudaGraphExec_t *out) {
 // a sequential schedule of about 2048 kernels).
 int launch_sweeps(flbp_engine *e, int mode, long long n) {
     if (e->L.nf_sell + e->L.nf_big == 0 && e->L.V == 0) return FLBP_OK;
-    const long long per = e->seq ? seq_sweep_launches(e, mode, 3) : 2;
+    const long long per = e->seq ? seq_sweep_launches(e, mode, 3) : 2 + (e->n_sets && e->n_set_cut ? 1 : 0);
     int kmax = 64;
     if (e->seq)
         while (kmax > 1 && (long long)kmax * per > 2048) kmax /= 2;
@@ -594,6 +627,13 @@ int refuse_seq(flbp_engine *e, const char *what) {
     return FLBP_ERR_STATE;
 }
 
+// Entry points of a single graph's run state that an engine of evidence sets does not support.
+int refuse_sets(flbp_engine *e, const char *what) {
+    if (!e->n_sets) return FLBP_OK;
+    set_error(std::string(what) + " is not available on an engine of evidence sets (use flbp_sets_run_tol)");
+    return FLBP_ERR_STATE;
+}
+
 int record_start(flbp_engine *e) {
     FLBP_CUDA(cudaEventRecord(e->ev0, e->stream));
     return FLBP_OK;
@@ -670,7 +710,7 @@ struct BatchSpec {
 };
 
 int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, flbp_engine **out,
-                  const BatchSpec *batch);
+                  const BatchSpec *batch, bool host_layout = false);
 
 }  // namespace
 
@@ -805,7 +845,7 @@ void adopt_dev_layout(flbp_engine *e, DevLayout &D) {
 }
 
 int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, flbp_engine **out,
-                  const BatchSpec *batch) {
+                  const BatchSpec *batch, bool host_layout) {
     auto clk = [] { return std::chrono::steady_clock::now(); };
     auto us = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
         return (int64_t)std::chrono::duration_cast<std::chrono::microseconds>(b - a).count();
@@ -835,7 +875,7 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
     int rc = FLBP_OK;
     // The host build runs first (a malformed graph is reported without a
     // GPU); the device build needs the engine's device and stream.
-    const bool on_device = !batch && use_device_layout(*graph);
+    const bool on_device = !batch && !host_layout && use_device_layout(*graph);
     if (!on_device) {
         GraphIds ids{0, nullptr, nullptr};
         if (batch)
@@ -1159,6 +1199,8 @@ int flbp_engine_destroy(flbp_engine *e) {
         if (b) cudaFree(b);
     for (void *b : e->d_in)
         if (b) cudaFree(b);
+    if (e->d_set_cut) cudaFree(e->d_set_cut);
+    if (e->d_set_slots) cudaFree(e->d_set_slots);
     if (e->h_ctl) cudaFreeHost(e->h_ctl);
     if (e->ev0) cudaEventDestroy(e->ev0);
     if (e->ev1) cudaEventDestroy(e->ev1);
@@ -1170,6 +1212,21 @@ int flbp_engine_destroy(flbp_engine *e) {
 int flbp_init(flbp_engine *e) {
     int rc = begin_call(e);
     if (rc) return rc;
+    if (e->n_sets) {  // every set's messages uniform, its clamped variables' v->f messages +-inf, its
+                      // beliefs 0 (those of a new engine, for the tolerance rule's first sweep)
+        FLBP_CUDA(cudaMemsetAsync(e->d_vf, 0, e->n_sets * e->set_vs * e->tsize, e->stream));
+        FLBP_CUDA(cudaMemsetAsync(e->d_belief, 0, e->n_sets * e->set_nv * sizeof(double), e->stream));
+        FLBP_CUDA(cudaMemsetAsync(e->d_fv, 0, e->n_sets * e->set_es * e->tsize, e->stream));
+        if (e->d_fvd) FLBP_CUDA(cudaMemsetAsync(e->d_fvd, 0, e->n_sets * e->set_es * e->tsize, e->stream));
+        FLBP_CUDA(e->prec == 64 ? sets_init_slots<double>(e->d_set_slots, e->n_set_slots, (double *)e->d_vf, e->set_vs,
+                                                          e->stream)
+                                : sets_init_slots<float>(e->d_set_slots, e->n_set_slots, (float *)e->d_vf, e->set_vs,
+                                                         e->stream));
+        e->launches += e->n_set_slots ? 1 : 0;
+        e->t = 0;
+        e->lowpass_valid = false;
+        return FLBP_OK;
+    }
     const size_t ns = std::max<size_t>(1, e->L.n_slots);
     FLBP_CUDA(cudaMemsetAsync(e->d_vf, 0, ns * e->tsize, e->stream));
     FLBP_CUDA(cudaMemsetAsync(e->d_fv, 0, e->n_ent * e->tsize, e->stream));
@@ -1187,7 +1244,7 @@ int flbp_init(flbp_engine *e) {
 
 int flbp_sweep(flbp_engine *e, int64_t n) {
     int rc = begin_call(e);
-    if (rc) return rc;
+    if (rc || (rc = refuse_sets(e, "flbp_sweep"))) return rc;
     if (n < 0) {
         set_error("negative sweep count");
         return FLBP_ERR_INVALID;
@@ -1201,7 +1258,7 @@ int flbp_sweep(flbp_engine *e, int64_t n) {
 
 int flbp_run_fixed(flbp_engine *e, int64_t sweeps, flbp_run_info *info) {
     int rc = begin_call(e);
-    if (rc) return rc;
+    if (rc || (rc = refuse_sets(e, "flbp_run_fixed"))) return rc;
     if (sweeps < 0) {
         set_error("negative sweep count");
         return FLBP_ERR_INVALID;
@@ -1223,7 +1280,7 @@ int flbp_run_fixed(flbp_engine *e, int64_t sweeps, flbp_run_info *info) {
 
 int flbp_run_tol(flbp_engine *e, double tol, int64_t maxiter, double maxtime, flbp_run_info *info) {
     int rc = begin_call(e);
-    if (rc) return rc;
+    if (rc || (rc = refuse_sets(e, "flbp_run_tol"))) return rc;
     const long long l0 = e->launches;
     reset_ctl_for_run(e, 1);
     Ctl &c = *e->h_ctl;
@@ -1248,7 +1305,7 @@ int flbp_run_tol(flbp_engine *e, double tol, int64_t maxiter, double maxtime, fl
 int flbp_run_lowpass(flbp_engine *e, double tol, int64_t min_iters, int64_t max_iters, int64_t hist_length,
                      double maxtime, flbp_run_info *info) {
     int rc = begin_call(e);
-    if (rc) return rc;
+    if (rc || (rc = refuse_sets(e, "flbp_run_lowpass"))) return rc;
     if (hist_length <= 0) {
         set_error("belief history length must be positive");
         return FLBP_ERR_INVALID;
@@ -1339,19 +1396,29 @@ static int fetch_internal(flbp_engine *e, const double *dsrc, double *out, int64
 int flbp_get_beliefs(flbp_engine *e, double *out, int64_t n) {
     int rc = begin_call(e);
     if (rc) return rc;
+    if (e->n_sets) {  // set k's beliefs at [k V, (k + 1) V)
+        const int64_t V = e->L.V;
+        if (n != V * (int64_t)e->n_sets) {
+            set_error("output length must equal the number of sets times the number of variables");
+            return FLBP_ERR_INVALID;
+        }
+        for (uint32_t k = 0; k < e->n_sets; k++)
+            if ((rc = fetch_internal(e, e->d_belief + (size_t)k * e->set_nv, out + (size_t)k * V, V))) return rc;
+        return FLBP_OK;
+    }
     return fetch_internal(e, e->d_belief, out, n);
 }
 
 int flbp_get_lowpass(flbp_engine *e, double *out, int64_t n) {
     int rc = begin_call(e);
-    if (rc) return rc;
+    if (rc || (rc = refuse_sets(e, "flbp_get_lowpass"))) return rc;
     if (!e->lowpass_valid) return fetch_internal(e, e->d_belief, out, n);
     return fetch_internal(e, e->d_lowpass, out, n);
 }
 
 int flbp_compute_beliefs(flbp_engine *e, double *out, int64_t n) {
     int rc = begin_call(e);
-    if (rc) return rc;
+    if (rc || (rc = refuse_sets(e, "flbp_compute_beliefs"))) return rc;
     reset_ctl_for_run(e, 0);
     if (!e->d_scratch && (rc = dalloc(e, &e->d_scratch, (size_t)e->L.V))) return rc;
     if ((rc = upload_ctl(e))) return rc;
@@ -1423,7 +1490,7 @@ static void pair_of(double lam, double &m0, double &m1) {
 
 int flbp_get_fv_messages(flbp_engine *e, double *m0, double *m1, int64_t n) {
     int rc = begin_call(e);
-    if (rc || (rc = ensure_host_layout(e))) return rc;
+    if (rc || (rc = refuse_sets(e, "message export")) || (rc = ensure_host_layout(e))) return rc;
     if (n != e->L.E) {
         set_error("output length must equal the number of edge slots");
         return FLBP_ERR_INVALID;
@@ -1440,7 +1507,7 @@ int flbp_get_fv_messages(flbp_engine *e, double *m0, double *m1, int64_t n) {
 
 int flbp_get_vf_messages(flbp_engine *e, double *m0, double *m1, int64_t n) {
     int rc = begin_call(e);
-    if (rc || (rc = ensure_host_layout(e))) return rc;
+    if (rc || (rc = refuse_sets(e, "message export")) || (rc = ensure_host_layout(e))) return rc;
     const HostLayout &L = e->L;
     if (n != L.E) {
         set_error("output length must equal the number of edge slots");
@@ -1513,7 +1580,7 @@ int flbp_kernel_times(flbp_engine *e, double *ms, int64_t *counts) {
 
 int flbp_set_tuning(flbp_engine *e, const flbp_tuning *t) {
     int rc = begin_call(e);
-    if (rc) return rc;
+    if (rc || (rc = refuse_sets(e, "flbp_set_tuning"))) return rc;
     if (!t || t->factor_form < 0 || t->factor_form > 2 || t->var_form < 0 || t->var_form > 2) {
         set_error("flbp_set_tuning: forms must be 0 (staged), 1 or 2 (direct)");
         return FLBP_ERR_INVALID;
@@ -1573,7 +1640,7 @@ TuneKey tune_key(const flbp_engine *e, int kind) {
 
 int flbp_autotune(flbp_engine *e, int32_t kind, int64_t sweeps, double tol, int32_t reps, flbp_tuning *chosen) {
     int rc = begin_call(e);
-    if (rc) return rc;
+    if (rc || (rc = refuse_sets(e, "flbp_autotune"))) return rc;
     if ((rc = refuse_seq(e, "flbp_autotune"))) return rc;
     if (kind < 0 || kind > 1 || sweeps < 1 || reps < 1) {
         set_error("flbp_autotune: kind must be 0 (fixed sweeps) or 1 (tolerance run), sweeps and reps positive");
@@ -1715,6 +1782,42 @@ int flbp_last_run_ms(flbp_engine *e, double *ms) {
 
 // ------------------------------------------------------------------ batched solves
 
+// Tolerance run of G independently stopping groups (graphs of a batched
+// engine, or evidence sets): group g stops after the first sweep in which
+// none of its beliefs moved by more than tol, or after maxiter sweeps.
+static int run_groups_tol(flbp_engine *e, uint32_t G, double tol, int64_t maxiter, double maxtime, int64_t *sweeps,
+                          int32_t *reasons, flbp_run_info *info) {
+    int rc;
+    const long long l0 = e->launches;
+    FLBP_CUDA(cudaMemsetAsync(e->d_gstate, 0, 4 * sizeof(int) * G, e->stream));
+    reset_ctl_for_run(e, 3);
+    Ctl &c = *e->h_ctl;
+    c.iters0 = 0;  // every group's sweep count starts at this call
+    c.tol = tol;
+    c.maxiter = maxiter;
+    c.maxtime_ns = maxtime * 1e9;
+    c.maxdiff = INFINITY;
+    if ((rc = record_start(e))) return rc;
+    long long done_sweeps = 0;
+    if (maxiter > 0 && maxtime > 0.0) {
+        if ((rc = upload_ctl(e)) || (rc = run_loop(e, 3, maxiter))) return rc;
+        if ((rc = download_ctl(e))) return rc;
+        done_sweeps = e->h_ctl->run_sweeps;
+    }
+    if ((rc = record_stop(e))) return rc;
+    std::vector<int> st(4 * (size_t)G);
+    FLBP_CUDA(cudaMemcpyAsync(st.data(), e->d_gstate, st.size() * sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+    FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    for (uint32_t g = 0; g < G; g++) {
+        if (sweeps) sweeps[g] = st[2 * (size_t)G + g];
+        if (reasons) reasons[g] = st[g] ? st[3 * (size_t)G + g] : FLBP_DIVERGED;
+    }
+    e->t += done_sweeps;
+    e->iters += done_sweeps;
+    fill_info(e, info, done_sweeps, l0);
+    return FLBP_OK;
+}
+
 int flbp_batch_create(const flbp_graph_desc *graphs, int64_t n_graphs, const flbp_engine_opts *opts,
                       flbp_engine **out) {
     if (!graphs || !out || n_graphs <= 0) {
@@ -1803,35 +1906,7 @@ int flbp_batch_run_tol(flbp_engine *e, double tol, int64_t maxiter, double maxti
         set_error("not a batched engine (create it with flbp_batch_create)");
         return FLBP_ERR_INVALID;
     }
-    const uint32_t G = e->n_graphs;
-    const long long l0 = e->launches;
-    FLBP_CUDA(cudaMemsetAsync(e->d_gstate, 0, 4 * sizeof(int) * G, e->stream));
-    reset_ctl_for_run(e, 3);
-    Ctl &c = *e->h_ctl;
-    c.iters0 = 0;  // every graph's sweep count starts at this call
-    c.tol = tol;
-    c.maxiter = maxiter;
-    c.maxtime_ns = maxtime * 1e9;
-    c.maxdiff = INFINITY;
-    if ((rc = record_start(e))) return rc;
-    long long done_sweeps = 0;
-    if (maxiter > 0 && maxtime > 0.0) {
-        if ((rc = upload_ctl(e)) || (rc = run_loop(e, 3, maxiter))) return rc;
-        if ((rc = download_ctl(e))) return rc;
-        done_sweeps = e->h_ctl->run_sweeps;
-    }
-    if ((rc = record_stop(e))) return rc;
-    std::vector<int> st(4 * (size_t)G);
-    FLBP_CUDA(cudaMemcpyAsync(st.data(), e->d_gstate, st.size() * sizeof(int), cudaMemcpyDeviceToHost, e->stream));
-    FLBP_CUDA(cudaStreamSynchronize(e->stream));
-    for (uint32_t g = 0; g < G; g++) {
-        if (sweeps) sweeps[g] = st[2 * (size_t)G + g];
-        if (reasons) reasons[g] = st[g] ? st[3 * (size_t)G + g] : FLBP_DIVERGED;
-    }
-    e->t += done_sweeps;
-    e->iters += done_sweeps;
-    fill_info(e, info, done_sweeps, l0);
-    return FLBP_OK;
+    return run_groups_tol(e, e->n_graphs, tol, maxiter, maxtime, sweeps, reasons, info);
 }
 
 }  // extern "C"
@@ -2092,7 +2167,7 @@ extern "C" {
 
 int flbp_adjoint_forward(flbp_engine *e, int64_t sweeps, int64_t every, double *beliefs, int64_t n) {
     int rc = begin_call(e);
-    if (rc || (rc = refuse_seq(e, "the adjoint")) || (rc = ensure_host_layout(e))) return rc;
+    if (rc || (rc = refuse_sets(e, "the adjoint")) || (rc = refuse_seq(e, "the adjoint")) || (rc = ensure_host_layout(e))) return rc;
     if (e->damping != 0.0) {
         set_error("the adjoint needs an engine without damping");
         return FLBP_ERR_INVALID;
@@ -2149,7 +2224,7 @@ int flbp_adjoint_forward(flbp_engine *e, int64_t sweeps, int64_t every, double *
 
 int flbp_adjoint_backward(flbp_engine *e, const double *grad_beliefs, double *grad_p, double *grad_q) {
     int rc = begin_call(e);
-    if (rc || (rc = refuse_seq(e, "the adjoint")) || (rc = ensure_host_layout(e))) return rc;
+    if (rc || (rc = refuse_sets(e, "the adjoint")) || (rc = refuse_seq(e, "the adjoint")) || (rc = ensure_host_layout(e))) return rc;
     const HostLayout &L = e->L;
     const size_t nv = std::max<int64_t>(1, L.V), nF = std::max<int64_t>(1, L.F);
     if (!e->d_adj_in && ((rc = dalloc(e, &e->d_adj_in, nv)) || (rc = dalloc(e, &e->d_adj_out, 2 * nF)))) return rc;
@@ -2175,7 +2250,7 @@ int flbp_adjoint_backward(flbp_engine *e, const double *grad_beliefs, double *gr
 
 int flbp_adjoint_backward_device(flbp_engine *e, const double *grad_beliefs, double *grad_p, double *grad_q) {
     int rc = begin_call(e);
-    if (rc || (rc = refuse_seq(e, "the adjoint")) || (rc = ensure_host_layout(e))) return rc;
+    if (rc || (rc = refuse_sets(e, "the adjoint")) || (rc = refuse_seq(e, "the adjoint")) || (rc = ensure_host_layout(e))) return rc;
     if (!grad_beliefs && e->L.V) {
         set_error("grad_beliefs is required");
         return FLBP_ERR_INVALID;
@@ -2185,7 +2260,7 @@ int flbp_adjoint_backward_device(flbp_engine *e, const double *grad_beliefs, dou
 
 int flbp_get_beliefs_device(flbp_engine *e, double *out, int64_t n) {
     int rc = begin_call(e);
-    if (rc) return rc;
+    if (rc || (rc = refuse_sets(e, "flbp_get_beliefs_device"))) return rc;
     if (n != e->L.V) {
         set_error("output length must equal the number of variables");
         return FLBP_ERR_INVALID;
@@ -2202,7 +2277,7 @@ int flbp_get_beliefs_device(flbp_engine *e, double *out, int64_t n) {
 
 int flbp_set_factor_probs(flbp_engine *e, const double *p, const double *q) {
     int rc = begin_call(e);
-    if (rc || (rc = refuse_seq(e, "flbp_set_factor_probs")) || (rc = ensure_host_layout(e))) return rc;
+    if (rc || (rc = refuse_sets(e, "flbp_set_factor_probs")) || (rc = refuse_seq(e, "flbp_set_factor_probs")) || (rc = ensure_host_layout(e))) return rc;
     HostLayout &L = e->L;
     for (int64_t I = 0; I < L.F; I++) {
         if (!(p[I] >= 0.0 && p[I] <= 1.0) || !(q[I] >= 0.0 && q[I] <= 1.0)) {
@@ -2271,54 +2346,48 @@ __global__ void clamp_apply_kernel(const uint32_t *__restrict__ ents, uint32_t n
     if (i < n_b) bt_prior_words[bw[2 * i]] = bw[2 * i + 1];
 }
 
-}  // namespace
-
-extern "C" {
-
-int flbp_clamp_vars(flbp_engine *e, int64_t n, const int64_t *vars, const int32_t *values) {
-    int rc = begin_call(e);
-    if (rc || (rc = refuse_seq(e, "flbp_clamp_vars")) || (rc = ensure_host_layout(e))) return rc;
-    HostLayout &L = e->L;
-    if (n < 0 || (n > 0 && (!vars || !values))) {
-        set_error("clamp list is malformed");
-        return FLBP_ERR_INVALID;
-    }
-    if (e->clamp_state.empty()) e->clamp_state.assign((size_t)L.V, -1);
-    for (int64_t k = 0; k < n; k++) {
-        if (vars[k] < 0 || vars[k] >= L.V) {
-            set_error("clamped variable out of range: " + std::to_string(vars[k]));
-            return FLBP_ERR_INVALID;
-        }
-        if (values[k] != 0 && values[k] != 1) {
-            set_error("clamp value must be 0 or 1 (variable " + std::to_string(vars[k]) + ")");
-            return FLBP_ERR_INVALID;
-        }
-        const int8_t st = e->clamp_state[vars[k]];
-        if (st >= 0 && st != values[k]) {
-            set_error("variable " + std::to_string(vars[k]) + " is already clamped to the other value");
-            return FLBP_ERR_INVALID;
-        }
-        for (int64_t j = 0; j < k; j++)
-            if (vars[j] == vars[k] && values[j] != values[k]) {
-                set_error("variable " + std::to_string(vars[k]) + " is clamped to both values");
-                return FLBP_ERR_INVALID;
-            }
-    }
-    std::vector<uint8_t> folded((size_t)L.V, 0);
-    for (uint32_t v : L.prior_var) folded[v] = 1;
-    const size_t pwords = e->prec == 64 ? 4 : 2, cword = e->prec == 64 ? 2 : 1;
-    // Every change is staged and the engine's host state is updated only once
-    // the device has taken them.
-    std::vector<uint32_t> ents, pw, bw;  // (entry, slot), (word, value), (word, value)
+// The changes a set of clamps makes to an engine (flbp_clamp_vars), from
+// the layout L as it is and the variables' current clamp states: the
+// entries no message reaches any more ((entry, slot) pairs), the new prior
+// count words ((word, value) pairs, engine priors and big-tile copies), the
+// (slot, value) pairs of the clamped variables' v->f messages (appended to
+// `slots`), and the host-side updates.
+struct ClampPlan {
+    std::vector<uint32_t> ents, pw, bw, cut_slots, slots;
     std::vector<std::pair<int64_t, int8_t>> new_state;
     std::vector<std::pair<uint32_t, uint32_t>> new_cnt;  // (internal variable, count word)
-    std::vector<uint32_t> cut_slots, slots = e->clamp_slots;
+};
+
+// Checks a clamp list against the current states; "" when valid.
+std::string check_clamps(const HostLayout &L, const std::vector<int8_t> &state, int64_t n, const int64_t *vars,
+                         const int32_t *values) {
+    if (n < 0 || (n > 0 && (!vars || !values))) return "clamp list is malformed";
+    for (int64_t k = 0; k < n; k++) {
+        if (vars[k] < 0 || vars[k] >= L.V) return "clamped variable out of range: " + std::to_string(vars[k]);
+        if (values[k] != 0 && values[k] != 1)
+            return "clamp value must be 0 or 1 (variable " + std::to_string(vars[k]) + ")";
+        const int8_t st = state[vars[k]];
+        if (st >= 0 && st != values[k])
+            return "variable " + std::to_string(vars[k]) + " is already clamped to the other value";
+        for (int64_t j = 0; j < k; j++)
+            if (vars[j] == vars[k] && values[j] != values[k])
+                return "variable " + std::to_string(vars[k]) + " is clamped to both values";
+    }
+    return "";
+}
+
+void clamp_plan(const HostLayout &L, int prec, const std::vector<int8_t> &state, int64_t n, const int64_t *vars,
+                const int32_t *values, ClampPlan &P) {
+    std::vector<uint8_t> folded((size_t)L.V, 0);
+    for (uint32_t v : L.prior_var) folded[v] = 1;
+    const size_t pwords = prec == 64 ? 4 : 2, cword = prec == 64 ? 2 : 1;
+    std::vector<uint32_t> &ents = P.ents, &pw = P.pw, &bw = P.bw, &cut_slots = P.cut_slots, &slots = P.slots;
     std::unordered_set<int64_t> in_call;
     std::unordered_set<uint32_t> cut_now;
     for (int64_t k = 0; k < n; k++) {
         // clamping again to the same value changes nothing
-        if (e->clamp_state[vars[k]] >= 0 || !in_call.insert(vars[k]).second) continue;
-        new_state.push_back({vars[k], (int8_t)values[k]});
+        if (state[vars[k]] >= 0 || !in_call.insert(vars[k]).second) continue;
+        P.new_state.push_back({vars[k], (int8_t)values[k]});
         const uint32_t iv = L.internal_of_var[vars[k]];
         // the clamp: one exact-zero count in the variable's prior
         uint32_t cnt = L.prior_cnt[iv];
@@ -2327,7 +2396,7 @@ int flbp_clamp_vars(flbp_engine *e, int64_t n, const int64_t *vars, const int32_
         } else if (((cnt >> 16) & 0x7fffu) != 0x7fffu) {
             cnt += 1u << 16;
         }
-        new_cnt.push_back({iv, cnt});
+        P.new_cnt.push_back({iv, cnt});
         const uint32_t word = cnt | (folded[iv] ? 0x80000000u : 0u);
         pw.push_back((uint32_t)(pwords * iv + cword));
         pw.push_back(word);
@@ -2388,6 +2457,36 @@ int flbp_clamp_vars(flbp_engine *e, int64_t n, const int64_t *vars, const int32_
             }
         }
     }
+}
+
+}  // namespace
+
+extern "C" {
+
+int flbp_clamp_vars(flbp_engine *e, int64_t n, const int64_t *vars, const int32_t *values) {
+    int rc = begin_call(e);
+    if (rc || (rc = refuse_seq(e, "flbp_clamp_vars")) || (rc = refuse_sets(e, "flbp_clamp_vars")) ||
+        (rc = ensure_host_layout(e)))
+        return rc;
+    HostLayout &L = e->L;
+    if (n < 0 || (n > 0 && (!vars || !values))) {
+        set_error("clamp list is malformed");
+        return FLBP_ERR_INVALID;
+    }
+    if (e->clamp_state.empty()) e->clamp_state.assign((size_t)L.V, -1);
+    const std::string bad = check_clamps(L, e->clamp_state, n, vars, values);
+    if (!bad.empty()) {
+        set_error(bad);
+        return FLBP_ERR_INVALID;
+    }
+    // Every change is staged and the engine's host state is updated only once
+    // the device has taken them.
+    ClampPlan P;
+    P.slots = e->clamp_slots;
+    clamp_plan(L, e->prec, e->clamp_state, n, vars, values, P);
+    std::vector<uint32_t> &ents = P.ents, &pw = P.pw, &bw = P.bw, &cut_slots = P.cut_slots, &slots = P.slots;
+    auto &new_state = P.new_state;
+    auto &new_cnt = P.new_cnt;
     const uint32_t n_e = (uint32_t)(ents.size() / 2), n_p = (uint32_t)(pw.size() / 2), n_b = (uint32_t)(bw.size() / 2);
     const uint32_t m = std::max(n_e, std::max(n_p, n_b));
     if (m == 0) return FLBP_OK;
@@ -2444,6 +2543,124 @@ int flbp_clamp_vars(flbp_engine *e, int64_t n, const int64_t *vars, const int32_
     return FLBP_OK;
 }
 
+int flbp_sets_create(const flbp_graph_desc *graph, int64_t n_sets, const int64_t *set_off, const int64_t *set_vars,
+                     const int32_t *set_vals, const flbp_engine_opts *opts, flbp_engine **out) {
+    if (!out) {
+        set_error("null argument");
+        return FLBP_ERR_INVALID;
+    }
+    *out = nullptr;
+    if (n_sets <= 0 || n_sets > 65535 || !set_off || set_off[0] != 0) {
+        set_error("evidence sets: between 1 and 65535 sets, offsets starting at 0");
+        return FLBP_ERR_INVALID;
+    }
+    for (int64_t k = 0; k < n_sets; k++)
+        if (set_off[k + 1] < set_off[k]) {
+            set_error("evidence set offsets must not decrease (set " + std::to_string(k) + ")");
+            return FLBP_ERR_INVALID;
+        }
+    if (set_off[n_sets] > 0 && (!set_vars || !set_vals)) {
+        set_error("evidence sets lack their clamp arrays");
+        return FLBP_ERR_INVALID;
+    }
+    flbp_engine *e = nullptr;
+    int rc = create_engine(graph, opts, &e, nullptr, true);
+    if (rc) return rc;
+    auto fail = [&](int code) {
+        std::string msg = g_last_error;
+        flbp_engine_destroy(e);
+        set_error(msg);
+        return code;
+    };
+    const HostLayout &L = e->L;
+    const uint32_t S = (uint32_t)n_sets;
+    const size_t nv_pad = std::max<size_t>({(size_t)1, (size_t)L.V, 32ull * L.n_vgroups()});
+    const size_t ns = std::max<size_t>(1, L.n_slots), ne = e->n_ent;
+    // every set's clamps: validity, then its cut entries, prior words and slots
+    std::vector<uint32_t> base_prior, bt_prior;
+    packed_priors(e, nv_pad, base_prior, bt_prior);
+    std::vector<uint32_t> prior(base_prior.size() * S);
+    std::vector<uint2> cut;
+    std::vector<uint4> slots;
+    const std::vector<int8_t> state((size_t)L.V, -1);
+    for (uint32_t k = 0; k < S; k++) {
+        const int64_t n = set_off[k + 1] - set_off[k];
+        const int64_t *vars = n ? set_vars + set_off[k] : nullptr;
+        const int32_t *vals = n ? set_vals + set_off[k] : nullptr;
+        const std::string bad = check_clamps(L, state, n, vars, vals);
+        if (!bad.empty()) {
+            set_error("evidence set " + std::to_string(k) + ": " + bad);
+            return fail(FLBP_ERR_INVALID);
+        }
+        ClampPlan P;
+        clamp_plan(L, e->prec, state, n, vars, vals, P);
+        uint32_t *pk = prior.data() + (size_t)k * base_prior.size();
+        std::copy(base_prior.begin(), base_prior.end(), pk);
+        for (size_t i = 0; i + 1 < P.pw.size(); i += 2) pk[P.pw[i]] = P.pw[i + 1];
+        for (size_t i = 0; i + 1 < P.ents.size(); i += 2) cut.push_back(make_uint2(k, P.ents[i]));
+        for (size_t i = 0; i + 1 < P.slots.size(); i += 2) slots.push_back(make_uint4(k, P.slots[i], P.slots[i + 1], 0));
+    }
+    if (cut.size() >= UINT32_MAX || slots.size() >= UINT32_MAX) {
+        set_error("evidence sets: too many clamped entries");
+        return fail(FLBP_ERR_LIMIT);
+    }
+    // S copies of the run state; the layout stays single
+    for (void **b : {(void **)&e->d_vf, (void **)&e->d_fv, (void **)&e->d_fvd, (void **)&e->d_belief,
+                     (void **)&e->d_prior, (void **)&e->d_gstate})
+        if (*b) {
+            cudaFree(*b);
+            *b = nullptr;
+        }
+    const bool damp = e->damping != 0.0;
+    if ((rc = dalloc(e, (char **)&e->d_vf, S * ns * e->tsize)) || (rc = dalloc(e, (char **)&e->d_fv, S * ne * e->tsize)) ||
+        (damp && (rc = dalloc(e, (char **)&e->d_fvd, S * ne * e->tsize))) ||
+        (rc = dalloc(e, &e->d_belief, S * nv_pad)) || (rc = dalloc(e, &e->d_gstate, 4 * (size_t)S)) ||
+        (rc = dalloc(e, (uint32_t **)&e->d_prior, prior.size())) || (rc = upload(e, (uint32_t *)e->d_prior, prior)) ||
+        (!cut.empty() && ((rc = dalloc(e, &e->d_set_cut, cut.size())) || (rc = upload(e, e->d_set_cut, cut)))) ||
+        (!slots.empty() && ((rc = dalloc(e, &e->d_set_slots, slots.size())) || (rc = upload(e, e->d_set_slots, slots)))))
+        return fail(rc);
+    FLBP_CUDA(cudaMemsetAsync(e->d_belief, 0, S * nv_pad * sizeof(double), e->stream));
+    FLBP_CUDA(cudaMemsetAsync(e->d_gstate, 0, 4 * sizeof(int) * S, e->stream));
+    FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    e->n_sets = S;
+    e->set_vs = ns;
+    e->set_es = ne;
+    e->set_nv = nv_pad;
+    e->n_set_cut = (uint32_t)cut.size();
+    e->n_set_slots = (uint32_t)slots.size();
+    // Grid width per set: one wave of the direct form's resident blocks over
+    // all sets, at least one block and at most one per 16 items of a set.
+    auto width = [&](bool var, uint64_t items, uint64_t huge) -> unsigned {
+        const int bps = e->prec == 64 ? direct_blocks_per_sm<double>(1, var, damp) : direct_blocks_per_sm<float>(1, var, damp);
+        const uint64_t wave = (uint64_t)e->sms * (uint64_t)std::max(bps, 1);
+        const uint64_t need = std::max<uint64_t>(1, std::max<uint64_t>((items + kConsumerWarps - 1) / kConsumerWarps, huge));
+        return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(need, wave / S));
+    };
+    e->set_fgx = width(false, (uint64_t)(L.nf_big - L.nf_huge) + L.n_fgroups(), L.nf_huge);
+    e->set_vgx = width(true, (uint64_t)(L.nv_big - L.nv_huge) + L.n_vgroups(), L.nv_huge);
+    *out = e;
+    return FLBP_OK;
+}
+
+int flbp_sets_run_tol(flbp_engine *e, double tol, int64_t maxiter, double maxtime, int64_t *sweeps, int32_t *reasons,
+                      flbp_run_info *info) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    if (!e->n_sets) {
+        set_error("not an engine of evidence sets (create it with flbp_sets_create)");
+        return FLBP_ERR_INVALID;
+    }
+    return run_groups_tol(e, e->n_sets, tol, maxiter, maxtime, sweeps, reasons, info);
+}
+
+int flbp_sets_info(flbp_engine *e, int64_t *n_sets, int64_t *n_vars) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    if (n_sets) *n_sets = e->n_sets;
+    if (n_vars) *n_vars = e->L.V;
+    return FLBP_OK;
+}
+
 }  // extern "C"
 
 // ------------------------------------------------------------------ sequential schedules
@@ -2489,7 +2706,7 @@ extern "C" {
 
 int flbp_set_update_seq(flbp_engine *e, const int64_t *seq, int64_t n) {
     int rc = begin_call(e);
-    if (rc || (rc = ensure_host_layout(e))) return rc;
+    if (rc || (rc = refuse_sets(e, "sequential schedules")) || (rc = ensure_host_layout(e))) return rc;
     if (e->n_graphs > 0) {
         set_error("sequential update schedules are not available on batched engines");
         return FLBP_ERR_STATE;

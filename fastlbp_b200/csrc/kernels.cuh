@@ -203,6 +203,10 @@ struct FactorArgs {
     const uint2 *trange;      // batched solves: per tile, the range of its items' graphs
     uint32_t n_graphs;        // batched solves: number of graphs
     uint32_t nf_sell, nf_big, nf_huge, n_fgroups, n_tiles, n_tile_blocks;
+    // Evidence sets on one graph (direct form, set = blockIdx.y): per-set
+    // message strides and stopped flags; null / 0 otherwise.
+    const int *set_done = nullptr;
+    uint64_t set_vf_stride = 0, set_fv_stride = 0;
 };
 
 struct VarArgs {
@@ -228,6 +232,10 @@ struct VarArgs {
     int *gstate;
     const uint2 *trange;      // per tile, the range of its items' graphs
     uint32_t n_graphs;
+    // Evidence sets on one graph (direct form, set = blockIdx.y): per-set
+    // strides of messages, priors (bytes) and beliefs; gstate / n_graphs
+    // then hold the sets' stop state.
+    uint64_t set_vf_stride = 0, set_fv_stride = 0, set_prior_stride = 0, set_belief_stride = 0;
 };
 
 // ------------------------------------------------------------ accumulators
@@ -1313,7 +1321,7 @@ __device__ __forceinline__ void var_close(const VarArgs &a, Ctl *ctl, double dma
         if (BMODE == 2) atomicAdd(&ctl->nonconv, c);
         __threadfence();
         const unsigned int prev = atomicAdd(&ctl->arrive, 1u);
-        s_last = (prev == gridDim.x - 1);
+        s_last = (prev == gridDim.x * gridDim.y - 1);
     }
     __syncthreads();
     if (s_last) {

@@ -341,6 +341,33 @@ int flbp_batch_info(flbp_engine *eng, int64_t *n_graphs, int64_t *var_off);
 int flbp_batch_run_tol(flbp_engine *eng, double tol, int64_t maxiter, double maxtime, int64_t *sweeps,
                        int32_t *reasons, flbp_run_info *info);
 
+/* ---- evidence sets on one graph (no counterpart in the reference: its
+ * alarm-ranking loop clamps, rebuilds the graph and builds a new CausalBP
+ * for every label set, examples/bingo_wrapper.cu:25-77, fl_wrapper.cu:29-45) ----
+ *
+ * One engine over n_sets evidence sets of one graph: the graph's layout is
+ * stored once, each set has its own messages, priors and beliefs. Set k
+ * clamps the variables set_vars[set_off[k] .. set_off[k+1]) (graph variable
+ * order) to set_vals[...] (0 or 1) with the effect of flbp_clamp_vars on an
+ * engine of its own (the clamp rewrite of csrc/ext/causal_factor.cpp:63-100
+ * followed by a rebuild). flbp_init resets every set (uniform messages,
+ * the clamped variables' v->f messages +-inf, beliefs 0 as in a new
+ * engine); flbp_sets_run_tol then runs the reference's tolerance rule with
+ * each set stopping by itself (sweeps[k], reasons[k] as in
+ * flbp_batch_run_tol; NULL allowed), so that set k has the beliefs and
+ * sweep count of its own engine solved alone.
+ * flbp_get_beliefs returns n_sets * n_vars values, set k at
+ * [k n_vars, (k+1) n_vars). Runs use the direct form of both passes with
+ * the sets as the second grid dimension; calls of a single graph's run
+ * state (flbp_run_*, flbp_sweep, gradients, clamps, export, schedules)
+ * return FLBP_ERR_STATE. At most 65535 sets. */
+int flbp_sets_create(const flbp_graph_desc *graph, int64_t n_sets, const int64_t *set_off, const int64_t *set_vars,
+                     const int32_t *set_vals, const flbp_engine_opts *opts, flbp_engine **out);
+int flbp_sets_run_tol(flbp_engine *eng, double tol, int64_t maxiter, double maxtime, int64_t *sweeps,
+                      int32_t *reasons, flbp_run_info *info);
+/* Number of sets (0 for other engines) and variables per set; either pointer may be NULL. */
+int flbp_sets_info(flbp_engine *eng, int64_t *n_sets, int64_t *n_vars);
+
 /* ---- gradients through unrolled sweeps (no counterpart in the reference) ----
  *
  * flbp_adjoint_forward: init() and `sweeps` synchronous sweeps (engines

@@ -65,8 +65,8 @@ def parse():
     ap.add_argument("--graphs", type=int, default=512, help="batch / adjoint workloads: number of graphs")
     ap.add_argument("--every", type=int, default=10, help="adjoint workload: checkpoint interval")
     ap.add_argument("--fd-params", type=int, default=1000, help="adjoint workload: parameters checked by differences")
-    ap.add_argument("--extras", default="batched,adjoint",
-                    help="sub-records of the default line: comma-separated subset of batched,adjoint, or none")
+    ap.add_argument("--extras", default="batched,adjoint,sets",
+                    help="sub-records of the default line: comma-separated subset of batched,adjoint,sets, or none")
     ap.add_argument("--plan-only", action="store_true",
                     help="start the ranks, deal the batched graphs to them and print the plan; no GPU work")
     return ap.parse_args()
@@ -895,7 +895,8 @@ def run_ours(args, rank, world, local):
     extras = [x for x in args.extras.split(",") if x and x != "none"]
     for name in extras:
         try:
-            line[name] = {"batched": batched_record, "adjoint": adjoint_record}[name](args, rank, world, local)
+            line[name] = {"batched": batched_record, "adjoint": adjoint_record,
+                          "sets": sets_record}[name](args, rank, world, local)
         except Exception as ex:  # a sub-record must not cost the main line
             line[name] = {"error": "%s: %s" % (type(ex).__name__, ex)}
     return line
@@ -983,6 +984,81 @@ def batched_record(args, rank, world, local):
            "scaling": "strong: the graphs are dealt to the ranks"}
     be.close()
     for e in plain:
+        e.close()
+    return rec
+
+
+def sets_record(args, rank, world, local):
+    """Sub-record of the default line: the alarm-ranking loop's re-solves as
+    evidence sets. One 50 k-tuple graph (config-0 laws) and its first 64
+    labelled alarms; set k clamps labels 0..k (the evidence after the k-th
+    label), FP32, init + tolerance run (tol 1e-6, maxiter 500) per set. One
+    SetsEngine over all sets against one engine per set (flbp_clamp_vars on
+    a new engine, solved in turn), both built before timing (construction
+    seconds reported apart); sets dealt to ranks. Median of 5 steps of
+    each, whole solves timed by the wall clock (results on the device),
+    max over ranks."""
+    import torch
+
+    from fastlbp_b200 import CausalFactorGraph, Engine, SetsEngine, workloads
+    from fastlbp_b200.shard import partition
+
+    tol, maxiter, steps, n_sets = 1e-6, 500, 5, 64
+    fl, alarms, y = workloads.config4_graph(0)
+    g = CausalFactorGraph.from_factors(fl)
+    arrays = g.graph_arrays()
+    idx = [g.findVar(int(a)) for a in alarms[:n_sets]]
+    vals = [int(v) for v in y[:n_sets]]
+    mine = partition(np.ones(n_sets), world)[rank]
+    sets = [{idx[j]: vals[j] for j in range(k + 1)} for k in mine]
+    t0 = time.perf_counter()
+    se = SetsEngine(arrays, sets, precision=32)
+    t_create_sets = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    sep = []
+    for cl in sets:
+        e = Engine(arrays, precision=32)
+        e.set_tuning(1, 1)  # the direct form of the sets engine
+        e.clamp(list(cl.keys()), list(cl.values()))
+        sep.append(e)
+    t_create_sep = time.perf_counter() - t0
+    se.init()
+    se.run_sets_tol(tol, maxiter)  # captures the sweep graphs
+    for e in sep:
+        e.init()
+        e.run_tol(tol, maxiter, 1e9)
+    torch.cuda.synchronize()
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    ts, tp = [], []
+    for _ in range(steps):
+        barrier(world)
+        t0 = time.perf_counter()
+        se.init()
+        sweeps, _ = se.run_sets_tol(tol, maxiter)
+        ts.append(time.perf_counter() - t0)
+        barrier(world)
+        t0 = time.perf_counter()
+        psweeps = []
+        for e in sep:
+            e.init()
+            psweeps.append(e.run_tol(tol, maxiter, 1e9)["sweeps"])
+        tp.append(time.perf_counter() - t0)
+    clk = clocks.stop()
+    got = se.beliefs()
+    diff = max(float(np.nanmax(np.abs(got[k] - e.beliefs()))) for k, e in enumerate(sep))
+    t_s = allreduce_max(statistics.median(ts), world)
+    t_p = allreduce_max(statistics.median(tp), world)
+    rec = {"metric": "evidence sets/s (tol 1e-6)", "value": n_sets / t_s, "unit": "sets/s",
+           "separate": n_sets / t_p, "sets_over_separate": t_p / t_s, "steps": steps, "statistic": "median",
+           "sets": n_sets, "sets_this_rank": len(mine), "edge_slots": int(arrays["factor_offsets"][-1]),
+           "sweeps": {"min": int(sweeps.min()), "median": float(np.median(sweeps)), "max": int(sweeps.max()),
+                      "same_as_separate": bool(sweeps.tolist() == psweeps)},
+           "max_belief_diff_sets_vs_separate": diff, "seconds": {"sets": t_s, "separate": t_p},
+           "construct_seconds": {"sets": t_create_sets, "separate": t_create_sep}, "clocks": clk,
+           "scaling": "strong: the sets are dealt to the ranks"}
+    se.close()
+    for e in sep:
         e.close()
     return rec
 

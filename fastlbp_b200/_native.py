@@ -128,6 +128,7 @@ def lib():
         "flbp_clamp_vars": [_vp, C.c_int64, _i64p, _i32p],
         "flbp_layout_digest": [P(GraphDesc), _vp, _vp, C.c_uint32, C.c_int32, P(C.c_uint64)],
         "flbp_set_factor_probs": [_vp, _f64p, _f64p],
+        "flbp_set_factor_probs_device": [_vp, _vp, _vp],
         "flbp_update_seq": [P(GraphDesc), C.c_int32, _vp, _i64p],
         "flbp_shuffled_factors": [C.c_int64, C.c_uint32, _i32p],
         "flbp_seq_batches": [P(GraphDesc), _i64p, C.c_int64, _vp, P(C.c_int64)],
@@ -167,7 +168,7 @@ EXPORTED = ["flbp_last_error", "flbp_version", "flbp_engine_create", "flbp_engin
             "flbp_fg_from_factors", "flbp_fg_destroy", "flbp_fg_clamp", "flbp_fg_rebuild", "flbp_fg_sizes",
             "flbp_fg_var_labels", "flbp_fg_factors", "flbp_fg_neighbors", "flbp_fg_construct",
             "flbp_engine_create_from_fg", "flbp_run_fixed_device_noalloc", "flbp_batch_create", "flbp_batch_info",
-            "flbp_batch_run_tol", "flbp_adjoint_forward", "flbp_adjoint_backward", "flbp_set_factor_probs",
+            "flbp_batch_run_tol", "flbp_adjoint_forward", "flbp_adjoint_backward", "flbp_set_factor_probs", "flbp_set_factor_probs_device",
             "flbp_adjoint_backward_device", "flbp_get_beliefs_device", "flbp_clamp_vars", "flbp_layout_digest",
             "flbp_update_seq", "flbp_shuffled_factors", "flbp_seq_batches", "flbp_set_update_seq", "flbp_update_info",
             "flbp_set_seq_kernel", "flbp_set_tuning", "flbp_get_tuning", "flbp_autotune", "flbp_set_layout_builder",

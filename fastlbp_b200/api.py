@@ -429,6 +429,16 @@ class Engine:
         check(lib().flbp_set_factor_probs(self._h, np.ascontiguousarray(p, np.float64),
                                           np.ascontiguousarray(q, np.float64)))
 
+    def set_factor_probs_device(self, p, q) -> None:
+        """p, q: float64 CUDA tensors (reference factor order) that stay on the
+        device (flbp_set_factor_probs_device); the caller's stream must have
+        finished writing them."""
+        for t in (p, q):
+            if not (t.is_cuda and t.dtype.is_floating_point and t.element_size() == 8 and t.is_contiguous()
+                    and t.numel() == self.n_factors):
+                raise ValueError("p and q must be contiguous float64 CUDA tensors of n_factors values")
+        check(lib().flbp_set_factor_probs_device(self._h, C.c_void_p(p.data_ptr()), C.c_void_p(q.data_ptr())))
+
     def set_kernel_timing(self, enable: bool) -> None:
         check(lib().flbp_set_kernel_timing(self._h, 1 if enable else 0))
 

@@ -10,8 +10,9 @@ segment from its checkpoint. The engine keeps the state of its last forward
 call, so each forward must be followed by its backward before the next
 forward on the same engine. With p on the engine's CUDA device, beliefs and
 gradients stay on the device (flbp_get_beliefs_device,
-flbp_adjoint_backward_device); p itself goes to the host for
-flbp_set_factor_probs.
+flbp_adjoint_backward_device), and so does p: flbp_set_factor_probs_device
+takes it from device memory (q too, when given as a CUDA tensor; a host q
+is copied to the device once per call).
 """
 
 from __future__ import annotations
@@ -24,15 +25,20 @@ from .api import Engine
 
 class UnrolledBeliefs(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, p: torch.Tensor, engine: Engine, q: np.ndarray, sweeps: int, every: int):
-        engine.set_factor_probs(p.detach().to("cpu", torch.float64).numpy(), q)
+    def forward(ctx, p: torch.Tensor, engine: Engine, q, sweeps: int, every: int):
         ctx.engine = engine
         ctx.on_device = p.is_cuda
         if p.is_cuda:
+            pd = p.detach().to(torch.float64).contiguous()
+            qd = torch.as_tensor(q, dtype=torch.float64, device=p.device).contiguous()
+            torch.cuda.current_stream(p.device).synchronize()  # the engine's stream does not wait for torch's
+            engine.set_factor_probs_device(pd, qd)
             engine.adjoint_forward(int(sweeps), int(every), fetch=False)
             b = torch.empty(engine.n_vars, dtype=torch.float64, device=p.device)
             engine.beliefs_device(b)
             return b
+        qh = q.detach().to("cpu", torch.float64).numpy() if isinstance(q, torch.Tensor) else q
+        engine.set_factor_probs(p.detach().to("cpu", torch.float64).numpy(), qh)
         return torch.from_numpy(engine.adjoint_forward(int(sweeps), int(every)))
 
     @staticmethod
@@ -47,4 +53,6 @@ class UnrolledBeliefs(torch.autograd.Function):
 
 
 def unrolled_beliefs(p: torch.Tensor, engine: Engine, q, sweeps: int, every: int) -> torch.Tensor:
-    return UnrolledBeliefs.apply(p, engine, np.ascontiguousarray(q, np.float64), sweeps, every)
+    if not isinstance(q, torch.Tensor):
+        q = np.ascontiguousarray(q, np.float64)
+    return UnrolledBeliefs.apply(p, engine, q, sweeps, every)

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <numeric>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -89,6 +90,15 @@ struct flbp_engine {
     uint32_t *d_pri_fac = nullptr, *d_pri_var = nullptr;      // folded constants: caller factor, internal variable
     double *d_pri_coef = nullptr;                             // their d(constant)/dp
     bool pri_coef_valid = false;
+    // flbp_set_factor_probs_device: the maps it uses (big-tile (p, q) and
+    // prior copies' sources, the prior entries grouped by variable), the
+    // last p and q it took, and whether the host copies lag behind them
+    uint32_t *d_fbt_src = nullptr, *d_vbt_src = nullptr, *d_pri_uvar = nullptr, *d_pri_uoff = nullptr,
+             *d_pri_ord = nullptr;
+    double *d_pri_sign = nullptr, *d_p_keep = nullptr, *d_q_keep = nullptr;
+    unsigned long long *d_bad = nullptr;
+    uint32_t n_pri_uvar = 0;
+    bool probs_maps = false, host_probs_stale = false;
     double *d_adj_in = nullptr, *d_adj_out = nullptr;         // staging of the host-buffer backward call
     uint32_t *d_adj_groups = nullptr;  // sliced-ELL group ids by width class (see adj_group_n)
     double *d_ref_out = nullptr;       // per-variable results in the caller's order (readback staging)
@@ -1200,6 +1210,10 @@ int flbp_engine_destroy(flbp_engine *e) {
     for (void *b : e->d_in)
         if (b) cudaFree(b);
     if (e->d_set_cut) cudaFree(e->d_set_cut);
+    for (void *b : {(void *)e->d_fbt_src, (void *)e->d_vbt_src, (void *)e->d_pri_uvar, (void *)e->d_pri_uoff,
+                    (void *)e->d_pri_ord, (void *)e->d_pri_sign, (void *)e->d_p_keep, (void *)e->d_q_keep,
+                    (void *)e->d_bad})
+        if (b) cudaFree(b);
     if (e->d_set_slots) cudaFree(e->d_set_slots);
     if (e->h_ctl) cudaFreeHost(e->h_ctl);
     if (e->ev0) cudaEventDestroy(e->ev0);
@@ -2163,6 +2177,163 @@ int adjoint_backward_dev(flbp_engine *e, const double *grad_b, double *gp_out, d
 
 }  // namespace
 
+namespace {
+
+// The host copies of new factor probabilities (reference factor order): the
+// factors' (p, q) in the internal order and in the big-tile copies, and the
+// finite prior constants of the folded singletons, summed in prior-entry
+// order.
+void apply_probs_host(flbp_engine *e, const double *p, const double *q) {
+    HostLayout &L = e->L;
+    e->factor_p_host.assign(p, p + L.F);
+    e->factor_q_host.assign(q, q + L.F);
+    const uint32_t nf = L.nf_sell + L.nf_big;
+    for (uint32_t f = 0; f < nf; f++) {
+        L.f_pq[2 * f] = p[L.factor_of_internal[f]];
+        L.f_pq[2 * f + 1] = q[L.factor_of_internal[f]];
+    }
+    for (uint32_t t = 0; t < L.n_fbtiles; t++) {
+        const uint32_t *h = &L.fhdr[(size_t)kHdrWordsHost * t];
+        for (uint32_t j = 0; j < (h[1] & ~kBigTileFlag); j++) {
+            const size_t k = (size_t)kTileGroupsHost * t + j, fi = (size_t)L.nf_sell + h[0] + j;
+            L.fbt_pq[2 * k] = L.f_pq[2 * fi];
+            L.fbt_pq[2 * k + 1] = L.f_pq[2 * fi + 1];
+        }
+    }
+    std::fill(L.prior_fin.begin(), L.prior_fin.end(), 0.0);
+    for (size_t k = 0; k < L.prior_factor.size(); k++) {
+        const double pk = p[L.prior_factor[k]];
+        L.prior_fin[L.prior_var[k]] += L.prior_sign[k] * (std::log(pk) - std::log1p(-pk));
+    }
+    e->host_probs_stale = false;
+}
+
+// Brings the host copies up to the probabilities last given on the device.
+int sync_host_probs(flbp_engine *e) {
+    if (!e->host_probs_stale) return FLBP_OK;
+    const size_t F = (size_t)e->L.F;
+    std::vector<double> p(F), q(F);
+    FLBP_CUDA(cudaMemcpyAsync(p.data(), e->d_p_keep, F * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    FLBP_CUDA(cudaMemcpyAsync(q.data(), e->d_q_keep, F * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    apply_probs_host(e, p.data(), q.data());
+    return FLBP_OK;
+}
+
+// The maps of flbp_set_factor_probs_device, built once per engine.
+int ensure_prob_maps(flbp_engine *e) {
+    if (e->probs_maps) return FLBP_OK;
+    int rc;
+    if ((rc = ensure_adjoint_maps(e))) return rc;  // internal factor -> caller factor, prior entries
+    const HostLayout &L = e->L;
+    std::vector<uint32_t> fbt_src(std::max<size_t>(1, L.fbt_pq.size() / 2), UINT32_MAX);
+    for (uint32_t t = 0; t < L.n_fbtiles; t++) {
+        const uint32_t *h = &L.fhdr[(size_t)kHdrWordsHost * t];
+        for (uint32_t j = 0; j < (h[1] & ~kBigTileFlag); j++) fbt_src[(size_t)kTileGroupsHost * t + j] = L.nf_sell + h[0] + j;
+    }
+    std::vector<uint32_t> vbt_src(std::max<size_t>(1, L.vbt_deg.size()), UINT32_MAX);
+    for (uint32_t t = 0; t < L.n_vbtiles; t++) {
+        const uint32_t *h = &L.vhdr[(size_t)kHdrWordsHost * t];
+        for (uint32_t j = 0; j < (h[1] & ~kBigTileFlag); j++) vbt_src[(size_t)kTileGroupsHost * t + j] = L.nv_sell + h[0] + j;
+    }
+    // prior entries grouped by variable, in entry order within a variable
+    const size_t np = L.prior_var.size();
+    std::vector<uint32_t> ord(std::max<size_t>(1, np), 0), uvar, uoff;
+    std::iota(ord.begin(), ord.begin() + np, 0u);
+    std::stable_sort(ord.begin(), ord.begin() + np, [&](uint32_t a, uint32_t b) { return L.prior_var[a] < L.prior_var[b]; });
+    for (size_t i = 0; i < np; i++)
+        if (i == 0 || L.prior_var[ord[i]] != L.prior_var[ord[i - 1]]) {
+            uvar.push_back(L.prior_var[ord[i]]);
+            uoff.push_back((uint32_t)i);
+        }
+    uoff.push_back((uint32_t)np);
+    if (uvar.empty()) uvar.push_back(0);
+    std::vector<double> sign(std::max<size_t>(1, np), 0.0);
+    for (size_t k = 0; k < np; k++) sign[k] = L.prior_sign[k];
+    if ((rc = dalloc(e, &e->d_fbt_src, fbt_src.size())) || (rc = upload(e, e->d_fbt_src, fbt_src)) ||
+        (rc = dalloc(e, &e->d_vbt_src, vbt_src.size())) || (rc = upload(e, e->d_vbt_src, vbt_src)) ||
+        (rc = dalloc(e, &e->d_pri_ord, ord.size())) || (rc = upload(e, e->d_pri_ord, ord)) ||
+        (rc = dalloc(e, &e->d_pri_uvar, uvar.size())) || (rc = upload(e, e->d_pri_uvar, uvar)) ||
+        (rc = dalloc(e, &e->d_pri_uoff, uoff.size())) || (rc = upload(e, e->d_pri_uoff, uoff)) ||
+        (rc = dalloc(e, &e->d_pri_sign, sign.size())) || (rc = upload(e, e->d_pri_sign, sign)) ||
+        (rc = dalloc(e, &e->d_p_keep, (size_t)L.F)) || (rc = dalloc(e, &e->d_q_keep, (size_t)L.F)) ||
+        (rc = dalloc(e, &e->d_bad, 1)))
+        return rc;
+    e->n_pri_uvar = np ? (uint32_t)(uoff.size() - 1) : 0u;
+    e->probs_maps = true;
+    return FLBP_OK;
+}
+
+// The first factor (reference order) whose p or q lies outside [0, 1] (NaN included).
+__global__ void probs_check_kernel(const double *__restrict__ p, const double *__restrict__ q, int64_t F,
+                                   unsigned long long *bad) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < F; i += (int64_t)gridDim.x * blockDim.x) {
+        const double a = p[i], b = q[i];
+        if (!(a >= 0.0 && a <= 1.0) || !(b >= 0.0 && b <= 1.0)) atomicMin(bad, (unsigned long long)i);
+    }
+}
+
+// (p, q) of every internal factor and of every big-tile copy, in the message type.
+template <typename T>
+__global__ void probs_pq_kernel(const double *__restrict__ p, const double *__restrict__ q,
+                                const uint32_t *__restrict__ f_of_int, uint32_t nf, T *f_pq,
+                                const uint32_t *__restrict__ fbt_src, uint32_t n_fbt, T *fbt_pq) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < max(nf, n_fbt); i += gridDim.x * blockDim.x) {
+        if (i < nf) {
+            const uint32_t I = f_of_int[i];
+            f_pq[2 * i] = (T)p[I];
+            f_pq[2 * i + 1] = (T)q[I];
+        }
+        if (i < n_fbt && fbt_src[i] != UINT32_MAX) {
+            const uint32_t I = f_of_int[fbt_src[i]];
+            fbt_pq[2 * i] = (T)p[I];
+            fbt_pq[2 * i + 1] = (T)q[I];
+        }
+    }
+}
+
+// Finite prior constants of the folded singletons (the sum over a variable's
+// prior entries of sign (log p - log1p(-p)), in entry order) into the
+// engine's prior words, and each entry's d(constant)/dp for the adjoint.
+template <typename T>
+__global__ void probs_prior_kernel(const double *__restrict__ p, const uint32_t *__restrict__ uvar,
+                                   const uint32_t *__restrict__ uoff, uint32_t n_uvar, const uint32_t *__restrict__ ord,
+                                   const uint32_t *__restrict__ pri_fac, const double *__restrict__ sign, uint32_t np,
+                                   double *coef, uint32_t *prior_words) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < max(n_uvar, np); i += gridDim.x * blockDim.x) {
+        if (i < n_uvar) {
+            double s = 0.0;
+            for (uint32_t j = uoff[i]; j < uoff[i + 1]; j++) {
+                const uint32_t k = ord[j];
+                const double pk = p[pri_fac[k]];
+                s += sign[k] * (log(pk) - log1p(-pk));
+            }
+            const uint32_t v = uvar[i];
+            if (sizeof(T) == 8) {
+                *reinterpret_cast<double *>(prior_words + 4 * (size_t)v) = s;
+            } else {
+                *reinterpret_cast<float *>(prior_words + 2 * (size_t)v) = (float)s;
+            }
+        }
+        if (i < np) {
+            const double pk = p[pri_fac[i]];
+            coef[i] = (pk > 0.0 && pk < 1.0) ? sign[i] / (pk * (1.0 - pk)) : 0.0;
+        }
+    }
+}
+
+// The big-tile copies of the priors (pw words each).
+__global__ void probs_bt_prior_kernel(const uint32_t *__restrict__ src, uint32_t n, uint32_t pw,
+                                      const uint32_t *__restrict__ prior_words, uint32_t *bt_prior_words) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t v = src[i];
+        if (v == UINT32_MAX) continue;
+        for (uint32_t w = 0; w < pw; w++) bt_prior_words[(size_t)pw * i + w] = prior_words[(size_t)pw * v + w];
+    }
+}
+
+}  // namespace
+
 extern "C" {
 
 int flbp_adjoint_forward(flbp_engine *e, int64_t sweeps, int64_t every, double *beliefs, int64_t n) {
@@ -2277,34 +2448,23 @@ int flbp_get_beliefs_device(flbp_engine *e, double *out, int64_t n) {
 
 int flbp_set_factor_probs(flbp_engine *e, const double *p, const double *q) {
     int rc = begin_call(e);
-    if (rc || (rc = refuse_sets(e, "flbp_set_factor_probs")) || (rc = refuse_seq(e, "flbp_set_factor_probs")) || (rc = ensure_host_layout(e))) return rc;
+    if (rc || (rc = refuse_sets(e, "flbp_set_factor_probs")) || (rc = refuse_seq(e, "flbp_set_factor_probs")) ||
+        (rc = ensure_host_layout(e)))
+        return rc;
     HostLayout &L = e->L;
+    if (L.F > 0 && (!p || !q)) {
+        set_error("null argument");
+        return FLBP_ERR_INVALID;
+    }
     for (int64_t I = 0; I < L.F; I++) {
         if (!(p[I] >= 0.0 && p[I] <= 1.0) || !(q[I] >= 0.0 && q[I] <= 1.0)) {
             set_error("factor probabilities must lie in [0,1] (factor " + std::to_string(I) + ")");
             return FLBP_ERR_INVALID;
         }
     }
-    e->factor_p_host.assign(p, p + L.F);
+    apply_probs_host(e, p, q);
     e->pri_coef_valid = false;
     const uint32_t nf = L.nf_sell + L.nf_big;
-    for (uint32_t f = 0; f < nf; f++) {
-        L.f_pq[2 * f] = p[L.factor_of_internal[f]];
-        L.f_pq[2 * f + 1] = q[L.factor_of_internal[f]];
-    }
-    for (uint32_t t = 0; t < L.n_fbtiles; t++) {
-        const uint32_t *h = &L.fhdr[(size_t)kHdrWordsHost * t];
-        for (uint32_t j = 0; j < (h[1] & ~kBigTileFlag); j++) {
-            const size_t k = (size_t)kTileGroupsHost * t + j, fi = (size_t)L.nf_sell + h[0] + j;
-            L.fbt_pq[2 * k] = L.f_pq[2 * fi];
-            L.fbt_pq[2 * k + 1] = L.f_pq[2 * fi + 1];
-        }
-    }
-    std::fill(L.prior_fin.begin(), L.prior_fin.end(), 0.0);
-    for (size_t k = 0; k < L.prior_factor.size(); k++) {
-        const double pk = p[L.prior_factor[k]];
-        L.prior_fin[L.prior_var[k]] += L.prior_sign[k] * (std::log(pk) - std::log1p(-pk));
-    }
     const size_t nf_pad = std::max<size_t>(nf, 32ull * L.n_fgroups());
     const size_t nv_pad = std::max<size_t>((size_t)L.V, 32ull * L.n_vgroups());
     std::vector<double> pq64(2 * nf_pad, 0.0);
@@ -2320,6 +2480,59 @@ int flbp_set_factor_probs(flbp_engine *e, const double *p, const double *q) {
     if ((rc = upload(e, (uint32_t *)e->d_prior, prior)) || (rc = upload(e, (uint32_t *)e->d_vbt_prior, bt_prior)))
         return rc;
     FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    return FLBP_OK;
+}
+
+int flbp_set_factor_probs_device(flbp_engine *e, const double *p, const double *q) {
+    int rc = begin_call(e);
+    if (rc || (rc = refuse_sets(e, "flbp_set_factor_probs_device")) ||
+        (rc = refuse_seq(e, "flbp_set_factor_probs_device")) || (rc = ensure_host_layout(e)))
+        return rc;
+    const HostLayout &L = e->L;
+    if (L.F == 0) return FLBP_OK;
+    if (!p || !q) {
+        set_error("null argument");
+        return FLBP_ERR_INVALID;
+    }
+    if ((rc = ensure_prob_maps(e))) return rc;
+    // the range check first: a bad value leaves the engine as it was
+    const unsigned gF = (unsigned)std::min<int64_t>((L.F + 255) / 256, 8192);
+    FLBP_CUDA(cudaMemsetAsync(e->d_bad, 0xff, sizeof(unsigned long long), e->stream));
+    probs_check_kernel<<<gF, 256, 0, e->stream>>>(p, q, L.F, e->d_bad);
+    FLBP_CUDA(cudaGetLastError());
+    unsigned long long bad = 0;
+    FLBP_CUDA(cudaMemcpyAsync(&bad, e->d_bad, sizeof bad, cudaMemcpyDeviceToHost, e->stream));
+    FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    if (bad != ~0ull) {
+        set_error("factor probabilities must lie in [0,1] (factor " + std::to_string(bad) + ")");
+        return FLBP_ERR_INVALID;
+    }
+    FLBP_CUDA(cudaMemcpyAsync(e->d_p_keep, p, (size_t)L.F * sizeof(double), cudaMemcpyDeviceToDevice, e->stream));
+    FLBP_CUDA(cudaMemcpyAsync(e->d_q_keep, q, (size_t)L.F * sizeof(double), cudaMemcpyDeviceToDevice, e->stream));
+    const uint32_t nf = L.nf_sell + L.nf_big, n_fbt = (uint32_t)(L.fbt_pq.size() / 2);
+    const uint32_t n_vbt = (uint32_t)L.vbt_deg.size();
+    auto blocks = [](uint64_t n) { return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 8192)); };
+    const uint32_t pw = e->prec == 64 ? 4 : 2;
+    if (e->prec == 64) {
+        probs_pq_kernel<double><<<blocks(std::max(nf, n_fbt)), 256, 0, e->stream>>>(
+            e->d_p_keep, e->d_q_keep, e->d_f_of_int, nf, (double *)e->d_f_pq, e->d_fbt_src, n_fbt, (double *)e->d_fbt_pq);
+        probs_prior_kernel<double><<<blocks(std::max<uint64_t>(e->n_pri_uvar, L.prior_var.size())), 256, 0, e->stream>>>(
+            e->d_p_keep, e->d_pri_uvar, e->d_pri_uoff, e->n_pri_uvar, e->d_pri_ord, e->d_pri_fac, e->d_pri_sign,
+            (uint32_t)L.prior_var.size(), e->d_pri_coef, (uint32_t *)e->d_prior);
+    } else {
+        probs_pq_kernel<float><<<blocks(std::max(nf, n_fbt)), 256, 0, e->stream>>>(
+            e->d_p_keep, e->d_q_keep, e->d_f_of_int, nf, (float *)e->d_f_pq, e->d_fbt_src, n_fbt, (float *)e->d_fbt_pq);
+        probs_prior_kernel<float><<<blocks(std::max<uint64_t>(e->n_pri_uvar, L.prior_var.size())), 256, 0, e->stream>>>(
+            e->d_p_keep, e->d_pri_uvar, e->d_pri_uoff, e->n_pri_uvar, e->d_pri_ord, e->d_pri_fac, e->d_pri_sign,
+            (uint32_t)L.prior_var.size(), e->d_pri_coef, (uint32_t *)e->d_prior);
+    }
+    if (n_vbt)
+        probs_bt_prior_kernel<<<blocks(n_vbt), 256, 0, e->stream>>>(e->d_vbt_src, n_vbt, pw, (const uint32_t *)e->d_prior,
+                                                                     (uint32_t *)e->d_vbt_prior);
+    e->launches += 3 + (n_vbt ? 1 : 0);
+    FLBP_CUDA(cudaGetLastError());
+    e->pri_coef_valid = true;
+    e->host_probs_stale = true;
     return FLBP_OK;
 }
 
@@ -2716,6 +2929,7 @@ int flbp_set_update_seq(flbp_engine *e, const int64_t *seq, int64_t n) {
             set_error("sequential update schedules are not available after flbp_clamp_vars");
             return FLBP_ERR_STATE;
         }
+    if ((rc = sync_host_probs(e))) return rc;
     const HostLayout &L = e->L;
     SeqLayout Q;
     if (seq) {  // build before touching the engine, so that a bad sequence leaves it as it was

@@ -440,6 +440,15 @@ int flbp_clamp_vars(flbp_engine *eng, int64_t n, const int64_t *vars, const int3
  * after a learning step: constants folded into priors follow. The graph's
  * structure (which factors are singletons, clamped or reduced) stays. */
 int flbp_set_factor_probs(flbp_engine *eng, const double *p, const double *q);
+/* The same with p and q in the engine's device memory (F doubles each,
+ * complete when the call is made: the engine's stream does not wait for
+ * another stream). The range check runs on the device (one 8-byte read
+ * back); the update itself stays on the device: (p, q) in the internal
+ * and big-tile orders, the folded singletons' prior constants (the sum of
+ * sign (log p - log1p(-p)) over each variable's prior entries) and their
+ * derivatives for the adjoint. The host copies are refreshed only when a
+ * later call needs them (a sequential schedule). */
+int flbp_set_factor_probs_device(flbp_engine *eng, const double *p, const double *q);
 
 /* ---- Sequential schedules (updates=SEQFIX / TOPO) ----------------------
  * An update sequence lists every edge once, as its factor-major slot

@@ -273,3 +273,53 @@ def test_shared_rule_gradient_matches_central_differences():
         pm[r] -= eps
         fd = (loss_and_grad(pp)[0] - loss_and_grad(pm)[0]) / (2 * eps)
         assert abs(fd - shared[r]) <= 1e-4 * max(abs(shared[r]), 1e-3 * scale), (r, fd, shared[r])
+
+
+@pytest.mark.parametrize("prec", [32, 64])
+def test_device_factor_probs_match_host(prec):
+    """flbp_set_factor_probs_device against flbp_set_factor_probs with the
+    same new p and q: beliefs after a fixed run (FP64 1e-12; FP32 1e-6, the
+    folded priors' logarithms being the device's), gradients (1e-9
+    relative), an out-of-range value rejected with the engine unchanged,
+    and a sequential schedule set afterwards built on the new values."""
+    from fastlbp_b200 import FlbpError
+
+    a = _graph("large")
+    rng = np.random.default_rng(17)
+    p = np.clip(np.asarray(a["factor_p"], np.float64) * rng.uniform(0.9, 1.0, len(a["factor_p"])), 0.0, 1.0)
+    q = np.asarray(a["factor_q"], np.float64)
+    host, dev = Engine(a, precision=prec), Engine(a, precision=prec)
+    host.set_factor_probs(p, q)
+    pd, qd = torch.as_tensor(p, device="cuda"), torch.as_tensor(q, device="cuda")
+    torch.cuda.synchronize()
+    dev.set_factor_probs_device(pd, qd)
+    tol = 1e-12 if prec == 64 else 1e-6
+    T, K = 12, 4
+    bh, bd = host.adjoint_forward(T, K), dev.adjoint_forward(T, K)
+    assert np.max(np.abs(bh - bd)) <= tol
+    idx, _ = _labels(a, seed=8)
+    g = np.zeros(host.n_vars)
+    g[idx] = rng.standard_normal(idx.size)
+    gh, gd = host.adjoint_backward(g)[0], dev.adjoint_backward(g)[0]
+    if prec == 64:
+        assert np.max(np.abs(gh - gd)) <= 1e-9 * np.max(np.abs(gh))
+    else:
+        assert np.linalg.norm(gh - gd) <= 1e-4 * np.linalg.norm(gh)
+    bad = pd.clone()
+    bad[5] = 1.5
+    torch.cuda.synchronize()
+    with pytest.raises(FlbpError):
+        dev.set_factor_probs_device(bad, qd)
+    assert np.array_equal(dev.adjoint_forward(T, K), bd)
+    # a sequential schedule set afterwards reads the new values on the host
+    from fastlbp_b200 import update_seq
+
+    seq = update_seq(a, "SEQFIX", 42)
+    host.set_update_seq(seq)
+    dev.set_update_seq(seq)
+    for e in (host, dev):
+        e.init()
+        e.run_fixed(5)
+    assert np.max(np.abs(host.beliefs() - dev.beliefs())) <= tol
+    host.close()
+    dev.close()

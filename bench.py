@@ -621,6 +621,19 @@ def run_fl(args, rank, world, local):
     bp.run(1e-6, 500, 1e9)
     t_cpu = time.perf_counter() - t0
     bo = bp.beliefs()
+    # The same recurrence in FP64 log-odds (no underflow), and the reference
+    # arithmetic once more with every belief marked that depends on a
+    # probability product that underflowed to an exact zero.
+    bl = O.OracleBP(og, threads=os.cpu_count() or 1, arith="lodds")
+    bl.init()
+    bl.run(1e-6, 500, 1e9)
+    b_lo = bl.beliefs()
+    bt = O.OracleBP(og, threads=os.cpu_count() or 1, arith="track")
+    bt.init()
+    bt.run(1e-6, 500, 1e9)
+    tainted, n_uf = bt.underflow()
+    off_ref = np.abs(b - bo) > 1e-5
+    off_ref_nan = np.isnan(b) != np.isnan(bo)
     # the same comparison after a few sweeps, before any chaotic growth of rounding differences
     e10 = Engine(arr, precision=args.precision)
     e10.init()
@@ -636,6 +649,7 @@ def run_fl(args, rank, world, local):
     stm = stm[(stm < labels.size)]
     stm = stm[labels[stm] < fl.info["n_inputs"]]
     rho = float(spearmanr(b[stm], bo[stm]).statistic)
+    rho_lo = float(spearmanr(b[stm], b_lo[stm]).statistic)
     top = {}
     for k in (10, 100):
         a_ = set(stm[np.argsort(-b[stm], kind="stable")[:k]].tolist())
@@ -657,7 +671,22 @@ def run_fl(args, rank, world, local):
             "oracle_final_residual_converged": bool(bp.iters < 500),
             "nan_beliefs": {"engine": int(np.isnan(b).sum()), "oracle": int(np.isnan(bo).sum()),
                             "same_positions": bool(np.array_equal(np.isnan(b), np.isnan(bo)))},
-            "ranking": dict(statements=int(stm.size), spearman=rho, **top),
+            "ranking": dict(statements=int(stm.size), spearman=rho, spearman_vs_logodds_oracle=rho_lo, **top),
+            "vs_logodds_oracle": {
+                "max_belief_error": float(np.nanmax(np.abs(b - b_lo))),
+                "vars_off_by_more_than_1e-5": int(np.sum(np.abs(b - b_lo) > 1e-5)),
+                "nan_same_positions": bool(np.array_equal(np.isnan(b), np.isnan(b_lo))),
+                "oracle_sweeps": bl.iters,
+                "oracle": "the PARALL recurrence in FP64 log-odds (no probability products, no underflow)"},
+            "underflow": {
+                "events": n_uf, "tainted_vars": int(tainted.sum()),
+                "off_by_more_than_1e-5_vs_reference_arith": int(off_ref.sum()),
+                "of_those_tainted": int((off_ref & tainted).sum()),
+                "of_those_untainted": int((off_ref & ~tainted).sum()),
+                "nan_mismatch_untainted": int((off_ref_nan & ~tainted).sum()),
+                "tracked_run_sweeps": bt.iters,
+                "meaning": "tainted: the reference-arithmetic belief depends on a probability product that "
+                           "underflowed to an exact zero"},
             "cpu_oracle_seconds": t_cpu, "cpu_cores": os.cpu_count()}
 
 

@@ -160,16 +160,17 @@ __global__ void __launch_bounds__(kDirectThreads, MINB) factor_direct_kernel(Fac
 }
 
 // One sliced-ELL variable group of width W, direct: lane = variable, entries
-// at base + 32 k + lane (padding entries hold 0 and kSentinel).
+// at base + 32 k + lane (padding entries hold 0 and kSentinel). W = 0: a
+// group of variables without entries (their beliefs come from the priors).
 template <typename T, int W, int BMODE, bool WRITE_VF, bool DAMP>
 __device__ __forceinline__ double var_group_direct(const VarArgs &a, const T *__restrict__ fv, T *__restrict__ vf,
                                                    T *__restrict__ fvd, T d, uint32_t base, uint32_t v, bool live,
                                                    double pscale, double tol, int lane, unsigned long long &cnt) {
     constexpr bool RESID = (BMODE == 1 || BMODE == 2 || BMODE == 4);
     const T inf = Num<T>::inf();
-    T x[W];
-    T xo[DAMP ? W : 1];
-    uint32_t en[W];
+    T x[W > 0 ? W : 1];
+    T xo[DAMP && W > 0 ? W : 1];
+    uint32_t en[W > 0 ? W : 1];
 #pragma unroll
     for (int k = 0; k < W; k++) x[k] = fv[base + 32u * k + lane];
     if (DAMP) {
@@ -217,13 +218,13 @@ __device__ __forceinline__ double var_group_direct_w(int w, const VarArgs &a, co
     switch (w) {
 #define FLBP_W(N) \
     case N: return var_group_direct<T, N, BMODE, WRITE_VF, DAMP>(a, fv, vf, fvd, d, base, v, live, pscale, tol, lane, cnt);
-        FLBP_W(1) FLBP_W(2) FLBP_W(3) FLBP_W(4) FLBP_W(5) FLBP_W(6) FLBP_W(7) FLBP_W(8) FLBP_W(9) FLBP_W(10)
-        FLBP_W(11) FLBP_W(12) FLBP_W(13) FLBP_W(14) FLBP_W(15) FLBP_W(16)
+        FLBP_W(0) FLBP_W(1) FLBP_W(2) FLBP_W(3) FLBP_W(4) FLBP_W(5) FLBP_W(6) FLBP_W(7) FLBP_W(8) FLBP_W(9)
+        FLBP_W(10) FLBP_W(11) FLBP_W(12) FLBP_W(13) FLBP_W(14) FLBP_W(15) FLBP_W(16)
 #undef FLBP_W
         default: return 0.0;
     }
 }
-static_assert(kSellVarDegree == 16, "var_group_direct_w instantiates widths 1..16");
+static_assert(kSellVarDegree == 16, "var_group_direct_w instantiates widths 0..16");
 
 // One large variable that fits a warp (big variable b, internal index
 // nv_sell + b), direct: the warp's lanes stride over its entries. Returns the

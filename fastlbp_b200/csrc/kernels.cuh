@@ -769,13 +769,21 @@ __device__ __forceinline__ void factor_tile_big(const T *vb, const uint32_t *ps,
     if (lane == 0) eP = T(1), eR = T(0);
     if (lane == 31) xP = T(1), xR = T(0);
     if ((kind & HEAD_MASK) == HEAD_FREE) {
-        auto logP = [&]() {  // rare: whole-body log-sigmoid sum, by the whole warp
+        auto logP = [&]() {  // rare: whole-body log-sigmoid sum, by the whole warp, -inf terms counted apart
             typedef AccOps<typename WideAcc<T>::type> O;
             typename WideAcc<T>::type l = O::zero();
-            for (uint32_t k = lane; k < nbody; k += 32) O::add(l, log_sigmoid<T>(sgn * vb[1 + k]));
+            int nz = 0;
+            for (uint32_t k = lane; k < nbody; k += 32) {
+                const T ls = log_sigmoid<T>(sgn * vb[1 + k]);
+                if (ls == -Num<T>::inf()) nz++;
+                else O::add(l, ls);
+            }
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) O::combine(l, O::shfl_xor(l, o));
-            return (T)O::value(l);
+            for (int o = 16; o > 0; o >>= 1) {
+                O::combine(l, O::shfl_xor(l, o));
+                nz += __shfl_xor_sync(0xffffffffu, nz, o);
+            }
+            return nz ? -Num<T>::inf() : (T)O::value(l);
         };
         const T o = sgn * head_from_pair<T>(P, R, p, q, logP);
         if (lane == 0) put_fv<T>(fv, ps[0], o);

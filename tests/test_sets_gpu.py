@@ -124,6 +124,7 @@ def test_sets_match_oracle(prec, tol):
         assert np.array_equal(np.isnan(want), np.isnan(fixed[k])), k
         ok = ~np.isnan(want)
         assert np.max(np.abs(fixed[k][ok] - want[ok])) <= tol, k
+        ref = O.OracleBP(og)  # a new one: the reference's sweep count runs on across run calls
         ref.init()
         ref.run(1e-6, 400, 1e9)
         assert abs(int(sweeps[k]) - ref.iters) <= (0 if prec == 64 else 1), k

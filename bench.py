@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--fd-params", type=int, default=1000, help="adjoint workload: parameters checked by differences")
     ap.add_argument("--extras", default="batched,adjoint,sets",
                     help="sub-records of the default line: comma-separated subset of batched,adjoint,sets, or none")
+    ap.add_argument("--forms", default="auto",
+                    help="pass forms of the single-graph workload: auto (the autotuner) or F,V (0 staged, 1-2 direct)")
     ap.add_argument("--plan-only", action="store_true",
                     help="start the ranks, deal the batched graphs to them and print the plan; no GPU work")
     return ap.parse_args()
@@ -203,6 +205,7 @@ def run_batch(args, rank, world, local):
         be.init()
         be.run_batch_tol(tol, maxiter)
         for e in plain:
+            e.reset_counts()  # a plain solve is a new engine's (maxiter counts from 0)
             e.init()
             e.run_tol(tol, maxiter, 1e9)
     torch.cuda.synchronize()
@@ -217,6 +220,7 @@ def run_batch(args, rank, world, local):
         t0 = time.perf_counter()
         psweeps = []
         for e in plain:
+            e.reset_counts()
             e.init()
             psweeps.append(e.run_tol(tol, maxiter, 1e9)["sweeps"])
         tp.append(time.perf_counter() - t0)
@@ -834,7 +838,13 @@ def run_ours(args, rank, world, local):
     V = int(arr["n_vars"])
     stream = torch.cuda.current_stream()
     eng = Engine(arr, precision=args.precision, damping=args.damping, stream=stream.cuda_stream)
-    tuned = eng.autotune(args.sweeps)
+    if args.forms == "auto":
+        tuned = eng.autotune(args.sweeps)
+    else:
+        ff, vf = (int(x) for x in args.forms.split(","))
+        eng.set_tuning(ff, vf)
+        tuned = None
+    forms = eng.tuning()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     total_ms, launches, clk = sweep_timing(eng, args, stream, flush, world)
@@ -868,8 +878,7 @@ def run_ours(args, rank, world, local):
         s.record(stream)
         t0 = time.perf_counter()
         eng2 = Engine(arr, precision=args.precision, damping=args.damping, stream=stream.cuda_stream)
-        if tuned:
-            eng2.set_tuning(tuned["factor_form"], tuned["var_form"])
+        eng2.set_tuning(forms["factor_form"], forms["var_form"])
         eng2.init()
         eng2.run_fixed(args.sweeps)
         out = eng2.beliefs()
@@ -890,8 +899,8 @@ def run_ours(args, rank, world, local):
     if args.damping != 0.0:
         for prec in (32, 64):
             e0 = Engine(arr, precision=prec, damping=0.0, stream=stream.cuda_stream)
-            if tuned and prec == args.precision:
-                e0.set_tuning(tuned["factor_form"], tuned["var_form"])
+            if prec == args.precision:
+                e0.set_tuning(forms["factor_form"], forms["var_form"])
             a0 = argparse.Namespace(**vars(args))
             a0.steps = max(3, min(args.steps, 5))
             ms0, _, _ = sweep_timing(e0, a0, stream, flush, world)
@@ -976,7 +985,11 @@ def batched_record(args, rank, world, local):
     plain_forms = sorted({(e.tuning()["factor_form"], e.tuning()["var_form"]) for e in plain})
     be.init()
     be.run_batch_tol(tol, maxiter)  # captures the sweep graphs
+    # A plain solve is a new engine's: the sweep count that maxiter limits
+    # and the tolerance rule's previous beliefs start afresh each time
+    # (as the batched engine's per-graph state does).
     for e in plain:
+        e.reset_counts()
         e.init()
         e.run_tol(tol, maxiter, 1e9)
     torch.cuda.synchronize()
@@ -993,6 +1006,7 @@ def batched_record(args, rank, world, local):
         t0 = time.perf_counter()
         psweeps = []
         for e in plain:
+            e.reset_counts()
             e.init()
             psweeps.append(e.run_tol(tol, maxiter, 1e9)["sweeps"])
         tp.append(time.perf_counter() - t0)
@@ -1054,6 +1068,7 @@ def sets_record(args, rank, world, local):
     se.init()
     se.run_sets_tol(tol, maxiter)  # captures the sweep graphs
     for e in sep:
+        e.reset_counts()
         e.init()
         e.run_tol(tol, maxiter, 1e9)
     torch.cuda.synchronize()
@@ -1070,6 +1085,7 @@ def sets_record(args, rank, world, local):
         t0 = time.perf_counter()
         psweeps = []
         for e in sep:
+            e.reset_counts()
             e.init()
             psweeps.append(e.run_tol(tol, maxiter, 1e9)["sweeps"])
         tp.append(time.perf_counter() - t0)

@@ -143,6 +143,7 @@ def lib():
         "flbp_sets_create": [P(GraphDesc), C.c_int64, _i64p, _vp, _vp, P(EngineOpts), P(_vp)],
         "flbp_sets_run_tol": [_vp, C.c_double, C.c_int64, C.c_double, _i64p, _i32p, P(RunInfo)],
         "flbp_sets_info": [_vp, P(C.c_int64), P(C.c_int64)],
+        "flbp_reset_counts": [_vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -172,4 +173,4 @@ EXPORTED = ["flbp_last_error", "flbp_version", "flbp_engine_create", "flbp_engin
             "flbp_adjoint_backward_device", "flbp_get_beliefs_device", "flbp_clamp_vars", "flbp_layout_digest",
             "flbp_update_seq", "flbp_shuffled_factors", "flbp_seq_batches", "flbp_set_update_seq", "flbp_update_info",
             "flbp_set_seq_kernel", "flbp_set_tuning", "flbp_get_tuning", "flbp_autotune", "flbp_set_layout_builder",
-            "flbp_engine_layout_digest", "flbp_sets_create", "flbp_sets_run_tol", "flbp_sets_info"]
+            "flbp_engine_layout_digest", "flbp_sets_create", "flbp_sets_run_tol", "flbp_sets_info", "flbp_reset_counts"]

@@ -324,6 +324,11 @@ class Engine:
     def init(self):
         check(lib().flbp_init(self._h))
 
+    def reset_counts(self):
+        """Sweep count and beliefs back to a new engine's (flbp_reset_counts):
+        init() + run_tol then gives what a newly built engine gives."""
+        check(lib().flbp_reset_counts(self._h))
+
     def sweep(self, n: int = 1):
         check(lib().flbp_sweep(self._h, int(n)))
 

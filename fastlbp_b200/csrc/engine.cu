@@ -1292,6 +1292,18 @@ int flbp_run_fixed(flbp_engine *e, int64_t sweeps, flbp_run_info *info) {
     return FLBP_OK;
 }
 
+int flbp_reset_counts(flbp_engine *e) {
+    int rc = begin_call(e);
+    if (rc) return rc;
+    const size_t nv = e->n_sets ? e->n_sets * e->set_nv
+                                : std::max<size_t>({(size_t)1, (size_t)e->L.V, 32ull * e->L.n_vgroups()});
+    FLBP_CUDA(cudaMemsetAsync(e->d_belief, 0, nv * sizeof(double), e->stream));
+    FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    e->iters = 0;
+    e->lowpass_valid = false;
+    return FLBP_OK;
+}
+
 int flbp_run_tol(flbp_engine *e, double tol, int64_t maxiter, double maxtime, flbp_run_info *info) {
     int rc = begin_call(e);
     if (rc || (rc = refuse_sets(e, "flbp_run_tol"))) return rc;

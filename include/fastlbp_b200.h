@@ -105,8 +105,17 @@ int flbp_init(flbp_engine *eng);
 
 /* Tolerance-driven loop: sweep while sweeps < maxiter, max |belief change| >
  * tol and elapsed < maxtime seconds. Replaces CausalBP::run()
- * (csrc/ext/causal_bp.cu:858-910). */
+ * (csrc/ext/causal_bp.cu:858-910). As the reference's _iters, `sweeps`
+ * counts every sweep since the engine was constructed (init() does not
+ * reset it), and the first sweep's belief change is taken against the
+ * beliefs the engine holds (0 in a new engine). */
 int flbp_run_tol(flbp_engine *eng, double tol, int64_t maxiter, double maxtime, flbp_run_info *info);
+
+/* The run state a new engine starts with: sweep count 0 and beliefs 0, so
+ * that init() + flbp_run_tol gives what a newly constructed engine gives
+ * (the reference resets both only on construction,
+ * csrc/ext/causal_bp.cu:371). Messages are left to init(). */
+int flbp_reset_counts(flbp_engine *eng);
 
 /* Exactly `sweeps` sweeps, then one belief evaluation; low-pass beliefs equal
  * the beliefs and the returned fraction is 1. Replaces

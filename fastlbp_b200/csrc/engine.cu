@@ -2003,6 +2003,9 @@ void launch_adjoint_step(flbp_engine *e, const void *vf, const void *fv, const v
 // segment writes each sweep's states straight into the segment buffers).
 template <typename T>
 void launch_factor_pass_on(flbp_engine *e, const void *vf, void *fv) {
+    // the staged form's tile counter: the variable pass resets it, and none
+    // need have run since the last factor pass
+    cudaMemsetAsync(reinterpret_cast<char *>(e->d_ctl) + offsetof(Ctl, fnext), 0, sizeof(unsigned int), e->stream);
     const FactorArgs fa = factor_args<T>(e);
     launch_factor<T>(e, fa, vf, fv);
     e->launches += 1;

@@ -451,16 +451,18 @@ __device__ __forceinline__ bool graph_done(const uint32_t *s_done, const int *gd
     return g < 32u * kDoneWords ? ((s_done[g >> 5] >> (g & 31)) & 1u) != 0 : gdone[g] != 0;
 }
 
-// Producer warp of a pass. A single graph's pass walks the block's tiles
-// blockIdx.x + i gridDim.x in order (neighbouring blocks work on neighbouring
-// tiles at any moment, which keeps the scattered stores of a pass close
-// together). A batched solve instead takes chunks of kChunkTiles consecutive
-// tiles from the pass's counter, so that blocks whose tiles belong to stopped
-// graphs take more, and leaves out tiles whose graphs have all stopped. One
-// stage per remaining tile is filled with fill(stage, header in shared
-// memory, full barrier); a stage whose header word 1 is kEndTile closes the
-// stream. All lanes call it; lane 0 issues the copies. After a timeout it
-// records FLBP_ERR_TIMEOUT, lets its own copies land and returns false.
+// Producer warp of a pass. Blocks take tiles from the pass's counter (zero
+// when the pass starts: each pass resets the other's), claiming the next
+// while the current one is staged: a single graph's pass one tile per
+// claim, so that blocks that drew cheaper tiles take more and all SMs finish
+// together (claims run in tile order, so neighbouring blocks work on
+// neighbouring tiles at any moment, which keeps the scattered stores of a
+// pass close together); a batched solve chunks of kChunkTiles consecutive
+// tiles, leaving out tiles whose graphs have all stopped. One stage per
+// remaining tile is filled with fill(stage, header in shared memory, full
+// barrier); a stage whose header word 1 is kEndTile closes the stream. All
+// lanes call it; lane 0 issues the copies. After a timeout it records
+// FLBP_ERR_TIMEOUT, lets its own copies land and returns false.
 constexpr uint32_t kChunkTiles = 4;
 
 template <int STAGES, typename Fill>
@@ -469,25 +471,23 @@ __device__ bool produce_tiles(const uint4 *thdr, const uint2 *trange, const uint
                               uint64_t *full, uint64_t *empty, int lane, Ctl *ctl, Fill fill) {
     uint32_t issued = 0;
     bool ok = true;
-    const bool dynamic = trange != nullptr;
+    const bool batched = trange != nullptr;
     // round r covers tiles tile_at(r, 0..width-1)
-    const uint32_t width = dynamic ? kChunkTiles : 32u;
-    const uint32_t nb = gridDim.x;
-    uint32_t round = dynamic ? __shfl_sync(0xffffffffu, lane == 0 ? atomicAdd(counter, 1u) : 0u, 0) : 0u;
+    const uint32_t width = batched ? kChunkTiles : 1u;
+    uint32_t round = __shfl_sync(0xffffffffu, lane == 0 ? atomicAdd(counter, 1u) : 0u, 0);
     auto tile_at = [&](uint32_t r, uint32_t k) -> uint32_t {  // n_tiles when out of range
-        const uint64_t t = dynamic ? (uint64_t)r * width + k : (uint64_t)blockIdx.x + ((uint64_t)r * width + k) * nb;
+        const uint64_t t = (uint64_t)r * width + k;
         return t < n_tiles ? (uint32_t)t : n_tiles;
     };
     // The round's tile headers, one per lane, loaded by the whole warp at
     // once, so that lane 0 issues every stage's copies without waiting for a
     // header load.
-    __shared__ uint4 s_hdr[32][kHdrWords / 4];
+    __shared__ uint4 s_hdr[kChunkTiles][kHdrWords / 4];
     while (ok && tile_at(round, 0) < n_tiles) {
-        const uint32_t next = dynamic ? __shfl_sync(0xffffffffu, lane == 0 ? atomicAdd(counter, 1u) : 0u, 0)
-                                      : round + 1;
+        const uint32_t next = __shfl_sync(0xffffffffu, lane == 0 ? atomicAdd(counter, 1u) : 0u, 0);
         const uint32_t t = (uint32_t)lane < width ? tile_at(round, lane) : n_tiles;
         bool act = t < n_tiles;
-        if (act && dynamic) {  // active unless every graph of the tile has stopped
+        if (act && batched) {  // active unless every graph of the tile has stopped
             const uint2 r = trange[t];
             bool stopped = r.y >= r.x && r.y - r.x <= 32;
             for (uint32_t g = r.x; stopped && g <= r.y; g++) stopped = graph_done(s_done, gdone, g);

@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <numeric>
+#include <queue>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -86,6 +87,8 @@ struct flbp_engine {
     void *d_lam = nullptr, *d_lam2 = nullptr, *d_mu = nullptr, *d_gp = nullptr, *d_gq = nullptr;
     void *d_gprior = nullptr, *d_gs = nullptr;
     size_t adj_ckpt_n = 0, adj_seg_n = 0;
+    // staged form: each block's tiles (tile_list / tile_off of the passes)
+    uint32_t *d_ftlist = nullptr, *d_ftoff = nullptr, *d_vtlist = nullptr, *d_vtoff = nullptr;
     uint32_t *d_int_of_var = nullptr, *d_f_of_int = nullptr;  // caller variable -> internal; internal factor -> caller
     uint32_t *d_pri_fac = nullptr, *d_pri_var = nullptr;      // folded constants: caller factor, internal variable
     double *d_pri_coef = nullptr;                             // their d(constant)/dp
@@ -198,6 +201,8 @@ FactorArgs factor_args(flbp_engine *e) {
     a.nf_huge = e->L.nf_huge;
     a.n_fgroups = e->L.n_fgroups();
     a.thdr = reinterpret_cast<const uint4 *>(e->d_ftiles);
+    a.tile_list = e->d_ftlist;
+    a.tile_off = e->d_ftoff;
     a.n_tiles = e->L.n_ftiles;
     a.n_tile_blocks = e->f_tile_blocks;
     a.f_graph = nullptr;
@@ -225,6 +230,8 @@ VarArgs var_args(flbp_engine *e) {
     a.nv_huge = e->L.nv_huge;
     a.n_vgroups = e->L.n_vgroups();
     a.thdr = reinterpret_cast<const uint4 *>(e->d_vtiles);
+    a.tile_list = e->d_vtlist;
+    a.tile_off = e->d_vtoff;
     a.n_tiles = e->L.n_vtiles;
     a.n_tile_blocks = e->v_tile_blocks;
     a.hist_len = e->hist_cap;
@@ -722,6 +729,9 @@ struct BatchSpec {
 int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, flbp_engine **out,
                   const BatchSpec *batch, bool host_layout = false);
 
+// Cost of one item of a tile, in slots, for dealing tiles to blocks.
+constexpr double kTileCostFactorItem = 0.3, kTileCostVarItem = 4.0;
+
 }  // namespace
 
 extern "C" int flbp_engine_create(const flbp_graph_desc *graph, const flbp_engine_opts *opts, flbp_engine **out) {
@@ -852,6 +862,43 @@ void adopt_dev_layout(flbp_engine *e, DevLayout &D) {
     e->d_vbt_prior = D.vbt_prior;
     e->bytes += D.bytes;
     D = DevLayout();
+}
+
+// Deals the tiles of a pass to its `nb` blocks so that every block's total
+// cost is about the same (largest first, each to the least loaded block;
+// the huge items a block takes first count towards its load). A tile costs
+// its slots plus `per_item` per item: a factor's head and denominators, a
+// variable's prior, belief and residual cost more than one slot. Each
+// block's tiles are kept in tile order.
+void deal_tiles(const hvec<uint32_t> &hdr, uint32_t n_tiles, uint32_t nb, double per_item,
+                const std::vector<double> &huge_load, std::vector<uint32_t> &list, std::vector<uint32_t> &off) {
+    std::vector<std::pair<double, uint32_t>> cost(n_tiles);
+    for (uint32_t t = 0; t < n_tiles; t++) {
+        const uint32_t *h = &hdr[(size_t)kHdrWordsHost * t];
+        const uint32_t n = h[1] & ~kBigTileFlag;
+        const double items = (h[1] & kBigTileFlag) ? n : 32.0 * n;
+        cost[t] = {(double)(h[2 + n] - h[2]) + per_item * items, t};
+    }
+    std::stable_sort(cost.begin(), cost.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
+    typedef std::pair<double, uint32_t> Load;  // (load, block)
+    std::priority_queue<Load, std::vector<Load>, std::greater<Load>> q;
+    for (uint32_t b = 0; b < nb; b++) q.push({b < huge_load.size() ? huge_load[b] : 0.0, b});
+    std::vector<std::vector<uint32_t>> per(nb);
+    for (const auto &c : cost) {
+        Load l = q.top();
+        q.pop();
+        per[l.second].push_back(c.second);
+        l.first += c.first;
+        q.push(l);
+    }
+    list.clear();
+    off.assign(1, 0u);
+    for (auto &p : per) {
+        std::sort(p.begin(), p.end());
+        list.insert(list.end(), p.begin(), p.end());
+        off.push_back((uint32_t)list.size());
+    }
+    if (list.empty()) list.push_back(0u);
 }
 
 int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, flbp_engine **out,
@@ -1090,6 +1137,20 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
         FLBP_CUDA(cudaMemsetAsync(e->d_gstate, 0, 4 * sizeof(int) * std::max<size_t>(1, e->n_graphs), e->stream));
         FLBP_CUDA(cudaStreamSynchronize(e->stream));
     }
+    {  // each staged block's tiles
+        std::vector<double> fh((size_t)e->factor_grid, 0.0), vh((size_t)e->var_grid, 0.0);
+        for (uint32_t b = 0; b < L.nf_huge; b++) fh[b % e->factor_grid] += (double)L.fb_deg[b];
+        for (uint32_t b = 0; b < L.nv_huge; b++) vh[b % e->var_grid] += (double)L.vb_deg[b];
+        std::vector<uint32_t> fl, fo, vl, vo;
+        deal_tiles(L.fhdr, L.n_ftiles, (uint32_t)e->factor_grid, kTileCostFactorItem, fh, fl, fo);
+        deal_tiles(L.vhdr, L.n_vtiles, (uint32_t)e->var_grid, kTileCostVarItem, vh, vl, vo);
+        if ((rc = dalloc(e, &e->d_ftlist, fl.size())) || (rc = upload(e, e->d_ftlist, fl)) ||
+            (rc = dalloc(e, &e->d_ftoff, fo.size())) || (rc = upload(e, e->d_ftoff, fo)) ||
+            (rc = dalloc(e, &e->d_vtlist, vl.size())) || (rc = upload(e, e->d_vtlist, vl)) ||
+            (rc = dalloc(e, &e->d_vtoff, vo.size())) || (rc = upload(e, e->d_vtoff, vo)))
+            return fail(rc);
+        FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    }
     e->create_us[3] = us(t_begin, clk()) - e->create_us[0] - e->create_us[1] - e->create_us[2];
     *out = e;
     return FLBP_OK;
@@ -1210,6 +1271,8 @@ int flbp_engine_destroy(flbp_engine *e) {
     for (void *b : e->d_in)
         if (b) cudaFree(b);
     if (e->d_set_cut) cudaFree(e->d_set_cut);
+    for (void *b : {(void *)e->d_ftlist, (void *)e->d_ftoff, (void *)e->d_vtlist, (void *)e->d_vtoff})
+        if (b) cudaFree(b);
     for (void *b : {(void *)e->d_fbt_src, (void *)e->d_vbt_src, (void *)e->d_pri_uvar, (void *)e->d_pri_uoff,
                     (void *)e->d_pri_ord, (void *)e->d_pri_sign, (void *)e->d_p_keep, (void *)e->d_q_keep,
                     (void *)e->d_bad})
@@ -2003,9 +2066,6 @@ void launch_adjoint_step(flbp_engine *e, const void *vf, const void *fv, const v
 // segment writes each sweep's states straight into the segment buffers).
 template <typename T>
 void launch_factor_pass_on(flbp_engine *e, const void *vf, void *fv) {
-    // the staged form's tile counter: the variable pass resets it, and none
-    // need have run since the last factor pass
-    cudaMemsetAsync(reinterpret_cast<char *>(e->d_ctl) + offsetof(Ctl, fnext), 0, sizeof(unsigned int), e->stream);
     const FactorArgs fa = factor_args<T>(e);
     launch_factor<T>(e, fa, vf, fv);
     e->launches += 1;

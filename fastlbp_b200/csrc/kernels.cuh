@@ -203,6 +203,9 @@ struct FactorArgs {
     const uint2 *trange;      // batched solves: per tile, the range of its items' graphs
     uint32_t n_graphs;        // batched solves: number of graphs
     uint32_t nf_sell, nf_big, nf_huge, n_fgroups, n_tiles, n_tile_blocks;
+    // Staged form on one graph: block b's tiles tile_list[tile_off[b] ..
+    // tile_off[b + 1]) (null: tiles b, b + gridDim.x, ...).
+    const uint32_t *tile_list = nullptr, *tile_off = nullptr;
     // Evidence sets on one graph (direct form, set = blockIdx.y): per-set
     // message strides and stopped flags; null / 0 otherwise.
     const int *set_done = nullptr;
@@ -232,6 +235,8 @@ struct VarArgs {
     int *gstate;
     const uint2 *trange;      // per tile, the range of its items' graphs
     uint32_t n_graphs;
+    // Staged form on one graph: block b's tiles (see FactorArgs).
+    const uint32_t *tile_list = nullptr, *tile_off = nullptr;
     // Evidence sets on one graph (direct form, set = blockIdx.y): per-set
     // strides of messages, priors (bytes) and beliefs; gstate / n_graphs
     // then hold the sets' stop state.
@@ -451,43 +456,50 @@ __device__ __forceinline__ bool graph_done(const uint32_t *s_done, const int *gd
     return g < 32u * kDoneWords ? ((s_done[g >> 5] >> (g & 31)) & 1u) != 0 : gdone[g] != 0;
 }
 
-// Producer warp of a pass. Blocks take tiles from the pass's counter (zero
-// when the pass starts: each pass resets the other's), claiming the next
-// while the current one is staged: a single graph's pass one tile per
-// claim, so that blocks that drew cheaper tiles take more and all SMs finish
-// together (claims run in tile order, so neighbouring blocks work on
-// neighbouring tiles at any moment, which keeps the scattered stores of a
-// pass close together); a batched solve chunks of kChunkTiles consecutive
-// tiles, leaving out tiles whose graphs have all stopped. One stage per
-// remaining tile is filled with fill(stage, header in shared memory, full
-// barrier); a stage whose header word 1 is kEndTile closes the stream. All
-// lanes call it; lane 0 issues the copies. After a timeout it records
-// FLBP_ERR_TIMEOUT, lets its own copies land and returns false.
+// Producer warp of a pass. A single graph's pass walks the block's own
+// tiles in order: the list the engine dealt it (tile_list / tile_off, tiles
+// of about equal total cost per block, so that all SMs finish together), or
+// without a list tiles blockIdx.x + i gridDim.x. A batched solve instead takes chunks of kChunkTiles consecutive
+// tiles from the pass's counter, so that blocks whose tiles belong to stopped
+// graphs take more, and leaves out tiles whose graphs have all stopped. One
+// stage per remaining tile is filled with fill(stage, header in shared
+// memory, full barrier); a stage whose header word 1 is kEndTile closes the
+// stream. All lanes call it; lane 0 issues the copies. After a timeout it
+// records FLBP_ERR_TIMEOUT, lets its own copies land and returns false.
 constexpr uint32_t kChunkTiles = 4;
 
 template <int STAGES, typename Fill>
-__device__ bool produce_tiles(const uint4 *thdr, const uint2 *trange, const uint32_t *s_done, const int *gdone,
-                              uint32_t n_tiles, unsigned int *counter, unsigned char *smem, size_t stage_bytes,
-                              uint64_t *full, uint64_t *empty, int lane, Ctl *ctl, Fill fill) {
+__device__ bool produce_tiles(const uint4 *thdr, const uint2 *trange, const uint32_t *tile_list,
+                              const uint32_t *tile_off, const uint32_t *s_done, const int *gdone, uint32_t n_tiles,
+                              unsigned int *counter, unsigned char *smem, size_t stage_bytes, uint64_t *full,
+                              uint64_t *empty, int lane, Ctl *ctl, Fill fill) {
     uint32_t issued = 0;
     bool ok = true;
-    const bool batched = trange != nullptr;
+    const bool dynamic = trange != nullptr;
     // round r covers tiles tile_at(r, 0..width-1)
-    const uint32_t width = batched ? kChunkTiles : 1u;
-    uint32_t round = __shfl_sync(0xffffffffu, lane == 0 ? atomicAdd(counter, 1u) : 0u, 0);
+    const uint32_t width = dynamic ? kChunkTiles : 32u;
+    const uint32_t nb = gridDim.x;
+    uint32_t round = dynamic ? __shfl_sync(0xffffffffu, lane == 0 ? atomicAdd(counter, 1u) : 0u, 0) : 0u;
+    const bool listed = !dynamic && tile_list != nullptr;
+    const uint32_t l0 = listed ? tile_off[blockIdx.x] : 0u, ln = listed ? tile_off[blockIdx.x + 1] - l0 : 0u;
     auto tile_at = [&](uint32_t r, uint32_t k) -> uint32_t {  // n_tiles when out of range
-        const uint64_t t = (uint64_t)r * width + k;
+        if (listed) {
+            const uint64_t i = (uint64_t)r * width + k;
+            return i < ln ? tile_list[l0 + i] : n_tiles;
+        }
+        const uint64_t t = dynamic ? (uint64_t)r * width + k : (uint64_t)blockIdx.x + ((uint64_t)r * width + k) * nb;
         return t < n_tiles ? (uint32_t)t : n_tiles;
     };
     // The round's tile headers, one per lane, loaded by the whole warp at
     // once, so that lane 0 issues every stage's copies without waiting for a
     // header load.
-    __shared__ uint4 s_hdr[kChunkTiles][kHdrWords / 4];
+    __shared__ uint4 s_hdr[32][kHdrWords / 4];
     while (ok && tile_at(round, 0) < n_tiles) {
-        const uint32_t next = __shfl_sync(0xffffffffu, lane == 0 ? atomicAdd(counter, 1u) : 0u, 0);
+        const uint32_t next = dynamic ? __shfl_sync(0xffffffffu, lane == 0 ? atomicAdd(counter, 1u) : 0u, 0)
+                                      : round + 1;
         const uint32_t t = (uint32_t)lane < width ? tile_at(round, lane) : n_tiles;
         bool act = t < n_tiles;
-        if (act && batched) {  // active unless every graph of the tile has stopped
+        if (act && dynamic) {  // active unless every graph of the tile has stopped
             const uint2 r = trange[t];
             bool stopped = r.y >= r.x && r.y - r.x <= 32;
             for (uint32_t g = r.x; stopped && g <= r.y; g++) stopped = graph_done(s_done, gdone, g);
@@ -945,8 +957,8 @@ __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArg
                 bulk_g2s(st + FS::pos, a.f_pos + gb[2], ns * 4u, bar);
             }
         };
-        produce_tiles<STAGES>(a.thdr, a.f_graph ? a.trange : nullptr, s_done, a.gdone, n_tiles, &ctl->fnext, smem,
-                              FS::bytes, full, empty, lane, ctl, fill);
+        produce_tiles<STAGES>(a.thdr, a.f_graph ? a.trange : nullptr, a.tile_list, a.tile_off, s_done, a.gdone, n_tiles,
+                              &ctl->fnext, smem, FS::bytes, full, empty, lane, ctl, fill);
         return;
     }
 
@@ -1406,8 +1418,8 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
                 if (DAMP) bulk_g2s(st + VS::xo, fvd + gb[2], ns * (uint32_t)sizeof(T), bar);
             }
         };
-        produce_tiles<STAGES>(a.thdr, a.v_graph ? a.trange : nullptr, s_done, a.gstate, n_tiles, &ctl->vnext, smem,
-                              VS::bytes, full, empty, lane, ctl, fill);
+        produce_tiles<STAGES>(a.thdr, a.v_graph ? a.trange : nullptr, a.tile_list, a.tile_off, s_done, a.gstate,
+                              n_tiles, &ctl->vnext, smem, VS::bytes, full, empty, lane, ctl, fill);
     } else {  // consumer warps: variables too large for a tile first
         {  // one per block
             __shared__ typename WideAcc<T>::type s_s[kConsumerWarps];

@@ -23,7 +23,10 @@ LIB = os.path.join(HERE, "libfastlbp_b200.so")
 SOURCES = ["engine.cu", "direct.cu", "dlayout.cu", "layout.cpp", "model.cpp", "causal_bp.cpp", "fg_capi.cpp", "noalloc.cu", "schedule.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "nvcc")
-COMMON = ["-std=c++17", "-O3", "-lineinfo", "-ccbin", "g++", "-Xcompiler", "-fPIC", "-I" + INCLUDE]
+# -ftz=true: FP32 device arithmetic flushes subnormal results to zero (fewer instructions around the
+# approximate transcendentals). The message formulas take any product that falls below the smallest
+# normal in log space, so no FP32 message depends on a subnormal value.
+COMMON = ["-std=c++17", "-O3", "-lineinfo", "-ccbin", "g++", "-Xcompiler", "-fPIC", "-ftz=true", "-I" + INCLUDE]
 OPENMP = ["-Xcompiler", "-fopenmp"]  # the host layout build runs on all host threads
 
 

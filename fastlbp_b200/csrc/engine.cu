@@ -87,8 +87,8 @@ struct flbp_engine {
     void *d_lam = nullptr, *d_lam2 = nullptr, *d_mu = nullptr, *d_gp = nullptr, *d_gq = nullptr;
     void *d_gprior = nullptr, *d_gs = nullptr;
     size_t adj_ckpt_n = 0, adj_seg_n = 0;
-    // staged form: each block's tiles (tile_list / tile_off of the passes)
-    uint32_t *d_ftlist = nullptr, *d_ftoff = nullptr, *d_vtlist = nullptr, *d_vtoff = nullptr;
+    // staged factor pass: each block's tiles (FactorArgs::tile_list / tile_off)
+    uint32_t *d_ftlist = nullptr, *d_ftoff = nullptr;
     uint32_t *d_int_of_var = nullptr, *d_f_of_int = nullptr;  // caller variable -> internal; internal factor -> caller
     uint32_t *d_pri_fac = nullptr, *d_pri_var = nullptr;      // folded constants: caller factor, internal variable
     double *d_pri_coef = nullptr;                             // their d(constant)/dp
@@ -230,8 +230,6 @@ VarArgs var_args(flbp_engine *e) {
     a.nv_huge = e->L.nv_huge;
     a.n_vgroups = e->L.n_vgroups();
     a.thdr = reinterpret_cast<const uint4 *>(e->d_vtiles);
-    a.tile_list = e->d_vtlist;
-    a.tile_off = e->d_vtoff;
     a.n_tiles = e->L.n_vtiles;
     a.n_tile_blocks = e->v_tile_blocks;
     a.hist_len = e->hist_cap;
@@ -729,8 +727,8 @@ struct BatchSpec {
 int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, flbp_engine **out,
                   const BatchSpec *batch, bool host_layout = false);
 
-// Cost of one item of a tile, in slots, for dealing tiles to blocks.
-constexpr double kTileCostFactorItem = 0.3, kTileCostVarItem = 4.0;
+// Cost of one factor of a tile, in slots, for dealing tiles to blocks.
+constexpr double kTileCostFactorItem = 0.3;
 
 }  // namespace
 
@@ -867,9 +865,8 @@ void adopt_dev_layout(flbp_engine *e, DevLayout &D) {
 // Deals the tiles of a pass to its `nb` blocks so that every block's total
 // cost is about the same (largest first, each to the least loaded block;
 // the huge items a block takes first count towards its load). A tile costs
-// its slots plus `per_item` per item: a factor's head and denominators, a
-// variable's prior, belief and residual cost more than one slot. Each
-// block's tiles are kept in tile order.
+// its slots plus `per_item` per item (a factor's head and denominators cost
+// more than one slot). Each block's tiles are kept in tile order.
 void deal_tiles(const hvec<uint32_t> &hdr, uint32_t n_tiles, uint32_t nb, double per_item,
                 const std::vector<double> &huge_load, std::vector<uint32_t> &list, std::vector<uint32_t> &off) {
     std::vector<std::pair<double, uint32_t>> cost(n_tiles);
@@ -1137,17 +1134,13 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
         FLBP_CUDA(cudaMemsetAsync(e->d_gstate, 0, 4 * sizeof(int) * std::max<size_t>(1, e->n_graphs), e->stream));
         FLBP_CUDA(cudaStreamSynchronize(e->stream));
     }
-    {  // each staged block's tiles
-        std::vector<double> fh((size_t)e->factor_grid, 0.0), vh((size_t)e->var_grid, 0.0);
+    {  // each staged factor block's tiles (the variable pass keeps tiles b, b + grid, ...: measured faster)
+        std::vector<double> fh((size_t)e->factor_grid, 0.0);
         for (uint32_t b = 0; b < L.nf_huge; b++) fh[b % e->factor_grid] += (double)L.fb_deg[b];
-        for (uint32_t b = 0; b < L.nv_huge; b++) vh[b % e->var_grid] += (double)L.vb_deg[b];
-        std::vector<uint32_t> fl, fo, vl, vo;
+        std::vector<uint32_t> fl, fo;
         deal_tiles(L.fhdr, L.n_ftiles, (uint32_t)e->factor_grid, kTileCostFactorItem, fh, fl, fo);
-        deal_tiles(L.vhdr, L.n_vtiles, (uint32_t)e->var_grid, kTileCostVarItem, vh, vl, vo);
         if ((rc = dalloc(e, &e->d_ftlist, fl.size())) || (rc = upload(e, e->d_ftlist, fl)) ||
-            (rc = dalloc(e, &e->d_ftoff, fo.size())) || (rc = upload(e, e->d_ftoff, fo)) ||
-            (rc = dalloc(e, &e->d_vtlist, vl.size())) || (rc = upload(e, e->d_vtlist, vl)) ||
-            (rc = dalloc(e, &e->d_vtoff, vo.size())) || (rc = upload(e, e->d_vtoff, vo)))
+            (rc = dalloc(e, &e->d_ftoff, fo.size())) || (rc = upload(e, e->d_ftoff, fo)))
             return fail(rc);
         FLBP_CUDA(cudaStreamSynchronize(e->stream));
     }
@@ -1271,7 +1264,7 @@ int flbp_engine_destroy(flbp_engine *e) {
     for (void *b : e->d_in)
         if (b) cudaFree(b);
     if (e->d_set_cut) cudaFree(e->d_set_cut);
-    for (void *b : {(void *)e->d_ftlist, (void *)e->d_ftoff, (void *)e->d_vtlist, (void *)e->d_vtoff})
+    for (void *b : {(void *)e->d_ftlist, (void *)e->d_ftoff})
         if (b) cudaFree(b);
     for (void *b : {(void *)e->d_fbt_src, (void *)e->d_vbt_src, (void *)e->d_pri_uvar, (void *)e->d_pri_uoff,
                     (void *)e->d_pri_ord, (void *)e->d_pri_sign, (void *)e->d_p_keep, (void *)e->d_q_keep,

@@ -235,8 +235,6 @@ struct VarArgs {
     int *gstate;
     const uint2 *trange;      // per tile, the range of its items' graphs
     uint32_t n_graphs;
-    // Staged form on one graph: block b's tiles (see FactorArgs).
-    const uint32_t *tile_list = nullptr, *tile_off = nullptr;
     // Evidence sets on one graph (direct form, set = blockIdx.y): per-set
     // strides of messages, priors (bytes) and beliefs; gstate / n_graphs
     // then hold the sets' stop state.
@@ -1418,8 +1416,8 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
                 if (DAMP) bulk_g2s(st + VS::xo, fvd + gb[2], ns * (uint32_t)sizeof(T), bar);
             }
         };
-        produce_tiles<STAGES>(a.thdr, a.v_graph ? a.trange : nullptr, a.tile_list, a.tile_off, s_done, a.gstate,
-                              n_tiles, &ctl->vnext, smem, VS::bytes, full, empty, lane, ctl, fill);
+        produce_tiles<STAGES>(a.thdr, a.v_graph ? a.trange : nullptr, nullptr, nullptr, s_done, a.gstate, n_tiles,
+                              &ctl->vnext, smem, VS::bytes, full, empty, lane, ctl, fill);
     } else {  // consumer warps: variables too large for a tile first
         {  // one per block
             __shared__ typename WideAcc<T>::type s_s[kConsumerWarps];

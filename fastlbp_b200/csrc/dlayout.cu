@@ -8,6 +8,7 @@
 
 #include <cub/cub.cuh>
 #include <cuda_runtime.h>
+#include <omp.h>
 #include <thrust/iterator/counting_iterator.h>
 #include <thrust/iterator/transform_iterator.h>
 
@@ -42,11 +43,7 @@ __device__ __forceinline__ bool classify_ok(const DevGraphIn &in, int64_t I) {
     const int64_t h = in.head[I];
     if (h < s0 || h >= s1) return false;
     if (t == FLBP_SINGLETON) return d == 1;
-    if (in.clamped && in.clamped[I]) {
-        const double m0 = in.mask0 ? in.mask0[I] : 1.0, m1 = in.mask1 ? in.mask1[I] : 1.0;
-        if (!((m0 == 0.0 || m0 == 1.0) && (m1 == 0.0 || m1 == 1.0))) return false;
-    }
-    return true;
+    return true;  // head masks other than 0 / 1 never reach the device build
 }
 
 // bad[0]: first factor whose offsets decrease; bad[1]: first slot whose
@@ -84,12 +81,10 @@ __global__ void k_classify(DevGraphIn in, int64_t F, uint8_t *active, uint8_t *h
         uint8_t act = 0, hs = HEAD_FREE;
         double c = 0.0;
         if (t != FLBP_SINGLETON) {
-            if (in.clamped && in.clamped[I]) {
-                const double m0 = in.mask0 ? in.mask0[I] : 1.0, m1 = in.mask1 ? in.mask1[I] : 1.0;
-                if (!(m0 == 1.0 && m1 == 1.0)) {
-                    c = (m0 == 0.0) ? inf : -inf;
-                    hs = (m0 == 0.0 && m1 == 1.0) ? HEAD_ONE : (m0 == 1.0 && m1 == 0.0) ? HEAD_ZERO : HEAD_NONE;
-                }
+            const uint8_t m = in.mcode ? in.mcode[I] : kMaskFree;
+            if (m != kMaskFree) {  // m0 == 0: +inf; (0, 1) head 1, (1, 0) head 0, (0, 0) neither
+                c = (m == kMaskZero) ? -inf : inf;
+                hs = (m == kMaskOne) ? HEAD_ONE : (m == kMaskZero) ? HEAD_ZERO : HEAD_NONE;
             }
             act = d > 1 ? 1 : 0;
         }
@@ -262,7 +257,7 @@ __global__ void k_u64_to_u32(const uint64_t *a, uint64_t n, uint32_t *b) {
 }
 
 // (variable, device slot) of every entry, reference slots in increasing order.
-__global__ void k_pair_vars(const uint32_t *ref_slots, const int64_t *slot_var, const uint32_t *dev_slot, uint64_t n,
+__global__ void k_pair_vars(const uint32_t *ref_slots, const int32_t *slot_var, const uint32_t *dev_slot, uint64_t n,
                             uint32_t *vars, uint32_t *dslots) {
     GS_LOOP(i, n) {
         const uint32_t e = ref_slots[i];
@@ -468,13 +463,39 @@ int build_layout_device(const flbp_graph_desc &g, const DevGraphIn &in, int prec
     DL_CHECK(P.err);
     DL_CHECK(cudaMemsetAsync(cnt, 0, 4 * sizeof(unsigned long long), st));
     if (F > 0) k_classify<<<grid_for(F), kTPB, 0, st>>>(in, F, active, hstate, fconst, fkey, fidx, cnt);
-    std::vector<uint32_t> li;  // log-odds of p of every singleton and every factor of one slot, on the host
+    // log-odds of p of every singleton and every factor of one slot, on the host (all threads;
+    // each thread's factors in a contiguous chunk, so the list is in factor order)
+    std::vector<uint32_t> li;
     std::vector<double> lv;
-    for (int64_t I = 0; I < F; I++)
-        if (g.factor_type[I] == FLBP_SINGLETON || g.factor_offsets[I + 1] - g.factor_offsets[I] == 1) {
-            li.push_back((uint32_t)I);
-            lv.push_back(folded_logit(g.factor_p[I]));
+    {
+        auto folded_at = [&](int64_t I) {
+            return g.factor_type[I] == FLBP_SINGLETON || g.factor_offsets[I + 1] - g.factor_offsets[I] == 1;
+        };
+        const int nt = F >= (1 << 16) ? std::max(1, omp_get_max_threads()) : 1;
+        std::vector<int64_t> cnt_t((size_t)nt + 1, 0);
+#pragma omp parallel num_threads(nt)
+        {
+            const int t = omp_get_thread_num(), T = omp_get_num_threads();  // T <= nt
+            const int64_t a = F * t / T, b = F * (t + 1) / T;
+            int64_t c = 0;
+            for (int64_t I = a; I < b; I++) c += folded_at(I) ? 1 : 0;
+            cnt_t[(size_t)t + 1] = c;
+#pragma omp barrier
+#pragma omp single
+            {
+                for (int k = 0; k < T; k++) cnt_t[(size_t)k + 1] += cnt_t[(size_t)k];
+                li.resize((size_t)cnt_t[(size_t)T]);
+                lv.resize((size_t)cnt_t[(size_t)T]);
+            }
+            int64_t o = cnt_t[(size_t)t];
+            for (int64_t I = a; I < b; I++)
+                if (folded_at(I)) {
+                    li[(size_t)o] = (uint32_t)I;
+                    lv[(size_t)o] = folded_logit(g.factor_p[I]);
+                    o++;
+                }
         }
+    }
     if (!li.empty()) {
         uint32_t *dli = P.get<uint32_t>(li.size());
         double *dlv = P.get<double>(lv.size());

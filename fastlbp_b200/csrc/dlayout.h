@@ -20,11 +20,19 @@
 
 namespace flbp {
 
-// The caller's graph arrays, copied to the device (reference order).
+// The caller's graph arrays on the device (reference order), in a compact
+// form: offsets, slot variables and heads as int32 (the device build serves
+// graphs below 2^30 slots), factor types as int8, and per factor the masks
+// of a clamped head as one code (kMaskFree: not clamped or masks (1, 1);
+// kMaskOne (0, 1); kMaskZero (1, 0); kMaskNone (0, 0)), null when no head
+// is clamped. Values that do not fit (and masks other than 0 / 1) send the
+// graph to the host build, which reports them.
+constexpr uint8_t kMaskFree = 0, kMaskOne = 1, kMaskZero = 2, kMaskNone = 3;
 struct DevGraphIn {
-    const int64_t *off = nullptr, *slot_var = nullptr, *head = nullptr;
-    const int32_t *type = nullptr, *clamped = nullptr;
-    const double *p = nullptr, *q = nullptr, *mask0 = nullptr, *mask1 = nullptr;
+    const int32_t *off = nullptr, *slot_var = nullptr, *head = nullptr;
+    const int8_t *type = nullptr;
+    const uint8_t *mcode = nullptr;
+    const double *p = nullptr, *q = nullptr;
 };
 
 // Device buffers of a layout (owned by the caller once built). Per-item

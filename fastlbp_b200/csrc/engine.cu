@@ -14,6 +14,7 @@
 #include <limits>
 #include <atomic>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <tuple>
@@ -795,6 +796,73 @@ void keep_host_graph(flbp_engine *e, const flbp_graph_desc &g) {
 
 // Device build of the layout: the caller's arrays are copied to the device
 // (and kept there for ensure_host_layout), then dlayout.cu builds the layout.
+// Host -> device copies of a graph's inputs go through a pair of pinned
+// staging buffers per device (allocated once per process): the host threads
+// pack the next chunk while the previous one is copied.
+struct PinnedStage {
+    std::mutex mu;
+    char *buf[2] = {nullptr, nullptr};
+    cudaEvent_t done[2] = {nullptr, nullptr};
+};
+constexpr size_t kStageBytes = 8u << 20;
+std::mutex g_stage_mu;
+std::map<int, std::unique_ptr<PinnedStage>> g_stages;
+
+// The staging buffers of `dev` (the current device); null if they cannot be had.
+PinnedStage *stage_for(int dev) {
+    std::lock_guard<std::mutex> lock(g_stage_mu);
+    auto &slot = g_stages[dev];
+    if (!slot) {
+        auto st = std::make_unique<PinnedStage>();
+        for (int k = 0; k < 2; k++)
+            if (cudaHostAlloc((void **)&st->buf[k], kStageBytes, cudaHostAllocDefault) != cudaSuccess ||
+                cudaEventCreateWithFlags(&st->done[k], cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                for (int j = 0; j < 2; j++) {
+                    if (st->buf[j]) cudaFreeHost(st->buf[j]);
+                    if (st->done[j]) cudaEventDestroy(st->done[j]);
+                }
+                return nullptr;
+            }
+        slot = std::move(st);
+    }
+    return slot.get();
+}
+
+// n elements get(i) of type X to dst on the engine's stream, through the
+// staging buffers S (held by the caller), or straight from `plain` (n
+// elements already of type X) without them.
+template <typename X, typename Get>
+cudaError_t staged_h2d(flbp_engine *e, PinnedStage *S, X *dst, size_t n, Get get, const X *plain = nullptr) {
+    if (!S) {
+        if (plain) return cudaMemcpyAsync(dst, plain, n * sizeof(X), cudaMemcpyHostToDevice, e->stream);
+        std::vector<X> tmp(n);
+#pragma omp parallel for if (n >= (1 << 15))
+        for (int64_t i = 0; i < (int64_t)n; i++) tmp[(size_t)i] = get((size_t)i);
+        cudaError_t ce = cudaMemcpyAsync(dst, tmp.data(), n * sizeof(X), cudaMemcpyHostToDevice, e->stream);
+        return ce == cudaSuccess ? cudaStreamSynchronize(e->stream) : ce;
+    }
+    const size_t per = kStageBytes / sizeof(X);
+    int k = 0;
+    for (size_t c = 0; c < n; c += per, k ^= 1) {
+        const size_t m = std::min(per, n - c);
+        cudaError_t ce = cudaEventSynchronize(S->done[k]);  // the buffer's previous chunk has been copied
+        if (ce != cudaSuccess) return ce;
+        X *b = reinterpret_cast<X *>(S->buf[k]);
+#pragma omp parallel for if (m >= (1 << 15))
+        for (int64_t i = 0; i < (int64_t)m; i++) b[i] = get(c + (size_t)i);
+        if ((ce = cudaMemcpyAsync(dst + c, b, m * sizeof(X), cudaMemcpyHostToDevice, e->stream)) != cudaSuccess ||
+            (ce = cudaEventRecord(S->done[k], e->stream)) != cudaSuccess)
+            return ce;
+    }
+    return cudaSuccess;
+}
+
+// device_layout's answer when the compact device input cannot hold the
+// graph (a value beyond int32, a factor type or head mask the build
+// rejects): the host build takes it, and reports what is wrong.
+constexpr int kUseHostBuild = -1;
+
 int device_layout(flbp_engine *e, const flbp_graph_desc &g, DevLayout &D) {
     std::string err;
     int rc = check_graph_shape(g, err);
@@ -803,30 +871,84 @@ int device_layout(flbp_engine *e, const flbp_graph_desc &g, DevLayout &D) {
         return rc;
     }
     const size_t F = (size_t)g.n_factors, E = (size_t)g.n_slots;
-    struct In {
-        const void *src;
-        size_t bytes;
+    // the compact device input (DevGraphIn): int32 offsets, slot variables
+    // and heads, int8 types, the head masks as one code, p and q as given
+    std::atomic<int> bad{0};
+    auto i32 = [&](int64_t x) -> int32_t {
+        if (x < INT32_MIN || x > INT32_MAX) {
+            bad.store(1, std::memory_order_relaxed);
+            return 0;
+        }
+        return (int32_t)x;
     };
-    const In ins[9] = {{g.factor_offsets, F ? (F + 1) * 8 : 0}, {g.slot_var, E * 8}, {g.factor_head, F * 8},
-                       {g.factor_type, F * 4}, {g.factor_p, F * 8}, {g.factor_q, F * 8},
-                       {g.factor_head_clamped, g.factor_head_clamped ? F * 4 : 0},
-                       {g.factor_mask0, g.factor_mask0 ? F * 8 : 0}, {g.factor_mask1, g.factor_mask1 ? F * 8 : 0}};
-    for (int k = 0; k < 9; k++) {
-        if (!ins[k].bytes || !ins[k].src) continue;
-        FLBP_CUDA(cudaMalloc(&e->d_in[k], ins[k].bytes));
-        FLBP_CUDA(cudaMemcpyAsync(e->d_in[k], ins[k].src, ins[k].bytes, cudaMemcpyHostToDevice, e->stream));
-        e->h2d_bytes += ins[k].bytes;
+    const bool any_clamped = g.factor_head_clamped != nullptr && F > 0;
+    const size_t sz[7] = {F ? (F + 1) * 4 : 0, E * 4, F * 4, F, F * 8, F * 8, any_clamped ? F : 0};
+    for (int k = 0; k < 7; k++) {
+        if (!sz[k]) continue;
+        FLBP_CUDA(cudaMalloc(&e->d_in[k], sz[k]));
+        e->h2d_bytes += sz[k];
+    }
+    PinnedStage *S = stage_for(e->device);
+    std::unique_lock<std::mutex> lock;
+    if (S) lock = std::unique_lock<std::mutex>(S->mu);
+    cudaError_t ce = cudaSuccess;
+    auto go = [&](cudaError_t c) {
+        if (ce == cudaSuccess) ce = c;
+    };
+    const int64_t *off = g.factor_offsets, *sv = g.slot_var, *hd = g.factor_head;
+    const int32_t *ty = g.factor_type, *cl = g.factor_head_clamped;
+    const double *m0 = g.factor_mask0, *m1 = g.factor_mask1;
+    if (F) go(staged_h2d<int32_t>(e, S, (int32_t *)e->d_in[0], F + 1, [&](size_t i) { return i32(off[i]); }));
+    if (E) go(staged_h2d<int32_t>(e, S, (int32_t *)e->d_in[1], E, [&](size_t i) { return i32(sv[i]); }));
+    if (F) {
+        go(staged_h2d<int32_t>(e, S, (int32_t *)e->d_in[2], F, [&](size_t i) { return i32(hd[i]); }));
+        go(staged_h2d<int8_t>(e, S, (int8_t *)e->d_in[3], F, [&](size_t i) -> int8_t {
+            const int32_t t = ty[i];
+            if (t != FLBP_SINGLETON && t != FLBP_AND && t != FLBP_OR) {
+                bad.store(1, std::memory_order_relaxed);
+                return 0;
+            }
+            return (int8_t)t;
+        }));
+        go(staged_h2d<double>(e, S, (double *)e->d_in[4], F, [&](size_t i) { return g.factor_p[i]; }, g.factor_p));
+        go(staged_h2d<double>(e, S, (double *)e->d_in[5], F, [&](size_t i) { return g.factor_q[i]; }, g.factor_q));
+    }
+    if (any_clamped)
+        go(staged_h2d<uint8_t>(e, S, (uint8_t *)e->d_in[6], F, [&](size_t i) -> uint8_t {
+            if (!cl[i] || ty[i] == FLBP_SINGLETON) return kMaskFree;
+            const double a = m0 ? m0[i] : 1.0, b = m1 ? m1[i] : 1.0;
+            if (!((a == 0.0 || a == 1.0) && (b == 0.0 || b == 1.0))) {
+                bad.store(1, std::memory_order_relaxed);
+                return kMaskFree;
+            }
+            return a == 1.0 ? (b == 1.0 ? kMaskFree : kMaskZero) : (b == 1.0 ? kMaskOne : kMaskNone);
+        }));
+    if (S) {  // the buffers are free again once their last copies have landed
+        if (ce == cudaSuccess) ce = cudaEventSynchronize(S->done[0]);
+        if (ce == cudaSuccess) ce = cudaEventSynchronize(S->done[1]);
+        lock.unlock();
+    }
+    if (ce != cudaSuccess) {
+        set_error(std::string("graph upload failed: ") + cudaGetErrorString(ce));
+        return FLBP_ERR_CUDA;
+    }
+    if (bad.load()) {
+        for (void *&b : e->d_in)
+            if (b) {
+                cudaFree(b);
+                b = nullptr;
+            }
+        e->h2d_bytes = 0;
+        return kUseHostBuild;
     }
     DevGraphIn &in = e->din;
-    in.off = (const int64_t *)e->d_in[0];
-    in.slot_var = (const int64_t *)e->d_in[1];
-    in.head = (const int64_t *)e->d_in[2];
-    in.type = (const int32_t *)e->d_in[3];
+    in.off = (const int32_t *)e->d_in[0];
+    in.slot_var = (const int32_t *)e->d_in[1];
+    in.head = (const int32_t *)e->d_in[2];
+    in.type = (const int8_t *)e->d_in[3];
     in.p = (const double *)e->d_in[4];
     in.q = (const double *)e->d_in[5];
-    in.clamped = (const int32_t *)e->d_in[6];
-    in.mask0 = (const double *)e->d_in[7];
-    in.mask1 = (const double *)e->d_in[8];
+    in.mcode = (const uint8_t *)e->d_in[6];
     rc = build_layout_device(g, in, e->prec, e->L, D, err, e->stream);
     if (rc) {
         free_dev_layout(D);
@@ -929,7 +1051,7 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
     int rc = FLBP_OK;
     // The host build runs first (a malformed graph is reported without a
     // GPU); the device build needs the engine's device and stream.
-    const bool on_device = !batch && !host_layout && use_device_layout(*graph);
+    bool on_device = !batch && !host_layout && use_device_layout(*graph);
     if (!on_device) {
         GraphIds ids{0, nullptr, nullptr};
         if (batch)
@@ -983,7 +1105,16 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
     DevLayout DL;
     if (on_device) {
         auto tc0 = clk();
-        if ((rc = device_layout(e, *graph, DL))) return fail(rc);
+        rc = device_layout(e, *graph, DL);
+        if (rc == kUseHostBuild) {  // the host build takes the graph (and reports what is wrong with it)
+            if ((rc = build_layout(*graph, e->L, err, nullptr))) {
+                set_error(err);
+                return fail(rc);
+            }
+            keep_host_graph(e, *graph);
+        } else if (rc) {
+            return fail(rc);
+        }
         e->create_us[0] = us(tc0, clk());
     }
     const HostLayout &L = e->L;
@@ -1176,18 +1307,26 @@ int apply_forms(flbp_engine *e, int ff, int vf) {
 // build runs on them; its result equals the device build's (tested).
 int ensure_host_layout(flbp_engine *e) {
     if (e->L.complete) return FLBP_OK;
+    // the compact device input (device_layout) back to the caller's arrays
     const size_t F = (size_t)e->L.F, E = (size_t)e->L.E;
-    std::vector<int64_t> off(F ? F + 1 : 0), sv(E), head(F);
-    std::vector<int32_t> type(F), clamped(e->d_in[6] ? F : 0);
-    std::vector<double> p(F), q(F), m0(e->d_in[7] ? F : 0), m1(e->d_in[8] ? F : 0);
-    void *dst[9] = {off.data(), sv.data(), head.data(), type.data(), p.data(), q.data(), clamped.data(), m0.data(),
-                    m1.data()};
-    const size_t bytes[9] = {off.size() * 8, E * 8, F * 8, F * 4, F * 8, F * 8, clamped.size() * 4, m0.size() * 8,
-                             m1.size() * 8};
-    for (int k = 0; k < 9; k++)
+    std::vector<int32_t> off32(F ? F + 1 : 0), sv32(E), head32(F);
+    std::vector<int8_t> type8(F);
+    std::vector<uint8_t> mcode(e->d_in[6] ? F : 0);
+    std::vector<double> p(F), q(F);
+    void *dst[7] = {off32.data(), sv32.data(), head32.data(), type8.data(), p.data(), q.data(), mcode.data()};
+    const size_t bytes[7] = {off32.size() * 4, E * 4, F * 4, F, F * 8, F * 8, mcode.size()};
+    for (int k = 0; k < 7; k++)
         if (e->d_in[k] && bytes[k])
             FLBP_CUDA(cudaMemcpyAsync(dst[k], e->d_in[k], bytes[k], cudaMemcpyDeviceToHost, e->stream));
     FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    std::vector<int64_t> off(off32.begin(), off32.end()), sv(sv32.begin(), sv32.end()), head(head32.begin(), head32.end());
+    std::vector<int32_t> type(type8.begin(), type8.end()), clamped(mcode.size());
+    std::vector<double> m0(mcode.size()), m1(mcode.size());
+    for (size_t I = 0; I < mcode.size(); I++) {
+        clamped[I] = mcode[I] != kMaskFree;
+        m0[I] = (mcode[I] == kMaskOne || mcode[I] == kMaskNone) ? 0.0 : 1.0;
+        m1[I] = (mcode[I] == kMaskZero || mcode[I] == kMaskNone) ? 0.0 : 1.0;
+    }
     flbp_graph_desc g{};
     g.n_vars = e->L.V;
     g.n_factors = (int64_t)F;

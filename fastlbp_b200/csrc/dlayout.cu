@@ -15,6 +15,8 @@
 #include <algorithm>
 #include <cstring>
 #include <limits>
+#include <mutex>
+#include <map>
 #include <vector>
 
 #include "dlayout.h"
@@ -340,14 +342,48 @@ __global__ void k_pack_prior(const double *fin, const uint32_t *cpos, const uint
 }
 
 // Stream-ordered device memory of the build: temporaries released at the end.
+// Stream-ordered device memory for the build's temporaries, from a memory
+// pool of the builder's own per device that keeps up to kPoolKeep bytes
+// reserved between builds (so that the next engine's build does not map its
+// temporaries anew), or from the device's default pool if that fails.
+constexpr uint64_t kPoolKeep = 1ull << 30;
+std::mutex g_pool_mu;
+std::map<int, cudaMemPool_t> g_pools;
+
+cudaMemPool_t builder_pool() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    auto it = g_pools.find(dev);
+    if (it != g_pools.end()) return it->second;
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+        cudaGetLastError();
+        pool = nullptr;
+    } else {
+        uint64_t keep = kPoolKeep;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    g_pools[dev] = pool;
+    return pool;
+}
+
 struct Pool {
     cudaStream_t st;
+    cudaMemPool_t pool = builder_pool();
     std::vector<void *> tmp;
     cudaError_t err = cudaSuccess;
     template <typename X>
     X *get(size_t n) {
         void *p = nullptr;
-        if (err == cudaSuccess) err = cudaMallocAsync(&p, std::max<size_t>(1, n) * sizeof(X), st);
+        const size_t bytes = std::max<size_t>(1, n) * sizeof(X);
+        if (err == cudaSuccess)
+            err = pool ? cudaMallocFromPoolAsync(&p, bytes, pool, st) : cudaMallocAsync(&p, bytes, st);
         if (p) tmp.push_back(p);
         return static_cast<X *>(p);
     }

@@ -858,6 +858,68 @@ cudaError_t staged_h2d(flbp_engine *e, PinnedStage *S, X *dst, size_t n, Get get
     return cudaSuccess;
 }
 
+// Pinned host copies of the engines' control blocks: slots of a few pinned
+// slabs shared by all engines of the process (a pinned allocation of its own
+// per engine would cost more than the rest of a small engine's creation).
+struct CtlSlots {
+    std::mutex mu;
+    std::vector<Ctl *> free;
+};
+CtlSlots g_ctl_slots;
+constexpr size_t kCtlSlab = 256;
+
+Ctl *ctl_slot_get() {
+    std::lock_guard<std::mutex> lock(g_ctl_slots.mu);
+    if (g_ctl_slots.free.empty()) {
+        Ctl *slab = nullptr;
+        if (cudaHostAlloc((void **)&slab, kCtlSlab * sizeof(Ctl), cudaHostAllocPortable) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        for (size_t i = 0; i < kCtlSlab; i++) g_ctl_slots.free.push_back(slab + (kCtlSlab - 1 - i));
+    }
+    Ctl *c = g_ctl_slots.free.back();
+    g_ctl_slots.free.pop_back();
+    std::memset(c, 0, sizeof(Ctl));
+    return c;
+}
+
+void ctl_slot_put(Ctl *c) {
+    std::lock_guard<std::mutex> lock(g_ctl_slots.mu);
+    g_ctl_slots.free.push_back(c);
+}
+
+// n elements from device memory to the caller's host memory through the
+// staging buffers S (held by the caller; without them a plain copy): each
+// chunk's device copy is in flight while the host threads copy out the
+// previous one. Returns once dst holds everything.
+template <typename X>
+cudaError_t staged_d2h(flbp_engine *e, PinnedStage *S, X *dst, const X *src, size_t n) {
+    cudaError_t ce;
+    if (!S) {
+        if ((ce = cudaMemcpyAsync(dst, src, n * sizeof(X), cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess)
+            return ce;
+        return cudaStreamSynchronize(e->stream);
+    }
+    const size_t per = kStageBytes / sizeof(X), nch = (n + per - 1) / per;
+    auto issue = [&](size_t c) -> cudaError_t {
+        const size_t o = c * per, m = std::min(per, n - o);
+        cudaError_t r = cudaMemcpyAsync(S->buf[c & 1], src + o, m * sizeof(X), cudaMemcpyDeviceToHost, e->stream);
+        return r == cudaSuccess ? cudaEventRecord(S->done[c & 1], e->stream) : r;
+    };
+    for (size_t c = 0; c < nch && c < 2; c++)
+        if ((ce = issue(c)) != cudaSuccess) return ce;
+    for (size_t c = 0; c < nch; c++) {
+        if ((ce = cudaEventSynchronize(S->done[c & 1])) != cudaSuccess) return ce;
+        const size_t o = c * per, m = std::min(per, n - o);
+        const X *b = reinterpret_cast<const X *>(S->buf[c & 1]);
+#pragma omp parallel for if (m >= (1 << 15))
+        for (int64_t i = 0; i < (int64_t)m; i++) dst[o + (size_t)i] = b[i];
+        if (c + 2 < nch && (ce = issue(c + 2)) != cudaSuccess) return ce;
+    }
+    return cudaSuccess;
+}
+
 // device_layout's answer when the compact device input cannot hold the
 // graph (a value beyond int32, a factor type or head mask the build
 // rejects): the host build takes it, and reports what is wrong.
@@ -1162,7 +1224,7 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
             (rc = dalloc(e, &e->d_lowpass, (size_t)L.V)) || (rc = dalloc(e, &e->d_ctl, 1)) ||
             (rc = dalloc(e, &e->d_ref_out, (size_t)L.V)))
             return fail(rc);
-        if (cudaMallocHost((void **)&e->h_ctl, sizeof(Ctl)) != cudaSuccess) {
+        if (!(e->h_ctl = ctl_slot_get())) {
             set_error("pinned allocation failed");
             return fail(FLBP_ERR_NOMEM);
         }
@@ -1186,7 +1248,7 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
             (rc = dalloc(e, &e->d_belief, nv_pad)) || (rc = dalloc(e, &e->d_lowpass, (size_t)L.V)) ||
             (rc = dalloc(e, &e->d_ctl, 1)))
             return fail(rc);
-        if (cudaMallocHost((void **)&e->h_ctl, sizeof(Ctl)) != cudaSuccess) {
+        if (!(e->h_ctl = ctl_slot_get())) {
             set_error("pinned allocation failed");
             return fail(FLBP_ERR_NOMEM);
         }
@@ -1410,7 +1472,7 @@ int flbp_engine_destroy(flbp_engine *e) {
                     (void *)e->d_bad})
         if (b) cudaFree(b);
     if (e->d_set_slots) cudaFree(e->d_set_slots);
-    if (e->h_ctl) cudaFreeHost(e->h_ctl);
+    if (e->h_ctl) ctl_slot_put(e->h_ctl);
     if (e->ev0) cudaEventDestroy(e->ev0);
     if (e->ev1) cudaEventDestroy(e->ev1);
     if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
@@ -1609,8 +1671,10 @@ static int fetch_internal(flbp_engine *e, const double *dsrc, double *out, int64
     gather_vars_kernel<<<(unsigned)((n + 255) / 256), 256, 0, e->stream>>>(dsrc, e->d_int_of_var, n, e->d_ref_out);
     e->launches += 1;
     FLBP_CUDA(cudaGetLastError());
-    FLBP_CUDA(cudaMemcpyAsync(out, e->d_ref_out, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
-    FLBP_CUDA(cudaStreamSynchronize(e->stream));
+    PinnedStage *S = n >= (1 << 16) ? stage_for(e->device) : nullptr;  // large outputs through the staging buffers
+    std::unique_lock<std::mutex> lock;
+    if (S) lock = std::unique_lock<std::mutex>(S->mu);
+    FLBP_CUDA(staged_d2h<double>(e, S, out, e->d_ref_out, (size_t)n));
     return FLBP_OK;
 }
 

@@ -140,20 +140,27 @@ __device__ __forceinline__ T head_out(T lo, T p, T q, T lp) {
 template <typename T>
 struct BodyDen {
     T lden, zero_out, r, alh;  // alh = |lh|
-    bool pos;                  // lh >= 0
+    T pu, qu, pw, qw;          // u = pu Po + qu Ro, w = pw Po + qw Ro of a body slot
+    bool dead;                 // lden == -inf: every body output is zero_out
 };
 
 template <typename T>
 __device__ __forceinline__ BodyDen<T> body_den(T lh, T p, T q) {
     BodyDen<T> D;
-    D.pos = lh >= T(0);
+    const bool pos = lh >= T(0);
     D.alh = fabs(lh);
     D.r = Num<T>::exp(-D.alh);
-    const T u = D.pos ? q : T(1) - q, w = D.pos ? T(1) - q : q;
+    const T u = pos ? q : T(1) - q, w = pos ? T(1) - q : q;
     D.lden = Num<T>::log(u == T(0) ? w : fma(D.r, w, u)) - (u == T(0) ? D.alh : T(0));
-    const T s = D.pos ? (p - q) : (q - p);
+    const T s = pos ? (p - q) : (q - p);
     D.zero_out = is_nan(lh) ? lh : ((s > T(0)) ? Num<T>::inf() : Num<T>::nan());
     if (is_nan(lh)) D.lden = -Num<T>::inf();
+    D.dead = D.lden == -Num<T>::inf();
+    // a = p Po + q Ro, b = (1-p) Po + (1-q) Ro; u = a, w = b for lh >= 0, swapped otherwise
+    D.pu = pos ? p : T(1) - p;
+    D.qu = pos ? q : T(1) - q;
+    D.pw = pos ? T(1) - p : p;
+    D.qw = pos ? T(1) - q : q;
     return D;
 }
 
@@ -161,10 +168,9 @@ __device__ __forceinline__ BodyDen<T> body_den(T lh, T p, T q) {
 template <typename T>
 __device__ __forceinline__ T body_out_pr(T Po, T Ro, T p, T q, const BodyDen<T> &D) {
     // explicit fused forms: the result must not depend on how a caller's code is contracted
-    const T a = fma(p, Po, q * Ro), b = fma(T(1) - p, Po, (T(1) - q) * Ro);
-    const T u = D.pos ? a : b, w = D.pos ? b : a;
+    const T u = fma(D.pu, Po, D.qu * Ro), w = fma(D.pw, Po, D.qw * Ro);
     const T lnum = Num<T>::log(u == T(0) ? w : fma(D.r, w, u)) - (u == T(0) ? D.alh : T(0));
-    return (D.lden == -Num<T>::inf()) ? D.zero_out : lnum - D.lden;
+    return D.dead ? D.zero_out : lnum - D.lden;
 }
 
 // Body output from lo = log Po.
@@ -388,11 +394,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
 
 // Bounded wait for a stage; false on timeout.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;  // the common case: no clock read
     const long long t0 = clock64();
-    while (!mbar_try_wait(bar, parity)) {
-        if (clock64() - t0 > kWaitCycles) return false;
+    for (uint32_t i = 1;; i++) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 15u) == 0 && clock64() - t0 > kWaitCycles) return false;
     }
-    return true;
 }
 
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {

@@ -78,6 +78,7 @@ struct flbp_engine {
     uint32_t *d_f_graph = nullptr, *d_v_graph = nullptr;  // internal factor / variable -> graph
     int *d_gstate = nullptr;  // [4][n_graphs]: stopped, moved, sweeps, stop reason
     uint2 *d_ftrange = nullptr, *d_vtrange = nullptr;  // per tile: range of its items' graphs
+    uint32_t *d_act_f = nullptr, *d_act_v = nullptr;   // batched runs: the passes' tiles that hold a live graph
     // Adjoint: checkpoints of vf every adj_k sweeps of the last adjoint forward
     // run (adj_t sweeps), per-sweep states of one segment, and derivatives.
     long long adj_t = 0, adj_k = 0;
@@ -445,6 +446,7 @@ void launch_sweep(flbp_engine *e, int mode, int which = 3) {
         }
         return;
     }
+    const bool live_lists = mode == 3 && e->d_act_f;  // batched staged passes walk the live tiles only
     if (which & 1) {
         FactorArgs fa = factor_args<T>(e);
         if (mode == 3) {
@@ -452,6 +454,13 @@ void launch_sweep(flbp_engine *e, int mode, int which = 3) {
             fa.gdone = e->d_gstate;
             fa.trange = e->d_ftrange;
             fa.n_graphs = e->n_graphs;
+            if (live_lists) {
+                active_tiles_kernel<<<e->sms, 256, 0, e->stream>>>(e->d_ftrange, e->L.n_ftiles, e->d_vtrange,
+                                                                   e->L.n_vtiles, e->d_gstate, e->d_act_f, e->d_act_v,
+                                                                   e->d_ctl);
+                fa.act_list = e->d_act_f;
+                fa.n_act = &e->d_ctl->n_act_f;
+            }
         }
         launch_factor<T>(e, fa, e->d_vf, e->d_fv);
     }
@@ -462,6 +471,10 @@ void launch_sweep(flbp_engine *e, int mode, int which = 3) {
         va.gstate = e->d_gstate;
         va.trange = e->d_vtrange;
         va.n_graphs = e->n_graphs;
+        if (live_lists) {
+            va.act_list = e->d_act_v;
+            va.n_act = &e->d_ctl->n_act_v;
+        }
     }
     if (e->damping != 0.0) launch_var_mode<T, true>(e, va, mode);
     else launch_var_mode<T, false>(e, va, mode);
@@ -529,7 +542,8 @@ int sweep_graph(flbp_engine *e, int mode, int n, cudaGraphExec_t *out) {
 // a sequential schedule of about 2048 kernels).
 int launch_sweeps(flbp_engine *e, int mode, long long n) {
     if (e->L.nf_sell + e->L.nf_big == 0 && e->L.V == 0) return FLBP_OK;
-    const long long per = e->seq ? seq_sweep_launches(e, mode, 3) : 2 + (e->n_sets && e->n_set_cut ? 1 : 0);
+    const long long per = e->seq ? seq_sweep_launches(e, mode, 3)
+                                 : 2 + (e->n_sets && e->n_set_cut ? 1 : 0) + (mode == 3 && e->d_act_f ? 1 : 0);
     int kmax = 64;
     if (e->seq)
         while (kmax > 1 && (long long)kmax * per > 2048) kmax /= 2;
@@ -1322,7 +1336,8 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
             (rc = dalloc(e, &e->d_gstate, 4 * (size_t)e->n_graphs)) || (rc = upload(e, e->d_f_graph, fg)) ||
             (rc = upload(e, e->d_v_graph, vg)) || (rc = dalloc(e, &e->d_ftrange, fr.size())) ||
             (rc = dalloc(e, &e->d_vtrange, vr.size())) || (rc = upload(e, e->d_ftrange, fr)) ||
-            (rc = upload(e, e->d_vtrange, vr)))
+            (rc = upload(e, e->d_vtrange, vr)) || (rc = dalloc(e, &e->d_act_f, fr.size())) ||
+            (rc = dalloc(e, &e->d_act_v, vr.size())))
             return fail(rc);
         FLBP_CUDA(cudaMemsetAsync(e->d_gstate, 0, 4 * sizeof(int) * std::max<size_t>(1, e->n_graphs), e->stream));
         FLBP_CUDA(cudaStreamSynchronize(e->stream));
@@ -1465,7 +1480,7 @@ int flbp_engine_destroy(flbp_engine *e) {
     for (void *b : e->d_in)
         if (b) cudaFree(b);
     if (e->d_set_cut) cudaFree(e->d_set_cut);
-    for (void *b : {(void *)e->d_ftlist, (void *)e->d_ftoff})
+    for (void *b : {(void *)e->d_ftlist, (void *)e->d_ftoff, (void *)e->d_act_f, (void *)e->d_act_v})
         if (b) cudaFree(b);
     for (void *b : {(void *)e->d_fbt_src, (void *)e->d_vbt_src, (void *)e->d_pri_uvar, (void *)e->d_pri_uoff,
                     (void *)e->d_pri_ord, (void *)e->d_pri_sign, (void *)e->d_p_keep, (void *)e->d_q_keep,

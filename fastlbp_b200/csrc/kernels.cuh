@@ -58,7 +58,9 @@ struct Ctl {
     double damping;
     double pscale;                    // 1 - damping^t: weight of the finite constant priors
     unsigned int fnext, vnext;        // next chunk of tiles of the factor / variable pass (reset by the other pass)
-    unsigned int pad2[2];
+    // batched solves: tiles of the factor / variable pass that hold a live
+    // graph (active_tiles_kernel), and whether those lists are current
+    unsigned int n_act_f, n_act_v, lists_ok, pad2;
 };
 
 template <typename T>
@@ -212,6 +214,10 @@ struct FactorArgs {
     // Staged form on one graph: block b's tiles tile_list[tile_off[b] ..
     // tile_off[b + 1]) (null: tiles b, b + gridDim.x, ...).
     const uint32_t *tile_list = nullptr, *tile_off = nullptr;
+    // Staged form of a batched solve: the tiles that hold a live graph,
+    // act_list[0 .. *n_act) (null: every tile).
+    const uint32_t *act_list = nullptr;
+    const unsigned int *n_act = nullptr;
     // Evidence sets on one graph (direct form, set = blockIdx.y): per-set
     // message strides and stopped flags; null / 0 otherwise.
     const int *set_done = nullptr;
@@ -241,6 +247,9 @@ struct VarArgs {
     int *gstate;
     const uint2 *trange;      // per tile, the range of its items' graphs
     uint32_t n_graphs;
+    // Staged form of a batched solve: the live tiles (see FactorArgs).
+    const uint32_t *act_list = nullptr;
+    const unsigned int *n_act = nullptr;
     // Evidence sets on one graph (direct form, set = blockIdx.y): per-set
     // strides of messages, priors (bytes) and beliefs; gstate / n_graphs
     // then hold the sets' stop state.
@@ -475,9 +484,10 @@ constexpr uint32_t kChunkTiles = 4;
 
 template <int STAGES, typename Fill>
 __device__ bool produce_tiles(const uint4 *thdr, const uint2 *trange, const uint32_t *tile_list,
-                              const uint32_t *tile_off, const uint32_t *s_done, const int *gdone, uint32_t n_tiles,
-                              unsigned int *counter, unsigned char *smem, size_t stage_bytes, uint64_t *full,
-                              uint64_t *empty, int lane, Ctl *ctl, Fill fill) {
+                              const uint32_t *tile_off, const uint32_t *act_list, const unsigned int *n_act,
+                              const uint32_t *s_done, const int *gdone, uint32_t n_tiles, unsigned int *counter,
+                              unsigned char *smem, size_t stage_bytes, uint64_t *full, uint64_t *empty, int lane,
+                              Ctl *ctl, Fill fill) {
     uint32_t issued = 0;
     bool ok = true;
     const bool dynamic = trange != nullptr;
@@ -487,10 +497,16 @@ __device__ bool produce_tiles(const uint4 *thdr, const uint2 *trange, const uint
     uint32_t round = dynamic ? __shfl_sync(0xffffffffu, lane == 0 ? atomicAdd(counter, 1u) : 0u, 0) : 0u;
     const bool listed = !dynamic && tile_list != nullptr;
     const uint32_t l0 = listed ? tile_off[blockIdx.x] : 0u, ln = listed ? tile_off[blockIdx.x + 1] - l0 : 0u;
+    const bool live_list = dynamic && act_list != nullptr;
+    const uint32_t n_live = live_list ? *(volatile const unsigned int *)n_act : 0u;
     auto tile_at = [&](uint32_t r, uint32_t k) -> uint32_t {  // n_tiles when out of range
         if (listed) {
             const uint64_t i = (uint64_t)r * width + k;
             return i < ln ? tile_list[l0 + i] : n_tiles;
+        }
+        if (live_list) {
+            const uint64_t i = (uint64_t)r * width + k;
+            return i < n_live ? act_list[i] : n_tiles;
         }
         const uint64_t t = dynamic ? (uint64_t)r * width + k : (uint64_t)blockIdx.x + ((uint64_t)r * width + k) * nb;
         return t < n_tiles ? (uint32_t)t : n_tiles;
@@ -904,6 +920,7 @@ __device__ __forceinline__ void sweep_open(Ctl *ctl) {
     ctl->nonconv = 0ull;
     ctl->arrive = 0u;
     ctl->vnext = 0u;  // the variable pass of this sweep starts after this kernel
+    ctl->lists_ok = 1u;  // batched solves: active_tiles_kernel has run before this pass
 }
 
 // Factor pass. Every block runs a STAGES-deep pipeline over its tiles (tile
@@ -962,8 +979,8 @@ __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArg
                 bulk_g2s(st + FS::pos, a.f_pos + gb[2], ns * 4u, bar);
             }
         };
-        produce_tiles<STAGES>(a.thdr, a.f_graph ? a.trange : nullptr, a.tile_list, a.tile_off, s_done, a.gdone, n_tiles,
-                              &ctl->fnext, smem, FS::bytes, full, empty, lane, ctl, fill);
+        produce_tiles<STAGES>(a.thdr, a.f_graph ? a.trange : nullptr, a.tile_list, a.tile_off, a.act_list, a.n_act,
+                              s_done, a.gdone, n_tiles, &ctl->fnext, smem, FS::bytes, full, empty, lane, ctl, fill);
         return;
     }
 
@@ -1257,28 +1274,36 @@ static __device__ void stop_rules(Ctl *ctl) {
 // every thread of the last block of the variable pass. The run ends when all
 // graphs have stopped, or at maxtime.
 static __device__ void batch_stop_rules(Ctl *ctl, const VarArgs &a) {
-    __shared__ int s_open;
-    if (threadIdx.x == 0) s_open = 0;
+    __shared__ int s_open, s_stopped;
+    if (threadIdx.x == 0) s_open = s_stopped = 0;
     __syncthreads();
     const uint32_t G = a.n_graphs;
     int *done = a.gstate, *moved = a.gstate + G, *iters = a.gstate + 2 * G, *reason = a.gstate + 3 * G;
-    int open = 0;
+    int open = 0, stopped = 0;
     for (uint32_t g = threadIdx.x; g < G; g += blockDim.x) {
         if (done[g]) continue;
         iters[g] += 1;
         if (!moved[g]) {
             done[g] = 1;
             reason[g] = FLBP_ALL_CONVERGED;
+            stopped = 1;
         } else if (ctl->iters0 + iters[g] >= ctl->maxiter) {
             done[g] = 1;
             reason[g] = FLBP_DIVERGED;
+            stopped = 1;
         } else {
             open++;
         }
         moved[g] = 0;
     }
     if (open) atomicAdd(&s_open, open);
+    if (stopped) s_stopped = 1;
     __syncthreads();
+    if (s_stopped && threadIdx.x == 0) {  // the live-tile lists are rebuilt before the next sweep
+        ctl->lists_ok = 0u;
+        ctl->n_act_f = 0u;
+        ctl->n_act_v = 0u;
+    }
     if (threadIdx.x == 0) {
         ctl->maxdiff = __longlong_as_double((long long)ctl->maxdiff_bits);
         unsigned long long now;
@@ -1289,6 +1314,40 @@ static __device__ void batch_stop_rules(Ctl *ctl, const VarArgs &a) {
         }
         __threadfence();
     }
+}
+
+// Batched solves, before a sweep's factor pass: unless the lists are
+// current, the tiles of each pass whose graph range holds a live graph
+// (ranges of more than 32 graphs count as live) are appended to the pass's
+// list, in any order (each tile's items are computed on their own, so the
+// order changes no result). The stop rules empty the lists when a graph
+// stops; the factor pass marks them current.
+__device__ __forceinline__ void append_live(const uint2 *tr, uint32_t n, const int *done, uint32_t *list,
+                                            unsigned int *count) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+        const uint32_t t = base + lane;
+        bool live = false;
+        if (t < n) {
+            const uint2 r = tr[t];
+            bool stopped = r.y >= r.x && r.y - r.x <= 32;
+            for (uint32_t g = r.x; stopped && g <= r.y; g++) stopped = done[g] != 0;
+            live = !stopped;
+        }
+        const unsigned int bits = __ballot_sync(0xffffffffu, live);
+        unsigned int at = 0;
+        if (lane == 0 && bits) at = atomicAdd(count, (unsigned int)__popc(bits));
+        at = __shfl_sync(0xffffffffu, at, 0);
+        if (live) list[at + __popc(bits & ((1u << lane) - 1u))] = t;
+    }
+}
+
+static __global__ void active_tiles_kernel(const uint2 *ftr, uint32_t nft, const uint2 *vtr, uint32_t nvt, const int *done,
+                                           uint32_t *flist, uint32_t *vlist, Ctl *ctl) {
+    if (*(volatile int *)&ctl->done || *(volatile unsigned int *)&ctl->lists_ok) return;
+    append_live(ftr, nft, done, flist, &ctl->n_act_f);
+    append_live(vtr, nvt, done, vlist, &ctl->n_act_v);
 }
 
 // Batched solves: graph g had a belief move by more than tol this sweep.
@@ -1423,8 +1482,8 @@ __global__ void __launch_bounds__(kBlockThreadsDev) var_pass_kernel(VarArgs a, c
                 if (DAMP) bulk_g2s(st + VS::xo, fvd + gb[2], ns * (uint32_t)sizeof(T), bar);
             }
         };
-        produce_tiles<STAGES>(a.thdr, a.v_graph ? a.trange : nullptr, nullptr, nullptr, s_done, a.gstate, n_tiles,
-                              &ctl->vnext, smem, VS::bytes, full, empty, lane, ctl, fill);
+        produce_tiles<STAGES>(a.thdr, a.v_graph ? a.trange : nullptr, nullptr, nullptr, a.act_list, a.n_act, s_done,
+                              a.gstate, n_tiles, &ctl->vnext, smem, VS::bytes, full, empty, lane, ctl, fill);
     } else {  // consumer warps: variables too large for a tile first
         {  // one per block
             __shared__ typename WideAcc<T>::type s_s[kConsumerWarps];

@@ -1,6 +1,7 @@
 // C-ABI engine: device buffers, sweep launches, the three run loops of
 // CausalBP and host exports. Kernels live in kernels.cuh.
 
+#include <cub/cub.cuh>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -79,6 +80,9 @@ struct flbp_engine {
     int *d_gstate = nullptr;  // [4][n_graphs]: stopped, moved, sweeps, stop reason
     uint2 *d_ftrange = nullptr, *d_vtrange = nullptr;  // per tile: range of its items' graphs
     uint32_t *d_act_f = nullptr, *d_act_v = nullptr;   // batched runs: the passes' tiles that hold a live graph
+    uint8_t *d_act_flag = nullptr;                      // their flags (factor tiles, then variable tiles)
+    void *d_cub_tmp = nullptr;                          // and the compaction's temporary storage
+    size_t cub_tmp_bytes = 0;
     // Adjoint: checkpoints of vf every adj_k sweeps of the last adjoint forward
     // run (adj_t sweeps), per-sweep states of one segment, and derivatives.
     long long adj_t = 0, adj_k = 0;
@@ -454,10 +458,17 @@ void launch_sweep(flbp_engine *e, int mode, int which = 3) {
             fa.gdone = e->d_gstate;
             fa.trange = e->d_ftrange;
             fa.n_graphs = e->n_graphs;
-            if (live_lists) {
-                active_tiles_kernel<<<e->sms, 256, 0, e->stream>>>(e->d_ftrange, e->L.n_ftiles, e->d_vtrange,
-                                                                   e->L.n_vtiles, e->d_gstate, e->d_act_f, e->d_act_v,
-                                                                   e->d_ctl);
+            if (live_lists) {  // flags, then the live tiles of each pass in tile order
+                live_tile_flags_kernel<<<e->sms, 256, 0, e->stream>>>(e->d_ftrange, e->L.n_ftiles, e->d_vtrange,
+                                                                      e->L.n_vtiles, e->d_gstate, e->d_act_flag,
+                                                                      e->d_act_flag + e->L.n_ftiles, e->d_ctl);
+                cub::CountingInputIterator<uint32_t> it(0);
+                size_t tb = e->cub_tmp_bytes;
+                cub::DeviceSelect::Flagged(e->d_cub_tmp, tb, it, e->d_act_flag, e->d_act_f, &e->d_ctl->n_act_f,
+                                           (int)e->L.n_ftiles, e->stream);
+                tb = e->cub_tmp_bytes;
+                cub::DeviceSelect::Flagged(e->d_cub_tmp, tb, it, e->d_act_flag + e->L.n_ftiles, e->d_act_v,
+                                           &e->d_ctl->n_act_v, (int)e->L.n_vtiles, e->stream);
                 fa.act_list = e->d_act_f;
                 fa.n_act = &e->d_ctl->n_act_f;
             }
@@ -543,7 +554,7 @@ int sweep_graph(flbp_engine *e, int mode, int n, cudaGraphExec_t *out) {
 int launch_sweeps(flbp_engine *e, int mode, long long n) {
     if (e->L.nf_sell + e->L.nf_big == 0 && e->L.V == 0) return FLBP_OK;
     const long long per = e->seq ? seq_sweep_launches(e, mode, 3)
-                                 : 2 + (e->n_sets && e->n_set_cut ? 1 : 0) + (mode == 3 && e->d_act_f ? 1 : 0);
+                                 : 2 + (e->n_sets && e->n_set_cut ? 1 : 0) + (mode == 3 && e->d_act_f ? 3 : 0);
     int kmax = 64;
     if (e->seq)
         while (kmax > 1 && (long long)kmax * per > 2048) kmax /= 2;
@@ -1337,8 +1348,18 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
             (rc = upload(e, e->d_v_graph, vg)) || (rc = dalloc(e, &e->d_ftrange, fr.size())) ||
             (rc = dalloc(e, &e->d_vtrange, vr.size())) || (rc = upload(e, e->d_ftrange, fr)) ||
             (rc = upload(e, e->d_vtrange, vr)) || (rc = dalloc(e, &e->d_act_f, fr.size())) ||
-            (rc = dalloc(e, &e->d_act_v, vr.size())))
+            (rc = dalloc(e, &e->d_act_v, vr.size())) || (rc = dalloc(e, &e->d_act_flag, fr.size() + vr.size())))
             return fail(rc);
+        {
+            cub::CountingInputIterator<uint32_t> it(0);
+            size_t a = 0, b = 0;
+            cub::DeviceSelect::Flagged(nullptr, a, it, e->d_act_flag, e->d_act_f, (unsigned int *)nullptr,
+                                       (int)fr.size(), e->stream);
+            cub::DeviceSelect::Flagged(nullptr, b, it, e->d_act_flag, e->d_act_v, (unsigned int *)nullptr,
+                                       (int)vr.size(), e->stream);
+            e->cub_tmp_bytes = std::max<size_t>({a, b, 16});
+            if ((rc = dalloc(e, (char **)&e->d_cub_tmp, e->cub_tmp_bytes))) return fail(rc);
+        }
         FLBP_CUDA(cudaMemsetAsync(e->d_gstate, 0, 4 * sizeof(int) * std::max<size_t>(1, e->n_graphs), e->stream));
         FLBP_CUDA(cudaStreamSynchronize(e->stream));
     }
@@ -1480,7 +1501,8 @@ int flbp_engine_destroy(flbp_engine *e) {
     for (void *b : e->d_in)
         if (b) cudaFree(b);
     if (e->d_set_cut) cudaFree(e->d_set_cut);
-    for (void *b : {(void *)e->d_ftlist, (void *)e->d_ftoff, (void *)e->d_act_f, (void *)e->d_act_v})
+    for (void *b : {(void *)e->d_ftlist, (void *)e->d_ftoff, (void *)e->d_act_f, (void *)e->d_act_v,
+                    (void *)e->d_act_flag, e->d_cub_tmp})
         if (b) cudaFree(b);
     for (void *b : {(void *)e->d_fbt_src, (void *)e->d_vbt_src, (void *)e->d_pri_uvar, (void *)e->d_pri_uoff,
                     (void *)e->d_pri_ord, (void *)e->d_pri_sign, (void *)e->d_p_keep, (void *)e->d_q_keep,

@@ -58,9 +58,8 @@ struct Ctl {
     double damping;
     double pscale;                    // 1 - damping^t: weight of the finite constant priors
     unsigned int fnext, vnext;        // next chunk of tiles of the factor / variable pass (reset by the other pass)
-    // batched solves: tiles of the factor / variable pass that hold a live
-    // graph (active_tiles_kernel), and whether those lists are current
-    unsigned int n_act_f, n_act_v, lists_ok, pad2;
+    // batched solves: number of tiles of the factor / variable pass that hold a live graph
+    unsigned int n_act_f, n_act_v;
 };
 
 template <typename T>
@@ -920,7 +919,6 @@ __device__ __forceinline__ void sweep_open(Ctl *ctl) {
     ctl->nonconv = 0ull;
     ctl->arrive = 0u;
     ctl->vnext = 0u;  // the variable pass of this sweep starts after this kernel
-    ctl->lists_ok = 1u;  // batched solves: active_tiles_kernel has run before this pass
 }
 
 // Factor pass. Every block runs a STAGES-deep pipeline over its tiles (tile
@@ -1274,36 +1272,28 @@ static __device__ void stop_rules(Ctl *ctl) {
 // every thread of the last block of the variable pass. The run ends when all
 // graphs have stopped, or at maxtime.
 static __device__ void batch_stop_rules(Ctl *ctl, const VarArgs &a) {
-    __shared__ int s_open, s_stopped;
-    if (threadIdx.x == 0) s_open = s_stopped = 0;
+    __shared__ int s_open;
+    if (threadIdx.x == 0) s_open = 0;
     __syncthreads();
     const uint32_t G = a.n_graphs;
     int *done = a.gstate, *moved = a.gstate + G, *iters = a.gstate + 2 * G, *reason = a.gstate + 3 * G;
-    int open = 0, stopped = 0;
+    int open = 0;
     for (uint32_t g = threadIdx.x; g < G; g += blockDim.x) {
         if (done[g]) continue;
         iters[g] += 1;
         if (!moved[g]) {
             done[g] = 1;
             reason[g] = FLBP_ALL_CONVERGED;
-            stopped = 1;
         } else if (ctl->iters0 + iters[g] >= ctl->maxiter) {
             done[g] = 1;
             reason[g] = FLBP_DIVERGED;
-            stopped = 1;
         } else {
             open++;
         }
         moved[g] = 0;
     }
     if (open) atomicAdd(&s_open, open);
-    if (stopped) s_stopped = 1;
     __syncthreads();
-    if (s_stopped && threadIdx.x == 0) {  // the live-tile lists are rebuilt before the next sweep
-        ctl->lists_ok = 0u;
-        ctl->n_act_f = 0u;
-        ctl->n_act_v = 0u;
-    }
     if (threadIdx.x == 0) {
         ctl->maxdiff = __longlong_as_double((long long)ctl->maxdiff_bits);
         unsigned long long now;
@@ -1316,38 +1306,20 @@ static __device__ void batch_stop_rules(Ctl *ctl, const VarArgs &a) {
     }
 }
 
-// Batched solves, before a sweep's factor pass: unless the lists are
-// current, the tiles of each pass whose graph range holds a live graph
-// (ranges of more than 32 graphs count as live) are appended to the pass's
-// list, in any order (each tile's items are computed on their own, so the
-// order changes no result). The stop rules empty the lists when a graph
-// stops; the factor pass marks them current.
-__device__ __forceinline__ void append_live(const uint2 *tr, uint32_t n, const int *done, uint32_t *list,
-                                            unsigned int *count) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
-        const uint32_t t = base + lane;
-        bool live = false;
-        if (t < n) {
-            const uint2 r = tr[t];
-            bool stopped = r.y >= r.x && r.y - r.x <= 32;
-            for (uint32_t g = r.x; stopped && g <= r.y; g++) stopped = done[g] != 0;
-            live = !stopped;
-        }
-        const unsigned int bits = __ballot_sync(0xffffffffu, live);
-        unsigned int at = 0;
-        if (lane == 0 && bits) at = atomicAdd(count, (unsigned int)__popc(bits));
-        at = __shfl_sync(0xffffffffu, at, 0);
-        if (live) list[at + __popc(bits & ((1u << lane) - 1u))] = t;
+// Batched solves, before a sweep's factor pass: per tile of each pass,
+// whether its graph range holds a live graph (ranges of more than 32
+// graphs count as live). The engine compacts the flags into the passes'
+// tile lists, in tile order.
+static __global__ void live_tile_flags_kernel(const uint2 *ftr, uint32_t nft, const uint2 *vtr, uint32_t nvt,
+                                              const int *done, uint8_t *fflag, uint8_t *vflag, const Ctl *ctl) {
+    if (*(volatile const int *)&ctl->done) return;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nft + nvt; i += gridDim.x * blockDim.x) {
+        const uint2 r = i < nft ? ftr[i] : vtr[i - nft];
+        bool stopped = r.y >= r.x && r.y - r.x <= 32;
+        for (uint32_t g = r.x; stopped && g <= r.y; g++) stopped = done[g] != 0;
+        if (i < nft) fflag[i] = stopped ? 0 : 1;
+        else vflag[i - nft] = stopped ? 0 : 1;
     }
-}
-
-static __global__ void active_tiles_kernel(const uint2 *ftr, uint32_t nft, const uint2 *vtr, uint32_t nvt, const int *done,
-                                           uint32_t *flist, uint32_t *vlist, Ctl *ctl) {
-    if (*(volatile int *)&ctl->done || *(volatile unsigned int *)&ctl->lists_ok) return;
-    append_live(ftr, nft, done, flist, &ctl->n_act_f);
-    append_live(vtr, nvt, done, vlist, &ctl->n_act_v);
 }
 
 // Batched solves: graph g had a belief move by more than tol this sweep.

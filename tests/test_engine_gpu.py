@@ -250,3 +250,30 @@ def test_fault_localisation_statement_ranking():
     d_e = b[stm][:, None] - b[stm][None, :]
     sure = np.abs(d_o) > 2 * TOL[32]
     assert np.all(np.sign(d_e[sure]) == np.sign(d_o[sure]))
+
+
+def test_reset_counts_gives_a_new_engines_run():
+    """run_tol's maxiter counts every sweep since construction (the
+    reference's _iters), so a second tolerance run on the same engine can
+    stop at the limit; flbp_reset_counts gives the engine a new engine's
+    sweep count and beliefs, and the next init() + run_tol repeats a new
+    engine's run bit for bit."""
+    fl = workloads.config0(2)
+    g, _ = _pair(fl)
+    a = g.graph_arrays()
+    fresh = Engine(a, precision=32)
+    fresh.init()
+    want = fresh.run_tol(1e-6, 60, 1e9)
+    b_want = fresh.beliefs()
+    eng = Engine(a, precision=32)
+    for _ in range(3):
+        eng.init()
+        eng.run_tol(1e-6, 60, 1e9)
+    eng.init()
+    capped = eng.run_tol(1e-6, 60, 1e9)
+    assert capped["sweeps"] < want["sweeps"]  # the limit counts the earlier runs' sweeps too
+    eng.reset_counts()
+    eng.init()
+    got = eng.run_tol(1e-6, 60, 1e9)
+    assert got["sweeps"] == want["sweeps"] and got["reason"] == want["reason"]
+    assert np.array_equal(eng.beliefs(), b_want)

@@ -450,7 +450,8 @@ void launch_sweep(flbp_engine *e, int mode, int which = 3) {
         }
         return;
     }
-    const bool live_lists = mode == 3 && e->d_act_f;  // batched staged passes walk the live tiles only
+    // batched staged passes walk the live tiles only (the direct forms skip stopped graphs' items themselves)
+    const bool live_lists = mode == 3 && e->d_act_f && (e->f_form == 0 || e->v_form == 0);
     if (which & 1) {
         FactorArgs fa = factor_args<T>(e);
         if (mode == 3) {
@@ -554,7 +555,8 @@ int sweep_graph(flbp_engine *e, int mode, int n, cudaGraphExec_t *out) {
 int launch_sweeps(flbp_engine *e, int mode, long long n) {
     if (e->L.nf_sell + e->L.nf_big == 0 && e->L.V == 0) return FLBP_OK;
     const long long per = e->seq ? seq_sweep_launches(e, mode, 3)
-                                 : 2 + (e->n_sets && e->n_set_cut ? 1 : 0) + (mode == 3 && e->d_act_f ? 3 : 0);
+                                 : 2 + (e->n_sets && e->n_set_cut ? 1 : 0) +
+                                       (mode == 3 && e->d_act_f && (e->f_form == 0 || e->v_form == 0) ? 3 : 0);
     int kmax = 64;
     if (e->seq)
         while (kmax > 1 && (long long)kmax * per > 2048) kmax /= 2;

@@ -421,43 +421,8 @@ void free_dev_layout(DevLayout &D) {
         }                                                                  \
     } while (0)
 
-// Every singleton and every factor of one slot (factor order) with the
-// log-odds of its p, folded_logit(p), computed on `threads` host threads
-// (0: all); each thread takes a contiguous chunk of factors.
-void folded_logits(const flbp_graph_desc &g, int threads, std::vector<uint32_t> &li, std::vector<double> &lv) {
-    const int64_t F = g.n_factors;
-    auto folded_at = [&](int64_t I) {
-        return g.factor_type[I] == FLBP_SINGLETON || g.factor_offsets[I + 1] - g.factor_offsets[I] == 1;
-    };
-    const int nt = F >= (1 << 16) ? std::max(1, threads > 0 ? threads : omp_get_max_threads()) : 1;
-    std::vector<int64_t> cnt_t((size_t)nt + 1, 0);
-#pragma omp parallel num_threads(nt)
-    {
-        const int t = omp_get_thread_num(), T = omp_get_num_threads();  // T <= nt
-        const int64_t a = F * t / T, b = F * (t + 1) / T;
-        int64_t c = 0;
-        for (int64_t I = a; I < b; I++) c += folded_at(I) ? 1 : 0;
-        cnt_t[(size_t)t + 1] = c;
-#pragma omp barrier
-#pragma omp single
-        {
-            for (int k = 0; k < T; k++) cnt_t[(size_t)k + 1] += cnt_t[(size_t)k];
-            li.resize((size_t)cnt_t[(size_t)T]);
-            lv.resize((size_t)cnt_t[(size_t)T]);
-        }
-        int64_t o = cnt_t[(size_t)t];
-        for (int64_t I = a; I < b; I++)
-            if (folded_at(I)) {
-                li[(size_t)o] = (uint32_t)I;
-                lv[(size_t)o] = folded_logit(g.factor_p[I]);
-                o++;
-            }
-    }
-}
-
 int build_layout_device(const flbp_graph_desc &g, const DevGraphIn &in, int prec, HostLayout &L, DevLayout &D,
-                        std::string &err, cudaStream_t st, const std::vector<uint32_t> *li_in,
-                        const std::vector<double> *lv_in) {
+                        std::string &err, cudaStream_t st) {
     const int64_t V = g.n_vars, F = g.n_factors, E = g.n_slots;
     L = HostLayout();
     L.complete = false;
@@ -534,11 +499,39 @@ int build_layout_device(const flbp_graph_desc &g, const DevGraphIn &in, int prec
     DL_CHECK(P.err);
     DL_CHECK(cudaMemsetAsync(cnt, 0, 4 * sizeof(unsigned long long), st));
     if (F > 0) k_classify<<<grid_for(F), kTPB, 0, st>>>(in, F, active, hstate, fconst, fkey, fidx, cnt);
-    std::vector<uint32_t> li_own;
-    std::vector<double> lv_own;
-    if (!li_in || !lv_in) folded_logits(g, 0, li_own, lv_own);
-    const std::vector<uint32_t> &li = li_in && lv_in ? *li_in : li_own;
-    const std::vector<double> &lv = li_in && lv_in ? *lv_in : lv_own;
+    // log-odds of p of every singleton and every factor of one slot, on the host (all threads;
+    // each thread's factors in a contiguous chunk, so the list is in factor order)
+    std::vector<uint32_t> li;
+    std::vector<double> lv;
+    {
+        auto folded_at = [&](int64_t I) {
+            return g.factor_type[I] == FLBP_SINGLETON || g.factor_offsets[I + 1] - g.factor_offsets[I] == 1;
+        };
+        const int nt = F >= (1 << 16) ? std::max(1, omp_get_max_threads()) : 1;
+        std::vector<int64_t> cnt_t((size_t)nt + 1, 0);
+#pragma omp parallel num_threads(nt)
+        {
+            const int t = omp_get_thread_num(), T = omp_get_num_threads();  // T <= nt
+            const int64_t a = F * t / T, b = F * (t + 1) / T;
+            int64_t c = 0;
+            for (int64_t I = a; I < b; I++) c += folded_at(I) ? 1 : 0;
+            cnt_t[(size_t)t + 1] = c;
+#pragma omp barrier
+#pragma omp single
+            {
+                for (int k = 0; k < T; k++) cnt_t[(size_t)k + 1] += cnt_t[(size_t)k];
+                li.resize((size_t)cnt_t[(size_t)T]);
+                lv.resize((size_t)cnt_t[(size_t)T]);
+            }
+            int64_t o = cnt_t[(size_t)t];
+            for (int64_t I = a; I < b; I++)
+                if (folded_at(I)) {
+                    li[(size_t)o] = (uint32_t)I;
+                    lv[(size_t)o] = folded_logit(g.factor_p[I]);
+                    o++;
+                }
+        }
+    }
     if (!li.empty()) {
         uint32_t *dli = P.get<uint32_t>(li.size());
         double *dlv = P.get<double>(lv.size());

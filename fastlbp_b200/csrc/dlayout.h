@@ -15,7 +15,6 @@
 
 #include <cstdint>
 #include <string>
-#include <vector>
 
 #include "engine_internal.h"
 
@@ -53,16 +52,8 @@ struct DevLayout {
 // copy `in`, for messages of `prec` bits (32 / 64). Fills the counts and
 // small arrays of L (L.complete false) and the buffers of D. On a malformed
 // graph returns the host build's error code and message.
-// The folded constants' log-odds (folded_logits) may be passed in, computed
-// while the inputs were being copied.
 int build_layout_device(const flbp_graph_desc &g, const DevGraphIn &in, int prec, HostLayout &L, DevLayout &D,
-                        std::string &err, cudaStream_t st, const std::vector<uint32_t> *li_in = nullptr,
-                        const std::vector<double> *lv_in = nullptr);
-
-// Every singleton and every factor of one slot, in factor order, with the
-// log-odds of its p (the host build's folded_logit), on `threads` host
-// threads (0: all).
-void folded_logits(const flbp_graph_desc &g, int threads, std::vector<uint32_t> &li, std::vector<double> &lv);
+                        std::string &err, cudaStream_t st);
 
 // Frees the buffers of D.
 void free_dev_layout(DevLayout &D);

@@ -14,7 +14,6 @@
 #include <cstring>
 #include <limits>
 #include <atomic>
-#include <future>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -971,10 +970,6 @@ int device_layout(flbp_engine *e, const flbp_graph_desc &g, DevLayout &D) {
         }
         return (int32_t)x;
     };
-    // the folded constants' log-odds on a few host threads while the inputs are packed and copied
-    std::vector<uint32_t> li;
-    std::vector<double> lv;
-    auto logits = std::async(std::launch::async, [&] { folded_logits(g, 4, li, lv); });
     const bool any_clamped = g.factor_head_clamped != nullptr && F > 0;
     const size_t sz[7] = {F ? (F + 1) * 4 : 0, E * 4, F * 4, F, F * 8, F * 8, any_clamped ? F : 0};
     for (int k = 0; k < 7; k++) {
@@ -1043,8 +1038,7 @@ int device_layout(flbp_engine *e, const flbp_graph_desc &g, DevLayout &D) {
     in.p = (const double *)e->d_in[4];
     in.q = (const double *)e->d_in[5];
     in.mcode = (const uint8_t *)e->d_in[6];
-    logits.get();
-    rc = build_layout_device(g, in, e->prec, e->L, D, err, e->stream, &li, &lv);
+    rc = build_layout_device(g, in, e->prec, e->L, D, err, e->stream);
     if (rc) {
         free_dev_layout(D);
         set_error(err);

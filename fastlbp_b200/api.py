@@ -349,8 +349,15 @@ class Engine:
                                      float(maxtime), self._info()))
         return self.info.as_dict()
 
-    def beliefs(self) -> np.ndarray:
-        out = np.zeros(self.n_vars)
+    def beliefs(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Beliefs P(x_i = 1) of the last run, in variable order; into `out`
+        (a C-contiguous float64 array of n_vars elements, e.g. one buffer
+        reused over many solves) when given."""
+        if out is None:
+            out = np.empty(self.n_vars)
+        elif not (isinstance(out, np.ndarray) and out.dtype == np.float64 and out.flags.c_contiguous
+                  and out.size == self.n_vars):
+            raise FlbpError("out must be a C-contiguous float64 array of n_vars elements")
         check(lib().flbp_get_beliefs(self._h, out, out.size))
         return out
 

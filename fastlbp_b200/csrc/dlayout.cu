@@ -3,12 +3,11 @@
 // scans, with the same results bit for bit. Counting sorts of the host build
 // become stable radix sorts of (class, tie-break) keys whose input is in
 // index order, so items of equal key keep index order as on the host. The
-// folded constants' log-odds are computed on the host (folded_logit) and
-// summed per variable in factor order, as the host build sums them.
+// folded constants' log-odds (det_logit, the same bits on host and device)
+// are summed per variable in factor order, as the host build sums them.
 
 #include <cub/cub.cuh>
 #include <cuda_runtime.h>
-#include <omp.h>
 #include <thrust/iterator/counting_iterator.h>
 #include <thrust/iterator/transform_iterator.h>
 
@@ -20,6 +19,7 @@
 #include <vector>
 
 #include "dlayout.h"
+#include "logodds.h"
 
 namespace flbp {
 
@@ -29,6 +29,19 @@ constexpr unsigned kTPB = 256;
 
 unsigned grid_for(uint64_t n) {
     return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + kTPB - 1) / kTPB, 148ull * 16));
+}
+
+// Sum over a warp (every lane active). Counters that every item adds to
+// take one atomic per warp: thousands of them instead of millions on one
+// address, which the memory system would serialise.
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long x) {
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+__device__ __forceinline__ void warp_add(unsigned long long *dst, unsigned long long x) {
+    x = warp_sum(x);
+    if ((threadIdx.x & 31) == 0 && x) atomicAdd(dst, x);
 }
 
 #define GS_LOOP(i, n)                                                                                  \
@@ -70,23 +83,30 @@ constexpr int kFactorKeyBits = 38;
 constexpr uint64_t kInactiveKey = (1ull << kFactorKeyBits) - 1;
 
 // Active / head state / constant message of every factor (the host's
-// classify_factor; finite folded constants are filled in by
-// k_scatter_logit), the factor sort keys and counts: cnt[0] sliced-ELL
-// factors, cnt[1] large ones, cnt[2] slots of active factors.
+// classify_factor: +-det_logit(p) of singletons and of unclamped factors of
+// one slot, +-inf of clamped heads), the factor sort keys and counts:
+// cnt[0] sliced-ELL factors, cnt[1] large ones, cnt[2] slots of active
+// factors.
 __global__ void k_classify(DevGraphIn in, int64_t F, uint8_t *active, uint8_t *hstate, double *fconst,
                            uint64_t *fkey, uint32_t *fidx, unsigned long long *cnt) {
     const double inf = __longlong_as_double(0x7ff0000000000000ll);
+    unsigned long long n_sell = 0, n_big = 0, n_slots = 0;
     GS_LOOP(i, F) {
         const int64_t I = (int64_t)i;
         const int64_t d = in.off[I + 1] - in.off[I];
         const int32_t t = in.type[I];
         uint8_t act = 0, hs = HEAD_FREE;
         double c = 0.0;
-        if (t != FLBP_SINGLETON) {
+        if (t == FLBP_SINGLETON) {
+            c = det_logit(in.p[I]);
+        } else {
             const uint8_t m = in.mcode ? in.mcode[I] : kMaskFree;
             if (m != kMaskFree) {  // m0 == 0: +inf; (0, 1) head 1, (1, 0) head 0, (0, 0) neither
                 c = (m == kMaskZero) ? -inf : inf;
                 hs = (m == kMaskOne) ? HEAD_ONE : (m == kMaskZero) ? HEAD_ZERO : HEAD_NONE;
+            } else if (d == 1) {
+                const double l = det_logit(in.p[I]);
+                c = (t == FLBP_AND) ? l : -l;
             }
             act = d > 1 ? 1 : 0;
         }
@@ -98,28 +118,19 @@ __global__ void k_classify(DevGraphIn in, int64_t F, uint8_t *active, uint8_t *h
         if (act) {
             if (d <= (int64_t)kSellFactorDegree) {
                 key = (uint64_t)d << 33;
-                atomicAdd(&cnt[0], 1ull);
+                n_sell++;
             } else {
                 const uint64_t huge = (uint64_t)(d - 1 > (int64_t)kBigFactorBody ? 0 : 1);
                 key = (17ull << 33) | (huge << 32) | (uint64_t)(0xffffffffu - (uint32_t)d);
-                atomicAdd(&cnt[1], 1ull);
+                n_big++;
             }
-            atomicAdd(&cnt[2], (unsigned long long)d);
+            n_slots += (unsigned long long)d;
         }
         fkey[I] = key;
     }
-}
-
-// Finite constants of singletons and of factors reduced to their head: the
-// host's log-odds of p, negated for OR (folded_logit(p) per listed factor).
-__global__ void k_scatter_logit(DevGraphIn in, const uint32_t *idx, const double *lg, uint64_t n,
-                                const uint8_t *hstate, double *fconst) {
-    GS_LOOP(k, n) {
-        const uint32_t I = idx[k];
-        const int32_t t = in.type[I];
-        if (t == FLBP_SINGLETON) fconst[I] = lg[k];
-        else if (hstate[I] == HEAD_FREE) fconst[I] = (t == FLBP_AND) ? lg[k] : -lg[k];
-    }
+    warp_add(&cnt[0], n_sell);
+    warp_add(&cnt[1], n_big);
+    warp_add(&cnt[2], n_slots);
 }
 
 // Per active factor in internal order: kind, (p, q), degree; large ones'
@@ -207,12 +218,13 @@ __global__ void k_entries(DevGraphIn in, const uint32_t *foi, uint32_t nf, const
 constexpr int kVarKeyBits = 39;
 __global__ void k_var_keys(const uint32_t *vdeg, const uint32_t *first, uint64_t V, uint64_t *vkey, uint32_t *vidx,
                            unsigned long long *cnt) {
+    unsigned long long n_sell = 0;
     GS_LOOP(v, V) {
         const uint32_t d = vdeg[v];
         uint64_t key;
         if (d <= kSellVarDegree) {
             key = ((uint64_t)d << 34) | (d == 0 ? 0ull : (uint64_t)first[v]);
-            atomicAdd(cnt, 1ull);
+            n_sell++;
         } else {
             const uint64_t huge = d > kTileSlotsHost ? 0 : 1;
             key = (17ull << 34) | (huge << 32) | (uint64_t)(0xffffffffu - d);
@@ -220,6 +232,7 @@ __global__ void k_var_keys(const uint32_t *vdeg, const uint32_t *first, uint64_t
         vkey[v] = key;
         vidx[v] = (uint32_t)v;
     }
+    warp_add(cnt, n_sell);
 }
 
 __global__ void k_inverse(const uint32_t *order, uint64_t n, uint32_t *inv) {
@@ -341,16 +354,21 @@ __global__ void k_pack_prior(const double *fin, const uint32_t *cpos, const uint
     }
 }
 
-// Stream-ordered device memory of the build: temporaries released at the end.
-// Stream-ordered device memory for the build's temporaries, from a memory
-// pool of the builder's own per device that keeps up to kPoolKeep bytes
-// reserved between builds (so that the next engine's build does not map its
-// temporaries anew), or from the device's default pool if that fails.
-constexpr uint64_t kPoolKeep = 1ull << 30;
+// Device memory of engines and of their layout builds comes from a memory
+// pool per device that keeps up to kPoolKeep bytes reserved when it is
+// freed: the next engine's buffers and build temporaries are then taken
+// from memory already mapped instead of new cudaMalloc calls (which cost
+// more than the rest of a small engine's creation, and milliseconds for a
+// large one). Allocations are ordered on the creating stream; buffers are
+// freed with cudaFreeAsync on the stream that uses them, or with cudaFree
+// once that stream has finished (cudaFree does not wait for work that still
+// reads pool memory). If the pool cannot be made, the device's default
+// pool serves.
+constexpr uint64_t kPoolKeep = 4ull << 30;
 std::mutex g_pool_mu;
 std::map<int, cudaMemPool_t> g_pools;
 
-cudaMemPool_t builder_pool() {
+cudaMemPool_t device_pool() {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
     std::lock_guard<std::mutex> lock(g_pool_mu);
@@ -375,7 +393,7 @@ cudaMemPool_t builder_pool() {
 
 struct Pool {
     cudaStream_t st;
-    cudaMemPool_t pool = builder_pool();
+    cudaMemPool_t pool = device_pool();
     std::vector<void *> tmp;
     cudaError_t err = cudaSuccess;
     template <typename X>
@@ -393,22 +411,28 @@ struct Pool {
 };
 
 template <typename X>
-cudaError_t dalloc_out(X **p, size_t n, DevLayout &D) {
+cudaError_t dalloc_out(X **p, size_t n, DevLayout &D, cudaStream_t st) {
     *p = nullptr;
     const size_t bytes = std::max<size_t>(1, n) * sizeof(X);
-    cudaError_t e = cudaMalloc((void **)p, bytes);
+    cudaError_t e = pool_malloc((void **)p, bytes, st);
     if (e == cudaSuccess) D.bytes += bytes;
     return e;
 }
 
 }  // namespace
 
-void free_dev_layout(DevLayout &D) {
+cudaError_t pool_malloc(void **p, size_t bytes, cudaStream_t st) {
+    *p = nullptr;
+    cudaMemPool_t pool = device_pool();
+    return pool ? cudaMallocFromPoolAsync(p, bytes, pool, st) : cudaMallocAsync(p, bytes, st);
+}
+
+void free_dev_layout(DevLayout &D, cudaStream_t st) {
     void *bufs[] = {D.f_pos,      D.fg_base, D.fb_off, D.fb_deg,   D.vg_base, D.vb_off, D.vb_deg,
                     D.v_ent,      D.ftiles,  D.vtiles, D.fbt_deg,  D.vbt_deg, D.int_of_var, D.f_kind,
                     D.f_deg,      D.fbt_kind, D.f_pq,  D.fbt_pq,   D.prior,   D.vbt_prior};
     for (void *b : bufs)
-        if (b) cudaFree(b);
+        if (b) cudaFreeAsync(b, st);
     D = DevLayout();
 }
 
@@ -490,7 +514,7 @@ int build_layout_device(const flbp_graph_desc &g, const DevGraphIn &in, int prec
         }
     }
 
-    // --- classify, folded log-odds from the host, internal factor order --------------------
+    // --- classify, folded log-odds, internal factor order --------------------
     uint8_t *active = P.get<uint8_t>(F), *hstate = P.get<uint8_t>(F);
     double *fconst = P.get<double>(F);
     uint64_t *fkey = P.get<uint64_t>(F), *fkey2 = P.get<uint64_t>(F);
@@ -499,47 +523,6 @@ int build_layout_device(const flbp_graph_desc &g, const DevGraphIn &in, int prec
     DL_CHECK(P.err);
     DL_CHECK(cudaMemsetAsync(cnt, 0, 4 * sizeof(unsigned long long), st));
     if (F > 0) k_classify<<<grid_for(F), kTPB, 0, st>>>(in, F, active, hstate, fconst, fkey, fidx, cnt);
-    // log-odds of p of every singleton and every factor of one slot, on the host (all threads;
-    // each thread's factors in a contiguous chunk, so the list is in factor order)
-    std::vector<uint32_t> li;
-    std::vector<double> lv;
-    {
-        auto folded_at = [&](int64_t I) {
-            return g.factor_type[I] == FLBP_SINGLETON || g.factor_offsets[I + 1] - g.factor_offsets[I] == 1;
-        };
-        const int nt = F >= (1 << 16) ? std::max(1, omp_get_max_threads()) : 1;
-        std::vector<int64_t> cnt_t((size_t)nt + 1, 0);
-#pragma omp parallel num_threads(nt)
-        {
-            const int t = omp_get_thread_num(), T = omp_get_num_threads();  // T <= nt
-            const int64_t a = F * t / T, b = F * (t + 1) / T;
-            int64_t c = 0;
-            for (int64_t I = a; I < b; I++) c += folded_at(I) ? 1 : 0;
-            cnt_t[(size_t)t + 1] = c;
-#pragma omp barrier
-#pragma omp single
-            {
-                for (int k = 0; k < T; k++) cnt_t[(size_t)k + 1] += cnt_t[(size_t)k];
-                li.resize((size_t)cnt_t[(size_t)T]);
-                lv.resize((size_t)cnt_t[(size_t)T]);
-            }
-            int64_t o = cnt_t[(size_t)t];
-            for (int64_t I = a; I < b; I++)
-                if (folded_at(I)) {
-                    li[(size_t)o] = (uint32_t)I;
-                    lv[(size_t)o] = folded_logit(g.factor_p[I]);
-                    o++;
-                }
-        }
-    }
-    if (!li.empty()) {
-        uint32_t *dli = P.get<uint32_t>(li.size());
-        double *dlv = P.get<double>(lv.size());
-        DL_CHECK(P.err);
-        DL_CHECK(cudaMemcpyAsync(dli, li.data(), li.size() * 4, cudaMemcpyHostToDevice, st));
-        DL_CHECK(cudaMemcpyAsync(dlv, lv.data(), lv.size() * 8, cudaMemcpyHostToDevice, st));
-        k_scatter_logit<<<grid_for(li.size()), kTPB, 0, st>>>(in, dli, dlv, li.size(), hstate, fconst);
-    }
     if (F > 0) DL_CHECK(sort_pairs(fkey, fkey2, fidx, foi, (size_t)F, kFactorKeyBits));
     unsigned long long hc[4];
     DL_CHECK(cudaGetLastError());
@@ -552,10 +535,10 @@ int build_layout_device(const flbp_graph_desc &g, const DevGraphIn &in, int prec
     D.nf_pad = std::max<size_t>(nf, 32ull * ngf);
 
     // --- per-factor arrays, device slots -----------------------------------------------------
-    DL_CHECK(dalloc_out(&D.f_kind, D.nf_pad, D));
-    DL_CHECK(dalloc_out(&D.f_deg, D.nf_pad, D));
-    DL_CHECK(dalloc_out((char **)&D.f_pq, 2 * D.nf_pad * tsz, D));
-    DL_CHECK(dalloc_out(&D.fb_deg, nf_big, D));
+    DL_CHECK(dalloc_out(&D.f_kind, D.nf_pad, D, st));
+    DL_CHECK(dalloc_out(&D.f_deg, D.nf_pad, D, st));
+    DL_CHECK(dalloc_out((char **)&D.f_pq, 2 * D.nf_pad * tsz, D, st));
+    DL_CHECK(dalloc_out(&D.fb_deg, nf_big, D, st));
     DL_CHECK(cudaMemsetAsync(D.f_kind, 0, D.nf_pad, st));
     DL_CHECK(cudaMemsetAsync(D.f_deg, 0, D.nf_pad, st));
     DL_CHECK(cudaMemsetAsync(D.f_pq, 0, 2 * D.nf_pad * tsz, st));
@@ -589,8 +572,8 @@ int build_layout_device(const flbp_graph_desc &g, const DevGraphIn &in, int prec
     DL_CHECK(cudaMemsetAsync(dev_slot, 0xff, std::max<int64_t>(1, E) * 4, st));
     if (nf > 0) k_dev_slot<<<grid_for(nf), kTPB, 0, st>>>(in, foi, nf, nf_sell, gbase, boff, dev_slot);
     // group bases and run offsets as 32-bit arrays, and their host copies
-    DL_CHECK(dalloc_out(&D.fg_base, (size_t)ngf + 1, D));
-    DL_CHECK(dalloc_out(&D.fb_off, (size_t)nf_big + 1, D));
+    DL_CHECK(dalloc_out(&D.fg_base, (size_t)ngf + 1, D, st));
+    DL_CHECK(dalloc_out(&D.fb_off, (size_t)nf_big + 1, D, st));
     k_u64_to_u32<<<grid_for((uint64_t)ngf + 1), kTPB, 0, st>>>(gbase, (uint64_t)ngf + 1, D.fg_base);
     k_u64_to_u32<<<grid_for((uint64_t)nf_big + 1), kTPB, 0, st>>>(boff, (uint64_t)nf_big + 1, D.fb_off);
     L.fg_base.resize((size_t)ngf + 1);
@@ -613,7 +596,7 @@ int build_layout_device(const flbp_graph_desc &g, const DevGraphIn &in, int prec
     uint64_t *vkey = P.get<uint64_t>(V), *vkey2 = P.get<uint64_t>(V);
     uint32_t *vidx = P.get<uint32_t>(V), *order = P.get<uint32_t>(V);
     DL_CHECK(P.err);
-    DL_CHECK(dalloc_out(&D.int_of_var, (size_t)V, D));
+    DL_CHECK(dalloc_out(&D.int_of_var, (size_t)V, D, st));
     DL_CHECK(cudaMemsetAsync(vdeg, 0, std::max<int64_t>(1, V) * 4, st));
     DL_CHECK(cudaMemsetAsync(first, 0xff, std::max<int64_t>(1, V) * 4, st));
     DL_CHECK(cudaMemsetAsync(var_of_dev, 0xff, std::max<uint64_t>(1, n_slots) * 4, st));
@@ -638,7 +621,7 @@ int build_layout_device(const flbp_graph_desc &g, const DevGraphIn &in, int prec
     uint64_t *vgsz = P.get<uint64_t>((size_t)ngv + 1), *vgb = P.get<uint64_t>((size_t)ngv + 1);
     uint64_t *vsz = P.get<uint64_t>((size_t)nv_big + 1), *vbo = P.get<uint64_t>((size_t)nv_big + 1);
     DL_CHECK(P.err);
-    DL_CHECK(dalloc_out(&D.vb_deg, nv_big, D));
+    DL_CHECK(dalloc_out(&D.vb_deg, nv_big, D, st));
     if (ngv > 0) k_group_sizes<<<grid_for(ngv), kTPB, 0, st>>>(nullptr, vdeg, order, nv_sell, ngv, vgsz);
     DL_CHECK(excl_scan(vgsz, vgb, ngv, 0));
     if (nv_big > 0) k_big_var<<<grid_for(nv_big), kTPB, 0, st>>>(order, vdeg, nv_sell, nv_big, D.vb_deg, vsz);
@@ -653,15 +636,15 @@ int build_layout_device(const flbp_graph_desc &g, const DevGraphIn &in, int prec
         return FLBP_ERR_LIMIT;
     }
     D.n_ent = n_ent;
-    DL_CHECK(dalloc_out(&D.vg_base, (size_t)ngv + 1, D));
-    DL_CHECK(dalloc_out(&D.vb_off, (size_t)nv_big + 1, D));
+    DL_CHECK(dalloc_out(&D.vg_base, (size_t)ngv + 1, D, st));
+    DL_CHECK(dalloc_out(&D.vb_off, (size_t)nv_big + 1, D, st));
     k_u64_to_u32<<<grid_for((uint64_t)ngv + 1), kTPB, 0, st>>>(vgb, (uint64_t)ngv + 1, D.vg_base);
     k_u64_to_u32<<<grid_for((uint64_t)nv_big + 1), kTPB, 0, st>>>(vbo, (uint64_t)nv_big + 1, D.vb_off);
     uint32_t *epos = P.get<uint32_t>(V), *estride = P.get<uint32_t>(V);
     DL_CHECK(P.err);
     if (V > 0) k_epos<<<grid_for(V), kTPB, 0, st>>>(D.int_of_var, V, nv_sell, vgb, vbo, epos, estride);
-    DL_CHECK(dalloc_out(&D.v_ent, n_ent, D));
-    DL_CHECK(dalloc_out(&D.f_pos, n_slots, D));
+    DL_CHECK(dalloc_out(&D.v_ent, n_ent, D, st));
+    DL_CHECK(dalloc_out(&D.f_pos, n_slots, D, st));
     k_fill_u32<<<grid_for(n_ent), kTPB, 0, st>>>(D.v_ent, n_ent, kSentinel);
     k_fill_u32<<<grid_for(n_slots), kTPB, 0, st>>>(D.f_pos, n_slots, kSentinel);
     {
@@ -714,7 +697,7 @@ int build_layout_device(const flbp_graph_desc &g, const DevGraphIn &in, int prec
         DL_CHECK(cudaMemsetAsync(cneg, 0, D.nv_pad * 4, st));
         DL_CHECK(cudaMemsetAsync(folded, 0, D.nv_pad, st));
         DL_CHECK(cudaMemsetAsync(fin, 0, D.nv_pad * 8, st));
-        DL_CHECK(dalloc_out((char **)&D.prior, D.nv_pad * psz, D));
+        DL_CHECK(dalloc_out((char **)&D.prior, D.nv_pad * psz, D, st));
         DL_CHECK(cudaMemsetAsync(D.prior, 0, D.nv_pad * psz, st));
         if (F > 0) {
             k_prior_counts<<<grid_for(F), kTPB, 0, st>>>(in, F, active, hstate, fconst, D.int_of_var, cpos, cneg,
@@ -760,7 +743,7 @@ int build_layout_device(const flbp_graph_desc &g, const DevGraphIn &in, int prec
     }
     bt_prior.resize(L.vbt_deg.size() * (psz / 4));
     auto up = [&](auto **dst, const auto &src, size_t n_elems) -> cudaError_t {
-        cudaError_t e = dalloc_out(dst, n_elems, D);
+        cudaError_t e = dalloc_out(dst, n_elems, D, st);
         if (e == cudaSuccess && !src.empty())
             e = cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(src[0]), cudaMemcpyHostToDevice, st);
         return e;

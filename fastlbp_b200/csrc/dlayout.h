@@ -55,7 +55,12 @@ struct DevLayout {
 int build_layout_device(const flbp_graph_desc &g, const DevGraphIn &in, int prec, HostLayout &L, DevLayout &D,
                         std::string &err, cudaStream_t st);
 
-// Frees the buffers of D.
-void free_dev_layout(DevLayout &D);
+// Frees the buffers of D in the order of stream st.
+void free_dev_layout(DevLayout &D, cudaStream_t st);
+
+// Device memory from the per-device pool that engines and layout builds
+// share, ordered on st; freed with cudaFreeAsync, or with cudaFree once no
+// queued work reads it.
+cudaError_t pool_malloc(void **p, size_t bytes, cudaStream_t st);
 
 }  // namespace flbp

@@ -2,6 +2,7 @@
 // CausalBP and host exports. Kernels live in kernels.cuh.
 
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -29,6 +30,7 @@
 #include "adjoint.cuh"
 #include "direct_launch.h"
 #include "dlayout.h"
+#include "logodds.h"
 #include "seq.cuh"
 
 namespace flbp {
@@ -463,7 +465,7 @@ void launch_sweep(flbp_engine *e, int mode, int which = 3) {
                 live_tile_flags_kernel<<<e->sms, 256, 0, e->stream>>>(e->d_ftrange, e->L.n_ftiles, e->d_vtrange,
                                                                       e->L.n_vtiles, e->d_gstate, e->d_act_flag,
                                                                       e->d_act_flag + e->L.n_ftiles, e->d_ctl);
-                cub::CountingInputIterator<uint32_t> it(0);
+                thrust::counting_iterator<uint32_t> it(0);
                 size_t tb = e->cub_tmp_bytes;
                 cub::DeviceSelect::Flagged(e->d_cub_tmp, tb, it, e->d_act_flag, e->d_act_f, &e->d_ctl->n_act_f,
                                            (int)e->L.n_ftiles, e->stream);
@@ -637,11 +639,17 @@ void reset_ctl_for_run(flbp_engine *e, int mode) {
     c.pscale = (e->damping == 0.0) ? 1.0 : 1.0 - std::pow(e->damping, (double)e->t);
 }
 
+// Frees a buffer of dalloc in the order of the engine's stream (work
+// already queued there may still read it).
+inline void dfree(flbp_engine *e, void *p) {
+    if (p) cudaFreeAsync(p, e->stream);
+}
+
 template <typename X>
 int dalloc(flbp_engine *e, X **p, size_t n) {
     *p = nullptr;
     if (n == 0) n = 1;
-    FLBP_CUDA(cudaMalloc((void **)p, n * sizeof(X)));
+    FLBP_CUDA(pool_malloc((void **)p, n * sizeof(X), e->stream));
     e->bytes += n * sizeof(X);
     return FLBP_OK;
 }
@@ -974,7 +982,7 @@ int device_layout(flbp_engine *e, const flbp_graph_desc &g, DevLayout &D) {
     const size_t sz[7] = {F ? (F + 1) * 4 : 0, E * 4, F * 4, F, F * 8, F * 8, any_clamped ? F : 0};
     for (int k = 0; k < 7; k++) {
         if (!sz[k]) continue;
-        FLBP_CUDA(cudaMalloc(&e->d_in[k], sz[k]));
+        FLBP_CUDA(pool_malloc(&e->d_in[k], sz[k], e->stream));
         e->h2d_bytes += sz[k];
     }
     PinnedStage *S = stage_for(e->device);
@@ -1040,7 +1048,7 @@ int device_layout(flbp_engine *e, const flbp_graph_desc &g, DevLayout &D) {
     in.mcode = (const uint8_t *)e->d_in[6];
     rc = build_layout_device(g, in, e->prec, e->L, D, err, e->stream);
     if (rc) {
-        free_dev_layout(D);
+        free_dev_layout(D, e->stream);
         set_error(err);
         return rc;
     }
@@ -1353,7 +1361,7 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
             (rc = dalloc(e, &e->d_act_v, vr.size())) || (rc = dalloc(e, &e->d_act_flag, fr.size() + vr.size())))
             return fail(rc);
         {
-            cub::CountingInputIterator<uint32_t> it(0);
+            thrust::counting_iterator<uint32_t> it(0);
             size_t a = 0, b = 0;
             cub::DeviceSelect::Flagged(nullptr, a, it, e->d_act_flag, e->d_act_f, (unsigned int *)nullptr,
                                        (int)fr.size(), e->stream);
@@ -1638,9 +1646,9 @@ int flbp_run_lowpass(flbp_engine *e, double tol, int64_t min_iters, int64_t max_
     }
     const size_t V = (size_t)e->L.V;
     if ((uint64_t)hist_length > e->hist_cap) {
-        if (e->d_hist) cudaFree(e->d_hist);
-        if (e->d_hist_next) cudaFree(e->d_hist_next);
-        if (e->d_hist_count) cudaFree(e->d_hist_count);
+        dfree(e, e->d_hist);
+        dfree(e, e->d_hist_next);
+        dfree(e, e->d_hist_count);
         e->d_hist = nullptr;
         e->d_hist_next = e->d_hist_count = nullptr;
         e->hist_cap = 0;
@@ -2513,7 +2521,7 @@ void apply_probs_host(flbp_engine *e, const double *p, const double *q) {
     std::fill(L.prior_fin.begin(), L.prior_fin.end(), 0.0);
     for (size_t k = 0; k < L.prior_factor.size(); k++) {
         const double pk = p[L.prior_factor[k]];
-        L.prior_fin[L.prior_var[k]] += L.prior_sign[k] * (std::log(pk) - std::log1p(-pk));
+        L.prior_fin[L.prior_var[k]] += L.prior_sign[k] * det_logit(pk);
     }
     e->host_probs_stale = false;
 }
@@ -2603,7 +2611,7 @@ __global__ void probs_pq_kernel(const double *__restrict__ p, const double *__re
 }
 
 // Finite prior constants of the folded singletons (the sum over a variable's
-// prior entries of sign (log p - log1p(-p)), in entry order) into the
+// prior entries of sign det_logit(p), in entry order) into the
 // engine's prior words, and each entry's d(constant)/dp for the adjoint.
 template <typename T>
 __global__ void probs_prior_kernel(const double *__restrict__ p, const uint32_t *__restrict__ uvar,
@@ -2616,7 +2624,7 @@ __global__ void probs_prior_kernel(const double *__restrict__ p, const uint32_t 
             for (uint32_t j = uoff[i]; j < uoff[i + 1]; j++) {
                 const uint32_t k = ord[j];
                 const double pk = p[pri_fac[k]];
-                s += sign[k] * (log(pk) - log1p(-pk));
+                s += sign[k] * det_logit(pk);
             }
             const uint32_t v = uvar[i];
             if (sizeof(T) == 8) {
@@ -2665,15 +2673,15 @@ int flbp_adjoint_forward(flbp_engine *e, int64_t sweeps, int64_t every, double *
     const size_t nck = (size_t)((sweeps + every - 1) / every);
     const size_t nseg = (size_t)std::min<int64_t>(every, sweeps);
     if (nck > e->adj_ckpt_n) {
-        if (e->d_ckpt) cudaFree(e->d_ckpt);
+        dfree(e, e->d_ckpt);
         e->d_ckpt = nullptr;
         e->adj_ckpt_n = 0;
         if ((rc = dalloc(e, (char **)&e->d_ckpt, nck * ns * e->tsize))) return rc;
         e->adj_ckpt_n = nck;
     }
     if (nseg > e->adj_seg_n) {
-        if (e->d_seg_vf) cudaFree(e->d_seg_vf);
-        if (e->d_seg_fv) cudaFree(e->d_seg_fv);
+        dfree(e, e->d_seg_vf);
+        dfree(e, e->d_seg_fv);
         e->d_seg_vf = e->d_seg_fv = nullptr;
         e->adj_seg_n = 0;
         if ((rc = dalloc(e, (char **)&e->d_seg_vf, nseg * ns * e->tsize)) ||
@@ -3016,7 +3024,7 @@ int flbp_clamp_vars(flbp_engine *e, int64_t n, const int64_t *vars, const int32_
     // the device side: the clamped slots' list, the run state a new engine
     // starts with (previous beliefs 0, for the tolerance rule), the updates
     if (slots.size() > e->clamp_slots_cap) {
-        if (e->d_clamp_slots) cudaFree(e->d_clamp_slots);
+        dfree(e, e->d_clamp_slots);
         e->d_clamp_slots = nullptr;
         e->clamp_slots_cap = 0;
         if ((rc = dalloc(e, &e->d_clamp_slots, 2 * slots.size()))) return rc;
@@ -3131,7 +3139,7 @@ int flbp_sets_create(const flbp_graph_desc *graph, int64_t n_sets, const int64_t
     for (void **b : {(void **)&e->d_vf, (void **)&e->d_fv, (void **)&e->d_fvd, (void **)&e->d_belief,
                      (void **)&e->d_prior, (void **)&e->d_gstate})
         if (*b) {
-            cudaFree(*b);
+            dfree(e, *b);
             *b = nullptr;
         }
     const bool damp = e->damping != 0.0;
@@ -3195,7 +3203,7 @@ void free_seq(flbp_engine *e) {
                     e->d_sq_pq,   e->d_sq_fv,  e->d_sq_vf,    e->d_sq_nw,  e->d_sq_S,    e->d_sq_cnt, e->d_sq_irec,
                     e->d_sq_tvar, e->d_sq_bo};
     for (void *b : bufs)
-        if (b) cudaFree(b);
+        dfree(e, b);
     e->d_sq_foff = e->d_sq_var = e->d_sq_items = e->d_sq_tgt = e->d_sq_iota = nullptr;
     e->d_sq_irec = e->d_sq_tvar = e->d_sq_bo = nullptr;
     e->seq_cluster = false;

@@ -235,10 +235,6 @@ void build_export_maps(HostLayout &L);
 bool classify_factor(const flbp_graph_desc &g, int64_t I, uint8_t &active, uint8_t &head_state, double &fconst,
                      std::string *msg);
 
-// log(p) - log1p(-p): the log-odds of a folded constant (computed on the
-// host by both layout builds, so that they agree bit for bit).
-double folded_logit(double p);
-
 // Tiles and headers of both passes, and the large items' per-tile
 // constants, from L's group bases and large-item runs; big_kind / big_pq:
 // kind and (p, q) of every large factor in internal order.

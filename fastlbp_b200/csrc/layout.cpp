@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "engine_internal.h"
+#include "logodds.h"
 
 namespace flbp {
 
@@ -38,7 +39,7 @@ namespace {
 
 constexpr double kInf = std::numeric_limits<double>::infinity();
 
-inline double logit(double p) { return std::log(p) - std::log1p(-p); }
+inline double logit(double p) { return det_logit(p); }
 
 // Items [0, n) cut into T contiguous chunks (T = 1 for small n), one per
 // parallel iteration, so that per-chunk results combine in index order.
@@ -197,7 +198,6 @@ bool classify_factor(const flbp_graph_desc &g, int64_t I, uint8_t &active, uint8
     return true;
 }
 
-double folded_logit(double p) { return logit(p); }
 
 int check_graph_shape(const flbp_graph_desc &g, std::string &err) {
     const int64_t V = g.n_vars, F = g.n_factors, E = g.n_slots;

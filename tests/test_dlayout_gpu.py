@@ -42,6 +42,16 @@ def _graphs():
     g3.clamp_labels(cl2)
     out["cfg2_clamped"] = g3.rebuild().graph_arrays()
     out["large_items"] = CausalFactorGraph.from_factors(_large_item_graph(3)).graph_arrays()
+    # folded constants of extreme probabilities (0, 1, subnormal, next to 1): both builds take
+    # their log-odds from the same code, so even these give the same bits
+    a = dict(CausalFactorGraph.from_factors(workloads.config0(5)).graph_arrays())
+    deg = np.diff(a["factor_offsets"])
+    folded = np.flatnonzero((a["factor_type"] == workloads.SINGLETON) | (deg == 1))
+    vals = [5e-324, 1e-300, 1e-17, 0.3, 0.5, 1 - 2.0 ** -53, 0.999999, 1e-8, 0.0, 1.0] + [0.9] * 20
+    p = a["factor_p"].copy()
+    p[folded] = np.resize(np.array(vals), folded.size)
+    a["factor_p"] = p
+    out["extreme_p"] = a
     return out
 
 

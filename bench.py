@@ -873,6 +873,10 @@ def run_ours(args, rank, world, local):
                 "frac_event_mode": round(alg[dom] / (per[dom] / 1e3) / 1e9 / peak, 4),
                 "timing": "pass share of the sweep (CUDA events from event nodes of graph-replayed sweeps) x the "
                           "graph-replayed sweep time of the timed steps (CUDA events on the launching stream)",
+                "per_kernel": {k: {"achieved": round(alg[k] / (replay[k] / 1e3) / 1e9, 1),
+                                   "frac": round(alg[k] / (replay[k] / 1e3) / 1e9 / peak, 4),
+                                   "alg_bytes_per_launch": alg[k], "traffic": ncu_traffic().get(k)}
+                               for k in replay},
                 "sweep_ms_graph_replay": round(sweep_ms, 5),
                 "sweep_frac": round((24.0 * E + 16.0 * F + 12.0 * V) / (sweep_ms / 1e3) / 1e9 / peak, 4)}
 

@@ -1,11 +1,11 @@
 // Allocation-free fixed-sweep solve (flbp_run_fixed_device_noalloc).
 //
 // Some callers cannot allocate device memory at the moment they need a solve:
-// code running inside a CUDA stream capture (cudaMalloc is not recorded into
-// a graph and synchronises the device), latency-critical serving loops whose
-// policy forbids allocation after start-up, and hosts whose GPU memory is
-// owned by another allocator (a framework's caching allocator) that does not
-// allow out-of-band cudaMalloc. This entry point lets them run the synchronous
+// latency-critical serving loops whose policy forbids allocation after
+// start-up (cudaMalloc synchronises the device and can stall other work), and
+// hosts whose GPU memory is owned by another allocator (a framework's caching
+// allocator, a plugin host that hands out fixed pools) that does not allow
+// out-of-band cudaMalloc. This entry point lets them run the synchronous
 // sweep with buffers they already own: the graph and the belief output are
 // the caller's device arrays, and the two message arrays live in one
 // file-scope __device__ array of fixed size, held by every GPU that loads the

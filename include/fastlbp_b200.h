@@ -215,10 +215,10 @@ int flbp_autotune(flbp_engine *eng, int32_t kind, int64_t sweeps, double tol, in
 /* ------------------------------------------------------------------------
  * Allocation-free solve. No counterpart in FastLBP.
  *
- * For callers that may not allocate GPU memory when they solve: code running
- * under CUDA stream capture (cudaMalloc cannot be recorded and synchronises
- * the device), serving loops whose policy forbids allocation after start-up,
- * and processes whose GPU memory belongs to another allocator. The caller
+ * For callers that may not allocate GPU memory when they solve: serving
+ * loops whose policy forbids allocation after start-up (cudaMalloc
+ * synchronises the device), and processes or plugin hosts whose GPU memory
+ * belongs to another allocator. The caller
  * passes the graph and the belief output as device arrays it owns; the two
  * message arrays live in a fixed scratch array inside the library (2 x
  * FLBP_NOALLOC_MAX_SLOTS floats = 4 MiB, held by every GPU that loads the

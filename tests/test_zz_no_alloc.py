@@ -1,8 +1,8 @@
 """The allocation-free entry point, flbp_run_fixed_device_noalloc.
 
-It exists for callers that may not allocate GPU memory at solve time (code
-under stream capture, serving loops with a no-allocation policy, processes
-whose GPU memory belongs to another allocator): the graph and the belief
+It exists for callers that may not allocate GPU memory at solve time
+(serving loops with a no-allocation policy, processes whose GPU memory
+belongs to another allocator): the graph and the belief
 output are device arrays the caller owns, and the messages live in the
 library's fixed 4 MiB scratch array. This file runs last so that a failure
 here does not hide the other tests; it passes alone or after them.

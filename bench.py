@@ -855,7 +855,13 @@ def run_ours(args, rank, world, local):
     per = pass_timing(eng, args, flush)
     # Algorithmic bytes per launch (per-unit figures x units): factor pass
     # 12 B per edge slot + 16 B per factor; variable pass 12 B per slot + 12 B per variable.
-    alg = {"factor_pass": 12.0 * E + 16.0 * F, "var_pass": 12.0 * E + 12.0 * V}
+    # Damping mixes every slot's new f->v message with its previous one, so a
+    # damped sweep must also read the previous message of every slot once:
+    # + 4 B per slot, counted in the pass that applies the damping (the
+    # variable pass). The undamped figures are kept beside them.
+    alg_undamped = {"factor_pass": 12.0 * E + 16.0 * F, "var_pass": 12.0 * E + 12.0 * V}
+    damp_bytes = 4.0 * E if args.damping != 0.0 else 0.0
+    alg = {"factor_pass": alg_undamped["factor_pass"], "var_pass": alg_undamped["var_pass"] + damp_bytes}
     dom = max(per, key=per.get)
     peak, peak_kind = peaks()
     traffic = ncu_traffic().get(dom)
@@ -878,7 +884,13 @@ def run_ours(args, rank, world, local):
                                    "alg_bytes_per_launch": alg[k], "traffic": ncu_traffic().get(k)}
                                for k in replay},
                 "sweep_ms_graph_replay": round(sweep_ms, 5),
-                "sweep_frac": round((24.0 * E + 16.0 * F + 12.0 * V) / (sweep_ms / 1e3) / 1e9 / peak, 4)}
+                "sweep_frac": round((24.0 * E + 16.0 * F + 12.0 * V + damp_bytes) / (sweep_ms / 1e3) / 1e9 / peak, 4),
+                "damping_bytes_per_sweep": damp_bytes,
+                "undamped_bytes": {"frac": round(alg_undamped[dom] / (replay[dom] / 1e3) / 1e9 / peak, 4),
+                                   "alg_bytes_per_launch": alg_undamped[dom],
+                                   "sweep_frac": round((24.0 * E + 16.0 * F + 12.0 * V) / (sweep_ms / 1e3) / 1e9 / peak,
+                                                       4),
+                                   "note": "per-unit figures without the previous-message read that damping needs"}}
 
     # End to end through the C ABI with host arrays.
     e2e_ms, h2d, phases = [], 0, []

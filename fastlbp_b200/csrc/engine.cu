@@ -1085,7 +1085,10 @@ void adopt_dev_layout(flbp_engine *e, DevLayout &D) {
 // cost is about the same (largest first, each to the least loaded block;
 // the huge items a block takes first count towards its load). A tile costs
 // its slots plus `per_item` per item (a factor's head and denominators cost
-// more than one slot). Each block's tiles are kept in tile order.
+// more than one slot). Each block's tiles are kept in tile order. With
+// enough tiles, the smallest `tail` of them (one per block) are dealt to no
+// block: they follow the lists as a shared tail (off[nb] .. off[nb + 1]),
+// which the blocks that finish their own tiles first claim one at a time.
 void deal_tiles(const hvec<uint32_t> &hdr, uint32_t n_tiles, uint32_t nb, double per_item,
                 const std::vector<double> &huge_load, std::vector<uint32_t> &list, std::vector<uint32_t> &off) {
     std::vector<std::pair<double, uint32_t>> cost(n_tiles);
@@ -1100,6 +1103,10 @@ void deal_tiles(const hvec<uint32_t> &hdr, uint32_t n_tiles, uint32_t nb, double
     std::priority_queue<Load, std::vector<Load>, std::greater<Load>> q;
     for (uint32_t b = 0; b < nb; b++) q.push({b < huge_load.size() ? huge_load[b] : 0.0, b});
     std::vector<std::vector<uint32_t>> per(nb);
+    const size_t tail = (n_tiles >= 8ull * nb) ? nb : 0;
+    std::vector<uint32_t> shared;
+    for (size_t k = cost.size() - tail; k < cost.size(); k++) shared.push_back(cost[k].second);
+    cost.resize(cost.size() - tail);
     for (const auto &c : cost) {
         Load l = q.top();
         q.pop();
@@ -1114,6 +1121,9 @@ void deal_tiles(const hvec<uint32_t> &hdr, uint32_t n_tiles, uint32_t nb, double
         list.insert(list.end(), p.begin(), p.end());
         off.push_back((uint32_t)list.size());
     }
+    std::sort(shared.begin(), shared.end());
+    list.insert(list.end(), shared.begin(), shared.end());
+    off.push_back((uint32_t)list.size());
     if (list.empty()) list.push_back(0u);
 }
 

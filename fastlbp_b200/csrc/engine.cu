@@ -346,21 +346,26 @@ void launch_seq_sweep(flbp_engine *e, int mode, int which) {
 }
 
 constexpr int kStages = 3;  // bulk-copy pipeline depth of the variable pass (and of the FP64 factor pass)
-// FP32 factor-pass stages are small enough for a fourth with two blocks per SM
-template <typename T>
-constexpr int kFactorStages = sizeof(T) == 4 ? 4 : 3;
+// FP32 factor-pass stages are small enough for a fourth with two blocks per
+// SM, and without the batched solves' per-factor graph (GID false: one
+// graph) for a fifth
+template <typename T, bool GID>
+constexpr int kFactorStages = sizeof(T) == 4 ? (GID ? 4 : 5) : 3;
 constexpr int kBlockThreads = kBlockThreadsDev;  // 16 consumer warps + 1 producer warp
 
-template <typename T>
+template <typename T, bool GID>
 constexpr size_t factor_smem() {
-    return (size_t)kFactorStages<T> * FactorStage<T>::bytes;
+    return (size_t)kFactorStages<T, GID> * FactorStage<T, GID>::bytes;
 }
 
 template <typename T, bool DAMP>
 constexpr size_t var_smem() {
     return (size_t)kStages * VarStage<T, DAMP>::bytes;
 }
-static_assert(factor_smem<double>() <= 227 * 1024, "factor-pass stages exceed shared memory");
+static_assert(factor_smem<double, true>() <= 227 * 1024 && factor_smem<double, false>() <= 227 * 1024,
+              "factor-pass stages exceed shared memory");
+// two blocks per SM (228 KB) with the static shared memory and 1 KB reserved per block
+static_assert(2 * (factor_smem<float, false>() + 6 * 1024) <= 228 * 1024, "single-graph FP32 stages: two blocks per SM");
 static_assert(var_smem<double, true>() <= 227 * 1024, "variable-pass stages exceed shared memory");
 static_assert(kTileGroupsHost == (uint32_t)kTileGroups && kTileSlotsHost == (uint32_t)kTileSlots,
               "host tiling must match the kernels' stage sizes");
@@ -375,7 +380,11 @@ cudaError_t configure_kernels(bool damp, int *fb, int *vb) {
         cudaError_t e2 = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         if (e2 != cudaSuccess) err = e2;
     };
-    set((const void *)factor_pass_kernel<T, kFactorStages<T>>, factor_smem<T>());
+    set((const void *)factor_pass_kernel<T, kFactorStages<T, true>, true>, factor_smem<T, true>());
+    set((const void *)factor_pass_kernel<T, kFactorStages<T, false>, false>, factor_smem<T, false>());
+    if (err == cudaSuccess)  // the single-graph stages fill two blocks' worth of the SM's shared memory
+        err = cudaFuncSetAttribute((const void *)factor_pass_kernel<T, kFactorStages<T, false>, false>,
+                                   cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     set((const void *)var_pass_kernel<T, 0, true, false, kStages>, var_smem<T, false>());
     set((const void *)var_pass_kernel<T, 1, true, false, kStages>, var_smem<T, false>());
     set((const void *)var_pass_kernel<T, 2, true, false, kStages>, var_smem<T, false>());
@@ -385,7 +394,13 @@ cudaError_t configure_kernels(bool damp, int *fb, int *vb) {
     set((const void *)var_pass_kernel<T, 4, true, false, kStages>, var_smem<T, false>());
     set((const void *)var_pass_kernel<T, 4, true, true, kStages>, var_smem<T, true>());
     set((const void *)var_pass_kernel<T, 3, false, false, kStages>, var_smem<T, false>());
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(fb, factor_pass_kernel<T, kFactorStages<T>>, kBlockThreads, factor_smem<T>());
+    // one grid for both kernels: the fewer resident blocks of the two
+    int fb1 = 0, fb2 = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fb1, factor_pass_kernel<T, kFactorStages<T, true>, true>,
+                                                  kBlockThreads, factor_smem<T, true>());
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fb2, factor_pass_kernel<T, kFactorStages<T, false>, false>,
+                                                  kBlockThreads, factor_smem<T, false>());
+    *fb = std::min(fb1, fb2);
     if (damp)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(vb, var_pass_kernel<T, 2, true, true, kStages>, kBlockThreads,
                                                       var_smem<T, true>());
@@ -413,8 +428,12 @@ void launch_factor(flbp_engine *e, const FactorArgs &fa, const void *vf, void *f
                                 e->stream);
         return;
     }
-    factor_pass_kernel<T, kFactorStages<T>><<<e->factor_grid, kBlockThreads, factor_smem<T>(), e->stream>>>(
-        fa, (const T *)vf, (T *)fv, e->d_ctl);
+    if (fa.f_graph)
+        factor_pass_kernel<T, kFactorStages<T, true>, true>
+            <<<e->factor_grid, kBlockThreads, factor_smem<T, true>(), e->stream>>>(fa, (const T *)vf, (T *)fv, e->d_ctl);
+    else
+        factor_pass_kernel<T, kFactorStages<T, false>, false>
+            <<<e->factor_grid, kBlockThreads, factor_smem<T, false>(), e->stream>>>(fa, (const T *)vf, (T *)fv, e->d_ctl);
 }
 
 template <typename T, bool DAMP>

@@ -626,8 +626,10 @@ __device__ bool produce_tiles(const uint4 *thdr, const uint2 *trange, const uint
     return __shfl_sync(0xffffffffu, ok, 0);
 }
 
-// Shared-memory layout of one factor-pass stage.
-template <typename T>
+// Shared-memory layout of one factor-pass stage. Batched solves (GID) also
+// stage the graph of every factor; a single graph's pass has no use for it,
+// and the room it leaves takes a fifth FP32 stage at two blocks per SM.
+template <typename T, bool GID = true>
 struct FactorStage {
     static constexpr size_t hdr = 0;                                   // uint32[kHdrWords]
     static constexpr size_t vbuf = 128;                                // T[kTileSlots]: incoming vf
@@ -636,7 +638,7 @@ struct FactorStage {
     static constexpr size_t kind = deg + kTileItems;                   // uint8[kTileItems]
     static constexpr size_t pq = kind + kTileItems;                    // T[2 * kTileItems]
     static constexpr size_t gid = pq + 2 * sizeof(T) * kTileItems;     // uint32[kTileItems]: graph (batched solves)
-    static constexpr size_t bytes = (gid + 4 * kTileItems + 127) & ~(size_t)127;
+    static constexpr size_t bytes = (gid + (GID ? 4 * kTileItems : 0) + 127) & ~(size_t)127;
 };
 
 // Shared-memory layout of one variable-pass stage.
@@ -977,12 +979,14 @@ __device__ __forceinline__ void sweep_open(Ctl *ctl) {
 // group j, one per lane, or big factor j with the whole warp - and scatters
 // the outputs to fv. Factors too large for a tile are taken first, one per
 // warp, while the producer's first loads are in flight.
-template <typename T, int STAGES>
+// GID: the kernel of batched solves (a.f_graph set), which stages every
+// factor's graph; without it a.f_graph must be null.
+template <typename T, int STAGES, bool GID>
 __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArgs a, const T *__restrict__ vf,
                                                                        T *__restrict__ fv, Ctl *ctl) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES];
-    typedef FactorStage<T> FS;
+    typedef FactorStage<T, GID> FS;
     if (*(volatile int *)&ctl->done) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) sweep_open(ctl);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -1013,12 +1017,13 @@ __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArg
                          2u * kTileGroups * (uint32_t)sizeof(T), bar);
             } else {
                 const uint32_t items = 32u * n;
+                const bool gid = GID && a.f_graph;
                 mbar_arrive_expect_tx(bar, ns * (uint32_t)(sizeof(T) + 4) + 2u * items +
-                                               2u * items * (uint32_t)sizeof(T) + (a.f_graph ? 4u * items : 0u));
+                                               2u * items * (uint32_t)sizeof(T) + (gid ? 4u * items : 0u));
                 bulk_g2s(st + FS::deg, a.f_deg + 32ull * g0, items, bar);
                 bulk_g2s(st + FS::kind, a.f_kind + 32ull * g0, items, bar);
                 bulk_g2s(st + FS::pq, pq_g + 64ull * g0, 2u * items * (uint32_t)sizeof(T), bar);
-                if (a.f_graph) bulk_g2s(st + FS::gid, a.f_graph + 32ull * g0, 4u * items, bar);
+                if (gid) bulk_g2s(st + FS::gid, a.f_graph + 32ull * g0, 4u * items, bar);
             }
             if (ns) {
                 bulk_g2s(st + FS::vbuf, vf + gb[2], ns * (uint32_t)sizeof(T), bar);
@@ -1059,7 +1064,7 @@ __global__ void __launch_bounds__(kBlockThreadsDev) factor_pass_kernel(FactorArg
             const uint32_t base = gb[2 + wid] - gb[2], f = 32u * wid + lane;
             const int w = (int)((gb[3 + wid] - gb[2 + wid]) >> 5);
             int deg = st[FS::deg + f];
-            if (a.f_graph && graph_done(s_done, a.gdone, reinterpret_cast<const uint32_t *>(st + FS::gid)[f]))
+            if (GID && a.f_graph && graph_done(s_done, a.gdone, reinterpret_cast<const uint32_t *>(st + FS::gid)[f]))
                 deg = 0;  // stopped graph
             const T *pq = reinterpret_cast<const T *>(st + FS::pq);
             if (deg > 0)

@@ -97,6 +97,7 @@ struct flbp_engine {
     size_t adj_ckpt_n = 0, adj_seg_n = 0;
     // staged factor pass: each block's tiles (FactorArgs::tile_list / tile_off)
     uint32_t *d_ftlist = nullptr, *d_ftoff = nullptr;
+    uint32_t f_tail_tiles = 0;  // tiles of the staged factor pass's shared tail
     uint32_t *d_int_of_var = nullptr, *d_f_of_int = nullptr;  // caller variable -> internal; internal factor -> caller
     uint32_t *d_pri_fac = nullptr, *d_pri_var = nullptr;      // folded constants: caller factor, internal variable
     double *d_pri_coef = nullptr;                             // their d(constant)/dp
@@ -1407,6 +1408,7 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
         for (uint32_t b = 0; b < L.nf_huge; b++) fh[b % e->factor_grid] += (double)L.fb_deg[b];
         std::vector<uint32_t> fl, fo;
         deal_tiles(L.fhdr, L.n_ftiles, (uint32_t)e->factor_grid, kTileCostFactorItem, fh, fl, fo);
+        e->f_tail_tiles = fo[fo.size() - 1] - fo[fo.size() - 2];
         if ((rc = dalloc(e, &e->d_ftlist, fl.size())) || (rc = upload(e, e->d_ftlist, fl)) ||
             (rc = dalloc(e, &e->d_ftoff, fo.size())) || (rc = upload(e, e->d_ftoff, fo)))
             return fail(rc);
@@ -1906,13 +1908,14 @@ int flbp_engine_stats(flbp_engine *e, int64_t *c, int64_t n) {
         set_error("null argument");
         return FLBP_ERR_INVALID;
     }
-    const int64_t v[18] = {e->L.V, e->L.F, e->L.E, (int64_t)(e->L.nf_sell + e->L.nf_big),
+    const int64_t v[21] = {e->L.V, e->L.F, e->L.E, (int64_t)(e->L.nf_sell + e->L.nf_big),
                            (int64_t)e->L.n_active_slots, (int64_t)e->L.nf_big, (int64_t)e->L.nv_big,
                            (int64_t)e->bytes, (int64_t)e->h2d_bytes, (int64_t)e->launches,
                            (int64_t)e->L.nf_huge, (int64_t)e->L.nv_huge, (int64_t)e->L.n_fbtiles,
                            (int64_t)e->L.n_vbtiles, e->create_us[0], e->create_us[1], e->create_us[2],
-                           e->create_us[3]};
-    for (int64_t i = 0; i < n && i < 18; i++) c[i] = v[i];
+                           e->create_us[3], (int64_t)e->L.n_ftiles, (int64_t)e->L.n_vtiles,
+                           (int64_t)(e->n_graphs ? 0u : e->f_tail_tiles)};  // batched solves claim tiles instead
+    for (int64_t i = 0; i < n && i < 21; i++) c[i] = v[i];
     return FLBP_OK;
 }
 

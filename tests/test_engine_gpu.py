@@ -223,6 +223,33 @@ def test_large_items(prec, damping):
     assert np.max(np.abs(eng.beliefs() - bp.beliefs())) <= TOL[prec]
 
 
+def test_shared_tail_of_factor_tiles():
+    """A graph with at least 8 factor tiles per block of the staged factor
+    pass, so that the smallest tiles form the shared tail that blocks
+    finishing early claim: FP32 damped sweeps within the FP32 tolerance of
+    the FP64 oracle, and a second run split over two run calls (the tail's
+    counters reused by every launch) bit-equal to the first."""
+    fl = workloads.config1(seed=7, scale=0.6)
+    g, og = _pair(fl)
+    eng = Engine.from_graph(g, precision=32, damping=0.1)
+    eng.set_tuning(0, 0)  # the staged forms
+    st = eng.stats()
+    assert st["factor_tiles"] >= 8 * eng.tuning()["factor_blocks"]
+    assert st["factor_tail_tiles"] == eng.tuning()["factor_blocks"]
+    bp = O.OracleBP(og, damping=0.1)
+    bp.init()
+    bp.run_fixed(1e-6, 10, 1)
+    eng.init()
+    eng.run_fixed(10)
+    b1, bo = eng.beliefs(), bp.beliefs()
+    assert np.array_equal(np.isnan(b1), np.isnan(bo))
+    assert np.nanmax(np.abs(b1 - bo)) <= TOL[32]
+    eng.init()
+    eng.run_fixed(4)
+    eng.run_fixed(6)
+    assert np.array_equal(eng.beliefs(), b1, equal_nan=True)
+
+
 def test_fault_localisation_statement_ranking():
     """cfg2 shape at reduced size: tolerance run (tol 1e-6, maxiter 500) in
     FP32 against the FP64 oracle. Beliefs within the FP32 tolerance, and the

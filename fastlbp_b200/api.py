@@ -382,12 +382,12 @@ class Engine:
         return m0, m1
 
     def stats(self) -> Dict[str, int]:
-        c = np.zeros(21, np.int64)
+        c = np.zeros(20, np.int64)
         check(lib().flbp_engine_stats(self._h, c, c.size))
         keys = ["vars", "factors", "slots", "active_factors", "active_slots", "warp_factors", "warp_vars", "bytes",
                 "h2d_bytes", "launches", "huge_factors", "huge_vars", "big_factor_tiles", "big_var_tiles",
                 "create_us_layout", "create_us_alloc", "create_us_upload", "create_us_rest", "factor_tiles",
-                "var_tiles", "factor_tail_tiles"]
+                "var_tiles"]
         return dict(zip(keys, (int(x) for x in c)))
 
     # gradients through unrolled sweeps --------------------------------------

@@ -97,7 +97,6 @@ struct flbp_engine {
     size_t adj_ckpt_n = 0, adj_seg_n = 0;
     // staged factor pass: each block's tiles (FactorArgs::tile_list / tile_off)
     uint32_t *d_ftlist = nullptr, *d_ftoff = nullptr;
-    uint32_t f_tail_tiles = 0;  // tiles of the staged factor pass's shared tail
     uint32_t *d_int_of_var = nullptr, *d_f_of_int = nullptr;  // caller variable -> internal; internal factor -> caller
     uint32_t *d_pri_fac = nullptr, *d_pri_var = nullptr;      // folded constants: caller factor, internal variable
     double *d_pri_coef = nullptr;                             // their d(constant)/dp
@@ -1105,10 +1104,7 @@ void adopt_dev_layout(flbp_engine *e, DevLayout &D) {
 // cost is about the same (largest first, each to the least loaded block;
 // the huge items a block takes first count towards its load). A tile costs
 // its slots plus `per_item` per item (a factor's head and denominators cost
-// more than one slot). Each block's tiles are kept in tile order. With
-// enough tiles, the smallest `tail` of them (one per block) are dealt to no
-// block: they follow the lists as a shared tail (off[nb] .. off[nb + 1]),
-// which the blocks that finish their own tiles first claim one at a time.
+// more than one slot). Each block's tiles are kept in tile order.
 void deal_tiles(const hvec<uint32_t> &hdr, uint32_t n_tiles, uint32_t nb, double per_item,
                 const std::vector<double> &huge_load, std::vector<uint32_t> &list, std::vector<uint32_t> &off) {
     std::vector<std::pair<double, uint32_t>> cost(n_tiles);
@@ -1123,10 +1119,6 @@ void deal_tiles(const hvec<uint32_t> &hdr, uint32_t n_tiles, uint32_t nb, double
     std::priority_queue<Load, std::vector<Load>, std::greater<Load>> q;
     for (uint32_t b = 0; b < nb; b++) q.push({b < huge_load.size() ? huge_load[b] : 0.0, b});
     std::vector<std::vector<uint32_t>> per(nb);
-    const size_t tail = (n_tiles >= 8ull * nb) ? nb : 0;
-    std::vector<uint32_t> shared;
-    for (size_t k = cost.size() - tail; k < cost.size(); k++) shared.push_back(cost[k].second);
-    cost.resize(cost.size() - tail);
     for (const auto &c : cost) {
         Load l = q.top();
         q.pop();
@@ -1141,9 +1133,6 @@ void deal_tiles(const hvec<uint32_t> &hdr, uint32_t n_tiles, uint32_t nb, double
         list.insert(list.end(), p.begin(), p.end());
         off.push_back((uint32_t)list.size());
     }
-    std::sort(shared.begin(), shared.end());
-    list.insert(list.end(), shared.begin(), shared.end());
-    off.push_back((uint32_t)list.size());
     if (list.empty()) list.push_back(0u);
 }
 
@@ -1408,7 +1397,6 @@ int create_engine(const flbp_graph_desc *graph, const flbp_engine_opts *opts, fl
         for (uint32_t b = 0; b < L.nf_huge; b++) fh[b % e->factor_grid] += (double)L.fb_deg[b];
         std::vector<uint32_t> fl, fo;
         deal_tiles(L.fhdr, L.n_ftiles, (uint32_t)e->factor_grid, kTileCostFactorItem, fh, fl, fo);
-        e->f_tail_tiles = fo[fo.size() - 1] - fo[fo.size() - 2];
         if ((rc = dalloc(e, &e->d_ftlist, fl.size())) || (rc = upload(e, e->d_ftlist, fl)) ||
             (rc = dalloc(e, &e->d_ftoff, fo.size())) || (rc = upload(e, e->d_ftoff, fo)))
             return fail(rc);
@@ -1908,14 +1896,13 @@ int flbp_engine_stats(flbp_engine *e, int64_t *c, int64_t n) {
         set_error("null argument");
         return FLBP_ERR_INVALID;
     }
-    const int64_t v[21] = {e->L.V, e->L.F, e->L.E, (int64_t)(e->L.nf_sell + e->L.nf_big),
+    const int64_t v[20] = {e->L.V, e->L.F, e->L.E, (int64_t)(e->L.nf_sell + e->L.nf_big),
                            (int64_t)e->L.n_active_slots, (int64_t)e->L.nf_big, (int64_t)e->L.nv_big,
                            (int64_t)e->bytes, (int64_t)e->h2d_bytes, (int64_t)e->launches,
                            (int64_t)e->L.nf_huge, (int64_t)e->L.nv_huge, (int64_t)e->L.n_fbtiles,
                            (int64_t)e->L.n_vbtiles, e->create_us[0], e->create_us[1], e->create_us[2],
-                           e->create_us[3], (int64_t)e->L.n_ftiles, (int64_t)e->L.n_vtiles,
-                           (int64_t)(e->n_graphs ? 0u : e->f_tail_tiles)};  // batched solves claim tiles instead
-    for (int64_t i = 0; i < n && i < 21; i++) c[i] = v[i];
+                           e->create_us[3], (int64_t)e->L.n_ftiles, (int64_t)e->L.n_vtiles};
+    for (int64_t i = 0; i < n && i < 20; i++) c[i] = v[i];
     return FLBP_OK;
 }
 

@@ -60,10 +60,6 @@ struct Ctl {
     unsigned int fnext, vnext;        // next chunk of tiles of the factor / variable pass (reset by the other pass)
     // batched solves: number of tiles of the factor / variable pass that hold a live graph
     unsigned int n_act_f, n_act_v;
-    // Staged factor pass on one graph: next tile of the shared tail of the
-    // dealt lists, and producers done claiming; the last producer of a
-    // launch to finish sets both back to 0.
-    unsigned int ftail, ftail_done;
 };
 
 template <typename T>
@@ -215,9 +211,7 @@ struct FactorArgs {
     uint32_t n_graphs;        // batched solves: number of graphs
     uint32_t nf_sell, nf_big, nf_huge, n_fgroups, n_tiles, n_tile_blocks;
     // Staged form on one graph: block b's tiles tile_list[tile_off[b] ..
-    // tile_off[b + 1]), then the shared tail tile_list[tile_off[gridDim.x] ..
-    // tile_off[gridDim.x + 1]) claimed through Ctl::ftail (null: tiles b,
-    // b + gridDim.x, ...).
+    // tile_off[b + 1]) (null: tiles b, b + gridDim.x, ...).
     const uint32_t *tile_list = nullptr, *tile_off = nullptr;
     // Staged form of a batched solve: the tiles that hold a live graph,
     // act_list[0 .. *n_act) (null: every tile).
@@ -477,10 +471,8 @@ __device__ __forceinline__ bool graph_done(const uint32_t *s_done, const int *gd
 
 // Producer warp of a pass. A single graph's pass walks the block's own
 // tiles in order: the list the engine dealt it (tile_list / tile_off, tiles
-// of about equal total cost per block, so that all SMs finish together,
-// followed by claims on the shared tail of small tiles, which evens out
-// what the cost model and the tile size leave uneven), or without a list
-// tiles blockIdx.x + i gridDim.x. A batched solve instead takes chunks of kChunkTiles consecutive
+// of about equal total cost per block, so that all SMs finish together), or
+// without a list tiles blockIdx.x + i gridDim.x. A batched solve instead takes chunks of kChunkTiles consecutive
 // tiles from the pass's counter, so that blocks whose tiles belong to stopped
 // graphs take more, and leaves out tiles whose graphs have all stopped. One
 // stage per remaining tile is filled with fill(stage, header in shared
@@ -564,46 +556,6 @@ __device__ bool produce_tiles(const uint4 *thdr, const uint2 *trange, const uint
         __syncwarp();  // s_hdr is rewritten next round
         ok = __shfl_sync(0xffffffffu, ok, 0);
         round = next;
-    }
-    if (listed && tile_off[nb + 1] > tile_off[nb]) {
-        // The shared tail: tiles left out of every block's list, claimed one
-        // at a time by the blocks that reach the end of their own lists
-        // first. Every producer counts itself out once it stops claiming;
-        // the last one sets the counters back to 0 for the next launch.
-        const uint32_t t0 = tile_off[nb], tn = tile_off[nb + 1] - t0;
-        while (ok) {
-            const uint32_t i = __shfl_sync(0xffffffffu, lane == 0 ? atomicAdd(&ctl->ftail, 1u) : 0u, 0);
-            if (i >= tn) break;
-            const uint32_t t = tile_list[t0 + i];
-            if (lane < kHdrWords / 4) {
-                const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&s_hdr[0][lane]);
-                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst),
-                             "l"(thdr + (size_t)(kHdrWords / 4) * t + lane)
-                             : "memory");
-            }
-            asm volatile("cp.async.wait_all;" ::: "memory");
-            __syncwarp();
-            if (lane == 0) {
-                const int s = (int)(issued % STAGES);
-                if (issued >= (uint32_t)STAGES && !mbar_wait_bounded(&empty[s], ((issued / STAGES) - 1) & 1u)) {
-                    ok = false;
-                } else {
-                    unsigned char *st = smem + (size_t)s * stage_bytes;
-                    uint32_t *gb = reinterpret_cast<uint32_t *>(st);
-#pragma unroll
-                    for (int k = 0; k < kHdrWords / 4; k++) reinterpret_cast<uint4 *>(gb)[k] = s_hdr[0][k];
-                    fill(st, gb, &full[s]);
-                    issued++;
-                }
-            }
-            __syncwarp();
-            ok = __shfl_sync(0xffffffffu, ok, 0);
-        }
-        if (lane == 0) __threadfence();  // this producer's last claim before its count
-        if (lane == 0 && atomicAdd(&ctl->ftail_done, 1u) == nb - 1) {
-            atomicExch(&ctl->ftail, 0u);
-            atomicExch(&ctl->ftail_done, 0u);
-        }
     }
     if (lane == 0) {
         if (ok) {  // end marker

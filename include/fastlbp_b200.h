@@ -161,10 +161,8 @@ int flbp_get_vf_messages(flbp_engine *eng, double *m0, double *m1, int64_t n_slo
  * the wall time (microseconds) of create's phases: host layout, device
  * allocation, host->device copies (with their host-side packing), and the
  * rest (device and stream set-up, kernel configuration, initial state),
- * then the tiles of the factor pass, the tiles of the variable pass, and
- * the factor tiles left to the shared tail that blocks finishing early
- * claim (0 below 8 tiles per block). Entries past n_counts are not
- * written. */
+ * then the tiles of the factor pass and the tiles of the variable pass.
+ * Entries past n_counts are not written. */
 int flbp_engine_stats(flbp_engine *eng, int64_t *counts, int64_t n_counts);
 
 /* Per-pass timing mode (for measurement): while enabled, every sweep is

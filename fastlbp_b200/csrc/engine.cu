@@ -135,6 +135,8 @@ struct flbp_engine {
     std::vector<uint32_t> clamp_slots;
     uint32_t *d_clamp_slots = nullptr;
     size_t clamp_slots_cap = 0;
+    uint32_t *d_clamp_upd = nullptr;  // a clamp call's update lists (grow-only)
+    size_t clamp_upd_cap = 0;
     uint8_t *d_f_kind = nullptr, *d_f_deg = nullptr;
     void *d_prior = nullptr;
     double *d_belief = nullptr, *d_lowpass = nullptr, *d_hist = nullptr;
@@ -1522,7 +1524,7 @@ int flbp_engine_destroy(flbp_engine *e) {
                     e->d_fbt_kind, e->d_fbt_pq, e->d_vbt_prior, e->d_f_graph, e->d_v_graph, e->d_gstate, e->d_ftrange, e->d_vtrange,
                     e->d_ckpt, e->d_seg_vf, e->d_seg_fv, e->d_lam, e->d_lam2, e->d_mu, e->d_gp, e->d_gq,
                     e->d_gprior, e->d_gs, e->d_int_of_var, e->d_f_of_int, e->d_pri_fac, e->d_pri_var, e->d_pri_coef,
-                    e->d_adj_in, e->d_adj_out, e->d_adj_groups, e->d_ref_out, e->d_clamp_slots,
+                    e->d_adj_in, e->d_adj_out, e->d_adj_groups, e->d_ref_out, e->d_clamp_slots, e->d_clamp_upd,
                     e->d_sq_foff, e->d_sq_var, e->d_sq_items, e->d_sq_tgt, e->d_sq_iota, e->d_sq_kind,
                     e->d_sq_cst, e->d_sq_pq, e->d_sq_fv, e->d_sq_vf, e->d_sq_nw, e->d_sq_S, e->d_sq_cnt};
     for (void *b : bufs)
@@ -3052,8 +3054,15 @@ int flbp_clamp_vars(flbp_engine *e, int64_t n, const int64_t *vars, const int32_
     if ((rc = upload(e, e->d_clamp_slots, slots)) || (rc = launch_clamp_slots(e, (uint32_t)(slots.size() / 2))))
         return rc;
     FLBP_CUDA(cudaMemsetAsync(e->d_belief, 0, (size_t)std::max<int64_t>(1, L.V) * sizeof(double), e->stream));
-    uint32_t *d = nullptr;
-    FLBP_CUDA(cudaMalloc((void **)&d, (ents.size() + pw.size() + bw.size()) * sizeof(uint32_t)));
+    const size_t n_upd = ents.size() + pw.size() + bw.size();
+    if (n_upd > e->clamp_upd_cap) {  // kept between calls: no allocation per label in a labelling loop
+        dfree(e, e->d_clamp_upd);
+        e->d_clamp_upd = nullptr;
+        e->clamp_upd_cap = 0;
+        if ((rc = dalloc(e, &e->d_clamp_upd, 2 * n_upd))) return rc;
+        e->clamp_upd_cap = 2 * n_upd;
+    }
+    uint32_t *d = e->d_clamp_upd;
     cudaError_t ce = cudaSuccess;
     auto put = [&](const std::vector<uint32_t> &v, size_t at) {
         if (!v.empty() && ce == cudaSuccess)
@@ -3077,7 +3086,6 @@ int flbp_clamp_vars(flbp_engine *e, int64_t n, const int64_t *vars, const int32_
         ce = cudaGetLastError();
     }
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
-    cudaFree(d);
     if (ce != cudaSuccess) {
         set_error(std::string("clamp update failed: ") + cudaGetErrorString(ce));
         return FLBP_ERR_CUDA;
